@@ -1,0 +1,236 @@
+// Encode driver (Core/idx2Encode.cpp:276-444).
+#include "encoder.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <errno.h>
+#include <functional>
+#include <sys/stat.h>
+#include <unordered_map>
+
+namespace idx2g
+{
+
+static uint32_t spread3(uint32_t x)
+{
+  uint32_t r = 0;
+  for (int i = 0; i < 10; ++i)
+    r |= ((x >> i) & 1u) << (3 * i);
+  return r;
+}
+static uint32_t compact3(uint32_t c)
+{
+  uint32_t r = 0;
+  for (int i = 0; i < 10; ++i)
+    r |= ((c >> (3 * i)) & 1u) << i;
+  return r;
+}
+
+void subband_blocks(const dataset_format& f, int level, int sb, std::vector<block_geom>* out)
+{
+  out->clear();
+  const subband& s = f.subbands[(size_t)sb];
+  v3 nb = (s.g.dims + f.block_dims - v3(1)) / f.block_dims;
+  uint32_t last = spread3((uint32_t)nb.x - 1) | (spread3((uint32_t)nb.y - 1) << 1) |
+                  (spread3((uint32_t)nb.z - 1) << 2);
+  for (uint32_t b = 0; b <= last; ++b)
+  {
+    v3 z3((int)compact3(b), (int)compact3(b >> 1), (int)compact3(b >> 2));
+    if (!all_lt(z3, nb))
+    {
+      // Core/idx2Common.h:23 idx2_NextMorton
+      int lsb = __builtin_ctz(b);
+      b = (((b >> (lsb + 1)) + 1) << (lsb + 1)) - 1;
+      continue;
+    }
+    v3 d3 = z3 * f.block_dims;
+    v3 bd = vmin(f.block_dims, s.g.dims - d3);
+    bool coded_next = sb == 0 && level + 1 < f.nlevels && bd == f.block_dims;
+    if (coded_next)
+      continue;
+    block_geom g;
+    g.dx = (uint8_t)z3.x;
+    g.dy = (uint8_t)z3.y;
+    g.dz = (uint8_t)z3.z;
+    g.bx = (uint8_t)bd.x;
+    g.by = (uint8_t)bd.y;
+    g.bz = (uint8_t)bd.z;
+    g.code = (uint16_t)b;
+    out->push_back(g);
+  }
+}
+
+int make_encode_plan(const dataset_format& f, encode_plan* plan)
+{
+  const int L = f.nlevels;
+  plan->levels.assign((size_t)L, {});
+  plan->events.clear();
+  // parents under construction: key (level, linear) -> entry + children waiting
+  struct pending
+  {
+    brick_entry e;
+    int ndone = 0;
+    std::vector<std::pair<int, int>> children;  // (level, index)
+  };
+  std::vector<std::unordered_map<u64, pending>> pool((size_t)L);
+  const v3 sb_nonext = v3(f.subbands[0].g.dims.x - (f.subbands[0].g.dims.x > 1),
+                          f.subbands[0].g.dims.y - (f.subbands[0].g.dims.y > 1),
+                          f.subbands[0].g.dims.z - (f.subbands[0].g.dims.z > 1));
+
+  std::function<void(int, int)> encode_brick = [&](int level, int idx) {
+    for (int sb = 0; sb < f.nsubbands(); ++sb)
+    {
+      if (sb == 0 && level + 1 < L)
+      {
+        brick_entry& me = plan->levels[(size_t)level][(size_t)idx];
+        v3 pb3 = me.brick3 / f.group_brick3;
+        u64 plin = linear_brick(f, level + 1, pb3);
+        auto& pm = pool[(size_t)level + 1];
+        auto it = pm.find(plin);
+        if (it == pm.end())
+        {
+          pending p;
+          p.e.brick3 = pb3;
+          p.e.linear = plin;
+          v3 from3 = pb3 * f.group_brick3;
+          extent c = crop(extent{ from3, f.group_brick3 }, extent{ v3(0), f.nbricks3[(size_t)level] });
+          p.e.nchildren = (int)prod(c.dims);
+          p.e.valid = c.dims * sb_nonext;
+          it = pm.emplace(plin, p).first;
+        }
+        me.pos_in_parent = me.brick3 % f.group_brick3;
+        it->second.children.push_back({ level, idx });
+        if (++it->second.ndone == it->second.e.nchildren)
+        {
+          int pidx = (int)plan->levels[(size_t)level + 1].size();
+          plan->levels[(size_t)level + 1].push_back(it->second.e);
+          for (auto& ch : it->second.children)
+            plan->levels[(size_t)ch.first][(size_t)ch.second].parent = pidx;
+          pm.erase(it);
+          encode_brick(level + 1, pidx);
+        }
+      }
+      plan->events.push_back({ level, idx, sb });
+    }
+  };
+
+  const v3 nb0 = f.nbricks3[0];
+  extent all{ v3(0), nb0 };
+  traverse(f.bricks_order[0], v3(0), nb0, all, all, [&](const traverse_item& t) {
+    brick_entry e;
+    e.brick3 = t.from3;
+    e.linear = linear_brick(f, 0, t.from3);
+    extent be{ t.from3 * f.brick_dims, f.brick_dims };
+    extent c = crop(be, extent{ v3(0), f.dims });
+    e.valid = c.dims;
+    int idx = (int)plan->levels[0].size();
+    plan->levels[0].push_back(e);
+    encode_brick(0, idx);
+  });
+  for (int l = 1; l < L; ++l)
+    if (!pool[(size_t)l].empty())
+      return UnknownError;
+  return NoError;
+}
+
+int make_dirs_for(const std::string& path)
+{
+  size_t pos = 0;
+  while ((pos = path.find('/', pos + 1)) != std::string::npos)
+  {
+    std::string d = path.substr(0, pos);
+    if (d.empty())
+      continue;
+    if (mkdir(d.c_str(), 0755) != 0 && errno != EEXIST)
+      return CannotCreateDirectory;
+  }
+  return NoError;
+}
+
+int write_file(const std::string& path, const std::vector<uint8_t>& data)
+{
+  if (make_dirs_for(path) != NoError)
+    return CannotCreateDirectory;
+  FILE* fp = fopen(path.c_str(), "wb");
+  if (!fp)
+    return FileCreateFailed;
+  size_t n = data.empty() ? 0 : fwrite(data.data(), 1, data.size(), fp);
+  fclose(fp);
+  return n == data.size() ? NoError : FileWriteFailed;
+}
+
+static double now_s()
+{
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
+                   std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
+                   encode_timing* timing)
+{
+  encode_plan plan;
+  int e = make_encode_plan(*f, &plan);
+  if (e)
+    return e;
+  double t0 = now_s();
+  std::vector<level_output> outs((size_t)f->nlevels);
+  for (int l = 0; l < f->nlevels; ++l)
+  {
+    e = coder->run_level(l, plan, &outs[(size_t)l]);
+    if (e)
+      return e;
+  }
+  coder->value_range(&f->value_min, &f->value_max);
+  double t1 = now_s();
+
+  packer pk(*f, f->tolerance);
+  for (const encode_event& ev : plan.events)
+  {
+    const level_output& o = outs[(size_t)ev.level];
+    size_t bs = (size_t)ev.brick * (size_t)o.nsb + (size_t)ev.subband;
+    subband_result r;
+    r.level = ev.level;
+    r.brick = plan.levels[(size_t)ev.level][(size_t)ev.brick].linear;
+    r.subband = ev.subband;
+    r.exps = o.exps.data() + bs * kMaxBlocksPerSubband;
+    r.nexps = o.nexps[(size_t)ev.subband];
+    r.kmin = o.kmin[bs];
+    r.kmax = o.kmax[bs];
+    r.sizes = o.sizes.data() + bs * kKeyWindow;
+    r.bytes = o.stream.data() + o.offset[bs];
+    e = pk.add(r);
+    if (e)
+      return e;
+  }
+  e = pk.finish();
+  if (e)
+    return e;
+  double t2 = now_s();
+
+  files->clear();
+  for (auto& kv : pk.files())
+    (*files)[kv.first] = std::move(kv.second.data);
+  std::string meta = meta_text(*f, *p) + pk.stats_text();
+  std::string meta_path = p->out_dir + "/" + p->name + "/" + p->field + ".idx2";
+  (*files)[meta_path] = std::vector<uint8_t>(meta.begin(), meta.end());
+  if (write_files)
+  {
+    for (auto& kv : *files)
+    {
+      e = write_file(kv.first, kv.second);
+      if (e)
+        return e;
+    }
+  }
+  double t3 = now_s();
+  if (timing)
+  {
+    timing->device_s = t1 - t0;
+    timing->pack_s = t2 - t1;
+    timing->write_s = t3 - t2;
+  }
+  return NoError;
+}
+
+} // namespace idx2g

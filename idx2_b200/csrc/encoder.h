@@ -1,0 +1,98 @@
+// Encode driver: the order in which the reference encodes bricks and subbands,
+// the level-by-level device stage, and the final packing into files.
+//
+// The reference encodes depth-first: for every level-0 brick in traversal order
+// it transforms the brick, and while emitting subband 0 it hands the low band to
+// the parent, encoding the parent as soon as its last child arrives
+// (Core/idx2Encode.cpp:276-340, :395-426).  Here the same recursion only fixes the
+// ORDER: the device stage transforms and codes all bricks of one level at once,
+// and the packer replays the (level, brick, subband) events afterwards.
+#pragma once
+
+#include "format.h"
+#include "packer.h"
+
+#include <map>
+#include <string>
+#include <vector>
+
+namespace idx2g
+{
+
+struct brick_entry
+{
+  v3 brick3;           // brick coordinates on its level
+  u64 linear = 0;      // GetLinearBrick
+  v3 valid;            // ExtentLocal dims: valid samples inside the 32^3 brick
+  int parent = -1;     // index of the parent in the next level's list
+  v3 pos_in_parent;    // LocalBrickPos3
+  int nchildren = 0;   // for parents: NChildrenMax
+};
+
+struct encode_event
+{
+  int level, brick, subband;
+};
+
+struct encode_plan
+{
+  std::vector<std::vector<brick_entry>> levels;  // per level, in encode order
+  std::vector<encode_event> events;              // EncodeSubband calls in order
+};
+
+int make_encode_plan(const dataset_format& f, encode_plan* plan);
+
+// Block geometry of one subband: the coded blocks in the reference's Morton walk
+// (Core/idx2Encode.cpp:157-174), packed as d3 (offset / 4) and block dims.
+struct block_geom
+{
+  uint8_t dx, dy, dz;  // block offset in units of 4 samples
+  uint8_t bx, by, bz;  // block dims (1..4)
+  uint16_t code;       // Morton code
+};
+// Geometry of the coded blocks of subband sb at a level; skips CodedInNextLevel blocks.
+void subband_blocks(const dataset_format& f, int level, int sb, std::vector<block_geom>* out);
+
+// Coder output of one level, in host memory.
+constexpr int kMaxBlocksPerSubband = 128;  // >= 125 (5^3)
+constexpr int kKeyWindow = 128;            // channel keys per (brick, subband)
+
+struct level_output
+{
+  int nbricks = 0, nsb = 0;
+  std::vector<int> nexps;        // per subband (identical for every brick of the level)
+  std::vector<int16_t> exps;     // [brick][sb][kMaxBlocksPerSubband]
+  std::vector<int32_t> kmin;     // [brick][sb]
+  std::vector<int32_t> kmax;     // [brick][sb]
+  std::vector<uint64_t> offset;  // [brick][sb] byte offset of the channel streams
+  std::vector<uint32_t> sizes;   // [brick][sb][kKeyWindow]
+  std::vector<uint8_t> stream;
+};
+
+// A device (or test) stage that transforms and codes every brick of a level.
+class brick_coder
+{
+public:
+  virtual ~brick_coder() = default;
+  // Runs level `level` for `bricks` (encode order). Level 0 reads the input field;
+  // level > 0 reads the parent bricks assembled by the previous level's run.
+  virtual int run_level(int level, const encode_plan& plan, level_output* out) = 0;
+  // min / max over the input field (valid after level 0)
+  virtual void value_range(double* vmin, double* vmax) = 0;
+};
+
+struct encode_timing
+{
+  double device_s = 0, pack_s = 0, write_s = 0;
+};
+
+// Full encode: plan, device stage for every level, packing, files (Core/idx2Encode.cpp:390).
+// files receives path -> bytes; write_files controls whether they are written to disk.
+int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
+                   std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
+                   encode_timing* timing);
+
+int write_file(const std::string& path, const std::vector<uint8_t>& data);
+int make_dirs_for(const std::string& path);
+
+} // namespace idx2g

@@ -1,0 +1,209 @@
+// Test driver: runs the library's encode plan and packer (host C++) with the
+// oracle's CPU brick coder as the device stage, so that the packing logic can
+// be compared with the reference's files on a machine without a GPU.
+// Built and run by tests/test_packer_cpu.py.
+//
+//   oracle_encode <raw> <nx> <ny> <nz> <float32|float64> <levels> <tol> <out_dir>
+//                 <name> <field> [bx by bz] [bricks_per_chunk chunks_per_file files_per_dir]
+#include "encoder.h"
+#include "format.h"
+
+extern "C"
+{
+#include "idx2_oracle.h"
+}
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+using namespace idx2g;
+
+namespace
+{
+
+class oracle_coder : public brick_coder
+{
+public:
+  oracle_coder(const dataset_format& f, const void* field) : f_(f), field_(field) {}
+
+  int run_level(int level, const encode_plan& plan, level_output* out) override
+  {
+    const bool is2d = f_.is2d();
+    const int NB = 33 * 33 * (is2d ? 1 : 33);
+    const std::vector<brick_entry>& bricks = plan.levels[(size_t)level];
+    const int nsb = f_.nsubbands();
+    const int L = f_.nlevels;
+    if (level + 1 < L)
+      next_.assign(plan.levels[(size_t)level + 1].size() * (size_t)NB, 0.0);
+    out->nbricks = (int)bricks.size();
+    out->nsb = nsb;
+    out->nexps.assign((size_t)nsb, 0);
+    out->exps.assign(bricks.size() * (size_t)nsb * kMaxBlocksPerSubband, 0);
+    out->kmin.assign(bricks.size() * (size_t)nsb, 1);
+    out->kmax.assign(bricks.size() * (size_t)nsb, 0);
+    out->offset.assign(bricks.size() * (size_t)nsb, 0);
+    out->sizes.assign(bricks.size() * (size_t)nsb * kKeyWindow, 0);
+    out->stream.clear();
+    std::vector<double> buf((size_t)NB);
+    std::vector<uint8_t> rec(1 << 24);
+    for (size_t bi = 0; bi < bricks.size(); ++bi)
+    {
+      const brick_entry& b = bricks[bi];
+      if (level == 0)
+      {
+        std::fill(buf.begin(), buf.end(), 0.0);
+        v3 from = b.brick3 * f_.brick_dims;
+        for (int z = 0; z < b.valid.z; ++z)
+          for (int y = 0; y < b.valid.y; ++y)
+            for (int x = 0; x < b.valid.x; ++x)
+            {
+              size_t src = ((size_t)(from.z + z) * (size_t)f_.dims.y + (size_t)(from.y + y)) *
+                             (size_t)f_.dims.x +
+                           (size_t)(from.x + x);
+              double v = f_.type == dtype::float32 ? (double)((const float*)field_)[src]
+                                                   : ((const double*)field_)[src];
+              buf[((size_t)z * 33 + (size_t)y) * 33 + (size_t)x] = v;
+              vmin_ = v < vmin_ ? v : vmin_;
+              vmax_ = vmax_ < v ? v : vmax_;
+            }
+      }
+      else
+      {
+        std::copy(cur_.begin() + (long)(bi * (size_t)NB), cur_.begin() + (long)((bi + 1) * (size_t)NB),
+                  buf.begin());
+      }
+      int valid[3] = { b.valid.x, b.valid.y, b.valid.z };
+      oracle_brick_forward(buf.data(), is2d, valid, level, level + 1 == L);
+      if (level + 1 < L)
+      {
+        int pos[3] = { b.pos_in_parent.x, b.pos_in_parent.y, b.pos_in_parent.z };
+        oracle_copy_to_parent(buf.data(), next_.data() + (size_t)b.parent * (size_t)NB, is2d, pos);
+      }
+      long n = oracle_encode_brick(buf.data(), is2d, level, L, f_.type == dtype::float32, f_.tolerance,
+                                   f_.bit_planes_per_chunk, rec.data(), (long)rec.size());
+      if (n < 0)
+        return UnknownError;
+      const uint8_t* p = rec.data();
+      for (int s = 0; s < nsb; ++s)
+      {
+        size_t bs = bi * (size_t)nsb + (size_t)s;
+        int32_t ne;
+        memcpy(&ne, p, 4);
+        p += 4;
+        out->nexps[(size_t)s] = ne;
+        memcpy(out->exps.data() + bs * kMaxBlocksPerSubband, p, 2 * (size_t)ne);
+        p += 2 * (size_t)ne;
+        int32_t nch;
+        memcpy(&nch, p, 4);
+        p += 4;
+        struct ch
+        {
+          int key, nbytes;
+          const uint8_t* data;
+        };
+        std::vector<ch> chs;
+        for (int c = 0; c < nch; ++c)
+        {
+          int32_t key, fb, lb, nbytes;
+          memcpy(&key, p, 4);
+          memcpy(&fb, p + 4, 4);
+          memcpy(&lb, p + 8, 4);
+          memcpy(&nbytes, p + 12, 4);
+          p += 16;
+          chs.push_back({ key, nbytes, p });
+          p += nbytes;
+        }
+        if (chs.empty())
+          continue;
+        int kmin = 1 << 30, kmax = -1;
+        for (auto& c : chs)
+        {
+          kmin = c.key < kmin ? c.key : kmin;
+          kmax = c.key > kmax ? c.key : kmax;
+        }
+        if (kmax - kmin + 1 > kKeyWindow)
+          return DeviceStreamOverflow;
+        out->kmin[bs] = kmin;
+        out->kmax[bs] = kmax;
+        out->offset[bs] = out->stream.size();
+        std::sort(chs.begin(), chs.end(), [](const ch& a, const ch& b) { return a.key < b.key; });
+        for (auto& c : chs)
+        {
+          out->sizes[bs * kKeyWindow + (size_t)(c.key - kmin)] = (uint32_t)c.nbytes;
+          out->stream.insert(out->stream.end(), c.data, c.data + c.nbytes);
+        }
+      }
+    }
+    cur_.swap(next_);
+    return NoError;
+  }
+
+  void value_range(double* vmin, double* vmax) override
+  {
+    *vmin = vmin_;
+    *vmax = vmax_;
+  }
+
+private:
+  const dataset_format& f_;
+  const void* field_;
+  std::vector<double> cur_, next_;
+  double vmin_ = 1.7976931348623157e308, vmax_ = -1.7976931348623157e308;
+};
+
+} // namespace
+
+int main(int argc, char** argv)
+{
+  if (argc < 11)
+  {
+    fprintf(stderr, "usage: oracle_encode raw nx ny nz dtype levels tol out_dir name field [bx by bz] "
+                    "[bricks_per_chunk chunks_per_file files_per_dir]\n");
+    return 2;
+  }
+  params p;
+  p.dims = v3(atoi(argv[2]), atoi(argv[3]), atoi(argv[4]));
+  p.type = strcmp(argv[5], "float32") == 0 ? dtype::float32 : dtype::float64;
+  p.num_levels = atoi(argv[6]);
+  p.tolerance = atof(argv[7]);
+  p.out_dir = argv[8];
+  p.name = argv[9];
+  p.field = argv[10];
+  if (argc >= 14)
+    p.brick_dims = v3(atoi(argv[11]), atoi(argv[12]), atoi(argv[13]));
+  if (argc >= 17)
+  {
+    p.bricks_per_chunk = atoi(argv[14]);
+    p.chunks_per_file = atoi(argv[15]);
+    p.files_per_dir = atoi(argv[16]);
+  }
+  dataset_format f;
+  int e = finalize(&f, &p);
+  if (e)
+  {
+    fprintf(stderr, "finalize error %d\n", e);
+    return 10 + e;
+  }
+  size_t n = (size_t)prod(p.dims);
+  size_t es = p.type == dtype::float32 ? 4 : 8;
+  std::vector<uint8_t> raw(n * es);
+  FILE* fp = fopen(argv[1], "rb");
+  if (!fp || fread(raw.data(), 1, raw.size(), fp) != raw.size())
+  {
+    fprintf(stderr, "cannot read %s\n", argv[1]);
+    return 3;
+  }
+  fclose(fp);
+  oracle_coder coder(f, raw.data());
+  std::map<std::string, std::vector<uint8_t>> files;
+  e = encode_dataset(&f, &p, &coder, &files, true, nullptr);
+  if (e)
+  {
+    fprintf(stderr, "encode error %d\n", e);
+    return 10 + e;
+  }
+  return 0;
+}
