@@ -1,0 +1,273 @@
+// C ABI of the library (include/idx2g.h).
+#include "../../include/idx2g.h"
+
+#include "decoder.h"
+#include "device.h"
+#include "encoder.h"
+#include "format.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+using namespace idx2g;
+
+struct idx2g_ctx
+{
+  device_ctx d;
+};
+
+namespace
+{
+
+void to_params(const idx2g_params* in, params* p)
+{
+  p->name = in->name;
+  p->field = in->field;
+  p->dims = v3(in->dims[0], in->dims[1], in->dims[2]);
+  p->type = in->dtype == IDX2G_FLOAT32 ? dtype::float32 : dtype::float64;
+  p->brick_dims = v3(in->brick_dims[0], in->brick_dims[1], in->brick_dims[2]);
+  p->num_levels = in->num_levels;
+  p->tolerance = in->tolerance;
+  p->bricks_per_chunk = in->bricks_per_chunk;
+  p->chunks_per_file = in->chunks_per_file;
+  p->files_per_dir = in->files_per_dir;
+  p->bit_planes_per_chunk = in->bit_planes_per_chunk;
+  p->bit_planes_per_file = in->bit_planes_per_file;
+  p->version[0] = in->version[0];
+  p->version[1] = in->version[1];
+  p->out_dir = in->out_dir[0] ? in->out_dir : ".";
+  p->input_file = in->input_file;
+  p->in_dir = in->in_dir[0] ? in->in_dir : ".";
+  p->has_extent = in->has_extent != 0;
+  if (p->has_extent)
+  {
+    v3 f(in->first[0], in->first[1], in->first[2]);
+    v3 l(in->last[0], in->last[1], in->last[2]);
+    p->decode_extent.from = f;
+    p->decode_extent.dims = l - f + v3(1);
+  }
+  p->downsampling = v3(in->downsampling[0], in->downsampling[1], in->downsampling[2]);
+  p->decode_tolerance = in->decode_tolerance;
+}
+
+} // namespace
+
+extern "C"
+{
+
+IDX2G_API void idx2g_params_init(idx2g_params* p)
+{
+  memset(p, 0, sizeof *p);
+  p->dtype = IDX2G_FLOAT64;
+  p->brick_dims[0] = p->brick_dims[1] = p->brick_dims[2] = 32;
+  p->bricks_per_chunk = 4096;
+  p->chunks_per_file = 64;
+  p->files_per_dir = 64;
+  p->bit_planes_per_chunk = 1;
+  p->bit_planes_per_file = 16;
+  p->version[0] = 1;
+  p->version[1] = 0;
+  strcpy(p->out_dir, ".");
+  strcpy(p->in_dir, ".");
+}
+
+IDX2G_API const char* idx2g_error_string(int code)
+{
+  static const char* names[] = { "NoError", "UnknownError", "SizeZero", "SizeTooSmall",
+                                 "SizeMismatched", "DimensionMismatched", "DimensionsTooMany",
+                                 "AttributeNotFound", "OptionNotSupported", "TypeNotSupported",
+                                 "FileCreateFailed", "FileReadFailed", "FileWriteFailed",
+                                 "FileOpenFailed", "FileCloseFailed", "FileSeekFailed",
+                                 "FileTellFailed", "ParseFailed", "OutOfMemory", "DimensionsRepeated",
+                                 "DimensionTooSmall", "BrickSizeNotPowerOfTwo", "BrickSizeTooBig",
+                                 "TooManyLevels", "TooManyTransformPassesPerLevel",
+                                 "TooManyLevelsOrTransformPasses", "TooManyBricksPerFile",
+                                 "TooManyFilesPerDir", "NotSupportedInVersion",
+                                 "CannotCreateDirectory", "SyntaxError", "TooManyBricksPerChunk",
+                                 "TooManyChunksPerFile", "ChunksPerFileNotPowerOf2",
+                                 "BricksPerChunkNotPowerOf2", "ChunkNotFound", "BrickNotFound",
+                                 "FileNotFound", "UnsupportedScheme" };
+  if (code >= 0 && code < (int)(sizeof names / sizeof names[0]))
+    return names[code];
+  switch (code)
+  {
+    case CudaError:
+      return "CudaError";
+    case InvalidArgument:
+      return "InvalidArgument";
+    case DeviceStreamOverflow:
+      return "DeviceStreamOverflow";
+    case CorruptStream:
+      return "CorruptStream";
+    default:
+      return "Unknown";
+  }
+}
+
+IDX2G_API const char* idx2g_version(void) { return "idx2g 0.1 (sm_100a)"; }
+
+IDX2G_API int idx2g_ctx_create(int device, void* stream, idx2g_ctx** out)
+{
+  if (!out)
+    return InvalidArgument;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0)
+    return CudaError;
+  if (cudaSetDevice(device) != cudaSuccess)
+    return CudaError;
+  idx2g_ctx* c = new (std::nothrow) idx2g_ctx;
+  if (!c)
+    return OutOfMemory;
+  c->d.device = device;
+  cudaDeviceGetAttribute(&c->d.num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (stream)
+  {
+    c->d.stream = (cudaStream_t)stream;
+    c->d.own_stream = false;
+  }
+  else
+  {
+    if (cudaStreamCreateWithFlags(&c->d.stream, cudaStreamNonBlocking) != cudaSuccess)
+    {
+      delete c;
+      return CudaError;
+    }
+    c->d.own_stream = true;
+  }
+  *out = c;
+  return NoError;
+}
+
+IDX2G_API int idx2g_ctx_destroy(idx2g_ctx* c)
+{
+  if (!c)
+    return NoError;
+  if (c->d.own_stream && c->d.stream)
+    cudaStreamDestroy(c->d.stream);
+  delete c;
+  return NoError;
+}
+
+IDX2G_API int idx2g_check_params(const idx2g_params* in)
+{
+  if (!in)
+    return InvalidArgument;
+  params p;
+  to_params(in, &p);
+  dataset_format f;
+  return finalize(&f, &p);
+}
+
+IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* field,
+                           int field_on_device, idx2g_encode_info* info)
+{
+  if (!c || !in || !field)
+    return InvalidArgument;
+  cudaSetDevice(c->d.device);
+  params p;
+  to_params(in, &p);
+  dataset_format f;
+  int e = finalize(&f, &p);
+  if (e)
+    return e;
+  const bool f32 = p.type == dtype::float32;
+  const size_t bytes = (size_t)prod(p.dims) * (f32 ? 4 : 8);
+  auto t0 = std::chrono::steady_clock::now();
+  const void* d_field = field;
+  void* owned = nullptr;
+  if (!field_on_device)
+  {
+    if (cudaMalloc(&owned, bytes) != cudaSuccess)
+      return OutOfMemory;
+    cudaMemcpyAsync(owned, field, bytes, cudaMemcpyHostToDevice, c->d.stream);
+    d_field = owned;
+  }
+  std::map<std::string, std::vector<uint8_t>> files;
+  encode_timing tm;
+  long long stream_bytes = 0, exp_bytes = 0;
+  double kms = 0;
+  long long launches = 0;
+  {
+    gpu_coder coder(&c->d, f, d_field, f32);
+    e = encode_dataset(&f, &p, &coder, &files, true, &tm);
+    stream_bytes = coder.stream_bytes();
+    exp_bytes = coder.exp_bytes();
+    kms = coder.kernel_ms();
+    launches = coder.kernel_launches();
+  }
+  if (owned)
+    cudaFree(owned);
+  if (e)
+    return e;
+  auto t1 = std::chrono::steady_clock::now();
+  (void)t0;
+  (void)t1;
+  if (info)
+  {
+    memset(info, 0, sizeof *info);
+    info->kernel_ms = kms;
+    info->device_s = tm.device_s;
+    info->pack_s = tm.pack_s;
+    info->write_s = tm.write_s;
+    info->stream_bytes = stream_bytes;
+    info->exp_bytes = exp_bytes;
+    long long fb = 0;
+    for (auto& kv : files)
+      fb += (long long)kv.second.size();
+    info->file_bytes = fb;
+    info->kernel_launches = launches;
+    info->value_min = f.value_min;
+    info->value_max = f.value_max;
+  }
+  return NoError;
+}
+
+IDX2G_API int idx2g_dataset_open(idx2g_ctx* c, const idx2g_params* in, idx2g_dataset** ds)
+{
+  if (!c || !in || !ds)
+    return InvalidArgument;
+  params p;
+  to_params(in, &p);
+  return dataset_open(&c->d, p, (dataset_handle**)ds);
+}
+
+IDX2G_API int idx2g_output_grid(const idx2g_dataset* ds, const idx2g_params* in, int from3[3],
+                                int dims3[3], int strd3[3])
+{
+  if (!ds || !in)
+    return InvalidArgument;
+  params p;
+  to_params(in, &p);
+  grid g;
+  int e = dataset_output_grid((const dataset_handle*)ds, p, &g);
+  if (e)
+    return e;
+  for (int d = 0; d < 3; ++d)
+  {
+    from3[d] = g.from[d];
+    dims3[d] = g.dims[d];
+    strd3[d] = g.strd[d];
+  }
+  return NoError;
+}
+
+IDX2G_API int idx2g_decode(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* in, void* out,
+                           size_t out_bytes, int out_on_device, double* kernel_ms)
+{
+  if (!c || !ds || !in || !out)
+    return InvalidArgument;
+  params p;
+  to_params(in, &p);
+  return dataset_decode(&c->d, (dataset_handle*)ds, p, out, out_bytes, out_on_device != 0, kernel_ms);
+}
+
+IDX2G_API int idx2g_dataset_close(idx2g_dataset* ds)
+{
+  dataset_close((dataset_handle*)ds);
+  return NoError;
+}
+
+} // extern "C"

@@ -1,0 +1,425 @@
+// Device-side building blocks of the idx2 brick codec for sm_100a.
+//
+// Arithmetic follows the reference operation for operation (FP64 lifting in the
+// reference's order, integer zfp lifting, negabinary shuffle), so results are
+// bit-identical to the CPU implementation; the file is compiled with
+// --fmad=false so no expression is contracted into an FMA.
+#pragma once
+
+#include <cstdint>
+
+namespace idx2g
+{
+namespace dev
+{
+
+constexpr int kExt = 33;           // extended brick side (32 + 1)
+constexpr int kBrick3D = 33 * 33 * 33;
+constexpr int kBrick2D = 33 * 33;
+
+struct dgrid
+{
+  int from[3], dims[3], strd[3];
+};
+
+__device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
+
+// One CDF5/3 lifting sweep along axis a over the lines of grid G, split over the
+// threads of the CTA (Core/Wavelet.h:178 FLiftCdf53, :250 ILiftCdf53, lift_option
+// Normal). Each thread runs whole lines in the reference's sample order.
+__device__ void lift_sweep(double* F, const int N[3], const dgrid& G, const int M[3], int a,
+                           bool forward)
+{
+  const int P = G.from[a], D = G.dims[a], S = G.strd[a];
+  if (D == 1)
+    return;
+  const int b = a == 0 ? 1 : 0;
+  const int c = a == 2 ? 1 : 2;
+  const int st[3] = { 1, N[0], N[0] * N[1] };
+  const int x0 = imin(P + S * D, M[a]);
+  const int x1 = imin(P + S * (D - 1), M[a]);
+  const int x2 = P + S * (D - 2);
+  const int x3 = P + S * (D - 3);
+  const bool ext = (D % 2) == 0;
+  const int s = st[a];
+  const int nlines = G.dims[b] * G.dims[c];
+  for (int li = threadIdx.x; li < nlines; li += blockDim.x)
+  {
+    const int u = G.from[b] + (li % G.dims[b]) * G.strd[b];
+    const int v = G.from[c] + (li / G.dims[b]) * G.strd[c];
+    double* L = F + imin(u, M[b]) * st[b] + imin(v, M[c]) * st[c];
+#define AT(t) L[(t) * s]
+    if (forward)
+    {
+      if (ext)
+      {
+        double A = AT(x2), B = AT(x1);
+        AT(x0) = __dsub_rn(__dmul_rn(2.0, B), A);
+      }
+      for (int x = P + S; x < P + S * (D - 2); x += 2 * S)
+        AT(x) = __dsub_rn(AT(x), __dmul_rn(__dadd_rn(AT(x - S), AT(x + S)), 0.5));
+      if (!ext)
+        AT(x2) = __dsub_rn(AT(x2), __dmul_rn(__dadd_rn(AT(x1), AT(x3)), 0.5));
+      else if (x1 < M[a])
+        AT(x1) = 0;
+      for (int x = P + S; x < P + S * (D - 2); x += 2 * S)
+      {
+        double V = __dmul_rn(AT(x), 0.25);
+        AT(x - S) = __dadd_rn(AT(x - S), V);
+        AT(x + S) = __dadd_rn(AT(x + S), V);
+      }
+      if (!ext)
+      {
+        double V = __dmul_rn(AT(x2), 0.25);
+        AT(x3) = __dadd_rn(AT(x3), V);
+        AT(x1) = __dadd_rn(AT(x1), V);
+      }
+    }
+    else
+    {
+      for (int x = P + S; x < P + S * (D - 2); x += 2 * S)
+      {
+        double V = __dmul_rn(AT(x), 0.25);
+        AT(x - S) = __dsub_rn(AT(x - S), V);
+        AT(x + S) = __dsub_rn(AT(x + S), V);
+      }
+      if (!ext)
+      {
+        double V = __dmul_rn(AT(x2), 0.25);
+        AT(x3) = __dsub_rn(AT(x3), V);
+        AT(x1) = __dsub_rn(AT(x1), V);
+      }
+      else
+      {
+        double A = AT(x0), B = AT(x2);
+        AT(x1) = __dmul_rn(__dadd_rn(A, B), 0.5);
+      }
+      for (int x = P + S; x < P + S * (D - 2); x += 2 * S)
+        AT(x) = __dadd_rn(AT(x), __dmul_rn(__dadd_rn(AT(x - S), AT(x + S)), 0.5));
+      if (!ext)
+        AT(x2) = __dadd_rn(AT(x2), __dmul_rn(__dadd_rn(AT(x1), AT(x3)), 0.5));
+    }
+#undef AT
+  }
+}
+
+// The grid sequence of the multi-level transform on the first dims3 samples
+// (Core/Wavelet.cpp:210 ForwardCdf53 / :304 InverseCdf53 with a transform order).
+struct lift_stack
+{
+  dgrid g[16];
+  int8_t axis[16];
+  int n;
+};
+
+__device__ void build_stack(const int dims3[3], int nlevels, uint64_t order, lift_stack* st)
+{
+  int level = 0;
+  uint64_t prev = order;
+  int D3[3] = { dims3[0], dims3[1], dims3[2] };
+  int R3[3] = { dims3[0], dims3[1], dims3[2] };
+  int S3[3] = { 1, 1, 1 };
+  dgrid G;
+  for (int k = 0; k < 3; ++k)
+  {
+    G.from[k] = 0;
+    G.dims[k] = dims3[k];
+    G.strd[k] = 1;
+  }
+  st->n = 0;
+  while (level < nlevels)
+  {
+    int d = (int)(order & 3);
+    order >>= 2;
+    if (d == 3)
+    {
+      if (order == 3)
+        order = prev;
+      else
+        prev = order;
+      for (int k = 0; k < 3; ++k)
+      {
+        G.strd[k] = S3[k];
+        G.dims[k] = D3[k];
+        R3[k] = D3[k];
+      }
+      ++level;
+    }
+    else
+    {
+      if (st->n < 16)
+      {
+        st->g[st->n] = G;
+        st->axis[st->n] = (int8_t)d;
+        ++st->n;
+      }
+      R3[d] = D3[d] + (D3[d] % 2 == 0);
+      for (int k = 0; k < 3; ++k)
+        G.dims[k] = R3[k];
+      D3[d] = (R3[d] + 1) >> 1;
+      S3[d] <<= 1;
+    }
+  }
+}
+
+// Core/Math.h:524 Exponent<f64>, via the IEEE exponent field (glibc frexp semantics:
+// infinities and NaNs give 0).
+__device__ __forceinline__ int exponent_f64(double v)
+{
+  if (v == 0)
+    return -1023;
+  long long bits = __double_as_longlong(v);
+  int e = (int)((bits >> 52) & 0x7ff);
+  if (e == 0x7ff)
+    return 0;
+  if (e == 0)
+    return -1022;  // denormal: frexp gives <= -1022, clamped to 1 - bias
+  return e - 1022;
+}
+
+__device__ __forceinline__ int exponent_f32(float v)
+{
+  if (v == 0)
+    return -127;
+  int bits = __float_as_int(v);
+  int e = (bits >> 23) & 0xff;
+  if (e == 0xff)
+    return 0;
+  if (e == 0)
+    return -126;
+  return e - 126;
+}
+
+// 2^k as a double (ldexp(1, k)).
+__device__ __forceinline__ double pow2(int k)
+{
+  if (k > 1023)
+    return __longlong_as_double(0x7ff0000000000000ll);
+  if (k >= -1022)
+    return __longlong_as_double((long long)(k + 1023) << 52);
+  if (k >= -1074)
+    return __longlong_as_double(1ll << (k + 1074));
+  return 0.0;
+}
+
+// Truncating double -> int64 with the x86 cvttsd2si result for NaN / out of range.
+__device__ __forceinline__ long long trunc_i64(double v)
+{
+  if (!(v < 9223372036854775808.0 && v >= -9223372036854775808.0))
+    return (long long)0x8000000000000000ull;
+  return __double2ll_rz(v);
+}
+
+// zfp 4-point lifting (Core/Zfp.h:145 FLift, :181 ILift).
+__device__ __forceinline__ void fwd_lift4(long long* p, int s)
+{
+  long long x = p[0], y = p[s], z = p[2 * s], w = p[3 * s];
+  x += w;
+  x >>= 1;
+  w -= x;
+  z += y;
+  z >>= 1;
+  y -= z;
+  x += z;
+  x >>= 1;
+  z -= x;
+  w += y;
+  w >>= 1;
+  y -= w;
+  w += y >> 1;
+  y -= w >> 1;
+  p[0] = x;
+  p[s] = y;
+  p[2 * s] = z;
+  p[3 * s] = w;
+}
+
+__device__ __forceinline__ void inv_lift4(long long* p, int s)
+{
+  long long x = p[0], y = p[s], z = p[2 * s], w = p[3 * s];
+  y += w >> 1;
+  w -= y >> 1;
+  y += w;
+  w = (long long)((unsigned long long)w << 1);
+  w -= y;
+  z += x;
+  x = (long long)((unsigned long long)x << 1);
+  x -= z;
+  y += z;
+  z = (long long)((unsigned long long)z << 1);
+  z -= y;
+  w += x;
+  x = (long long)((unsigned long long)x << 1);
+  x -= w;
+  p[0] = x;
+  p[s] = y;
+  p[2 * s] = z;
+  p[3 * s] = w;
+}
+
+// Warp-cooperative forward zfp transform of one block held in shared memory
+// (Core/Zfp.h:262 ForwardZfp(P, D)): lines of each pass go to different lanes.
+__device__ __forceinline__ void warp_fwd_zfp(long long* q, int nd, int lane)
+{
+  if (nd == 3)
+  {
+    if (lane < 16)
+      fwd_lift4(q + 4 * (lane & 3) + 16 * (lane >> 2), 1);
+    __syncwarp();
+    if (lane < 16)
+      fwd_lift4(q + 16 * (lane & 3) + (lane >> 2), 4);
+    __syncwarp();
+    if (lane < 16)
+      fwd_lift4(q + (lane & 3) + 4 * (lane >> 2), 16);
+    __syncwarp();
+  }
+  else if (nd == 2)
+  {
+    if (lane < 4)
+      fwd_lift4(q + 4 * lane, 1);
+    __syncwarp();
+    if (lane < 4)
+      fwd_lift4(q + lane, 4);
+    __syncwarp();
+  }
+  else if (nd == 1)
+  {
+    if (lane == 0)
+      fwd_lift4(q, 1);
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ void warp_inv_zfp(long long* q, int nd, int lane)
+{
+  if (nd == 3)
+  {
+    if (lane < 16)
+      inv_lift4(q + (lane & 3) + 4 * (lane >> 2), 16);
+    __syncwarp();
+    if (lane < 16)
+      inv_lift4(q + 16 * (lane & 3) + (lane >> 2), 4);
+    __syncwarp();
+    if (lane < 16)
+      inv_lift4(q + 4 * (lane & 3) + 16 * (lane >> 2), 1);
+    __syncwarp();
+  }
+  else if (nd == 2)
+  {
+    if (lane < 4)
+      inv_lift4(q + lane, 4);
+    __syncwarp();
+    if (lane < 4)
+      inv_lift4(q + 4 * lane, 1);
+    __syncwarp();
+  }
+  else if (nd == 1)
+  {
+    if (lane == 0)
+      inv_lift4(q, 1);
+    __syncwarp();
+  }
+}
+
+constexpr unsigned long long kNegaMask = 0xaaaaaaaaaaaaaaaaull;
+
+// Coefficient order by total sequency (Core/Zfp.h:419 Perm3, :498 Perm2), as flat
+// indices x + 4y + 16z into the block.
+static __constant__ uint8_t kPerm3d[64] = {
+  0,  1,  4,  16, 20, 17, 5,  2,  8,  32, 21, 6,  18, 24, 9,  33, 36, 3,  12, 48, 22, 25,
+  37, 40, 34, 10, 7,  19, 28, 13, 49, 52, 41, 38, 26, 23, 29, 53, 11, 35, 44, 14, 50, 56,
+  42, 27, 39, 45, 30, 54, 57, 60, 51, 15, 43, 46, 58, 61, 55, 31, 62, 59, 47, 63
+};
+static __constant__ uint8_t kPerm2d[16] = { 0, 1, 4, 5, 2, 8, 6, 9, 3, 12, 10, 7, 13, 11, 14, 15 };
+
+__device__ __forceinline__ int perm(int nd, int i)
+{
+  return nd == 3 ? (int)kPerm3d[i] : (nd == 2 ? (int)kPerm2d[i] : i);
+}
+
+// Number of coded planes of a block (Core/idx2Encode.cpp:195-206, BitPlanesPerChunk 1):
+// planes 63 .. lowbp with lowbp = max(64 - EndBitPlane, 57 + Exponent(tol) - EMax).
+__device__ __forceinline__ int coded_planes(int emax, int etol, int end_bp)
+{
+  int low = 57 + etol - emax;
+  int lim = 64 - end_bp;
+  low = low > lim ? low : lim;
+  return low <= 63 ? 64 - low : 0;
+}
+
+// Bit length of one plane of the group-test coder (Core/Zfp.h:771 Encode<u64>) with
+// nin significant coefficients before the plane and plane bits x.
+__device__ __forceinline__ int plane_bits(unsigned long long x, int nin, int nvals)
+{
+  unsigned long long r = nin < 64 ? (x >> nin) : 0ull;
+  if (r == 0)
+    return nin + (nin < nvals ? 1 : 0);
+  int k = __popcll(r);
+  int s = 63 - __clzll(x);
+  return k + s + (s < nvals - 1 ? 2 : 0);
+}
+
+__device__ __forceinline__ int plane_nout(unsigned long long x, int nin)
+{
+  int m = x ? 64 - __clzll(x) : 0;
+  return m > nin ? m : nin;
+}
+
+// OR nbits (<= 32) of v into a zero-initialised bit stream at bit position pos.
+__device__ __forceinline__ void or_bits(uint32_t* words, unsigned long long pos, uint32_t v, int n)
+{
+  if (n <= 0 || v == 0)
+    return;
+  if (n < 32)
+    v &= (1u << n) - 1u;
+  unsigned long long w = pos >> 5;
+  int sh = (int)(pos & 31);
+  atomicOr(words + w, v << sh);
+  if (sh + n > 32)
+    atomicOr(words + w + 1, v >> (32 - sh));
+}
+
+// Write the bits of one plane (Core/Zfp.h:771 Encode<u64>) at bit position pos of a
+// zero-initialised stream. Only one-bits are stored.
+__device__ void write_plane(uint32_t* words, unsigned long long pos, unsigned long long x, int nin,
+                            int nvals)
+{
+  // raw bits of the already significant coefficients
+  int n = nin;
+  for (int i = 0; i < n; i += 32)
+  {
+    int m = n - i < 32 ? n - i : 32;
+    or_bits(words, pos + (unsigned long long)i, (uint32_t)(x >> i), m);
+  }
+  pos += (unsigned long long)n;
+  unsigned long long r = n < 64 ? (x >> n) : 0ull;
+  while (n < nvals)
+  {
+    if (r == 0)
+    {
+      pos += 1;  // group bit 0
+      break;
+    }
+    or_bits(words, pos, 1u, 1);  // group bit 1
+    pos += 1;
+    int t = __ffsll((long long)r) - 1;
+    int s = n + t;
+    if (s < nvals - 1)
+    {
+      pos += (unsigned long long)t;  // t zero bits
+      or_bits(words, pos, 1u, 1);
+      pos += 1;
+      n = s + 1;
+      r = (t + 1 < 64) ? (r >> (t + 1)) : 0ull;
+    }
+    else
+    {
+      pos += (unsigned long long)t;  // zeros up to the last coefficient, which is implied
+      n = nvals;
+      r = 0;
+    }
+  }
+}
+
+} // namespace dev
+} // namespace idx2g

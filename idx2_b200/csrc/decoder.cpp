@@ -1,0 +1,533 @@
+// Decode side, host part (Core/idx2Decode.cpp:326-540, Core/idx2Read.cpp).
+//
+// dataset_open reads the metadata file and every data file of the dataset once,
+// parses the chunk tables (file tails, chunk headers), decompresses the exponent
+// chunks and builds a device-resident index:
+//   blob      all bit-plane chunk bytes, as stored in the files
+//   exps      per (level, brick, subband): the block exponents (coded blocks, Morton order)
+//   chan      per (level, brick, subband): the byte offset in blob of the brick's data in
+//             the chunk of each bit-plane channel present
+// dataset_decode then plans the request (ROI, downsampling, tolerance) on the host and runs
+// one device launch per decoded level, coarsest first.
+#include "decoder.h"
+#include "decode_device.h"
+#include "packer.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <unordered_map>
+
+namespace idx2g
+{
+
+namespace
+{
+
+struct bit_reader
+{
+  const uint8_t* p;
+  size_t n;
+  uint64_t pos = 0;
+  uint64_t get(int bits)
+  {
+    uint64_t v = 0;
+    for (int i = 0; i < bits; ++i)
+    {
+      uint64_t q = pos + (uint64_t)i;
+      uint64_t b = (q >> 3) < n ? (p[q >> 3] >> (q & 7)) & 1u : 0;
+      v |= b << i;
+    }
+    pos += (uint64_t)bits;
+    return v;
+  }
+  uint64_t varbyte()
+  {
+    // Core/VarInt.h:30 ReadVarByte
+    uint64_t v = 0;
+    int sh = 0;
+    while (true)
+    {
+      v = (get(7) << (7 * sh++)) + v;
+      if (get(1) == 0)
+        break;
+      if (sh > 10)
+        break;
+    }
+    return v;
+  }
+  uint64_t unary()
+  {
+    uint64_t v = 0;
+    while (!get(1))
+    {
+      ++v;
+      if ((pos >> 3) > n)
+        break;
+    }
+    return v;
+  }
+  void next_byte() { pos = (pos + 7) & ~7ull; }
+};
+
+int32_t rd_i32(const std::vector<uint8_t>& d, size_t off)
+{
+  int32_t v;
+  memcpy(&v, d.data() + off, 4);
+  return v;
+}
+
+bool read_whole(const std::string& path, std::vector<uint8_t>* out)
+{
+  FILE* fp = fopen(path.c_str(), "rb");
+  if (!fp)
+    return false;
+  fseek(fp, 0, SEEK_END);
+  long sz = ftell(fp);
+  fseek(fp, 0, SEEK_SET);
+  out->resize((size_t)(sz > 0 ? sz : 0));
+  size_t r = sz > 0 ? fread(out->data(), 1, (size_t)sz, fp) : 0;
+  fclose(fp);
+  return r == out->size();
+}
+
+} // namespace
+
+struct dataset_handle
+{
+  dataset_format f;
+  params p0;
+  // per level: dense map from linear brick id to brick index (-1 if none)
+  std::vector<std::vector<int>> brick_index;
+  std::vector<std::vector<v3>> brick3;           // per level, per brick index
+  std::vector<std::vector<int>> brick_in_chunk;  // per level, per brick index
+  std::vector<std::vector<int>> blocks_per_sb;   // per level, per subband (coded blocks)
+  // host index
+  std::vector<int16_t> exps;                     // [level offset + brick][sb][kMaxBlocksPerSubband]
+  std::vector<size_t> level_brick_base;          // brick index base of each level in flat tables
+  std::vector<int32_t> chan_kmin, chan_n;        // [flat brick][sb]
+  std::vector<uint64_t> chan_first;              // [flat brick][sb] index into chan_off
+  std::vector<uint64_t> chan_off;                // byte offset in blob, ~0 = absent
+  std::vector<uint8_t> blob;
+  size_t blob_bytes = 0;
+  // device copies
+  decode_device dev;
+};
+
+static int load_index(dataset_handle* h)
+{
+  dataset_format& f = h->f;
+  const int L = f.nlevels;
+  const int nsb = f.nsubbands();
+  h->brick_index.assign((size_t)L, {});
+  h->brick3.assign((size_t)L, {});
+  h->brick_in_chunk.assign((size_t)L, {});
+  h->blocks_per_sb.assign((size_t)L, std::vector<int>((size_t)nsb, 0));
+  h->level_brick_base.assign((size_t)L + 1, 0);
+
+  // enumerate bricks of every level with their index in the chunk, using the decoder's
+  // file -> chunk -> brick traversal over the whole volume (Core/idx2Decode.cpp:403-470)
+  for (int l = 0; l < L; ++l)
+  {
+    size_t nlin = (size_t)1 << f.bricks_order_str[(size_t)l].size();
+    h->brick_index[(size_t)l].assign(nlin, -1);
+    v3 b3 = f.brick_dims;
+    for (int k = 0; k < l; ++k)
+      b3 = b3 * f.group_brick3;
+    v3 c3 = f.bricks_per_chunk3[(size_t)l] * b3;
+    v3 fl3 = c3 * f.chunks_per_file3[(size_t)l];
+    extent vol{ v3(0), f.dims };
+    extent eb{ vol.from / b3, vol.last() / b3 - vol.from / b3 + v3(1) };
+    extent ec{ vol.from / c3, vol.last() / c3 - vol.from / c3 + v3(1) };
+    extent ef{ vol.from / fl3, vol.last() / fl3 - vol.from / fl3 + v3(1) };
+    traverse(f.files_order[(size_t)l], v3(0), f.nfiles3[(size_t)l], ef, ef, [&](const traverse_item& fi) {
+      traverse(f.chunks_order_in_file[(size_t)l], fi.from3 * f.chunks_per_file3[(size_t)l],
+               f.chunks_per_file3[(size_t)l], ec, ec, [&](const traverse_item& ci) {
+                 traverse(f.bricks_order_in_chunk[(size_t)l], ci.from3 * f.bricks_per_chunk3[(size_t)l],
+                          f.bricks_per_chunk3[(size_t)l], eb, eb, [&](const traverse_item& bi) {
+                            u64 lin = linear_brick(f, l, bi.from3);
+                            if (lin >= nlin || h->brick_index[(size_t)l][lin] >= 0)
+                              return;
+                            h->brick_index[(size_t)l][lin] = (int)h->brick3[(size_t)l].size();
+                            h->brick3[(size_t)l].push_back(bi.from3);
+                            h->brick_in_chunk[(size_t)l].push_back(bi.item_in_parent);
+                          });
+               });
+    });
+    h->level_brick_base[(size_t)l + 1] = h->level_brick_base[(size_t)l] + h->brick3[(size_t)l].size();
+    for (int s = 0; s < nsb; ++s)
+    {
+      std::vector<block_geom> g;
+      subband_blocks(f, l, s, &g);
+      h->blocks_per_sb[(size_t)l][(size_t)s] = (int)g.size();
+    }
+  }
+  const size_t nflat = h->level_brick_base[(size_t)L];
+  h->exps.assign(nflat * (size_t)nsb * kMaxBlocksPerSubband, 0);
+  h->chan_kmin.assign(nflat * (size_t)nsb, 0);
+  h->chan_n.assign(nflat * (size_t)nsb, 0);
+  h->chan_first.assign(nflat * (size_t)nsb, 0);
+  // collected channel entries: (flat brick, sb) -> list of (bpkey, blob offset)
+  std::vector<std::vector<std::pair<int, uint64_t>>> chans(nflat * (size_t)nsb);
+
+  // the set of data files: one per (level, brick >> log2(bricks per file))
+  std::map<std::string, int> files;  // path -> level
+  for (int l = 0; l < L; ++l)
+    for (size_t i = 0; i < h->brick3[(size_t)l].size(); ++i)
+      files[file_path(f, linear_brick(f, l, h->brick3[(size_t)l][i]), l)] = l;
+
+  const int esz = f.type == dtype::float32 ? 1 : 2;
+  for (auto& kv : files)
+  {
+    std::vector<uint8_t> d;
+    if (!read_whole(kv.first, &d))
+      continue;  // a missing file leaves its bricks undecoded (Core/idx2Decode.cpp:166-168)
+    const int level = kv.second;
+    if (d.size() < 16)
+      return CorruptStream;
+    // exponent section (Core/idx2Read.cpp:252 ReadFileExponents)
+    size_t E = d.size();
+    int32_t total = rd_i32(d, E - 4);
+    int32_t nexp = rd_i32(d, E - 8);
+    int32_t asz = rd_i32(d, E - 12);
+    if (total < 16 || (size_t)total > E || asz < 0 || (size_t)asz + 16 > (size_t)total)
+      return CorruptStream;
+    std::vector<uint8_t> addrs_raw;
+    if (zstd_decompress(d.data() + E - 12 - (size_t)asz, (size_t)asz, &addrs_raw))
+      return CorruptStream;
+    int32_t ssz = rd_i32(d, E - 16 - (size_t)asz);
+    if (ssz < 0 || (size_t)ssz + (size_t)asz + 16 > (size_t)total)
+      return CorruptStream;
+    bit_reader sr{ d.data() + E - 16 - (size_t)asz - (size_t)ssz, (size_t)ssz };
+    size_t exp_beg = E - (size_t)total;
+    size_t off = exp_beg;
+    for (int c = 0; c < nexp; ++c)
+    {
+      uint64_t csz = sr.varbyte();
+      if ((size_t)c * 8 + 8 > addrs_raw.size() || off + csz > E)
+        return CorruptStream;
+      u64 addr;
+      memcpy(&addr, addrs_raw.data() + (size_t)c * 8, 8);
+      std::vector<uint8_t> ex;
+      if (zstd_decompress(d.data() + off, (size_t)csz, &ex))
+        return CorruptStream;
+      off += csz;
+      int sb = (int)((addr >> 12) & 0x3F);
+      int lv = (int)((addr >> 60) & 0xF);
+      u64 chunk = (addr >> 18) & 0x3FFFFFFFFFFull;
+      if (lv != level || sb >= nsb)
+        continue;
+      // every brick of this chunk: exps at BrickInChunk * BlockCount * esz
+      int shift = log2_ceil(f.bricks_per_chunk[(size_t)lv]);
+      u64 first = chunk << shift, last = (chunk + 1) << shift;
+      const int bc = h->blocks_per_sb[(size_t)lv][(size_t)sb];
+      for (u64 lin = first; lin < last && lin < h->brick_index[(size_t)lv].size(); ++lin)
+      {
+        int bi = h->brick_index[(size_t)lv][lin];
+        if (bi < 0)
+          continue;
+        size_t pos = (size_t)h->brick_in_chunk[(size_t)lv][(size_t)bi] * (size_t)bc * (size_t)esz;
+        size_t flat = h->level_brick_base[(size_t)lv] + (size_t)bi;
+        int16_t* dst = h->exps.data() + (flat * (size_t)nsb + (size_t)sb) * kMaxBlocksPerSubband;
+        for (int b = 0; b < bc; ++b)
+        {
+          size_t q = pos + (size_t)b * (size_t)esz;
+          int v = 0;
+          if (q + (size_t)esz <= ex.size())
+            v = esz == 2 ? (int)ex[q] | ((int)ex[q + 1] << 8) : (int)ex[q];
+          dst[b] = (int16_t)(esz == 2 ? v - 1023 : v - 127);
+        }
+      }
+    }
+    if (exp_beg == 0)
+      continue;
+    // bit-plane section (Core/idx2Read.cpp:82 ReadFile)
+    size_t E2 = exp_beg;
+    int32_t nch = rd_i32(d, E2 - 4);
+    int32_t asz2 = rd_i32(d, E2 - 8);
+    if (asz2 < 0 || (size_t)asz2 + 12 > E2)
+      return CorruptStream;
+    std::vector<uint8_t> caddrs;
+    if (zstd_decompress(d.data() + E2 - 8 - (size_t)asz2, (size_t)asz2, &caddrs))
+      return CorruptStream;
+    int32_t ssz2 = rd_i32(d, E2 - 12 - (size_t)asz2);
+    if (ssz2 < 0 || (size_t)ssz2 + (size_t)asz2 + 12 > E2)
+      return CorruptStream;
+    bit_reader csr{ d.data() + E2 - 12 - (size_t)asz2 - (size_t)ssz2, (size_t)ssz2 };
+    size_t body_end = E2 - 12 - (size_t)asz2 - (size_t)ssz2;
+    size_t blob_base = h->blob.size();
+    h->blob.insert(h->blob.end(), d.begin(), d.begin() + (long)body_end);
+    size_t coff = 0;
+    for (int c = 0; c < nch; ++c)
+    {
+      uint64_t csz = csr.varbyte();
+      if ((size_t)c * 8 + 8 > caddrs.size() || coff + csz > body_end)
+        return CorruptStream;
+      u64 addr;
+      memcpy(&addr, caddrs.data() + (size_t)c * 8, 8);
+      int sb = (int)((addr >> 12) & 0x3F);
+      int lv = (int)((addr >> 60) & 0xF);
+      int bpkey = (int)(addr & 0xFFF);
+      // chunk header (Core/idx2Decode.cpp:507 DecompressChunk)
+      bit_reader cr{ d.data() + coff, (size_t)csz };
+      int nbr = (int)cr.varbyte();
+      std::vector<u64> bricks((size_t)(nbr > 0 ? nbr : 0));
+      if (nbr > 0)
+      {
+        u64 b = cr.varbyte();
+        bricks[0] = b;
+        for (int i = 1; i < nbr; ++i)
+        {
+          b += cr.unary() + 1;
+          bricks[(size_t)i] = b;
+        }
+      }
+      cr.next_byte();
+      std::vector<uint64_t> offs((size_t)(nbr > 0 ? nbr : 0), 0);
+      uint64_t acc = 0;
+      for (int i = 1; i < nbr; ++i)
+      {
+        acc += cr.varbyte();
+        offs[(size_t)i] = acc;
+      }
+      if (nbr > 0)
+        cr.varbyte();
+      uint64_t data_start = cr.pos >> 3;
+      if (lv == level && sb < nsb)
+      {
+        for (int i = 0; i < nbr; ++i)
+        {
+          u64 lin = bricks[(size_t)i];
+          if (lin >= h->brick_index[(size_t)lv].size())
+            continue;
+          int bi = h->brick_index[(size_t)lv][lin];
+          if (bi < 0)
+            continue;
+          size_t flat = h->level_brick_base[(size_t)lv] + (size_t)bi;
+          chans[flat * (size_t)nsb + (size_t)sb].push_back(
+            { bpkey, (uint64_t)(blob_base + coff + data_start + offs[(size_t)i]) });
+        }
+      }
+      coff += csz;
+    }
+  }
+  // flatten the channel table
+  h->chan_off.clear();
+  for (size_t i = 0; i < chans.size(); ++i)
+  {
+    auto& v = chans[i];
+    if (v.empty())
+    {
+      h->chan_kmin[i] = 1;
+      h->chan_n[i] = 0;
+      h->chan_first[i] = h->chan_off.size();
+      continue;
+    }
+    int kmin = 1 << 30, kmax = -1;
+    for (auto& e : v)
+    {
+      kmin = std::min(kmin, e.first);
+      kmax = std::max(kmax, e.first);
+    }
+    h->chan_kmin[i] = kmin;
+    h->chan_n[i] = kmax - kmin + 1;
+    h->chan_first[i] = h->chan_off.size();
+    h->chan_off.resize(h->chan_off.size() + (size_t)(kmax - kmin + 1), ~0ull);
+    for (auto& e : v)
+      h->chan_off[h->chan_first[i] + (size_t)(e.first - kmin)] = e.second;
+  }
+  h->blob_bytes = h->blob.size();
+  return NoError;
+}
+
+int dataset_open(device_ctx* ctx, const params& pin, dataset_handle** out)
+{
+  *out = nullptr;
+  std::vector<uint8_t> meta;
+  if (!read_whole(pin.input_file, &meta))
+    return FileNotFound;
+  dataset_handle* h = new dataset_handle;
+  h->p0 = pin;
+  int e = parse_meta(std::string(meta.begin(), meta.end()), &h->f);
+  if (!e)
+  {
+    params p = pin;
+    p.downsampling = v3(0);
+    e = finalize_read(&h->f, &p);
+  }
+  if (!e)
+    e = load_index(h);
+  if (!e)
+    e = h->dev.upload(ctx, h->exps, h->chan_kmin, h->chan_n, h->chan_first, h->chan_off, h->blob);
+  if (e)
+  {
+    delete h;
+    return e;
+  }
+  h->blob.clear();
+  h->blob.shrink_to_fit();
+  *out = h;
+  return NoError;
+}
+
+// Decode masks and spacings of a request (Core/idx2Common.cpp:403-461).
+static void request_format(const dataset_handle* h, const params& p, dataset_format* f)
+{
+  *f = h->f;
+  f->downsampling = p.downsampling;
+  params q = p;
+  q.in_dir = h->f.dir;
+  finalize_read(f, &q);
+}
+
+int dataset_output_grid(const dataset_handle* h, const params& p, grid* g)
+{
+  dataset_format f;
+  request_format(h, p, &f);
+  extent ext = p.has_extent ? p.decode_extent : extent{ v3(0), f.dims };
+  *g = output_grid(f, ext);
+  return NoError;
+}
+
+int dataset_decode(device_ctx* ctx, dataset_handle* h, const params& p, void* out, size_t out_bytes,
+                   bool out_on_device, double* kernel_ms)
+{
+  dataset_format f;
+  request_format(h, p, &f);
+  extent ext = p.has_extent ? p.decode_extent : extent{ v3(0), f.dims };
+  grid og = output_grid(f, ext);
+  const size_t esz = f.type == dtype::float32 ? 4 : 8;
+  const size_t need = (size_t)prod(og.dims) * esz;
+  if (out_bytes < need)
+    return SizeTooSmall;
+  const double tol = std::max(f.tolerance, p.decode_tolerance);  // Core/idx2Decode.cpp:364
+  const int L = f.nlevels;
+  const int nsb = f.nsubbands();
+
+  decode_request rq;
+  rq.nlevels = L;
+  rq.nsb = nsb;
+  rq.is2d = f.is2d();
+  rq.f32 = f.type == dtype::float32;
+  rq.etol = exponent_f64(tol);
+  rq.out_from = og.from;
+  rq.out_dims = og.dims;
+  rq.out_strd = og.strd;
+  // decoded levels: from the coarsest down while the mask is not empty
+  int lmin = L;
+  for (int l = L - 1; l >= 0; --l)
+  {
+    if (f.decode_masks[(size_t)l] == 0)
+      break;
+    lmin = l;
+  }
+  std::vector<std::vector<int>> sel((size_t)L);  // selected brick indices per level
+  std::vector<std::unordered_map<int, int>> pos_of((size_t)L);
+  for (int l = L - 1; l >= lmin; --l)
+  {
+    v3 b3 = f.brick_dims;
+    for (int k = 0; k < l; ++k)
+      b3 = b3 * f.group_brick3;
+    v3 bf = ext.from / b3, bl = ext.last() / b3;
+    bl = vmin(bl, f.nbricks3[(size_t)l] - v3(1));
+    decode_level lv;
+    lv.level = l;
+    lv.mask = f.decode_masks[(size_t)l];
+    lv.is_output = (l == 0 || f.decode_masks[(size_t)l - 1] == 0);
+    for (int s = 0; s < nsb; ++s)
+      for (int d = 0; d < 3; ++d)
+        lv.spacing[s][d] = f.decode_spacings[(size_t)l][(size_t)s][d];
+    for (int bz = bf.z; bz <= bl.z; ++bz)
+      for (int by = bf.y; by <= bl.y; ++by)
+        for (int bx = bf.x; bx <= bl.x; ++bx)
+        {
+          v3 b(bx, by, bz);
+          u64 lin = linear_brick(f, l, b);
+          if (lin >= h->brick_index[(size_t)l].size())
+            continue;
+          int bi = h->brick_index[(size_t)l][lin];
+          if (bi < 0)
+            continue;
+          decode_brick db;
+          db.flat = (long long)(h->level_brick_base[(size_t)l] + (size_t)bi);
+          db.parent = -1;
+          db.pos[0] = db.pos[1] = db.pos[2] = 0;
+          if (l + 1 < L)
+          {
+            v3 pb = b / f.group_brick3;
+            u64 plin = linear_brick(f, l + 1, pb);
+            int pbi = plin < h->brick_index[(size_t)l + 1].size() ? h->brick_index[(size_t)l + 1][plin] : -1;
+            auto it = pbi >= 0 ? pos_of[(size_t)l + 1].find(pbi) : pos_of[(size_t)l + 1].end();
+            db.parent = it == pos_of[(size_t)l + 1].end() ? -1 : it->second;
+            v3 lp = b % f.group_brick3;
+            db.pos[0] = lp.x;
+            db.pos[1] = lp.y;
+            db.pos[2] = lp.z;
+          }
+          if (lv.is_output)
+          {
+            // Core/idx2Decode.cpp:431-442
+            grid bg;
+            bg.from = b * b3;
+            bg.dims = f.brick_dims;
+            bg.strd = v3(1 << l);
+            grid ob = crop(og, bg);
+            if (prod(ob.dims) <= 0)
+              continue;
+            grid local = relative(ob, bg);
+            grid dst = relative(ob, og);
+            for (int d = 0; d < 3; ++d)
+            {
+              db.src_from[d] = local.from[d];
+              db.src_strd[d] = local.strd[d];
+              db.dims[d] = ob.dims[d];
+              db.dst_from[d] = dst.from[d];
+              db.dst_strd[d] = dst.strd[d];
+            }
+          }
+          pos_of[(size_t)l][bi] = (int)lv.bricks.size();
+          lv.bricks.push_back(db);
+        }
+    for (int s = 0; s < nsb; ++s)
+    {
+      std::vector<block_geom> g;
+      subband_blocks(f, l, s, &g);
+      lv.nblocks[s] = (int)g.size();
+      for (size_t b = 0; b < g.size(); ++b)
+        lv.geom[s][b] = (uint64_t)g[b].dx | ((uint64_t)g[b].dy << 8) | ((uint64_t)g[b].dz << 16) |
+                        ((uint64_t)g[b].bx << 24) | ((uint64_t)g[b].by << 32) | ((uint64_t)g[b].bz << 40);
+    }
+    // de-normalisation weights (Core/Wavelet.cpp:151-177)
+    double scal[16], wave[16];
+    double n1 = 3, n2 = 23;
+    for (int i = 0; i < 16; ++i)
+    {
+      scal[i] = sqrt(n1 / (1 << (i + 1)));
+      n1 = n1 * 4 - 1;
+      wave[i] = sqrt(n2 / (1 << (i + 5)));
+      n2 = n2 * 4 - 33;
+    }
+    lv.norm_mask = 0;
+    for (int s = 0; s < nsb; ++s)
+    {
+      const subband& sb = f.subbands[(size_t)s];
+      double wx = f.brick_dims_ext.x == 1 ? 1
+                  : (sb.low_high.x == 0 ? scal[l + sb.level_rev.x - 1] : wave[l + sb.level_rev.x]);
+      double wy = f.brick_dims_ext.y == 1 ? 1
+                  : (sb.low_high.y == 0 ? scal[l + sb.level_rev.y - 1] : wave[l + sb.level_rev.y]);
+      double wz = f.brick_dims_ext.z == 1 ? 1
+                  : (sb.low_high.z == 0 ? scal[l + sb.level_rev.z - 1] : wave[l + sb.level_rev.z]);
+      lv.inv_weight[s] = 1.0 / (wx * wy * wz);
+      if (!(s == 0 && l + 1 != L))
+        lv.norm_mask |= 1 << s;
+    }
+    rq.levels.push_back(std::move(lv));
+  }
+  return h->dev.decode(ctx, rq, out, need, out_on_device, kernel_ms);
+}
+
+void dataset_close(dataset_handle* h) { delete h; }
+
+} // namespace idx2g

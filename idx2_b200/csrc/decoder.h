@@ -1,0 +1,19 @@
+// Decode side: dataset index (host parse of the data files, device-resident copy of
+// the chunk payloads) and the level-by-level device decode (Core/idx2Decode.cpp:326).
+#pragma once
+
+#include "device.h"
+#include "format.h"
+
+namespace idx2g
+{
+
+struct dataset_handle;
+
+int dataset_open(device_ctx* ctx, const params& p, dataset_handle** out);
+int dataset_output_grid(const dataset_handle* ds, const params& p, grid* g);
+int dataset_decode(device_ctx* ctx, dataset_handle* ds, const params& p, void* out, size_t out_bytes,
+                   bool out_on_device, double* kernel_ms);
+void dataset_close(dataset_handle* ds);
+
+} // namespace idx2g

@@ -1,0 +1,676 @@
+// Encode kernels for sm_100a and the device stage of the encoder.
+//
+// One persistent CTA per brick slot runs the whole per-brick pipeline of the
+// reference (Core/idx2Encode.cpp:276-335 EncodeBrick and :141-256
+// EncodeSubbandBlocks):
+//   A  gather the brick (level 0: from the field, widened to FP64; level > 0: the
+//      parent brick assembled by the children) into the CTA's FP64 slot,
+//   B  extrapolation round trip + one-level CDF5/3 + subband normalisation,
+//   C  hand the low band to the parent brick of the next level,
+//   D  per subband: warp-per-block exponent / quantise / zfp / shuffle, bit planes
+//      by warp ballot, closed-form plane lengths, per-channel scan, bit scatter.
+// The channel streams of a (brick, subband) are placed with one atomic cursor
+// bump; the host packer reads them back by offset.
+#include "codec_device.cuh"
+#include "device.h"
+#include "encoder.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+namespace idx2g
+{
+
+namespace
+{
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kMaxPlanes = 64;
+
+struct enc_brick
+{
+  int b3[3];      // brick coordinates (level 0: field origin = b3 * 32)
+  int valid[3];   // valid dims
+  int parent;     // parent index in the next level, -1 if none
+  int pos[3];     // position inside the parent (0/1 per axis)
+};
+
+struct enc_args
+{
+  int level, nlevels, is2d, f32_exp, etol, end_bp, nsb, nbricks;
+  uint64_t order;
+  const void* field;
+  int field_f32;
+  long long fdims[3];
+  const enc_brick* bricks;
+  const double* in_bricks;   // level > 0: [nbricks][NB] assembled parents
+  double* slots;             // [gridDim][NB]
+  double* parent_bricks;     // [nparents][NB] (zeroed), null on the coarsest level
+  const uint64_t* geom;      // [nsb][kMaxBlocksPerSubband]
+  const int* nblocks;        // [nsb]
+  double weight[8];
+  int norm_mask;
+  int16_t* exps;
+  int32_t* kmin;
+  int32_t* kmax;
+  unsigned long long* offset;
+  uint32_t* sizes;
+  uint32_t* stream;
+  unsigned long long cap_bytes;
+  unsigned long long* cursor;
+  int* error;
+  double* bmin;
+  double* bmax;
+};
+
+// shared memory layout (dynamic)
+struct enc_smem
+{
+  unsigned long long X[kMaxBlocksPerSubband][kMaxPlanes];  // plane bit masks
+  uint16_t off[kMaxBlocksPerSubband][kMaxPlanes];          // bit offset inside the channel
+  uint8_t nin[kMaxBlocksPerSubband][kMaxPlanes];           // significant coefficients before plane
+  long long q[kWarps][64];                                 // per-warp block scratch
+  int16_t emax[kMaxBlocksPerSubband];
+  int16_t ktop[kMaxBlocksPerSubband];
+  uint8_t np[kMaxBlocksPerSubband];
+  uint8_t nvals_log[kMaxBlocksPerSubband];
+  uint32_t key_bits[kKeyWindow];
+  uint32_t key_base[kKeyWindow];
+  dev::lift_stack stack;
+  double red[2][kWarps];
+  int kmin, kmax;
+  unsigned long long region;
+  int ok;
+};
+
+__device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
+{
+  d3[0] = (int)(g & 0xff) * 4;
+  d3[1] = (int)((g >> 8) & 0xff) * 4;
+  d3[2] = (int)((g >> 16) & 0xff) * 4;
+  bd[0] = (int)((g >> 24) & 0xff);
+  bd[1] = (int)((g >> 32) & 0xff);
+  bd[2] = (int)((g >> 40) & 0xff);
+}
+
+__device__ __forceinline__ void subband_grid(int is2d, int s, int from[3], int dims[3], int strd[3])
+{
+  int h[3] = { 0, 0, 0 };
+  if (is2d)
+  {
+    h[0] = (s >> 1) & 1;
+    h[1] = s & 1;
+  }
+  else
+  {
+    h[0] = (s >> 2) & 1;
+    h[1] = (s >> 1) & 1;
+    h[2] = s & 1;
+  }
+  for (int k = 0; k < 3; ++k)
+  {
+    if (is2d && k == 2)
+    {
+      from[k] = 0;
+      dims[k] = 1;
+      strd[k] = 1;
+    }
+    else
+    {
+      from[k] = h[k];
+      dims[k] = h[k] ? 16 : 17;
+      strd[k] = 2;
+    }
+  }
+}
+
+__device__ __forceinline__ double warp_max(double v)
+{
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    double w = __shfl_xor_sync(0xffffffffu, v, o);
+    v = v < w ? w : v;
+  }
+  return v;
+}
+
+__global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  enc_smem& sm = *reinterpret_cast<enc_smem*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int N[3] = { 33, 33, a.is2d ? 1 : 33 };
+  const int NB = N[0] * N[1] * N[2];
+  double* F = a.slots + (size_t)blockIdx.x * (size_t)NB;
+
+  for (int bi = blockIdx.x; bi < a.nbricks; bi += gridDim.x)
+  {
+    const enc_brick br = a.bricks[bi];
+    // ---------------- A: gather ----------------
+    if (a.level == 0)
+    {
+      for (int i = tid; i < NB; i += kThreads)
+        F[i] = 0.0;
+      __syncthreads();
+      double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
+      const int vx = br.valid[0], vy = br.valid[1], vz = br.valid[2];
+      const int nvalid = vx * vy * vz;
+      for (int i = tid; i < nvalid; i += kThreads)
+      {
+        int x = i % vx, y = (i / vx) % vy, z = i / (vx * vy);
+        long long gx = (long long)br.b3[0] * 32 + x, gy = (long long)br.b3[1] * 32 + y,
+                  gz = (long long)br.b3[2] * (a.is2d ? 1 : 32) + z;
+        long long src = (gz * a.fdims[1] + gy) * a.fdims[0] + gx;
+        double v = a.field_f32 ? (double)((const float*)a.field)[src] : ((const double*)a.field)[src];
+        F[(z * 33 + y) * 33 + x] = v;
+        mn = v < mn ? v : mn;
+        mx = mx < v ? v : mx;
+      }
+      for (int o = 16; o > 0; o >>= 1)
+      {
+        double w1 = __shfl_xor_sync(0xffffffffu, mn, o), w2 = __shfl_xor_sync(0xffffffffu, mx, o);
+        mn = w1 < mn ? w1 : mn;
+        mx = mx < w2 ? w2 : mx;
+      }
+      if (lane == 0)
+      {
+        sm.red[0][warp] = mn;
+        sm.red[1][warp] = mx;
+      }
+      __syncthreads();
+      if (tid == 0)
+      {
+        for (int w = 1; w < kWarps; ++w)
+        {
+          mn = sm.red[0][w] < mn ? sm.red[0][w] : mn;
+          mx = mx < sm.red[1][w] ? sm.red[1][w] : mx;
+        }
+        a.bmin[bi] = mn;
+        a.bmax[bi] = mx;
+      }
+    }
+    else
+    {
+      const double* src = a.in_bricks + (size_t)bi * (size_t)NB;
+      for (int i = tid; i < NB; i += kThreads)
+        F[i] = src[i];
+    }
+    __syncthreads();
+
+    // ---------------- B: transform ----------------
+    {
+      const int M[3] = { 32, 32, a.is2d ? 1 : 32 };
+      if (tid == 0)
+        dev::build_stack(br.valid, 5, a.order, &sm.stack);
+      __syncthreads();
+      const int nf = sm.stack.n;
+      for (int i = 0; i < nf; ++i)
+      {
+        dev::lift_sweep(F, N, sm.stack.g[i], M, sm.stack.axis[i], true);
+        __syncthreads();
+      }
+      if (tid == 0)
+        dev::build_stack(N, 5, a.order, &sm.stack);
+      __syncthreads();
+      const int ni = sm.stack.n;
+      for (int i = ni - 1; i >= 0; --i)
+      {
+        dev::lift_sweep(F, N, sm.stack.g[i], M, sm.stack.axis[i], false);
+        __syncthreads();
+      }
+      dev::dgrid G;
+      for (int k = 0; k < 3; ++k)
+      {
+        G.from[k] = 0;
+        G.dims[k] = N[k];
+        G.strd[k] = 1;
+      }
+      for (int ax = 0; ax < (a.is2d ? 2 : 3); ++ax)
+      {
+        dev::lift_sweep(F, N, G, N, ax, true);
+        __syncthreads();
+      }
+      for (int s = 0; s < a.nsb; ++s)
+      {
+        if (!((a.norm_mask >> s) & 1))
+          continue;
+        int from[3], dims[3], strd[3];
+        subband_grid(a.is2d, s, from, dims, strd);
+        const double W = a.weight[s];
+        const int n = dims[0] * dims[1] * dims[2];
+        for (int i = tid; i < n; i += kThreads)
+        {
+          int x = i % dims[0], y = (i / dims[0]) % dims[1], z = i / (dims[0] * dims[1]);
+          int idx = ((from[2] + z * strd[2]) * 33 + (from[1] + y * strd[1])) * 33 + (from[0] + x * strd[0]);
+          F[idx] = __dmul_rn(F[idx], W);
+        }
+      }
+      __syncthreads();
+    }
+
+    // ---------------- C: low band to the parent ----------------
+    if (a.parent_bricks && br.parent >= 0)
+    {
+      double* P = a.parent_bricks + (size_t)br.parent * (size_t)NB;
+      const int nz = a.is2d ? 1 : 16;
+      for (int i = tid; i < 16 * 16 * nz; i += kThreads)
+      {
+        int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
+        int cz = a.is2d ? 0 : 2 * z;
+        P[((br.pos[2] * nz + z) * 33 + (br.pos[1] * 16 + y)) * 33 + (br.pos[0] * 16 + x)] =
+          F[(cz * 33 + 2 * y) * 33 + 2 * x];
+      }
+    }
+
+    // ---------------- D: block coding per subband ----------------
+    for (int s = 0; s < a.nsb; ++s)
+    {
+      int from[3], dims[3], strd[3];
+      subband_grid(a.is2d, s, from, dims, strd);
+      const int nb = a.nblocks[s];
+      const uint64_t* geom = a.geom + (size_t)s * kMaxBlocksPerSubband;
+      const size_t bs = (size_t)bi * (size_t)a.nsb + (size_t)s;
+
+      // D1: warp per block
+      for (int b = warp; b < nb; b += kWarps)
+      {
+        int d3[3], bd[3];
+        unpack_geom(geom[b], d3, bd);
+        const int nd = (bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1);
+        const int nv = 1 << (2 * nd);
+        const int prec = 63 - nd;
+        long long* q = sm.q[warp];
+        double v0 = 0, v1 = 0;
+        int j0 = lane, j1 = lane + 32;
+        if (j0 < nv)
+        {
+          int x = j0 % bd[0], y = (j0 / bd[0]) % bd[1], z = j0 / (bd[0] * bd[1]);
+          v0 = F[((from[2] + (d3[2] + z) * strd[2]) * 33 + (from[1] + (d3[1] + y) * strd[1])) * 33 +
+                 (from[0] + (d3[0] + x) * strd[0])];
+        }
+        if (j1 < nv)
+        {
+          int x = j1 % bd[0], y = (j1 / bd[0]) % bd[1], z = j1 / (bd[0] * bd[1]);
+          v1 = F[((from[2] + (d3[2] + z) * strd[2]) * 33 + (from[1] + (d3[1] + y) * strd[1])) * 33 +
+                 (from[0] + (d3[0] + x) * strd[0])];
+        }
+        double m = fabs(v0);
+        double m1 = fabs(v1);
+        m = m < m1 ? m1 : m;
+        m = warp_max(m);
+        const int emax = a.f32_exp ? dev::exponent_f32(__double2float_rn(m)) : dev::exponent_f64(m);
+        const double scale = dev::pow2(prec - 1 - emax);
+        if (j0 < nv)
+          q[j0] = dev::trunc_i64(__dmul_rn(scale, v0));
+        if (j1 < nv)
+          q[j1] = dev::trunc_i64(__dmul_rn(scale, v1));
+        __syncwarp();
+        dev::warp_fwd_zfp(q, nd, lane);
+        unsigned long long u0 = 0, u1 = 0;
+        if (j0 < nv)
+          u0 = ((unsigned long long)q[dev::perm(nd, j0)] + dev::kNegaMask) ^ dev::kNegaMask;
+        if (j1 < nv)
+          u1 = ((unsigned long long)q[dev::perm(nd, j1)] + dev::kNegaMask) ^ dev::kNegaMask;
+        __syncwarp();
+        const int np = dev::coded_planes(emax, a.etol, a.end_bp);
+        for (int k = 0; k < np; ++k)
+        {
+          const int bit = 63 - k;
+          unsigned lo = __ballot_sync(0xffffffffu, (u0 >> bit) & 1ull);
+          unsigned hi = __ballot_sync(0xffffffffu, (u1 >> bit) & 1ull);
+          if (lane == 0)
+            sm.X[b][k] = (unsigned long long)lo | ((unsigned long long)hi << 32);
+        }
+        if (lane == 0)
+        {
+          sm.emax[b] = (int16_t)emax;
+          sm.ktop[b] = (int16_t)(emax + 63 + 1024);
+          sm.np[b] = (uint8_t)np;
+          sm.nvals_log[b] = (uint8_t)(2 * nd);
+          a.exps[bs * kMaxBlocksPerSubband + (size_t)b] = (int16_t)emax;
+        }
+      }
+      __syncthreads();
+
+      // D2: significance chain per block
+      for (int b = tid; b < nb; b += kThreads)
+      {
+        int n = 0;
+        const int np = sm.np[b];
+        for (int k = 0; k < np; ++k)
+        {
+          sm.nin[b][k] = (uint8_t)n;
+          n = dev::plane_nout(sm.X[b][k], n);
+        }
+      }
+      if (tid == 0)
+      {
+        int kmin = 1 << 30, kmax = -(1 << 30);
+        for (int b = 0; b < nb; ++b)
+        {
+          if (!sm.np[b])
+            continue;
+          int lo = sm.ktop[b] - sm.np[b] + 1, hi = sm.ktop[b];
+          kmin = lo < kmin ? lo : kmin;
+          kmax = hi > kmax ? hi : kmax;
+        }
+        if (kmax < kmin)
+        {
+          kmin = 1;
+          kmax = 0;
+        }
+        sm.kmin = kmin;
+        sm.kmax = kmax;
+        sm.ok = (kmax - kmin + 1) <= kKeyWindow;
+        if (!sm.ok)
+          atomicExch(a.error, 1);
+      }
+      __syncthreads();
+      const int kmin = sm.kmin, kmax = sm.kmax;
+      const int nkeys = sm.ok ? kmax - kmin + 1 : 0;
+
+      // D3: per channel key, bit offsets of the blocks in Morton order
+      for (int t = tid; t < nkeys; t += kThreads)
+      {
+        const int key = kmin + t;
+        unsigned acc = 0;
+        for (int b = 0; b < nb; ++b)
+        {
+          const int kk = sm.ktop[b] - key;
+          if (kk < 0 || kk >= sm.np[b])
+            continue;
+          sm.off[b][kk] = (uint16_t)acc;
+          acc += (unsigned)dev::plane_bits(sm.X[b][kk], sm.nin[b][kk], 1 << sm.nvals_log[b]);
+        }
+        sm.key_bits[t] = acc;
+      }
+      __syncthreads();
+
+      // D4: channel byte bases and the region of this (brick, subband)
+      if (tid == 0)
+      {
+        unsigned base = 0;
+        for (int t = 0; t < nkeys; ++t)
+        {
+          sm.key_base[t] = base;
+          base += (sm.key_bits[t] + 7) / 8;
+        }
+        unsigned long long region = atomicAdd(a.cursor, (unsigned long long)base);
+        if (region + base > a.cap_bytes)
+          atomicExch(a.error, 2);
+        sm.region = region;
+        a.offset[bs] = region;
+        a.kmin[bs] = nkeys ? kmin : 1;
+        a.kmax[bs] = nkeys ? kmax : 0;
+      }
+      __syncthreads();
+      for (int t = tid; t < kKeyWindow; t += kThreads)
+        a.sizes[bs * kKeyWindow + (size_t)t] = t < nkeys ? (sm.key_bits[t] + 7) / 8 : 0u;
+      const unsigned long long region = sm.region;
+      const bool fits = region + (nkeys ? sm.key_base[nkeys - 1] + (sm.key_bits[nkeys - 1] + 7) / 8 : 0) <=
+                        a.cap_bytes;
+
+      // D5: scatter the plane bits
+      if (fits)
+      {
+        for (int idx = tid; idx < nb * kMaxPlanes; idx += kThreads)
+        {
+          const int b = idx >> 6, kk = idx & 63;
+          if (kk >= sm.np[b])
+            continue;
+          const int t = sm.ktop[b] - kk - kmin;
+          const unsigned long long pos =
+            (region + sm.key_base[t]) * 8ull + (unsigned long long)sm.off[b][kk];
+          dev::write_plane(a.stream, pos, sm.X[b][kk], sm.nin[b][kk], 1 << sm.nvals_log[b]);
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Host-side weights of one level (Core/Wavelet.cpp:111-137, Core/Wavelet.h:19).
+void level_weights(const dataset_format& f, int level, double w[8], int* mask)
+{
+  double scal[16], wave[16];
+  double n1 = 3, n2 = 23;
+  for (int i = 0; i < 16; ++i)
+  {
+    scal[i] = sqrt(n1 / (1 << (i + 1)));
+    n1 = n1 * 4 - 1;
+    wave[i] = sqrt(n2 / (1 << (i + 5)));
+    n2 = n2 * 4 - 33;
+  }
+  const bool coarsest = level + 1 == f.nlevels;
+  *mask = 0;
+  for (int s = 0; s < f.nsubbands(); ++s)
+  {
+    const subband& sb = f.subbands[(size_t)s];
+    double wx = f.brick_dims_ext.x == 1 ? 1
+                : (sb.low_high.x == 0 ? scal[level + sb.level_rev.x - 1] : wave[level + sb.level_rev.x]);
+    double wy = f.brick_dims_ext.y == 1 ? 1
+                : (sb.low_high.y == 0 ? scal[level + sb.level_rev.y - 1] : wave[level + sb.level_rev.y]);
+    double wz = f.brick_dims_ext.z == 1 ? 1
+                : (sb.low_high.z == 0 ? scal[level + sb.level_rev.z - 1] : wave[level + sb.level_rev.z]);
+    w[s] = wx * wy * wz;
+    if (s == 0 && !coarsest)
+      continue;
+    *mask |= 1 << s;
+  }
+}
+
+} // namespace
+
+// ---------------------------------------------------------------------------
+// device stage
+// ---------------------------------------------------------------------------
+
+gpu_coder::gpu_coder(device_ctx* ctx, const dataset_format& f, const void* d_field, bool field_f32)
+  : ctx_(ctx), f_(f), d_field_(d_field), field_f32_(field_f32)
+{
+}
+
+gpu_coder::~gpu_coder()
+{
+  for (void* p : owned_)
+    cudaFree(p);
+}
+
+void* gpu_coder::dev_alloc(size_t bytes)
+{
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess)
+    return nullptr;
+  owned_.push_back(p);
+  return p;
+}
+
+int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
+{
+  if (f_.bit_planes_per_chunk != 1)
+    return OptionNotSupported;
+  if (f_.brick_dims.x != 32 || f_.brick_dims.y != 32 || (f_.brick_dims.z != 32 && f_.brick_dims.z != 1))
+    return OptionNotSupported;
+  cudaStream_t st = ctx_->stream;
+  const bool is2d = f_.is2d();
+  const int NB = 33 * 33 * (is2d ? 1 : 33);
+  const std::vector<brick_entry>& bricks = plan.levels[(size_t)level];
+  const int nbr = (int)bricks.size();
+  const int nsb = f_.nsubbands();
+  const bool has_parent = level + 1 < f_.nlevels;
+  const int npar = has_parent ? (int)plan.levels[(size_t)level + 1].size() : 0;
+
+  std::vector<enc_brick> hb((size_t)nbr);
+  for (int i = 0; i < nbr; ++i)
+  {
+    const brick_entry& e = bricks[(size_t)i];
+    hb[(size_t)i] = enc_brick{ { e.brick3.x, e.brick3.y, e.brick3.z },
+                               { e.valid.x, e.valid.y, e.valid.z },
+                               e.parent,
+                               { e.pos_in_parent.x, e.pos_in_parent.y, e.pos_in_parent.z } };
+  }
+  std::vector<uint64_t> geom((size_t)nsb * kMaxBlocksPerSubband, 0);
+  std::vector<int> nblocks((size_t)nsb, 0);
+  for (int s = 0; s < nsb; ++s)
+  {
+    std::vector<block_geom> g;
+    subband_blocks(f_, level, s, &g);
+    nblocks[(size_t)s] = (int)g.size();
+    for (size_t b = 0; b < g.size(); ++b)
+      geom[(size_t)s * kMaxBlocksPerSubband + b] =
+        (uint64_t)g[b].dx | ((uint64_t)g[b].dy << 8) | ((uint64_t)g[b].dz << 16) |
+        ((uint64_t)g[b].bx << 24) | ((uint64_t)g[b].by << 32) | ((uint64_t)g[b].bz << 40);
+  }
+
+  enc_args a;
+  memset(&a, 0, sizeof a);
+  a.level = level;
+  a.nlevels = f_.nlevels;
+  a.is2d = is2d;
+  a.f32_exp = f_.type == dtype::float32;
+  a.etol = exponent_f64(f_.tolerance);
+  a.end_bp = f_.type == dtype::float32 ? 32 : 64;
+  a.nsb = nsb;
+  a.nbricks = nbr;
+  a.order = f_.transform_order;
+  a.field = d_field_;
+  a.field_f32 = field_f32_;
+  a.fdims[0] = f_.dims.x;
+  a.fdims[1] = f_.dims.y;
+  a.fdims[2] = f_.dims.z;
+  level_weights(f_, level, a.weight, &a.norm_mask);
+
+  auto* d_bricks = (enc_brick*)dev_alloc(sizeof(enc_brick) * (size_t)nbr);
+  auto* d_geom = (uint64_t*)dev_alloc(geom.size() * 8);
+  auto* d_nblocks = (int*)dev_alloc((size_t)nsb * sizeof(int));
+  if (!d_bricks || !d_geom || !d_nblocks)
+    return OutOfMemory;
+  cudaMemcpyAsync(d_bricks, hb.data(), sizeof(enc_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_geom, geom.data(), geom.size() * 8, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_nblocks, nblocks.data(), (size_t)nsb * sizeof(int), cudaMemcpyHostToDevice, st);
+
+  int nsm = ctx_->num_sms;
+  int grid = nbr < 2 * nsm ? nbr : 2 * nsm;
+  if (grid < 1)
+    grid = 1;
+  double* d_slots = (double*)dev_alloc((size_t)grid * (size_t)NB * sizeof(double));
+  double* d_parents = has_parent ? (double*)dev_alloc((size_t)npar * (size_t)NB * sizeof(double)) : nullptr;
+  const size_t nbs = (size_t)nbr * (size_t)nsb;
+  auto* d_exps = (int16_t*)dev_alloc(nbs * kMaxBlocksPerSubband * 2);
+  auto* d_kmin = (int32_t*)dev_alloc(nbs * 4);
+  auto* d_kmax = (int32_t*)dev_alloc(nbs * 4);
+  auto* d_off = (unsigned long long*)dev_alloc(nbs * 8);
+  auto* d_sizes = (uint32_t*)dev_alloc(nbs * kKeyWindow * 4);
+  auto* d_misc = (unsigned long long*)dev_alloc(64);
+  double* d_bmin = (double*)dev_alloc((size_t)nbr * 8);
+  double* d_bmax = (double*)dev_alloc((size_t)nbr * 8);
+  if (!d_slots || (has_parent && !d_parents) || !d_exps || !d_kmin || !d_kmax || !d_off || !d_sizes ||
+      !d_misc || !d_bmin || !d_bmax)
+    return OutOfMemory;
+
+  unsigned long long cap = (unsigned long long)nbr * 16384ull + (16ull << 20);
+  for (int attempt = 0; attempt < 4; ++attempt)
+  {
+    uint32_t* d_stream = (uint32_t*)dev_alloc((size_t)cap);
+    if (!d_stream)
+      return OutOfMemory;
+    cudaMemsetAsync(d_stream, 0, (size_t)cap, st);
+    cudaMemsetAsync(d_misc, 0, 64, st);
+    if (has_parent)
+      cudaMemsetAsync(d_parents, 0, (size_t)npar * (size_t)NB * sizeof(double), st);
+    a.bricks = d_bricks;
+    a.in_bricks = level > 0 ? in_bricks_ : nullptr;
+    a.slots = d_slots;
+    a.parent_bricks = d_parents;
+    a.geom = d_geom;
+    a.nblocks = d_nblocks;
+    a.exps = d_exps;
+    a.kmin = d_kmin;
+    a.kmax = d_kmax;
+    a.offset = d_off;
+    a.sizes = d_sizes;
+    a.stream = d_stream;
+    a.cap_bytes = cap;
+    a.cursor = d_misc;
+    a.error = (int*)(d_misc + 1);
+    a.bmin = d_bmin;
+    a.bmax = d_bmax;
+    const size_t smem = sizeof(enc_smem);
+    cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaEvent_t ev0, ev1;
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+    cudaEventRecord(ev0, st);
+    k_encode_level<<<grid, kThreads, smem, st>>>(a);
+    cudaEventRecord(ev1, st);
+    if (cudaGetLastError() != cudaSuccess)
+      return CudaError;
+    ++launches_;
+    unsigned long long misc[2];
+    cudaMemcpyAsync(misc, d_misc, 16, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
+    int err = (int)(misc[1] & 0xffffffffu);
+    if (err == 1)
+      return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
+    if (err == 2)
+    {
+      cap = misc[0] + (1ull << 20);
+      continue;
+    }
+    kernel_ms_ += ms;
+    stream_bytes_ += (long long)misc[0];
+    for (int s = 0; s < nsb; ++s)
+      exp_bytes_ += (long long)nbr * nblocks[(size_t)s] * (f_.type == dtype::float32 ? 1 : 2);
+    // results to the host
+    out->nbricks = nbr;
+    out->nsb = nsb;
+    out->nexps = nblocks;
+    out->exps.resize(nbs * kMaxBlocksPerSubband);
+    out->kmin.resize(nbs);
+    out->kmax.resize(nbs);
+    out->offset.resize(nbs);
+    out->sizes.resize(nbs * kKeyWindow);
+    out->stream.resize((size_t)misc[0]);
+    cudaMemcpyAsync(out->exps.data(), d_exps, nbs * kMaxBlocksPerSubband * 2, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->kmin.data(), d_kmin, nbs * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->kmax.data(), d_kmax, nbs * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->offset.data(), d_off, nbs * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->sizes.data(), d_sizes, nbs * kKeyWindow * 4, cudaMemcpyDeviceToHost, st);
+    if (misc[0])
+      cudaMemcpyAsync(out->stream.data(), d_stream, (size_t)misc[0], cudaMemcpyDeviceToHost, st);
+    if (level == 0)
+    {
+      std::vector<double> mn((size_t)nbr), mx((size_t)nbr);
+      cudaMemcpyAsync(mn.data(), d_bmin, (size_t)nbr * 8, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(mx.data(), d_bmax, (size_t)nbr * 8, cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess)
+        return CudaError;
+      for (int i = 0; i < nbr; ++i)
+      {
+        vmin_ = mn[(size_t)i] < vmin_ ? mn[(size_t)i] : vmin_;
+        vmax_ = vmax_ < mx[(size_t)i] ? mx[(size_t)i] : vmax_;
+      }
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    in_bricks_ = d_parents;
+    return NoError;
+  }
+  return DeviceStreamOverflow;
+}
+
+void gpu_coder::value_range(double* vmin, double* vmax)
+{
+  *vmin = vmin_;
+  *vmax = vmax_;
+}
+
+} // namespace idx2g

@@ -1,0 +1,92 @@
+"""Decode side of the Python mirror: idx2::Init / GetOutputGrid / Decode / Destroy
+(idx2.cpp:23-52) over the C ABI."""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from ._lib import Idx2Error, Params, ctx, lib
+
+
+class Dataset:
+    """A compressed dataset made resident on the device (idx2g_dataset_open)."""
+
+    def __init__(self, idx2_file: str, in_dir: Optional[str] = None, device: int = 0):
+        if in_dir is None:
+            # the CLI's rule: the directory two levels above the .idx2 file
+            parent = os.path.dirname(idx2_file)
+            in_dir = os.path.dirname(parent) or "."
+            if in_dir == parent:
+                in_dir = "./"
+        self.device = device
+        self.params = Params(input_file=idx2_file, in_dir=in_dir)
+        self._ctx = ctx(device)
+        h = ctypes.c_void_p()
+        cp = self.params.to_c()
+        rc = lib().idx2g_dataset_open(self._ctx.h, ctypes.byref(cp), ctypes.byref(h))
+        if rc:
+            raise Idx2Error(rc, "idx2g_dataset_open")
+        self.h = h
+
+    def _req(self, first, last, downsampling, tolerance) -> Params:
+        p = Params(input_file=self.params.input_file, in_dir=self.params.in_dir,
+                   downsampling=tuple(downsampling), decode_tolerance=float(tolerance))
+        if first is not None:
+            p.first, p.last = tuple(first), tuple(last)
+        return p
+
+    def output_grid(self, first=None, last=None, downsampling=(0, 0, 0)):
+        p = self._req(first, last, downsampling, 0.0)
+        f, d, s = (ctypes.c_int * 3)(), (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+        cp = p.to_c()
+        rc = lib().idx2g_output_grid(self.h, ctypes.byref(cp), f, d, s)
+        if rc:
+            raise Idx2Error(rc, "idx2g_output_grid")
+        return tuple(f), tuple(d), tuple(s)
+
+    def decode(self, first: Optional[Sequence[int]] = None, last: Optional[Sequence[int]] = None,
+               downsampling=(0, 0, 0), tolerance: float = 0.0, out=None, dtype=None):
+        """Decode to a numpy array (or into `out`: numpy array or CUDA torch tensor) shaped
+        (nz, ny, nx) of the output grid."""
+        _, dims, _ = self.output_grid(first, last, downsampling)
+        p = self._req(first, last, downsampling, tolerance)
+        cp = p.to_c()
+        if out is None:
+            out = np.zeros((dims[2], dims[1], dims[0]), dtype=dtype or self.dtype)
+        on_dev = 0
+        try:
+            import torch
+            if isinstance(out, torch.Tensor):
+                on_dev = int(out.is_cuda)
+                ptr, nbytes = out.data_ptr(), out.numel() * out.element_size()
+            else:
+                ptr, nbytes = out.ctypes.data, out.nbytes
+        except ImportError:
+            ptr, nbytes = out.ctypes.data, out.nbytes
+        kms = ctypes.c_double(0)
+        rc = lib().idx2g_decode(self._ctx.h, self.h, ctypes.byref(cp), ctypes.c_void_p(ptr),
+                                ctypes.c_size_t(nbytes), on_dev, ctypes.byref(kms))
+        if rc:
+            raise Idx2Error(rc, "idx2g_decode")
+        self.last_kernel_ms = kms.value
+        return out
+
+    @property
+    def dtype(self):
+        with open(self.params.input_file) as f:
+            txt = f.read()
+        return np.float32 if '"float32"' in txt else np.float64
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().idx2g_dataset_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

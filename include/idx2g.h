@@ -1,0 +1,117 @@
+/* idx2g: B200 (sm_100a) implementation of the idx2 encode/decode hot path.
+ *
+ * C ABI: plain pointers, sizes and integer error codes; no C++ or torch types.
+ * The entry points replace the reference's library calls for this path:
+ *
+ *   idx2g_encode          <- idx2::Encode(idx2_file*, const params&, brick_copier&)
+ *                            (Source/Core/idx2Encode.h:144, Core/idx2Encode.cpp:390)
+ *                            together with the SetParams + Finalize steps of idx2App
+ *                            (Source/Applications/idx2App.cpp:217, Core/idx2Common.cpp:726)
+ *   idx2g_check_params    <- Finalize's validation (Core/idx2Common.cpp:726-754)
+ *   idx2g_dataset_open    <- idx2::Init(idx2_file*, params&) (Source/idx2.cpp:23)
+ *   idx2g_output_grid     <- idx2::GetOutputGrid (Source/idx2.cpp:36, Core/idx2Common.cpp:772)
+ *   idx2g_decode          <- idx2::Decode(idx2_file*, params&, buffer*) (Source/idx2.cpp:43,
+ *                            Core/idx2Decode.cpp:326) with OutMode RegularGridMem
+ *   idx2g_dataset_close   <- idx2::Destroy (Source/idx2.cpp:52)
+ *
+ * Error codes are the reference's idx2_err_code values (Core/ErrorCodes.h:6-10 followed by
+ * Core/idx2Common.h:36-56): 0 is NoError, 22 BrickSizeTooBig, 23 TooManyLevels, ...
+ * Codes >= 100 belong to this library (see idx2g_error_string).
+ *
+ * Threading: one idx2g_ctx per host thread; all device work of a context is ordered on its
+ * CUDA stream. The caller owns every buffer it passes in.
+ */
+#ifndef IDX2G_H
+#define IDX2G_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IDX2G_API __attribute__((visibility("default")))
+
+enum
+{
+  IDX2G_FLOAT32 = 0,
+  IDX2G_FLOAT64 = 1
+};
+
+/* Mirrors idx2::params (Core/idx2Common.h:74-108). */
+typedef struct idx2g_params
+{
+  /* metadata and encode parameters */
+  char name[64];
+  char field[64];
+  int dims[3];
+  int dtype;               /* IDX2G_FLOAT32 or IDX2G_FLOAT64 */
+  int brick_dims[3];       /* default 32 32 32; 2D fields use 32 32 1 */
+  int num_levels;          /* 0: guess as the reference does */
+  double tolerance;        /* absolute tolerance of the encode */
+  int bricks_per_chunk;    /* default 4096 */
+  int chunks_per_file;     /* default 64 */
+  int files_per_dir;       /* default 64 */
+  int bit_planes_per_chunk;/* default 1 */
+  int bit_planes_per_file; /* default 16 */
+  int version[2];          /* 1 0 */
+  char out_dir[512];       /* encode output directory (default ".") */
+  /* decode parameters */
+  char input_file[512];    /* path of the .idx2 metadata file */
+  char in_dir[512];        /* directory holding <name>/<field>/... (default ".") */
+  int has_extent;          /* 1: decode only [first, last] (inclusive) */
+  int first[3];
+  int last[3];
+  int downsampling[3];     /* per-axis downsampling factor (power of two exponent) */
+  double decode_tolerance;
+} idx2g_params;
+
+typedef struct idx2g_encode_info
+{
+  double kernel_ms;        /* device time of the brick kernels (CUDA events) */
+  double device_s;         /* wall time of the device stage incl. copies */
+  double pack_s;           /* host packing (chunks, zstd) */
+  double write_s;          /* file writes */
+  long long stream_bytes;  /* bit-plane stream bytes produced on the device */
+  long long exp_bytes;     /* uncompressed exponent bytes */
+  long long file_bytes;    /* total bytes of the written files */
+  long long kernel_launches;
+  double value_min, value_max;
+} idx2g_encode_info;
+
+typedef struct idx2g_ctx idx2g_ctx;
+typedef struct idx2g_dataset idx2g_dataset;
+
+/* Defaults of the reference's params / idx2App options. */
+IDX2G_API void idx2g_params_init(idx2g_params* p);
+IDX2G_API const char* idx2g_error_string(int code);
+IDX2G_API const char* idx2g_version(void);
+
+/* device: CUDA ordinal; stream: a cudaStream_t or NULL (the context creates one). */
+IDX2G_API int idx2g_ctx_create(int device, void* stream, idx2g_ctx** ctx);
+IDX2G_API int idx2g_ctx_destroy(idx2g_ctx* ctx);
+
+/* Validate encode parameters exactly as Finalize does; returns the reference's code. */
+IDX2G_API int idx2g_check_params(const idx2g_params* p);
+
+/* Encode a field (x fastest, dims from p) and write <out_dir>/<name>/<field>.idx2 and the
+   data files. field_on_device: 1 if field is a device pointer on the context's device. */
+IDX2G_API int idx2g_encode(idx2g_ctx* ctx, const idx2g_params* p, const void* field,
+                           int field_on_device, idx2g_encode_info* info);
+
+/* Decode side (idx2.cpp:23-52). open reads the metadata file (p->input_file) and the chunk
+   index of every data file and makes the compressed dataset resident on the device. */
+IDX2G_API int idx2g_dataset_open(idx2g_ctx* ctx, const idx2g_params* p, idx2g_dataset** ds);
+IDX2G_API int idx2g_output_grid(const idx2g_dataset* ds, const idx2g_params* p, int from3[3],
+                                int dims3[3], int strd3[3]);
+/* Decode into out (Prod(dims3) elements of the dataset's dtype). out_on_device: 1 if out is
+   a device pointer on the context's device. */
+IDX2G_API int idx2g_decode(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p, void* out,
+                           size_t out_bytes, int out_on_device, double* kernel_ms);
+IDX2G_API int idx2g_dataset_close(idx2g_dataset* ds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
