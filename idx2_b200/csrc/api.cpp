@@ -270,4 +270,31 @@ IDX2G_API int idx2g_dataset_close(idx2g_dataset* ds)
   return NoError;
 }
 
+IDX2G_API int idx2g_dataset_info(const idx2g_dataset* ds, char* name, char* field, int dims3[3],
+                                 int* dt, int* num_levels, double* tolerance, long long* resident)
+{
+  if (!ds)
+    return InvalidArgument;
+  const dataset_format& f = dataset_fmt((const dataset_handle*)ds);
+  if (name)
+    snprintf(name, 64, "%s", f.name.c_str());
+  if (field)
+    snprintf(field, 64, "%s", f.field.c_str());
+  if (dims3)
+  {
+    dims3[0] = f.dims.x;
+    dims3[1] = f.dims.y;
+    dims3[2] = f.dims.z;
+  }
+  if (dt)
+    *dt = f.type == dtype::float32 ? IDX2G_FLOAT32 : IDX2G_FLOAT64;
+  if (num_levels)
+    *num_levels = f.nlevels;
+  if (tolerance)
+    *tolerance = f.tolerance;
+  if (resident)
+    *resident = (long long)dataset_resident_bytes((const dataset_handle*)ds);
+  return NoError;
+}
+
 } // extern "C"

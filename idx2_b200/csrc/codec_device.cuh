@@ -27,7 +27,7 @@ __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 // One CDF5/3 lifting sweep along axis a over the lines of grid G, split over the
 // threads of the CTA (Core/Wavelet.h:178 FLiftCdf53, :250 ILiftCdf53, lift_option
 // Normal). Each thread runs whole lines in the reference's sample order.
-__device__ void lift_sweep(double* F, const int N[3], const dgrid& G, const int M[3], int a,
+inline __device__ void lift_sweep(double* F, const int N[3], const dgrid& G, const int M[3], int a,
                            bool forward)
 {
   const int P = G.from[a], D = G.dims[a], S = G.strd[a];
@@ -112,7 +112,7 @@ struct lift_stack
   int n;
 };
 
-__device__ void build_stack(const int dims3[3], int nlevels, uint64_t order, lift_stack* st)
+inline __device__ void build_stack(const int dims3[3], int nlevels, uint64_t order, lift_stack* st)
 {
   int level = 0;
   uint64_t prev = order;
@@ -381,7 +381,7 @@ __device__ __forceinline__ void or_bits(uint32_t* words, unsigned long long pos,
 
 // Write the bits of one plane (Core/Zfp.h:771 Encode<u64>) at bit position pos of a
 // zero-initialised stream. Only one-bits are stored.
-__device__ void write_plane(uint32_t* words, unsigned long long pos, unsigned long long x, int nin,
+inline __device__ void write_plane(uint32_t* words, unsigned long long pos, unsigned long long x, int nin,
                             int nvals)
 {
   // raw bits of the already significant coefficients

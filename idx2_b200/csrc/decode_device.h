@@ -60,6 +60,7 @@ private:
   unsigned long long* first_ = nullptr;
   unsigned long long* off_ = nullptr;
   uint8_t* blob_ = nullptr;
+  size_t blob_bytes_ = 0;
   size_t resident_ = 0;
 };
 

@@ -530,4 +530,8 @@ int dataset_decode(device_ctx* ctx, dataset_handle* h, const params& p, void* ou
 
 void dataset_close(dataset_handle* h) { delete h; }
 
+const dataset_format& dataset_fmt(const dataset_handle* h) { return h->f; }
+
+size_t dataset_resident_bytes(const dataset_handle* h) { return h->dev.resident_bytes(); }
+
 } // namespace idx2g

@@ -15,5 +15,7 @@ int dataset_output_grid(const dataset_handle* ds, const params& p, grid* g);
 int dataset_decode(device_ctx* ctx, dataset_handle* ds, const params& p, void* out, size_t out_bytes,
                    bool out_on_device, double* kernel_ms);
 void dataset_close(dataset_handle* ds);
+const dataset_format& dataset_fmt(const dataset_handle* ds);
+size_t dataset_resident_bytes(const dataset_handle* ds);
 
 } // namespace idx2g

@@ -110,6 +110,13 @@ IDX2G_API int idx2g_decode(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params
                            size_t out_bytes, int out_on_device, double* kernel_ms);
 IDX2G_API int idx2g_dataset_close(idx2g_dataset* ds);
 
+/* Metadata of an open dataset (the fields of the .idx2 file): name and field (64 bytes
+   each, NUL-terminated), dims, dtype, number of levels, encode tolerance, and the bytes
+   the dataset keeps resident on the device. */
+IDX2G_API int idx2g_dataset_info(const idx2g_dataset* ds, char* name, char* field, int dims3[3],
+                                 int* dtype, int* num_levels, double* tolerance,
+                                 long long* resident_bytes);
+
 #ifdef __cplusplus
 }
 #endif

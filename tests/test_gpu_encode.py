@@ -66,3 +66,24 @@ def test_encode_from_device_tensor(idx2g, ref_app, tmp_path):
     idx2g.encode(t, out_dir=str(tmp_path / "ours"), name="kat", field_name="f",
                  num_levels=levels, tolerance=tol)
     assert compare_dirs(ref_dir, str(tmp_path / "ours" / "kat")) == []
+
+
+def _golden_cases():
+    import json
+    here = os.path.dirname(os.path.abspath(__file__))
+    return json.load(open(os.path.join(here, "golden", "datasets.json")))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", _golden_cases(), ids=lambda c: c["name"])
+def test_encode_matches_golden_files(idx2g, tmp_path, case):
+    """Against the committed reference output (no reference build needed)."""
+    import hashlib
+    from golden.golden_inputs import make_dataset_field
+    f = make_dataset_field(case)
+    assert hashlib.sha256(f.tobytes()).hexdigest() == case["field_sha"]
+    idx2g.encode(f, out_dir=str(tmp_path), name=case["name"], field_name="f", num_levels=case["levels"],
+                 tolerance=case["tol"], brick_dims=tuple(case["brick"]))
+    here = os.path.dirname(os.path.abspath(__file__))
+    diffs = compare_dirs(os.path.join(here, "golden", "datasets", case["name"]), str(tmp_path / case["name"]))
+    assert diffs == [], diffs[:3]
