@@ -1,0 +1,366 @@
+#!/usr/bin/env python
+"""Benchmark of the idx2 encode/decode hot path on B200.
+
+Workload (default, "grf1024"): a 1024^3 float32 k^-5/3 Gaussian random field (seeded,
+unit variance) with 20 tanh fronts of width 2 cells, 3 levels, 32^3 bricks, absolute
+tolerance 1e-3. One step = encode the field (every level) + decode it back at full
+resolution and the encode tolerance. The synthetic field stands in for a simulation
+dataset (no dataset is available offline). Inputs are 4.3 GB per direction, far larger
+than L2 (126 MB), so no L2 flush is needed between steps.
+
+  value : encode+decode GB/s of raw field bytes (2 x 4.29 GB per step) with the field and
+          the compressed dataset resident in HBM (idx2g_encode_device + idx2g_decode into a
+          device buffer), timed with CUDA events on the library's stream, max over ranks.
+  e2e   : the same metric through the C ABI with host buffers: idx2g_encode of a pinned host
+          field (H2D, kernels, D2H, packing, zstd, files in a tmpfs) + idx2g_dataset_open of
+          the files + idx2g_decode into a pinned host buffer.
+
+N > 1 (torchrun): every rank encodes/decodes its own independent field (weak scaling, no
+collective on the data path; timing uses a barrier and a max-reduction over ranks).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--side 1024]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+LEVELS = 3
+TOL = 1e-3
+METRIC = "encode+decode GB/s (raw field bytes) at 1e-3 tol"
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[0]))
+                mx = float(s[1])
+                for n, v in zip(names, s[3:7]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except Exception:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_field(side, seed, device):
+    from idx2_b200.synthetic import grf_field_torch
+    return grf_field_torch(side, side, side, seed=seed, scale="unit", n_fronts=20, device=device)
+
+
+def reference_sample(side):
+    """Bounded CPU sample of the workload: same generator, 512 x 512 x 256 region."""
+    import torch
+    nx, ny, nz = min(512, side), min(512, side), min(256, side)
+    f = make_field(side, 7, "cuda" if torch.cuda.is_available() else "cpu")
+    return f[:nz, :ny, :nx].contiguous().cpu().numpy()
+
+
+def run_reference_cli(sample, tmp, steps, warmup):
+    """Encode + sequential decode of the sample with the reference's own CLI (oracle/_ref)."""
+    app = os.path.join(ROOT, "oracle", "_ref", "idx2App")
+    nz, ny, nx = sample.shape
+    raw = os.path.join(tmp, f"grf-f-[{nx}-{ny}-{nz}]-Float32.raw")
+    sample.tofile(raw)
+    times = []
+    for i in range(warmup + steps):
+        out = os.path.join(tmp, "refds")
+        shutil.rmtree(out, ignore_errors=True)
+        t0 = time.perf_counter()
+        r = subprocess.run([app, "--encode", raw, "--num_levels", str(LEVELS), "--tolerance", str(TOL),
+                            "--out_dir", out], capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-300:] + r.stderr[-300:])
+        r = subprocess.run([app, "--decode", os.path.join(out, "grf", "f.idx2"), "--out_dir", tmp,
+                            "--out_file", "dec.raw"], capture_output=True, text=True)
+        if r.returncode:
+            raise RuntimeError(r.stdout[-300:] + r.stderr[-300:])
+        t1 = time.perf_counter()
+        if i >= warmup:
+            times.append(t1 - t0)
+    return times
+
+
+def cpu_baseline(side, steps=1, warmup=0):
+    app = os.path.join(ROOT, "oracle", "_ref", "idx2App")
+    if not os.path.exists(app):
+        return {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref was not built on this machine"}
+    sample = reference_sample(side)
+    with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as tmp:
+        times = run_reference_cli(sample, tmp, steps, warmup)
+    t = statistics.median(times)
+    nz, ny, nx = sample.shape
+    return {"value": 2 * sample.nbytes / t / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+            "sample": f"{nx}x{ny}x{nz} float32 region of the same field; idx2App --encode (L={LEVELS}, "
+                      f"tol {TOL}) + sequential --decode, median of {len(times)}, {t:.2f} s per pass"}
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    app = os.path.join(ROOT, "oracle", "_ref", "idx2App")
+    if not os.path.exists(app):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference built from "
+                          "its sources) is not present on this machine"}))
+        return
+    sample = reference_sample(args.side)
+    with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as tmp:
+        times = run_reference_cli(sample, tmp, args.steps, args.warmup)
+    t = sum(times) / len(times)
+    nz, ny, nx = sample.shape
+    v = 2 * sample.nbytes / t / 1e9
+    desc = (f"{nx}x{ny}x{nz} float32 region of the {args.side}^3 field per step; idx2App --encode + "
+            f"sequential --decode (the reference encode is single-threaded)")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"grf{args.side}: {args.side}^3 float32 k^-5/3 GRF + 20 fronts, "
+                       f"{LEVELS} levels, 32^3 bricks, tol {TOL}; encode + full-res decode",
+                       "parallelism": f"dp{world}"},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": 1, "kind": "reference", "sample": desc},
+            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def ours(args, rank, world, local_rank):
+    import ctypes
+    import torch
+    import idx2_b200 as idx2
+    from idx2_b200 import _lib
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    side = args.side
+    field = make_field(side, 7 + rank, dev)
+    raw_bytes = field.numel() * field.element_size()
+    stream = torch.cuda.Stream(device=dev)
+    h = ctypes.c_void_p()
+    rc = _lib.lib().idx2g_ctx_create(local_rank, ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h))
+    assert rc == 0, rc
+    p = _lib.Params(name="grf", field="f", dims=(side, side, side), dtype="float32", num_levels=LEVELS,
+                    tolerance=TOL)
+    cp = p.to_c()
+    tmp = tempfile.mkdtemp(prefix=f"idx2bench{rank}_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        # one encode to files, and the dataset made resident for the device-side decode
+        host = field.cpu().pin_memory()
+        cpo = _lib.Params(name="grf", field="f", dims=(side, side, side), dtype="float32", num_levels=LEVELS,
+                          tolerance=TOL, out_dir=tmp).to_c()
+        info = _lib.EncodeInfo()
+        rc = _lib.lib().idx2g_encode(h, ctypes.byref(cpo), ctypes.c_void_p(host.data_ptr()), 0, ctypes.byref(info))
+        assert rc == 0, rc
+        dsp = _lib.Params(input_file=os.path.join(tmp, "grf", "f.idx2"), in_dir=tmp).to_c()
+        dsh = ctypes.c_void_p()
+        rc = _lib.lib().idx2g_dataset_open(h, ctypes.byref(dsp), ctypes.byref(dsh))
+        assert rc == 0, rc
+        out_dev = torch.empty_like(field)
+        out_host = torch.empty(field.shape, dtype=field.dtype).pin_memory()
+        kms = ctypes.c_double(0)
+
+        def device_step(rec):
+            einfo = _lib.EncodeInfo()
+            rc = _lib.lib().idx2g_encode_device(h, ctypes.byref(cp), ctypes.c_void_p(field.data_ptr()),
+                                                ctypes.byref(einfo))
+            assert rc == 0, rc
+            rc = _lib.lib().idx2g_decode(h, dsh, ctypes.byref(dsp), ctypes.c_void_p(out_dev.data_ptr()),
+                                         ctypes.c_size_t(raw_bytes), 1, ctypes.byref(kms))
+            assert rc == 0, rc
+            if rec is not None:
+                rec.append((einfo.num_levels, [einfo.level_kernel_ms[i] for i in range(einfo.num_levels)],
+                            [einfo.level_out_bytes[i] for i in range(einfo.num_levels)], kms.value,
+                            einfo.kernel_launches))
+
+        for _ in range(args.warmup):
+            device_step(None)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        recs = []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local_rank) as clocks:
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(args.steps):
+                device_step(recs)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        dev_ms = e0.elapsed_time(e1) / args.steps
+        # correctness of the timed decode: full-resolution output within the expected error
+        max_err = float((out_dev.double() - field.double()).abs().max())
+        t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t)
+
+        # e2e through the C ABI with host buffers
+        e2e_times = []
+        h2d = d2h = 0
+        for i in range(0 if args.no_e2e else args.warmup + args.steps):
+            shutil.rmtree(os.path.join(tmp, "e2e"), ignore_errors=True)
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p2 = _lib.Params(name="grf", field="f", dims=(side, side, side), dtype="float32",
+                             num_levels=LEVELS, tolerance=TOL, out_dir=os.path.join(tmp, "e2e")).to_c()
+            info2 = _lib.EncodeInfo()
+            rc = _lib.lib().idx2g_encode(h, ctypes.byref(p2), ctypes.c_void_p(host.data_ptr()), 0,
+                                         ctypes.byref(info2))
+            assert rc == 0, rc
+            dp2 = _lib.Params(input_file=os.path.join(tmp, "e2e", "grf", "f.idx2"),
+                              in_dir=os.path.join(tmp, "e2e")).to_c()
+            dh2 = ctypes.c_void_p()
+            rc = _lib.lib().idx2g_dataset_open(h, ctypes.byref(dp2), ctypes.byref(dh2))
+            assert rc == 0, rc
+            rc = _lib.lib().idx2g_decode(h, dh2, ctypes.byref(dp2), ctypes.c_void_p(out_host.data_ptr()),
+                                         ctypes.c_size_t(raw_bytes), 0, ctypes.byref(kms))
+            assert rc == 0, rc
+            rsd = ctypes.c_longlong(0)
+            _lib.lib().idx2g_dataset_info(dh2, None, None, (ctypes.c_int * 3)(), None, None, None,
+                                          ctypes.byref(rsd))
+            _lib.lib().idx2g_dataset_close(dh2)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            if i >= args.warmup:
+                e2e_times.append(t1 - t0)
+                h2d = raw_bytes + rsd.value
+                d2h = raw_bytes + info2.stream_bytes + info2.exp_bytes
+        tt = torch.tensor([sum(e2e_times) / len(e2e_times) if e2e_times else float("nan")], device=dev,
+                          dtype=torch.float64)
+        if dist:
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt)
+        _lib.lib().idx2g_dataset_close(dsh)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        _lib.lib().idx2g_ctx_destroy(h)
+        return
+    nlev, lvl_ms, lvl_bytes, dec_ms, launches = recs[-1]
+    enc_ms = sum(sum(r[1]) for r in recs) / len(recs)
+    # dominant kernel: the level-0 encode launch
+    l0_ms = sum(r[1][0] for r in recs) / len(recs)
+    l0_bytes = raw_bytes + lvl_bytes[0]
+    peak, kind = hbm_peak()
+    achieved = l0_bytes / (l0_ms * 1e-3) / 1e9
+    value = world * 2 * raw_bytes / (dev_ms * 1e-3) / 1e9
+    base = cpu_baseline(side) if world == 1 and not args.no_cpu else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded k^-5/3 GRF, 20 tanh fronts)",
+        "config": {"workload": f"grf{side}: {side}^3 float32 k^-5/3 GRF + 20 fronts, {LEVELS} levels, 32^3 "
+                               f"bricks, tol {TOL}; step = encode (all levels) + full-res decode",
+                   "parallelism": f"dp{world} (independent field per GPU)",
+                   "l2": "inputs (4.3 GB) >> L2; no flush needed"},
+        "encode_gbs": raw_bytes / (enc_ms * 1e-3) / 1e9,
+        "decode_gbs": raw_bytes / (dec_ms * 1e-3) / 1e9,
+        "encode_level_ms": lvl_ms, "decode_ms": dec_ms,
+        "compressed_bytes": int(sum(lvl_bytes)),
+        "decode_max_abs_err": max_err,
+        "roofline": {"bound": "hbm", "kernel": "k_encode_level (level 0)", "achieved": achieved,
+                     "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else kind,
+                     "algorithmic_bytes": l0_bytes, "traffic": None},
+        "cpu_baseline": base,
+        "e2e": {"value": world * 2 * raw_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s},
+        "clocks": clocks.summary(),
+        "gpu_launches": int(args.steps * (launches + LEVELS)),
+    }
+    print(json.dumps(line))
+    if dist:
+        dist.destroy_process_group()
+    _lib.lib().idx2g_ctx_destroy(h)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--side", type=int, default=1024)
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg (profiling runs)")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

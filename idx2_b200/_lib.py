@@ -62,6 +62,9 @@ class EncodeInfo(ctypes.Structure):
         ("kernel_launches", ctypes.c_longlong),
         ("value_min", ctypes.c_double),
         ("value_max", ctypes.c_double),
+        ("num_levels", ctypes.c_int),
+        ("level_kernel_ms", ctypes.c_double * 16),
+        ("level_out_bytes", ctypes.c_longlong * 16),
     ]
 
 
@@ -87,6 +90,12 @@ def lib():
             L.idx2g_check_params.argtypes = [ctypes.POINTER(_CParams)]
             L.idx2g_encode.argtypes = [ctypes.c_void_p, ctypes.POINTER(_CParams), ctypes.c_void_p,
                                        ctypes.c_int, ctypes.POINTER(EncodeInfo)]
+            L.idx2g_encode_device.argtypes = [ctypes.c_void_p, ctypes.POINTER(_CParams), ctypes.c_void_p,
+                                              ctypes.POINTER(EncodeInfo)]
+            L.idx2g_dataset_info.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,
+                                             ctypes.c_int * 3, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_longlong)]
             L.idx2g_dataset_open.argtypes = [ctypes.c_void_p, ctypes.POINTER(_CParams),
                                              ctypes.POINTER(ctypes.c_void_p)]
             L.idx2g_output_grid.argtypes = [ctypes.c_void_p, ctypes.POINTER(_CParams),
@@ -248,4 +257,22 @@ def encode(field, out_dir: str = ".", name: str = "field", field_name: str = "da
     del keep
     if rc:
         raise Idx2Error(rc, "idx2g_encode")
+    return info
+
+
+def encode_device(field, num_levels: int, tolerance: float, brick_dims=None, device: int = 0) -> EncodeInfo:
+    """Device stage of the encoder on a CUDA tensor (no packing, no files)."""
+    ptr, on_dev, dt, dims, keep = _field_ptr(field)
+    if not on_dev:
+        raise Idx2Error(101, "encode_device needs a CUDA tensor")
+    if brick_dims is None:
+        brick_dims = (32, 32, 1) if dims[2] == 1 else (32, 32, 32)
+    p = Params(name="f", field="f", dims=dims, dtype=dt, brick_dims=brick_dims, num_levels=num_levels,
+               tolerance=tolerance)
+    cp = p.to_c()
+    info = EncodeInfo()
+    rc = lib().idx2g_encode_device(ctx(device).h, ctypes.byref(cp), ctypes.c_void_p(ptr), ctypes.byref(info))
+    del keep
+    if rc:
+        raise Idx2Error(rc, "idx2g_encode_device")
     return info

@@ -137,6 +137,8 @@ IDX2G_API int idx2g_ctx_create(int device, void* stream, idx2g_ctx** out)
     }
     c->d.own_stream = true;
   }
+  cudaEventCreate(&c->d.ev0);
+  cudaEventCreate(&c->d.ev1);
   *out = c;
   return NoError;
 }
@@ -145,6 +147,10 @@ IDX2G_API int idx2g_ctx_destroy(idx2g_ctx* c)
 {
   if (!c)
     return NoError;
+  cudaSetDevice(c->d.device);
+  if (c->d.stream)
+    cudaStreamSynchronize(c->d.stream);
+  c->d.release();
   if (c->d.own_stream && c->d.stream)
     cudaStreamDestroy(c->d.stream);
   delete c;
@@ -190,6 +196,8 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
   long long stream_bytes = 0, exp_bytes = 0;
   double kms = 0;
   long long launches = 0;
+  std::vector<float> lms;
+  std::vector<long long> lbytes;
   {
     gpu_coder coder(&c->d, f, d_field, f32);
     e = encode_dataset(&f, &p, &coder, &files, true, &tm);
@@ -197,6 +205,8 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
     exp_bytes = coder.exp_bytes();
     kms = coder.kernel_ms();
     launches = coder.kernel_launches();
+    lms = coder.level_ms();
+    lbytes = coder.level_bytes();
   }
   if (owned)
     cudaFree(owned);
@@ -221,6 +231,52 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
     info->kernel_launches = launches;
     info->value_min = f.value_min;
     info->value_max = f.value_max;
+    info->num_levels = (int)lms.size();
+    for (size_t i = 0; i < lms.size() && i < 16; ++i)
+    {
+      info->level_kernel_ms[i] = lms[i];
+      info->level_out_bytes[i] = lbytes[i];
+    }
+  }
+  return NoError;
+}
+
+IDX2G_API int idx2g_encode_device(idx2g_ctx* c, const idx2g_params* in, const void* d_field,
+                                  idx2g_encode_info* info)
+{
+  if (!c || !in || !d_field)
+    return InvalidArgument;
+  cudaSetDevice(c->d.device);
+  params p;
+  to_params(in, &p);
+  dataset_format f;
+  int e = finalize(&f, &p);
+  if (e)
+    return e;
+  gpu_coder coder(&c->d, f, d_field, p.type == dtype::float32);
+  coder.set_keep_device(true);
+  std::vector<level_output> outs;
+  auto t0 = std::chrono::steady_clock::now();
+  e = encode_levels(&f, &coder, &outs);
+  auto t1 = std::chrono::steady_clock::now();
+  if (e)
+    return e;
+  if (info)
+  {
+    memset(info, 0, sizeof *info);
+    info->kernel_ms = coder.kernel_ms();
+    info->device_s = std::chrono::duration<double>(t1 - t0).count();
+    info->stream_bytes = coder.stream_bytes();
+    info->exp_bytes = coder.exp_bytes();
+    info->kernel_launches = coder.kernel_launches();
+    info->value_min = f.value_min;
+    info->value_max = f.value_max;
+    info->num_levels = (int)coder.level_ms().size();
+    for (size_t i = 0; i < coder.level_ms().size() && i < 16; ++i)
+    {
+      info->level_kernel_ms[i] = coder.level_ms()[i];
+      info->level_out_bytes[i] = coder.level_bytes()[i];
+    }
   }
   return NoError;
 }

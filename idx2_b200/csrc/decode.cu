@@ -424,31 +424,17 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   const int NB = 33 * 33 * (rq.is2d ? 1 : 33);
-  std::vector<void*> tmp;
-  auto alloc = [&](size_t bytes) -> void* {
-    void* p = nullptr;
-    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess)
-      return nullptr;
-    tmp.push_back(p);
-    return p;
-  };
-  auto cleanup = [&]() {
-    for (void* p : tmp)
-      cudaFree(p);
-  };
+  auto cleanup = []() {};
   void* d_out = out;
   if (!out_on_device)
   {
-    d_out = alloc(out_bytes);
+    d_out = ctx->ws("dec.out", out_bytes);
     if (!d_out)
-    {
-      cleanup();
       return OutOfMemory;
-    }
   }
   cudaMemsetAsync(d_out, 0, out_bytes, st);
-  int* d_err = (int*)alloc(16);
-  uint64_t* d_geom = (uint64_t*)alloc(sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
+  int* d_err = (int*)ctx->ws("dec.err", 16);
+  uint64_t* d_geom = (uint64_t*)ctx->ws("dec.geom", sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
   if (!d_err || !d_geom)
   {
     cleanup();
@@ -457,20 +443,21 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
   cudaMemsetAsync(d_err, 0, 16, st);
   const size_t smem = sizeof(dec_smem);
   cudaFuncSetAttribute(k_decode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
+  cudaEvent_t e0 = ctx->ev0, e1 = ctx->ev1;
   float total_ms = 0;
   double* prev = nullptr;
+  int li = 0;
   for (const decode_level& lv : rq.levels)
   {
+    ++li;
     const int nbr = (int)lv.bricks.size();
     if (nbr == 0)
       continue;
-    decode_brick* d_bricks = (decode_brick*)alloc(sizeof(decode_brick) * (size_t)nbr);
-    double* d_level = lv.is_output ? nullptr : (double*)alloc((size_t)nbr * (size_t)NB * 8);
+    decode_brick* d_bricks = (decode_brick*)ctx->ws("dec.bricks", sizeof(decode_brick) * (size_t)nbr);
+    double* d_level =
+      lv.is_output ? nullptr : (double*)ctx->ws(li % 2 ? "dec.levA" : "dec.levB", (size_t)nbr * (size_t)NB * 8);
     int grid = nbr < 2 * ctx->num_sms ? nbr : 2 * ctx->num_sms;
-    double* d_slots = lv.is_output ? (double*)alloc((size_t)grid * (size_t)NB * 8) : nullptr;
+    double* d_slots = lv.is_output ? (double*)ctx->ws("dec.slots", (size_t)grid * (size_t)NB * 8) : nullptr;
     if (!d_bricks || (!lv.is_output && !d_level) || (lv.is_output && !d_slots))
     {
       cleanup();
@@ -531,8 +518,6 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
     if (lv.is_output)
       break;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   int herr = 0;
   cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, st);
   if (!out_on_device)

@@ -473,20 +473,7 @@ gpu_coder::gpu_coder(device_ctx* ctx, const dataset_format& f, const void* d_fie
 {
 }
 
-gpu_coder::~gpu_coder()
-{
-  for (void* p : owned_)
-    cudaFree(p);
-}
-
-void* gpu_coder::dev_alloc(size_t bytes)
-{
-  void* p = nullptr;
-  if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess)
-    return nullptr;
-  owned_.push_back(p);
-  return p;
-}
+gpu_coder::~gpu_coder() {}
 
 int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
 {
@@ -543,41 +530,44 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
   a.fdims[2] = f_.dims.z;
   level_weights(f_, level, a.weight, &a.norm_mask);
 
-  auto* d_bricks = (enc_brick*)dev_alloc(sizeof(enc_brick) * (size_t)nbr);
-  auto* d_geom = (uint64_t*)dev_alloc(geom.size() * 8);
-  auto* d_nblocks = (int*)dev_alloc((size_t)nsb * sizeof(int));
-  if (!d_bricks || !d_geom || !d_nblocks)
+  // workspace buffers, kept by the context across calls (grow-only)
+  int nsm = ctx_->num_sms;
+  int grid = nbr < 2 * nsm ? nbr : 2 * nsm;
+  if (grid < 1)
+    grid = 1;
+  const size_t nbs = (size_t)nbr * (size_t)nsb;
+  auto* d_bricks = (enc_brick*)ctx_->ws("enc.bricks", sizeof(enc_brick) * (size_t)nbr);
+  auto* d_geom = (uint64_t*)ctx_->ws("enc.geom", geom.size() * 8);
+  auto* d_nblocks = (int*)ctx_->ws("enc.nblocks", (size_t)nsb * sizeof(int));
+  double* d_slots = (double*)ctx_->ws("enc.slots", (size_t)grid * (size_t)NB * sizeof(double));
+  double* d_parents = has_parent ? (double*)ctx_->ws(level % 2 ? "enc.parA" : "enc.parB",
+                                                     (size_t)npar * (size_t)NB * sizeof(double))
+                                 : nullptr;
+  auto* d_exps = (int16_t*)ctx_->ws(level % 2 ? "enc.expsA" : "enc.expsB", nbs * kMaxBlocksPerSubband * 2);
+  auto* d_kmin = (int32_t*)ctx_->ws(level % 2 ? "enc.kminA" : "enc.kminB", nbs * 4);
+  auto* d_kmax = (int32_t*)ctx_->ws(level % 2 ? "enc.kmaxA" : "enc.kmaxB", nbs * 4);
+  auto* d_off = (unsigned long long*)ctx_->ws(level % 2 ? "enc.offA" : "enc.offB", nbs * 8);
+  auto* d_sizes = (uint32_t*)ctx_->ws(level % 2 ? "enc.sizesA" : "enc.sizesB", nbs * kKeyWindow * 4);
+  auto* d_misc = (unsigned long long*)ctx_->ws("enc.misc", 64);
+  double* d_bmin = (double*)ctx_->ws("enc.bmin", (size_t)nbr * 8);
+  double* d_bmax = (double*)ctx_->ws("enc.bmax", (size_t)nbr * 8);
+  if (!d_bricks || !d_geom || !d_nblocks || !d_slots || (has_parent && !d_parents) || !d_exps || !d_kmin ||
+      !d_kmax || !d_off || !d_sizes || !d_misc || !d_bmin || !d_bmax)
     return OutOfMemory;
   cudaMemcpyAsync(d_bricks, hb.data(), sizeof(enc_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_geom, geom.data(), geom.size() * 8, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_nblocks, nblocks.data(), (size_t)nsb * sizeof(int), cudaMemcpyHostToDevice, st);
 
-  int nsm = ctx_->num_sms;
-  int grid = nbr < 2 * nsm ? nbr : 2 * nsm;
-  if (grid < 1)
-    grid = 1;
-  double* d_slots = (double*)dev_alloc((size_t)grid * (size_t)NB * sizeof(double));
-  double* d_parents = has_parent ? (double*)dev_alloc((size_t)npar * (size_t)NB * sizeof(double)) : nullptr;
-  const size_t nbs = (size_t)nbr * (size_t)nsb;
-  auto* d_exps = (int16_t*)dev_alloc(nbs * kMaxBlocksPerSubband * 2);
-  auto* d_kmin = (int32_t*)dev_alloc(nbs * 4);
-  auto* d_kmax = (int32_t*)dev_alloc(nbs * 4);
-  auto* d_off = (unsigned long long*)dev_alloc(nbs * 8);
-  auto* d_sizes = (uint32_t*)dev_alloc(nbs * kKeyWindow * 4);
-  auto* d_misc = (unsigned long long*)dev_alloc(64);
-  double* d_bmin = (double*)dev_alloc((size_t)nbr * 8);
-  double* d_bmax = (double*)dev_alloc((size_t)nbr * 8);
-  if (!d_slots || (has_parent && !d_parents) || !d_exps || !d_kmin || !d_kmax || !d_off || !d_sizes ||
-      !d_misc || !d_bmin || !d_bmax)
-    return OutOfMemory;
-
+  const char* sname = level % 2 ? "enc.streamA" : "enc.streamB";
   unsigned long long cap = (unsigned long long)nbr * 16384ull + (16ull << 20);
+  if (ctx_->ws_size(sname) > cap)
+    cap = ctx_->ws_size(sname);
   for (int attempt = 0; attempt < 4; ++attempt)
   {
-    uint32_t* d_stream = (uint32_t*)dev_alloc((size_t)cap);
+    uint32_t* d_stream = (uint32_t*)ctx_->ws_zeroed(sname, (size_t)cap);
     if (!d_stream)
       return OutOfMemory;
-    cudaMemsetAsync(d_stream, 0, (size_t)cap, st);
+    cap = ctx_->ws_size(sname);
     cudaMemsetAsync(d_misc, 0, 64, st);
     if (has_parent)
       cudaMemsetAsync(d_parents, 0, (size_t)npar * (size_t)NB * sizeof(double), st);
@@ -600,12 +590,9 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     a.bmax = d_bmax;
     const size_t smem = sizeof(enc_smem);
     cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaEvent_t ev0, ev1;
-    cudaEventCreate(&ev0);
-    cudaEventCreate(&ev1);
-    cudaEventRecord(ev0, st);
+    cudaEventRecord(ctx_->ev0, st);
     k_encode_level<<<grid, kThreads, smem, st>>>(a);
-    cudaEventRecord(ev1, st);
+    cudaEventRecord(ctx_->ev1, st);
     if (cudaGetLastError() != cudaSuccess)
       return CudaError;
     ++launches_;
@@ -614,9 +601,8 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     if (cudaStreamSynchronize(st) != cudaSuccess)
       return CudaError;
     float ms = 0;
-    cudaEventElapsedTime(&ms, ev0, ev1);
-    cudaEventDestroy(ev0);
-    cudaEventDestroy(ev1);
+    cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
+    ctx_->ws_mark_dirty(sname, (size_t)(misc[0] < cap ? misc[0] : cap));
     int err = (int)(misc[1] & 0xffffffffu);
     if (err == 1)
       return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
@@ -626,26 +612,16 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
       continue;
     }
     kernel_ms_ += ms;
+    level_ms_.push_back(ms);
     stream_bytes_ += (long long)misc[0];
+    long long eb = 0;
     for (int s = 0; s < nsb; ++s)
-      exp_bytes_ += (long long)nbr * nblocks[(size_t)s] * (f_.type == dtype::float32 ? 1 : 2);
-    // results to the host
+      eb += (long long)nbr * nblocks[(size_t)s] * (f_.type == dtype::float32 ? 1 : 2);
+    exp_bytes_ += eb;
+    level_bytes_.push_back((long long)misc[0] + eb);
     out->nbricks = nbr;
     out->nsb = nsb;
     out->nexps = nblocks;
-    out->exps.resize(nbs * kMaxBlocksPerSubband);
-    out->kmin.resize(nbs);
-    out->kmax.resize(nbs);
-    out->offset.resize(nbs);
-    out->sizes.resize(nbs * kKeyWindow);
-    out->stream.resize((size_t)misc[0]);
-    cudaMemcpyAsync(out->exps.data(), d_exps, nbs * kMaxBlocksPerSubband * 2, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->kmin.data(), d_kmin, nbs * 4, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->kmax.data(), d_kmax, nbs * 4, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->offset.data(), d_off, nbs * 8, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->sizes.data(), d_sizes, nbs * kKeyWindow * 4, cudaMemcpyDeviceToHost, st);
-    if (misc[0])
-      cudaMemcpyAsync(out->stream.data(), d_stream, (size_t)misc[0], cudaMemcpyDeviceToHost, st);
     if (level == 0)
     {
       std::vector<double> mn((size_t)nbr), mx((size_t)nbr);
@@ -659,8 +635,25 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
         vmax_ = vmax_ < mx[(size_t)i] ? mx[(size_t)i] : vmax_;
       }
     }
-    if (cudaStreamSynchronize(st) != cudaSuccess)
-      return CudaError;
+    if (!keep_device_)
+    {
+      // results to the host for the packer
+      out->exps.resize(nbs * kMaxBlocksPerSubband);
+      out->kmin.resize(nbs);
+      out->kmax.resize(nbs);
+      out->offset.resize(nbs);
+      out->sizes.resize(nbs * kKeyWindow);
+      out->stream.resize((size_t)misc[0]);
+      cudaMemcpyAsync(out->exps.data(), d_exps, nbs * kMaxBlocksPerSubband * 2, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(out->kmin.data(), d_kmin, nbs * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(out->kmax.data(), d_kmax, nbs * 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(out->offset.data(), d_off, nbs * 8, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(out->sizes.data(), d_sizes, nbs * kKeyWindow * 4, cudaMemcpyDeviceToHost, st);
+      if (misc[0])
+        cudaMemcpyAsync(out->stream.data(), d_stream, (size_t)misc[0], cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess)
+        return CudaError;
+    }
     in_bricks_ = d_parents;
     return NoError;
   }

@@ -165,23 +165,35 @@ static double now_s()
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_output>* outs,
+                  encode_plan* plan_out)
+{
+  encode_plan local;
+  encode_plan& plan = plan_out ? *plan_out : local;
+  int e = make_encode_plan(*f, &plan);
+  if (e)
+    return e;
+  outs->assign((size_t)f->nlevels, level_output());
+  for (int l = 0; l < f->nlevels; ++l)
+  {
+    e = coder->run_level(l, plan, &(*outs)[(size_t)l]);
+    if (e)
+      return e;
+  }
+  coder->value_range(&f->value_min, &f->value_max);
+  return NoError;
+}
+
 int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
                    std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
                    encode_timing* timing)
 {
   encode_plan plan;
-  int e = make_encode_plan(*f, &plan);
+  double t0 = now_s();
+  std::vector<level_output> outs;
+  int e = encode_levels(f, coder, &outs, &plan);
   if (e)
     return e;
-  double t0 = now_s();
-  std::vector<level_output> outs((size_t)f->nlevels);
-  for (int l = 0; l < f->nlevels; ++l)
-  {
-    e = coder->run_level(l, plan, &outs[(size_t)l]);
-    if (e)
-      return e;
-  }
-  coder->value_range(&f->value_min, &f->value_max);
   double t1 = now_s();
 
   packer pk(*f, f->tolerance);

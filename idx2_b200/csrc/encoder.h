@@ -92,6 +92,10 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
                    std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
                    encode_timing* timing);
 
+// The device stage only: plan + every level through the coder.
+int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_output>* outs,
+                  encode_plan* plan_out = nullptr);
+
 int write_file(const std::string& path, const std::vector<uint8_t>& data);
 int make_dirs_for(const std::string& path);
 

@@ -70,3 +70,46 @@ def grf_field(nx: int, ny: int, nz: int, seed: int = 7, scale: str = "range",
         s = f.std()
         f = (f - f.mean()) / (s if s > 0 else 1.0)
     return f.astype(dtype)
+
+
+def grf_field_torch(nx: int, ny: int, nz: int, seed: int = 7, scale: str = "unit", n_fronts: int = 0,
+                    device: str = "cuda", dtype=None):
+    """GPU version of grf_field for large fields (e.g. 1024^3): a k^-5/3 Gaussian random
+    field generated with torch.fft on the device, optional tanh shells (width 2 cells)."""
+    import torch
+    dtype = dtype or torch.float32
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    noise = torch.randn((nz, ny, nx), generator=g, device=device, dtype=torch.float32)
+    spec = torch.fft.rfftn(noise)
+    del noise
+    kz = torch.fft.fftfreq(nz, device=device)[:, None, None]
+    ky = torch.fft.fftfreq(ny, device=device)[None, :, None]
+    kx = torch.fft.rfftfreq(nx, device=device)[None, None, :]
+    k = torch.sqrt(kx * kx + ky * ky + kz * kz)
+    k[0, 0, 0] = 1.0
+    amp = k.pow(-(5.0 / 3.0 + 2.0) / 2.0)
+    amp[0, 0, 0] = 0.0
+    spec *= amp
+    del k, amp
+    f = torch.fft.irfftn(spec, s=(nz, ny, nx))
+    del spec
+    if n_fronts:
+        cpu = torch.Generator()
+        cpu.manual_seed(seed + 1)
+        std = float(f.std())
+        zz = torch.arange(nz, device=device, dtype=torch.float32)[:, None, None]
+        yy = torch.arange(ny, device=device, dtype=torch.float32)[None, :, None]
+        xx = torch.arange(nx, device=device, dtype=torch.float32)[None, None, :]
+        for _ in range(n_fronts):
+            c = torch.rand(3, generator=cpu) * torch.tensor([nx, ny, nz], dtype=torch.float32)
+            r0 = float(0.05 + 0.25 * torch.rand(1, generator=cpu)) * min(nx, ny, max(nz, 1))
+            r = torch.sqrt((xx - float(c[0])) ** 2 + (yy - float(c[1])) ** 2 + (zz - float(c[2])) ** 2)
+            f += std * torch.tanh((r - r0) / 2.0)
+            del r
+    if scale == "range":
+        lo, hi = f.min(), f.max()
+        f = 2.0 * (f - lo) / (hi - lo) - 1.0
+    elif scale == "unit":
+        f = (f - f.mean()) / f.std()
+    return f.to(dtype).contiguous()

@@ -77,6 +77,9 @@ typedef struct idx2g_encode_info
   long long file_bytes;    /* total bytes of the written files */
   long long kernel_launches;
   double value_min, value_max;
+  int num_levels;
+  double level_kernel_ms[16];      /* device time of each level's launch */
+  long long level_out_bytes[16];   /* stream + exponent bytes produced by each level */
 } idx2g_encode_info;
 
 typedef struct idx2g_ctx idx2g_ctx;
@@ -98,6 +101,12 @@ IDX2G_API int idx2g_check_params(const idx2g_params* p);
    data files. field_on_device: 1 if field is a device pointer on the context's device. */
 IDX2G_API int idx2g_encode(idx2g_ctx* ctx, const idx2g_params* p, const void* field,
                            int field_on_device, idx2g_encode_info* info);
+
+/* The device stage of idx2g_encode alone: transform and code every brick of every level of
+   a device-resident field, leaving the coded streams in the context's device workspace (no
+   packing, no files). For measuring the kernels; the streams are the ones idx2g_encode packs. */
+IDX2G_API int idx2g_encode_device(idx2g_ctx* ctx, const idx2g_params* p, const void* d_field,
+                                  idx2g_encode_info* info);
 
 /* Decode side (idx2.cpp:23-52). open reads the metadata file (p->input_file) and the chunk
    index of every data file and makes the compressed dataset resident on the device. */
