@@ -394,14 +394,25 @@ int dataset_output_grid(const dataset_handle* h, const params& p, grid* g)
 int dataset_decode(device_ctx* ctx, dataset_handle* h, const params& p, void* out, size_t out_bytes,
                    bool out_on_device, double* kernel_ms)
 {
+  decode_request rq;
+  size_t need = 0;
+  int e = plan_decode(h, p, &rq, &need);
+  if (e)
+    return e;
+  if (out_bytes < need)
+    return SizeTooSmall;
+  return h->dev.decode(ctx, rq, out, need, out_on_device, kernel_ms);
+}
+
+int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out, size_t* need_out)
+{
   dataset_format f;
   request_format(h, p, &f);
   extent ext = p.has_extent ? p.decode_extent : extent{ v3(0), f.dims };
   grid og = output_grid(f, ext);
   const size_t esz = f.type == dtype::float32 ? 4 : 8;
   const size_t need = (size_t)prod(og.dims) * esz;
-  if (out_bytes < need)
-    return SizeTooSmall;
+  *need_out = need;
   const double tol = std::max(f.tolerance, p.decode_tolerance);  // Core/idx2Decode.cpp:364
   const int L = f.nlevels;
   const int nsb = f.nsubbands();
@@ -525,7 +536,8 @@ int dataset_decode(device_ctx* ctx, dataset_handle* h, const params& p, void* ou
     }
     rq.levels.push_back(std::move(lv));
   }
-  return h->dev.decode(ctx, rq, out, need, out_on_device, kernel_ms);
+  *rq_out = std::move(rq);
+  return NoError;
 }
 
 void dataset_close(dataset_handle* h) { delete h; }

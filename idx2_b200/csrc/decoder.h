@@ -9,6 +9,11 @@ namespace idx2g
 {
 
 struct dataset_handle;
+struct decode_request;
+
+// Plan a decode request on the host (ROI, downsampling masks, tolerance, per-level brick
+// lists); need_bytes is the size of the output grid.
+int plan_decode(const dataset_handle* ds, const params& p, decode_request* rq, size_t* need_bytes);
 
 int dataset_open(device_ctx* ctx, const params& p, dataset_handle** out);
 int dataset_output_grid(const dataset_handle* ds, const params& p, grid* g);
