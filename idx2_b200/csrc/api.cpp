@@ -101,6 +101,8 @@ IDX2G_API const char* idx2g_error_string(int code)
       return "DeviceStreamOverflow";
     case CorruptStream:
       return "CorruptStream";
+    case ScratchTooSmall:
+      return "ScratchTooSmall";
     default:
       return "Unknown";
   }
@@ -318,6 +320,18 @@ IDX2G_API int idx2g_decode(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* 
   params p;
   to_params(in, &p);
   return dataset_decode(&c->d, (dataset_handle*)ds, p, out, out_bytes, out_on_device != 0, kernel_ms);
+}
+
+// Allocation-free decode (include/idx2g.h): for callers that cannot allocate device memory at
+// decode time; all temporaries are in the fixed scratch array of decode.cu.
+IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* in, void* d_out,
+                                   size_t out_bytes, double* kernel_ms)
+{
+  if (!c || !ds || !in || !d_out)
+    return InvalidArgument;
+  params p;
+  to_params(in, &p);
+  return dataset_decode_noalloc(&c->d, (dataset_handle*)ds, p, d_out, out_bytes, kernel_ms);
 }
 
 IDX2G_API int idx2g_dataset_close(idx2g_dataset* ds)

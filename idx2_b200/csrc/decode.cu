@@ -15,6 +15,7 @@
 #include "decode_device.h"
 
 #include <cstring>
+#include <mutex>
 
 namespace idx2g
 {
@@ -525,6 +526,174 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
   cudaError_t ce = cudaStreamSynchronize(st);
   cleanup();
   if (ce != cudaSuccess)
+    return CudaError;
+  if (herr)
+    return DeviceStreamOverflow;
+  if (kernel_ms)
+    *kernel_ms = total_ms;
+  return NoError;
+}
+
+
+// ---------------------------------------------------------------------------
+// Allocation-free decode (idx2g_decode_noalloc)
+//
+// For callers that cannot allocate device memory at decode time: applications whose device
+// memory is owned by another allocator (a framework's caching allocator or a pool sized to
+// the whole GPU) and latency-bound serving loops, where a cudaMalloc either fails or
+// synchronises the device. Such a caller opens the dataset once beforehand (that step
+// allocates the resident dataset) and then decodes into its own device buffer; every
+// temporary of the decode lives in the fixed array below.
+//
+// The array is a file-scope __device__ variable: every GPU that loads this library holds its
+// kNoAllocScratchBytes (about 7.3 MB) until the process exits. Limits: at most
+// kNoAllocMaxBricks bricks on the output level and at most kNoAllocLevelBricks bricks on each
+// coarser level a request decodes; larger requests are rejected with ScratchTooSmall.
+// All calls share the array and it keeps the last call's contents: the error word is cleared
+// at the start of every call, and calls that overlap on the GPU (on different streams or
+// different contexts of the same device) race on it.
+// ---------------------------------------------------------------------------
+
+namespace
+{
+
+constexpr int kNoAllocSlots = 8;          // output-level brick slots (= CTAs of that launch)
+constexpr int kNoAllocLevelBricks = 8;    // bricks of each coarser (non-output) level
+constexpr int kNoAllocMaxBricks = 4096;   // bricks of the output level
+constexpr size_t kBrickBytes = (size_t)33 * 33 * 33 * sizeof(double);
+constexpr size_t kOffSlots = 0;
+constexpr size_t kOffLevA = kOffSlots + (size_t)kNoAllocSlots * kBrickBytes;
+constexpr size_t kOffLevB = kOffLevA + (size_t)kNoAllocLevelBricks * kBrickBytes;
+constexpr size_t kOffBricks = kOffLevB + (size_t)kNoAllocLevelBricks * kBrickBytes;
+constexpr size_t kOffGeom = kOffBricks + (((size_t)kNoAllocMaxBricks * sizeof(decode_brick) + 255) & ~(size_t)255);
+constexpr size_t kOffErr = kOffGeom + sizeof(uint64_t) * 8 * kMaxBlocksPerSubband;
+constexpr size_t kNoAllocScratchBytes = kOffErr + 256;
+
+static __device__ __align__(256) unsigned char g_decode_scratch[kNoAllocScratchBytes];
+
+// Device address of g_decode_scratch per device, resolved once per device by the first call
+// on that device (with that device current). In host code the symbol is only a stand-in.
+std::mutex g_scratch_mu;
+void* g_scratch_addr[64] = {};
+
+int scratch_address(int device, unsigned char** out)
+{
+  if (device < 0 || device >= 64)
+    return InvalidArgument;
+  std::lock_guard<std::mutex> lock(g_scratch_mu);
+  if (!g_scratch_addr[device])
+  {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_decode_scratch) != cudaSuccess || !p)
+      return CudaError;
+    g_scratch_addr[device] = p;
+  }
+  *out = (unsigned char*)g_scratch_addr[device];
+  return NoError;
+}
+
+} // namespace
+
+int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, void* d_out, size_t out_bytes,
+                                  double* kernel_ms)
+{
+  // limits of the fixed scratch
+  bool seen_output = false;
+  for (const decode_level& lv : rq.levels)
+  {
+    if (seen_output)
+      break;
+    const size_t nbr = lv.bricks.size();
+    if (lv.is_output)
+    {
+      seen_output = true;
+      if (nbr > (size_t)kNoAllocMaxBricks)
+        return ScratchTooSmall;
+    }
+    else if (nbr > (size_t)kNoAllocLevelBricks)
+      return ScratchTooSmall;
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess)
+    return CudaError;
+  unsigned char* base = nullptr;
+  int e = scratch_address(ctx->device, &base);
+  if (e)
+    return e;
+  cudaStream_t st = ctx->stream;
+  const int NB = 33 * 33 * (rq.is2d ? 1 : 33);
+  double* slots = (double*)(base + kOffSlots);
+  double* lev[2] = { (double*)(base + kOffLevA), (double*)(base + kOffLevB) };
+  decode_brick* d_bricks = (decode_brick*)(base + kOffBricks);
+  uint64_t* d_geom = (uint64_t*)(base + kOffGeom);
+  int* d_err = (int*)(base + kOffErr);
+  cudaMemsetAsync(d_out, 0, out_bytes, st);
+  cudaMemsetAsync(d_err, 0, 16, st);
+  const size_t smem = sizeof(dec_smem);
+  cudaFuncSetAttribute(k_decode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  float total_ms = 0;
+  double* prev = nullptr;
+  int li = 0;
+  for (const decode_level& lv : rq.levels)
+  {
+    const int nbr = (int)lv.bricks.size();
+    if (nbr == 0)
+      continue;
+    double* d_level = lv.is_output ? nullptr : lev[li % 2];
+    ++li;
+    int grid = lv.is_output ? (nbr < kNoAllocSlots ? nbr : kNoAllocSlots) : nbr;
+    cudaMemcpyAsync(d_bricks, lv.bricks.data(), sizeof(decode_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_geom, lv.geom, sizeof(uint64_t) * 8 * kMaxBlocksPerSubband, cudaMemcpyHostToDevice, st);
+    dec_args a;
+    memset(&a, 0, sizeof a);
+    a.level = lv.level;
+    a.nlevels = rq.nlevels;
+    a.is2d = rq.is2d;
+    a.nsb = rq.nsb;
+    a.nbricks = nbr;
+    a.etol = rq.etol;
+    a.end_bp = rq.f32 ? 32 : 64;
+    a.mask = lv.mask;
+    a.norm_mask = lv.norm_mask;
+    a.is_output = lv.is_output;
+    a.out_f32 = rq.f32;
+    memcpy(a.spacing, lv.spacing, sizeof a.spacing);
+    memcpy(a.nblocks, lv.nblocks, sizeof a.nblocks);
+    memcpy(a.inv_weight, lv.inv_weight, sizeof a.inv_weight);
+    a.geom = d_geom;
+    a.bricks = d_bricks;
+    a.exps = exps_;
+    a.ckmin = kmin_;
+    a.cn = n_;
+    a.cfirst = first_;
+    a.coff = off_;
+    a.blob = blob_;
+    a.blob_bytes = blob_bytes_;
+    a.parents = prev;
+    a.bricks_out = d_level;
+    a.slots = slots;
+    a.out = d_out;
+    a.out_dims[0] = rq.out_dims.x;
+    a.out_dims[1] = rq.out_dims.y;
+    a.out_dims[2] = rq.out_dims.z;
+    a.error = d_err;
+    (void)NB;
+    cudaEventRecord(ctx->ev0, st);
+    k_decode_level<<<grid, kThreads, smem, st>>>(a);
+    cudaEventRecord(ctx->ev1, st);
+    if (cudaGetLastError() != cudaSuccess)
+      return CudaError;
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    total_ms += ms;
+    prev = d_level;
+    if (lv.is_output)
+      break;
+  }
+  int herr = 0;
+  cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess)
     return CudaError;
   if (herr)
     return DeviceStreamOverflow;

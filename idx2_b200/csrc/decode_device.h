@@ -51,6 +51,10 @@ public:
              const std::vector<uint64_t>& off, const std::vector<uint8_t>& blob);
   int decode(device_ctx* ctx, const decode_request& rq, void* out, size_t out_bytes, bool out_on_device,
              double* kernel_ms);
+  // Allocation-free decode into a device buffer: every temporary lives in a fixed static
+  // device array of decode.cu (limits and semantics there and in include/idx2g.h).
+  int decode_noalloc(device_ctx* ctx, const decode_request& rq, void* d_out, size_t out_bytes,
+                     double* kernel_ms);
   size_t resident_bytes() const { return resident_; }
 
 private:

@@ -542,6 +542,19 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
 
 void dataset_close(dataset_handle* h) { delete h; }
 
+int dataset_decode_noalloc(device_ctx* ctx, dataset_handle* h, const params& p, void* d_out, size_t out_bytes,
+                           double* kernel_ms)
+{
+  decode_request rq;
+  size_t need = 0;
+  int e = plan_decode(h, p, &rq, &need);
+  if (e)
+    return e;
+  if (out_bytes < need)
+    return SizeTooSmall;
+  return h->dev.decode_noalloc(ctx, rq, d_out, need, kernel_ms);
+}
+
 const dataset_format& dataset_fmt(const dataset_handle* h) { return h->f; }
 
 size_t dataset_resident_bytes(const dataset_handle* h) { return h->dev.resident_bytes(); }

@@ -20,6 +20,9 @@ int dataset_output_grid(const dataset_handle* ds, const params& p, grid* g);
 int dataset_decode(device_ctx* ctx, dataset_handle* ds, const params& p, void* out, size_t out_bytes,
                    bool out_on_device, double* kernel_ms);
 void dataset_close(dataset_handle* ds);
+// Allocation-free variant of dataset_decode (device output only; see decode.cu).
+int dataset_decode_noalloc(device_ctx* ctx, dataset_handle* ds, const params& p, void* d_out,
+                           size_t out_bytes, double* kernel_ms);
 const dataset_format& dataset_fmt(const dataset_handle* ds);
 size_t dataset_resident_bytes(const dataset_handle* ds);
 

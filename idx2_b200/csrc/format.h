@@ -64,6 +64,7 @@ enum err : int
   InvalidArgument = 101,
   DeviceStreamOverflow = 102,
   CorruptStream = 103,
+  ScratchTooSmall = 104,  // request larger than the allocation-free decode's fixed scratch
 };
 
 struct v3

@@ -119,6 +119,23 @@ IDX2G_API int idx2g_decode(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params
                            size_t out_bytes, int out_on_device, double* kernel_ms);
 IDX2G_API int idx2g_dataset_close(idx2g_dataset* ds);
 
+/* Allocation-free decode. No counterpart in the reference: it exists for callers that cannot
+   allocate device memory when they decode -- applications whose device memory belongs to
+   another allocator (a framework's caching allocator, a pool sized to the whole GPU) and
+   latency-bound serving loops, where cudaMalloc fails or synchronises the device. Open the
+   dataset first (idx2g_dataset_open allocates the resident dataset), then call this with a
+   device output buffer; it calls no cudaMalloc / cudaFree and no allocating library routine.
+   Its temporaries live in a fixed device array of about 7.3 MB that every GPU loading the
+   library holds until the process exits. Limits: at most 4096 bricks on the output level and
+   8 bricks on each coarser level the request decodes; larger requests return
+   ScratchTooSmall (104). The first call on a device resolves the array's device address
+   (cudaGetSymbolAddress) with that device current; make that first call before any stream
+   capture. All calls share the array and it keeps the last call's contents (the error word
+   is cleared by every call); calls that overlap on the GPU race on it. The result equals
+   idx2g_decode's. */
+IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p,
+                                   void* d_out, size_t out_bytes, double* kernel_ms);
+
 /* Metadata of an open dataset (the fields of the .idx2 file): name and field (64 bytes
    each, NUL-terminated), dims, dtype, number of levels, encode tolerance, and the bytes
    the dataset keeps resident on the device. */
