@@ -103,6 +103,150 @@ inline __device__ void lift_sweep(double* F, const int N[3], const dgrid& G, con
   }
 }
 
+// One CDF5/3 line held in registers: samples at positions k*S (k < D) plus, for even D,
+// the extrapolated sample in slot D. Same operations and order as lift_sweep (the reference's
+// clamps to M never apply to the grids of the brick transforms: every position is <= 32).
+template <bool FWD>
+__device__ __forceinline__ void lift_regs(double (&v)[33], int D)
+{
+  const bool ext = (D % 2) == 0;
+  if (FWD)
+  {
+    if (ext)
+    {
+#pragma unroll
+      for (int k = 2; k < 33; ++k)
+        if (k == D)
+          v[k] = __dsub_rn(__dmul_rn(2.0, v[k - 1]), v[k - 2]);
+    }
+#pragma unroll
+    for (int k = 1; k < 31; k += 2)
+      if (k < D - 2)
+        v[k] = __dsub_rn(v[k], __dmul_rn(__dadd_rn(v[k - 1], v[k + 1]), 0.5));
+#pragma unroll
+    for (int k = 1; k < 32; ++k)
+    {
+      if (!ext && k == D - 2)
+        v[k] = __dsub_rn(v[k], __dmul_rn(__dadd_rn(v[k + 1], v[k - 1]), 0.5));
+      if (ext && k == D - 1)
+        v[k] = 0.0;
+    }
+#pragma unroll
+    for (int k = 1; k < 31; k += 2)
+      if (k < D - 2)
+      {
+        double V = __dmul_rn(v[k], 0.25);
+        v[k - 1] = __dadd_rn(v[k - 1], V);
+        v[k + 1] = __dadd_rn(v[k + 1], V);
+      }
+    if (!ext)
+    {
+#pragma unroll
+      for (int k = 1; k < 32; ++k)
+        if (k == D - 2)
+        {
+          double V = __dmul_rn(v[k], 0.25);
+          v[k - 1] = __dadd_rn(v[k - 1], V);
+          v[k + 1] = __dadd_rn(v[k + 1], V);
+        }
+    }
+  }
+  else
+  {
+#pragma unroll
+    for (int k = 1; k < 31; k += 2)
+      if (k < D - 2)
+      {
+        double V = __dmul_rn(v[k], 0.25);
+        v[k - 1] = __dsub_rn(v[k - 1], V);
+        v[k + 1] = __dsub_rn(v[k + 1], V);
+      }
+#pragma unroll
+    for (int k = 1; k < 32; ++k)
+    {
+      if (!ext && k == D - 2)
+      {
+        double V = __dmul_rn(v[k], 0.25);
+        v[k - 1] = __dsub_rn(v[k - 1], V);
+        v[k + 1] = __dsub_rn(v[k + 1], V);
+      }
+      if (ext && k == D - 1)
+        v[k] = __dmul_rn(__dadd_rn(v[k + 1], v[k - 1]), 0.5);
+    }
+#pragma unroll
+    for (int k = 1; k < 31; k += 2)
+      if (k < D - 2)
+        v[k] = __dadd_rn(v[k], __dmul_rn(__dadd_rn(v[k - 1], v[k + 1]), 0.5));
+    if (!ext)
+    {
+#pragma unroll
+      for (int k = 1; k < 32; ++k)
+        if (k == D - 2)
+          v[k] = __dadd_rn(v[k], __dmul_rn(__dadd_rn(v[k + 1], v[k - 1]), 0.5));
+    }
+  }
+}
+
+// One line with a compile-time length D: load, lift in registers, store. The inverse reads
+// the extrapolated slot D of an even-length line, the forward writes it.
+template <int D, bool FWD>
+__device__ __forceinline__ void lift_line_fixed(double* L, int s)
+{
+  constexpr bool ext = (D % 2) == 0;
+  constexpr int nload = D + (ext && !FWD ? 1 : 0);
+  constexpr int nstore = D + (ext && FWD ? 1 : 0);
+  double v[33];
+#pragma unroll
+  for (int k = 0; k < 33; ++k)
+    v[k] = k < nload ? L[k * s] : 0.0;
+  lift_regs<FWD>(v, D);
+#pragma unroll
+  for (int k = 0; k < nstore; ++k)
+    L[k * s] = v[k];
+}
+
+template <bool FWD>
+__device__ __noinline__ void lift_line(double* L, int s, int D)
+{
+  switch (D)
+  {
+#define IDX2G_LIFT_CASE(n) \
+  case n:                  \
+    lift_line_fixed<n, FWD>(L, s); \
+    break;
+    IDX2G_LIFT_CASE(2) IDX2G_LIFT_CASE(3) IDX2G_LIFT_CASE(4) IDX2G_LIFT_CASE(5) IDX2G_LIFT_CASE(6)
+    IDX2G_LIFT_CASE(7) IDX2G_LIFT_CASE(8) IDX2G_LIFT_CASE(9) IDX2G_LIFT_CASE(10) IDX2G_LIFT_CASE(11)
+    IDX2G_LIFT_CASE(12) IDX2G_LIFT_CASE(13) IDX2G_LIFT_CASE(14) IDX2G_LIFT_CASE(15) IDX2G_LIFT_CASE(16)
+    IDX2G_LIFT_CASE(17) IDX2G_LIFT_CASE(18) IDX2G_LIFT_CASE(19) IDX2G_LIFT_CASE(20) IDX2G_LIFT_CASE(21)
+    IDX2G_LIFT_CASE(22) IDX2G_LIFT_CASE(23) IDX2G_LIFT_CASE(24) IDX2G_LIFT_CASE(25) IDX2G_LIFT_CASE(26)
+    IDX2G_LIFT_CASE(27) IDX2G_LIFT_CASE(28) IDX2G_LIFT_CASE(29) IDX2G_LIFT_CASE(30) IDX2G_LIFT_CASE(31)
+    IDX2G_LIFT_CASE(32) IDX2G_LIFT_CASE(33)
+#undef IDX2G_LIFT_CASE
+    default:
+      break;
+  }
+}
+
+// A lifting sweep over the lines of G with each line in registers.
+template <bool FWD>
+__device__ void lift_sweep_regs(double* F, const int N[3], const dgrid& G, int a)
+{
+  const int D = G.dims[a], S = G.strd[a];
+  if (D == 1)
+    return;
+  const int b = a == 0 ? 1 : 0;
+  const int c = a == 2 ? 1 : 2;
+  const int st[3] = { 1, N[0], N[0] * N[1] };
+  const int s = st[a] * S;
+  const int nlines = G.dims[b] * G.dims[c];
+  for (int li = threadIdx.x; li < nlines; li += blockDim.x)
+  {
+    const int u = (li % G.dims[b]) * G.strd[b];
+    const int w = (li / G.dims[b]) * G.strd[c];
+    lift_line<FWD>(F + u * st[b] + w * st[c], s, D);
+  }
+}
+
 // The grid sequence of the multi-level transform on the first dims3 samples
 // (Core/Wavelet.cpp:210 ForwardCdf53 / :304 InverseCdf53 with a transform order).
 struct lift_stack

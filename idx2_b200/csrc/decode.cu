@@ -23,350 +23,7 @@ namespace idx2g
 namespace
 {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-
-struct dec_args
-{
-  int level, nlevels, is2d, nsb, nbricks, etol, end_bp, mask, norm_mask, is_output, out_f32;
-  int spacing[8][3];
-  int nblocks[8];
-  double inv_weight[8];
-  const uint64_t* geom;               // [8][kMaxBlocksPerSubband]
-  const decode_brick* bricks;
-  const int16_t* exps;                // [flat][sb][kMaxBlocksPerSubband]
-  const int32_t* ckmin;
-  const int32_t* cn;
-  const unsigned long long* cfirst;
-  const unsigned long long* coff;
-  const uint8_t* blob;
-  unsigned long long blob_bytes;
-  const double* parents;              // decoded bricks of the coarser level
-  double* bricks_out;                 // decoded bricks of this level (non-output level)
-  double* slots;                      // per-CTA slots (output level)
-  void* out;
-  int out_dims[3];
-  int* error;
-};
-
-struct dec_smem
-{
-  unsigned long long coef[kMaxBlocksPerSubband][64];
-  long long q[kWarps][64];
-  int16_t emax[kMaxBlocksPerSubband];
-  int16_t ktop[kMaxBlocksPerSubband];
-  uint8_t np[kMaxBlocksPerSubband];
-  uint8_t nbps[kMaxBlocksPerSubband];
-  uint8_t nd[kMaxBlocksPerSubband];
-  uint8_t bypass[kMaxBlocksPerSubband];
-  uint8_t nst[2][kKeyWindow];
-  uint8_t stop[2][kKeyWindow];
-  int kmax_w, nkeys;
-};
-
-__device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
-{
-  d3[0] = (int)(g & 0xff) * 4;
-  d3[1] = (int)((g >> 8) & 0xff) * 4;
-  d3[2] = (int)((g >> 16) & 0xff) * 4;
-  bd[0] = (int)((g >> 24) & 0xff);
-  bd[1] = (int)((g >> 32) & 0xff);
-  bd[2] = (int)((g >> 40) & 0xff);
-}
-
-__device__ __forceinline__ void subband_grid(int is2d, int s, int from[3], int dims[3], int strd[3])
-{
-  int h[3] = { 0, 0, 0 };
-  if (is2d)
-  {
-    h[0] = (s >> 1) & 1;
-    h[1] = s & 1;
-  }
-  else
-  {
-    h[0] = (s >> 2) & 1;
-    h[1] = (s >> 1) & 1;
-    h[2] = s & 1;
-  }
-  for (int k = 0; k < 3; ++k)
-  {
-    if (is2d && k == 2)
-    {
-      from[k] = 0;
-      dims[k] = 1;
-      strd[k] = 1;
-    }
-    else
-    {
-      from[k] = h[k];
-      dims[k] = h[k] ? 16 : 17;
-      strd[k] = 2;
-    }
-  }
-}
-
-// Read n <= 64 bits at bit position pos of the blob (LSB-first); bits past the end read 0.
-__device__ __forceinline__ unsigned long long read_bits(const uint8_t* blob, unsigned long long nbytes,
-                                                        unsigned long long pos, int n)
-{
-  if (n <= 0)
-    return 0;
-  unsigned long long v = 0;
-  int got = 0;
-  while (got < n)
-  {
-    unsigned long long byte = (pos + (unsigned long long)got) >> 3;
-    int sh = (int)((pos + (unsigned long long)got) & 7);
-    unsigned long long b = byte < nbytes ? (unsigned long long)(blob[byte] >> sh) : 0ull;
-    int take = 8 - sh;
-    if (take > n - got)
-      take = n - got;
-    b &= (1ull << take) - 1ull;
-    v |= b << got;
-    got += take;
-  }
-  return v;
-}
-
-__global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
-{
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  dec_smem& sm = *reinterpret_cast<dec_smem*>(smem_raw);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int N[3] = { 33, 33, a.is2d ? 1 : 33 };
-  const int NB = N[0] * N[1] * N[2];
-
-  for (int bi = blockIdx.x; bi < a.nbricks; bi += gridDim.x)
-  {
-    const decode_brick br = a.bricks[bi];
-    double* F = a.is_output ? a.slots + (size_t)blockIdx.x * (size_t)NB
-                            : a.bricks_out + (size_t)bi * (size_t)NB;
-    // 1: zero + parent low band (Core/idx2Decode.cpp:285-293)
-    for (int i = tid; i < NB; i += kThreads)
-      F[i] = 0.0;
-    __syncthreads();
-    if (br.parent >= 0 && a.parents && (a.mask & 1))
-    {
-      const double* P = a.parents + (size_t)br.parent * (size_t)NB;
-      const int nz = a.is2d ? 1 : 16;
-      for (int i = tid; i < 16 * 16 * nz; i += kThreads)
-      {
-        int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
-        int cz = a.is2d ? 0 : 2 * z;
-        F[(cz * 33 + 2 * y) * 33 + 2 * x] =
-          P[((br.pos[2] * nz + z) * 33 + (br.pos[1] * 16 + y)) * 33 + (br.pos[0] * 16 + x)];
-      }
-    }
-    __syncthreads();
-
-    // 2-3: subbands
-    for (int s = 0; s < a.nsb; ++s)
-    {
-      if (!((a.mask >> s) & 1))
-        continue;
-      int from[3], dims[3], strd[3];
-      subband_grid(a.is2d, s, from, dims, strd);
-      const int nb = a.nblocks[s];
-      const uint64_t* geom = a.geom + (size_t)s * kMaxBlocksPerSubband;
-      const size_t fs = (size_t)br.flat * (size_t)a.nsb + (size_t)s;
-      const int16_t* ex = a.exps + fs * kMaxBlocksPerSubband;
-      for (int b = tid; b < nb; b += kThreads)
-      {
-        int d3[3], bd[3];
-        unpack_geom(geom[b], d3, bd);
-        const int emax = ex[b];
-        sm.emax[b] = (int16_t)emax;
-        sm.ktop[b] = (int16_t)(emax + 63 + 1024);
-        sm.np[b] = (uint8_t)dev::coded_planes(emax, a.etol, a.end_bp);
-        sm.nbps[b] = 0;
-        sm.nd[b] = (uint8_t)((bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1));
-        sm.bypass[b] = (uint8_t)((d3[0] % a.spacing[s][0]) != 0 || (d3[1] % a.spacing[s][1]) != 0 ||
-                                 (d3[2] % a.spacing[s][2]) != 0);
-      }
-      for (int i = tid; i < nb * 64; i += kThreads)
-        sm.coef[i >> 6][i & 63] = 0ull;
-      __syncthreads();
-      if (tid == 0)
-      {
-        int kmax = -(1 << 30), kmin = 1 << 30;
-        for (int b = 0; b < nb; ++b)
-        {
-          if (!sm.np[b])
-            continue;
-          kmax = sm.ktop[b] > kmax ? sm.ktop[b] : kmax;
-          int lo = sm.ktop[b] - sm.np[b] + 1;
-          kmin = lo < kmin ? lo : kmin;
-        }
-        int nk = kmax >= kmin ? kmax - kmin + 1 : 0;
-        if (nk > kKeyWindow)
-        {
-          atomicExch(a.error, 1);
-          nk = 0;
-        }
-        sm.kmax_w = kmax;
-        sm.nkeys = nk;
-      }
-      __syncthreads();
-      const int nkeys = sm.nkeys, kmax = sm.kmax_w;
-      // channel of thread j
-      unsigned long long cur = ~0ull;
-      int key = kmax - tid;
-      if (tid < nkeys)
-      {
-        const int ck = a.ckmin[fs], cn = a.cn[fs];
-        if (key >= ck && key < ck + cn)
-        {
-          unsigned long long o = a.coff[a.cfirst[fs] + (unsigned long long)(key - ck)];
-          if (o != ~0ull)
-            cur = o * 8ull;
-        }
-        sm.nst[0][tid] = 0;
-        sm.stop[0][tid] = 0;
-      }
-      __syncthreads();
-      // wavefront over (block, plane)
-      const int steps = nkeys > 0 ? nb + nkeys - 1 : 0;
-      for (int t = 0; t < steps; ++t)
-      {
-        const int rb = t & 1, wb = rb ^ 1;
-        if (tid < nkeys)
-        {
-          const int b = t - tid;
-          uint8_t out_n = 0, out_stop = 0;
-          if (b >= 0 && b < nb)
-          {
-            const int top = sm.ktop[b], np = sm.np[b];
-            if (np > 0 && key <= top && key > top - np)
-            {
-              int n = key == top ? 0 : sm.nst[rb][tid - 1];
-              int stopped = key == top ? 0 : sm.stop[rb][tid - 1];
-              if (stopped || cur == ~0ull)
-              {
-                out_stop = 1;
-                out_n = (uint8_t)n;
-              }
-              else
-              {
-                // Core/Zfp.h:990 Decode<u64>
-                const int nvals = 1 << (2 * sm.nd[b]);
-                unsigned long long X = n > 0 ? read_bits(a.blob, a.blob_bytes, cur, n) : 0ull;
-                cur += (unsigned long long)n;
-                while (n < nvals)
-                {
-                  unsigned long long g = read_bits(a.blob, a.blob_bytes, cur, 1);
-                  cur += 1;
-                  if (!g)
-                    break;
-                  while (n + 1 < nvals)
-                  {
-                    unsigned long long bit = read_bits(a.blob, a.blob_bytes, cur, 1);
-                    cur += 1;
-                    if (bit)
-                      break;
-                    ++n;
-                  }
-                  X += 1ull << n;
-                  ++n;
-                }
-                const int bp = 63 - (top - key);
-                if (!sm.bypass[b])
-                  for (unsigned long long y = X; y; y &= y - 1)
-                  {
-                    int i = __ffsll((long long)y) - 1;
-                    sm.coef[b][i] += 1ull << bp;
-                  }
-                sm.nbps[b] += 1;
-                out_n = (uint8_t)n;
-              }
-            }
-          }
-          sm.nst[wb][tid] = out_n;
-          sm.stop[wb][tid] = out_stop;
-        }
-        __syncthreads();
-      }
-      // 3: reconstruct blocks (warp per block)
-      for (int b = warp; b < nb; b += kWarps)
-      {
-        if (sm.nbps[b] == 0 || sm.bypass[b])
-          continue;
-        int d3[3], bd[3];
-        unpack_geom(geom[b], d3, bd);
-        const int nd = sm.nd[b];
-        const int nv = 1 << (2 * nd);
-        long long* q = sm.q[warp];
-        for (int i = lane; i < nv; i += 32)
-          q[dev::perm(nd, i)] = (long long)((sm.coef[b][i] ^ dev::kNegaMask) - dev::kNegaMask);
-        __syncwarp();
-        dev::warp_inv_zfp(q, nd, lane);
-        const int prec = 63 - nd;
-        const double scale = __ddiv_rn(1.0, dev::pow2(prec - 1 - sm.emax[b]));
-        for (int j = lane; j < nv; j += 32)
-        {
-          int x = j % bd[0], y = (j / bd[0]) % bd[1], z = j / (bd[0] * bd[1]);
-          F[((from[2] + (d3[2] + z) * strd[2]) * 33 + (from[1] + (d3[1] + y) * strd[1])) * 33 +
-            (from[0] + (d3[0] + x) * strd[0])] = __dmul_rn(scale, __ll2double_rn(q[j]));
-        }
-        __syncwarp();
-      }
-      __syncthreads();
-    }
-
-    // 4: de-normalise + inverse CDF5/3 (Core/Wavelet.cpp:144-203)
-    for (int s = 0; s < a.nsb; ++s)
-    {
-      if (!((a.norm_mask >> s) & 1))
-        continue;
-      int from[3], dims[3], strd[3];
-      subband_grid(a.is2d, s, from, dims, strd);
-      const double W = a.inv_weight[s];
-      const int n = dims[0] * dims[1] * dims[2];
-      for (int i = tid; i < n; i += kThreads)
-      {
-        int x = i % dims[0], y = (i / dims[0]) % dims[1], z = i / (dims[0] * dims[1]);
-        int idx = ((from[2] + z * strd[2]) * 33 + (from[1] + y * strd[1])) * 33 + (from[0] + x * strd[0]);
-        F[idx] = __dmul_rn(F[idx], W);
-      }
-    }
-    __syncthreads();
-    {
-      dev::dgrid G;
-      for (int k = 0; k < 3; ++k)
-      {
-        G.from[k] = 0;
-        G.dims[k] = N[k];
-        G.strd[k] = 1;
-      }
-      for (int ax = a.is2d ? 1 : 2; ax >= 0; --ax)
-      {
-        dev::lift_sweep(F, N, G, N, ax, false);
-        __syncthreads();
-      }
-    }
-
-    // 5: output (Core/idx2Decode.cpp:431-442 CopyGridGrid)
-    if (a.is_output)
-    {
-      const int n = br.dims[0] * br.dims[1] * br.dims[2];
-      for (int i = tid; i < n; i += kThreads)
-      {
-        int x = i % br.dims[0], y = (i / br.dims[0]) % br.dims[1], z = i / (br.dims[0] * br.dims[1]);
-        int sx = br.src_from[0] + x * br.src_strd[0], sy = br.src_from[1] + y * br.src_strd[1],
-            sz = br.src_from[2] + z * br.src_strd[2];
-        long long dx = br.dst_from[0] + (long long)x * br.dst_strd[0],
-                  dy = br.dst_from[1] + (long long)y * br.dst_strd[1],
-                  dz = br.dst_from[2] + (long long)z * br.dst_strd[2];
-        long long di = (dz * a.out_dims[1] + dy) * a.out_dims[0] + dx;
-        double v = F[(sz * 33 + sy) * 33 + sx];
-        if (a.out_f32)
-          ((float*)a.out)[di] = __double2float_rn(v);
-        else
-          ((double*)a.out)[di] = v;
-      }
-    }
-    __syncthreads();
-  }
-}
+#include "decode_kernel.cuh"
 
 } // namespace
 

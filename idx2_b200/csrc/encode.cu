@@ -29,6 +29,7 @@ namespace
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kMaxPlanes = 64;
+constexpr unsigned kStageBytes = 8192;
 
 struct enc_brick
 {
@@ -79,6 +80,8 @@ struct enc_smem
   uint8_t nvals_log[kMaxBlocksPerSubband];
   uint32_t key_bits[kKeyWindow];
   uint32_t key_base[kKeyWindow];
+  uint32_t stage[kStageBytes / 4];  // one (brick, subband) region being assembled
+  unsigned alloc;
   dev::lift_stack stack;
   double red[2][kWarps];
   int kmin, kmax;
@@ -202,53 +205,86 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
 
     // ---------------- B: transform ----------------
     {
-      const int M[3] = { 32, 32, a.is2d ? 1 : 32 };
+      // extrapolation round trip (Core/Wavelet.cpp:68): forward on the valid dims, then the
+      // inverse on the 33^3 grid except its last sweep (X at full resolution), which is fused
+      // with the first sweep of the real transform below
       if (tid == 0)
         dev::build_stack(br.valid, 5, a.order, &sm.stack);
       __syncthreads();
       const int nf = sm.stack.n;
       for (int i = 0; i < nf; ++i)
       {
-        dev::lift_sweep(F, N, sm.stack.g[i], M, sm.stack.axis[i], true);
+        dev::lift_sweep_regs<true>(F, N, sm.stack.g[i], sm.stack.axis[i]);
         __syncthreads();
       }
       if (tid == 0)
         dev::build_stack(N, 5, a.order, &sm.stack);
       __syncthreads();
       const int ni = sm.stack.n;
-      for (int i = ni - 1; i >= 0; --i)
+      for (int i = ni - 1; i >= 1; --i)
       {
-        dev::lift_sweep(F, N, sm.stack.g[i], M, sm.stack.axis[i], false);
+        dev::lift_sweep_regs<false>(F, N, sm.stack.g[i], sm.stack.axis[i]);
         __syncthreads();
       }
-      dev::dgrid G;
-      for (int k = 0; k < 3; ++k)
+      // inverse X (D = 33) then forward X of the one-level transform (Core/Wavelet.cpp:81)
+      for (int li = tid; li < 33 * N[2]; li += kThreads)
       {
-        G.from[k] = 0;
-        G.dims[k] = N[k];
-        G.strd[k] = 1;
+        double* row = F + li * 33;
+        double v[33];
+#pragma unroll
+        for (int k = 0; k < 33; ++k)
+          v[k] = row[k];
+        dev::lift_regs<false>(v, 33);
+        dev::lift_regs<true>(v, 33);
+#pragma unroll
+        for (int k = 0; k < 33; ++k)
+          row[k] = v[k];
       }
-      for (int ax = 0; ax < (a.is2d ? 2 : 3); ++ax)
+      __syncthreads();
+      // forward Y, and forward Z; subband normalisation applied as the last sweep stores
+      // (Core/Wavelet.cpp:111-137)
+      for (int li = tid; li < 33 * N[2]; li += kThreads)
       {
-        dev::lift_sweep(F, N, G, N, ax, true);
-        __syncthreads();
-      }
-      for (int s = 0; s < a.nsb; ++s)
-      {
-        if (!((a.norm_mask >> s) & 1))
-          continue;
-        int from[3], dims[3], strd[3];
-        subband_grid(a.is2d, s, from, dims, strd);
-        const double W = a.weight[s];
-        const int n = dims[0] * dims[1] * dims[2];
-        for (int i = tid; i < n; i += kThreads)
+        const int x = li % 33, z = li / 33;
+        double* col = F + z * 33 * 33 + x;
+        double v[33];
+#pragma unroll
+        for (int k = 0; k < 33; ++k)
+          v[k] = col[k * 33];
+        dev::lift_regs<true>(v, 33);
+#pragma unroll
+        for (int k = 0; k < 33; ++k)
         {
-          int x = i % dims[0], y = (i / dims[0]) % dims[1], z = i / (dims[0] * dims[1]);
-          int idx = ((from[2] + z * strd[2]) * 33 + (from[1] + y * strd[1])) * 33 + (from[0] + x * strd[0]);
-          F[idx] = __dmul_rn(F[idx], W);
+          double f = v[k];
+          if (a.is2d)
+          {
+            const int s = ((x & 1) << 1) | (k & 1);
+            f = ((a.norm_mask >> s) & 1) ? __dmul_rn(f, a.weight[s]) : f;
+          }
+          col[k * 33] = f;
         }
       }
       __syncthreads();
+      if (!a.is2d)
+      {
+        for (int li = tid; li < 33 * 33; li += kThreads)
+        {
+          const int x = li % 33, y = li / 33;
+          double* col = F + y * 33 + x;
+          double v[33];
+#pragma unroll
+          for (int k = 0; k < 33; ++k)
+            v[k] = col[k * 33 * 33];
+          dev::lift_regs<true>(v, 33);
+#pragma unroll
+          for (int k = 0; k < 33; ++k)
+          {
+            const int s = ((x & 1) << 2) | ((y & 1) << 1) | (k & 1);
+            col[k * 33 * 33] = ((a.norm_mask >> s) & 1) ? __dmul_rn(v[k], a.weight[s]) : v[k];
+          }
+        }
+        __syncthreads();
+      }
     }
 
     // ---------------- C: low band to the parent ----------------
@@ -390,6 +426,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
       __syncthreads();
 
       // D4: channel byte bases and the region of this (brick, subband)
+      // (regions are whole 32-bit words so every CTA owns the words it writes)
       if (tid == 0)
       {
         unsigned base = 0;
@@ -398,10 +435,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
           sm.key_base[t] = base;
           base += (sm.key_bits[t] + 7) / 8;
         }
-        unsigned long long region = atomicAdd(a.cursor, (unsigned long long)base);
-        if (region + base > a.cap_bytes)
+        const unsigned alloc = (base + 3u) & ~3u;
+        unsigned long long region = atomicAdd(a.cursor, (unsigned long long)alloc);
+        if (region + alloc > a.cap_bytes)
           atomicExch(a.error, 2);
         sm.region = region;
+        sm.alloc = alloc;
         a.offset[bs] = region;
         a.kmin[bs] = nkeys ? kmin : 1;
         a.kmax[bs] = nkeys ? kmax : 0;
@@ -410,21 +449,33 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
       for (int t = tid; t < kKeyWindow; t += kThreads)
         a.sizes[bs * kKeyWindow + (size_t)t] = t < nkeys ? (sm.key_bits[t] + 7) / 8 : 0u;
       const unsigned long long region = sm.region;
-      const bool fits = region + (nkeys ? sm.key_base[nkeys - 1] + (sm.key_bits[nkeys - 1] + 7) / 8 : 0) <=
-                        a.cap_bytes;
+      const unsigned alloc = sm.alloc;
+      const bool fits = region + alloc <= a.cap_bytes;
 
-      // D5: scatter the plane bits
-      if (fits)
+      // D5: scatter the plane bits, into shared memory when the region is small enough, else
+      // straight into the (zeroed) global region; then the region is stored with plain writes
+      if (fits && alloc)
       {
+        const bool staged = alloc <= kStageBytes;
+        uint32_t* words = staged ? sm.stage : a.stream + region / 4;
+        for (unsigned i = tid; i < alloc / 4; i += kThreads)
+          words[i] = 0u;
+        __syncthreads();
         for (int idx = tid; idx < nb * kMaxPlanes; idx += kThreads)
         {
           const int b = idx >> 6, kk = idx & 63;
           if (kk >= sm.np[b])
             continue;
           const int t = sm.ktop[b] - kk - kmin;
-          const unsigned long long pos =
-            (region + sm.key_base[t]) * 8ull + (unsigned long long)sm.off[b][kk];
-          dev::write_plane(a.stream, pos, sm.X[b][kk], sm.nin[b][kk], 1 << sm.nvals_log[b]);
+          const unsigned long long pos = (unsigned long long)sm.key_base[t] * 8ull + (unsigned long long)sm.off[b][kk];
+          dev::write_plane(words, pos, sm.X[b][kk], sm.nin[b][kk], 1 << sm.nvals_log[b]);
+        }
+        __syncthreads();
+        if (staged)
+        {
+          uint32_t* dst = a.stream + region / 4;
+          for (unsigned i = tid; i < alloc / 4; i += kThreads)
+            dst[i] = sm.stage[i];
         }
       }
       __syncthreads();
@@ -564,7 +615,7 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     cap = ctx_->ws_size(sname);
   for (int attempt = 0; attempt < 4; ++attempt)
   {
-    uint32_t* d_stream = (uint32_t*)ctx_->ws_zeroed(sname, (size_t)cap);
+    uint32_t* d_stream = (uint32_t*)ctx_->ws(sname, (size_t)cap);
     if (!d_stream)
       return OutOfMemory;
     cap = ctx_->ws_size(sname);
