@@ -259,6 +259,7 @@ def ours(args, rank, world, local_rank):
 
         # e2e through the C ABI with host buffers
         e2e_times = []
+        e2e_parts = []
         h2d = d2h = 0
         for i in range(0 if args.no_e2e else args.warmup + args.steps):
             shutil.rmtree(os.path.join(tmp, "e2e"), ignore_errors=True)
@@ -272,11 +273,13 @@ def ours(args, rank, world, local_rank):
             rc = _lib.lib().idx2g_encode(h, ctypes.byref(p2), ctypes.c_void_p(host.data_ptr()), 0,
                                          ctypes.byref(info2))
             assert rc == 0, rc
+            ta = time.perf_counter()
             dp2 = _lib.Params(input_file=os.path.join(tmp, "e2e", "grf", "f.idx2"),
                               in_dir=os.path.join(tmp, "e2e")).to_c()
             dh2 = ctypes.c_void_p()
             rc = _lib.lib().idx2g_dataset_open(h, ctypes.byref(dp2), ctypes.byref(dh2))
             assert rc == 0, rc
+            tb = time.perf_counter()
             rc = _lib.lib().idx2g_decode(h, dh2, ctypes.byref(dp2), ctypes.c_void_p(out_host.data_ptr()),
                                          ctypes.c_size_t(raw_bytes), 0, ctypes.byref(kms))
             assert rc == 0, rc
@@ -288,6 +291,9 @@ def ours(args, rank, world, local_rank):
             t1 = time.perf_counter()
             if i >= args.warmup:
                 e2e_times.append(t1 - t0)
+                e2e_parts.append({"encode_s": ta - t0, "encode_device_s": info2.device_s,
+                                  "encode_pack_s": info2.pack_s, "encode_write_s": info2.write_s,
+                                  "open_s": tb - ta, "decode_s": t1 - tb})
                 h2d = raw_bytes + rsd.value
                 d2h = raw_bytes + info2.stream_bytes + info2.exp_bytes
         tt = torch.tensor([sum(e2e_times) / len(e2e_times) if e2e_times else float("nan")], device=dev,
@@ -333,7 +339,9 @@ def ours(args, rank, world, local_rank):
                      "algorithmic_bytes": l0_bytes, "traffic": None},
         "cpu_baseline": base,
         "e2e": {"value": world * 2 * raw_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s},
+                "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s,
+                "breakdown_s": ({k: round(sum(d[k] for d in e2e_parts) / len(e2e_parts), 4)
+                                 for k in e2e_parts[0]} if e2e_parts else None)},
         "clocks": clocks.summary(),
         "gpu_launches": int(args.steps * (launches + LEVELS)),
     }

@@ -193,7 +193,6 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
     cudaMemcpyAsync(owned, field, bytes, cudaMemcpyHostToDevice, c->d.stream);
     d_field = owned;
   }
-  std::map<std::string, std::vector<uint8_t>> files;
   encode_timing tm;
   long long stream_bytes = 0, exp_bytes = 0;
   double kms = 0;
@@ -202,7 +201,7 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
   std::vector<long long> lbytes;
   {
     gpu_coder coder(&c->d, f, d_field, f32);
-    e = encode_dataset(&f, &p, &coder, &files, true, &tm);
+    e = encode_dataset(&f, &p, &coder, nullptr, true, &tm);
     stream_bytes = coder.stream_bytes();
     exp_bytes = coder.exp_bytes();
     kms = coder.kernel_ms();
@@ -226,10 +225,7 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
     info->write_s = tm.write_s;
     info->stream_bytes = stream_bytes;
     info->exp_bytes = exp_bytes;
-    long long fb = 0;
-    for (auto& kv : files)
-      fb += (long long)kv.second.size();
-    info->file_bytes = fb;
+    info->file_bytes = (long long)tm.file_bytes;
     info->kernel_launches = launches;
     info->value_min = f.value_min;
     info->value_max = f.value_max;

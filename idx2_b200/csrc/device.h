@@ -72,12 +72,34 @@ struct device_ctx
     if (d > b.dirty)
       b.dirty = d;
   }
+  // Pinned host buffer of at least `bytes` bytes (grow-only, kept across calls).
+  std::map<std::string, buf> pins;
+  void* pinned(const std::string& name, size_t bytes)
+  {
+    buf& b = pins[name];
+    if (b.n < bytes || !b.p)
+    {
+      if (b.p)
+        cudaFreeHost(b.p);
+      b.p = nullptr;
+      b.n = 0;
+      size_t want = bytes + bytes / 4 + 4096;
+      if (cudaMallocHost(&b.p, want) != cudaSuccess)
+        return nullptr;
+      b.n = want;
+    }
+    return b.p;
+  }
   void release()
   {
     for (auto& kv : bufs)
       if (kv.second.p)
         cudaFree(kv.second.p);
     bufs.clear();
+    for (auto& kv : pins)
+      if (kv.second.p)
+        cudaFreeHost(kv.second.p);
+    pins.clear();
     if (ev0)
       cudaEventDestroy(ev0);
     if (ev1)

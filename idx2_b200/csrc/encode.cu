@@ -54,11 +54,7 @@ struct enc_args
   const int* nblocks;        // [nsb]
   double weight[8];
   int norm_mask;
-  int16_t* exps;
-  int32_t* kmin;
-  int32_t* kmax;
   unsigned long long* offset;
-  uint32_t* sizes;
   uint32_t* stream;
   unsigned long long cap_bytes;
   unsigned long long* cursor;
@@ -81,7 +77,7 @@ struct enc_smem
   uint32_t key_bits[kKeyWindow];
   uint32_t key_base[kKeyWindow];
   uint32_t stage[kStageBytes / 4];  // one (brick, subband) region being assembled
-  unsigned alloc;
+  unsigned alloc, hdr;
   dev::lift_stack stack;
   double red[2][kWarps];
   int kmin, kmax;
@@ -366,7 +362,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
           sm.ktop[b] = (int16_t)(emax + 63 + 1024);
           sm.np[b] = (uint8_t)np;
           sm.nvals_log[b] = (uint8_t)(2 * nd);
-          a.exps[bs * kMaxBlocksPerSubband + (size_t)b] = (int16_t)emax;
         }
       }
       __syncthreads();
@@ -435,21 +430,21 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
           sm.key_base[t] = base;
           base += (sm.key_bits[t] + 7) / 8;
         }
-        const unsigned alloc = (base + 3u) & ~3u;
+        // region: header (kmin, nkeys), exponents, channel sizes, channel streams
+        const unsigned hdr = 8u + ((2u * (unsigned)nb + 3u) & ~3u) + 4u * (unsigned)nkeys;
+        const unsigned alloc = hdr + ((base + 3u) & ~3u);
         unsigned long long region = atomicAdd(a.cursor, (unsigned long long)alloc);
         if (region + alloc > a.cap_bytes)
           atomicExch(a.error, 2);
         sm.region = region;
         sm.alloc = alloc;
+        sm.hdr = hdr;
         a.offset[bs] = region;
-        a.kmin[bs] = nkeys ? kmin : 1;
-        a.kmax[bs] = nkeys ? kmax : 0;
       }
       __syncthreads();
-      for (int t = tid; t < kKeyWindow; t += kThreads)
-        a.sizes[bs * kKeyWindow + (size_t)t] = t < nkeys ? (sm.key_bits[t] + 7) / 8 : 0u;
       const unsigned long long region = sm.region;
       const unsigned alloc = sm.alloc;
+      const unsigned hdr = sm.hdr;
       const bool fits = region + alloc <= a.cap_bytes;
 
       // D5: scatter the plane bits, into shared memory when the region is small enough, else
@@ -461,13 +456,25 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         for (unsigned i = tid; i < alloc / 4; i += kThreads)
           words[i] = 0u;
         __syncthreads();
+        if (tid == 0)
+        {
+          words[0] = (uint32_t)(nkeys ? kmin : 1);
+          words[1] = (uint32_t)nkeys;
+        }
+        uint16_t* ew = reinterpret_cast<uint16_t*>(words + 2);
+        for (int b = tid; b < nb; b += kThreads)
+          ew[b] = (uint16_t)sm.emax[b];
+        uint32_t* sw = words + 2 + ((2u * (unsigned)nb + 3u) >> 2);
+        for (int t = tid; t < nkeys; t += kThreads)
+          sw[t] = (sm.key_bits[t] + 7) / 8;
         for (int idx = tid; idx < nb * kMaxPlanes; idx += kThreads)
         {
           const int b = idx >> 6, kk = idx & 63;
           if (kk >= sm.np[b])
             continue;
           const int t = sm.ktop[b] - kk - kmin;
-          const unsigned long long pos = (unsigned long long)sm.key_base[t] * 8ull + (unsigned long long)sm.off[b][kk];
+          const unsigned long long pos =
+            ((unsigned long long)hdr + sm.key_base[t]) * 8ull + (unsigned long long)sm.off[b][kk];
           dev::write_plane(words, pos, sm.X[b][kk], sm.nin[b][kk], 1 << sm.nvals_log[b]);
         }
         __syncthreads();
@@ -594,23 +601,19 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
   double* d_parents = has_parent ? (double*)ctx_->ws(level % 2 ? "enc.parA" : "enc.parB",
                                                      (size_t)npar * (size_t)NB * sizeof(double))
                                  : nullptr;
-  auto* d_exps = (int16_t*)ctx_->ws(level % 2 ? "enc.expsA" : "enc.expsB", nbs * kMaxBlocksPerSubband * 2);
-  auto* d_kmin = (int32_t*)ctx_->ws(level % 2 ? "enc.kminA" : "enc.kminB", nbs * 4);
-  auto* d_kmax = (int32_t*)ctx_->ws(level % 2 ? "enc.kmaxA" : "enc.kmaxB", nbs * 4);
   auto* d_off = (unsigned long long*)ctx_->ws(level % 2 ? "enc.offA" : "enc.offB", nbs * 8);
-  auto* d_sizes = (uint32_t*)ctx_->ws(level % 2 ? "enc.sizesA" : "enc.sizesB", nbs * kKeyWindow * 4);
   auto* d_misc = (unsigned long long*)ctx_->ws("enc.misc", 64);
   double* d_bmin = (double*)ctx_->ws("enc.bmin", (size_t)nbr * 8);
   double* d_bmax = (double*)ctx_->ws("enc.bmax", (size_t)nbr * 8);
-  if (!d_bricks || !d_geom || !d_nblocks || !d_slots || (has_parent && !d_parents) || !d_exps || !d_kmin ||
-      !d_kmax || !d_off || !d_sizes || !d_misc || !d_bmin || !d_bmax)
+  if (!d_bricks || !d_geom || !d_nblocks || !d_slots || (has_parent && !d_parents) || !d_off || !d_misc ||
+      !d_bmin || !d_bmax)
     return OutOfMemory;
   cudaMemcpyAsync(d_bricks, hb.data(), sizeof(enc_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_geom, geom.data(), geom.size() * 8, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_nblocks, nblocks.data(), (size_t)nsb * sizeof(int), cudaMemcpyHostToDevice, st);
 
   const char* sname = level % 2 ? "enc.streamA" : "enc.streamB";
-  unsigned long long cap = (unsigned long long)nbr * 16384ull + (16ull << 20);
+  unsigned long long cap = (unsigned long long)nbr * (unsigned long long)NB * 2ull + (16ull << 20);
   if (ctx_->ws_size(sname) > cap)
     cap = ctx_->ws_size(sname);
   for (int attempt = 0; attempt < 4; ++attempt)
@@ -628,11 +631,7 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     a.parent_bricks = d_parents;
     a.geom = d_geom;
     a.nblocks = d_nblocks;
-    a.exps = d_exps;
-    a.kmin = d_kmin;
-    a.kmax = d_kmax;
     a.offset = d_off;
-    a.sizes = d_sizes;
     a.stream = d_stream;
     a.cap_bytes = cap;
     a.cursor = d_misc;
@@ -688,20 +687,20 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     }
     if (!keep_device_)
     {
-      // results to the host for the packer
-      out->exps.resize(nbs * kMaxBlocksPerSubband);
-      out->kmin.resize(nbs);
-      out->kmax.resize(nbs);
+      // results to the host for the packer: region offsets and the regions
       out->offset.resize(nbs);
-      out->sizes.resize(nbs * kKeyWindow);
-      out->stream.resize((size_t)misc[0]);
-      cudaMemcpyAsync(out->exps.data(), d_exps, nbs * kMaxBlocksPerSubband * 2, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(out->kmin.data(), d_kmin, nbs * 4, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(out->kmax.data(), d_kmax, nbs * 4, cudaMemcpyDeviceToHost, st);
       cudaMemcpyAsync(out->offset.data(), d_off, nbs * 8, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(out->sizes.data(), d_sizes, nbs * kKeyWindow * 4, cudaMemcpyDeviceToHost, st);
       if (misc[0])
-        cudaMemcpyAsync(out->stream.data(), d_stream, (size_t)misc[0], cudaMemcpyDeviceToHost, st);
+      {
+        // into pinned host memory kept by the context (one buffer per level)
+        char name[32];
+        snprintf(name, sizeof name, "enc.pin%d", level);
+        uint8_t* pin = (uint8_t*)ctx_->pinned(name, (size_t)misc[0]);
+        if (!pin)
+          return OutOfMemory;
+        cudaMemcpyAsync(pin, d_stream, (size_t)misc[0], cudaMemcpyDeviceToHost, st);
+        out->ext_stream = pin;
+      }
       if (cudaStreamSynchronize(st) != cudaSuccess)
         return CudaError;
     }

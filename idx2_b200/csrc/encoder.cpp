@@ -1,12 +1,14 @@
 // Encode driver (Core/idx2Encode.cpp:276-444).
 #include "encoder.h"
 
+#include <atomic>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <errno.h>
 #include <functional>
 #include <sys/stat.h>
+#include <thread>
 #include <unordered_map>
 
 namespace idx2g
@@ -205,12 +207,13 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
     r.level = ev.level;
     r.brick = plan.levels[(size_t)ev.level][(size_t)ev.brick].linear;
     r.subband = ev.subband;
-    r.exps = o.exps.data() + bs * kMaxBlocksPerSubband;
     r.nexps = o.nexps[(size_t)ev.subband];
-    r.kmin = o.kmin[bs];
-    r.kmax = o.kmax[bs];
-    r.sizes = o.sizes.data() + bs * kKeyWindow;
-    r.bytes = o.stream.data() + o.offset[bs];
+    region_view v = view_region(o.bytes() + o.offset[bs], r.nexps);
+    r.exps = v.exps;
+    r.kmin = v.kmin;
+    r.kmax = v.kmax;
+    r.sizes = v.sizes;
+    r.bytes = v.bytes;
     e = pk.add(r);
     if (e)
       return e;
@@ -220,20 +223,39 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
     return e;
   double t2 = now_s();
 
-  files->clear();
-  for (auto& kv : pk.files())
-    (*files)[kv.first] = std::move(kv.second.data);
   std::string meta = meta_text(*f, *p) + pk.stats_text();
   std::string meta_path = p->out_dir + "/" + p->name + "/" + p->field + ".idx2";
-  (*files)[meta_path] = std::vector<uint8_t>(meta.begin(), meta.end());
+  std::vector<const std::pair<const std::string, file_buffer>*> list;
+  unsigned long long total = meta.size();
+  for (auto& kv : pk.files())
+  {
+    list.push_back(&kv);
+    total += kv.second.nbytes;
+  }
+  if (files)
+  {
+    files->clear();
+    for (auto* kv : list)
+    {
+      std::vector<uint8_t>& d = (*files)[kv->first];
+      d.reserve(kv->second.nbytes);
+      for (const segment& s : kv->second.parts)
+        d.insert(d.end(), s.p, s.p + s.n);
+    }
+    (*files)[meta_path] = std::vector<uint8_t>(meta.begin(), meta.end());
+  }
   if (write_files)
   {
-    for (auto& kv : *files)
-    {
-      e = write_file(kv.first, kv.second);
-      if (e)
-        return e;
-    }
+    e = write_file(meta_path, std::vector<uint8_t>(meta.begin(), meta.end()));
+    if (e)
+      return e;
+    std::vector<std::pair<std::string, const file_buffer*>> wl;
+    wl.reserve(list.size());
+    for (auto* kv : list)
+      wl.push_back({ kv->first, &kv->second });
+    e = idx2g::write_files(wl);
+    if (e)
+      return e;
   }
   double t3 = now_s();
   if (timing)
@@ -241,6 +263,8 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
     timing->device_s = t1 - t0;
     timing->pack_s = t2 - t1;
     timing->write_s = t3 - t2;
+    timing->file_bytes = total;
+    timing->nfiles = (int)list.size() + 1;
   }
   return NoError;
 }

@@ -12,6 +12,7 @@
 #include "format.h"
 #include "packer.h"
 
+#include <cstring>
 #include <map>
 #include <string>
 #include <vector>
@@ -57,16 +58,45 @@ void subband_blocks(const dataset_format& f, int level, int sb, std::vector<bloc
 constexpr int kMaxBlocksPerSubband = 128;  // >= 125 (5^3)
 constexpr int kKeyWindow = 128;            // channel keys per (brick, subband)
 
+// The coder output of one (brick, subband) is a self-describing region of the level's
+// stream, 4-byte aligned:
+//   int32 kmin, int32 nkeys                       channel keys kmin .. kmin + nkeys - 1
+//   int16 exps[nexps], padded to 4 bytes          block exponents, coded blocks in Morton order
+//   uint32 sizes[nkeys]                           bytes of each channel stream (0: absent)
+//   channel streams back to back, ascending key, each byte-aligned; padded to 4 bytes
+struct region_view
+{
+  int kmin = 1, kmax = 0;
+  const int16_t* exps = nullptr;
+  const uint32_t* sizes = nullptr;
+  const uint8_t* bytes = nullptr;
+};
+inline size_t region_header_bytes(int nexps, int nkeys)
+{
+  return 8 + (((size_t)nexps * 2 + 3) & ~(size_t)3) + (size_t)nkeys * 4;
+}
+inline region_view view_region(const uint8_t* r, int nexps)
+{
+  region_view v;
+  int32_t kmin, nkeys;
+  memcpy(&kmin, r, 4);
+  memcpy(&nkeys, r + 4, 4);
+  v.kmin = nkeys > 0 ? kmin : 1;
+  v.kmax = nkeys > 0 ? kmin + nkeys - 1 : 0;
+  v.exps = reinterpret_cast<const int16_t*>(r + 8);
+  v.sizes = reinterpret_cast<const uint32_t*>(r + 8 + (((size_t)nexps * 2 + 3) & ~(size_t)3));
+  v.bytes = r + region_header_bytes(nexps, nkeys > 0 ? nkeys : 0);
+  return v;
+}
+
 struct level_output
 {
   int nbricks = 0, nsb = 0;
   std::vector<int> nexps;        // per subband (identical for every brick of the level)
-  std::vector<int16_t> exps;     // [brick][sb][kMaxBlocksPerSubband]
-  std::vector<int32_t> kmin;     // [brick][sb]
-  std::vector<int32_t> kmax;     // [brick][sb]
-  std::vector<uint64_t> offset;  // [brick][sb] byte offset of the channel streams
-  std::vector<uint32_t> sizes;   // [brick][sb][kKeyWindow]
-  std::vector<uint8_t> stream;
+  std::vector<uint64_t> offset;  // [brick][sb] byte offset of the region in stream
+  std::vector<uint8_t> stream;   // the regions (or, when ext_stream is set, in that buffer)
+  const uint8_t* ext_stream = nullptr;
+  const uint8_t* bytes() const { return ext_stream ? ext_stream : stream.data(); }
 };
 
 // A device (or test) stage that transforms and codes every brick of a level.
@@ -84,10 +114,13 @@ public:
 struct encode_timing
 {
   double device_s = 0, pack_s = 0, write_s = 0;
+  unsigned long long file_bytes = 0;  // data files + metadata file
+  int nfiles = 0;
 };
 
 // Full encode: plan, device stage for every level, packing, files (Core/idx2Encode.cpp:390).
-// files receives path -> bytes; write_files controls whether they are written to disk.
+// files (may be null) receives path -> bytes; write_files controls whether they are
+// written to disk (several files at a time).
 int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
                    std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
                    encode_timing* timing);

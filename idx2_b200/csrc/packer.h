@@ -5,12 +5,18 @@
 // the packer replays the reference's channel / chunk / file state machine over
 // those results in the reference's encode order, so chunk contents and chunk
 // order inside each file are the reference's.
+//
+// Brick data is never copied while packing: channels and files hold references
+// (segments) into the coder output, which must outlive the packer; files are
+// written from their segment lists.
 #pragma once
 
 #include "format.h"
 
 #include <cstdint>
+#include <deque>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -22,9 +28,9 @@ struct bit_writer
 {
   std::vector<uint8_t> bytes;
   uint64_t nbits = 0;
-  void put(uint64_t v, int n);
-  void put_varbyte(uint64_t v);  // Core/VarInt.h:14
-  void put_unary(uint64_t v);    // Core/VarInt.h:82
+  void put(uint64_t v, int n);    // n <= 57
+  void put_varbyte(uint64_t v);   // Core/VarInt.h:14
+  void put_unary(uint64_t v);     // Core/VarInt.h:82
   size_t size() const { return (size_t)((nbits + 7) / 8); }
   void clear()
   {
@@ -65,25 +71,35 @@ struct pack_stats
     exp_chunks_raw, exp_chunks_z, exp_chunk_sizes, exp_addrs_raw, exp_addrs_z;
 };
 
+struct segment
+{
+  const uint8_t* p;
+  size_t n;
+};
+
 struct file_buffer
 {
-  std::vector<uint8_t> data;        // chunks in write order (then metadata at flush)
-  bit_writer chunk_sizes;           // varbyte sizes of bit-plane chunks
-  std::vector<u64> chunk_addrs;     // chunk addresses
+  std::vector<segment> parts;                       // file content, in order
+  std::deque<std::vector<uint8_t>> owned;           // bytes the parts point into
+  size_t nbytes = 0;
+  bit_writer chunk_sizes;                           // varbyte sizes of bit-plane chunks
+  std::vector<u64> chunk_addrs;                     // chunk addresses
   bool has_chunks = false;
-  std::vector<uint8_t> exp_data;    // zstd-compressed exponent chunks
-  bit_writer exp_sizes;
+  std::vector<int> exp_chunks;                      // indices into the packer's exponent chunks
   std::vector<u64> exp_addrs;
   bool has_exps = false;
+  void append_owned(std::vector<uint8_t>&& v);
+  void append_ref(const uint8_t* p, size_t n);
 };
 
 class packer
 {
 public:
   packer(const dataset_format& f, double tolerance);
+  ~packer();
   // One EncodeSubband call of the reference (Core/idx2Encode.cpp:261).
   int add(const subband_result& r);
-  // FlushChunks + FlushChunkExponents (Core/idx2Write.cpp:317, :121); fills files.
+  // FlushChunks + FlushChunkExponents (Core/idx2Write.cpp:317, :121).
   int finish();
   std::map<std::string, file_buffer>& files() { return files_; }
   const pack_stats& stats() const { return stats_; }
@@ -94,15 +110,23 @@ private:
   struct channel
   {
     bit_writer deltas, sizes;
-    std::vector<uint8_t> bricks;
+    std::vector<segment> bricks;
+    size_t brick_bytes = 0;
     u64 last_chunk = 0, last_brick = 0;
     int nbricks = 0;
+    uint32_t key = 0;
   };
   struct sub_channel
   {
     std::vector<uint8_t> brick_exps;
     u64 last_chunk = 0, last_brick = 0;
   };
+  struct exp_chunk
+  {
+    std::vector<uint8_t> raw, z;
+  };
+  channel& chan(int level, int subband, int bpkey);
+  channel* find_chan(int level, int subband, int bpkey);
   void write_chunk(channel& c, int level, int subband, int bpkey);
   void write_chunk_exps(sub_channel& s, int level, int subband);
   void first_touch_order(const subband_result& r, std::vector<int>* keys) const;
@@ -110,8 +134,10 @@ private:
   const dataset_format& f_;
   double tol_;
   int etol_;
-  std::map<uint32_t, channel> channels_;  // ordered by channel key
+  std::vector<int32_t> chan_index_;   // (level, subband, bpkey) -> index into channels_, -1
+  std::deque<channel> channels_;
   std::map<std::pair<int, int>, sub_channel> subs_;
+  std::deque<exp_chunk> exp_chunks_;  // compressed in parallel at finish
   std::map<std::string, file_buffer> files_;
   pack_stats stats_;
 };
@@ -129,5 +155,8 @@ inline bool plane_coded(int bp, int emax, int etol, int bpc)
   return !(too_high && ((realbp + 1024) % bpc) == 0);
 }
 int exponent_f64(double v);
+
+// Write files from their parts (creating directories), with several threads.
+int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& files);
 
 } // namespace idx2g

@@ -41,11 +41,7 @@ public:
     out->nbricks = (int)bricks.size();
     out->nsb = nsb;
     out->nexps.assign((size_t)nsb, 0);
-    out->exps.assign(bricks.size() * (size_t)nsb * kMaxBlocksPerSubband, 0);
-    out->kmin.assign(bricks.size() * (size_t)nsb, 1);
-    out->kmax.assign(bricks.size() * (size_t)nsb, 0);
     out->offset.assign(bricks.size() * (size_t)nsb, 0);
-    out->sizes.assign(bricks.size() * (size_t)nsb * kKeyWindow, 0);
     out->stream.clear();
     std::vector<double> buf((size_t)NB);
     std::vector<uint8_t> rec(1 << 24);
@@ -94,7 +90,7 @@ public:
         memcpy(&ne, p, 4);
         p += 4;
         out->nexps[(size_t)s] = ne;
-        memcpy(out->exps.data() + bs * kMaxBlocksPerSubband, p, 2 * (size_t)ne);
+        const uint8_t* exps = p;
         p += 2 * (size_t)ne;
         int32_t nch;
         memcpy(&nch, p, 4);
@@ -116,25 +112,31 @@ public:
           chs.push_back({ key, nbytes, p });
           p += nbytes;
         }
-        if (chs.empty())
-          continue;
+        // region in the layout of encoder.h: header, exponents, sizes, channel streams
         int kmin = 1 << 30, kmax = -1;
         for (auto& c : chs)
         {
           kmin = c.key < kmin ? c.key : kmin;
           kmax = c.key > kmax ? c.key : kmax;
         }
-        if (kmax - kmin + 1 > kKeyWindow)
+        const int nkeys = chs.empty() ? 0 : kmax - kmin + 1;
+        if (nkeys > kKeyWindow)
           return DeviceStreamOverflow;
-        out->kmin[bs] = kmin;
-        out->kmax[bs] = kmax;
-        out->offset[bs] = out->stream.size();
+        std::vector<uint8_t>& st = out->stream;
+        out->offset[bs] = st.size();
+        size_t base = st.size();
+        st.resize(base + region_header_bytes(ne, nkeys), 0);
+        int32_t h[2] = { nkeys ? kmin : 1, nkeys };
+        memcpy(st.data() + base, h, 8);
+        memcpy(st.data() + base + 8, exps, 2 * (size_t)ne);
+        uint32_t* sizes = (uint32_t*)(st.data() + base + 8 + ((2 * (size_t)ne + 3) & ~(size_t)3));
         std::sort(chs.begin(), chs.end(), [](const ch& a, const ch& b) { return a.key < b.key; });
         for (auto& c : chs)
-        {
-          out->sizes[bs * kKeyWindow + (size_t)(c.key - kmin)] = (uint32_t)c.nbytes;
-          out->stream.insert(out->stream.end(), c.data, c.data + c.nbytes);
-        }
+          sizes[c.key - kmin] = (uint32_t)c.nbytes;
+        for (auto& c : chs)
+          st.insert(st.end(), c.data, c.data + c.nbytes);
+        while (st.size() % 4)
+          st.push_back(0);
       }
     }
     cur_.swap(next_);
@@ -198,8 +200,7 @@ int main(int argc, char** argv)
   }
   fclose(fp);
   oracle_coder coder(f, raw.data());
-  std::map<std::string, std::vector<uint8_t>> files;
-  e = encode_dataset(&f, &p, &coder, &files, true, nullptr);
+  e = encode_dataset(&f, &p, &coder, nullptr, true, nullptr);
   if (e)
   {
     fprintf(stderr, "encode error %d\n", e);
