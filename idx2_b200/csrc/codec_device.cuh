@@ -565,5 +565,85 @@ inline __device__ void write_plane(uint32_t* words, unsigned long long pos, unsi
   }
 }
 
+// 192-bit little-endian bit string in three words.
+struct bits192
+{
+  unsigned long long w0 = 0, w1 = 0, w2 = 0;
+  __device__ __forceinline__ void set(int p)
+  {
+    if (p < 64)
+      w0 |= 1ull << p;
+    else if (p < 128)
+      w1 |= 1ull << (p - 64);
+    else
+      w2 |= 1ull << (p - 128);
+  }
+  // bits [b, b + 32), b >= 0
+  __device__ __forceinline__ uint32_t get32(int b) const
+  {
+    const int k = b >> 6, o = b & 63;
+    const unsigned long long lo = k == 0 ? w0 : (k == 1 ? w1 : (k == 2 ? w2 : 0ull));
+    const unsigned long long hi = k == 0 ? w1 : (k == 1 ? w2 : 0ull);
+    return (uint32_t)(o ? ((lo >> o) | (hi << (64 - o))) : lo);
+  }
+};
+
+// The code of one bit plane (Core/Zfp.h:771 Encode<u64>) built in registers: the first nin
+// bits of x raw, then for every further one-bit a group bit 1, the zero bits up to it and
+// the one-bit itself (implied when it is the last coefficient), then a group bit 0 while
+// coefficients remain. At most 64 + 2 * 64 + 1 bits; returns the length.
+__device__ __forceinline__ int plane_code(unsigned long long x, int nin, int nvals, bits192* c)
+{
+  c->w0 = nin >= 64 ? x : (x & ((1ull << nin) - 1ull));
+  c->w1 = c->w2 = 0;
+  int len = nin, n = nin;
+  unsigned long long r = n < 64 ? (x >> n) : 0ull;
+  while (n < nvals)
+  {
+    if (r == 0)
+    {
+      len += 1;
+      break;
+    }
+    c->set(len);
+    len += 1;
+    const int t = __ffsll((long long)r) - 1;
+    const int s = n + t;
+    len += t;
+    if (s < nvals - 1)
+    {
+      c->set(len);
+      len += 1;
+      n = s + 1;
+      r = (t + 1 < 64) ? (r >> (t + 1)) : 0ull;
+    }
+    else
+    {
+      n = nvals;
+      r = 0;
+    }
+  }
+  return len;
+}
+
+// OR a code of len bits into a zero-initialised word stream at bit position pos.
+__device__ __forceinline__ void or_code(uint32_t* words, unsigned long long pos, const bits192& c, int len)
+{
+  if (len <= 0)
+    return;
+  uint32_t* w = words + (pos >> 5);
+  const int sh = (int)(pos & 31);
+  const uint32_t first = (uint32_t)(c.w0 << sh);
+  if (first)
+    atomicOr(w, first);
+  const int nw = (sh + len + 31) >> 5;
+  for (int i = 1; i < nw; ++i)
+  {
+    const uint32_t v = c.get32(32 * i - sh);
+    if (v)
+      atomicOr(w + i, v);
+  }
+}
+
 } // namespace dev
 } // namespace idx2g

@@ -52,7 +52,7 @@ static int up(T** dst, const std::vector<T>& v, cudaStream_t st, size_t pad = 0)
 
 int decode_device::upload(device_ctx* ctx, const std::vector<int16_t>& exps, const std::vector<int32_t>& kmin,
                           const std::vector<int32_t>& n, const std::vector<uint64_t>& first,
-                          const std::vector<uint64_t>& off, const std::vector<uint8_t>& blob)
+                          const std::vector<uint64_t>& off, const uint8_t* blob, size_t blob_bytes)
 {
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
@@ -66,11 +66,21 @@ int decode_device::upload(device_ctx* ctx, const std::vector<int16_t>& exps, con
   if (!e)
     e = up((uint64_t**)&off_, off, st);
   if (!e)
-    e = up((uint8_t**)&blob_, blob, st, 16);
+  {
+    // the blob (padded with 16 zero bytes for the bit readers' look-ahead)
+    if (cudaMalloc((void**)&blob_, blob_bytes + 32) != cudaSuccess)
+      e = OutOfMemory;
+    else
+    {
+      if (blob_bytes)
+        cudaMemcpyAsync(blob_, blob, blob_bytes, cudaMemcpyHostToDevice, st);
+      cudaMemsetAsync(blob_ + blob_bytes, 0, 32, st);
+    }
+  }
   if (e)
     return e;
-  resident_ = exps.size() * 2 + kmin.size() * 4 + n.size() * 4 + first.size() * 8 + off.size() * 8 + blob.size();
-  blob_bytes_ = blob.size();
+  resident_ = exps.size() * 2 + kmin.size() * 4 + n.size() * 4 + first.size() * 8 + off.size() * 8 + blob_bytes;
+  blob_bytes_ = blob_bytes;
   if (cudaStreamSynchronize(st) != cudaSuccess)
     return CudaError;
   return NoError;

@@ -48,7 +48,7 @@ public:
   ~decode_device();
   int upload(device_ctx* ctx, const std::vector<int16_t>& exps, const std::vector<int32_t>& kmin,
              const std::vector<int32_t>& n, const std::vector<uint64_t>& first,
-             const std::vector<uint64_t>& off, const std::vector<uint8_t>& blob);
+             const std::vector<uint64_t>& off, const uint8_t* blob, size_t blob_bytes);
   int decode(device_ctx* ctx, const decode_request& rq, void* out, size_t out_bytes, bool out_on_device,
              double* kernel_ms);
   // Allocation-free decode into a device buffer: every temporary lives in a fixed static

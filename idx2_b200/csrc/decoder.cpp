@@ -17,7 +17,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
+#include <fcntl.h>
 #include <map>
+#include <sys/stat.h>
+#include <thread>
+#include <unistd.h>
 #include <unordered_map>
 
 namespace idx2g
@@ -26,32 +31,39 @@ namespace idx2g
 namespace
 {
 
+// LSB-first bit reader over a byte range (Core/BitStream.h); reads past the end give zeros.
 struct bit_reader
 {
   const uint8_t* p;
   size_t n;
   uint64_t pos = 0;
-  uint64_t get(int bits)
+  // at least 57 valid bits starting at pos
+  uint64_t peek() const
   {
-    uint64_t v = 0;
-    for (int i = 0; i < bits; ++i)
-    {
-      uint64_t q = pos + (uint64_t)i;
-      uint64_t b = (q >> 3) < n ? (p[q >> 3] >> (q & 7)) & 1u : 0;
-      v |= b << i;
-    }
+    const size_t b = (size_t)(pos >> 3);
+    uint64_t w = 0;
+    if (b + 8 <= n)
+      memcpy(&w, p + b, 8);
+    else if (b < n)
+      memcpy(&w, p + b, n - b);
+    return w >> (pos & 7);
+  }
+  uint64_t get(int bits)  // bits <= 57
+  {
+    uint64_t v = peek() & ((1ull << bits) - 1);
     pos += (uint64_t)bits;
     return v;
   }
   uint64_t varbyte()
   {
-    // Core/VarInt.h:30 ReadVarByte
+    // Core/VarInt.h:30 ReadVarByte: 7 value bits then a continuation bit
     uint64_t v = 0;
     int sh = 0;
     while (true)
     {
-      v = (get(7) << (7 * sh++)) + v;
-      if (get(1) == 0)
+      uint64_t b = get(8);
+      v = ((b & 0x7F) << (7 * sh++)) + v;
+      if (!(b >> 7))
         break;
       if (sh > 10)
         break;
@@ -60,22 +72,30 @@ struct bit_reader
   }
   uint64_t unary()
   {
+    // Core/VarInt.h:90 ReadUnary: zero bits up to the next one bit
     uint64_t v = 0;
-    while (!get(1))
+    while (true)
     {
-      ++v;
+      uint64_t w = peek() & ((1ull << 57) - 1);
+      if (w)
+      {
+        int z = __builtin_ctzll(w);
+        pos += (uint64_t)z + 1;
+        return v + (uint64_t)z;
+      }
+      v += 57;
+      pos += 57;
       if ((pos >> 3) > n)
-        break;
+        return v;
     }
-    return v;
   }
   void next_byte() { pos = (pos + 7) & ~7ull; }
 };
 
-int32_t rd_i32(const std::vector<uint8_t>& d, size_t off)
+inline int32_t rd_i32(const uint8_t* d, size_t off)
 {
   int32_t v;
-  memcpy(&v, d.data() + off, 4);
+  memcpy(&v, d + off, 4);
   return v;
 }
 
@@ -91,6 +111,27 @@ bool read_whole(const std::string& path, std::vector<uint8_t>* out)
   size_t r = sz > 0 ? fread(out->data(), 1, (size_t)sz, fp) : 0;
   fclose(fp);
   return r == out->size();
+}
+
+// Run f(i) for i in [0, n) on a pool of threads.
+template <typename F>
+void parallel_for(size_t n, F&& f)
+{
+  unsigned nt = std::thread::hardware_concurrency();
+  nt = nt ? (nt > 32 ? 32 : nt) : 4;
+  if (nt > n)
+    nt = (unsigned)(n ? n : 1);
+  std::atomic<size_t> next{ 0 };
+  auto work = [&]() {
+    for (size_t i; (i = next.fetch_add(1)) < n;)
+      f(i);
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; ++t)
+    th.emplace_back(work);
+  work();
+  for (auto& t : th)
+    t.join();
 }
 
 } // namespace
@@ -110,13 +151,41 @@ struct dataset_handle
   std::vector<int32_t> chan_kmin, chan_n;        // [flat brick][sb]
   std::vector<uint64_t> chan_first;              // [flat brick][sb] index into chan_off
   std::vector<uint64_t> chan_off;                // byte offset in blob, ~0 = absent
-  std::vector<uint8_t> blob;
+  const uint8_t* blob = nullptr;                 // every data file back to back (pinned host memory)
   size_t blob_bytes = 0;
   // device copies
   decode_device dev;
 };
 
-static int load_index(dataset_handle* h)
+namespace
+{
+
+struct data_file
+{
+  std::string path;
+  int level;
+  size_t base = 0, size = 0;
+};
+
+// a chunk located in the blob
+struct chunk_ref
+{
+  size_t off, size;
+  u64 addr;
+  int level;
+};
+
+// one brick's data inside a bit-plane chunk
+struct chan_entry
+{
+  uint32_t slot;  // flat brick * nsb + subband
+  int32_t bpkey;
+  uint64_t off;   // byte offset in the blob
+};
+
+} // namespace
+
+static int load_index(device_ctx* ctx, dataset_handle* h)
 {
   dataset_format& f = h->f;
   const int L = f.nlevels;
@@ -165,43 +234,103 @@ static int load_index(dataset_handle* h)
     }
   }
   const size_t nflat = h->level_brick_base[(size_t)L];
-  h->exps.assign(nflat * (size_t)nsb * kMaxBlocksPerSubband, 0);
-  h->chan_kmin.assign(nflat * (size_t)nsb, 0);
-  h->chan_n.assign(nflat * (size_t)nsb, 0);
-  h->chan_first.assign(nflat * (size_t)nsb, 0);
-  // collected channel entries: (flat brick, sb) -> list of (bpkey, blob offset)
-  std::vector<std::vector<std::pair<int, uint64_t>>> chans(nflat * (size_t)nsb);
+  const size_t nslots = nflat * (size_t)nsb;
+  if (nslots >= 0xFFFFFFFFull)
+    return OptionNotSupported;
+  h->exps.assign(nslots * kMaxBlocksPerSubband, 0);
+  h->chan_kmin.assign(nslots, 0);
+  h->chan_n.assign(nslots, 0);
+  h->chan_first.assign(nslots, 0);
 
-  // the set of data files: one per (level, brick >> log2(bricks per file))
-  std::map<std::string, int> files;  // path -> level
+  // the set of data files: one per (level, brick >> log2(bricks per file)); a missing file
+  // leaves its bricks undecoded (Core/idx2Decode.cpp:166-168)
+  std::map<std::string, int> names;
   for (int l = 0; l < L; ++l)
     for (size_t i = 0; i < h->brick3[(size_t)l].size(); ++i)
-      files[file_path(f, linear_brick(f, l, h->brick3[(size_t)l][i]), l)] = l;
-
-  const int esz = f.type == dtype::float32 ? 1 : 2;
-  for (auto& kv : files)
+      names[file_path(f, linear_brick(f, l, h->brick3[(size_t)l][i]), l)] = l;
+  std::vector<data_file> files;
+  size_t total = 0;
+  for (auto& kv : names)
   {
-    std::vector<uint8_t> d;
-    if (!read_whole(kv.first, &d))
-      continue;  // a missing file leaves its bricks undecoded (Core/idx2Decode.cpp:166-168)
-    const int level = kv.second;
-    if (d.size() < 16)
+    struct stat st;
+    if (stat(kv.first.c_str(), &st) != 0 || !S_ISREG(st.st_mode))
+      continue;
+    data_file df;
+    df.path = kv.first;
+    df.level = kv.second;
+    df.base = total;
+    df.size = (size_t)st.st_size;
+    total += (df.size + 15) & ~(size_t)15;
+    files.push_back(df);
+  }
+
+  // every file into one pinned buffer, in ranges of 16 MB read by a pool of threads
+  uint8_t* blob = (uint8_t*)ctx->pinned("dec.files", total + 16);
+  if (!blob)
+    return OutOfMemory;
+  {
+    struct range
+    {
+      int file;
+      size_t off, n;
+    };
+    std::vector<range> rs;
+    const size_t R = (size_t)16 << 20;
+    for (size_t i = 0; i < files.size(); ++i)
+      for (size_t o = 0; o < files[i].size; o += R)
+        rs.push_back({ (int)i, o, std::min(R, files[i].size - o) });
+    std::vector<int> fds(files.size(), -1);
+    for (size_t i = 0; i < files.size(); ++i)
+      fds[i] = open(files[i].path.c_str(), O_RDONLY);
+    std::atomic<int> bad{ 0 };
+    parallel_for(rs.size(), [&](size_t k) {
+      const range& r = rs[k];
+      size_t done = 0;
+      while (done < r.n)
+      {
+        ssize_t got = fds[(size_t)r.file] < 0 ? -1
+                      : pread(fds[(size_t)r.file], blob + files[(size_t)r.file].base + r.off + done,
+                              r.n - done, (off_t)(r.off + done));
+        if (got <= 0)
+        {
+          bad = 1;
+          return;
+        }
+        done += (size_t)got;
+      }
+    });
+    for (int fd : fds)
+      if (fd >= 0)
+        close(fd);
+    if (bad)
+      return FileReadFailed;
+  }
+  h->blob = blob;
+  h->blob_bytes = total;
+
+  // file tails: exponent chunks and bit-plane chunks
+  std::vector<chunk_ref> exp_chunks, bp_chunks;
+  for (const data_file& df : files)
+  {
+    const uint8_t* d = blob + df.base;
+    const int level = df.level;
+    if (df.size < 16)
       return CorruptStream;
     // exponent section (Core/idx2Read.cpp:252 ReadFileExponents)
-    size_t E = d.size();
-    int32_t total = rd_i32(d, E - 4);
+    const size_t E = df.size;
+    int32_t total_e = rd_i32(d, E - 4);
     int32_t nexp = rd_i32(d, E - 8);
     int32_t asz = rd_i32(d, E - 12);
-    if (total < 16 || (size_t)total > E || asz < 0 || (size_t)asz + 16 > (size_t)total)
+    if (total_e < 16 || (size_t)total_e > E || asz < 0 || (size_t)asz + 16 > (size_t)total_e || nexp < 0)
       return CorruptStream;
     std::vector<uint8_t> addrs_raw;
-    if (zstd_decompress(d.data() + E - 12 - (size_t)asz, (size_t)asz, &addrs_raw))
+    if (zstd_decompress(d + E - 12 - (size_t)asz, (size_t)asz, &addrs_raw))
       return CorruptStream;
     int32_t ssz = rd_i32(d, E - 16 - (size_t)asz);
-    if (ssz < 0 || (size_t)ssz + (size_t)asz + 16 > (size_t)total)
+    if (ssz < 0 || (size_t)ssz + (size_t)asz + 16 > (size_t)total_e)
       return CorruptStream;
-    bit_reader sr{ d.data() + E - 16 - (size_t)asz - (size_t)ssz, (size_t)ssz };
-    size_t exp_beg = E - (size_t)total;
+    bit_reader sr{ d + E - 16 - (size_t)asz - (size_t)ssz, (size_t)ssz };
+    const size_t exp_beg = E - (size_t)total_e;
     size_t off = exp_beg;
     for (int c = 0; c < nexp; ++c)
     {
@@ -210,55 +339,27 @@ static int load_index(dataset_handle* h)
         return CorruptStream;
       u64 addr;
       memcpy(&addr, addrs_raw.data() + (size_t)c * 8, 8);
-      std::vector<uint8_t> ex;
-      if (zstd_decompress(d.data() + off, (size_t)csz, &ex))
-        return CorruptStream;
+      exp_chunks.push_back({ df.base + off, (size_t)csz, addr, level });
       off += csz;
-      int sb = (int)((addr >> 12) & 0x3F);
-      int lv = (int)((addr >> 60) & 0xF);
-      u64 chunk = (addr >> 18) & 0x3FFFFFFFFFFull;
-      if (lv != level || sb >= nsb)
-        continue;
-      // every brick of this chunk: exps at BrickInChunk * BlockCount * esz
-      int shift = log2_ceil(f.bricks_per_chunk[(size_t)lv]);
-      u64 first = chunk << shift, last = (chunk + 1) << shift;
-      const int bc = h->blocks_per_sb[(size_t)lv][(size_t)sb];
-      for (u64 lin = first; lin < last && lin < h->brick_index[(size_t)lv].size(); ++lin)
-      {
-        int bi = h->brick_index[(size_t)lv][lin];
-        if (bi < 0)
-          continue;
-        size_t pos = (size_t)h->brick_in_chunk[(size_t)lv][(size_t)bi] * (size_t)bc * (size_t)esz;
-        size_t flat = h->level_brick_base[(size_t)lv] + (size_t)bi;
-        int16_t* dst = h->exps.data() + (flat * (size_t)nsb + (size_t)sb) * kMaxBlocksPerSubband;
-        for (int b = 0; b < bc; ++b)
-        {
-          size_t q = pos + (size_t)b * (size_t)esz;
-          int v = 0;
-          if (q + (size_t)esz <= ex.size())
-            v = esz == 2 ? (int)ex[q] | ((int)ex[q + 1] << 8) : (int)ex[q];
-          dst[b] = (int16_t)(esz == 2 ? v - 1023 : v - 127);
-        }
-      }
     }
     if (exp_beg == 0)
       continue;
     // bit-plane section (Core/idx2Read.cpp:82 ReadFile)
-    size_t E2 = exp_beg;
+    const size_t E2 = exp_beg;
+    if (E2 < 12)
+      return CorruptStream;
     int32_t nch = rd_i32(d, E2 - 4);
     int32_t asz2 = rd_i32(d, E2 - 8);
-    if (asz2 < 0 || (size_t)asz2 + 12 > E2)
+    if (asz2 < 0 || (size_t)asz2 + 12 > E2 || nch < 0)
       return CorruptStream;
     std::vector<uint8_t> caddrs;
-    if (zstd_decompress(d.data() + E2 - 8 - (size_t)asz2, (size_t)asz2, &caddrs))
+    if (zstd_decompress(d + E2 - 8 - (size_t)asz2, (size_t)asz2, &caddrs))
       return CorruptStream;
     int32_t ssz2 = rd_i32(d, E2 - 12 - (size_t)asz2);
     if (ssz2 < 0 || (size_t)ssz2 + (size_t)asz2 + 12 > E2)
       return CorruptStream;
-    bit_reader csr{ d.data() + E2 - 12 - (size_t)asz2 - (size_t)ssz2, (size_t)ssz2 };
-    size_t body_end = E2 - 12 - (size_t)asz2 - (size_t)ssz2;
-    size_t blob_base = h->blob.size();
-    h->blob.insert(h->blob.end(), d.begin(), d.begin() + (long)body_end);
+    bit_reader csr{ d + E2 - 12 - (size_t)asz2 - (size_t)ssz2, (size_t)ssz2 };
+    const size_t body_end = E2 - 12 - (size_t)asz2 - (size_t)ssz2;
     size_t coff = 0;
     for (int c = 0; c < nch; ++c)
     {
@@ -267,78 +368,138 @@ static int load_index(dataset_handle* h)
         return CorruptStream;
       u64 addr;
       memcpy(&addr, caddrs.data() + (size_t)c * 8, 8);
-      int sb = (int)((addr >> 12) & 0x3F);
-      int lv = (int)((addr >> 60) & 0xF);
-      int bpkey = (int)(addr & 0xFFF);
-      // chunk header (Core/idx2Decode.cpp:507 DecompressChunk)
-      bit_reader cr{ d.data() + coff, (size_t)csz };
-      int nbr = (int)cr.varbyte();
-      std::vector<u64> bricks((size_t)(nbr > 0 ? nbr : 0));
-      if (nbr > 0)
-      {
-        u64 b = cr.varbyte();
-        bricks[0] = b;
-        for (int i = 1; i < nbr; ++i)
-        {
-          b += cr.unary() + 1;
-          bricks[(size_t)i] = b;
-        }
-      }
-      cr.next_byte();
-      std::vector<uint64_t> offs((size_t)(nbr > 0 ? nbr : 0), 0);
-      uint64_t acc = 0;
-      for (int i = 1; i < nbr; ++i)
-      {
-        acc += cr.varbyte();
-        offs[(size_t)i] = acc;
-      }
-      if (nbr > 0)
-        cr.varbyte();
-      uint64_t data_start = cr.pos >> 3;
-      if (lv == level && sb < nsb)
-      {
-        for (int i = 0; i < nbr; ++i)
-        {
-          u64 lin = bricks[(size_t)i];
-          if (lin >= h->brick_index[(size_t)lv].size())
-            continue;
-          int bi = h->brick_index[(size_t)lv][lin];
-          if (bi < 0)
-            continue;
-          size_t flat = h->level_brick_base[(size_t)lv] + (size_t)bi;
-          chans[flat * (size_t)nsb + (size_t)sb].push_back(
-            { bpkey, (uint64_t)(blob_base + coff + data_start + offs[(size_t)i]) });
-        }
-      }
+      bp_chunks.push_back({ df.base + coff, (size_t)csz, addr, level });
       coff += csz;
     }
   }
-  // flatten the channel table
-  h->chan_off.clear();
-  for (size_t i = 0; i < chans.size(); ++i)
+
+  // exponent chunks: decompress and spread over their bricks (chunks own disjoint rows)
+  const int esz = f.type == dtype::float32 ? 1 : 2;
+  std::atomic<int> err{ 0 };
+  parallel_for(exp_chunks.size(), [&](size_t k) {
+    const chunk_ref& c = exp_chunks[k];
+    int sb = (int)((c.addr >> 12) & 0x3F);
+    int lv = (int)((c.addr >> 60) & 0xF);
+    u64 chunk = (c.addr >> 18) & 0x3FFFFFFFFFFull;
+    if (lv != c.level || sb >= nsb)
+      return;
+    std::vector<uint8_t> ex;
+    if (zstd_decompress(blob + c.off, c.size, &ex))
+    {
+      err = CorruptStream;
+      return;
+    }
+    // every brick of this chunk: exps at BrickInChunk * BlockCount * esz
+    int shift = log2_ceil(f.bricks_per_chunk[(size_t)lv]);
+    u64 first = chunk << shift, last = (chunk + 1) << shift;
+    const int bc = h->blocks_per_sb[(size_t)lv][(size_t)sb];
+    for (u64 lin = first; lin < last && lin < h->brick_index[(size_t)lv].size(); ++lin)
+    {
+      int bi = h->brick_index[(size_t)lv][lin];
+      if (bi < 0)
+        continue;
+      size_t pos = (size_t)h->brick_in_chunk[(size_t)lv][(size_t)bi] * (size_t)bc * (size_t)esz;
+      size_t flat = h->level_brick_base[(size_t)lv] + (size_t)bi;
+      int16_t* dst = h->exps.data() + (flat * (size_t)nsb + (size_t)sb) * kMaxBlocksPerSubband;
+      for (int b = 0; b < bc; ++b)
+      {
+        size_t q = pos + (size_t)b * (size_t)esz;
+        int v = 0;
+        if (q + (size_t)esz <= ex.size())
+          v = esz == 2 ? (int)ex[q] | ((int)ex[q + 1] << 8) : (int)ex[q];
+        dst[b] = (int16_t)(esz == 2 ? v - 1023 : v - 127);
+      }
+    }
+  });
+  if (err)
+    return err;
+
+  // bit-plane chunk headers (Core/idx2Decode.cpp:507 DecompressChunk), one task per chunk
+  std::vector<std::vector<chan_entry>> entries(bp_chunks.size());
+  parallel_for(bp_chunks.size(), [&](size_t k) {
+    const chunk_ref& c = bp_chunks[k];
+    int sb = (int)((c.addr >> 12) & 0x3F);
+    int lv = (int)((c.addr >> 60) & 0xF);
+    int bpkey = (int)(c.addr & 0xFFF);
+    if (lv != c.level || sb >= nsb)
+      return;
+    bit_reader cr{ blob + c.off, c.size };
+    const uint64_t nbr64 = cr.varbyte();
+    if (nbr64 > c.size * 8 + 1)
+    {
+      err = CorruptStream;
+      return;
+    }
+    const int nbr = (int)nbr64;
+    std::vector<u64> bricks((size_t)nbr);
+    if (nbr > 0)
+    {
+      u64 b = cr.varbyte();
+      bricks[0] = b;
+      for (int i = 1; i < nbr; ++i)
+      {
+        b += cr.unary() + 1;
+        bricks[(size_t)i] = b;
+      }
+    }
+    cr.next_byte();
+    std::vector<uint64_t> offs((size_t)nbr, 0);
+    uint64_t acc = 0;
+    for (int i = 1; i < nbr; ++i)
+    {
+      acc += cr.varbyte();
+      offs[(size_t)i] = acc;
+    }
+    if (nbr > 0)
+      cr.varbyte();
+    const uint64_t data_start = cr.pos >> 3;
+    std::vector<chan_entry>& out = entries[k];
+    out.reserve((size_t)nbr);
+    const std::vector<int>& index = h->brick_index[(size_t)lv];
+    for (int i = 0; i < nbr; ++i)
+    {
+      u64 lin = bricks[(size_t)i];
+      if (lin >= index.size())
+        continue;
+      int bi = index[lin];
+      if (bi < 0)
+        continue;
+      size_t flat = h->level_brick_base[(size_t)lv] + (size_t)bi;
+      out.push_back({ (uint32_t)(flat * (size_t)nsb + (size_t)sb), bpkey,
+                      (uint64_t)(c.off + data_start + offs[(size_t)i]) });
+    }
+  });
+  if (err)
+    return err;
+
+  // channel table: key range per (brick, subband), then the offsets
+  std::vector<int32_t> kmax(nslots, -1);
+  std::vector<int32_t>& kmin = h->chan_kmin;
+  std::fill(kmin.begin(), kmin.end(), 1 << 30);
+  for (const auto& v : entries)
+    for (const chan_entry& e : v)
+    {
+      kmin[e.slot] = std::min(kmin[e.slot], e.bpkey);
+      kmax[e.slot] = std::max(kmax[e.slot], e.bpkey);
+    }
+  uint64_t nchan = 0;
+  for (size_t i = 0; i < nslots; ++i)
   {
-    auto& v = chans[i];
-    if (v.empty())
+    if (kmax[i] < 0)
     {
-      h->chan_kmin[i] = 1;
+      kmin[i] = 1;
       h->chan_n[i] = 0;
-      h->chan_first[i] = h->chan_off.size();
-      continue;
     }
-    int kmin = 1 << 30, kmax = -1;
-    for (auto& e : v)
-    {
-      kmin = std::min(kmin, e.first);
-      kmax = std::max(kmax, e.first);
-    }
-    h->chan_kmin[i] = kmin;
-    h->chan_n[i] = kmax - kmin + 1;
-    h->chan_first[i] = h->chan_off.size();
-    h->chan_off.resize(h->chan_off.size() + (size_t)(kmax - kmin + 1), ~0ull);
-    for (auto& e : v)
-      h->chan_off[h->chan_first[i] + (size_t)(e.first - kmin)] = e.second;
+    else
+      h->chan_n[i] = kmax[i] - kmin[i] + 1;
+    h->chan_first[i] = nchan;
+    nchan += (uint64_t)h->chan_n[i];
   }
-  h->blob_bytes = h->blob.size();
+  h->chan_off.assign(nchan, ~0ull);
+  parallel_for(entries.size(), [&](size_t k) {
+    for (const chan_entry& e : entries[k])
+      h->chan_off[h->chan_first[e.slot] + (size_t)(e.bpkey - kmin[e.slot])] = e.off;
+  });
   return NoError;
 }
 
@@ -358,16 +519,16 @@ int dataset_open(device_ctx* ctx, const params& pin, dataset_handle** out)
     e = finalize_read(&h->f, &p);
   }
   if (!e)
-    e = load_index(h);
+    e = load_index(ctx, h);
   if (!e)
-    e = h->dev.upload(ctx, h->exps, h->chan_kmin, h->chan_n, h->chan_first, h->chan_off, h->blob);
+    e = h->dev.upload(ctx, h->exps, h->chan_kmin, h->chan_n, h->chan_first, h->chan_off, h->blob,
+                      h->blob_bytes);
+  h->blob = nullptr;  // the pinned staging buffer stays with the context
   if (e)
   {
     delete h;
     return e;
   }
-  h->blob.clear();
-  h->blob.shrink_to_fit();
   *out = h;
   return NoError;
 }

@@ -26,9 +26,36 @@ namespace idx2g
 namespace
 {
 
+// Per-phase cycle counters of thread 0 of every CTA, for profiling builds only
+// (-DIDX2G_PHASE_TIMING); compiled out otherwise.
+#ifdef IDX2G_PHASE_TIMING
+__device__ unsigned long long g_phase_cycles[16];
+#define ENC_PHASE_INIT \
+  long long ph_[12] = {};  \
+  long long ph_t = 0;
+#define ENC_PHASE_START \
+  if (threadIdx.x == 0) \
+    ph_t = clock64();
+#define ENC_PHASE(k)                 \
+  if (threadIdx.x == 0)              \
+  {                                  \
+    const long long t_ = clock64();  \
+    ph_[k] += t_ - ph_t;             \
+    ph_t = t_;                       \
+  }
+#define ENC_PHASE_FLUSH            \
+  if (threadIdx.x == 0)            \
+    for (int k = 0; k < 12; ++k)   \
+      atomicAdd(&g_phase_cycles[k], (unsigned long long)ph_[k]);
+#else
+#define ENC_PHASE_INIT
+#define ENC_PHASE_START
+#define ENC_PHASE(k)
+#define ENC_PHASE_FLUSH
+#endif
+
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kMaxPlanes = 64;
 constexpr unsigned kStageBytes = 8192;
 
 struct enc_brick
@@ -42,6 +69,7 @@ struct enc_brick
 struct enc_args
 {
   int level, nlevels, is2d, f32_exp, etol, end_bp, nsb, nbricks;
+  int planes;  // plane capacity per block in shared memory (32 or 64)
   uint64_t order;
   const void* field;
   int field_f32;
@@ -63,17 +91,20 @@ struct enc_args
   double* bmax;
 };
 
-// shared memory layout (dynamic)
+// shared memory layout: this struct, then the per-(block, plane) arrays of one subband
+// sized by the number of planes a block can have (32 for float32 data, 64 for float64):
+//   unsigned long long X[kMaxBlocksPerSubband][P]   plane bit masks
+//   uint16_t off[kMaxBlocksPerSubband][P]            plane bit lengths, then bit offsets
+//   uint8_t nin[kMaxBlocksPerSubband][P]             significant coefficients before the plane
 struct enc_smem
 {
-  unsigned long long X[kMaxBlocksPerSubband][kMaxPlanes];  // plane bit masks
-  uint16_t off[kMaxBlocksPerSubband][kMaxPlanes];          // bit offset inside the channel
-  uint8_t nin[kMaxBlocksPerSubband][kMaxPlanes];           // significant coefficients before plane
-  long long q[kWarps][64];                                 // per-warp block scratch
+  long long q[kWarps][2][64];  // per-warp scratch of two blocks
   int16_t emax[kMaxBlocksPerSubband];
   int16_t ktop[kMaxBlocksPerSubband];
   uint8_t np[kMaxBlocksPerSubband];
   uint8_t nvals_log[kMaxBlocksPerSubband];
+  uint8_t perm3[64];
+  uint8_t perm2[16];
   uint32_t key_bits[kKeyWindow];
   uint32_t key_base[kKeyWindow];
   uint32_t stage[kStageBytes / 4];  // one (brick, subband) region being assembled
@@ -84,6 +115,11 @@ struct enc_smem
   unsigned long long region;
   int ok;
 };
+
+inline size_t enc_smem_bytes(int planes)
+{
+  return ((sizeof(enc_smem) + 15) & ~(size_t)15) + (size_t)kMaxBlocksPerSubband * (size_t)planes * (8 + 2 + 1);
+}
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
 {
@@ -136,37 +172,100 @@ __device__ __forceinline__ double warp_max(double v)
   return v;
 }
 
+// Offset in the brick of sample j of a block (block dims are 4 or 1 per axis since the
+// subbands of a 33^3 brick are 17 or 16 wide).
+__device__ __forceinline__ int block_sample(int base, int lx, int ly, int j, int sy, int sz)
+{
+  const int x = j & lx;
+  const int y = (j >> (lx ? 2 : 0)) & ly;
+  const int z = j >> ((lx ? 2 : 0) + (ly ? 2 : 0));
+  return base + 2 * x + sy * y + sz * z;
+}
+
+struct block_info
+{
+  int base, lx, ly, nd;
+};
+
+__device__ __forceinline__ block_info block_at(const uint64_t* geom, int b, const int from[3], int is2d)
+{
+  int d3[3], bd[3];
+  unpack_geom(geom[b], d3, bd);
+  block_info bi;
+  bi.base = (from[2] + (is2d ? 0 : 2 * d3[2])) * 33 * 33 + (from[1] + 2 * d3[1]) * 33 + from[0] + 2 * d3[0];
+  bi.lx = bd[0] > 1 ? 3 : 0;
+  bi.ly = bd[1] > 1 ? 3 : 0;
+  bi.nd = (bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1);
+  return bi;
+}
+
 __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   enc_smem& sm = *reinterpret_cast<enc_smem*>(smem_raw);
+  const int P = a.planes;
+  unsigned long long* const Xp =
+    reinterpret_cast<unsigned long long*>(smem_raw + ((sizeof(enc_smem) + 15) & ~(size_t)15));
+  uint16_t* const OFF = reinterpret_cast<uint16_t*>(Xp + (size_t)kMaxBlocksPerSubband * P);
+  uint8_t* const NIN = reinterpret_cast<uint8_t*>(OFF + (size_t)kMaxBlocksPerSubband * P);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int N[3] = { 33, 33, a.is2d ? 1 : 33 };
   const int NB = N[0] * N[1] * N[2];
+  const int SZ = a.is2d ? 0 : 2 * 33 * 33;  // sample stride along z inside a subband
   double* F = a.slots + (size_t)blockIdx.x * (size_t)NB;
+  if (tid < 64)
+    sm.perm3[tid] = dev::perm(3, tid);
+  if (tid < 16)
+    sm.perm2[tid] = dev::perm(2, tid);
+  ENC_PHASE_INIT
 
   for (int bi = blockIdx.x; bi < a.nbricks; bi += gridDim.x)
   {
     const enc_brick br = a.bricks[bi];
+    ENC_PHASE_START
     // ---------------- A: gather ----------------
     if (a.level == 0)
     {
-      for (int i = tid; i < NB; i += kThreads)
-        F[i] = 0.0;
-      __syncthreads();
-      double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
       const int vx = br.valid[0], vy = br.valid[1], vz = br.valid[2];
-      const int nvalid = vx * vy * vz;
-      for (int i = tid; i < nvalid; i += kThreads)
+      double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
+      const long long gx0 = (long long)br.b3[0] * 32, gy0 = (long long)br.b3[1] * 32,
+                      gz0 = (long long)br.b3[2] * (a.is2d ? 1 : 32);
+      // rows (y, z) of the brick, one warp per row, lanes along x; samples outside the
+      // valid region (and the x = 32 column) are zero
+      const int nrows = 33 * N[2];
+      constexpr int U = 4;
+      for (int r0 = warp * U; r0 < nrows; r0 += kWarps * U)
       {
-        int x = i % vx, y = (i / vx) % vy, z = i / (vx * vy);
-        long long gx = (long long)br.b3[0] * 32 + x, gy = (long long)br.b3[1] * 32 + y,
-                  gz = (long long)br.b3[2] * (a.is2d ? 1 : 32) + z;
-        long long src = (gz * a.fdims[1] + gy) * a.fdims[0] + gx;
-        double v = a.field_f32 ? (double)((const float*)a.field)[src] : ((const double*)a.field)[src];
-        F[(z * 33 + y) * 33 + x] = v;
-        mn = v < mn ? v : mn;
-        mx = mx < v ? v : mx;
+        float fv[U];
+        double dv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+          const int r = r0 + u, y = r % 33, z = r / 33;
+          const bool in = r < nrows && y < vy && z < vz && lane < vx;
+          const long long src = ((gz0 + z) * a.fdims[1] + gy0 + y) * a.fdims[0] + gx0 + lane;
+          if (a.field_f32)
+            fv[u] = in ? __ldcs((const float*)a.field + src) : 0.0f;
+          else
+            dv[u] = in ? __ldcs((const double*)a.field + src) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+          const int r = r0 + u, y = r % 33, z = r / 33;
+          if (r >= nrows)
+            break;
+          const bool in = y < vy && z < vz && lane < vx;
+          const double v = a.field_f32 ? (double)fv[u] : dv[u];
+          F[r * 33 + lane] = v;
+          if (lane == 0)
+            F[r * 33 + 32] = 0.0;
+          if (in)
+          {
+            mn = v < mn ? v : mn;
+            mx = mx < v ? v : mx;
+          }
+        }
       }
       for (int o = 16; o > 0; o >>= 1)
       {
@@ -193,11 +292,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
     }
     else
     {
+      // (bricks are NB = 33^3 doubles, an odd count: only 8-byte alignment is guaranteed)
       const double* src = a.in_bricks + (size_t)bi * (size_t)NB;
       for (int i = tid; i < NB; i += kThreads)
-        F[i] = src[i];
+        F[i] = __ldcs(src + i);
     }
     __syncthreads();
+    ENC_PHASE(0)
 
     // ---------------- B: transform ----------------
     {
@@ -213,6 +314,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         dev::lift_sweep_regs<true>(F, N, sm.stack.g[i], sm.stack.axis[i]);
         __syncthreads();
       }
+      ENC_PHASE(1)
       if (tid == 0)
         dev::build_stack(N, 5, a.order, &sm.stack);
       __syncthreads();
@@ -222,6 +324,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         dev::lift_sweep_regs<false>(F, N, sm.stack.g[i], sm.stack.axis[i]);
         __syncthreads();
       }
+      ENC_PHASE(2)
       // inverse X (D = 33) then forward X of the one-level transform (Core/Wavelet.cpp:81)
       for (int li = tid; li < 33 * N[2]; li += kThreads)
       {
@@ -237,6 +340,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
           row[k] = v[k];
       }
       __syncthreads();
+      ENC_PHASE(3)
       // forward Y, and forward Z; subband normalisation applied as the last sweep stores
       // (Core/Wavelet.cpp:111-137)
       for (int li = tid; li < 33 * N[2]; li += kThreads)
@@ -261,6 +365,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         }
       }
       __syncthreads();
+      ENC_PHASE(4)
       if (!a.is2d)
       {
         for (int li = tid; li < 33 * 33; li += kThreads)
@@ -282,6 +387,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         __syncthreads();
       }
     }
+    ENC_PHASE(5)
 
     // ---------------- C: low band to the parent ----------------
     if (a.parent_bricks && br.parent >= 0)
@@ -292,10 +398,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
       {
         int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
         int cz = a.is2d ? 0 : 2 * z;
-        P[((br.pos[2] * nz + z) * 33 + (br.pos[1] * 16 + y)) * 33 + (br.pos[0] * 16 + x)] =
-          F[(cz * 33 + 2 * y) * 33 + 2 * x];
+        __stcs(P + ((br.pos[2] * nz + z) * 33 + (br.pos[1] * 16 + y)) * 33 + (br.pos[0] * 16 + x),
+               F[(cz * 33 + 2 * y) * 33 + 2 * x]);
       }
     }
+    ENC_PHASE(6)
 
     // ---------------- D: block coding per subband ----------------
     for (int s = 0; s < a.nsb; ++s)
@@ -306,149 +413,313 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
       const uint64_t* geom = a.geom + (size_t)s * kMaxBlocksPerSubband;
       const size_t bs = (size_t)bi * (size_t)a.nsb + (size_t)s;
 
-      // D1: warp per block
-      for (int b = warp; b < nb; b += kWarps)
+      // D1: a warp codes two blocks (lanes own samples j and j + 32 of each): exponent,
+      // quantisation, zfp transform, shuffle, bit-plane masks by ballot; then the
+      // significance chain and the plane lengths, lane-parallel over the planes.
+      // The samples of the warp's next pair are loaded while the current pair is coded.
+      const int npairs = (nb + 1) >> 1;
+      double cv[4];
+      block_info cA, cB;
+      auto load_pair = [&](int pr, double v[4], block_info& A, block_info& B) {
+        const int b0 = 2 * pr, b1 = 2 * pr + 1;
+        A = block_at(geom, b0, from, a.is2d);
+        const bool hb = b1 < nb;
+        B = hb ? block_at(geom, b1, from, a.is2d) : A;
+        const int nvA = 1 << (2 * A.nd), nvB = hb ? 1 << (2 * B.nd) : 0;
+        v[0] = lane < nvA ? F[block_sample(A.base, A.lx, A.ly, lane, 66, SZ)] : 0.0;
+        v[1] = lane + 32 < nvA ? F[block_sample(A.base, A.lx, A.ly, lane + 32, 66, SZ)] : 0.0;
+        v[2] = lane < nvB ? F[block_sample(B.base, B.lx, B.ly, lane, 66, SZ)] : 0.0;
+        v[3] = lane + 32 < nvB ? F[block_sample(B.base, B.lx, B.ly, lane + 32, 66, SZ)] : 0.0;
+      };
+      if (warp < npairs)
+        load_pair(warp, cv, cA, cB);
+      for (int pr = warp; pr < npairs; pr += kWarps)
       {
-        int d3[3], bd[3];
-        unpack_geom(geom[b], d3, bd);
-        const int nd = (bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1);
-        const int nv = 1 << (2 * nd);
-        const int prec = 63 - nd;
-        long long* q = sm.q[warp];
-        double v0 = 0, v1 = 0;
-        int j0 = lane, j1 = lane + 32;
-        if (j0 < nv)
+        double nv_[4] = { 0, 0, 0, 0 };
+        block_info nA = cA, nB = cB;
+        if (pr + kWarps < npairs)
+          load_pair(pr + kWarps, nv_, nA, nB);
+        const int bA = 2 * pr, bB = 2 * pr + 1;
+        const bool hasB = bB < nb;
+        const int ndA = cA.nd, ndB = hasB ? cB.nd : 0;
+        const int nvA = 1 << (2 * ndA), nvB = hasB ? 1 << (2 * ndB) : 0;
+        // block maxima
+        double mA = fabs(cv[0]), mB = fabs(cv[2]);
         {
-          int x = j0 % bd[0], y = (j0 / bd[0]) % bd[1], z = j0 / (bd[0] * bd[1]);
-          v0 = F[((from[2] + (d3[2] + z) * strd[2]) * 33 + (from[1] + (d3[1] + y) * strd[1])) * 33 +
-                 (from[0] + (d3[0] + x) * strd[0])];
+          const double m1 = fabs(cv[1]), m3 = fabs(cv[3]);
+          mA = mA < m1 ? m1 : mA;
+          mB = mB < m3 ? m3 : mB;
         }
-        if (j1 < nv)
+        mA = warp_max(mA);
+        mB = warp_max(mB);
+        const int eA = a.f32_exp ? dev::exponent_f32(__double2float_rn(mA)) : dev::exponent_f64(mA);
+        const int eB = a.f32_exp ? dev::exponent_f32(__double2float_rn(mB)) : dev::exponent_f64(mB);
+        const double sA = dev::pow2(63 - ndA - 1 - eA), sB = dev::pow2(63 - ndB - 1 - eB);
+        long long* qA = sm.q[warp][0];
+        long long* qB = sm.q[warp][1];
+        if (lane < nvA)
+          qA[lane] = dev::trunc_i64(__dmul_rn(sA, cv[0]));
+        if (lane + 32 < nvA)
+          qA[lane + 32] = dev::trunc_i64(__dmul_rn(sA, cv[1]));
+        if (lane < nvB)
+          qB[lane] = dev::trunc_i64(__dmul_rn(sB, cv[2]));
+        if (lane + 32 < nvB)
+          qB[lane + 32] = dev::trunc_i64(__dmul_rn(sB, cv[3]));
+        __syncwarp();
+        // zfp transform (Core/Zfp.h:262): the 16 lines of a pass of block A on lanes 0-15,
+        // of block B on lanes 16-31
         {
-          int x = j1 % bd[0], y = (j1 / bd[0]) % bd[1], z = j1 / (bd[0] * bd[1]);
-          v1 = F[((from[2] + (d3[2] + z) * strd[2]) * 33 + (from[1] + (d3[1] + y) * strd[1])) * 33 +
-                 (from[0] + (d3[0] + x) * strd[0])];
+          // (the halves share no data: each synchronises on its own 16 lanes)
+          const int h = lane >> 4, l = lane & 15;
+          const unsigned hm = h ? 0xffff0000u : 0x0000ffffu;
+          long long* q = h ? qB : qA;
+          const int nd = h ? ndB : ndA;
+          if (nd == 3)
+          {
+            dev::fwd_lift4(q + 4 * (l & 3) + 16 * (l >> 2), 1);
+            __syncwarp(hm);
+            dev::fwd_lift4(q + 16 * (l & 3) + (l >> 2), 4);
+            __syncwarp(hm);
+            dev::fwd_lift4(q + (l & 3) + 4 * (l >> 2), 16);
+          }
+          else if (nd == 2)
+          {
+            if (l < 4)
+              dev::fwd_lift4(q + 4 * l, 1);
+            __syncwarp(hm);
+            if (l < 4)
+              dev::fwd_lift4(q + l, 4);
+          }
+          else if (nd == 1)
+          {
+            if (l == 0)
+              dev::fwd_lift4(q, 1);
+          }
+          __syncwarp();
         }
-        double m = fabs(v0);
-        double m1 = fabs(v1);
-        m = m < m1 ? m1 : m;
-        m = warp_max(m);
-        const int emax = a.f32_exp ? dev::exponent_f32(__double2float_rn(m)) : dev::exponent_f64(m);
-        const double scale = dev::pow2(prec - 1 - emax);
-        if (j0 < nv)
-          q[j0] = dev::trunc_i64(__dmul_rn(scale, v0));
-        if (j1 < nv)
-          q[j1] = dev::trunc_i64(__dmul_rn(scale, v1));
+        // shuffle to sequency order, negabinary (Core/Zfp.h:419-520)
+        auto permj = [&](int nd, int j) -> int {
+          return nd == 3 ? (int)sm.perm3[j] : (nd == 2 ? (int)sm.perm2[j & 15] : j);
+        };
+        unsigned long long uA0 = 0, uA1 = 0, uB0 = 0, uB1 = 0;
+        if (lane < nvA)
+          uA0 = ((unsigned long long)qA[permj(ndA, lane)] + dev::kNegaMask) ^ dev::kNegaMask;
+        if (lane + 32 < nvA)
+          uA1 = ((unsigned long long)qA[permj(ndA, lane + 32)] + dev::kNegaMask) ^ dev::kNegaMask;
+        if (lane < nvB)
+          uB0 = ((unsigned long long)qB[permj(ndB, lane)] + dev::kNegaMask) ^ dev::kNegaMask;
+        if (lane + 32 < nvB)
+          uB1 = ((unsigned long long)qB[permj(ndB, lane + 32)] + dev::kNegaMask) ^ dev::kNegaMask;
         __syncwarp();
-        dev::warp_fwd_zfp(q, nd, lane);
-        unsigned long long u0 = 0, u1 = 0;
-        if (j0 < nv)
-          u0 = ((unsigned long long)q[dev::perm(nd, j0)] + dev::kNegaMask) ^ dev::kNegaMask;
-        if (j1 < nv)
-          u1 = ((unsigned long long)q[dev::perm(nd, j1)] + dev::kNegaMask) ^ dev::kNegaMask;
-        __syncwarp();
-        const int np = dev::coded_planes(emax, a.etol, a.end_bp);
-        for (int k = 0; k < np; ++k)
+        const int npA = dev::coded_planes(eA, a.etol, a.end_bp);
+        const int npB = hasB ? dev::coded_planes(eB, a.etol, a.end_bp) : 0;
+        const int npM = npA > npB ? npA : npB;
+        unsigned long long* XA = Xp + (size_t)bA * P;
+        unsigned long long* XB = Xp + (size_t)bB * P;
+        for (int k = 0; k < npM; ++k)
         {
           const int bit = 63 - k;
-          unsigned lo = __ballot_sync(0xffffffffu, (u0 >> bit) & 1ull);
-          unsigned hi = __ballot_sync(0xffffffffu, (u1 >> bit) & 1ull);
-          if (lane == 0)
-            sm.X[b][k] = (unsigned long long)lo | ((unsigned long long)hi << 32);
+          const unsigned a0 = __ballot_sync(0xffffffffu, (uA0 >> bit) & 1ull);
+          const unsigned a1 = __ballot_sync(0xffffffffu, (uA1 >> bit) & 1ull);
+          const unsigned b0 = __ballot_sync(0xffffffffu, (uB0 >> bit) & 1ull);
+          const unsigned b1 = __ballot_sync(0xffffffffu, (uB1 >> bit) & 1ull);
+          if (lane == 0 && k < npA)
+            XA[k] = (unsigned long long)a0 | ((unsigned long long)a1 << 32);
+          if (lane == 1 && k < npB)
+            XB[k] = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
         }
         if (lane == 0)
         {
-          sm.emax[b] = (int16_t)emax;
-          sm.ktop[b] = (int16_t)(emax + 63 + 1024);
-          sm.np[b] = (uint8_t)np;
-          sm.nvals_log[b] = (uint8_t)(2 * nd);
+          sm.emax[bA] = (int16_t)eA;
+          sm.ktop[bA] = (int16_t)(eA + 63 + 1024);
+          sm.np[bA] = (uint8_t)npA;
+          sm.nvals_log[bA] = (uint8_t)(2 * ndA);
         }
+        if (lane == 1 && hasB)
+        {
+          sm.emax[bB] = (int16_t)eB;
+          sm.ktop[bB] = (int16_t)(eB + 63 + 1024);
+          sm.np[bB] = (uint8_t)npB;
+          sm.nvals_log[bB] = (uint8_t)(2 * ndB);
+        }
+        __syncwarp();
+        // significance chain: nin(k) = max over planes k' < k of the highest one-bit + 1
+        // (Core/Zfp.h:771), an exclusive prefix maximum over the planes; plane lengths
+        {
+          int carryA = 0, carryB = 0;
+          for (int k0 = 0; k0 < npM; k0 += 32)
+          {
+            const int k = k0 + lane;
+            const unsigned long long xa = k < npA ? XA[k] : 0ull;
+            const unsigned long long xb = k < npB ? XB[k] : 0ull;
+            int ma = xa ? 64 - __clzll(xa) : 0, mb = xb ? 64 - __clzll(xb) : 0;
+            int ia = ma, ib = mb;  // inclusive prefix max
+            for (int o = 1; o < 32; o <<= 1)
+            {
+              const int ta = __shfl_up_sync(0xffffffffu, ia, o), tb = __shfl_up_sync(0xffffffffu, ib, o);
+              if (lane >= o)
+              {
+                ia = ia > ta ? ia : ta;
+                ib = ib > tb ? ib : tb;
+              }
+            }
+            int ea = __shfl_up_sync(0xffffffffu, ia, 1), eb = __shfl_up_sync(0xffffffffu, ib, 1);
+            ea = lane ? ea : 0;
+            eb = lane ? eb : 0;
+            const int nA_ = ea > carryA ? ea : carryA, nB_ = eb > carryB ? eb : carryB;
+            if (k < npA)
+            {
+              NIN[(size_t)bA * P + k] = (uint8_t)nA_;
+              OFF[(size_t)bA * P + k] = (uint16_t)dev::plane_bits(xa, nA_, nvA);
+            }
+            if (k < npB)
+            {
+              NIN[(size_t)bB * P + k] = (uint8_t)nB_;
+              OFF[(size_t)bB * P + k] = (uint16_t)dev::plane_bits(xb, nB_, nvB);
+            }
+            const int ta = __shfl_sync(0xffffffffu, ia, 31), tb = __shfl_sync(0xffffffffu, ib, 31);
+            carryA = carryA > ta ? carryA : ta;
+            carryB = carryB > tb ? carryB : tb;
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          cv[i] = nv_[i];
+        cA = nA;
+        cB = nB;
       }
       __syncthreads();
+      ENC_PHASE(7)
 
-      // D2: significance chain per block
-      for (int b = tid; b < nb; b += kThreads)
+      // key range of the subband
+      if (warp == 0)
       {
-        int n = 0;
-        const int np = sm.np[b];
-        for (int k = 0; k < np; ++k)
+        int lo = 1 << 30, hi = -(1 << 30);
+        for (int b = lane; b < nb; b += 32)
         {
-          sm.nin[b][k] = (uint8_t)n;
-          n = dev::plane_nout(sm.X[b][k], n);
-        }
-      }
-      if (tid == 0)
-      {
-        int kmin = 1 << 30, kmax = -(1 << 30);
-        for (int b = 0; b < nb; ++b)
-        {
-          if (!sm.np[b])
+          const int n = sm.np[b];
+          if (!n)
             continue;
-          int lo = sm.ktop[b] - sm.np[b] + 1, hi = sm.ktop[b];
-          kmin = lo < kmin ? lo : kmin;
-          kmax = hi > kmax ? hi : kmax;
+          const int t = sm.ktop[b];
+          lo = t - n + 1 < lo ? t - n + 1 : lo;
+          hi = t > hi ? t : hi;
         }
-        if (kmax < kmin)
+        for (int o = 16; o > 0; o >>= 1)
         {
-          kmin = 1;
-          kmax = 0;
+          const int l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+          lo = l2 < lo ? l2 : lo;
+          hi = h2 > hi ? h2 : hi;
         }
-        sm.kmin = kmin;
-        sm.kmax = kmax;
-        sm.ok = (kmax - kmin + 1) <= kKeyWindow;
-        if (!sm.ok)
-          atomicExch(a.error, 1);
+        if (lane == 0)
+        {
+          if (hi < lo)
+          {
+            lo = 1;
+            hi = 0;
+          }
+          sm.kmin = lo;
+          sm.kmax = hi;
+          sm.ok = (hi - lo + 1) <= kKeyWindow;
+          if (!sm.ok)
+            atomicExch(a.error, 1);
+        }
       }
       __syncthreads();
       const int kmin = sm.kmin, kmax = sm.kmax;
       const int nkeys = sm.ok ? kmax - kmin + 1 : 0;
+      ENC_PHASE(8)
 
-      // D3: per channel key, bit offsets of the blocks in Morton order
-      for (int t = tid; t < nkeys; t += kThreads)
+      // D3: per channel key (a warp each), bit offsets of the blocks in Morton order: an
+      // exclusive scan of the plane lengths, in place
+      for (int t = warp; t < nkeys; t += kWarps)
       {
         const int key = kmin + t;
-        unsigned acc = 0;
-        for (int b = 0; b < nb; ++b)
+        uint32_t v[4];
+        int kk[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
         {
-          const int kk = sm.ktop[b] - key;
-          if (kk < 0 || kk >= sm.np[b])
-            continue;
-          sm.off[b][kk] = (uint16_t)acc;
-          acc += (unsigned)dev::plane_bits(sm.X[b][kk], sm.nin[b][kk], 1 << sm.nvals_log[b]);
+          const int b = lane * 4 + i;
+          kk[i] = b < nb ? sm.ktop[b] - key : -1;
+          const bool in = kk[i] >= 0 && b < nb && kk[i] < sm.np[b];
+          kk[i] = in ? kk[i] : -1;
+          v[i] = in ? OFF[(size_t)b * P + kk[i]] : 0u;
         }
-        sm.key_bits[t] = acc;
+        const uint32_t tot = v[0] + v[1] + v[2] + v[3];
+        uint32_t inc = tot;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o)
+            inc += y;
+        }
+        uint32_t acc = inc - tot;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+          if (kk[i] >= 0)
+            OFF[(size_t)(lane * 4 + i) * P + kk[i]] = (uint16_t)acc;
+          acc += v[i];
+        }
+        if (lane == 31)
+          sm.key_bits[t] = inc;
       }
       __syncthreads();
+      ENC_PHASE(9)
 
       // D4: channel byte bases and the region of this (brick, subband)
       // (regions are whole 32-bit words so every CTA owns the words it writes)
-      if (tid == 0)
+      if (warp == 0)
       {
-        unsigned base = 0;
-        for (int t = 0; t < nkeys; ++t)
+        uint32_t v[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
         {
-          sm.key_base[t] = base;
-          base += (sm.key_bits[t] + 7) / 8;
+          const int t = lane * 4 + i;
+          v[i] = t < nkeys ? (sm.key_bits[t] + 7u) / 8u : 0u;
         }
-        // region: header (kmin, nkeys), exponents, channel sizes, channel streams
-        const unsigned hdr = 8u + ((2u * (unsigned)nb + 3u) & ~3u) + 4u * (unsigned)nkeys;
-        const unsigned alloc = hdr + ((base + 3u) & ~3u);
-        unsigned long long region = atomicAdd(a.cursor, (unsigned long long)alloc);
-        if (region + alloc > a.cap_bytes)
-          atomicExch(a.error, 2);
-        sm.region = region;
-        sm.alloc = alloc;
-        sm.hdr = hdr;
-        a.offset[bs] = region;
+        const uint32_t tot = v[0] + v[1] + v[2] + v[3];
+        uint32_t inc = tot;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o)
+            inc += y;
+        }
+        uint32_t acc = inc - tot;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+          const int t = lane * 4 + i;
+          if (t < nkeys)
+            sm.key_base[t] = acc;
+          acc += v[i];
+        }
+        const uint32_t base = __shfl_sync(0xffffffffu, inc, 31);
+        if (lane == 0)
+        {
+          // region: header (kmin, nkeys), exponents, channel sizes, channel streams
+          const unsigned hdr = 8u + ((2u * (unsigned)nb + 3u) & ~3u) + 4u * (unsigned)nkeys;
+          const unsigned alloc = hdr + ((base + 3u) & ~3u);
+          unsigned long long region = atomicAdd(a.cursor, (unsigned long long)alloc);
+          if (region + alloc > a.cap_bytes)
+            atomicExch(a.error, 2);
+          sm.region = region;
+          sm.alloc = alloc;
+          sm.hdr = hdr;
+          a.offset[bs] = region;
+        }
       }
       __syncthreads();
       const unsigned long long region = sm.region;
       const unsigned alloc = sm.alloc;
       const unsigned hdr = sm.hdr;
       const bool fits = region + alloc <= a.cap_bytes;
+      ENC_PHASE(10)
 
-      // D5: scatter the plane bits, into shared memory when the region is small enough, else
-      // straight into the (zeroed) global region; then the region is stored with plain writes
+      // D5: the plane codes, built in registers and ORed into shared memory when the region
+      // is small enough, else straight into the (zeroed) global region; then the region is
+      // stored with plain writes
       if (fits && alloc)
       {
         const bool staged = alloc <= kStageBytes;
@@ -467,27 +738,32 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         uint32_t* sw = words + 2 + ((2u * (unsigned)nb + 3u) >> 2);
         for (int t = tid; t < nkeys; t += kThreads)
           sw[t] = (sm.key_bits[t] + 7) / 8;
-        for (int idx = tid; idx < nb * kMaxPlanes; idx += kThreads)
+        const int lp = P == 64 ? 6 : 5;
+        for (int idx = tid; idx < nb * P; idx += kThreads)
         {
-          const int b = idx >> 6, kk = idx & 63;
+          const int b = idx >> lp, kk = idx & (P - 1);
           if (kk >= sm.np[b])
             continue;
           const int t = sm.ktop[b] - kk - kmin;
           const unsigned long long pos =
-            ((unsigned long long)hdr + sm.key_base[t]) * 8ull + (unsigned long long)sm.off[b][kk];
-          dev::write_plane(words, pos, sm.X[b][kk], sm.nin[b][kk], 1 << sm.nvals_log[b]);
+            ((unsigned long long)hdr + sm.key_base[t]) * 8ull + (unsigned long long)OFF[idx];
+          dev::bits192 c;
+          const int len = dev::plane_code(Xp[idx], NIN[idx], 1 << sm.nvals_log[b], &c);
+          dev::or_code(words, pos, c, len);
         }
         __syncthreads();
         if (staged)
         {
           uint32_t* dst = a.stream + region / 4;
           for (unsigned i = tid; i < alloc / 4; i += kThreads)
-            dst[i] = sm.stage[i];
+            __stcs(dst + i, sm.stage[i]);
         }
       }
       __syncthreads();
+      ENC_PHASE(11)
     }
   }
+  ENC_PHASE_FLUSH
 }
 
 // Host-side weights of one level (Core/Wavelet.cpp:111-137, Core/Wavelet.h:19).
@@ -578,6 +854,7 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
   a.f32_exp = f_.type == dtype::float32;
   a.etol = exponent_f64(f_.tolerance);
   a.end_bp = f_.type == dtype::float32 ? 32 : 64;
+  a.planes = a.end_bp;
   a.nsb = nsb;
   a.nbricks = nbr;
   a.order = f_.transform_order;
@@ -638,7 +915,7 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     a.error = (int*)(d_misc + 1);
     a.bmin = d_bmin;
     a.bmax = d_bmax;
-    const size_t smem = sizeof(enc_smem);
+    const size_t smem = enc_smem_bytes(a.planes);
     cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaEventRecord(ctx_->ev0, st);
     k_encode_level<<<grid, kThreads, smem, st>>>(a);
@@ -709,6 +986,16 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
   }
   return DeviceStreamOverflow;
 }
+
+#ifdef IDX2G_PHASE_TIMING
+// Profiling builds: read and clear the per-phase cycle counters of the encode kernel.
+extern "C" __attribute__((visibility("default"))) void idx2g_debug_phase_cycles(unsigned long long* out)
+{
+  cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(g_phase_cycles));
+  unsigned long long z[16] = {};
+  cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
+}
+#endif
 
 void gpu_coder::value_range(double* vmin, double* vmax)
 {
