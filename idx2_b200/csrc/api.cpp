@@ -185,13 +185,14 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
   const size_t bytes = (size_t)prod(p.dims) * (f32 ? 4 : 8);
   auto t0 = std::chrono::steady_clock::now();
   const void* d_field = field;
-  void* owned = nullptr;
   if (!field_on_device)
   {
-    if (cudaMalloc(&owned, bytes) != cudaSuccess)
+    // the field goes to a device buffer of the context's workspace (kept across calls)
+    void* staged = c->d.ws("enc.field", bytes);
+    if (!staged)
       return OutOfMemory;
-    cudaMemcpyAsync(owned, field, bytes, cudaMemcpyHostToDevice, c->d.stream);
-    d_field = owned;
+    cudaMemcpyAsync(staged, field, bytes, cudaMemcpyHostToDevice, c->d.stream);
+    d_field = staged;
   }
   encode_timing tm;
   long long stream_bytes = 0, exp_bytes = 0;
@@ -209,8 +210,6 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
     lms = coder.level_ms();
     lbytes = coder.level_bytes();
   }
-  if (owned)
-    cudaFree(owned);
   if (e)
     return e;
   auto t1 = std::chrono::steady_clock::now();

@@ -459,6 +459,10 @@ static int finalize_common(dataset_format* f, params* p)
       int inc = std::min(len - acc, log2_ceil(f->files_per_dir));
       dd.push_back(inc);
       acc += inc;
+      // the depth is limited to 4 (idx2_file::MaxSpatialDepth); with one file per directory
+      // (inc = 0) the reference's loop never ends, here it is the same error
+      if (dd.size() > 4)
+        return TooManyFilesPerDir;
     }
     if (dd.size() > 4)
       return TooManyFilesPerDir;

@@ -275,191 +275,146 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
 
 namespace
 {
-constexpr int kKeySpace = 4096;  // bit-plane keys are 12-bit (Core/idx2Lookup.h:21)
-inline size_t chan_slot(int level, int subband, int bpkey)
+
+constexpr uint64_t kFinalFlush = ~0ull;  // stamp of the writes of the final flushes
+
+template <typename F>
+void run_parallel(size_t n, F&& fn)
 {
-  return ((size_t)(level & 15) * 64 + (size_t)(subband & 63)) * kKeySpace + (size_t)(bpkey & (kKeySpace - 1));
+  unsigned nt = std::thread::hardware_concurrency();
+  nt = nt ? (nt > 32 ? 32 : nt) : 4;
+  if (nt > n)
+    nt = (unsigned)(n ? n : 1);
+  std::atomic<size_t> next{ 0 };
+  auto work = [&]() {
+    for (size_t i; (i = next.fetch_add(1)) < n;)
+      fn(i);
+  };
+  std::vector<std::thread> th;
+  for (unsigned t = 1; t < nt; ++t)
+    th.emplace_back(work);
+  work();
+  for (auto& t : th)
+    t.join();
 }
+
+struct channel
+{
+  bit_writer deltas, sizes;
+  std::vector<segment> bricks;
+  size_t brick_bytes = 0;
+  u64 last_chunk = 0, last_brick = 0;
+  int nbricks = 0;
+  int bpkey = 0;
+};
+
+struct chunk_rec
+{
+  uint64_t event;
+  uint32_t rank;
+  int bpkey;
+  u64 last_brick;
+  std::vector<segment> parts;  // header (owned by the group), then brick data
+  size_t bytes;
+  double deltas_bytes, sizes_bytes;
+};
+
+struct exp_rec
+{
+  uint64_t event;
+  uint32_t rank;
+  u64 last_brick;
+  std::vector<uint8_t> raw, z;
+};
+
+template <typename T>
+bool stamp_less(const T* a, const T* b)
+{
+  return a->event != b->event ? a->event < b->event : a->rank < b->rank;
+}
+
 } // namespace
+
+struct packer::group
+{
+  int level = 0, subband = 0;
+  std::vector<uint32_t> events;  // indices into packer::events_, in order
+  std::vector<int32_t> index;    // bpkey -> channel, -1
+  std::deque<channel> chans;
+  std::vector<uint8_t> brick_exps;
+  u64 exp_last_chunk = 0, exp_last_brick = 0;
+  std::deque<std::vector<uint8_t>> owned;
+  std::vector<chunk_rec> chunks;
+  std::vector<exp_rec> exps;
+
+  channel& chan(int bpkey)
+  {
+    int32_t& i = index[(size_t)bpkey];
+    if (i < 0)
+    {
+      i = (int32_t)chans.size();
+      chans.emplace_back();
+      chans.back().bpkey = bpkey;
+    }
+    return chans[(size_t)i];
+  }
+
+  // Core/idx2Write.cpp:221 WriteChunk: varbyte NBricks | deltas | sizes | brick data
+  void write_chunk(channel& c, uint64_t event, uint32_t rank)
+  {
+    bit_writer head;
+    head.put_varbyte((uint64_t)c.nbricks);
+    owned.emplace_back();
+    std::vector<uint8_t>& meta = owned.back();
+    meta.reserve(head.size() + c.deltas.size() + c.sizes.size());
+    meta.insert(meta.end(), head.bytes.begin(), head.bytes.begin() + (long)head.size());
+    meta.insert(meta.end(), c.deltas.bytes.begin(), c.deltas.bytes.begin() + (long)c.deltas.size());
+    meta.insert(meta.end(), c.sizes.bytes.begin(), c.sizes.bytes.begin() + (long)c.sizes.size());
+    chunk_rec r;
+    r.event = event;
+    r.rank = rank;
+    r.bpkey = c.bpkey;
+    r.last_brick = c.last_brick;
+    r.bytes = meta.size() + c.brick_bytes;
+    r.deltas_bytes = (double)c.deltas.size();
+    r.sizes_bytes = (double)c.sizes.size();
+    r.parts.reserve(c.bricks.size() + 1);
+    if (!meta.empty())
+      r.parts.push_back({ meta.data(), meta.size() });
+    for (const segment& sg : c.bricks)
+      r.parts.push_back(sg);
+    chunks.push_back(std::move(r));
+    c.deltas.clear();
+    c.sizes.clear();
+    c.bricks.clear();
+    c.brick_bytes = 0;
+  }
+
+  // Core/idx2Write.cpp:38 WriteChunkExponents (compression deferred)
+  void write_exps(uint64_t event, uint32_t rank)
+  {
+    exp_rec r;
+    r.event = event;
+    r.rank = rank;
+    r.last_brick = exp_last_brick;
+    r.raw.swap(brick_exps);
+    brick_exps.clear();
+    exps.push_back(std::move(r));
+  }
+};
 
 packer::packer(const dataset_format& f, double tolerance) : f_(f), tol_(tolerance)
 {
   etol_ = exponent_f64(tolerance);
-  chan_index_.assign((size_t)16 * 64 * kKeySpace, -1);
 }
 
 packer::~packer() = default;
 
-packer::channel* packer::find_chan(int level, int subband, int bpkey)
-{
-  int32_t i = chan_index_[chan_slot(level, subband, bpkey)];
-  return i < 0 ? nullptr : &channels_[(size_t)i];
-}
-
-packer::channel& packer::chan(int level, int subband, int bpkey)
-{
-  int32_t& i = chan_index_[chan_slot(level, subband, bpkey)];
-  if (i < 0)
-  {
-    i = (int32_t)channels_.size();
-    channels_.emplace_back();
-    channels_.back().key = channel_key(bpkey, level, subband);
-  }
-  return channels_[(size_t)i];
-}
-
-void packer::first_touch_order(const subband_result& r, std::vector<int>* keys) const
-{
-  // order in which EncodeSubbandBlocks first meets each channel: blocks in Morton order,
-  // planes from the top down (Core/idx2Encode.cpp:157-249)
-  keys->clear();
-  if (r.kmin > r.kmax)
-    return;
-  std::vector<char> seen((size_t)(r.kmax - r.kmin + 1), 0);
-  const int end_bp = f_.type == dtype::float32 ? 32 : 64;
-  const int bpc = f_.bit_planes_per_chunk;
-  for (int b = 0; b < r.nexps; ++b)
-  {
-    int emax = r.exps[b];
-    for (int bp = 63; bp >= 64 - end_bp; --bp)
-    {
-      if (!plane_coded(bp, emax, etol_, bpc))
-        break;
-      int key = (bp + emax + 1024) / bpc;
-      if (key < r.kmin || key > r.kmax)
-        continue;
-      char& s = seen[(size_t)(key - r.kmin)];
-      if (!s)
-      {
-        s = 1;
-        keys->push_back(key);
-      }
-    }
-  }
-}
-
-void packer::write_chunk(channel& c, int level, int subband, int bpkey)
-{
-  // Core/idx2Write.cpp:221 WriteChunk: varbyte NBricks | deltas | sizes | brick data
-  stats_.brick_deltas.add((double)c.deltas.size());
-  stats_.brick_sizes.add((double)c.sizes.size());
-  bit_writer head;
-  head.put_varbyte((uint64_t)c.nbricks);
-  std::vector<uint8_t> meta;
-  meta.reserve(head.size() + c.deltas.size() + c.sizes.size());
-  meta.insert(meta.end(), head.bytes.begin(), head.bytes.begin() + (long)head.size());
-  meta.insert(meta.end(), c.deltas.bytes.begin(), c.deltas.bytes.begin() + (long)c.deltas.size());
-  meta.insert(meta.end(), c.sizes.bytes.begin(), c.sizes.bytes.begin() + (long)c.sizes.size());
-  const size_t chunk_bytes = meta.size() + c.brick_bytes;
-  file_buffer& fb = files_[file_path(f_, c.last_brick, level)];
-  fb.append_owned(std::move(meta));
-  for (const segment& s : c.bricks)
-    fb.append_ref(s.p, s.n);
-  stats_.bit_plane_chunks.add((double)chunk_bytes);
-  fb.has_chunks = true;
-  fb.chunk_sizes.put_varbyte(chunk_bytes);
-  fb.chunk_addrs.push_back(chunk_address(f_, c.last_brick, level, subband, bpkey));
-  c.deltas.clear();
-  c.sizes.clear();
-  c.bricks.clear();
-  c.brick_bytes = 0;
-}
-
-void packer::write_chunk_exps(sub_channel& s, int level, int subband)
-{
-  // Core/idx2Write.cpp:38 WriteChunkExponents (compression deferred to finish)
-  stats_.exp_chunks_raw.add((double)s.brick_exps.size());
-  exp_chunks_.emplace_back();
-  exp_chunks_.back().raw.swap(s.brick_exps);
-  s.brick_exps.clear();
-  file_buffer& fb = files_[file_path(f_, s.last_brick, level)];
-  fb.has_exps = true;
-  fb.exp_chunks.push_back((int)exp_chunks_.size() - 1);
-  fb.exp_addrs.push_back(chunk_address(f_, s.last_brick, level, subband, 0));
-}
-
 int packer::add(const subband_result& r)
 {
-  const int L = r.level, S = r.subband;
-  const u64 brick = r.brick;
-  const u64 bpc_bricks = (u64)f_.bricks_per_chunk[L];
-  const int shift = log2_ceil(f_.bricks_per_chunk[L]);
-
-  // pass 1: channels in first-touch order; a channel entering a new chunk flushes the
-  // previous one (Core/idx2Encode.cpp:233-249)
-  bool any_new = false;
-  for (int k = r.kmin; k <= r.kmax && !any_new; ++k)
-  {
-    if (!r.sizes[k - r.kmin])
-      continue;
-    channel* c = find_chan(L, S, k);
-    u64 last_chunk = c ? c->last_chunk : 0;
-    any_new = brick >= (last_chunk + 1) * bpc_bricks;
-  }
-  if (any_new)
-  {
-    std::vector<int> order;
-    first_touch_order(r, &order);
-    for (int k : order)
-    {
-      channel& c = chan(L, S, k);
-      if (brick >= (c.last_chunk + 1) * bpc_bricks)
-      {
-        if (c.brick_bytes)
-          write_chunk(c, L, S, k);
-        c.nbricks = 0;
-        c.last_chunk = brick >> shift;
-      }
-    }
-  }
-
-  // exponents (Core/idx2Encode.cpp:41 EncodeBrickSubbandExponents)
-  {
-    sub_channel& sc = subs_[{ L, S }];
-    if (brick >= (sc.last_chunk + 1) * bpc_bricks)
-    {
-      write_chunk_exps(sc, L, S);
-      sc.last_chunk = brick >> shift;
-    }
-    const size_t at = sc.brick_exps.size();
-    if (f_.type == dtype::float64)
-    {
-      sc.brick_exps.resize(at + 2 * (size_t)r.nexps);
-      for (int i = 0; i < r.nexps; ++i)
-      {
-        uint16_t v = (uint16_t)(r.exps[i] + 1023);
-        sc.brick_exps[at + 2 * (size_t)i] = (uint8_t)(v & 0xFF);
-        sc.brick_exps[at + 2 * (size_t)i + 1] = (uint8_t)(v >> 8);
-      }
-    }
-    else
-    {
-      sc.brick_exps.resize(at + (size_t)r.nexps);
-      for (int i = 0; i < r.nexps; ++i)
-        sc.brick_exps[at + (size_t)i] = (uint8_t)(r.exps[i] + 127);
-    }
-    sc.last_brick = brick;
-  }
-
-  // pass 2: brick metadata and data per channel (Core/idx2Encode.cpp:84)
-  size_t off = 0;
-  for (int k = r.kmin; k <= r.kmax; ++k)
-  {
-    const uint32_t nb = r.sizes[k - r.kmin];
-    if (!nb)
-      continue;
-    channel& c = chan(L, S, k);
-    if (c.nbricks == 0)
-      c.deltas.put_varbyte(brick);
-    else
-      c.deltas.put_unary(brick - c.last_brick - 1);
-    c.sizes.put_varbyte(nb);
-    c.bricks.push_back({ r.bytes + off, nb });
-    c.brick_bytes += nb;
-    off += nb;
-    ++c.nbricks;
-    c.last_brick = brick;
-  }
+  if (r.level < 0 || r.level >= 16 || r.subband < 0 || r.subband >= 64)
+    return InvalidArgument;
+  events_.push_back(r);
   return NoError;
 }
 
@@ -472,19 +427,227 @@ static void put_i32(std::vector<uint8_t>* v, int32_t x)
 
 int packer::finish()
 {
-  // FlushChunks (Core/idx2Write.cpp:317): every channel in key order
-  std::vector<channel*> order;
-  order.reserve(channels_.size());
-  for (channel& c : channels_)
-    order.push_back(&c);
-  std::sort(order.begin(), order.end(), [](const channel* a, const channel* b) { return a->key < b->key; });
-  for (channel* c : order)
+  constexpr int kKeySpace = 4096;  // bit-plane keys are 12-bit (Core/idx2Lookup.h:21)
+  // events by (level, subband), in order
   {
-    const int level = (int)(c->key & 0xF);
-    const int subband = (int)((c->key >> 4) & 0xFFF);
-    const int bpkey = (int)(c->key >> 16);
-    write_chunk(*c, level, subband, bpkey);
+    std::map<std::pair<int, int>, size_t> gi;
+    for (size_t e = 0; e < events_.size(); ++e)
+    {
+      const subband_result& r = events_[e];
+      auto it = gi.find({ r.level, r.subband });
+      if (it == gi.end())
+      {
+        it = gi.emplace(std::make_pair(r.level, r.subband), groups_.size()).first;
+        groups_.emplace_back(new group());
+        groups_.back()->level = r.level;
+        groups_.back()->subband = r.subband;
+        groups_.back()->index.assign(kKeySpace, -1);
+      }
+      groups_[it->second]->events.push_back((uint32_t)e);
+    }
   }
+  const int end_bp = f_.type == dtype::float32 ? 32 : 64;
+  const int bpc = f_.bit_planes_per_chunk;
+  std::atomic<int> err{ 0 };
+
+  // the state machine of every (level, subband) (Core/idx2Encode.cpp:41-137, :157-249)
+  run_parallel(groups_.size(), [&](size_t gidx) {
+    group& g = *groups_[gidx];
+    const int L = g.level;
+    const u64 bpc_bricks = (u64)f_.bricks_per_chunk[(size_t)L];
+    const int shift = log2_ceil(f_.bricks_per_chunk[(size_t)L]);
+    std::vector<int> order;
+    std::vector<char> seen;
+    for (uint32_t ei : g.events)
+    {
+      const subband_result& r = events_[ei];
+      const u64 brick = r.brick;
+      if (r.kmin <= r.kmax && (r.kmin < 0 || r.kmax >= kKeySpace))
+      {
+        err = InvalidArgument;
+        return;
+      }
+      // pass 1: channels in first-touch order (blocks in Morton order, planes top-down);
+      // a channel entering a new chunk flushes the previous one
+      bool any_new = false;
+      for (int k = r.kmin; k <= r.kmax && !any_new; ++k)
+      {
+        if (!r.sizes[k - r.kmin])
+          continue;
+        const int32_t ci = g.index[(size_t)k];
+        const u64 last_chunk = ci >= 0 ? g.chans[(size_t)ci].last_chunk : 0;
+        any_new = brick >= (last_chunk + 1) * bpc_bricks;
+      }
+      if (any_new)
+      {
+        order.clear();
+        if (r.kmin <= r.kmax)
+        {
+          seen.assign((size_t)(r.kmax - r.kmin + 1), 0);
+          for (int b = 0; b < r.nexps; ++b)
+          {
+            const int emax = r.exps[b];
+            for (int bp = 63; bp >= 64 - end_bp; --bp)
+            {
+              if (!plane_coded(bp, emax, etol_, bpc))
+                break;
+              const int key = (bp + emax + 1024) / bpc;
+              if (key < r.kmin || key > r.kmax)
+                continue;
+              char& sn = seen[(size_t)(key - r.kmin)];
+              if (!sn)
+              {
+                sn = 1;
+                order.push_back(key);
+              }
+            }
+          }
+        }
+        uint32_t rank = 0;
+        for (int k : order)
+        {
+          channel& c = g.chan(k);
+          if (brick >= (c.last_chunk + 1) * bpc_bricks)
+          {
+            if (c.brick_bytes)
+              g.write_chunk(c, ei, rank++);
+            c.nbricks = 0;
+            c.last_chunk = brick >> shift;
+          }
+        }
+      }
+      // exponents (Core/idx2Encode.cpp:41 EncodeBrickSubbandExponents)
+      if (brick >= (g.exp_last_chunk + 1) * bpc_bricks)
+      {
+        g.write_exps(ei, 0);
+        g.exp_last_chunk = brick >> shift;
+      }
+      const size_t at = g.brick_exps.size();
+      if (f_.type == dtype::float64)
+      {
+        g.brick_exps.resize(at + 2 * (size_t)r.nexps);
+        for (int i = 0; i < r.nexps; ++i)
+        {
+          const uint16_t v = (uint16_t)(r.exps[i] + 1023);
+          g.brick_exps[at + 2 * (size_t)i] = (uint8_t)(v & 0xFF);
+          g.brick_exps[at + 2 * (size_t)i + 1] = (uint8_t)(v >> 8);
+        }
+      }
+      else
+      {
+        g.brick_exps.resize(at + (size_t)r.nexps);
+        for (int i = 0; i < r.nexps; ++i)
+          g.brick_exps[at + (size_t)i] = (uint8_t)(r.exps[i] + 127);
+      }
+      g.exp_last_brick = brick;
+      // pass 2: brick metadata and data per channel (Core/idx2Encode.cpp:84)
+      size_t off = 0;
+      for (int k = r.kmin; k <= r.kmax; ++k)
+      {
+        const uint32_t nb = r.sizes[k - r.kmin];
+        if (!nb)
+          continue;
+        channel& c = g.chan(k);
+        if (c.nbricks == 0)
+          c.deltas.put_varbyte(brick);
+        else
+          c.deltas.put_unary(brick - c.last_brick - 1);
+        c.sizes.put_varbyte(nb);
+        c.bricks.push_back({ r.bytes + off, nb });
+        c.brick_bytes += nb;
+        off += nb;
+        ++c.nbricks;
+        c.last_brick = brick;
+      }
+    }
+  });
+  if (err)
+    return err;
+
+  // FlushChunks (Core/idx2Write.cpp:317): every channel in channel-key order
+  {
+    struct ref
+    {
+      uint32_t key;
+      group* g;
+      channel* c;
+    };
+    std::vector<ref> all;
+    for (auto& g : groups_)
+      for (channel& c : g->chans)
+        all.push_back({ channel_key(c.bpkey, g->level, g->subband), g.get(), &c });
+    std::sort(all.begin(), all.end(), [](const ref& a, const ref& b) { return a.key < b.key; });
+    for (size_t i = 0; i < all.size(); ++i)
+      all[i].g->write_chunk(*all[i].c, kFinalFlush, (uint32_t)i);
+  }
+  // FlushChunkExponents (:121): sub-channels by level descending, then subband
+  {
+    std::vector<group*> gs;
+    for (auto& g : groups_)
+      gs.push_back(g.get());
+    std::stable_sort(gs.begin(), gs.end(), [](const group* a, const group* b) {
+      if (a->level == b->level)
+        return a->subband < b->subband;
+      return a->level > b->level;
+    });
+    for (size_t i = 0; i < gs.size(); ++i)
+      gs[i]->write_exps(kFinalFlush, (uint32_t)i);
+  }
+
+  // bit-plane chunks in the sequential order: statistics and files
+  struct chunk_ref
+  {
+    const chunk_rec* c;
+    int level, subband;
+  };
+  std::vector<chunk_ref> chunks;
+  for (auto& g : groups_)
+    for (const chunk_rec& c : g->chunks)
+      chunks.push_back({ &c, g->level, g->subband });
+  std::sort(chunks.begin(), chunks.end(),
+            [](const chunk_ref& a, const chunk_ref& b) { return stamp_less(a.c, b.c); });
+  for (const chunk_ref& cr : chunks)
+  {
+    const chunk_rec& c = *cr.c;
+    stats_.brick_deltas.add(c.deltas_bytes);
+    stats_.brick_sizes.add(c.sizes_bytes);
+    stats_.bit_plane_chunks.add((double)c.bytes);
+    file_buffer& fb = files_[file_path(f_, c.last_brick, cr.level)];
+    for (const segment& sg : c.parts)
+      fb.append_ref(sg.p, sg.n);
+    fb.has_chunks = true;
+    fb.chunk_sizes.put_varbyte(c.bytes);
+    fb.chunk_addrs.push_back(chunk_address(f_, c.last_brick, cr.level, cr.subband, c.bpkey));
+  }
+  // exponent chunks in the sequential order, compressed in parallel
+  struct exp_ref
+  {
+    exp_rec* e;
+    int level, subband;
+  };
+  std::vector<exp_ref> exps;
+  for (auto& g : groups_)
+    for (exp_rec& e : g->exps)
+      exps.push_back({ &e, g->level, g->subband });
+  std::sort(exps.begin(), exps.end(), [](const exp_ref& a, const exp_ref& b) { return stamp_less(a.e, b.e); });
+  for (const exp_ref& er : exps)
+    stats_.exp_chunks_raw.add((double)er.e->raw.size());
+  run_parallel(exps.size(), [&](size_t i) {
+    if (zstd_compress(exps[i].e->raw.data(), exps[i].e->raw.size(), &exps[i].e->z))
+      err = UnknownError;
+  });
+  if (err)
+    return err;
+  for (const exp_ref& er : exps)
+  {
+    stats_.exp_chunks_z.add((double)er.e->z.size());
+    file_buffer& fb = files_[file_path(f_, er.e->last_brick, er.level)];
+    fb.has_exps = true;
+    fb.exp_parts.push_back({ er.e->z.data(), er.e->z.size() });
+    fb.exp_addrs.push_back(chunk_address(f_, er.e->last_brick, er.level, er.subband, 0));
+  }
+
+  // file tails
   for (auto& kv : files_)
   {
     file_buffer& fb = kv.second;
@@ -505,39 +668,6 @@ int packer::finish()
     stats_.chunk_addrs_z.add((double)z.size());
     fb.append_owned(std::move(tail));
   }
-  // FlushChunkExponents (:121): sub-channels by level descending, then subband
-  std::vector<std::pair<std::pair<int, int>, sub_channel*>> subs;
-  for (auto& kv : subs_)
-    subs.push_back({ kv.first, &kv.second });
-  std::stable_sort(subs.begin(), subs.end(), [](const auto& a, const auto& b) {
-    if (a.first.first == b.first.first)
-      return a.first.second < b.first.second;
-    return a.first.first > b.first.first;
-  });
-  for (auto& s : subs)
-    write_chunk_exps(*s.second, s.first.first, s.first.second);
-  // compress the exponent chunks in parallel (each is an independent zstd frame)
-  {
-    std::atomic<size_t> next{ 0 };
-    std::atomic<int> err{ 0 };
-    unsigned nt = std::thread::hardware_concurrency();
-    nt = nt ? (nt > 32 ? 32 : nt) : 4;
-    auto work = [&]() {
-      for (size_t i; (i = next.fetch_add(1)) < exp_chunks_.size();)
-        if (zstd_compress(exp_chunks_[i].raw.data(), exp_chunks_[i].raw.size(), &exp_chunks_[i].z))
-          err = UnknownError;
-    };
-    std::vector<std::thread> th;
-    for (unsigned t = 1; t < nt; ++t)
-      th.emplace_back(work);
-    work();
-    for (auto& t : th)
-      t.join();
-    if (err)
-      return err;
-    for (auto& c : exp_chunks_)
-      stats_.exp_chunks_z.add((double)c.z.size());
-  }
   for (auto& kv : files_)
   {
     file_buffer& fb = kv.second;
@@ -545,12 +675,11 @@ int packer::finish()
       continue;
     int total = 0;
     bit_writer sizes;
-    for (int ci : fb.exp_chunks)
+    for (const segment& sg : fb.exp_parts)
     {
-      exp_chunk& c = exp_chunks_[(size_t)ci];
-      fb.append_ref(c.z.data(), c.z.size());
-      total += (int)c.z.size();
-      sizes.put_varbyte(c.z.size());
+      fb.append_ref(sg.p, sg.n);
+      total += (int)sg.n;
+      sizes.put_varbyte(sg.n);
     }
     const size_t n = sizes.size();
     stats_.exp_chunk_sizes.add((double)n);

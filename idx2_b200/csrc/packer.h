@@ -85,60 +85,44 @@ struct file_buffer
   bit_writer chunk_sizes;                           // varbyte sizes of bit-plane chunks
   std::vector<u64> chunk_addrs;                     // chunk addresses
   bool has_chunks = false;
-  std::vector<int> exp_chunks;                      // indices into the packer's exponent chunks
+  std::vector<segment> exp_parts;                   // compressed exponent chunks
   std::vector<u64> exp_addrs;
   bool has_exps = false;
   void append_owned(std::vector<uint8_t>&& v);
   void append_ref(const uint8_t* p, size_t n);
 };
 
+// The packer records the (brick, subband) results in the reference's encode order and, at
+// finish, replays the channel state machine of every (level, subband) on its own thread:
+// channels of different (level, subband) never interact, and each chunk write is stamped
+// with its place in the sequential order (event index, then rank inside the event; the final
+// flushes after every event, in the reference's flush order), so the merged chunk order in
+// every file and the order of the statistics are those of a sequential pass.
 class packer
 {
 public:
   packer(const dataset_format& f, double tolerance);
   ~packer();
-  // One EncodeSubband call of the reference (Core/idx2Encode.cpp:261).
+  // One EncodeSubband call of the reference (Core/idx2Encode.cpp:261); r's arrays must
+  // outlive the packer.
   int add(const subband_result& r);
-  // FlushChunks + FlushChunkExponents (Core/idx2Write.cpp:317, :121).
+  // Channel / chunk state machine, FlushChunks + FlushChunkExponents (Core/idx2Write.cpp:317,
+  // :121), file assembly.
   int finish();
   std::map<std::string, file_buffer>& files() { return files_; }
   const pack_stats& stats() const { return stats_; }
   // The statistics block the reference appends to the metadata file (Core/idx2Write.cpp:389).
   std::string stats_text() const;
 
-private:
-  struct channel
-  {
-    bit_writer deltas, sizes;
-    std::vector<segment> bricks;
-    size_t brick_bytes = 0;
-    u64 last_chunk = 0, last_brick = 0;
-    int nbricks = 0;
-    uint32_t key = 0;
-  };
-  struct sub_channel
-  {
-    std::vector<uint8_t> brick_exps;
-    u64 last_chunk = 0, last_brick = 0;
-  };
-  struct exp_chunk
-  {
-    std::vector<uint8_t> raw, z;
-  };
-  channel& chan(int level, int subband, int bpkey);
-  channel* find_chan(int level, int subband, int bpkey);
-  void write_chunk(channel& c, int level, int subband, int bpkey);
-  void write_chunk_exps(sub_channel& s, int level, int subband);
-  void first_touch_order(const subband_result& r, std::vector<int>* keys) const;
+  struct group;  // the channels of one (level, subband)
 
+private:
   const dataset_format& f_;
   double tol_;
   int etol_;
-  std::vector<int32_t> chan_index_;   // (level, subband, bpkey) -> index into channels_, -1
-  std::deque<channel> channels_;
-  std::map<std::pair<int, int>, sub_channel> subs_;
-  std::deque<exp_chunk> exp_chunks_;  // compressed in parallel at finish
+  std::vector<subband_result> events_;
   std::map<std::string, file_buffer> files_;
+  std::vector<std::unique_ptr<group>> groups_;
   pack_stats stats_;
 };
 

@@ -87,3 +87,18 @@ def test_encode_matches_golden_files(idx2g, tmp_path, case):
     here = os.path.dirname(os.path.abspath(__file__))
     diffs = compare_dirs(os.path.join(here, "golden", "datasets", case["name"]), str(tmp_path / case["name"]))
     assert diffs == [], diffs[:3]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", __import__("test_packer_chunks").CHUNK_CASES,
+                         ids=__import__("test_packer_chunks").chunk_case_id)
+def test_encode_chunk_boundaries_match_reference(idx2g, ref_app, tmp_path, case):
+    from test_packer_chunks import chunk_field, ref_encode_chunked
+    dims, dtype, levels, tol, bd, bpc, cpf, fpd, seed = case
+    f = chunk_field(dims, dtype, seed)
+    _, ref_dir = ref_encode_chunked(ref_app, str(tmp_path), f, case)
+    idx2g.encode(f, out_dir=str(tmp_path / "ours"), name="kat", field_name="f", num_levels=levels,
+                 tolerance=tol, brick_dims=bd, bricks_per_chunk=bpc, chunks_per_file=cpf,
+                 files_per_dir=fpd)
+    diffs = compare_dirs(ref_dir, str(tmp_path / "ours" / "kat"))
+    assert diffs == [], diffs[:5]
