@@ -354,10 +354,10 @@ __device__ __forceinline__ long long trunc_i64(double v)
   return __double2ll_rz(v);
 }
 
-// zfp 4-point lifting (Core/Zfp.h:145 FLift, :181 ILift).
-__device__ __forceinline__ void fwd_lift4(long long* p, int s)
+// zfp 4-point lifting (Core/Zfp.h:145 FLift, :181 ILift), on four elements anywhere.
+__device__ __forceinline__ void fwd_lift4_at(long long* p0, long long* p1, long long* p2, long long* p3)
 {
-  long long x = p[0], y = p[s], z = p[2 * s], w = p[3 * s];
+  long long x = *p0, y = *p1, z = *p2, w = *p3;
   x += w;
   x >>= 1;
   w -= x;
@@ -372,11 +372,13 @@ __device__ __forceinline__ void fwd_lift4(long long* p, int s)
   y -= w;
   w += y >> 1;
   y -= w >> 1;
-  p[0] = x;
-  p[s] = y;
-  p[2 * s] = z;
-  p[3 * s] = w;
+  *p0 = x;
+  *p1 = y;
+  *p2 = z;
+  *p3 = w;
 }
+
+__device__ __forceinline__ void fwd_lift4(long long* p, int s) { fwd_lift4_at(p, p + s, p + 2 * s, p + 3 * s); }
 
 __device__ __forceinline__ void inv_lift4(long long* p, int s)
 {

@@ -54,8 +54,20 @@ __device__ unsigned long long g_phase_cycles[16];
 #define ENC_PHASE_FLUSH
 #endif
 
-constexpr int kThreads = 256;
+// CTA size: 256 threads with two CTAs per SM, or 512 with one (IDX2G_ENC_THREADS)
+#ifndef IDX2G_ENC_THREADS
+#define IDX2G_ENC_THREADS 256
+#endif
+constexpr int kThreads = IDX2G_ENC_THREADS;
 constexpr int kWarps = kThreads / 32;
+constexpr int kCtasPerSm = kThreads >= 512 ? 1 : 2;
+// per-block zfp scratch, one padding word after every 4 (conflict-free 4-point passes)
+constexpr int kQStride = 80;
+__device__ __forceinline__ int qpad(int i) { return i + (i >> 2); }
+// plane-major (plane, block) tables of a subband, rows padded against bank conflicts
+constexpr int kRowX = kMaxBlocksPerSubband + 1;    // unsigned long long
+constexpr int kRowOff = kMaxBlocksPerSubband + 2;  // uint16_t
+constexpr int kRowNin = kMaxBlocksPerSubband + 4;  // uint8_t
 constexpr unsigned kStageBytes = 8192;
 
 struct enc_brick
@@ -91,14 +103,14 @@ struct enc_args
   double* bmax;
 };
 
-// shared memory layout: this struct, then the per-(block, plane) arrays of one subband
+// shared memory layout: this struct, then the per-(plane, block) tables of one subband
 // sized by the number of planes a block can have (32 for float32 data, 64 for float64):
-//   unsigned long long X[kMaxBlocksPerSubband][P]   plane bit masks
-//   uint16_t off[kMaxBlocksPerSubband][P]            plane bit lengths, then bit offsets
-//   uint8_t nin[kMaxBlocksPerSubband][P]             significant coefficients before the plane
+//   unsigned long long X[P][kRowX]   plane bit masks
+//   uint16_t off[P][kRowOff]         plane bit lengths, then bit offsets in the channel
+//   uint8_t nin[P][kRowNin]          significant coefficients before the plane
 struct enc_smem
 {
-  long long q[kWarps][2][64];  // per-warp scratch of two blocks
+  long long q[kWarps][2][kQStride];  // per-warp scratch of two blocks
   int16_t emax[kMaxBlocksPerSubband];
   int16_t ktop[kMaxBlocksPerSubband];
   uint8_t np[kMaxBlocksPerSubband];
@@ -118,7 +130,8 @@ struct enc_smem
 
 inline size_t enc_smem_bytes(int planes)
 {
-  return ((sizeof(enc_smem) + 15) & ~(size_t)15) + (size_t)kMaxBlocksPerSubband * (size_t)planes * (8 + 2 + 1);
+  return ((sizeof(enc_smem) + 15) & ~(size_t)15) +
+         (size_t)planes * ((size_t)kRowX * 8 + (size_t)kRowOff * 2 + (size_t)kRowNin);
 }
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
@@ -172,6 +185,13 @@ __device__ __forceinline__ double warp_max(double v)
   return v;
 }
 
+// One zfp 4-point lifting line (Core/Zfp.h:145 FLift) on the padded per-block scratch:
+// elements i, i + s, i + 2s, i + 3s of the block.
+__device__ __forceinline__ void lift4_padded(long long* q, int i, int s)
+{
+  dev::fwd_lift4_at(q + qpad(i), q + qpad(i + s), q + qpad(i + 2 * s), q + qpad(i + 3 * s));
+}
+
 // Offset in the brick of sample j of a block (block dims are 4 or 1 per axis since the
 // subbands of a 33^3 brick are 17 or 16 wide).
 __device__ __forceinline__ int block_sample(int base, int lx, int ly, int j, int sy, int sz)
@@ -199,15 +219,15 @@ __device__ __forceinline__ block_info block_at(const uint64_t* geom, int b, cons
   return bi;
 }
 
-__global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc_args a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   enc_smem& sm = *reinterpret_cast<enc_smem*>(smem_raw);
   const int P = a.planes;
   unsigned long long* const Xp =
     reinterpret_cast<unsigned long long*>(smem_raw + ((sizeof(enc_smem) + 15) & ~(size_t)15));
-  uint16_t* const OFF = reinterpret_cast<uint16_t*>(Xp + (size_t)kMaxBlocksPerSubband * P);
-  uint8_t* const NIN = reinterpret_cast<uint8_t*>(OFF + (size_t)kMaxBlocksPerSubband * P);
+  uint16_t* const OFF = reinterpret_cast<uint16_t*>(Xp + (size_t)kRowX * P);
+  uint8_t* const NIN = reinterpret_cast<uint8_t*>(OFF + (size_t)kRowOff * P);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int N[3] = { 33, 33, a.is2d ? 1 : 33 };
   const int NB = N[0] * N[1] * N[2];
@@ -458,13 +478,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         long long* qA = sm.q[warp][0];
         long long* qB = sm.q[warp][1];
         if (lane < nvA)
-          qA[lane] = dev::trunc_i64(__dmul_rn(sA, cv[0]));
+          qA[qpad(lane)] = dev::trunc_i64(__dmul_rn(sA, cv[0]));
         if (lane + 32 < nvA)
-          qA[lane + 32] = dev::trunc_i64(__dmul_rn(sA, cv[1]));
+          qA[qpad(lane + 32)] = dev::trunc_i64(__dmul_rn(sA, cv[1]));
         if (lane < nvB)
-          qB[lane] = dev::trunc_i64(__dmul_rn(sB, cv[2]));
+          qB[qpad(lane)] = dev::trunc_i64(__dmul_rn(sB, cv[2]));
         if (lane + 32 < nvB)
-          qB[lane + 32] = dev::trunc_i64(__dmul_rn(sB, cv[3]));
+          qB[qpad(lane + 32)] = dev::trunc_i64(__dmul_rn(sB, cv[3]));
         __syncwarp();
         // zfp transform (Core/Zfp.h:262): the 16 lines of a pass of block A on lanes 0-15,
         // of block B on lanes 16-31
@@ -476,24 +496,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
           const int nd = h ? ndB : ndA;
           if (nd == 3)
           {
-            dev::fwd_lift4(q + 4 * (l & 3) + 16 * (l >> 2), 1);
+            lift4_padded(q, 4 * (l & 3) + 16 * (l >> 2), 1);
             __syncwarp(hm);
-            dev::fwd_lift4(q + 16 * (l & 3) + (l >> 2), 4);
+            lift4_padded(q, 16 * (l & 3) + (l >> 2), 4);
             __syncwarp(hm);
-            dev::fwd_lift4(q + (l & 3) + 4 * (l >> 2), 16);
+            lift4_padded(q, (l & 3) + 4 * (l >> 2), 16);
           }
           else if (nd == 2)
           {
             if (l < 4)
-              dev::fwd_lift4(q + 4 * l, 1);
+              lift4_padded(q, 4 * l, 1);
             __syncwarp(hm);
             if (l < 4)
-              dev::fwd_lift4(q + l, 4);
+              lift4_padded(q, l, 4);
           }
           else if (nd == 1)
           {
             if (l == 0)
-              dev::fwd_lift4(q, 1);
+              lift4_padded(q, 0, 1);
           }
           __syncwarp();
         }
@@ -503,19 +523,19 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         };
         unsigned long long uA0 = 0, uA1 = 0, uB0 = 0, uB1 = 0;
         if (lane < nvA)
-          uA0 = ((unsigned long long)qA[permj(ndA, lane)] + dev::kNegaMask) ^ dev::kNegaMask;
+          uA0 = ((unsigned long long)qA[qpad(permj(ndA, lane))] + dev::kNegaMask) ^ dev::kNegaMask;
         if (lane + 32 < nvA)
-          uA1 = ((unsigned long long)qA[permj(ndA, lane + 32)] + dev::kNegaMask) ^ dev::kNegaMask;
+          uA1 = ((unsigned long long)qA[qpad(permj(ndA, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
         if (lane < nvB)
-          uB0 = ((unsigned long long)qB[permj(ndB, lane)] + dev::kNegaMask) ^ dev::kNegaMask;
+          uB0 = ((unsigned long long)qB[qpad(permj(ndB, lane))] + dev::kNegaMask) ^ dev::kNegaMask;
         if (lane + 32 < nvB)
-          uB1 = ((unsigned long long)qB[permj(ndB, lane + 32)] + dev::kNegaMask) ^ dev::kNegaMask;
+          uB1 = ((unsigned long long)qB[qpad(permj(ndB, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
         __syncwarp();
         const int npA = dev::coded_planes(eA, a.etol, a.end_bp);
         const int npB = hasB ? dev::coded_planes(eB, a.etol, a.end_bp) : 0;
         const int npM = npA > npB ? npA : npB;
-        unsigned long long* XA = Xp + (size_t)bA * P;
-        unsigned long long* XB = Xp + (size_t)bB * P;
+        unsigned long long* XA = Xp + bA;  // plane k at XA[k * kRowX]
+        unsigned long long* XB = Xp + bB;
         for (int k = 0; k < npM; ++k)
         {
           const int bit = 63 - k;
@@ -524,9 +544,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
           const unsigned b0 = __ballot_sync(0xffffffffu, (uB0 >> bit) & 1ull);
           const unsigned b1 = __ballot_sync(0xffffffffu, (uB1 >> bit) & 1ull);
           if (lane == 0 && k < npA)
-            XA[k] = (unsigned long long)a0 | ((unsigned long long)a1 << 32);
+            XA[k * kRowX] = (unsigned long long)a0 | ((unsigned long long)a1 << 32);
           if (lane == 1 && k < npB)
-            XB[k] = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
+            XB[k * kRowX] = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
         }
         if (lane == 0)
         {
@@ -550,8 +570,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
           for (int k0 = 0; k0 < npM; k0 += 32)
           {
             const int k = k0 + lane;
-            const unsigned long long xa = k < npA ? XA[k] : 0ull;
-            const unsigned long long xb = k < npB ? XB[k] : 0ull;
+            const unsigned long long xa = k < npA ? XA[k * kRowX] : 0ull;
+            const unsigned long long xb = k < npB ? XB[k * kRowX] : 0ull;
             int ma = xa ? 64 - __clzll(xa) : 0, mb = xb ? 64 - __clzll(xb) : 0;
             int ia = ma, ib = mb;  // inclusive prefix max
             for (int o = 1; o < 32; o <<= 1)
@@ -569,13 +589,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
             const int nA_ = ea > carryA ? ea : carryA, nB_ = eb > carryB ? eb : carryB;
             if (k < npA)
             {
-              NIN[(size_t)bA * P + k] = (uint8_t)nA_;
-              OFF[(size_t)bA * P + k] = (uint16_t)dev::plane_bits(xa, nA_, nvA);
+              NIN[k * kRowNin + bA] = (uint8_t)nA_;
+              OFF[k * kRowOff + bA] = (uint16_t)dev::plane_bits(xa, nA_, nvA);
             }
             if (k < npB)
             {
-              NIN[(size_t)bB * P + k] = (uint8_t)nB_;
-              OFF[(size_t)bB * P + k] = (uint16_t)dev::plane_bits(xb, nB_, nvB);
+              NIN[k * kRowNin + bB] = (uint8_t)nB_;
+              OFF[k * kRowOff + bB] = (uint16_t)dev::plane_bits(xb, nB_, nvB);
             }
             const int ta = __shfl_sync(0xffffffffu, ia, 31), tb = __shfl_sync(0xffffffffu, ib, 31);
             carryA = carryA > ta ? carryA : ta;
@@ -634,35 +654,26 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
       for (int t = warp; t < nkeys; t += kWarps)
       {
         const int key = kmin + t;
-        uint32_t v[4];
-        int kk[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
+        uint32_t carry = 0;
+        for (int b0 = 0; b0 < nb; b0 += 32)
         {
-          const int b = lane * 4 + i;
-          kk[i] = b < nb ? sm.ktop[b] - key : -1;
-          const bool in = kk[i] >= 0 && b < nb && kk[i] < sm.np[b];
-          kk[i] = in ? kk[i] : -1;
-          v[i] = in ? OFF[(size_t)b * P + kk[i]] : 0u;
+          const int b = b0 + lane;
+          int kk = b < nb ? sm.ktop[b] - key : -1;
+          kk = (kk >= 0 && b < nb && kk < sm.np[b]) ? kk : -1;
+          const uint32_t v = kk >= 0 ? OFF[kk * kRowOff + b] : 0u;
+          uint32_t inc = v;
+          for (int o = 1; o < 32; o <<= 1)
+          {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o)
+              inc += y;
+          }
+          if (kk >= 0)
+            OFF[kk * kRowOff + b] = (uint16_t)(carry + inc - v);
+          carry += __shfl_sync(0xffffffffu, inc, 31);
         }
-        const uint32_t tot = v[0] + v[1] + v[2] + v[3];
-        uint32_t inc = tot;
-        for (int o = 1; o < 32; o <<= 1)
-        {
-          const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-          if (lane >= o)
-            inc += y;
-        }
-        uint32_t acc = inc - tot;
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-        {
-          if (kk[i] >= 0)
-            OFF[(size_t)(lane * 4 + i) * P + kk[i]] = (uint16_t)acc;
-          acc += v[i];
-        }
-        if (lane == 31)
-          sm.key_bits[t] = inc;
+        if (lane == 0)
+          sm.key_bits[t] = carry;
       }
       __syncthreads();
       ENC_PHASE(9)
@@ -738,17 +749,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_encode_level(const enc_args a)
         uint32_t* sw = words + 2 + ((2u * (unsigned)nb + 3u) >> 2);
         for (int t = tid; t < nkeys; t += kThreads)
           sw[t] = (sm.key_bits[t] + 7) / 8;
-        const int lp = P == 64 ? 6 : 5;
-        for (int idx = tid; idx < nb * P; idx += kThreads)
+        for (int idx = tid; idx < P * kMaxBlocksPerSubband; idx += kThreads)
         {
-          const int b = idx >> lp, kk = idx & (P - 1);
-          if (kk >= sm.np[b])
+          const int b = idx & (kMaxBlocksPerSubband - 1), kk = idx / kMaxBlocksPerSubband;
+          if (b >= nb || kk >= sm.np[b])
             continue;
           const int t = sm.ktop[b] - kk - kmin;
-          const unsigned long long pos =
-            ((unsigned long long)hdr + sm.key_base[t]) * 8ull + (unsigned long long)OFF[idx];
+          const unsigned long long pos = ((unsigned long long)hdr + sm.key_base[t]) * 8ull +
+                                         (unsigned long long)OFF[kk * kRowOff + b];
           dev::bits192 c;
-          const int len = dev::plane_code(Xp[idx], NIN[idx], 1 << sm.nvals_log[b], &c);
+          const int len =
+            dev::plane_code(Xp[kk * kRowX + b], NIN[kk * kRowNin + b], 1 << sm.nvals_log[b], &c);
           dev::or_code(words, pos, c, len);
         }
         __syncthreads();
@@ -867,7 +878,7 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
 
   // workspace buffers, kept by the context across calls (grow-only)
   int nsm = ctx_->num_sms;
-  int grid = nbr < 2 * nsm ? nbr : 2 * nsm;
+  int grid = nbr < kCtasPerSm * nsm ? nbr : kCtasPerSm * nsm;
   if (grid < 1)
     grid = 1;
   const size_t nbs = (size_t)nbr * (size_t)nsb;

@@ -10,6 +10,7 @@
 #include <cstring>
 #include <dlfcn.h>
 #include <fcntl.h>
+#include <sys/mman.h>
 #include <thread>
 #include <unistd.h>
 
@@ -173,15 +174,19 @@ void file_buffer::append_ref(const uint8_t* p, size_t n)
 
 int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& files)
 {
-  // Every file is cut into ranges of whole parts of about kRange bytes; a pool of
-  // threads gathers each range into a staging buffer and writes it at its offset.
+  // Every file is cut into ranges of whole parts of about kRange bytes, copied by a pool of
+  // threads. Large files are written through a shared mapping (writes to one file through
+  // write(2) are serialised by the kernel); small files, and any file that cannot be mapped,
+  // with pwrite from a staging buffer.
   constexpr size_t kRange = (size_t)16 << 20;
+  constexpr size_t kMapMin = (size_t)64 << 20;
   struct range
   {
     int file;
-    size_t p0, p1, offset;
+    size_t p0, p1, offset, bytes;
   };
   std::vector<int> fds(files.size(), -1);
+  std::vector<uint8_t*> maps(files.size(), nullptr);
   std::vector<range> ranges;
   int err = NoError;
   for (size_t i = 0; i < files.size() && !err; ++i)
@@ -191,11 +196,20 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
       err = CannotCreateDirectory;
       break;
     }
-    fds[i] = open(files[i].first.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    const size_t total = files[i].second->nbytes;
+    fds[i] = open(files[i].first.c_str(), O_RDWR | O_CREAT | O_TRUNC, 0644);
     if (fds[i] < 0)
     {
       err = FileCreateFailed;
       break;
+    }
+    if (total >= kMapMin && ftruncate(fds[i], (off_t)total) == 0)
+    {
+      void* m = mmap(nullptr, total, PROT_WRITE, MAP_SHARED, fds[i], 0);
+      if (m != MAP_FAILED)
+        maps[i] = (uint8_t*)m;
+      else if (ftruncate(fds[i], 0) != 0)
+        err = FileWriteFailed;
     }
     const std::vector<segment>& parts = files[i].second->parts;
     size_t off = 0, start = 0, acc = 0;
@@ -204,7 +218,7 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
       acc += parts[k].n;
       if (acc >= kRange || k + 1 == parts.size())
       {
-        ranges.push_back({ (int)i, start, k + 1, off });
+        ranges.push_back({ (int)i, start, k + 1, off, acc });
         off += acc;
         start = k + 1;
         acc = 0;
@@ -225,15 +239,22 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
       {
         const range& r = ranges[i];
         const std::vector<segment>& parts = files[(size_t)r.file].second->parts;
-        size_t n = 0;
-        for (size_t k = r.p0; k < r.p1; ++k)
-          n += parts[k].n;
+        if (maps[(size_t)r.file])
+        {
+          uint8_t* dst = maps[(size_t)r.file] + r.offset;
+          for (size_t k = r.p0; k < r.p1; ++k)
+          {
+            memcpy(dst, parts[k].p, parts[k].n);
+            dst += parts[k].n;
+          }
+          continue;
+        }
         const uint8_t* src;
         if (r.p1 - r.p0 == 1)
           src = parts[r.p0].p;
         else
         {
-          stage.resize(n);
+          stage.resize(r.bytes);
           size_t at = 0;
           for (size_t k = r.p0; k < r.p1; ++k)
           {
@@ -243,9 +264,9 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
           src = stage.data();
         }
         size_t done = 0;
-        while (done < n)
+        while (done < r.bytes)
         {
-          ssize_t w = pwrite(fds[(size_t)r.file], src + done, n - done, (off_t)(r.offset + done));
+          ssize_t w = pwrite(fds[(size_t)r.file], src + done, r.bytes - done, (off_t)(r.offset + done));
           if (w <= 0)
           {
             werr = FileWriteFailed;
@@ -263,6 +284,9 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
       t.join();
     err = werr;
   }
+  for (size_t i = 0; i < files.size(); ++i)
+    if (maps[i] && munmap(maps[i], files[i].second->nbytes) != 0 && !err)
+      err = FileWriteFailed;
   for (int fd : fds)
     if (fd >= 0 && close(fd) != 0 && !err)
       err = FileWriteFailed;
