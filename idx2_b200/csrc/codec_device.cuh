@@ -205,6 +205,32 @@ __device__ __forceinline__ void lift_line_fixed(double* L, int s)
     L[k * s] = v[k];
 }
 
+// The same with a compile-time stride (immediate offsets, no address registers).
+template <int D, bool FWD, int STRIDE>
+__device__ __forceinline__ void lift_line_strided(double* L)
+{
+  constexpr bool ext = (D % 2) == 0;
+  constexpr int nload = D + (ext && !FWD ? 1 : 0);
+  constexpr int nstore = D + (ext && FWD ? 1 : 0);
+  double v[33];
+#pragma unroll
+  for (int k = 0; k < 33; ++k)
+    v[k] = k < nload ? L[k * STRIDE] : 0.0;
+  lift_regs<FWD>(v, D);
+#pragma unroll
+  for (int k = 0; k < nstore; ++k)
+    L[k * STRIDE] = v[k];
+}
+
+// The lines of a sweep with a compile-time length and stride: line li starts at
+// (li % ub) * sb + (li / ub) * sc.
+template <int D, bool FWD, int STRIDE>
+__device__ __forceinline__ void sweep_strided(double* F, int nlines, int ub, int sb, int sc)
+{
+  for (int li = threadIdx.x; li < nlines; li += blockDim.x)
+    lift_line_strided<D, FWD, STRIDE>(F + (li % ub) * sb + (li / ub) * sc);
+}
+
 template <bool FWD>
 __device__ __noinline__ void lift_line(double* L, int s, int D)
 {
@@ -239,6 +265,31 @@ __device__ void lift_sweep_regs(double* F, const int N[3], const dgrid& G, int a
   const int st[3] = { 1, N[0], N[0] * N[1] };
   const int s = st[a] * S;
   const int nlines = G.dims[b] * G.dims[c];
+  // The first-level sweeps of 33^3 bricks (line lengths 32 and 33 with strides 1, 33, 1089)
+  // run with compile-time strides; other sweeps (edge bricks) go through the out-of-line switch.
+  if (S == 1 && N[0] == 33 && N[1] == 33 && (D == 32 || D == 33))
+  {
+    const int ub = G.dims[b], sb = G.strd[b] * st[b], sc = G.strd[c] * st[c];
+    if (D == 33)
+    {
+      if (a == 0)
+        sweep_strided<33, FWD, 1>(F, nlines, ub, sb, sc);
+      else if (a == 1)
+        sweep_strided<33, FWD, 33>(F, nlines, ub, sb, sc);
+      else
+        sweep_strided<33, FWD, 1089>(F, nlines, ub, sb, sc);
+    }
+    else
+    {
+      if (a == 0)
+        sweep_strided<32, FWD, 1>(F, nlines, ub, sb, sc);
+      else if (a == 1)
+        sweep_strided<32, FWD, 33>(F, nlines, ub, sb, sc);
+      else
+        sweep_strided<32, FWD, 1089>(F, nlines, ub, sb, sc);
+    }
+    return;
+  }
   for (int li = threadIdx.x; li < nlines; li += blockDim.x)
   {
     const int u = (li % G.dims[b]) * G.strd[b];
@@ -254,6 +305,7 @@ struct lift_stack
   dgrid g[16];
   int8_t axis[16];
   int n;
+  int coarse;  // first sweep of the second level: from there on every position is even
 };
 
 inline __device__ void build_stack(const int dims3[3], int nlevels, uint64_t order, lift_stack* st)
@@ -271,12 +323,15 @@ inline __device__ void build_stack(const int dims3[3], int nlevels, uint64_t ord
     G.strd[k] = 1;
   }
   st->n = 0;
+  st->coarse = -1;
   while (level < nlevels)
   {
     int d = (int)(order & 3);
     order >>= 2;
     if (d == 3)
     {
+      if (level == 0)
+        st->coarse = st->n;
       if (order == 3)
         order = prev;
       else
@@ -304,6 +359,22 @@ inline __device__ void build_stack(const int dims3[3], int nlevels, uint64_t ord
       S3[d] <<= 1;
     }
   }
+  if (st->coarse < 0)
+    st->coarse = st->n;
+}
+
+// A grid of even positions mapped onto the half-resolution lattice (position p -> p / 2);
+// axes of one sample keep stride 1.
+__device__ __forceinline__ dgrid half_grid(const dgrid& g)
+{
+  dgrid h;
+  for (int k = 0; k < 3; ++k)
+  {
+    h.from[k] = g.from[k] >> 1;
+    h.dims[k] = g.dims[k];
+    h.strd[k] = g.strd[k] >= 2 ? g.strd[k] >> 1 : 1;
+  }
+  return h;
 }
 
 // Core/Math.h:524 Exponent<f64>, via the IEEE exponent field (glibc frexp semantics:

@@ -27,6 +27,16 @@ namespace
 
 } // namespace
 
+#ifdef IDX2G_PHASE_TIMING
+// Profiling builds: read and clear the per-phase cycle counters of the decode kernel.
+extern "C" __attribute__((visibility("default"))) void idx2g_debug_dec_phase_cycles(unsigned long long* out)
+{
+  cudaMemcpyFromSymbol(out, g_dec_phase_cycles, sizeof(g_dec_phase_cycles));
+  unsigned long long z[16] = {};
+  cudaMemcpyToSymbol(g_dec_phase_cycles, z, sizeof(z));
+}
+#endif
+
 decode_device::~decode_device()
 {
   cudaFree(exps_);

@@ -2,6 +2,34 @@
 // anonymous namespace). See decode.cu for the pipeline overview.
 #pragma once
 
+// Per-phase cycle counters of thread 0 of every CTA, for profiling builds only
+// (-DIDX2G_PHASE_TIMING); compiled out otherwise.
+#ifdef IDX2G_PHASE_TIMING
+__device__ unsigned long long g_dec_phase_cycles[16];
+#define DEC_PHASE_INIT \
+  long long ph_[8] = {};   \
+  long long ph_t = 0;
+#define DEC_PHASE_START \
+  if (threadIdx.x == 0) \
+    ph_t = clock64();
+#define DEC_PHASE(k)                 \
+  if (threadIdx.x == 0)              \
+  {                                  \
+    const long long t_ = clock64();  \
+    ph_[k] += t_ - ph_t;             \
+    ph_t = t_;                       \
+  }
+#define DEC_PHASE_FLUSH           \
+  if (threadIdx.x == 0)           \
+    for (int k = 0; k < 8; ++k)   \
+      atomicAdd(&g_dec_phase_cycles[k], (unsigned long long)ph_[k]);
+#else
+#define DEC_PHASE_INIT
+#define DEC_PHASE_START
+#define DEC_PHASE(k)
+#define DEC_PHASE_FLUSH
+#endif
+
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRing = 32;  // steps a decoded plane stays in the per-warp ring (>= channels)
@@ -35,6 +63,11 @@ struct dec_smem
   {
     unsigned long long coef[kMaxBlocksPerSubband][64];  // CTA-wide path: one subband
     unsigned long long ring[kWarps][kRing][32];         // warp path: decoded planes in flight
+    struct
+    {
+      double v[kWarps][32][33];     // output rows of the X sweep, one per lane
+      long long base[kWarps][32];   // their offsets in the output (-1: no output)
+    } out;
   } u;
   long long q[kWarps][64];
   int16_t emax[8][kMaxBlocksPerSubband];
@@ -43,6 +76,8 @@ struct dec_smem
   uint8_t nbps[8][kMaxBlocksPerSubband];
   uint8_t nd[8][kMaxBlocksPerSubband];
   uint8_t bypass[8][kMaxBlocksPerSubband];
+  uint8_t perm3[64];
+  uint8_t perm2[16];
   uint8_t nst[2][kKeyWindow];
   uint8_t stop[2][kKeyWindow];
   int kmax[8], nkeys[8];
@@ -88,6 +123,24 @@ __device__ __forceinline__ void subband_grid(int is2d, int s, int from[3], int d
       strd[k] = 2;
     }
   }
+}
+
+// Decoded bricks are stored subband-major: the 33^3 samples are the 8 subbands (index
+// 4hx + 2hy + hz, of 17 - h samples per axis) one after the other, each dense and x-fastest.
+// Blocks then land in contiguous rows, and a line of the inverse transform reads two dense
+// streams (its even and odd samples).
+__device__ __forceinline__ int sbm_base(int hx, int hy, int hz, int is2d)
+{
+  const int dx = 17 - hx, dy = 17 - hy;
+  return is2d ? hx * 17 * 33 + hy * dx * 17 : hx * 17 * 33 * 33 + hy * dx * 17 * 33 + hz * dx * dy * 17;
+}
+
+// Position (x, y, z) of the brick in the subband-major layout.
+__device__ __forceinline__ int sbm(int x, int y, int z, int is2d)
+{
+  const int hx = x & 1, hy = y & 1, hz = z & 1;
+  const int dx = 17 - hx, dy = 17 - hy;
+  return sbm_base(hx, hy, hz, is2d) + (((z >> 1) * dy + (y >> 1)) * dx + (x >> 1));
 }
 
 // LSB-first bit reader over the blob with a 128-bit register window (Core/BitStream.h
@@ -162,26 +215,49 @@ __device__ __forceinline__ unsigned long long decode_plane(bit_reader& rd, int& 
 }
 
 // Inverse shuffle / inverse zfp / dequantise of one block and scatter into the brick
-// (Core/idx2Decode.cpp:203-227), by one warp; u holds the negabinary coefficients.
-__device__ __forceinline__ void reconstruct_block(double* F, long long* q, unsigned long long u0,
+// (Core/idx2Decode.cpp:203-227), by one warp; u holds the negabinary coefficients, perm the
+// coefficient order (Core/Zfp.h:419 Perm3, :498 Perm2) in shared memory.
+__device__ __forceinline__ void reconstruct_block(double* F, long long* q, const uint8_t* perm3,
+                                                  const uint8_t* perm2, unsigned long long u0,
                                                   unsigned long long u1, int nd, int emax, uint64_t g,
-                                                  const int from[3], const int strd[3], int lane)
+                                                  int s, int is2d, int lane)
 {
   int d3[3], bd[3];
   unpack_geom(g, d3, bd);
   const int nv = 1 << (2 * nd);
+  auto perm = [&](int j) -> int { return nd == 3 ? (int)perm3[j] : (nd == 2 ? (int)perm2[j & 15] : j); };
   if (lane < nv)
-    q[dev::perm(nd, lane)] = (long long)((u0 ^ dev::kNegaMask) - dev::kNegaMask);
+    q[perm(lane)] = (long long)((u0 ^ dev::kNegaMask) - dev::kNegaMask);
   if (lane + 32 < nv)
-    q[dev::perm(nd, lane + 32)] = (long long)((u1 ^ dev::kNegaMask) - dev::kNegaMask);
+    q[perm(lane + 32)] = (long long)((u1 ^ dev::kNegaMask) - dev::kNegaMask);
   __syncwarp();
   dev::warp_inv_zfp(q, nd, lane);
-  const double scale = __ddiv_rn(1.0, dev::pow2(63 - nd - 1 - emax));
+  // 1 / 2^k, exactly as the division of 1 by pow2(k) rounds (0 once 2^k overflows)
+  const int k = 63 - nd - 1 - emax;
+  const double scale = k > 1023 ? 0.0 : dev::pow2(-k);
+  int hx, hy, hz;
+  if (is2d)
+  {
+    hx = (s >> 1) & 1;
+    hy = s & 1;
+    hz = 0;
+  }
+  else
+  {
+    hx = (s >> 2) & 1;
+    hy = (s >> 1) & 1;
+    hz = s & 1;
+  }
+  const int dx = 17 - hx, dy = 17 - hy;
+  double* base = F + sbm_base(hx, hy, hz, is2d);
   for (int j = lane; j < nv; j += 32)
   {
-    int x = j % bd[0], y = (j / bd[0]) % bd[1], z = j / (bd[0] * bd[1]);
-    F[((from[2] + (d3[2] + z) * strd[2]) * 33 + (from[1] + (d3[1] + y) * strd[1])) * 33 +
-      (from[0] + (d3[0] + x) * strd[0])] = __dmul_rn(scale, __ll2double_rn(q[j]));
+    // block dims are 4 or 1 per axis
+    const int x = bd[0] > 1 ? (j & 3) : 0;
+    const int r = bd[0] > 1 ? j >> 2 : j;
+    const int y = bd[1] > 1 ? (r & 3) : 0;
+    const int z = bd[1] > 1 ? r >> 2 : r;
+    base[((d3[2] + z) * dy + (d3[1] + y)) * dx + (d3[0] + x)] = __dmul_rn(scale, __ll2double_rn(q[j]));
   }
   __syncwarp();
 }
@@ -208,6 +284,24 @@ __device__ __forceinline__ void ilift33(double (&v)[33])
   v[31] = __dadd_rn(v[31], __dmul_rn(__dadd_rn(v[32], v[30]), 0.5));
 }
 
+// One inverse line over two dense streams (even samples at c0, odd at c1, compile-time stride
+// ST), with the de-normalisation weights of the two streams applied as they are loaded.
+template <int ST>
+__device__ __forceinline__ void ilift_streams(double* c0, double* c1, bool n0, double w0, bool n1, double w1)
+{
+  double v[33];
+#pragma unroll
+  for (int k = 0; k < 33; ++k)
+  {
+    const double f = (k & 1) ? c1[(k >> 1) * ST] : c0[(k >> 1) * ST];
+    v[k] = (k & 1) ? (n1 ? __dmul_rn(f, w1) : f) : (n0 ? __dmul_rn(f, w0) : f);
+  }
+  ilift33(v);
+#pragma unroll
+  for (int k = 0; k < 33; ++k)
+    ((k & 1) ? c1 : c0)[(k >> 1) * ST] = v[k];
+}
+
 __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -215,10 +309,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int N[3] = { 33, 33, a.is2d ? 1 : 33 };
   const int NB = N[0] * N[1] * N[2];
+  DEC_PHASE_INIT
+  if (tid < 64)
+    sm.perm3[tid] = dev::perm(3, tid);
+  if (tid < 16)
+    sm.perm2[tid] = dev::perm(2, tid);
 
   for (int bi = blockIdx.x; bi < a.nbricks; bi += gridDim.x)
   {
-    const decode_brick br = a.bricks[bi];
+    const decode_brick& br = a.bricks[bi];
+    DEC_PHASE_START
     double* F = a.is_output ? a.slots + (size_t)blockIdx.x * (size_t)NB
                             : a.bricks_out + (size_t)bi * (size_t)NB;
     // 1: zero + parent low band (Core/idx2Decode.cpp:285-293)
@@ -232,12 +332,13 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       for (int i = tid; i < 16 * 16 * nz; i += kThreads)
       {
         int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
-        int cz = a.is2d ? 0 : 2 * z;
-        F[(cz * 33 + 2 * y) * 33 + 2 * x] =
-          P[((br.pos[2] * nz + z) * 33 + (br.pos[1] * 16 + y)) * 33 + (br.pos[0] * 16 + x)];
+        // even positions of the child: its subband 0, dense
+        F[(z * 17 + y) * 17 + x] =
+          P[sbm(br.pos[0] * 16 + x, br.pos[1] * 16 + y, br.pos[2] * nz + z, a.is2d)];
       }
     }
 
+    DEC_PHASE(0)
     // 2: per-block state of every decoded subband
     for (int i = tid; i < a.nsb * kMaxBlocksPerSubband; i += kThreads)
     {
@@ -288,6 +389,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       sm.wide = wide;
     }
     __syncthreads();
+    DEC_PHASE(1)
 
     if (!sm.wide)
     {
@@ -366,7 +468,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
               u0 |= ((P >> lane) & 1ull) << bp;
               u1 |= ((P >> (lane + 32)) & 1ull) << bp;
             }
-            reconstruct_block(F, sm.q[warp], u0, u1, sm.nd[s][bc], sm.emax[s][bc], geom[bc], from, strd, lane);
+            reconstruct_block(F, sm.q[warp], sm.perm3, sm.perm2, u0, u1, sm.nd[s][bc], sm.emax[s][bc],
+                              geom[bc], s, a.is2d, lane);
           }
           __syncwarp();
         }
@@ -447,13 +550,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         {
           if (sm.nbps[s][b] == 0 || sm.bypass[s][b])
             continue;
-          reconstruct_block(F, sm.q[warp], sm.u.coef[b][lane], sm.u.coef[b][lane + 32], sm.nd[s][b], sm.emax[s][b],
-                            geom[b], from, strd, lane);
+          reconstruct_block(F, sm.q[warp], sm.perm3, sm.perm2, sm.u.coef[b][lane], sm.u.coef[b][lane + 32],
+                            sm.nd[s][b], sm.emax[s][b], geom[b], s, a.is2d, lane);
         }
         __syncthreads();
       }
     }
     __syncthreads();
+    DEC_PHASE(2)
 
     // 4: de-normalise + inverse CDF5/3 Z, Y, X (Core/Wavelet.cpp:144-203); the
     // de-normalisation is applied as the Z lines are loaded, the output crop and cast as the
@@ -463,83 +567,106 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       for (int li = tid; li < 33 * 33; li += kThreads)
       {
         const int x = li % 33, y = li / 33;
-        double v[33];
-#pragma unroll
-        for (int z = 0; z < 33; ++z)
-        {
-          const int s = ((x & 1) << 2) | ((y & 1) << 1) | (z & 1);
-          double f = F[(z * 33 + y) * 33 + x];
-          v[z] = ((a.norm_mask >> s) & 1) ? __dmul_rn(f, a.inv_weight[s]) : f;
-        }
-        ilift33(v);
-#pragma unroll
-        for (int z = 0; z < 33; ++z)
-          F[(z * 33 + y) * 33 + x] = v[z];
+        // even and odd z samples of the column: two dense streams of stride dx * dy
+        const int hx = x & 1, hy = y & 1, dx = 17 - hx, dy = 17 - hy;
+        const int off = (y >> 1) * dx + (x >> 1), sz = dx * dy;
+        double* c0 = F + sbm_base(hx, hy, 0, 0) + off;
+        double* c1 = F + sbm_base(hx, hy, 1, 0) + off;
+        const int s0 = (hx << 2) | (hy << 1), s1 = s0 | 1;
+        const bool n0 = (a.norm_mask >> s0) & 1, n1 = (a.norm_mask >> s1) & 1;
+        const double w0 = a.inv_weight[s0], w1 = a.inv_weight[s1];
+        if (sz == 17 * 17)
+          ilift_streams<17 * 17>(c0, c1, n0, w0, n1, w1);
+        else if (sz == 16 * 17)
+          ilift_streams<16 * 17>(c0, c1, n0, w0, n1, w1);
+        else
+          ilift_streams<16 * 16>(c0, c1, n0, w0, n1, w1);
       }
       __syncthreads();
+      DEC_PHASE(3)
     }
     for (int li = tid; li < 33 * N[2]; li += kThreads)
     {
       const int x = li % 33, z = li / 33;
-      double v[33];
-#pragma unroll
-      for (int y = 0; y < 33; ++y)
-      {
-        double f = F[(z * 33 + y) * 33 + x];
-        if (a.is2d)
-        {
-          const int s = ((x & 1) << 1) | (y & 1);
-          f = ((a.norm_mask >> s) & 1) ? __dmul_rn(f, a.inv_weight[s]) : f;
-        }
-        v[y] = f;
-      }
-      ilift33(v);
-#pragma unroll
-      for (int y = 0; y < 33; ++y)
-        F[(z * 33 + y) * 33 + x] = v[y];
+      // even and odd y samples of the line: two dense streams of stride dx
+      const int hx = x & 1, hz = z & 1, dx = 17 - hx;
+      double* c0 = F + sbm_base(hx, 0, hz, a.is2d) + (z >> 1) * dx * 17 + (x >> 1);
+      double* c1 = F + sbm_base(hx, 1, hz, a.is2d) + (z >> 1) * dx * 16 + (x >> 1);
+      const int s0 = a.is2d ? (hx << 1) : ((hx << 2) | hz), s1 = a.is2d ? (s0 | 1) : (s0 | 2);
+      const bool n0 = a.is2d && ((a.norm_mask >> s0) & 1), n1 = a.is2d && ((a.norm_mask >> s1) & 1);
+      const double w0 = a.inv_weight[s0], w1 = a.inv_weight[s1];
+      if (dx == 17)
+        ilift_streams<17>(c0, c1, n0, w0, n1, w1);
+      else
+        ilift_streams<16>(c0, c1, n0, w0, n1, w1);
     }
     __syncthreads();
-    for (int li = tid; li < 33 * N[2]; li += kThreads)
+    DEC_PHASE(4)
+    // X, warp-uniform iterations (the output rows are staged per warp and written back
+    // row by row, lanes along x)
+    for (int li0 = warp * 32; li0 < 33 * N[2]; li0 += kThreads)
     {
+      const int li = li0 + lane;
+      const bool active = li < 33 * N[2];
       const int y = li % 33, z = li / 33;
-      double v[33];
-      double* row = F + (z * 33 + y) * 33;
-#pragma unroll
-      for (int x = 0; x < 33; ++x)
-        v[x] = row[x];
-      ilift33(v);
-      if (!a.is_output)
+      // 5: output (Core/idx2Decode.cpp:431-442 CopyGridGrid): where this row goes, decided
+      // before the row is loaded (fewer live registers around the lift)
+      long long obase = -1;
+      if (a.is_output && active)
       {
-#pragma unroll
-        for (int x = 0; x < 33; ++x)
-          row[x] = v[x];
-      }
-      else
-      {
-        // 5: output (Core/idx2Decode.cpp:431-442 CopyGridGrid) for the samples of this row
         const int ry = y - br.src_from[1], rz = z - br.src_from[2];
         if (ry >= 0 && rz >= 0 && ry % br.src_strd[1] == 0 && rz % br.src_strd[2] == 0 &&
             ry / br.src_strd[1] < br.dims[1] && rz / br.src_strd[2] < br.dims[2])
         {
           const long long oy = br.dst_from[1] + (long long)(ry / br.src_strd[1]) * br.dst_strd[1];
           const long long oz = br.dst_from[2] + (long long)(rz / br.src_strd[2]) * br.dst_strd[2];
-          const long long obase = (oz * a.out_dims[1] + oy) * a.out_dims[0];
-#pragma unroll
-          for (int x = 0; x < 33; ++x)
-          {
-            const int rx = x - br.src_from[0];
-            if (rx >= 0 && rx % br.src_strd[0] == 0 && rx / br.src_strd[0] < br.dims[0])
-            {
-              const long long di = obase + br.dst_from[0] + (long long)(rx / br.src_strd[0]) * br.dst_strd[0];
-              if (a.out_f32)
-                ((float*)a.out)[di] = __double2float_rn(v[x]);
-              else
-                ((double*)a.out)[di] = v[x];
-            }
-          }
+          obase = (oz * a.out_dims[1] + oy) * a.out_dims[0] + br.dst_from[0];
         }
+      }
+      if (active && (!a.is_output || obase >= 0))
+      {
+        // even and odd x samples of the row: two dense runs
+        const int hy = y & 1, hz = z & 1, dy = 17 - hy;
+        double* r0 = F + sbm_base(0, hy, hz, a.is2d) + ((z >> 1) * dy + (y >> 1)) * 17;
+        double* r1 = F + sbm_base(1, hy, hz, a.is2d) + ((z >> 1) * dy + (y >> 1)) * 16;
+        double v[33];
+#pragma unroll
+        for (int x = 0; x < 33; ++x)
+          v[x] = (x & 1) ? r1[x >> 1] : r0[x >> 1];
+        ilift33(v);
+        double* dst = a.is_output ? sm.u.out.v[warp][lane] : nullptr;
+#pragma unroll
+        for (int x = 0; x < 33; ++x)
+        {
+          if (a.is_output)
+            dst[x] = v[x];
+          else
+            ((x & 1) ? r1 : r0)[x >> 1] = v[x];
+        }
+      }
+      if (a.is_output)
+      {
+        // the warp's rows, lanes along x
+        sm.u.out.base[warp][lane] = obase;
+        __syncwarp();
+        const int n0 = br.dims[0];
+        for (int r = 0; r < 32; ++r)
+        {
+          const long long ob = sm.u.out.base[warp][r];
+          if (ob < 0 || lane >= n0)
+            continue;
+          const long long di = ob + (long long)lane * br.dst_strd[0];
+          const double val = sm.u.out.v[warp][r][br.src_from[0] + lane * br.src_strd[0]];
+          if (a.out_f32)
+            ((float*)a.out)[di] = __double2float_rn(val);
+          else
+            ((double*)a.out)[di] = val;
+        }
+        __syncwarp();
       }
     }
     __syncthreads();
+    DEC_PHASE(5)
   }
+  DEC_PHASE_FLUSH
 }

@@ -31,7 +31,7 @@ namespace
 #ifdef IDX2G_PHASE_TIMING
 __device__ unsigned long long g_phase_cycles[16];
 #define ENC_PHASE_INIT \
-  long long ph_[12] = {};  \
+  long long ph_[16] = {};  \
   long long ph_t = 0;
 #define ENC_PHASE_START \
   if (threadIdx.x == 0) \
@@ -45,7 +45,7 @@ __device__ unsigned long long g_phase_cycles[16];
   }
 #define ENC_PHASE_FLUSH            \
   if (threadIdx.x == 0)            \
-    for (int k = 0; k < 12; ++k)   \
+    for (int k = 0; k < 16; ++k)   \
       atomicAdd(&g_phase_cycles[k], (unsigned long long)ph_[k]);
 #else
 #define ENC_PHASE_INIT
@@ -130,8 +130,10 @@ struct enc_smem
 
 inline size_t enc_smem_bytes(int planes)
 {
-  return ((sizeof(enc_smem) + 15) & ~(size_t)15) +
-         (size_t)planes * ((size_t)kRowX * 8 + (size_t)kRowOff * 2 + (size_t)kRowNin);
+  // the coding tables, which also hold the 17^3 even lattice during the transform
+  const size_t tables = (size_t)planes * ((size_t)kRowX * 8 + (size_t)kRowOff * 2 + (size_t)kRowNin);
+  const size_t lattice = (size_t)17 * 17 * 17 * 8;
+  return ((sizeof(enc_smem) + 15) & ~(size_t)15) + (tables > lattice ? tables : lattice);
 }
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
@@ -183,6 +185,25 @@ __device__ __forceinline__ double warp_max(double v)
     v = v < w ? w : v;
   }
   return v;
+}
+
+// L2 prefetch of the field rows a level-0 brick will gather.
+__device__ __forceinline__ void prefetch_rows(const enc_args& a, const enc_brick& b)
+{
+  const int vx = b.valid[0], vy = b.valid[1], vz = b.valid[2];
+  const int esz = a.field_f32 ? 4 : 8;
+  const long long gx0 = (long long)b.b3[0] * 32, gy0 = (long long)b.b3[1] * 32,
+                  gz0 = (long long)b.b3[2] * (a.is2d ? 1 : 32);
+  for (int r = threadIdx.x; r < vy * vz; r += blockDim.x)
+  {
+    const int y = r % vy, z = r / vy;
+    const char* p = (const char*)a.field + (((gz0 + z) * a.fdims[1] + gy0 + y) * a.fdims[0] + gx0) * esz;
+    const char* q = p + (size_t)vx * esz - 1;
+    for (const char* c = p; c <= q; c += 128)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(c));
+    if ((((uintptr_t)q) >> 7) != (((uintptr_t)p + (((uintptr_t)(q - p)) & ~(uintptr_t)127)) >> 7))
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(q));
+  }
 }
 
 // One zfp 4-point lifting line (Core/Zfp.h:145 FLift) on the padded per-block scratch:
@@ -241,7 +262,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
 
   for (int bi = blockIdx.x; bi < a.nbricks; bi += gridDim.x)
   {
-    const enc_brick br = a.bricks[bi];
+    const enc_brick& br = a.bricks[bi];
     ENC_PHASE_START
     // ---------------- A: gather ----------------
     if (a.level == 0)
@@ -325,26 +346,61 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       // extrapolation round trip (Core/Wavelet.cpp:68): forward on the valid dims, then the
       // inverse on the 33^3 grid except its last sweep (X at full resolution), which is fused
       // with the first sweep of the real transform below
+      // The sweeps from the second level on touch only the even positions: the forward
+      // sweeps of levels 2.. and the inverse ones back to level 2 run on the 17^3 even
+      // lattice copied into shared memory (the coding tables' space, idle here), lifted in
+      // place sample by sample.
+      double* S = reinterpret_cast<double*>(Xp);
+      const int NS[3] = { 17, 17, a.is2d ? 1 : 17 };
+      const int nsub = NS[0] * NS[1] * NS[2];
       if (tid == 0)
         dev::build_stack(br.valid, 5, a.order, &sm.stack);
       __syncthreads();
-      const int nf = sm.stack.n;
-      for (int i = 0; i < nf; ++i)
+      const int nf = sm.stack.n, cf = sm.stack.coarse;
+      for (int i = 0; i < cf; ++i)
       {
         dev::lift_sweep_regs<true>(F, N, sm.stack.g[i], sm.stack.axis[i]);
         __syncthreads();
+        if (i == 0)
+        {
+          ENC_PHASE(1)
+        }
       }
-      ENC_PHASE(1)
+      ENC_PHASE(2)
+      for (int i = tid; i < nsub; i += kThreads)
+      {
+        const int x = i % 17, y = (i / 17) % 17, z = i / 289;
+        S[i] = F[(2 * z * 33 + 2 * y) * 33 + 2 * x];
+      }
+      __syncthreads();
+      for (int i = cf; i < nf; ++i)
+      {
+        dev::lift_sweep(S, NS, dev::half_grid(sm.stack.g[i]), NS, sm.stack.axis[i], true);
+        __syncthreads();
+      }
+      ENC_PHASE(3)
       if (tid == 0)
         dev::build_stack(N, 5, a.order, &sm.stack);
       __syncthreads();
-      const int ni = sm.stack.n;
-      for (int i = ni - 1; i >= 1; --i)
+      const int ni = sm.stack.n, ci = sm.stack.coarse;
+      for (int i = ni - 1; i >= ci; --i)
+      {
+        dev::lift_sweep(S, NS, dev::half_grid(sm.stack.g[i]), NS, sm.stack.axis[i], false);
+        __syncthreads();
+      }
+      for (int i = tid; i < nsub; i += kThreads)
+      {
+        const int x = i % 17, y = (i / 17) % 17, z = i / 289;
+        F[(2 * z * 33 + 2 * y) * 33 + 2 * x] = S[i];
+      }
+      __syncthreads();
+      ENC_PHASE(4)
+      for (int i = ci - 1; i >= 1; --i)
       {
         dev::lift_sweep_regs<false>(F, N, sm.stack.g[i], sm.stack.axis[i]);
         __syncthreads();
       }
-      ENC_PHASE(2)
+      ENC_PHASE(5)
       // inverse X (D = 33) then forward X of the one-level transform (Core/Wavelet.cpp:81)
       for (int li = tid; li < 33 * N[2]; li += kThreads)
       {
@@ -360,7 +416,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
           row[k] = v[k];
       }
       __syncthreads();
-      ENC_PHASE(3)
+      ENC_PHASE(6)
       // forward Y, and forward Z; subband normalisation applied as the last sweep stores
       // (Core/Wavelet.cpp:111-137)
       for (int li = tid; li < 33 * N[2]; li += kThreads)
@@ -385,7 +441,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         }
       }
       __syncthreads();
-      ENC_PHASE(4)
+      ENC_PHASE(7)
       if (!a.is2d)
       {
         for (int li = tid; li < 33 * 33; li += kThreads)
@@ -407,7 +463,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         __syncthreads();
       }
     }
-    ENC_PHASE(5)
+    ENC_PHASE(8)
 
     // ---------------- C: low band to the parent ----------------
     if (a.parent_bricks && br.parent >= 0)
@@ -422,11 +478,14 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
                F[(cz * 33 + 2 * y) * 33 + 2 * x]);
       }
     }
-    ENC_PHASE(6)
+    ENC_PHASE(9)
 
     // ---------------- D: block coding per subband ----------------
     for (int s = 0; s < a.nsb; ++s)
     {
+      // towards the end of the brick, ask L2 for the rows of this CTA's next brick
+      if (a.level == 0 && s == (a.nsb * 5) / 8 && bi + (int)gridDim.x < a.nbricks)
+        prefetch_rows(a, a.bricks[bi + gridDim.x]);
       int from[3], dims[3], strd[3];
       subband_grid(a.is2d, s, from, dims, strd);
       const int nb = a.nblocks[s];
@@ -609,7 +668,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         cB = nB;
       }
       __syncthreads();
-      ENC_PHASE(7)
+      ENC_PHASE(10)
 
       // key range of the subband
       if (warp == 0)
@@ -647,7 +706,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       __syncthreads();
       const int kmin = sm.kmin, kmax = sm.kmax;
       const int nkeys = sm.ok ? kmax - kmin + 1 : 0;
-      ENC_PHASE(8)
+      ENC_PHASE(11)
 
       // D3: per channel key (a warp each), bit offsets of the blocks in Morton order: an
       // exclusive scan of the plane lengths, in place
@@ -676,7 +735,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
           sm.key_bits[t] = carry;
       }
       __syncthreads();
-      ENC_PHASE(9)
+      ENC_PHASE(12)
 
       // D4: channel byte bases and the region of this (brick, subband)
       // (regions are whole 32-bit words so every CTA owns the words it writes)
@@ -726,7 +785,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       const unsigned alloc = sm.alloc;
       const unsigned hdr = sm.hdr;
       const bool fits = region + alloc <= a.cap_bytes;
-      ENC_PHASE(10)
+      ENC_PHASE(13)
 
       // D5: the plane codes, built in registers and ORed into shared memory when the region
       // is small enough, else straight into the (zeroed) global region; then the region is
@@ -771,7 +830,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         }
       }
       __syncthreads();
-      ENC_PHASE(11)
+      ENC_PHASE(14)
     }
   }
   ENC_PHASE_FLUSH
