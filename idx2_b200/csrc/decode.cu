@@ -111,7 +111,7 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
       return OutOfMemory;
   }
   cudaMemsetAsync(d_out, 0, out_bytes, st);
-  int* d_err = (int*)ctx->ws("dec.err", 16);
+  int* d_err = (int*)ctx->ws("dec.err", 16);  // [0] brick kernel, [1] plane kernel
   uint64_t* d_geom = (uint64_t*)ctx->ws("dec.geom", sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
   if (!d_err || !d_geom)
   {
@@ -176,6 +176,122 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
     a.out_dims[1] = rq.out_dims.y;
     a.out_dims[2] = rq.out_dims.z;
     a.error = d_err;
+
+    // bit planes of every (brick, subband) of the level: one warp each, tables allocated
+    // with a cursor in a grow-only workspace (relaunched larger if it overflows)
+    const size_t nunits = (size_t)nbr * (size_t)rq.nsb;
+    unsigned long long* d_uoff = (unsigned long long*)ctx->ws("dec.unitoff", nunits * 8);
+    unsigned long long* d_pcur = (unsigned long long*)ctx->ws("dec.pcursor", 16);
+    int* d_wide = (int*)ctx->ws("dec.widelist", nunits * 4);
+    if (!d_uoff || !d_pcur || !d_wide)
+    {
+      cleanup();
+      return OutOfMemory;
+    }
+    unsigned long long cap = (unsigned long long)nunits * 16384ull + (16ull << 20);
+    if (ctx->ws_size("dec.planes") > cap)
+      cap = ctx->ws_size("dec.planes");
+    dec1_args pa;
+    memset(&pa, 0, sizeof pa);
+    pa.nsb = rq.nsb;
+    pa.nbricks = nbr;
+    pa.etol = rq.etol;
+    pa.end_bp = a.end_bp;
+    pa.mask = lv.mask;
+    memcpy(pa.nblocks, lv.nblocks, sizeof pa.nblocks);
+    pa.geom = d_geom;
+    pa.bricks = d_bricks;
+    pa.exps = exps_;
+    pa.ckmin = kmin_;
+    pa.cn = n_;
+    pa.cfirst = first_;
+    pa.coff = off_;
+    pa.blob = blob_;
+    pa.blob_bytes = blob_bytes_;
+    pa.cursor = d_pcur;
+    pa.unit_off = d_uoff;
+    pa.error = d_err + 1;
+    pa.wide_count = (int*)(d_pcur + 1);
+    pa.wide_list = d_wide;
+    const int pgrid = (int)((nunits + kPlaneWarps - 1) / kPlaneWarps);
+    float level_ms = 0;
+    for (int attempt = 0; attempt < 3; ++attempt)
+    {
+      unsigned long long* d_planes = (unsigned long long*)ctx->ws("dec.planes", (size_t)cap);
+      if (!d_planes)
+      {
+        cleanup();
+        return OutOfMemory;
+      }
+      cap = ctx->ws_size("dec.planes");
+      pa.planes = d_planes;
+      pa.cap_bytes = cap;
+      cudaMemsetAsync(d_pcur, 0, 16, st);
+      cudaMemsetAsync(d_err + 1, 0, 4, st);
+      cudaEventRecord(e0, st);
+      k_decode_planes<false><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
+      cudaEventRecord(e1, st);
+      if (cudaGetLastError() != cudaSuccess)
+      {
+        cleanup();
+        return CudaError;
+      }
+      unsigned long long pc[2] = { 0, 0 };
+      cudaMemcpyAsync(pc, d_pcur, 16, cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess)
+      {
+        cleanup();
+        return CudaError;
+      }
+      float pms = 0;
+      cudaEventElapsedTime(&pms, e0, e1);
+      level_ms += pms;
+      const int nwide = (int)(pc[1] & 0xffffffffu);
+      if (nwide > 0)
+      {
+        // units of more than 32 channels
+        cudaEventRecord(e0, st);
+        k_decode_planes<true><<<(nwide + kPlaneWarps - 1) / kPlaneWarps, kPlaneWarps * 32, 0, st>>>(pa);
+        cudaEventRecord(e1, st);
+        if (cudaGetLastError() != cudaSuccess)
+        {
+          cleanup();
+          return CudaError;
+        }
+      }
+      int perr = 0;
+      unsigned long long used = 0;
+      cudaMemcpyAsync(&perr, d_err + 1, 4, cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(&used, d_pcur, 8, cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess)
+      {
+        cleanup();
+        return CudaError;
+      }
+      if (nwide > 0)
+      {
+        cudaEventElapsedTime(&pms, e0, e1);
+        level_ms += pms;
+      }
+      if (perr == 1)
+      {
+        cleanup();
+        return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
+      }
+      if (perr == 2)
+      {
+        cap = used + (1ull << 20);
+        continue;
+      }
+      a.planes = d_planes;
+      a.unit_off = d_uoff;
+      break;
+    }
+    if (!a.planes)
+    {
+      cleanup();
+      return DeviceStreamOverflow;
+    }
     cudaEventRecord(e0, st);
     k_decode_level<<<grid, kThreads, smem, st>>>(a);
     cudaEventRecord(e1, st);
@@ -191,7 +307,7 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
     }
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    total_ms += ms;
+    total_ms += ms + level_ms;
     prev = d_level;
     if (lv.is_output)
       break;

@@ -55,6 +55,32 @@ struct dec_args
   void* out;
   int out_dims[3];
   int* error;
+  // decoded bit planes from k_decode_planes (null: the kernel runs the wavefront itself)
+  const unsigned long long* planes;
+  const unsigned long long* unit_off;  // [brick][subband] byte offset of the unit's table, ~0: none
+};
+
+// Arguments of the bit-plane kernel (one warp per (brick, subband) unit).
+struct dec1_args
+{
+  int nsb, nbricks, etol, end_bp, mask;
+  int nblocks[8];
+  const uint64_t* geom;  // [8][kMaxBlocksPerSubband]
+  const decode_brick* bricks;
+  const int16_t* exps;
+  const int32_t* ckmin;
+  const int32_t* cn;
+  const unsigned long long* cfirst;
+  const unsigned long long* coff;
+  const uint8_t* blob;
+  unsigned long long blob_bytes;
+  unsigned long long* planes;       // tables, allocated with the cursor
+  unsigned long long cap_bytes;
+  unsigned long long* cursor;
+  unsigned long long* unit_off;
+  int* error;                       // 1: too many channels, 2: table capacity exceeded
+  int* wide_count;                  // units with more than 32 channels, deferred by the first pass
+  int* wide_list;
 };
 
 struct dec_smem
@@ -284,6 +310,198 @@ __device__ __forceinline__ void ilift33(double (&v)[33])
   v[31] = __dadd_rn(v[31], __dmul_rn(__dadd_rn(v[32], v[30]), 0.5));
 }
 
+// ---------------------------------------------------------------------------
+// Bit planes of one (brick, subband): the wavefront of the group-test decoder alone
+// (Core/idx2Decode.cpp:141-202). Channel c = kmax - key is owned by lane c % 32 (G groups of
+// 32 channels); at step t it decodes its plane of block t - c, taking the block's significance
+// count from channel c - 1 at step t - 1. The plane masks of step t are stored as row t of the
+// unit's table (row length nkeys): block b's plane in channel c is row b + c, column c.
+// ---------------------------------------------------------------------------
+constexpr int kPlaneWarps = 8;
+
+struct plane_smem
+{
+  int16_t ktop[kPlaneWarps][kMaxBlocksPerSubband];
+  uint8_t np[kPlaneWarps][kMaxBlocksPerSubband];
+  uint8_t nvl[kPlaneWarps][kMaxBlocksPerSubband];
+};
+
+template <int G>
+__device__ __forceinline__ void plane_wavefront(const dec1_args& a, size_t fs, int nb, int nkeys, int kmax,
+                                                const int16_t* ktop, const uint8_t* npl, const uint8_t* nvl,
+                                                unsigned long long* T, int lane)
+{
+  bit_reader rd[G];
+  bool has[G];
+  int n_out[G], stop_out[G];
+  const int ck = a.ckmin[fs], cn = a.cn[fs];
+  const unsigned long long cf = a.cfirst[fs];
+#pragma unroll
+  for (int g = 0; g < G; ++g)
+  {
+    const int c = 32 * g + lane, key = kmax - c;
+    has[g] = false;
+    n_out[g] = 0;
+    stop_out[g] = 0;
+    if (c < nkeys && key >= ck && key < ck + cn)
+    {
+      const unsigned long long o = a.coff[cf + (unsigned long long)(key - ck)];
+      if (o != ~0ull)
+      {
+        rd[g].init(a.blob, a.blob_bytes, o * 8ull);
+        has[g] = true;
+      }
+    }
+  }
+  const int steps = nb + nkeys - 1;
+  for (int t = 0; t < steps; ++t)
+  {
+    int nl[G], sl[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+    {
+      nl[g] = __shfl_up_sync(0xffffffffu, n_out[g], 1);
+      sl[g] = __shfl_up_sync(0xffffffffu, stop_out[g], 1);
+      if (g > 0)
+      {
+        const int x = __shfl_sync(0xffffffffu, n_out[g - 1], 31);
+        const int y = __shfl_sync(0xffffffffu, stop_out[g - 1], 31);
+        if (lane == 0)
+        {
+          nl[g] = x;
+          sl[g] = y;
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+    {
+      const int c = 32 * g + lane, b = t - c;
+      unsigned long long X = 0;
+      n_out[g] = 0;
+      stop_out[g] = 0;
+      if (c < nkeys && b >= 0 && b < nb)
+      {
+        const int top = ktop[b], np = npl[b], key = kmax - c;
+        if (np > 0 && key <= top && key > top - np)
+        {
+          int n = key == top ? 0 : nl[g];
+          const int stopped = key == top ? 0 : sl[g];
+          if (stopped || !has[g])
+          {
+            stop_out[g] = 1;
+            n_out[g] = n;
+          }
+          else
+          {
+            X = decode_plane(rd[g], n, 1 << nvl[b]);
+            n_out[g] = n;
+          }
+        }
+      }
+      if (c < nkeys)
+        T[(size_t)t * (size_t)nkeys + (size_t)c] = X;
+    }
+  }
+}
+
+// WIDE = false: every unit, those of up to 32 channels decoded at once (few registers, many
+// warps per SM), the others listed; WIDE = true: the listed units (up to kKeyWindow channels).
+template <bool WIDE>
+__global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_planes(const dec1_args a)
+{
+  __shared__ plane_smem sm;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nunits = WIDE ? *a.wide_count : a.nbricks * a.nsb;
+  for (int i = blockIdx.x * kPlaneWarps + warp; i < nunits; i += gridDim.x * kPlaneWarps)
+  {
+    const int unit = WIDE ? a.wide_list[i] : i;
+    const int bi = unit / a.nsb, s = unit - bi * a.nsb;
+    if (!((a.mask >> s) & 1))
+    {
+      if (lane == 0)
+        a.unit_off[unit] = ~0ull;
+      continue;
+    }
+    const int nb = a.nblocks[s];
+    const size_t fs = (size_t)a.bricks[bi].flat * (size_t)a.nsb + (size_t)s;
+    int16_t* ktop = sm.ktop[warp];
+    uint8_t* npl = sm.np[warp];
+    uint8_t* nvl = sm.nvl[warp];
+    int kmin = 1 << 30, kmax = -(1 << 30);
+    for (int b = lane; b < nb; b += 32)
+    {
+      int d3[3], bd[3];
+      unpack_geom(a.geom[(size_t)s * kMaxBlocksPerSubband + b], d3, bd);
+      const int emax = a.exps[fs * kMaxBlocksPerSubband + (size_t)b];
+      const int np = dev::coded_planes(emax, a.etol, a.end_bp);
+      const int top = emax + 63 + 1024;
+      ktop[b] = (int16_t)top;
+      npl[b] = (uint8_t)np;
+      nvl[b] = (uint8_t)(2 * ((bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1)));
+      if (np)
+      {
+        kmax = top > kmax ? top : kmax;
+        kmin = top - np + 1 < kmin ? top - np + 1 : kmin;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+      const int x = __shfl_xor_sync(0xffffffffu, kmax, o), y = __shfl_xor_sync(0xffffffffu, kmin, o);
+      kmax = x > kmax ? x : kmax;
+      kmin = y < kmin ? y : kmin;
+    }
+    __syncwarp();
+    int nkeys = kmax >= kmin ? kmax - kmin + 1 : 0;
+    if (nkeys > kKeyWindow)
+    {
+      if (lane == 0)
+        atomicExch(a.error, 1);
+      nkeys = 0;
+    }
+    if (nkeys == 0)
+    {
+      if (lane == 0)
+        a.unit_off[unit] = ~0ull;
+      continue;
+    }
+    if (!WIDE && nkeys > 32)
+    {
+      if (lane == 0)
+        a.wide_list[atomicAdd(a.wide_count, 1)] = unit;
+      continue;
+    }
+    const unsigned long long bytes = (unsigned long long)(nb + nkeys - 1) * (unsigned long long)nkeys * 8ull;
+    unsigned long long base = 0;
+    if (lane == 0)
+      base = atomicAdd(a.cursor, bytes);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base + bytes > a.cap_bytes)
+    {
+      if (lane == 0)
+      {
+        atomicExch(a.error, 2);
+        a.unit_off[unit] = ~0ull;
+      }
+      continue;
+    }
+    if (lane == 0)
+      a.unit_off[unit] = base;
+    unsigned long long* T = a.planes + base / 8;
+    if (!WIDE)
+      plane_wavefront<1>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+    else if (nkeys <= 32)
+      plane_wavefront<1>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+    else if (nkeys <= 64)
+      plane_wavefront<2>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+    else if (nkeys <= 96)
+      plane_wavefront<3>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+    else
+      plane_wavefront<4>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+    __syncwarp();
+  }
+}
+
 // One inverse line over two dense streams (even samples at c0, odd at c1, compile-time stride
 // ST), with the de-normalisation weights of the two streams applied as they are loaded.
 template <int ST>
@@ -391,7 +609,45 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
     __syncthreads();
     DEC_PHASE(1)
 
-    if (!sm.wide)
+    if (a.planes)
+    {
+      // 3: blocks rebuilt from the decoded planes (k_decode_planes), a warp per block
+      for (int s = 0; s < a.nsb; ++s)
+      {
+        if (!((a.mask >> s) & 1) || sm.nkeys[s] == 0)
+          continue;
+        const unsigned long long uo = a.unit_off[(size_t)bi * (size_t)a.nsb + (size_t)s];
+        if (uo == ~0ull)
+          continue;
+        const unsigned long long* T = a.planes + uo / 8;
+        const int nb = a.nblocks[s], nkeys = sm.nkeys[s], kmax = sm.kmax[s];
+        const uint64_t* geom = a.geom + (size_t)s * kMaxBlocksPerSubband;
+        for (int b = warp; b < nb; b += kWarps)
+        {
+          const int np = sm.np[s][b];
+          if (!np || sm.bypass[s][b])
+            continue;
+          const int c0 = kmax - sm.ktop[s][b];
+          // plane k of the block (bit plane 63 - k) is in channel c0 + k, table row b + c0 + k
+          const int k0 = lane, k1 = lane + 32;
+          const unsigned long long x0 =
+            (k0 < np && c0 + k0 < nkeys) ? T[(size_t)(b + c0 + k0) * (size_t)nkeys + (size_t)(c0 + k0)] : 0ull;
+          const unsigned long long x1 =
+            (k1 < np && c0 + k1 < nkeys) ? T[(size_t)(b + c0 + k1) * (size_t)nkeys + (size_t)(c0 + k1)] : 0ull;
+          unsigned long long u0 = 0, u1 = 0;
+          for (int k = 0; k < np; ++k)
+          {
+            const unsigned long long P = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, k & 31);
+            const int bp = 63 - k;
+            u0 |= ((P >> lane) & 1ull) << bp;
+            u1 |= ((P >> (lane + 32)) & 1ull) << bp;
+          }
+          reconstruct_block(F, sm.q[warp], sm.perm3, sm.perm2, u0, u1, sm.nd[s][b], sm.emax[s][b], geom[b], s,
+                            a.is2d, lane);
+        }
+      }
+    }
+    else if (!sm.wide)
     {
       // 3a: warp w decodes subband w. Lane j owns channel (kmax - j); at step t it decodes
       // that plane of block t - j, taking the block's significance count from lane j - 1 of
