@@ -451,9 +451,9 @@ __device__ __forceinline__ void fwd_lift4_at(long long* p0, long long* p1, long 
 
 __device__ __forceinline__ void fwd_lift4(long long* p, int s) { fwd_lift4_at(p, p + s, p + 2 * s, p + 3 * s); }
 
-__device__ __forceinline__ void inv_lift4(long long* p, int s)
+__device__ __forceinline__ void inv_lift4_at(long long* p0, long long* p1, long long* p2, long long* p3)
 {
-  long long x = p[0], y = p[s], z = p[2 * s], w = p[3 * s];
+  long long x = *p0, y = *p1, z = *p2, w = *p3;
   y += w >> 1;
   w -= y >> 1;
   y += w;
@@ -468,10 +468,27 @@ __device__ __forceinline__ void inv_lift4(long long* p, int s)
   w += x;
   x = (long long)((unsigned long long)x << 1);
   x -= w;
-  p[0] = x;
-  p[s] = y;
-  p[2 * s] = z;
-  p[3 * s] = w;
+  *p0 = x;
+  *p1 = y;
+  *p2 = z;
+  *p3 = w;
+}
+
+__device__ __forceinline__ void inv_lift4(long long* p, int s) { inv_lift4_at(p, p + s, p + 2 * s, p + 3 * s); }
+
+// 32 x 32 bit-matrix transpose across a warp: lane r holds row r; afterwards lane c holds
+// column c (bit r of the result = bit c of row r). Five exchange rounds of halving blocks.
+__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane)
+{
+  const uint32_t m[5] = { 0x0000ffffu, 0x00ff00ffu, 0x0f0f0f0fu, 0x33333333u, 0x55555555u };
+#pragma unroll
+  for (int i = 0; i < 5; ++i)
+  {
+    const int j = 16 >> i;
+    const uint32_t y = __shfl_xor_sync(0xffffffffu, x, j);
+    x = (lane & j) ? ((x & ~m[i]) | ((y & ~m[i]) >> j)) : ((x & m[i]) | ((y & m[i]) << j));
+  }
+  return x;
 }
 
 // Warp-cooperative forward zfp transform of one block held in shared memory

@@ -95,7 +95,7 @@ struct dec_smem
       long long base[kWarps][32];   // their offsets in the output (-1: no output)
     } out;
   } u;
-  long long q[kWarps][64];
+  long long q[kWarps][2][80];  // per-warp block scratch (two blocks, padded in the table path)
   int16_t emax[8][kMaxBlocksPerSubband];
   int16_t ktop[8][kMaxBlocksPerSubband];
   uint8_t np[8][kMaxBlocksPerSubband];
@@ -286,6 +286,16 @@ __device__ __forceinline__ void reconstruct_block(double* F, long long* q, const
     base[((d3[2] + z) * dy + (d3[1] + y)) * dx + (d3[0] + x)] = __dmul_rn(scale, __ll2double_rn(q[j]));
   }
   __syncwarp();
+}
+
+// Per-block zfp scratch with one padding word after every 4 (conflict-free 4-point passes).
+__device__ __forceinline__ int qpad(int i) { return i + (i >> 2); }
+
+// One inverse zfp 4-point line (Core/Zfp.h:181 ILift) on the padded scratch: elements
+// i, i + s, i + 2s, i + 3s of the block.
+__device__ __forceinline__ void ilift4_padded(long long* q, int i, int s)
+{
+  dev::inv_lift4_at(q + qpad(i), q + qpad(i + s), q + qpad(i + 2 * s), q + qpad(i + 3 * s));
 }
 
 // One-level inverse CDF5/3 of a 33-sample line held in registers (Core/Wavelet.h:250
@@ -622,28 +632,144 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         const unsigned long long* T = a.planes + uo / 8;
         const int nb = a.nblocks[s], nkeys = sm.nkeys[s], kmax = sm.kmax[s];
         const uint64_t* geom = a.geom + (size_t)s * kMaxBlocksPerSubband;
-        for (int b = warp; b < nb; b += kWarps)
+        int hx, hy, hz;
+        if (a.is2d)
         {
+          hx = (s >> 1) & 1;
+          hy = s & 1;
+          hz = 0;
+        }
+        else
+        {
+          hx = (s >> 2) & 1;
+          hy = (s >> 1) & 1;
+          hz = s & 1;
+        }
+        const int dx = 17 - hx, dy = 17 - hy;
+        double* const sbase = F + sbm_base(hx, hy, hz, a.is2d);
+        // plane k of block b (bit plane 63 - k) is in channel c0 + k, table row b + c0 + k;
+        // blocks with nothing to decode (no planes, or not part of the request) stay zero
+        auto load_planes = [&](int b, unsigned long long& x0, unsigned long long& x1) {
+          x0 = 0;
+          x1 = 0;
+          if (b >= nb)
+            return;
           const int np = sm.np[s][b];
           if (!np || sm.bypass[s][b])
-            continue;
+            return;
           const int c0 = kmax - sm.ktop[s][b];
-          // plane k of the block (bit plane 63 - k) is in channel c0 + k, table row b + c0 + k
-          const int k0 = lane, k1 = lane + 32;
-          const unsigned long long x0 =
-            (k0 < np && c0 + k0 < nkeys) ? T[(size_t)(b + c0 + k0) * (size_t)nkeys + (size_t)(c0 + k0)] : 0ull;
-          const unsigned long long x1 =
-            (k1 < np && c0 + k1 < nkeys) ? T[(size_t)(b + c0 + k1) * (size_t)nkeys + (size_t)(c0 + k1)] : 0ull;
-          unsigned long long u0 = 0, u1 = 0;
-          for (int k = 0; k < np; ++k)
+          if (lane < np && c0 + lane < nkeys)
+            x0 = T[(size_t)(b + c0 + lane) * (size_t)nkeys + (size_t)(c0 + lane)];
+          if (lane + 32 < np && c0 + lane + 32 < nkeys)
+            x1 = T[(size_t)(b + c0 + lane + 32) * (size_t)nkeys + (size_t)(c0 + lane + 32)];
+        };
+        // coefficient bit vectors from plane masks: lane l gets bit l (u0) and bit l + 32 (u1)
+        // of every plane, plane k at bit 63 - k
+        auto transpose = [&](unsigned long long x0, unsigned long long x1, bool two,
+                             unsigned long long& u0, unsigned long long& u1) {
+          u0 = (unsigned long long)__brev(dev::warp_transpose32((uint32_t)x0, lane)) << 32;
+          u1 = (unsigned long long)__brev(dev::warp_transpose32((uint32_t)(x0 >> 32), lane)) << 32;
+          if (two)
           {
-            const unsigned long long P = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, k & 31);
-            const int bp = 63 - k;
-            u0 |= ((P >> lane) & 1ull) << bp;
-            u1 |= ((P >> (lane + 32)) & 1ull) << bp;
+            u0 |= __brev(dev::warp_transpose32((uint32_t)x1, lane));
+            u1 |= __brev(dev::warp_transpose32((uint32_t)(x1 >> 32), lane));
           }
-          reconstruct_block(F, sm.q[warp], sm.perm3, sm.perm2, u0, u1, sm.nd[s][b], sm.emax[s][b], geom[b], s,
-                            a.is2d, lane);
+        };
+        const int npairs = (nb + 1) >> 1;
+        unsigned long long cA0 = 0, cA1 = 0, cB0 = 0, cB1 = 0;
+        if (warp < npairs)
+        {
+          load_planes(2 * warp, cA0, cA1);
+          load_planes(2 * warp + 1, cB0, cB1);
+        }
+        for (int pr = warp; pr < npairs; pr += kWarps)
+        {
+          // the next pair's plane masks are loaded while this pair is rebuilt
+          unsigned long long nA0 = 0, nA1 = 0, nB0 = 0, nB1 = 0;
+          if (pr + kWarps < npairs)
+          {
+            load_planes(2 * (pr + kWarps), nA0, nA1);
+            load_planes(2 * (pr + kWarps) + 1, nB0, nB1);
+          }
+          const int bA = 2 * pr, bB = 2 * pr + 1;
+          const bool hasB = bB < nb;
+          const bool actA = sm.np[s][bA] > 0 && !sm.bypass[s][bA];
+          const bool actB = hasB && sm.np[s][bB] > 0 && !sm.bypass[s][bB];
+          const int npA = sm.np[s][bA], npB = hasB ? sm.np[s][bB] : 0;
+          unsigned long long uA0, uA1, uB0, uB1;
+          transpose(cA0, cA1, npA > 32, uA0, uA1);
+          transpose(cB0, cB1, npB > 32, uB0, uB1);
+          const int ndA = sm.nd[s][bA], ndB = hasB ? sm.nd[s][bB] : 0;
+          const int nvA = actA ? 1 << (2 * ndA) : 0, nvB = actB ? 1 << (2 * ndB) : 0;
+          long long* qA = sm.q[warp][0];
+          long long* qB = sm.q[warp][1];
+          auto permj = [&](int nd, int j) -> int {
+            return nd == 3 ? (int)sm.perm3[j] : (nd == 2 ? (int)sm.perm2[j & 15] : j);
+          };
+          // inverse shuffle (Core/Zfp.h:520 InverseShuffle): negabinary to two's complement
+          if (lane < nvA)
+            qA[qpad(permj(ndA, lane))] = (long long)((uA0 ^ dev::kNegaMask) - dev::kNegaMask);
+          if (lane + 32 < nvA)
+            qA[qpad(permj(ndA, lane + 32))] = (long long)((uA1 ^ dev::kNegaMask) - dev::kNegaMask);
+          if (lane < nvB)
+            qB[qpad(permj(ndB, lane))] = (long long)((uB0 ^ dev::kNegaMask) - dev::kNegaMask);
+          if (lane + 32 < nvB)
+            qB[qpad(permj(ndB, lane + 32))] = (long long)((uB1 ^ dev::kNegaMask) - dev::kNegaMask);
+          __syncwarp();
+          // inverse zfp (Core/Zfp.h:287): block A on lanes 0-15, block B on lanes 16-31
+          {
+            const int h = lane >> 4, l = lane & 15;
+            const unsigned hm = h ? 0xffff0000u : 0x0000ffffu;
+            long long* q = h ? qB : qA;
+            const int nd = h ? (actB ? ndB : 0) : (actA ? ndA : 0);
+            if (nd == 3)
+            {
+              ilift4_padded(q, (l & 3) + 4 * (l >> 2), 16);
+              __syncwarp(hm);
+              ilift4_padded(q, 16 * (l & 3) + (l >> 2), 4);
+              __syncwarp(hm);
+              ilift4_padded(q, 4 * (l & 3) + 16 * (l >> 2), 1);
+            }
+            else if (nd == 2)
+            {
+              if (l < 4)
+                ilift4_padded(q, l, 4);
+              __syncwarp(hm);
+              if (l < 4)
+                ilift4_padded(q, 4 * l, 1);
+            }
+            else if (nd == 1)
+            {
+              if (l == 0)
+                ilift4_padded(q, 0, 1);
+            }
+            __syncwarp();
+          }
+          // dequantise (Core/Zfp.h Dequantize) and store into the subband
+          auto store_block = [&](int b, long long* q, int nd, int nv) {
+            int d3[3], bd[3];
+            unpack_geom(geom[b], d3, bd);
+            const int k = 63 - nd - 1 - sm.emax[s][b];
+            const double scale = k > 1023 ? 0.0 : dev::pow2(-k);
+            for (int j = lane; j < nv; j += 32)
+            {
+              const int x = bd[0] > 1 ? (j & 3) : 0;
+              const int r = bd[0] > 1 ? j >> 2 : j;
+              const int y = bd[1] > 1 ? (r & 3) : 0;
+              const int z = bd[1] > 1 ? r >> 2 : r;
+              sbase[((d3[2] + z) * dy + (d3[1] + y)) * dx + (d3[0] + x)] =
+                __dmul_rn(scale, __ll2double_rn(q[qpad(j)]));
+            }
+          };
+          if (actA)
+            store_block(bA, qA, ndA, nvA);
+          if (actB)
+            store_block(bB, qB, ndB, nvB);
+          __syncwarp();
+          cA0 = nA0;
+          cA1 = nA1;
+          cB0 = nB0;
+          cB1 = nB1;
         }
       }
     }
@@ -724,7 +850,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
               u0 |= ((P >> lane) & 1ull) << bp;
               u1 |= ((P >> (lane + 32)) & 1ull) << bp;
             }
-            reconstruct_block(F, sm.q[warp], sm.perm3, sm.perm2, u0, u1, sm.nd[s][bc], sm.emax[s][bc],
+            reconstruct_block(F, sm.q[warp][0], sm.perm3, sm.perm2, u0, u1, sm.nd[s][bc], sm.emax[s][bc],
                               geom[bc], s, a.is2d, lane);
           }
           __syncwarp();
@@ -806,7 +932,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         {
           if (sm.nbps[s][b] == 0 || sm.bypass[s][b])
             continue;
-          reconstruct_block(F, sm.q[warp], sm.perm3, sm.perm2, sm.u.coef[b][lane], sm.u.coef[b][lane + 32],
+          reconstruct_block(F, sm.q[warp][0], sm.perm3, sm.perm2, sm.u.coef[b][lane], sm.u.coef[b][lane + 32],
                             sm.nd[s][b], sm.emax[s][b], geom[b], s, a.is2d, lane);
         }
         __syncthreads();
