@@ -145,6 +145,8 @@ IDX2G_API int idx2g_ctx_create(int device, void* stream, idx2g_ctx** out)
   return NoError;
 }
 
+IDX2G_API long long idx2g_ctx_launches(const idx2g_ctx* c) { return c ? c->d.launches : 0; }
+
 IDX2G_API int idx2g_ctx_destroy(idx2g_ctx* c)
 {
   if (!c)

@@ -230,6 +230,7 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
       cudaMemsetAsync(d_err + 1, 0, 4, st);
       cudaEventRecord(e0, st);
       k_decode_planes<false><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
+      ++ctx->launches;
       cudaEventRecord(e1, st);
       if (cudaGetLastError() != cudaSuccess)
       {
@@ -252,6 +253,7 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
         // units of more than 32 channels
         cudaEventRecord(e0, st);
         k_decode_planes<true><<<(nwide + kPlaneWarps - 1) / kPlaneWarps, kPlaneWarps * 32, 0, st>>>(pa);
+        ++ctx->launches;
         cudaEventRecord(e1, st);
         if (cudaGetLastError() != cudaSuccess)
         {
@@ -294,6 +296,7 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
     }
     cudaEventRecord(e0, st);
     k_decode_level<<<grid, kThreads, smem, st>>>(a);
+    ++ctx->launches;
     cudaEventRecord(e1, st);
     if (cudaGetLastError() != cudaSuccess)
     {
@@ -472,6 +475,7 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
     (void)NB;
     cudaEventRecord(ctx->ev0, st);
     k_decode_level<<<grid, kThreads, smem, st>>>(a);
+    ++ctx->launches;
     cudaEventRecord(ctx->ev1, st);
     if (cudaGetLastError() != cudaSuccess)
       return CudaError;

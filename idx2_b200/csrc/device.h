@@ -21,6 +21,7 @@ struct device_ctx
   bool own_stream = false;
   int num_sms = 148;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  long long launches = 0;  // kernels launched on this context so far
 
   struct buf
   {

@@ -989,6 +989,7 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaEventRecord(ctx_->ev0, st);
     k_encode_level<<<grid, kThreads, smem, st>>>(a);
+    ++ctx_->launches;
     cudaEventRecord(ctx_->ev1, st);
     if (cudaGetLastError() != cudaSuccess)
       return CudaError;

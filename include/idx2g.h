@@ -139,6 +139,10 @@ IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2
 /* Metadata of an open dataset (the fields of the .idx2 file): name and field (64 bytes
    each, NUL-terminated), dims, dtype, number of levels, encode tolerance, and the bytes
    the dataset keeps resident on the device. */
+/* Number of kernels this library has launched on the context so far (a diagnostic for
+   benchmarks; no counterpart in the reference). */
+IDX2G_API long long idx2g_ctx_launches(const idx2g_ctx* ctx);
+
 IDX2G_API int idx2g_dataset_info(const idx2g_dataset* ds, char* name, char* field, int dims3[3],
                                  int* dtype, int* num_levels, double* tolerance,
                                  long long* resident_bytes);
