@@ -13,9 +13,9 @@ or a GPU is missing, every call raises.
 """
 from __future__ import annotations
 
-from ._lib import (Idx2Error, Params, check_params, encode, encode_device, lib, lib_path, ctx,
-                   error_string)
+from ._lib import (Idx2Error, Params, check_params, encode, encode_batch, encode_device, lib, lib_path,
+                   ctx, error_string)
 from .dataset import Dataset
 
-__all__ = ["Idx2Error", "Params", "check_params", "encode", "encode_device", "lib", "lib_path", "ctx",
+__all__ = ["Idx2Error", "Params", "check_params", "encode", "encode_batch", "encode_device", "lib", "lib_path", "ctx",
            "error_string", "Dataset"]

@@ -276,3 +276,55 @@ def encode_device(field, num_levels: int, tolerance: float, brick_dims=None, dev
     if rc:
         raise Idx2Error(rc, "idx2g_encode_device")
     return info
+
+
+BATCH_GRAPH = 1
+BATCH_DEVICE_ONLY = 2
+BATCH_AUTOTUNE = 4
+
+
+def encode_batch(fields, out_dir: str = ".", names=None, field_names=None, num_levels=None,
+                 tolerances=None, graph: bool = True, device_only: bool = False, autotune: bool = True,
+                 device: int = 0):
+    """Encode many fields in one device stage (idx2g_encode_batch): per level one launch over
+    the bricks of every field (captured in one CUDA graph when graph is set), then each field is
+    packed and written exactly as encode() would write it.
+
+    fields: list of numpy arrays or torch tensors (all on the host or all on the device);
+    names / field_names / num_levels / tolerances: one entry per field (defaults: field<i>, data,
+    the library default, machine epsilon). Returns one EncodeInfo per field."""
+    n = len(fields)
+    if n == 0:
+        return []
+    names = names or [f"field{i}" for i in range(n)]
+    field_names = field_names or ["data"] * n
+    num_levels = num_levels if num_levels is not None else [0] * n
+    tolerances = tolerances if tolerances is not None else [0.0] * n
+    ptrs, keeps, cps = [], [], (_CParams * n)()
+    on_dev = None
+    for i, f in enumerate(fields):
+        ptr, dev_, dt, dims, keep = _field_ptr(f)
+        if on_dev is None:
+            on_dev = dev_
+        elif on_dev != dev_:
+            raise Idx2Error(101, "encode_batch: fields must all be on the host or all on the device")
+        tol = tolerances[i]
+        if tol <= 0:
+            tol = float(np.finfo(np.float32 if dt == "float32" else np.float64).eps)
+        bd = (32, 32, 1) if dims[2] == 1 else (32, 32, 32)
+        cps[i] = Params(name=names[i], field=field_names[i], dims=dims, dtype=dt, brick_dims=bd,
+                        num_levels=num_levels[i], tolerance=tol, out_dir=out_dir).to_c()
+        ptrs.append(ptr)
+        keeps.append(keep)
+    arr = (ctypes.c_void_p * n)(*[ctypes.c_void_p(p) for p in ptrs])
+    infos = (EncodeInfo * n)()
+    flags = (BATCH_GRAPH if graph else 0) | (BATCH_DEVICE_ONLY if device_only else 0) | \
+        (BATCH_AUTOTUNE if autotune else 0)
+    L = lib()
+    L.idx2g_encode_batch.argtypes = [ctypes.c_void_p, ctypes.POINTER(_CParams), ctypes.c_void_p, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, ctypes.POINTER(EncodeInfo)]
+    rc = L.idx2g_encode_batch(ctx(device).h, cps, arr, n, int(bool(on_dev)), flags, infos)
+    del keeps
+    if rc:
+        raise Idx2Error(rc, "idx2g_encode_batch")
+    return list(infos)

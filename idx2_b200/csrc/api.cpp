@@ -10,6 +10,9 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <atomic>
+#include <thread>
+#include <vector>
 
 using namespace idx2g;
 
@@ -275,6 +278,165 @@ IDX2G_API int idx2g_encode_device(idx2g_ctx* c, const idx2g_params* in, const vo
     {
       info->level_kernel_ms[i] = coder.level_ms()[i];
       info->level_out_bytes[i] = coder.level_bytes()[i];
+    }
+  }
+  return NoError;
+}
+
+IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const void* const* fields, int n,
+                                 int fields_on_device, int flags, idx2g_encode_info* infos)
+{
+  if (!c || !in || !fields || n < 0)
+    return InvalidArgument;
+  if (n == 0)
+    return NoError;
+  cudaSetDevice(c->d.device);
+  cudaStream_t st = c->d.stream;
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<params> ps((size_t)n);
+  std::vector<dataset_format> fs((size_t)n);
+  std::vector<encode_plan> plans((size_t)n);
+  std::vector<std::vector<level_output>> outs((size_t)n);
+  size_t host_bytes = 0;
+  long long total_bricks = 0;
+  int nf64 = 0;
+  for (int i = 0; i < n; ++i)
+  {
+    if (!fields[i])
+      return InvalidArgument;
+    to_params(in + i, &ps[(size_t)i]);
+    int e = finalize(&fs[(size_t)i], &ps[(size_t)i]);
+    if (e)
+      return e;
+    e = make_encode_plan(fs[(size_t)i], &plans[(size_t)i]);
+    if (e)
+      return e;
+    host_bytes += (((size_t)prod(ps[(size_t)i].dims) * (ps[(size_t)i].type == dtype::float32 ? 4 : 8)) + 255) &
+                  ~(size_t)255;
+    total_bricks += (long long)plans[(size_t)i].levels[0].size();
+    nf64 += ps[(size_t)i].type == dtype::float64;
+  }
+  // fields to the device (one staging buffer of the context's workspace)
+  std::vector<const void*> dptr((size_t)n);
+  if (!fields_on_device)
+  {
+    uint8_t* staged = (uint8_t*)c->d.ws("enc.batchfields", host_bytes);
+    if (!staged)
+      return OutOfMemory;
+    size_t at = 0;
+    for (int i = 0; i < n; ++i)
+    {
+      const size_t b = (size_t)prod(ps[(size_t)i].dims) * (ps[(size_t)i].type == dtype::float32 ? 4 : 8);
+      cudaMemcpyAsync(staged + at, fields[i], b, cudaMemcpyHostToDevice, st);
+      dptr[(size_t)i] = staged + at;
+      at += (b + 255) & ~(size_t)255;
+    }
+  }
+  else
+    for (int i = 0; i < n; ++i)
+      dptr[(size_t)i] = fields[i];
+  std::vector<batch_field> bf((size_t)n);
+  for (int i = 0; i < n; ++i)
+  {
+    bf[(size_t)i].f = &fs[(size_t)i];
+    bf[(size_t)i].plan = &plans[(size_t)i];
+    bf[(size_t)i].d_field = dptr[(size_t)i];
+    bf[(size_t)i].f32 = ps[(size_t)i].type == dtype::float32;
+    bf[(size_t)i].outs = &outs[(size_t)i];
+  }
+  const bool graph = (flags & IDX2G_BATCH_GRAPH) != 0;
+  const bool device_only = (flags & IDX2G_BATCH_DEVICE_ONLY) != 0;
+  batch_tuning tune;
+  if (flags & IDX2G_BATCH_AUTOTUNE)
+  {
+    // the launch shape is timed once per batch signature and remembered by the context
+    char key[96];
+    snprintf(key, sizeof key, "%d/%lld/%d", n, total_bricks, nf64);
+    auto it = c->d.tuned.find(key);
+    if (it == c->d.tuned.end())
+    {
+      double best = 1e300;
+      int best_ctas = 2;
+      for (int ctas = 1; ctas <= 2; ++ctas)
+      {
+        std::vector<batch_field> trial = bf;
+        std::vector<std::vector<level_output>> touts((size_t)n);
+        for (int i = 0; i < n; ++i)
+          trial[(size_t)i].outs = &touts[(size_t)i];
+        batch_encoder te(&c->d, &trial, "b");
+        batch_tuning tt;
+        tt.ctas_per_sm = ctas;
+        int e = te.prepare(tt);
+        if (!e)
+          e = te.run_all(graph, true);
+        if (e)
+          return e;
+        if (te.kernel_ms() < best)
+        {
+          best = te.kernel_ms();
+          best_ctas = ctas;
+        }
+      }
+      it = c->d.tuned.emplace(key, best_ctas).first;
+    }
+    tune.ctas_per_sm = it->second;
+  }
+  batch_encoder enc(&c->d, &bf, "b");
+  int e = enc.prepare(tune);
+  if (!e)
+    e = enc.run_all(graph, device_only);
+  if (e)
+    return e;
+  const auto t1 = std::chrono::steady_clock::now();
+  for (int i = 0; i < n; ++i)
+  {
+    fs[(size_t)i].value_min = bf[(size_t)i].vmin;
+    fs[(size_t)i].value_max = bf[(size_t)i].vmax;
+  }
+  std::vector<encode_timing> tm((size_t)n);
+  if (!device_only)
+  {
+    // packing and files, several fields at a time
+    std::atomic<int> next{ 0 }, err{ 0 };
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = nt ? (nt > 16 ? 16 : nt) : 4;
+    if ((int)nt > n)
+      nt = (unsigned)n;
+    auto work = [&]() {
+      for (int i; (i = next.fetch_add(1)) < n;)
+      {
+        const int r = pack_dataset(&fs[(size_t)i], &ps[(size_t)i], plans[(size_t)i], outs[(size_t)i], nullptr,
+                                   true, &tm[(size_t)i]);
+        if (r)
+          err = r;
+      }
+    };
+    std::vector<std::thread> th;
+    for (unsigned t = 1; t < nt; ++t)
+      th.emplace_back(work);
+    work();
+    for (auto& t : th)
+      t.join();
+    if (err)
+      return err;
+  }
+  if (infos)
+  {
+    const double dev_s = std::chrono::duration<double>(t1 - t0).count();
+    for (int i = 0; i < n; ++i)
+    {
+      idx2g_encode_info* info = infos + i;
+      memset(info, 0, sizeof *info);
+      info->kernel_ms = enc.kernel_ms();
+      info->device_s = dev_s;
+      info->pack_s = tm[(size_t)i].pack_s;
+      info->write_s = tm[(size_t)i].write_s;
+      info->exp_bytes = bf[(size_t)i].exp_bytes;
+      info->file_bytes = (long long)tm[(size_t)i].file_bytes;
+      info->kernel_launches = enc.launches();
+      info->value_min = fs[(size_t)i].value_min;
+      info->value_max = fs[(size_t)i].value_max;
+      info->num_levels = fs[(size_t)i].nlevels;
     }
   }
   return NoError;

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 #include <map>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -22,6 +23,7 @@ struct device_ctx
   int num_sms = 148;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   long long launches = 0;  // kernels launched on this context so far
+  std::map<std::string, int> tuned;  // batched encode: CTAs per SM chosen per batch signature
 
   struct buf
   {
@@ -109,7 +111,59 @@ struct device_ctx
   }
 };
 
-// Device brick coder: transforms and codes every brick of a level in one launch.
+// One field of a device encode (a launch may cover the bricks of many fields).
+struct batch_field
+{
+  const dataset_format* f = nullptr;
+  const encode_plan* plan = nullptr;
+  const void* d_field = nullptr;  // device pointer
+  bool f32 = true;
+  std::vector<level_output>* outs = nullptr;  // receives one entry per level
+  double vmin = 1.7976931348623157e308, vmax = -1.7976931348623157e308;
+  long long stream_bytes = 0, exp_bytes = 0;
+  std::vector<float> level_ms;
+  std::vector<long long> level_bytes;
+};
+
+// Launch shape of the device encode.
+struct batch_tuning
+{
+  int ctas_per_sm = 2;  // 1 or 2 CTAs per SM
+};
+
+// The device stage for a set of fields: per level, one launch of the encode kernel over the
+// bricks of every field that has the level. Levels can be enqueued one by one (with the
+// results read back after each), or all at once, optionally captured in a CUDA graph.
+class batch_encoder
+{
+public:
+  batch_encoder(device_ctx* ctx, std::vector<batch_field>* fields, const std::string& tag);
+  ~batch_encoder();
+  int prepare(const batch_tuning& t);
+  int nlevels() const { return (int)levels_.size(); }
+  int enqueue_level(int l);
+  // Wait for level l, relaunch it with more room if its streams overflowed, read back the
+  // region offsets and streams (unless keep_device) into the fields' level outputs.
+  int collect_level(int l, bool keep_device);
+  // Every level: enqueued back to back (in one CUDA graph if use_graph), then collected.
+  int run_all(bool use_graph, bool keep_device);
+  double kernel_ms() const { return kernel_ms_; }
+  void add_kernel_ms(double ms) { kernel_ms_ += ms; }
+  long long launches() const { return launches_; }
+
+  struct level_launch;
+
+private:
+  device_ctx* ctx_;
+  std::vector<batch_field>* fields_;
+  std::string tag_;
+  batch_tuning tune_;
+  std::vector<std::unique_ptr<level_launch>> levels_;
+  double kernel_ms_ = 0;
+  long long launches_ = 0;
+};
+
+// Device brick coder for one field (brick_coder interface): a batch of one.
 class gpu_coder : public brick_coder
 {
 public:
@@ -119,25 +173,20 @@ public:
   void value_range(double* vmin, double* vmax) override;
   // Leave the coder output on the device (no copies for the packer).
   void set_keep_device(bool v) { keep_device_ = v; }
-  double kernel_ms() const { return kernel_ms_; }
-  long long kernel_launches() const { return launches_; }
-  long long stream_bytes() const { return stream_bytes_; }
-  long long exp_bytes() const { return exp_bytes_; }
-  const std::vector<float>& level_ms() const { return level_ms_; }
-  const std::vector<long long>& level_bytes() const { return level_bytes_; }
+  double kernel_ms() const { return enc_ ? enc_->kernel_ms() : 0.0; }
+  long long kernel_launches() const { return enc_ ? enc_->launches() : 0; }
+  long long stream_bytes() const { return fields_[0].stream_bytes; }
+  long long exp_bytes() const { return fields_[0].exp_bytes; }
+  const std::vector<float>& level_ms() const { return fields_[0].level_ms; }
+  const std::vector<long long>& level_bytes() const { return fields_[0].level_bytes; }
 
 private:
   device_ctx* ctx_;
   const dataset_format& f_;
-  const void* d_field_;
-  bool field_f32_;
   bool keep_device_ = false;
-  const double* in_bricks_ = nullptr;
-  double vmin_ = 1.7976931348623157e308, vmax_ = -1.7976931348623157e308;
-  double kernel_ms_ = 0;
-  long long launches_ = 0, stream_bytes_ = 0, exp_bytes_ = 0;
-  std::vector<float> level_ms_;
-  std::vector<long long> level_bytes_;
+  std::vector<level_output> outs_;
+  std::vector<batch_field> fields_;
+  std::unique_ptr<batch_encoder> enc_;
 };
 
 } // namespace idx2g

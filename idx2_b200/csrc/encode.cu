@@ -74,27 +74,37 @@ struct enc_brick
 {
   int b3[3];      // brick coordinates (level 0: field origin = b3 * 32)
   int valid[3];   // valid dims
-  int parent;     // parent index in the next level, -1 if none
+  int parent;     // parent index in the next level's brick list, -1 if none
   int pos[3];     // position inside the parent (0/1 per axis)
+  int field;      // entry of the launch's field table
 };
 
-struct enc_args
+// Per-field parameters of one level (a launch may cover the bricks of many fields).
+struct enc_field
 {
-  int level, nlevels, is2d, f32_exp, etol, end_bp, nsb, nbricks;
-  int planes;  // plane capacity per block in shared memory (32 or 64)
+  int is2d, f32_exp, etol, end_bp, nsb;
   uint64_t order;
   const void* field;
   int field_f32;
   long long fdims[3];
-  const enc_brick* bricks;
-  const double* in_bricks;   // level > 0: [nbricks][NB] assembled parents
-  double* slots;             // [gridDim][NB]
-  double* parent_bricks;     // [nparents][NB] (zeroed), null on the coarsest level
   const uint64_t* geom;      // [nsb][kMaxBlocksPerSubband]
   const int* nblocks;        // [nsb]
   double weight[8];
   int norm_mask;
-  unsigned long long* offset;
+};
+
+constexpr int kNB3 = 33 * 33 * 33;  // brick stride of slots and parent arrays (2D bricks use 33^2)
+
+struct enc_args
+{
+  int level, nbricks;
+  int planes;  // plane capacity per block in shared memory (32 or 64)
+  const enc_field* fields;
+  const enc_brick* bricks;
+  const double* in_bricks;   // level > 0: [nbricks][kNB3] assembled parents
+  double* slots;             // [gridDim][kNB3]
+  double* parent_bricks;     // [nparents][kNB3] (zeroed), null on the coarsest level
+  unsigned long long* offset;  // [nbricks][8] region offsets
   uint32_t* stream;
   unsigned long long cap_bytes;
   unsigned long long* cursor;
@@ -188,7 +198,7 @@ __device__ __forceinline__ double warp_max(double v)
 }
 
 // L2 prefetch of the field rows a level-0 brick will gather.
-__device__ __forceinline__ void prefetch_rows(const enc_args& a, const enc_brick& b)
+__device__ __forceinline__ void prefetch_rows(const enc_field& a, const enc_brick& b)
 {
   const int vx = b.valid[0], vy = b.valid[1], vz = b.valid[2];
   const int esz = a.field_f32 ? 4 : 8;
@@ -250,10 +260,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
   uint16_t* const OFF = reinterpret_cast<uint16_t*>(Xp + (size_t)kRowX * P);
   uint8_t* const NIN = reinterpret_cast<uint8_t*>(OFF + (size_t)kRowOff * P);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int N[3] = { 33, 33, a.is2d ? 1 : 33 };
-  const int NB = N[0] * N[1] * N[2];
-  const int SZ = a.is2d ? 0 : 2 * 33 * 33;  // sample stride along z inside a subband
-  double* F = a.slots + (size_t)blockIdx.x * (size_t)NB;
+  double* F = a.slots + (size_t)blockIdx.x * (size_t)kNB3;
   if (tid < 64)
     sm.perm3[tid] = dev::perm(3, tid);
   if (tid < 16)
@@ -263,6 +270,10 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
   for (int bi = blockIdx.x; bi < a.nbricks; bi += gridDim.x)
   {
     const enc_brick& br = a.bricks[bi];
+    const enc_field& fp = a.fields[br.field];
+    const int N[3] = { 33, 33, fp.is2d ? 1 : 33 };
+    const int NB = N[0] * N[1] * N[2];
+    const int SZ = fp.is2d ? 0 : 2 * 33 * 33;  // sample stride along z inside a subband
     ENC_PHASE_START
     // ---------------- A: gather ----------------
     if (a.level == 0)
@@ -270,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       const int vx = br.valid[0], vy = br.valid[1], vz = br.valid[2];
       double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
       const long long gx0 = (long long)br.b3[0] * 32, gy0 = (long long)br.b3[1] * 32,
-                      gz0 = (long long)br.b3[2] * (a.is2d ? 1 : 32);
+                      gz0 = (long long)br.b3[2] * (fp.is2d ? 1 : 32);
       // rows (y, z) of the brick, one warp per row, lanes along x; samples outside the
       // valid region (and the x = 32 column) are zero
       const int nrows = 33 * N[2];
@@ -284,11 +295,11 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         {
           const int r = r0 + u, y = r % 33, z = r / 33;
           const bool in = r < nrows && y < vy && z < vz && lane < vx;
-          const long long src = ((gz0 + z) * a.fdims[1] + gy0 + y) * a.fdims[0] + gx0 + lane;
-          if (a.field_f32)
-            fv[u] = in ? __ldcs((const float*)a.field + src) : 0.0f;
+          const long long src = ((gz0 + z) * fp.fdims[1] + gy0 + y) * fp.fdims[0] + gx0 + lane;
+          if (fp.field_f32)
+            fv[u] = in ? __ldcs((const float*)fp.field + src) : 0.0f;
           else
-            dv[u] = in ? __ldcs((const double*)a.field + src) : 0.0;
+            dv[u] = in ? __ldcs((const double*)fp.field + src) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < U; ++u)
@@ -297,7 +308,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
           if (r >= nrows)
             break;
           const bool in = y < vy && z < vz && lane < vx;
-          const double v = a.field_f32 ? (double)fv[u] : dv[u];
+          const double v = fp.field_f32 ? (double)fv[u] : dv[u];
           F[r * 33 + lane] = v;
           if (lane == 0)
             F[r * 33 + 32] = 0.0;
@@ -334,7 +345,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
     else
     {
       // (bricks are NB = 33^3 doubles, an odd count: only 8-byte alignment is guaranteed)
-      const double* src = a.in_bricks + (size_t)bi * (size_t)NB;
+      const double* src = a.in_bricks + (size_t)bi * (size_t)kNB3;
       for (int i = tid; i < NB; i += kThreads)
         F[i] = __ldcs(src + i);
     }
@@ -351,10 +362,10 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       // lattice copied into shared memory (the coding tables' space, idle here), lifted in
       // place sample by sample.
       double* S = reinterpret_cast<double*>(Xp);
-      const int NS[3] = { 17, 17, a.is2d ? 1 : 17 };
+      const int NS[3] = { 17, 17, fp.is2d ? 1 : 17 };
       const int nsub = NS[0] * NS[1] * NS[2];
       if (tid == 0)
-        dev::build_stack(br.valid, 5, a.order, &sm.stack);
+        dev::build_stack(br.valid, 5, fp.order, &sm.stack);
       __syncthreads();
       const int nf = sm.stack.n, cf = sm.stack.coarse;
       for (int i = 0; i < cf; ++i)
@@ -380,7 +391,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       }
       ENC_PHASE(3)
       if (tid == 0)
-        dev::build_stack(N, 5, a.order, &sm.stack);
+        dev::build_stack(N, 5, fp.order, &sm.stack);
       __syncthreads();
       const int ni = sm.stack.n, ci = sm.stack.coarse;
       for (int i = ni - 1; i >= ci; --i)
@@ -432,17 +443,17 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         for (int k = 0; k < 33; ++k)
         {
           double f = v[k];
-          if (a.is2d)
+          if (fp.is2d)
           {
             const int s = ((x & 1) << 1) | (k & 1);
-            f = ((a.norm_mask >> s) & 1) ? __dmul_rn(f, a.weight[s]) : f;
+            f = ((fp.norm_mask >> s) & 1) ? __dmul_rn(f, fp.weight[s]) : f;
           }
           col[k * 33] = f;
         }
       }
       __syncthreads();
       ENC_PHASE(7)
-      if (!a.is2d)
+      if (!fp.is2d)
       {
         for (int li = tid; li < 33 * 33; li += kThreads)
         {
@@ -457,7 +468,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
           for (int k = 0; k < 33; ++k)
           {
             const int s = ((x & 1) << 2) | ((y & 1) << 1) | (k & 1);
-            col[k * 33 * 33] = ((a.norm_mask >> s) & 1) ? __dmul_rn(v[k], a.weight[s]) : v[k];
+            col[k * 33 * 33] = ((fp.norm_mask >> s) & 1) ? __dmul_rn(v[k], fp.weight[s]) : v[k];
           }
         }
         __syncthreads();
@@ -468,12 +479,12 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
     // ---------------- C: low band to the parent ----------------
     if (a.parent_bricks && br.parent >= 0)
     {
-      double* P = a.parent_bricks + (size_t)br.parent * (size_t)NB;
-      const int nz = a.is2d ? 1 : 16;
+      double* P = a.parent_bricks + (size_t)br.parent * (size_t)kNB3;
+      const int nz = fp.is2d ? 1 : 16;
       for (int i = tid; i < 16 * 16 * nz; i += kThreads)
       {
         int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
-        int cz = a.is2d ? 0 : 2 * z;
+        int cz = fp.is2d ? 0 : 2 * z;
         __stcs(P + ((br.pos[2] * nz + z) * 33 + (br.pos[1] * 16 + y)) * 33 + (br.pos[0] * 16 + x),
                F[(cz * 33 + 2 * y) * 33 + 2 * x]);
       }
@@ -481,16 +492,16 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
     ENC_PHASE(9)
 
     // ---------------- D: block coding per subband ----------------
-    for (int s = 0; s < a.nsb; ++s)
+    for (int s = 0; s < fp.nsb; ++s)
     {
       // towards the end of the brick, ask L2 for the rows of this CTA's next brick
-      if (a.level == 0 && s == (a.nsb * 5) / 8 && bi + (int)gridDim.x < a.nbricks)
-        prefetch_rows(a, a.bricks[bi + gridDim.x]);
+      if (a.level == 0 && s == (fp.nsb * 5) / 8 && bi + (int)gridDim.x < a.nbricks)
+        prefetch_rows(a.fields[a.bricks[bi + gridDim.x].field], a.bricks[bi + gridDim.x]);
       int from[3], dims[3], strd[3];
-      subband_grid(a.is2d, s, from, dims, strd);
-      const int nb = a.nblocks[s];
-      const uint64_t* geom = a.geom + (size_t)s * kMaxBlocksPerSubband;
-      const size_t bs = (size_t)bi * (size_t)a.nsb + (size_t)s;
+      subband_grid(fp.is2d, s, from, dims, strd);
+      const int nb = fp.nblocks[s];
+      const uint64_t* geom = fp.geom + (size_t)s * kMaxBlocksPerSubband;
+      const size_t bs = (size_t)bi * 8 + (size_t)s;
 
       // D1: a warp codes two blocks (lanes own samples j and j + 32 of each): exponent,
       // quantisation, zfp transform, shuffle, bit-plane masks by ballot; then the
@@ -501,9 +512,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       block_info cA, cB;
       auto load_pair = [&](int pr, double v[4], block_info& A, block_info& B) {
         const int b0 = 2 * pr, b1 = 2 * pr + 1;
-        A = block_at(geom, b0, from, a.is2d);
+        A = block_at(geom, b0, from, fp.is2d);
         const bool hb = b1 < nb;
-        B = hb ? block_at(geom, b1, from, a.is2d) : A;
+        B = hb ? block_at(geom, b1, from, fp.is2d) : A;
         const int nvA = 1 << (2 * A.nd), nvB = hb ? 1 << (2 * B.nd) : 0;
         v[0] = lane < nvA ? F[block_sample(A.base, A.lx, A.ly, lane, 66, SZ)] : 0.0;
         v[1] = lane + 32 < nvA ? F[block_sample(A.base, A.lx, A.ly, lane + 32, 66, SZ)] : 0.0;
@@ -531,8 +542,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         }
         mA = warp_max(mA);
         mB = warp_max(mB);
-        const int eA = a.f32_exp ? dev::exponent_f32(__double2float_rn(mA)) : dev::exponent_f64(mA);
-        const int eB = a.f32_exp ? dev::exponent_f32(__double2float_rn(mB)) : dev::exponent_f64(mB);
+        const int eA = fp.f32_exp ? dev::exponent_f32(__double2float_rn(mA)) : dev::exponent_f64(mA);
+        const int eB = fp.f32_exp ? dev::exponent_f32(__double2float_rn(mB)) : dev::exponent_f64(mB);
         const double sA = dev::pow2(63 - ndA - 1 - eA), sB = dev::pow2(63 - ndB - 1 - eB);
         long long* qA = sm.q[warp][0];
         long long* qB = sm.q[warp][1];
@@ -590,8 +601,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         if (lane + 32 < nvB)
           uB1 = ((unsigned long long)qB[qpad(permj(ndB, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
         __syncwarp();
-        const int npA = dev::coded_planes(eA, a.etol, a.end_bp);
-        const int npB = hasB ? dev::coded_planes(eB, a.etol, a.end_bp) : 0;
+        const int npA = dev::coded_planes(eA, fp.etol, fp.end_bp);
+        const int npB = hasB ? dev::coded_planes(eB, fp.etol, fp.end_bp) : 0;
         const int npM = npA > npB ? npA : npB;
         unsigned long long* XA = Xp + bA;  // plane k at XA[k * kRowX]
         unsigned long long* XB = Xp + bB;
@@ -872,206 +883,431 @@ void level_weights(const dataset_format& f, int level, double w[8], int* mask)
 // device stage
 // ---------------------------------------------------------------------------
 
-gpu_coder::gpu_coder(device_ctx* ctx, const dataset_format& f, const void* d_field, bool field_f32)
-  : ctx_(ctx), f_(f), d_field_(d_field), field_f32_(field_f32)
+struct batch_encoder::level_launch
 {
+  int level = 0;
+  std::vector<enc_brick> bricks;
+  std::vector<enc_field> fields;  // geom / nblocks device pointers filled by prepare
+  std::vector<uint64_t> geom;     // [field][8][kMaxBlocksPerSubband]
+  std::vector<int> nblocks;       // [field][8]
+  std::vector<int> field_job;     // field table entry -> index in the batch
+  std::vector<int> job_first;     // batch index -> first brick (-1: no such level)
+  int nparents = 0;
+  int planes = 32;
+  int grid = 1;
+  size_t smem = 0;
+  unsigned long long cap = 0;
+  enc_brick* d_bricks = nullptr;
+  enc_field* d_fields = nullptr;
+  uint64_t* d_geom = nullptr;
+  int* d_nblocks = nullptr;
+  unsigned long long* d_off = nullptr;
+  unsigned long long* d_misc = nullptr;
+  double* d_bmin = nullptr;
+  double* d_bmax = nullptr;
+  double* d_parents = nullptr;
+  std::string sname;
+  enc_args args;
+};
+
+batch_encoder::batch_encoder(device_ctx* ctx, std::vector<batch_field>* fields, const std::string& tag)
+  : ctx_(ctx), fields_(fields), tag_(tag)
+{
+}
+
+batch_encoder::~batch_encoder() = default;
+
+int batch_encoder::prepare(const batch_tuning& t)
+{
+  tune_ = t;
+  std::vector<batch_field>& J = *fields_;
+  int L = 0;
+  for (batch_field& j : J)
+  {
+    const dataset_format& f = *j.f;
+    if (f.bit_planes_per_chunk != 1)
+      return OptionNotSupported;
+    if (f.brick_dims.x != 32 || f.brick_dims.y != 32 || (f.brick_dims.z != 32 && f.brick_dims.z != 1))
+      return OptionNotSupported;
+    L = f.nlevels > L ? f.nlevels : L;
+    j.outs->assign((size_t)f.nlevels, level_output());
+    j.level_ms.assign((size_t)f.nlevels, 0.f);
+    j.level_bytes.assign((size_t)f.nlevels, 0);
+  }
+  // first brick of every field in every level's launch
+  std::vector<std::vector<int>> first((size_t)L + 1, std::vector<int>(J.size(), -1));
+  std::vector<int> count((size_t)L + 1, 0);
+  for (int l = 0; l < L; ++l)
+    for (size_t j = 0; j < J.size(); ++j)
+      if (l < J[j].f->nlevels)
+      {
+        first[(size_t)l][j] = count[(size_t)l];
+        count[(size_t)l] += (int)J[j].plan->levels[(size_t)l].size();
+      }
+  levels_.clear();
+  cudaStream_t st = ctx_->stream;
+  size_t max_grid = 1;
+  for (int l = 0; l < L; ++l)
+  {
+    levels_.emplace_back(new level_launch());
+    level_launch& ll = *levels_.back();
+    ll.level = l;
+    ll.job_first = first[(size_t)l];
+    ll.nparents = count[(size_t)l + 1];
+    unsigned long long cap = 16ull << 20;
+    for (size_t j = 0; j < J.size(); ++j)
+    {
+      const dataset_format& f = *J[j].f;
+      if (l >= f.nlevels)
+        continue;
+      const int fi = (int)ll.fields.size();
+      enc_field ef;
+      memset(&ef, 0, sizeof ef);
+      ef.is2d = f.is2d();
+      ef.f32_exp = f.type == dtype::float32;
+      ef.etol = exponent_f64(f.tolerance);
+      ef.end_bp = f.type == dtype::float32 ? 32 : 64;
+      ef.nsb = f.nsubbands();
+      ef.order = f.transform_order;
+      ef.field = J[j].d_field;
+      ef.field_f32 = J[j].f32;
+      ef.fdims[0] = f.dims.x;
+      ef.fdims[1] = f.dims.y;
+      ef.fdims[2] = f.dims.z;
+      level_weights(f, l, ef.weight, &ef.norm_mask);
+      if (ef.end_bp == 64)
+        ll.planes = 64;
+      ll.fields.push_back(ef);
+      ll.field_job.push_back((int)j);
+      ll.geom.resize(ll.fields.size() * 8 * kMaxBlocksPerSubband, 0);
+      ll.nblocks.resize(ll.fields.size() * 8, 0);
+      for (int sb = 0; sb < ef.nsb; ++sb)
+      {
+        std::vector<block_geom> g;
+        subband_blocks(f, l, sb, &g);
+        ll.nblocks[(size_t)fi * 8 + (size_t)sb] = (int)g.size();
+        for (size_t b = 0; b < g.size(); ++b)
+          ll.geom[((size_t)fi * 8 + (size_t)sb) * kMaxBlocksPerSubband + b] =
+            (uint64_t)g[b].dx | ((uint64_t)g[b].dy << 8) | ((uint64_t)g[b].dz << 16) |
+            ((uint64_t)g[b].bx << 24) | ((uint64_t)g[b].by << 32) | ((uint64_t)g[b].bz << 40);
+      }
+      const std::vector<brick_entry>& bricks = J[j].plan->levels[(size_t)l];
+      const bool has_parent = l + 1 < f.nlevels;
+      for (const brick_entry& e : bricks)
+        ll.bricks.push_back(enc_brick{ { e.brick3.x, e.brick3.y, e.brick3.z },
+                                       { e.valid.x, e.valid.y, e.valid.z },
+                                       has_parent ? first[(size_t)l + 1][j] + e.parent : -1,
+                                       { e.pos_in_parent.x, e.pos_in_parent.y, e.pos_in_parent.z },
+                                       fi });
+      const unsigned long long NB = (unsigned long long)(ef.is2d ? 33 * 33 : kNB3);
+      cap += (unsigned long long)bricks.size() * NB * 2ull;
+    }
+    const int nbr = (int)ll.bricks.size();
+    const int lim = tune_.ctas_per_sm * ctx_->num_sms;
+    ll.grid = nbr < lim ? (nbr > 0 ? nbr : 1) : lim;
+    max_grid = (size_t)ll.grid > max_grid ? (size_t)ll.grid : max_grid;
+    char name[96];
+    snprintf(name, sizeof name, "enc.%s.L%d.stream", tag_.c_str(), l);
+    ll.sname = name;
+    ll.cap = cap > ctx_->ws_size(name) ? cap : ctx_->ws_size(name);
+    auto wsn = [&](const char* what, size_t bytes) -> void* {
+      char n2[96];
+      snprintf(n2, sizeof n2, "enc.%s.L%d.%s", tag_.c_str(), l, what);
+      return ctx_->ws(n2, bytes);
+    };
+    ll.d_bricks = (enc_brick*)wsn("bricks", sizeof(enc_brick) * (size_t)(nbr > 0 ? nbr : 1));
+    ll.d_fields = (enc_field*)wsn("fields", sizeof(enc_field) * (ll.fields.size() + 1));
+    ll.d_geom = (uint64_t*)wsn("geom", (ll.geom.size() + 1) * 8);
+    ll.d_nblocks = (int*)wsn("nblocks", (ll.nblocks.size() + 1) * 4);
+    ll.d_off = (unsigned long long*)wsn("off", (size_t)(nbr > 0 ? nbr : 1) * 8 * 8);
+    ll.d_misc = (unsigned long long*)wsn("misc", 64);
+    if (l == 0)
+    {
+      ll.d_bmin = (double*)wsn("bmin", (size_t)(nbr > 0 ? nbr : 1) * 8);
+      ll.d_bmax = (double*)wsn("bmax", (size_t)(nbr > 0 ? nbr : 1) * 8);
+    }
+    if (ll.nparents > 0)
+      ll.d_parents = (double*)wsn("parents", (size_t)ll.nparents * (size_t)kNB3 * 8);
+    uint32_t* d_stream = (uint32_t*)ctx_->ws(ll.sname, (size_t)ll.cap);
+    if (!ll.d_bricks || !ll.d_fields || !ll.d_geom || !ll.d_nblocks || !ll.d_off || !ll.d_misc ||
+        (l == 0 && (!ll.d_bmin || !ll.d_bmax)) || (ll.nparents > 0 && !ll.d_parents) || !d_stream)
+      return OutOfMemory;
+    ll.cap = ctx_->ws_size(ll.sname);
+    for (size_t fi = 0; fi < ll.fields.size(); ++fi)
+    {
+      ll.fields[fi].geom = ll.d_geom + fi * 8 * kMaxBlocksPerSubband;
+      ll.fields[fi].nblocks = ll.d_nblocks + fi * 8;
+    }
+    if (nbr > 0)
+      cudaMemcpyAsync(ll.d_bricks, ll.bricks.data(), sizeof(enc_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(ll.d_fields, ll.fields.data(), sizeof(enc_field) * ll.fields.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(ll.d_geom, ll.geom.data(), ll.geom.size() * 8, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(ll.d_nblocks, ll.nblocks.data(), ll.nblocks.size() * 4, cudaMemcpyHostToDevice, st);
+    enc_args& a = ll.args;
+    memset(&a, 0, sizeof a);
+    a.level = l;
+    a.nbricks = nbr;
+    a.planes = ll.planes;
+    a.fields = ll.d_fields;
+    a.bricks = ll.d_bricks;
+    a.in_bricks = l > 0 ? levels_[(size_t)l - 1]->d_parents : nullptr;
+    a.parent_bricks = ll.d_parents;
+    a.offset = ll.d_off;
+    a.stream = d_stream;
+    a.cap_bytes = ll.cap;
+    a.cursor = ll.d_misc;
+    a.error = (int*)(ll.d_misc + 1);
+    a.bmin = ll.d_bmin;
+    a.bmax = ll.d_bmax;
+    ll.smem = enc_smem_bytes(ll.planes);
+  }
+  double* d_slots = (double*)ctx_->ws("enc.slots", max_grid * (size_t)kNB3 * 8);
+  if (!d_slots)
+    return OutOfMemory;
+  size_t max_smem = 0;
+  for (auto& ll : levels_)
+  {
+    ll->args.slots = d_slots;
+    max_smem = ll->smem > max_smem ? ll->smem : max_smem;
+  }
+  cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+  return cudaGetLastError() == cudaSuccess ? NoError : CudaError;
+}
+
+int batch_encoder::enqueue_level(int l)
+{
+  level_launch& ll = *levels_[(size_t)l];
+  cudaStream_t st = ctx_->stream;
+  cudaMemsetAsync(ll.d_misc, 0, 64, st);
+  if (ll.nparents > 0)
+    cudaMemsetAsync(ll.d_parents, 0, (size_t)ll.nparents * (size_t)kNB3 * 8, st);
+  if (ll.args.nbricks > 0)
+  {
+    k_encode_level<<<ll.grid, kThreads, ll.smem, st>>>(ll.args);
+    ++launches_;
+    ++ctx_->launches;
+  }
+  return cudaGetLastError() == cudaSuccess ? NoError : CudaError;
+}
+
+int batch_encoder::collect_level(int l, bool keep_device)
+{
+  level_launch& ll = *levels_[(size_t)l];
+  cudaStream_t st = ctx_->stream;
+  std::vector<batch_field>& J = *fields_;
+  const int nbr = ll.args.nbricks;
+  unsigned long long misc[2] = { 0, 0 };
+  for (int attempt = 0;; ++attempt)
+  {
+    cudaMemcpyAsync(misc, ll.d_misc, 16, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    const int err = (int)(misc[1] & 0xffffffffu);
+    if (err == 1)
+      return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
+    if (err != 2)
+      break;
+    if (attempt >= 3)
+      return DeviceStreamOverflow;
+    // the regions did not fit: the level again with room for all of them (its outputs for
+    // the next level are recomputed identically)
+    uint32_t* d_stream = (uint32_t*)ctx_->ws(ll.sname, (size_t)(misc[0] + (1ull << 20)));
+    if (!d_stream)
+      return OutOfMemory;
+    ll.cap = ctx_->ws_size(ll.sname);
+    ll.args.stream = d_stream;
+    ll.args.cap_bytes = ll.cap;
+    cudaEventRecord(ctx_->ev0, st);
+    int e = enqueue_level(l);
+    cudaEventRecord(ctx_->ev1, st);
+    if (e)
+      return e;
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
+    kernel_ms_ += ms;
+  }
+  ctx_->ws_mark_dirty(ll.sname, (size_t)(misc[0] < ll.cap ? misc[0] : ll.cap));
+  const unsigned long long used = misc[0];
+  // per field: exponent bytes, level output, value range
+  std::vector<unsigned long long> off;
+  const uint8_t* pin = nullptr;
+  if (!keep_device && nbr > 0)
+  {
+    off.resize((size_t)nbr * 8);
+    cudaMemcpyAsync(off.data(), ll.d_off, off.size() * 8, cudaMemcpyDeviceToHost, st);
+    if (used)
+    {
+      char name[96];
+      snprintf(name, sizeof name, "enc.pin.%s.%d", tag_.c_str(), l);
+      pin = (const uint8_t*)ctx_->pinned(name, (size_t)used);
+      if (!pin)
+        return OutOfMemory;
+      cudaMemcpyAsync((void*)pin, ll.args.stream, (size_t)used, cudaMemcpyDeviceToHost, st);
+    }
+  }
+  std::vector<double> mn, mx;
+  if (l == 0 && nbr > 0)
+  {
+    mn.resize((size_t)nbr);
+    mx.resize((size_t)nbr);
+    cudaMemcpyAsync(mn.data(), ll.d_bmin, (size_t)nbr * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(mx.data(), ll.d_bmax, (size_t)nbr * 8, cudaMemcpyDeviceToHost, st);
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return CudaError;
+  for (size_t fi = 0; fi < ll.fields.size(); ++fi)
+  {
+    batch_field& bf = J[(size_t)ll.field_job[fi]];
+    const dataset_format& f = *bf.f;
+    const int j0 = ll.job_first[(size_t)ll.field_job[fi]];
+    const int jn = (int)bf.plan->levels[(size_t)l].size();
+    const int nsb = f.nsubbands();
+    level_output& o = (*bf.outs)[(size_t)l];
+    o.nbricks = jn;
+    o.nsb = nsb;
+    o.nexps.assign((size_t)nsb, 0);
+    long long eb = 0;
+    for (int sb = 0; sb < nsb; ++sb)
+    {
+      o.nexps[(size_t)sb] = ll.nblocks[fi * 8 + (size_t)sb];
+      eb += (long long)jn * o.nexps[(size_t)sb] * (f.type == dtype::float32 ? 1 : 2);
+    }
+    bf.exp_bytes += eb;
+    if (!keep_device)
+    {
+      o.offset.resize((size_t)jn * (size_t)nsb);
+      for (int b = 0; b < jn; ++b)
+        for (int sb = 0; sb < nsb; ++sb)
+          o.offset[(size_t)b * (size_t)nsb + (size_t)sb] = off[(size_t)(j0 + b) * 8 + (size_t)sb];
+      o.ext_stream = pin;
+    }
+    if (ll.fields.size() == 1)
+    {
+      bf.stream_bytes += (long long)used;
+      bf.level_bytes[(size_t)l] = (long long)used + eb;
+    }
+    if (l == 0)
+      for (int b = 0; b < jn; ++b)
+      {
+        const double a0 = mn[(size_t)(j0 + b)], a1 = mx[(size_t)(j0 + b)];
+        bf.vmin = a0 < bf.vmin ? a0 : bf.vmin;
+        bf.vmax = bf.vmax < a1 ? a1 : bf.vmax;
+      }
+  }
+  return NoError;
+}
+
+int batch_encoder::run_all(bool use_graph, bool keep_device)
+{
+  cudaStream_t st = ctx_->stream;
+  const int L = nlevels();
+  if (use_graph)
+  {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return CudaError;
+    int e = NoError;
+    for (int l = 0; l < L && !e; ++l)
+      e = enqueue_level(l);
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (e || ce != cudaSuccess || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+    {
+      if (g)
+        cudaGraphDestroy(g);
+      return e ? e : CudaError;
+    }
+    cudaEventRecord(ctx_->ev0, st);
+    cudaGraphLaunch(ge, st);
+    cudaEventRecord(ctx_->ev1, st);
+    const cudaError_t se = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(ge);
+    cudaGraphDestroy(g);
+    if (se != cudaSuccess)
+      return CudaError;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
+    kernel_ms_ += ms;
+    for (int l = 0; l < L; ++l)
+    {
+      e = collect_level(l, keep_device);
+      if (e)
+        return e;
+    }
+    return NoError;
+  }
+  for (int l = 0; l < L; ++l)
+  {
+    cudaEventRecord(ctx_->ev0, st);
+    int e = enqueue_level(l);
+    cudaEventRecord(ctx_->ev1, st);
+    if (e)
+      return e;
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
+    kernel_ms_ += ms;
+    for (batch_field& bf : *fields_)
+      if (l < (int)bf.level_ms.size())
+        bf.level_ms[(size_t)l] += ms;
+    e = collect_level(l, keep_device);
+    if (e)
+      return e;
+  }
+  return NoError;
+}
+
+gpu_coder::gpu_coder(device_ctx* ctx, const dataset_format& f, const void* d_field, bool field_f32)
+  : ctx_(ctx), f_(f)
+{
+  fields_.resize(1);
+  fields_[0].f = &f_;
+  fields_[0].d_field = d_field;
+  fields_[0].f32 = field_f32;
+  fields_[0].outs = &outs_;
 }
 
 gpu_coder::~gpu_coder() {}
 
 int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
 {
-  if (f_.bit_planes_per_chunk != 1)
-    return OptionNotSupported;
-  if (f_.brick_dims.x != 32 || f_.brick_dims.y != 32 || (f_.brick_dims.z != 32 && f_.brick_dims.z != 1))
-    return OptionNotSupported;
   cudaStream_t st = ctx_->stream;
-  const bool is2d = f_.is2d();
-  const int NB = 33 * 33 * (is2d ? 1 : 33);
-  const std::vector<brick_entry>& bricks = plan.levels[(size_t)level];
-  const int nbr = (int)bricks.size();
-  const int nsb = f_.nsubbands();
-  const bool has_parent = level + 1 < f_.nlevels;
-  const int npar = has_parent ? (int)plan.levels[(size_t)level + 1].size() : 0;
-
-  std::vector<enc_brick> hb((size_t)nbr);
-  for (int i = 0; i < nbr; ++i)
+  if (level == 0 || !enc_)
   {
-    const brick_entry& e = bricks[(size_t)i];
-    hb[(size_t)i] = enc_brick{ { e.brick3.x, e.brick3.y, e.brick3.z },
-                               { e.valid.x, e.valid.y, e.valid.z },
-                               e.parent,
-                               { e.pos_in_parent.x, e.pos_in_parent.y, e.pos_in_parent.z } };
+    fields_[0].plan = &plan;
+    enc_.reset(new batch_encoder(ctx_, &fields_, "s"));
+    int e = enc_->prepare(batch_tuning());
+    if (e)
+      return e;
   }
-  std::vector<uint64_t> geom((size_t)nsb * kMaxBlocksPerSubband, 0);
-  std::vector<int> nblocks((size_t)nsb, 0);
-  for (int s = 0; s < nsb; ++s)
-  {
-    std::vector<block_geom> g;
-    subband_blocks(f_, level, s, &g);
-    nblocks[(size_t)s] = (int)g.size();
-    for (size_t b = 0; b < g.size(); ++b)
-      geom[(size_t)s * kMaxBlocksPerSubband + b] =
-        (uint64_t)g[b].dx | ((uint64_t)g[b].dy << 8) | ((uint64_t)g[b].dz << 16) |
-        ((uint64_t)g[b].bx << 24) | ((uint64_t)g[b].by << 32) | ((uint64_t)g[b].bz << 40);
-  }
-
-  enc_args a;
-  memset(&a, 0, sizeof a);
-  a.level = level;
-  a.nlevels = f_.nlevels;
-  a.is2d = is2d;
-  a.f32_exp = f_.type == dtype::float32;
-  a.etol = exponent_f64(f_.tolerance);
-  a.end_bp = f_.type == dtype::float32 ? 32 : 64;
-  a.planes = a.end_bp;
-  a.nsb = nsb;
-  a.nbricks = nbr;
-  a.order = f_.transform_order;
-  a.field = d_field_;
-  a.field_f32 = field_f32_;
-  a.fdims[0] = f_.dims.x;
-  a.fdims[1] = f_.dims.y;
-  a.fdims[2] = f_.dims.z;
-  level_weights(f_, level, a.weight, &a.norm_mask);
-
-  // workspace buffers, kept by the context across calls (grow-only)
-  int nsm = ctx_->num_sms;
-  int grid = nbr < kCtasPerSm * nsm ? nbr : kCtasPerSm * nsm;
-  if (grid < 1)
-    grid = 1;
-  const size_t nbs = (size_t)nbr * (size_t)nsb;
-  auto* d_bricks = (enc_brick*)ctx_->ws("enc.bricks", sizeof(enc_brick) * (size_t)nbr);
-  auto* d_geom = (uint64_t*)ctx_->ws("enc.geom", geom.size() * 8);
-  auto* d_nblocks = (int*)ctx_->ws("enc.nblocks", (size_t)nsb * sizeof(int));
-  double* d_slots = (double*)ctx_->ws("enc.slots", (size_t)grid * (size_t)NB * sizeof(double));
-  double* d_parents = has_parent ? (double*)ctx_->ws(level % 2 ? "enc.parA" : "enc.parB",
-                                                     (size_t)npar * (size_t)NB * sizeof(double))
-                                 : nullptr;
-  auto* d_off = (unsigned long long*)ctx_->ws(level % 2 ? "enc.offA" : "enc.offB", nbs * 8);
-  auto* d_misc = (unsigned long long*)ctx_->ws("enc.misc", 64);
-  double* d_bmin = (double*)ctx_->ws("enc.bmin", (size_t)nbr * 8);
-  double* d_bmax = (double*)ctx_->ws("enc.bmax", (size_t)nbr * 8);
-  if (!d_bricks || !d_geom || !d_nblocks || !d_slots || (has_parent && !d_parents) || !d_off || !d_misc ||
-      !d_bmin || !d_bmax)
-    return OutOfMemory;
-  cudaMemcpyAsync(d_bricks, hb.data(), sizeof(enc_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d_geom, geom.data(), geom.size() * 8, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d_nblocks, nblocks.data(), (size_t)nsb * sizeof(int), cudaMemcpyHostToDevice, st);
-
-  const char* sname = level % 2 ? "enc.streamA" : "enc.streamB";
-  unsigned long long cap = (unsigned long long)nbr * (unsigned long long)NB * 2ull + (16ull << 20);
-  if (ctx_->ws_size(sname) > cap)
-    cap = ctx_->ws_size(sname);
-  for (int attempt = 0; attempt < 4; ++attempt)
-  {
-    uint32_t* d_stream = (uint32_t*)ctx_->ws(sname, (size_t)cap);
-    if (!d_stream)
-      return OutOfMemory;
-    cap = ctx_->ws_size(sname);
-    cudaMemsetAsync(d_misc, 0, 64, st);
-    if (has_parent)
-      cudaMemsetAsync(d_parents, 0, (size_t)npar * (size_t)NB * sizeof(double), st);
-    a.bricks = d_bricks;
-    a.in_bricks = level > 0 ? in_bricks_ : nullptr;
-    a.slots = d_slots;
-    a.parent_bricks = d_parents;
-    a.geom = d_geom;
-    a.nblocks = d_nblocks;
-    a.offset = d_off;
-    a.stream = d_stream;
-    a.cap_bytes = cap;
-    a.cursor = d_misc;
-    a.error = (int*)(d_misc + 1);
-    a.bmin = d_bmin;
-    a.bmax = d_bmax;
-    const size_t smem = enc_smem_bytes(a.planes);
-    cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaEventRecord(ctx_->ev0, st);
-    k_encode_level<<<grid, kThreads, smem, st>>>(a);
-    ++ctx_->launches;
-    cudaEventRecord(ctx_->ev1, st);
-    if (cudaGetLastError() != cudaSuccess)
-      return CudaError;
-    ++launches_;
-    unsigned long long misc[2];
-    cudaMemcpyAsync(misc, d_misc, 16, cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess)
-      return CudaError;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
-    ctx_->ws_mark_dirty(sname, (size_t)(misc[0] < cap ? misc[0] : cap));
-    int err = (int)(misc[1] & 0xffffffffu);
-    if (err == 1)
-      return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
-    if (err == 2)
-    {
-      cap = misc[0] + (1ull << 20);
-      continue;
-    }
-    kernel_ms_ += ms;
-    level_ms_.push_back(ms);
-    stream_bytes_ += (long long)misc[0];
-    long long eb = 0;
-    for (int s = 0; s < nsb; ++s)
-      eb += (long long)nbr * nblocks[(size_t)s] * (f_.type == dtype::float32 ? 1 : 2);
-    exp_bytes_ += eb;
-    level_bytes_.push_back((long long)misc[0] + eb);
-    out->nbricks = nbr;
-    out->nsb = nsb;
-    out->nexps = nblocks;
-    if (level == 0)
-    {
-      std::vector<double> mn((size_t)nbr), mx((size_t)nbr);
-      cudaMemcpyAsync(mn.data(), d_bmin, (size_t)nbr * 8, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(mx.data(), d_bmax, (size_t)nbr * 8, cudaMemcpyDeviceToHost, st);
-      if (cudaStreamSynchronize(st) != cudaSuccess)
-        return CudaError;
-      for (int i = 0; i < nbr; ++i)
-      {
-        vmin_ = mn[(size_t)i] < vmin_ ? mn[(size_t)i] : vmin_;
-        vmax_ = vmax_ < mx[(size_t)i] ? mx[(size_t)i] : vmax_;
-      }
-    }
-    if (!keep_device_)
-    {
-      // results to the host for the packer: region offsets and the regions
-      out->offset.resize(nbs);
-      cudaMemcpyAsync(out->offset.data(), d_off, nbs * 8, cudaMemcpyDeviceToHost, st);
-      if (misc[0])
-      {
-        // into pinned host memory kept by the context (one buffer per level)
-        char name[32];
-        snprintf(name, sizeof name, "enc.pin%d", level);
-        uint8_t* pin = (uint8_t*)ctx_->pinned(name, (size_t)misc[0]);
-        if (!pin)
-          return OutOfMemory;
-        cudaMemcpyAsync(pin, d_stream, (size_t)misc[0], cudaMemcpyDeviceToHost, st);
-        out->ext_stream = pin;
-      }
-      if (cudaStreamSynchronize(st) != cudaSuccess)
-        return CudaError;
-    }
-    in_bricks_ = d_parents;
-    return NoError;
-  }
-  return DeviceStreamOverflow;
+  if (level >= enc_->nlevels())
+    return UnknownError;
+  const double before = enc_->kernel_ms();
+  cudaEventRecord(ctx_->ev0, st);
+  int e = enc_->enqueue_level(level);
+  cudaEventRecord(ctx_->ev1, st);
+  if (e)
+    return e;
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return CudaError;
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
+  e = enc_->collect_level(level, keep_device_);
+  if (e)
+    return e;
+  fields_[0].level_ms[(size_t)level] = ms + (float)(enc_->kernel_ms() - before);
+  enc_->add_kernel_ms(ms);
+  *out = std::move(outs_[(size_t)level]);
+  return NoError;
 }
-
-#ifdef IDX2G_PHASE_TIMING
-// Profiling builds: read and clear the per-phase cycle counters of the encode kernel.
-extern "C" __attribute__((visibility("default"))) void idx2g_debug_phase_cycles(unsigned long long* out)
-{
-  cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(g_phase_cycles));
-  unsigned long long z[16] = {};
-  cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
-}
-#endif
 
 void gpu_coder::value_range(double* vmin, double* vmax)
 {
-  *vmin = vmin_;
-  *vmax = vmax_;
+  *vmin = fields_[0].vmin;
+  *vmax = fields_[0].vmax;
 }
 
 } // namespace idx2g

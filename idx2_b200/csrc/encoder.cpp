@@ -197,7 +197,18 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
   if (e)
     return e;
   double t1 = now_s();
+  e = pack_dataset(f, p, plan, outs, files, write_files, timing);
+  if (timing)
+    timing->device_s = t1 - t0;
+  return e;
+}
 
+int pack_dataset(const dataset_format* f, const params* p, const encode_plan& plan,
+                 const std::vector<level_output>& outs, std::map<std::string, std::vector<uint8_t>>* files,
+                 bool write_files, encode_timing* timing)
+{
+  double t1 = now_s();
+  int e = NoError;
   packer pk(*f, f->tolerance);
   for (const encode_event& ev : plan.events)
   {
@@ -260,7 +271,6 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
   double t3 = now_s();
   if (timing)
   {
-    timing->device_s = t1 - t0;
     timing->pack_s = t2 - t1;
     timing->write_s = t3 - t2;
     timing->file_bytes = total;

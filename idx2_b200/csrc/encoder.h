@@ -125,6 +125,11 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
                    std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
                    encode_timing* timing);
 
+// Packing and files for the device stage's outputs (the second half of encode_dataset).
+int pack_dataset(const dataset_format* f, const params* p, const encode_plan& plan,
+                 const std::vector<level_output>& outs, std::map<std::string, std::vector<uint8_t>>* files,
+                 bool write_files, encode_timing* timing);
+
 // The device stage only: plan + every level through the coder.
 int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_output>* outs,
                   encode_plan* plan_out = nullptr);

@@ -139,6 +139,22 @@ IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2
 /* Metadata of an open dataset (the fields of the .idx2 file): name and field (64 bytes
    each, NUL-terminated), dims, dtype, number of levels, encode tolerance, and the bytes
    the dataset keeps resident on the device. */
+/* Batched encode: n fields (params[i], field[i]) through one device stage, then each is
+   packed and written as idx2g_encode writes it (the files are identical). The reference
+   encodes one field per call (Core/idx2Encode.cpp:390 Encode); here the bricks of every
+   field share each level's launch, so many small or uneven fields fill the GPU together.
+   flags: IDX2G_BATCH_GRAPH captures the level launches in one CUDA graph;
+   IDX2G_BATCH_DEVICE_ONLY stops after the device stage (no packing, no files);
+   IDX2G_BATCH_AUTOTUNE times the launch shapes once per batch signature (field count, total
+   bricks, dtypes) on the context and keeps the fastest. infos may be null, else n entries;
+   kernel_ms and device_s are those of the whole batch. Fields rejected by the format rules
+   make the call fail with that error before any work. */
+#define IDX2G_BATCH_GRAPH 1
+#define IDX2G_BATCH_DEVICE_ONLY 2
+#define IDX2G_BATCH_AUTOTUNE 4
+IDX2G_API int idx2g_encode_batch(idx2g_ctx* ctx, const idx2g_params* params, const void* const* fields,
+                                 int n, int fields_on_device, int flags, idx2g_encode_info* infos);
+
 /* Number of kernels this library has launched on the context so far (a diagnostic for
    benchmarks; no counterpart in the reference). */
 IDX2G_API long long idx2g_ctx_launches(const idx2g_ctx* ctx);

@@ -1,0 +1,84 @@
+"""Batched encode (idx2g_encode_batch): many uneven fields through one device stage must give,
+field by field, the files of the single-field encode (which is itself checked against the
+reference), with and without the CUDA graph, and with the device stage alone."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from idx2_files import compare_dirs
+
+
+def _batch_fields(n, seed, max_side=110):
+    import idx2_b200
+    from idx2_b200.synthetic import bumps_field
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < n:
+        dims = [int(rng.integers(17, max_side + 1)) for _ in range(3)]
+        is2d = rng.integers(0, 8) == 0
+        if is2d:
+            dims[2] = 1
+        dt = "float32" if rng.integers(0, 2) == 0 else "float64"
+        levels = int(rng.integers(1, 4))
+        bd = (32, 32, 1) if is2d else (32, 32, 32)
+        p = idx2_b200.Params(dims=dims, dtype=dt, brick_dims=bd, num_levels=levels, tolerance=1e-3)
+        if idx2_b200.check_params(p) != 0:
+            continue  # rejected by the format rules (the reference rejects it too)
+        f = bumps_field(dims[0], dims[1], dims[2], seed=int(rng.integers(1 << 30)))
+        out.append((f.astype(np.float32 if dt == "float32" else np.float64), levels))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("graph", [True, False])
+def test_batch_matches_single_field_encode(idx2g, tmp_path, graph):
+    fields = _batch_fields(10, seed=21)
+    names = [f"b{i}" for i in range(len(fields))]
+    for (f, lv), nm in zip(fields, names):
+        idx2g.encode(f, out_dir=str(tmp_path / "single"), name=nm, field_name="f", num_levels=lv,
+                     tolerance=1e-3)
+    infos = idx2g.encode_batch([f for f, _ in fields], out_dir=str(tmp_path / "batch"), names=names,
+                               field_names=["f"] * len(fields), num_levels=[lv for _, lv in fields],
+                               tolerances=[1e-3] * len(fields), graph=graph, autotune=True)
+    assert len(infos) == len(fields)
+    assert infos[0].kernel_launches == max(lv for _, lv in fields)  # one launch per level
+    for nm in names:
+        diffs = compare_dirs(str(tmp_path / "single" / nm), str(tmp_path / "batch" / nm))
+        assert diffs == [], (nm, diffs[:3])
+
+
+@pytest.mark.gpu
+def test_batch_from_device_tensors_matches_reference(idx2g, ref_app, tmp_path):
+    import torch
+    fields = _batch_fields(6, seed=22, max_side=90)
+    names = [f"d{i}" for i in range(len(fields))]
+    idx2g.encode_batch([torch.from_numpy(f).cuda() for f, _ in fields], out_dir=str(tmp_path / "batch"),
+                       names=names, field_names=["f"] * len(fields), num_levels=[lv for _, lv in fields],
+                       tolerances=[1e-3] * len(fields))
+    for (f, lv), nm in zip(fields, names):
+        nz, ny, nx = f.shape if f.ndim == 3 else (1,) + f.shape
+        dt = "Float32" if f.dtype == np.float32 else "Float64"
+        raw = str(tmp_path / f"{nm}-f-[{nx}-{ny}-{nz}]-{dt}.raw")
+        f.tofile(raw)
+        args = [ref_app, "--encode", raw, "--num_levels", str(lv), "--tolerance", "0.001",
+                "--out_dir", str(tmp_path / "ref")]
+        if nz == 1:
+            args += ["--brick_size", "32", "32", "1"]
+        r = subprocess.run(args, capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout[-300:] + r.stderr[-300:]
+        diffs = compare_dirs(str(tmp_path / "ref" / nm), str(tmp_path / "batch" / nm))
+        assert diffs == [], (nm, diffs[:3])
+
+
+@pytest.mark.gpu
+def test_batch_device_only(idx2g, tmp_path):
+    fields = _batch_fields(5, seed=23, max_side=80)
+    infos = idx2g.encode_batch([f for f, _ in fields], out_dir=str(tmp_path / "none"),
+                               num_levels=[lv for _, lv in fields], tolerances=[1e-3] * len(fields),
+                               device_only=True)
+    assert not os.path.exists(str(tmp_path / "none"))
+    for (f, _), info in zip(fields, infos):
+        assert info.value_min == pytest.approx(float(f.min()))
+        assert info.value_max == pytest.approx(float(f.max()))
