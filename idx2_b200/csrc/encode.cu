@@ -131,6 +131,7 @@ struct enc_smem
   uint32_t key_base[kKeyWindow];
   uint32_t stage[kStageBytes / 4];  // one (brick, subband) region being assembled
   unsigned alloc, hdr;
+  enc_field fp;  // parameters of the current brick's field
   dev::lift_stack stack;
   double red[2][kWarps];
   int kmin, kmax;
@@ -270,7 +271,16 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
   for (int bi = blockIdx.x; bi < a.nbricks; bi += gridDim.x)
   {
     const enc_brick& br = a.bricks[bi];
-    const enc_field& fp = a.fields[br.field];
+    {
+      // the field's parameters to shared memory (read often, and across barriers)
+      static_assert(sizeof(enc_field) % 4 == 0, "enc_field is copied as words");
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(a.fields + br.field);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&sm.fp);
+      for (int i = tid; i < (int)(sizeof(enc_field) / 4); i += kThreads)
+        dst[i] = src[i];
+    }
+    __syncthreads();
+    const enc_field& fp = sm.fp;
     const int N[3] = { 33, 33, fp.is2d ? 1 : 33 };
     const int NB = N[0] * N[1] * N[2];
     const int SZ = fp.is2d ? 0 : 2 * 33 * 33;  // sample stride along z inside a subband
@@ -606,18 +616,6 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         const int npM = npA > npB ? npA : npB;
         unsigned long long* XA = Xp + bA;  // plane k at XA[k * kRowX]
         unsigned long long* XB = Xp + bB;
-        for (int k = 0; k < npM; ++k)
-        {
-          const int bit = 63 - k;
-          const unsigned a0 = __ballot_sync(0xffffffffu, (uA0 >> bit) & 1ull);
-          const unsigned a1 = __ballot_sync(0xffffffffu, (uA1 >> bit) & 1ull);
-          const unsigned b0 = __ballot_sync(0xffffffffu, (uB0 >> bit) & 1ull);
-          const unsigned b1 = __ballot_sync(0xffffffffu, (uB1 >> bit) & 1ull);
-          if (lane == 0 && k < npA)
-            XA[k * kRowX] = (unsigned long long)a0 | ((unsigned long long)a1 << 32);
-          if (lane == 1 && k < npB)
-            XB[k * kRowX] = (unsigned long long)b0 | ((unsigned long long)b1 << 32);
-        }
         if (lane == 0)
         {
           sm.emax[bA] = (int16_t)eA;
@@ -632,30 +630,44 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
           sm.np[bB] = (uint8_t)npB;
           sm.nvals_log[bB] = (uint8_t)(2 * ndB);
         }
-        __syncwarp();
-        // significance chain: nin(k) = max over planes k' < k of the highest one-bit + 1
-        // (Core/Zfp.h:771), an exclusive prefix maximum over the planes; plane lengths
+        // Bit planes by warp transposes: transposing the high words of (uA0 | uA1) gives lane c
+        // the mask of plane k = 31 - c (bit 63 - k of every coefficient), the low words planes
+        // 32..63 (k = 63 - c). Then the significance chain (Core/Zfp.h:771): nin(k) = max over
+        // planes k' < k of the highest one-bit + 1, a suffix maximum over the lanes; and the
+        // plane lengths.
         {
           int carryA = 0, carryB = 0;
-          for (int k0 = 0; k0 < npM; k0 += 32)
+          const int ngroups = npM > 32 ? 2 : 1;
+          for (int g = 0; g < ngroups; ++g)
           {
-            const int k = k0 + lane;
-            const unsigned long long xa = k < npA ? XA[k * kRowX] : 0ull;
-            const unsigned long long xb = k < npB ? XB[k * kRowX] : 0ull;
-            int ma = xa ? 64 - __clzll(xa) : 0, mb = xb ? 64 - __clzll(xb) : 0;
-            int ia = ma, ib = mb;  // inclusive prefix max
+            const int sh = g ? 0 : 32;
+            const int k = 31 - lane + 32 * g;
+            unsigned long long xa =
+              (unsigned long long)dev::warp_transpose32((uint32_t)(uA0 >> sh), lane) |
+              ((unsigned long long)dev::warp_transpose32((uint32_t)(uA1 >> sh), lane) << 32);
+            unsigned long long xb =
+              (unsigned long long)dev::warp_transpose32((uint32_t)(uB0 >> sh), lane) |
+              ((unsigned long long)dev::warp_transpose32((uint32_t)(uB1 >> sh), lane) << 32);
+            xa = k < npA ? xa : 0ull;
+            xb = k < npB ? xb : 0ull;
+            if (k < npA)
+              XA[k * kRowX] = xa;
+            if (k < npB)
+              XB[k * kRowX] = xb;
+            // inclusive maximum over planes <= k, i.e. over lanes >= lane
+            int ia = xa ? 64 - __clzll(xa) : 0, ib = xb ? 64 - __clzll(xb) : 0;
             for (int o = 1; o < 32; o <<= 1)
             {
-              const int ta = __shfl_up_sync(0xffffffffu, ia, o), tb = __shfl_up_sync(0xffffffffu, ib, o);
-              if (lane >= o)
+              const int ta = __shfl_down_sync(0xffffffffu, ia, o), tb = __shfl_down_sync(0xffffffffu, ib, o);
+              if (lane + o < 32)
               {
                 ia = ia > ta ? ia : ta;
                 ib = ib > tb ? ib : tb;
               }
             }
-            int ea = __shfl_up_sync(0xffffffffu, ia, 1), eb = __shfl_up_sync(0xffffffffu, ib, 1);
-            ea = lane ? ea : 0;
-            eb = lane ? eb : 0;
+            int ea = __shfl_down_sync(0xffffffffu, ia, 1), eb = __shfl_down_sync(0xffffffffu, ib, 1);
+            ea = lane < 31 ? ea : 0;
+            eb = lane < 31 ? eb : 0;
             const int nA_ = ea > carryA ? ea : carryA, nB_ = eb > carryB ? eb : carryB;
             if (k < npA)
             {
@@ -667,7 +679,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
               NIN[k * kRowNin + bB] = (uint8_t)nB_;
               OFF[k * kRowOff + bB] = (uint16_t)dev::plane_bits(xb, nB_, nvB);
             }
-            const int ta = __shfl_sync(0xffffffffu, ia, 31), tb = __shfl_sync(0xffffffffu, ib, 31);
+            const int ta = __shfl_sync(0xffffffffu, ia, 0), tb = __shfl_sync(0xffffffffu, ib, 0);
             carryA = carryA > ta ? carryA : ta;
             carryB = carryB > tb ? carryB : tb;
           }
@@ -1303,6 +1315,16 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
   *out = std::move(outs_[(size_t)level]);
   return NoError;
 }
+
+#ifdef IDX2G_PHASE_TIMING
+// Profiling builds: read and clear the per-phase cycle counters of the encode kernel.
+extern "C" __attribute__((visibility("default"))) void idx2g_debug_phase_cycles(unsigned long long* out)
+{
+  cudaMemcpyFromSymbol(out, g_phase_cycles, sizeof(g_phase_cycles));
+  unsigned long long z[16] = {};
+  cudaMemcpyToSymbol(g_phase_cycles, z, sizeof(z));
+}
+#endif
 
 void gpu_coder::value_range(double* vmin, double* vmax)
 {
