@@ -429,6 +429,53 @@ def batched_leg(dev, h, nfields=512, seed=7, reps=3):
             "timing": "wall clock of the device stage (fields resident on the device), median of 3"}
 
 
+def serve_leg(args):
+    """Decode serving: a device-resident compressed k^-5/3 field (3 levels, encoded at 1e-6)
+    answering a Poisson stream of ROI requests (sides 32-512, per-axis downsampling 0-3,
+    tolerance log-uniform 1e-6..1e-1), batched on arrival under the free-HBM budget, against
+    one-request-at-a-time decode of the same schedule. Prints one JSON line."""
+    import torch
+    import idx2_b200
+    from idx2_b200.synthetic import grf_field_torch
+    from idx2_b200.serving import Server, dataset_decoder, free_hbm_budget, poisson_schedule
+    dims = tuple(int(x) for x in args.serve_dims.split("x"))
+    dev = torch.device("cuda", 0)
+    tmp = tempfile.mkdtemp(prefix="idx2serve_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        t0 = time.perf_counter()
+        f = grf_field_torch(dims[0], dims[1], dims[2], seed=11, scale="unit", device=dev)
+        info = idx2_b200.encode(f, out_dir=tmp, name="serve", field_name="f", num_levels=3, tolerance=1e-6)
+        raw = f.numel() * f.element_size()
+        del f
+        torch.cuda.empty_cache()
+        ds = idx2_b200.Dataset(os.path.join(tmp, "serve", "f.idx2"))
+        setup_s = time.perf_counter() - t0
+        budget = free_hbm_budget()
+        dec = dataset_decoder(ds)
+        warm = poisson_schedule(32, args.serve_rate, dims, seed=1)
+        Server(dec, budget).run(warm, batched=True)
+        res = {}
+        for mode in ("batched", "one-at-a-time"):
+            sched = poisson_schedule(args.serve_requests, args.serve_rate, dims, seed=2)
+            st = Server(dec, budget).run(sched, batched=(mode == "batched"))
+            d = st.as_dict()
+            d["decoded_gbs"] = st.decoded_bytes / st.elapsed_s / 1e9
+            res[mode] = d
+        line = {"metric": "decode serving p50/p99 ms (ROI requests)", "impl": "ours",
+                "config": {"workload": f"serving: {dims[0]}x{dims[1]}x{dims[2]} float32 k^-5/3 field, 3 levels, "
+                                       f"encoded at 1e-6; Poisson {args.serve_rate:g} req/s, "
+                                       f"{args.serve_requests} requests, ROI sides 32-512, downsampling 0-3, "
+                                       f"tolerance log-uniform 1e-6..1e-1",
+                           "raw_bytes": int(raw), "compressed_bytes": int(info.file_bytes),
+                           "hbm_budget_bytes": int(budget), "setup_s": setup_s},
+                "batched": res["batched"], "one_at_a_time": res["one-at-a-time"],
+                "p99_speedup": res["one-at-a-time"]["p99_ms"] / max(res["batched"]["p99_ms"], 1e-9)}
+        print(json.dumps(line))
+        ds.close()
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -439,10 +486,18 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg (profiling runs)")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-field batched-encode leg")
+    ap.add_argument("--serve", action="store_true", help="run the decode-serving benchmark instead")
+    ap.add_argument("--serve-dims", default="2048x2048x1024", help="serving field dims (x, y, z)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrival rate (per second)")
+    ap.add_argument("--serve-requests", type=int, default=2000, help="requests per mode")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.serve:
+        if rank == 0:
+            serve_leg(args)
+        return
     if args.impl == "reference":
         reference_arm(args, rank, world)
     else:

@@ -481,6 +481,22 @@ IDX2G_API int idx2g_decode(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* 
   return dataset_decode(&c->d, (dataset_handle*)ds, p, out, out_bytes, out_on_device != 0, kernel_ms);
 }
 
+IDX2G_API int idx2g_decode_batch(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* in, int n,
+                                 void* const* outs, const size_t* out_bytes, int out_on_device, double* kernel_ms)
+{
+  if (!c || !ds || !in || !outs || !out_bytes || n < 0)
+    return InvalidArgument;
+  std::vector<params> ps((size_t)n);
+  for (int i = 0; i < n; ++i)
+  {
+    if (!outs[i])
+      return InvalidArgument;
+    to_params(in + i, &ps[(size_t)i]);
+  }
+  return dataset_decode_batch(&c->d, (dataset_handle*)ds, ps.data(), n, outs, out_bytes, out_on_device != 0,
+                              kernel_ms);
+}
+
 // Allocation-free decode (include/idx2g.h): for callers that cannot allocate device memory at
 // decode time; all temporaries are in the fixed scratch array of decode.cu.
 IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* in, void* d_out,

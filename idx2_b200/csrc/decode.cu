@@ -99,66 +99,128 @@ int decode_device::upload(device_ctx* ctx, const std::vector<int16_t>& exps, con
 int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, size_t out_bytes,
                           bool out_on_device, double* kernel_ms)
 {
+  std::vector<const decode_request*> rqs(1, &rq);
+  return decode_batch(ctx, rqs, &out, &out_bytes, out_on_device, kernel_ms);
+}
+
+int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_request*>& rqs,
+                                void* const* outs, const size_t* out_bytes, bool out_on_device, double* kernel_ms)
+{
+  const size_t n = rqs.size();
+  if (n == 0)
+    return NoError;
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
-  const int NB = 33 * 33 * (rq.is2d ? 1 : 33);
-  auto cleanup = []() {};
-  void* d_out = out;
+  const decode_request& r0 = *rqs[0];  // the dataset-wide fields are common to all requests
+  const int NB = 33 * 33 * (r0.is2d ? 1 : 33);
+  const int L = r0.nlevels;
+  // output grids on the device
+  std::vector<void*> d_out(n);
   if (!out_on_device)
   {
-    d_out = ctx->ws("dec.out", out_bytes);
-    if (!d_out)
+    size_t total = 0;
+    for (size_t i = 0; i < n; ++i)
+      total += (out_bytes[i] + 255) & ~(size_t)255;
+    uint8_t* stage = (uint8_t*)ctx->ws("dec.out", total);
+    if (!stage)
       return OutOfMemory;
+    size_t at = 0;
+    for (size_t i = 0; i < n; ++i)
+    {
+      d_out[i] = stage + at;
+      at += (out_bytes[i] + 255) & ~(size_t)255;
+    }
   }
-  cudaMemsetAsync(d_out, 0, out_bytes, st);
+  else
+    for (size_t i = 0; i < n; ++i)
+      d_out[i] = outs[i];
+  for (size_t i = 0; i < n; ++i)
+    if (out_bytes[i])
+      cudaMemsetAsync(d_out[i], 0, out_bytes[i], st);
   int* d_err = (int*)ctx->ws("dec.err", 16);  // [0] brick kernel, [1] plane kernel
   uint64_t* d_geom = (uint64_t*)ctx->ws("dec.geom", sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
   if (!d_err || !d_geom)
-  {
-    cleanup();
     return OutOfMemory;
-  }
   cudaMemsetAsync(d_err, 0, 16, st);
   const size_t smem = sizeof(dec_smem);
   cudaFuncSetAttribute(k_decode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaEvent_t e0 = ctx->ev0, e1 = ctx->ev1;
   float total_ms = 0;
   double* prev = nullptr;
+  std::vector<int> prev_base(n, -1), cur_base(n, -1);
+  std::vector<decode_brick> hb;
+  std::vector<decode_target> targets;
   int li = 0;
-  for (const decode_level& lv : rq.levels)
+  for (int l = L - 1; l >= 0; --l)
   {
-    ++li;
-    const int nbr = (int)lv.bricks.size();
-    if (nbr == 0)
-      continue;
-    decode_brick* d_bricks = (decode_brick*)ctx->ws("dec.bricks", sizeof(decode_brick) * (size_t)nbr);
-    double* d_level =
-      lv.is_output ? nullptr : (double*)ctx->ws(li % 2 ? "dec.levA" : "dec.levB", (size_t)nbr * (size_t)NB * 8);
-    int grid = nbr < 2 * ctx->num_sms ? nbr : 2 * ctx->num_sms;
-    double* d_slots = lv.is_output ? (double*)ctx->ws("dec.slots", (size_t)grid * (size_t)NB * 8) : nullptr;
-    if (!d_bricks || (!lv.is_output && !d_level) || (lv.is_output && !d_slots))
+    const size_t k = (size_t)(L - 1 - l);  // entry of level l in a request's level list
+    hb.clear();
+    targets.clear();
+    const decode_level* lw = nullptr;  // level-wide tables (common to all requests)
+    int nstore = 0;
+    for (size_t i = 0; i < n; ++i)
     {
-      cleanup();
-      return OutOfMemory;
+      cur_base[i] = -1;
+      const decode_request& rq = *rqs[i];
+      if (k >= rq.levels.size())
+        continue;
+      const decode_level& lv = rq.levels[k];
+      if (lv.bricks.empty())
+        continue;
+      lw = &lv;
+      decode_target t;
+      memset(&t, 0, sizeof t);
+      t.mask = lv.mask;
+      t.is_output = lv.is_output;
+      t.etol = rq.etol;
+      memcpy(t.spacing, lv.spacing, sizeof t.spacing);
+      t.out = d_out[i];
+      t.out_dims[0] = rq.out_dims.x;
+      t.out_dims[1] = rq.out_dims.y;
+      t.out_dims[2] = rq.out_dims.z;
+      const int ti = (int)targets.size();
+      targets.push_back(t);
+      cur_base[i] = lv.is_output ? -1 : nstore;
+      for (const decode_brick& b : lv.bricks)
+      {
+        decode_brick db = b;
+        db.req = ti;
+        db.parent = b.parent >= 0 && prev_base[i] >= 0 ? prev_base[i] + b.parent : -1;
+        db.store = lv.is_output ? -1 : nstore++;
+        hb.push_back(db);
+      }
     }
-    cudaMemcpyAsync(d_bricks, lv.bricks.data(), sizeof(decode_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_geom, lv.geom, sizeof(uint64_t) * 8 * kMaxBlocksPerSubband, cudaMemcpyHostToDevice, st);
+    prev_base = cur_base;
+    const int nbr = (int)hb.size();
+    if (nbr == 0)
+    {
+      prev = nullptr;
+      continue;
+    }
+    ++li;
+    decode_brick* d_bricks = (decode_brick*)ctx->ws("dec.bricks", sizeof(decode_brick) * (size_t)nbr);
+    decode_target* d_reqs = (decode_target*)ctx->ws("dec.reqs", sizeof(decode_target) * targets.size());
+    double* d_level = nstore ? (double*)ctx->ws(li % 2 ? "dec.levA" : "dec.levB", (size_t)nstore * (size_t)NB * 8)
+                             : nullptr;
+    int grid = nbr < 2 * ctx->num_sms ? nbr : 2 * ctx->num_sms;
+    double* d_slots = (double*)ctx->ws("dec.slots", (size_t)grid * (size_t)NB * 8);
+    if (!d_bricks || !d_reqs || (nstore && !d_level) || !d_slots)
+      return OutOfMemory;
+    cudaMemcpyAsync(d_bricks, hb.data(), sizeof(decode_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_reqs, targets.data(), sizeof(decode_target) * targets.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_geom, lw->geom, sizeof(uint64_t) * 8 * kMaxBlocksPerSubband, cudaMemcpyHostToDevice, st);
     dec_args a;
     memset(&a, 0, sizeof a);
-    a.level = lv.level;
-    a.nlevels = rq.nlevels;
-    a.is2d = rq.is2d;
-    a.nsb = rq.nsb;
+    a.level = l;
+    a.nlevels = L;
+    a.is2d = r0.is2d;
+    a.nsb = r0.nsb;
     a.nbricks = nbr;
-    a.etol = rq.etol;
-    a.end_bp = rq.f32 ? 32 : 64;
-    a.mask = lv.mask;
-    a.norm_mask = lv.norm_mask;
-    a.is_output = lv.is_output;
-    a.out_f32 = rq.f32;
-    memcpy(a.spacing, lv.spacing, sizeof a.spacing);
-    memcpy(a.nblocks, lv.nblocks, sizeof a.nblocks);
-    memcpy(a.inv_weight, lv.inv_weight, sizeof a.inv_weight);
+    a.end_bp = r0.f32 ? 32 : 64;
+    a.norm_mask = lw->norm_mask;
+    a.out_f32 = r0.f32;
+    memcpy(a.nblocks, lw->nblocks, sizeof a.nblocks);
+    memcpy(a.inv_weight, lw->inv_weight, sizeof a.inv_weight);
     a.geom = d_geom;
     a.bricks = d_bricks;
     a.exps = exps_;
@@ -171,34 +233,27 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
     a.parents = prev;
     a.bricks_out = d_level;
     a.slots = d_slots;
-    a.out = d_out;
-    a.out_dims[0] = rq.out_dims.x;
-    a.out_dims[1] = rq.out_dims.y;
-    a.out_dims[2] = rq.out_dims.z;
+    a.reqs = d_reqs;
     a.error = d_err;
 
     // bit planes of every (brick, subband) of the level: one warp each, tables allocated
     // with a cursor in a grow-only workspace (relaunched larger if it overflows)
-    const size_t nunits = (size_t)nbr * (size_t)rq.nsb;
+    const size_t nunits = (size_t)nbr * (size_t)r0.nsb;
     unsigned long long* d_uoff = (unsigned long long*)ctx->ws("dec.unitoff", nunits * 8);
     unsigned long long* d_pcur = (unsigned long long*)ctx->ws("dec.pcursor", 16);
     int* d_wide = (int*)ctx->ws("dec.widelist", nunits * 4);
     if (!d_uoff || !d_pcur || !d_wide)
-    {
-      cleanup();
       return OutOfMemory;
-    }
     unsigned long long cap = (unsigned long long)nunits * 16384ull + (16ull << 20);
     if (ctx->ws_size("dec.planes") > cap)
       cap = ctx->ws_size("dec.planes");
     dec1_args pa;
     memset(&pa, 0, sizeof pa);
-    pa.nsb = rq.nsb;
+    pa.nsb = r0.nsb;
     pa.nbricks = nbr;
-    pa.etol = rq.etol;
     pa.end_bp = a.end_bp;
-    pa.mask = lv.mask;
-    memcpy(pa.nblocks, lv.nblocks, sizeof pa.nblocks);
+    pa.reqs = d_reqs;
+    memcpy(pa.nblocks, lw->nblocks, sizeof pa.nblocks);
     pa.geom = d_geom;
     pa.bricks = d_bricks;
     pa.exps = exps_;
@@ -219,10 +274,7 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
     {
       unsigned long long* d_planes = (unsigned long long*)ctx->ws("dec.planes", (size_t)cap);
       if (!d_planes)
-      {
-        cleanup();
         return OutOfMemory;
-      }
       cap = ctx->ws_size("dec.planes");
       pa.planes = d_planes;
       pa.cap_bytes = cap;
@@ -233,17 +285,11 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
       ++ctx->launches;
       cudaEventRecord(e1, st);
       if (cudaGetLastError() != cudaSuccess)
-      {
-        cleanup();
         return CudaError;
-      }
       unsigned long long pc[2] = { 0, 0 };
       cudaMemcpyAsync(pc, d_pcur, 16, cudaMemcpyDeviceToHost, st);
       if (cudaStreamSynchronize(st) != cudaSuccess)
-      {
-        cleanup();
         return CudaError;
-      }
       float pms = 0;
       cudaEventElapsedTime(&pms, e0, e1);
       level_ms += pms;
@@ -256,30 +302,21 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
         ++ctx->launches;
         cudaEventRecord(e1, st);
         if (cudaGetLastError() != cudaSuccess)
-        {
-          cleanup();
           return CudaError;
-        }
       }
       int perr = 0;
       unsigned long long used = 0;
       cudaMemcpyAsync(&perr, d_err + 1, 4, cudaMemcpyDeviceToHost, st);
       cudaMemcpyAsync(&used, d_pcur, 8, cudaMemcpyDeviceToHost, st);
       if (cudaStreamSynchronize(st) != cudaSuccess)
-      {
-        cleanup();
         return CudaError;
-      }
       if (nwide > 0)
       {
         cudaEventElapsedTime(&pms, e0, e1);
         level_ms += pms;
       }
       if (perr == 1)
-      {
-        cleanup();
         return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
-      }
       if (perr == 2)
       {
         cap = used + (1ull << 20);
@@ -290,38 +327,27 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
       break;
     }
     if (!a.planes)
-    {
-      cleanup();
       return DeviceStreamOverflow;
-    }
     cudaEventRecord(e0, st);
     k_decode_level<<<grid, kThreads, smem, st>>>(a);
     ++ctx->launches;
     cudaEventRecord(e1, st);
     if (cudaGetLastError() != cudaSuccess)
-    {
-      cleanup();
       return CudaError;
-    }
     if (cudaStreamSynchronize(st) != cudaSuccess)
-    {
-      cleanup();
       return CudaError;
-    }
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     total_ms += ms + level_ms;
     prev = d_level;
-    if (lv.is_output)
-      break;
   }
   int herr = 0;
   cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, st);
   if (!out_on_device)
-    cudaMemcpyAsync(out, d_out, out_bytes, cudaMemcpyDeviceToHost, st);
-  cudaError_t ce = cudaStreamSynchronize(st);
-  cleanup();
-  if (ce != cudaSuccess)
+    for (size_t i = 0; i < n; ++i)
+      if (out_bytes[i])
+        cudaMemcpyAsync(outs[i], d_out[i], out_bytes[i], cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess)
     return CudaError;
   if (herr)
     return DeviceStreamOverflow;
@@ -363,7 +389,8 @@ constexpr size_t kOffLevB = kOffLevA + (size_t)kNoAllocLevelBricks * kBrickBytes
 constexpr size_t kOffBricks = kOffLevB + (size_t)kNoAllocLevelBricks * kBrickBytes;
 constexpr size_t kOffGeom = kOffBricks + (((size_t)kNoAllocMaxBricks * sizeof(decode_brick) + 255) & ~(size_t)255);
 constexpr size_t kOffErr = kOffGeom + sizeof(uint64_t) * 8 * kMaxBlocksPerSubband;
-constexpr size_t kNoAllocScratchBytes = kOffErr + 256;
+constexpr size_t kOffReq = kOffErr + 256;
+constexpr size_t kNoAllocScratchBytes = kOffReq + ((sizeof(decode_target) + 255) & ~(size_t)255);
 
 static __device__ __align__(256) unsigned char g_decode_scratch[kNoAllocScratchBytes];
 
@@ -422,6 +449,7 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
   decode_brick* d_bricks = (decode_brick*)(base + kOffBricks);
   uint64_t* d_geom = (uint64_t*)(base + kOffGeom);
   int* d_err = (int*)(base + kOffErr);
+  decode_target* d_req = (decode_target*)(base + kOffReq);
   cudaMemsetAsync(d_out, 0, out_bytes, st);
   cudaMemsetAsync(d_err, 0, 16, st);
   const size_t smem = sizeof(dec_smem);
@@ -439,6 +467,17 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
     int grid = lv.is_output ? (nbr < kNoAllocSlots ? nbr : kNoAllocSlots) : nbr;
     cudaMemcpyAsync(d_bricks, lv.bricks.data(), sizeof(decode_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_geom, lv.geom, sizeof(uint64_t) * 8 * kMaxBlocksPerSubband, cudaMemcpyHostToDevice, st);
+    decode_target t;
+    memset(&t, 0, sizeof t);
+    t.mask = lv.mask;
+    t.is_output = lv.is_output;
+    t.etol = rq.etol;
+    memcpy(t.spacing, lv.spacing, sizeof t.spacing);
+    t.out = d_out;
+    t.out_dims[0] = rq.out_dims.x;
+    t.out_dims[1] = rq.out_dims.y;
+    t.out_dims[2] = rq.out_dims.z;
+    cudaMemcpyAsync(d_req, &t, sizeof t, cudaMemcpyHostToDevice, st);
     dec_args a;
     memset(&a, 0, sizeof a);
     a.level = lv.level;
@@ -446,13 +485,9 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
     a.is2d = rq.is2d;
     a.nsb = rq.nsb;
     a.nbricks = nbr;
-    a.etol = rq.etol;
     a.end_bp = rq.f32 ? 32 : 64;
-    a.mask = lv.mask;
     a.norm_mask = lv.norm_mask;
-    a.is_output = lv.is_output;
     a.out_f32 = rq.f32;
-    memcpy(a.spacing, lv.spacing, sizeof a.spacing);
     memcpy(a.nblocks, lv.nblocks, sizeof a.nblocks);
     memcpy(a.inv_weight, lv.inv_weight, sizeof a.inv_weight);
     a.geom = d_geom;
@@ -467,10 +502,7 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
     a.parents = prev;
     a.bricks_out = d_level;
     a.slots = slots;
-    a.out = d_out;
-    a.out_dims[0] = rq.out_dims.x;
-    a.out_dims[1] = rq.out_dims.y;
-    a.out_dims[2] = rq.out_dims.z;
+    a.reqs = d_req;
     a.error = d_err;
     (void)NB;
     cudaEventRecord(ctx->ev0, st);

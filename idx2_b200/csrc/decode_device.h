@@ -10,14 +10,29 @@
 namespace idx2g
 {
 
-// One brick of a decode request.
+// One brick of a decode launch.
 struct decode_brick
 {
   long long flat;  // row in the flat (level, brick) tables
-  int parent;      // index of the parent in the previous (coarser) decoded level, -1 if none
+  int parent;      // the parent's store index in the previous (coarser) launch, -1 if none
   int pos[3];      // position inside the parent
   // output copy (only on the output level): brick-local source grid and output grid
   int src_from[3], src_strd[3], dims[3], dst_from[3], dst_strd[3];
+  int req;         // entry of the launch's request table
+  int store;       // index in the launch's array of kept bricks (-1: output brick)
+};
+
+// What one request needs on one level (a launch may serve the bricks of many requests).
+struct decode_target
+{
+  int mask;           // decoded subbands
+  int is_output;      // the request's finest level: bricks go to the output grid
+  int etol;           // Exponent(tolerance)
+  int pad;
+  int spacing[8][3];  // per subband: blocks not on this spacing are skipped (BypassDecode)
+  void* out;          // output grid (device)
+  int out_dims[3];
+  int pad2;
 };
 
 struct decode_level
@@ -51,6 +66,10 @@ public:
              const std::vector<uint64_t>& off, const uint8_t* blob, size_t blob_bytes);
   int decode(device_ctx* ctx, const decode_request& rq, void* out, size_t out_bytes, bool out_on_device,
              double* kernel_ms);
+  // Several requests on this dataset at once: per level one launch (of each kernel) over the
+  // bricks of every request that decodes the level. outs[i] receives request i's grid.
+  int decode_batch(device_ctx* ctx, const std::vector<const decode_request*>& rqs, void* const* outs,
+                   const size_t* out_bytes, bool out_on_device, double* kernel_ms);
   // Allocation-free decode into a device buffer: every temporary lives in a fixed static
   // device array of decode.cu (limits and semantics there and in include/idx2g.h).
   int decode_noalloc(device_ctx* ctx, const decode_request& rq, void* d_out, size_t out_bytes,

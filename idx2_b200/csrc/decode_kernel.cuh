@@ -36,8 +36,7 @@ constexpr int kRing = 32;  // steps a decoded plane stays in the per-warp ring (
 
 struct dec_args
 {
-  int level, nlevels, is2d, nsb, nbricks, etol, end_bp, mask, norm_mask, is_output, out_f32;
-  int spacing[8][3];
+  int level, nlevels, is2d, nsb, nbricks, end_bp, norm_mask, out_f32;
   int nblocks[8];
   double inv_weight[8];
   const uint64_t* geom;               // [8][kMaxBlocksPerSubband]
@@ -49,11 +48,10 @@ struct dec_args
   const unsigned long long* coff;
   const uint8_t* blob;
   unsigned long long blob_bytes;
-  const double* parents;              // decoded bricks of the coarser level
-  double* bricks_out;                 // decoded bricks of this level (non-output level)
-  double* slots;                      // per-CTA slots (output level)
-  void* out;
-  int out_dims[3];
+  const double* parents;              // kept bricks of the coarser launch
+  double* bricks_out;                 // kept bricks of this launch (by store index)
+  double* slots;                      // per-CTA slots (output bricks)
+  const decode_target* reqs;          // request table of the launch
   int* error;
   // decoded bit planes from k_decode_planes (null: the kernel runs the wavefront itself)
   const unsigned long long* planes;
@@ -63,7 +61,8 @@ struct dec_args
 // Arguments of the bit-plane kernel (one warp per (brick, subband) unit).
 struct dec1_args
 {
-  int nsb, nbricks, etol, end_bp, mask;
+  int nsb, nbricks, end_bp;
+  const decode_target* reqs;
   int nblocks[8];
   const uint64_t* geom;  // [8][kMaxBlocksPerSubband]
   const decode_brick* bricks;
@@ -108,6 +107,7 @@ struct dec_smem
   uint8_t stop[2][kKeyWindow];
   int kmax[8], nkeys[8];
   int wide;
+  decode_target rq;  // the current brick's request
 };
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
@@ -427,7 +427,8 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_plane
   {
     const int unit = WIDE ? a.wide_list[i] : i;
     const int bi = unit / a.nsb, s = unit - bi * a.nsb;
-    if (!((a.mask >> s) & 1))
+    const decode_target& rq = a.reqs[a.bricks[bi].req];
+    if (!((rq.mask >> s) & 1))
     {
       if (lane == 0)
         a.unit_off[unit] = ~0ull;
@@ -444,7 +445,7 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_plane
       int d3[3], bd[3];
       unpack_geom(a.geom[(size_t)s * kMaxBlocksPerSubband + b], d3, bd);
       const int emax = a.exps[fs * kMaxBlocksPerSubband + (size_t)b];
-      const int np = dev::coded_planes(emax, a.etol, a.end_bp);
+      const int np = dev::coded_planes(emax, rq.etol, a.end_bp);
       const int top = emax + 63 + 1024;
       ktop[b] = (int16_t)top;
       npl[b] = (uint8_t)np;
@@ -547,13 +548,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
   {
     const decode_brick& br = a.bricks[bi];
     DEC_PHASE_START
-    double* F = a.is_output ? a.slots + (size_t)blockIdx.x * (size_t)NB
-                            : a.bricks_out + (size_t)bi * (size_t)NB;
+    {
+      // the request's parameters to shared memory (read often, and across barriers)
+      static_assert(sizeof(decode_target) % 4 == 0, "decode_target is copied as words");
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(a.reqs + br.req);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&sm.rq);
+      for (int i = tid; i < (int)(sizeof(decode_target) / 4); i += kThreads)
+        dst[i] = src[i];
+    }
+    __syncthreads();
+    const decode_target& rq = sm.rq;
+    double* F = rq.is_output ? a.slots + (size_t)blockIdx.x * (size_t)NB
+                             : a.bricks_out + (size_t)br.store * (size_t)NB;
     // 1: zero + parent low band (Core/idx2Decode.cpp:285-293)
     for (int i = tid; i < NB; i += kThreads)
       F[i] = 0.0;
     __syncthreads();
-    if (br.parent >= 0 && a.parents && (a.mask & 1))
+    if (br.parent >= 0 && a.parents && (rq.mask & 1))
     {
       const double* P = a.parents + (size_t)br.parent * (size_t)NB;
       const int nz = a.is2d ? 1 : 16;
@@ -571,7 +582,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
     for (int i = tid; i < a.nsb * kMaxBlocksPerSubband; i += kThreads)
     {
       const int s = i / kMaxBlocksPerSubband, b = i % kMaxBlocksPerSubband;
-      if (!((a.mask >> s) & 1) || b >= a.nblocks[s])
+      if (!((rq.mask >> s) & 1) || b >= a.nblocks[s])
         continue;
       int d3[3], bd[3];
       unpack_geom(a.geom[(size_t)s * kMaxBlocksPerSubband + b], d3, bd);
@@ -579,18 +590,18 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       const int emax = a.exps[fs * kMaxBlocksPerSubband + (size_t)b];
       sm.emax[s][b] = (int16_t)emax;
       sm.ktop[s][b] = (int16_t)(emax + 63 + 1024);
-      sm.np[s][b] = (uint8_t)dev::coded_planes(emax, a.etol, a.end_bp);
+      sm.np[s][b] = (uint8_t)dev::coded_planes(emax, rq.etol, a.end_bp);
       sm.nbps[s][b] = 0;
       sm.nd[s][b] = (uint8_t)((bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1));
-      sm.bypass[s][b] = (uint8_t)((d3[0] % a.spacing[s][0]) != 0 || (d3[1] % a.spacing[s][1]) != 0 ||
-                                  (d3[2] % a.spacing[s][2]) != 0);
+      sm.bypass[s][b] = (uint8_t)((d3[0] % rq.spacing[s][0]) != 0 || (d3[1] % rq.spacing[s][1]) != 0 ||
+                                  (d3[2] % rq.spacing[s][2]) != 0);
     }
     __syncthreads();
     if (tid < a.nsb)
     {
       const int s = tid;
       int kmax = -(1 << 30), kmin = 1 << 30;
-      if ((a.mask >> s) & 1)
+      if ((rq.mask >> s) & 1)
         for (int b = 0; b < a.nblocks[s]; ++b)
         {
           if (!sm.np[s][b])
@@ -624,7 +635,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       // 3: blocks rebuilt from the decoded planes (k_decode_planes), a warp per block
       for (int s = 0; s < a.nsb; ++s)
       {
-        if (!((a.mask >> s) & 1) || sm.nkeys[s] == 0)
+        if (!((rq.mask >> s) & 1) || sm.nkeys[s] == 0)
           continue;
         const unsigned long long uo = a.unit_off[(size_t)bi * (size_t)a.nsb + (size_t)s];
         if (uo == ~0ull)
@@ -779,7 +790,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       // that plane of block t - j, taking the block's significance count from lane j - 1 of
       // step t - 1. Block t - (nkeys - 1) is complete after step t and is rebuilt at once.
       const int s = warp;
-      if (s < a.nsb && ((a.mask >> s) & 1) && sm.nkeys[s] > 0)
+      if (s < a.nsb && ((rq.mask >> s) & 1) && sm.nkeys[s] > 0)
       {
         const int nb = a.nblocks[s];
         const int nkeys = sm.nkeys[s], kmax = sm.kmax[s];
@@ -862,7 +873,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       // 3b: subbands with more than 32 channels: CTA-wide wavefront, one subband at a time
       for (int s = 0; s < a.nsb; ++s)
       {
-        if (!((a.mask >> s) & 1))
+        if (!((rq.mask >> s) & 1))
           continue;
         int from[3], dims[3], strd[3];
         subband_grid(a.is2d, s, from, dims, strd);
@@ -994,7 +1005,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       // 5: output (Core/idx2Decode.cpp:431-442 CopyGridGrid): where this row goes, decided
       // before the row is loaded (fewer live registers around the lift)
       long long obase = -1;
-      if (a.is_output && active)
+      if (rq.is_output && active)
       {
         const int ry = y - br.src_from[1], rz = z - br.src_from[2];
         if (ry >= 0 && rz >= 0 && ry % br.src_strd[1] == 0 && rz % br.src_strd[2] == 0 &&
@@ -1002,10 +1013,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         {
           const long long oy = br.dst_from[1] + (long long)(ry / br.src_strd[1]) * br.dst_strd[1];
           const long long oz = br.dst_from[2] + (long long)(rz / br.src_strd[2]) * br.dst_strd[2];
-          obase = (oz * a.out_dims[1] + oy) * a.out_dims[0] + br.dst_from[0];
+          obase = (oz * rq.out_dims[1] + oy) * rq.out_dims[0] + br.dst_from[0];
         }
       }
-      if (active && (!a.is_output || obase >= 0))
+      if (active && (!rq.is_output || obase >= 0))
       {
         // even and odd x samples of the row: two dense runs
         const int hy = y & 1, hz = z & 1, dy = 17 - hy;
@@ -1016,17 +1027,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         for (int x = 0; x < 33; ++x)
           v[x] = (x & 1) ? r1[x >> 1] : r0[x >> 1];
         ilift33(v);
-        double* dst = a.is_output ? sm.u.out.v[warp][lane] : nullptr;
+        double* dst = rq.is_output ? sm.u.out.v[warp][lane] : nullptr;
 #pragma unroll
         for (int x = 0; x < 33; ++x)
         {
-          if (a.is_output)
+          if (rq.is_output)
             dst[x] = v[x];
           else
             ((x & 1) ? r1 : r0)[x >> 1] = v[x];
         }
       }
-      if (a.is_output)
+      if (rq.is_output)
       {
         // the warp's rows, lanes along x
         sm.u.out.base[warp][lane] = obase;
@@ -1040,9 +1051,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
           const long long di = ob + (long long)lane * br.dst_strd[0];
           const double val = sm.u.out.v[warp][r][br.src_from[0] + lane * br.src_strd[0]];
           if (a.out_f32)
-            ((float*)a.out)[di] = __double2float_rn(val);
+            ((float*)rq.out)[di] = __double2float_rn(val);
           else
-            ((double*)a.out)[di] = val;
+            ((double*)rq.out)[di] = val;
         }
         __syncwarp();
       }

@@ -659,6 +659,8 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
               db.dst_strd[d] = dst.strd[d];
             }
           }
+          db.req = 0;
+          db.store = lv.is_output ? -1 : (int)lv.bricks.size();
           pos_of[(size_t)l][bi] = (int)lv.bricks.size();
           lv.bricks.push_back(db);
         }
@@ -699,6 +701,24 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
   }
   *rq_out = std::move(rq);
   return NoError;
+}
+
+int dataset_decode_batch(device_ctx* ctx, dataset_handle* h, const params* ps, int n, void* const* outs,
+                         const size_t* out_bytes, bool out_on_device, double* kernel_ms)
+{
+  std::vector<decode_request> rqs((size_t)n);
+  std::vector<const decode_request*> ptrs((size_t)n);
+  std::vector<size_t> need((size_t)n);
+  for (int i = 0; i < n; ++i)
+  {
+    int e = plan_decode(h, ps[i], &rqs[(size_t)i], &need[(size_t)i]);
+    if (e)
+      return e;
+    if (out_bytes[i] < need[(size_t)i])
+      return SizeTooSmall;
+    ptrs[(size_t)i] = &rqs[(size_t)i];
+  }
+  return h->dev.decode_batch(ctx, ptrs, outs, need.data(), out_on_device, kernel_ms);
 }
 
 void dataset_close(dataset_handle* h) { delete h; }

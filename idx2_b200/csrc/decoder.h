@@ -19,6 +19,9 @@ int dataset_open(device_ctx* ctx, const params& p, dataset_handle** out);
 int dataset_output_grid(const dataset_handle* ds, const params& p, grid* g);
 int dataset_decode(device_ctx* ctx, dataset_handle* ds, const params& p, void* out, size_t out_bytes,
                    bool out_on_device, double* kernel_ms);
+// Several requests at once (one launch per level over all of their bricks).
+int dataset_decode_batch(device_ctx* ctx, dataset_handle* ds, const params* ps, int n, void* const* outs,
+                         const size_t* out_bytes, bool out_on_device, double* kernel_ms);
 void dataset_close(dataset_handle* ds);
 // Allocation-free variant of dataset_decode (device output only; see decode.cu).
 int dataset_decode_noalloc(device_ctx* ctx, dataset_handle* ds, const params& p, void* d_out,

@@ -8,7 +8,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import Idx2Error, Params, ctx, lib
+from ._lib import Idx2Error, Params, _CParams, ctx, lib
 
 
 class Dataset:
@@ -73,6 +73,47 @@ class Dataset:
             raise Idx2Error(rc, "idx2g_decode")
         self.last_kernel_ms = kms.value
         return out
+
+    def decode_batch(self, requests, device_out: bool = True):
+        """Decode several requests in one call (idx2g_decode_batch): requests is a list of dicts
+        with optional keys first, last, downsampling, tolerance (as in decode). Returns one
+        array per request: CUDA torch tensors when device_out, numpy arrays otherwise."""
+        n = len(requests)
+        if n == 0:
+            return []
+        cps = (_CParams * n)()
+        outs, ptrs, sizes = [], [], []
+        dt = self.dtype
+        import torch
+        for i, r in enumerate(requests):
+            first, last = r.get("first"), r.get("last")
+            ds = r.get("downsampling", (0, 0, 0))
+            p = self._req(first, last, ds, r.get("tolerance", 0.0))
+            cps[i] = p.to_c()
+            _, dims, _ = self.output_grid(first, last, ds)
+            shape = (dims[2], dims[1], dims[0])
+            if device_out:
+                o = torch.empty(shape, dtype=torch.float32 if dt == np.float32 else torch.float64,
+                                device=torch.device("cuda", self.device))
+                ptrs.append(o.data_ptr())
+                sizes.append(o.numel() * o.element_size())
+            else:
+                o = np.empty(shape, dtype=dt)
+                ptrs.append(o.ctypes.data)
+                sizes.append(o.nbytes)
+            outs.append(o)
+        arr = (ctypes.c_void_p * n)(*[ctypes.c_void_p(q) for q in ptrs])
+        szs = (ctypes.c_size_t * n)(*sizes)
+        kms = ctypes.c_double(0)
+        L = lib()
+        L.idx2g_decode_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_CParams), ctypes.c_int,
+                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_double)]
+        rc = L.idx2g_decode_batch(self._ctx.h, self.h, cps, n, arr, szs, int(device_out), ctypes.byref(kms))
+        if rc:
+            raise Idx2Error(rc, "idx2g_decode_batch")
+        self.last_kernel_ms = kms.value
+        return outs
 
     @property
     def dtype(self):

@@ -119,6 +119,16 @@ IDX2G_API int idx2g_decode(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params
                            size_t out_bytes, int out_on_device, double* kernel_ms);
 IDX2G_API int idx2g_dataset_close(idx2g_dataset* ds);
 
+/* Several decode requests on one dataset at once (each with its own extent, downsampling and
+   tolerance, as in idx2g_decode): per level one launch over the bricks of every request that
+   decodes that level, so many small region-of-interest requests fill the GPU together. The
+   reference decodes one request per call (Core/idx2Decode.cpp:326 Decode). outs[i] receives
+   request i's grid (out_bytes[i] at least its size); all outs are device pointers when
+   out_on_device is 1, host pointers otherwise. */
+IDX2G_API int idx2g_decode_batch(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p, int n,
+                                 void* const* outs, const size_t* out_bytes, int out_on_device,
+                                 double* kernel_ms);
+
 /* Allocation-free decode. No counterpart in the reference: it exists for callers that cannot
    allocate device memory when they decode -- applications whose device memory belongs to
    another allocator (a framework's caching allocator, a pool sized to the whole GPU) and
