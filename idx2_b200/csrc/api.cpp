@@ -497,6 +497,54 @@ IDX2G_API int idx2g_decode_batch(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_pa
                               kernel_ms);
 }
 
+IDX2G_API long long idx2g_coeff_count(const idx2g_params* in)
+{
+  if (!in)
+    return -1;
+  params p;
+  to_params(in, &p);
+  dataset_format f;
+  if (finalize(&f, &p))
+    return -1;
+  return synth_coeff_count(f);
+}
+
+IDX2G_API int idx2g_coeffs(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* in, void* d_coeffs, size_t bytes,
+                           double* kernel_ms)
+{
+  if (!c || !ds || !in || !d_coeffs)
+    return InvalidArgument;
+  params p;
+  to_params(in, &p);
+  return dataset_coeffs(&c->d, (dataset_handle*)ds, p, d_coeffs, bytes, kernel_ms);
+}
+
+static int synth_call(idx2g_ctx* c, const idx2g_params* in, int nbatch, const void* src, void* dst, bool adjoint,
+                      double* kernel_ms)
+{
+  if (!c || !in || !src || !dst || nbatch < 1)
+    return InvalidArgument;
+  params p;
+  to_params(in, &p);
+  dataset_format f;
+  int e = finalize(&f, &p);
+  if (e)
+    return e;
+  return synth(&c->d, f, nbatch, src, dst, adjoint, kernel_ms);
+}
+
+IDX2G_API int idx2g_synth(idx2g_ctx* c, const idx2g_params* in, int nbatch, const void* d_coeffs, void* d_grid,
+                          double* kernel_ms)
+{
+  return synth_call(c, in, nbatch, d_coeffs, d_grid, false, kernel_ms);
+}
+
+IDX2G_API int idx2g_synth_adjoint(idx2g_ctx* c, const idx2g_params* in, int nbatch, const void* d_grid_grad,
+                                  void* d_coeff_grad, double* kernel_ms)
+{
+  return synth_call(c, in, nbatch, d_grid_grad, d_coeff_grad, true, kernel_ms);
+}
+
 // Allocation-free decode (include/idx2g.h): for callers that cannot allocate device memory at
 // decode time; all temporaries are in the fixed scratch array of decode.cu.
 IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* in, void* d_out,

@@ -104,7 +104,8 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
 }
 
 int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_request*>& rqs,
-                                void* const* outs, const size_t* out_bytes, bool out_on_device, double* kernel_ms)
+                                void* const* outs, const size_t* out_bytes, bool out_on_device, double* kernel_ms,
+                                void* coeff_out)
 {
   const size_t n = rqs.size();
   if (n == 0)
@@ -137,6 +138,18 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
   for (size_t i = 0; i < n; ++i)
     if (out_bytes[i])
       cudaMemsetAsync(d_out[i], 0, out_bytes[i], st);
+  // coefficient mode: brick base of every level in the tensor (finest level first)
+  std::vector<long long> coeff_base((size_t)L + 1, 0);
+  if (coeff_out)
+  {
+    for (int l = 0; l < L; ++l)
+    {
+      const size_t k = (size_t)(L - 1 - l);
+      coeff_base[(size_t)l + 1] =
+        coeff_base[(size_t)l] + (k < r0.levels.size() ? (long long)r0.levels[k].bricks.size() : 0);
+    }
+    cudaMemsetAsync(coeff_out, 0, (size_t)coeff_base[(size_t)L] * (size_t)NB * (r0.f32 ? 4 : 8), st);
+  }
   int* d_err = (int*)ctx->ws("dec.err", 16);  // [0] brick kernel, [1] plane kernel
   uint64_t* d_geom = (uint64_t*)ctx->ws("dec.geom", sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
   if (!d_err || !d_geom)
@@ -180,13 +193,17 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       t.out_dims[2] = rq.out_dims.z;
       const int ti = (int)targets.size();
       targets.push_back(t);
-      cur_base[i] = lv.is_output ? -1 : nstore;
+      cur_base[i] = lv.is_output || coeff_out ? -1 : nstore;
+      int li_in_level = 0;
       for (const decode_brick& b : lv.bricks)
       {
         decode_brick db = b;
         db.req = ti;
         db.parent = b.parent >= 0 && prev_base[i] >= 0 ? prev_base[i] + b.parent : -1;
-        db.store = lv.is_output ? -1 : nstore++;
+        if (coeff_out)
+          db.store = (int)(coeff_base[(size_t)l] + li_in_level++);
+        else
+          db.store = lv.is_output ? -1 : nstore++;
         hb.push_back(db);
       }
     }
@@ -235,6 +252,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
     a.slots = d_slots;
     a.reqs = d_reqs;
     a.error = d_err;
+    a.coeff_out = coeff_out;
 
     // bit planes of every (brick, subband) of the level: one warp each, tables allocated
     // with a cursor in a grow-only workspace (relaunched larger if it overflows)

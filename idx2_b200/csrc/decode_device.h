@@ -68,8 +68,10 @@ public:
              double* kernel_ms);
   // Several requests on this dataset at once: per level one launch (of each kernel) over the
   // bricks of every request that decodes the level. outs[i] receives request i's grid.
+  // coeff_out (coefficient mode, one full-field request): the dequantised coefficients of every
+  // brick (levels finest first, bricks row-major, 33^3 each) in place of the grid.
   int decode_batch(device_ctx* ctx, const std::vector<const decode_request*>& rqs, void* const* outs,
-                   const size_t* out_bytes, bool out_on_device, double* kernel_ms);
+                   const size_t* out_bytes, bool out_on_device, double* kernel_ms, void* coeff_out = nullptr);
   // Allocation-free decode into a device buffer: every temporary lives in a fixed static
   // device array of decode.cu (limits and semantics there and in include/idx2g.h).
   int decode_noalloc(device_ctx* ctx, const decode_request& rq, void* d_out, size_t out_bytes,

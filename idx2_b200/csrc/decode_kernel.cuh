@@ -53,6 +53,10 @@ struct dec_args
   double* slots;                      // per-CTA slots (output bricks)
   const decode_target* reqs;          // request table of the launch
   int* error;
+  // coefficient mode: the dequantised zfp-domain coefficients of every brick, at their sample
+  // positions in a 33^3 (33^2) brick of the dataset's dtype (brick `store` of the tensor), in
+  // place of the decoded grid
+  void* coeff_out;
   // decoded bit planes from k_decode_planes (null: the kernel runs the wavefront itself)
   const unsigned long long* planes;
   const unsigned long long* unit_off;  // [brick][subband] byte offset of the unit's table, ~0: none
@@ -561,10 +565,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
     double* F = rq.is_output ? a.slots + (size_t)blockIdx.x * (size_t)NB
                              : a.bricks_out + (size_t)br.store * (size_t)NB;
     // 1: zero + parent low band (Core/idx2Decode.cpp:285-293)
-    for (int i = tid; i < NB; i += kThreads)
-      F[i] = 0.0;
+    if (!a.coeff_out)
+      for (int i = tid; i < NB; i += kThreads)
+        F[i] = 0.0;
     __syncthreads();
-    if (br.parent >= 0 && a.parents && (rq.mask & 1))
+    if (!a.coeff_out && br.parent >= 0 && a.parents && (rq.mask & 1))
     {
       const double* P = a.parents + (size_t)br.parent * (size_t)NB;
       const int nz = a.is2d ? 1 : 16;
@@ -727,6 +732,41 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
           if (lane + 32 < nvB)
             qB[qpad(permj(ndB, lane + 32))] = (long long)((uB1 ^ dev::kNegaMask) - dev::kNegaMask);
           __syncwarp();
+          if (a.coeff_out)
+          {
+            // coefficient mode: q * 2^(EMax - Prec + 1) at the samples' positions, no inverse zfp
+            auto put = [&](int b, long long* q, int nd, int nv) {
+              int d3[3], bd[3];
+              unpack_geom(geom[b], d3, bd);
+              const int kk = 63 - nd - 1 - sm.emax[s][b];
+              const double scale = kk > 1023 ? 0.0 : dev::pow2(-kk);
+              const size_t cb = (size_t)br.store * (size_t)NB;
+              for (int j = lane; j < nv; j += 32)
+              {
+                const int x = bd[0] > 1 ? (j & 3) : 0;
+                const int r = bd[0] > 1 ? j >> 2 : j;
+                const int y = bd[1] > 1 ? (r & 3) : 0;
+                const int z = bd[1] > 1 ? r >> 2 : r;
+                const int px = hx + 2 * (d3[0] + x), py = hy + 2 * (d3[1] + y), pz = hz + 2 * (d3[2] + z);
+                const size_t at = cb + (size_t)((pz * 33 + py) * 33 + px);
+                const double v = __dmul_rn(scale, __ll2double_rn(q[qpad(j)]));
+                if (a.out_f32)
+                  ((float*)a.coeff_out)[at] = (float)v;
+                else
+                  ((double*)a.coeff_out)[at] = v;
+              }
+            };
+            if (actA)
+              put(bA, qA, ndA, nvA);
+            if (actB)
+              put(bB, qB, ndB, nvB);
+            __syncwarp();
+            cA0 = nA0;
+            cA1 = nA1;
+            cB0 = nB0;
+            cB1 = nB1;
+            continue;
+          }
           // inverse zfp (Core/Zfp.h:287): block A on lanes 0-15, block B on lanes 16-31
           {
             const int h = lane >> 4, l = lane & 15;
@@ -952,6 +992,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
     __syncthreads();
     DEC_PHASE(2)
 
+    if (a.coeff_out)
+      continue;
     // 4: de-normalise + inverse CDF5/3 Z, Y, X (Core/Wavelet.cpp:144-203); the
     // de-normalisation is applied as the Z lines are loaded, the output crop and cast as the
     // X lines are stored.

@@ -721,6 +721,29 @@ int dataset_decode_batch(device_ctx* ctx, dataset_handle* h, const params* ps, i
   return h->dev.decode_batch(ctx, ptrs, outs, need.data(), out_on_device, kernel_ms);
 }
 
+int dataset_coeffs(device_ctx* ctx, dataset_handle* h, const params& p, void* d_coeffs, size_t bytes,
+                   double* kernel_ms)
+{
+  params q = p;
+  q.has_extent = false;
+  q.downsampling = v3(0);
+  decode_request rq;
+  size_t need = 0;
+  int e = plan_decode(h, q, &rq, &need);
+  if (e)
+    return e;
+  const size_t nb = (size_t)(h->f.is2d() ? 33 * 33 : 33 * 33 * 33);
+  size_t count = 0;
+  for (const decode_level& lv : rq.levels)
+    count += lv.bricks.size() * nb;
+  if (bytes < count * (h->f.type == dtype::float32 ? 4 : 8))
+    return SizeTooSmall;
+  std::vector<const decode_request*> rqs(1, &rq);
+  void* none = nullptr;
+  size_t zero = 0;
+  return h->dev.decode_batch(ctx, rqs, &none, &zero, true, kernel_ms, d_coeffs);
+}
+
 void dataset_close(dataset_handle* h) { delete h; }
 
 int dataset_decode_noalloc(device_ctx* ctx, dataset_handle* h, const params& p, void* d_out, size_t out_bytes,

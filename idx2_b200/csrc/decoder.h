@@ -22,7 +22,17 @@ int dataset_decode(device_ctx* ctx, dataset_handle* ds, const params& p, void* o
 // Several requests at once (one launch per level over all of their bricks).
 int dataset_decode_batch(device_ctx* ctx, dataset_handle* ds, const params* ps, int n, void* const* outs,
                          const size_t* out_bytes, bool out_on_device, double* kernel_ms);
+// The dequantised coefficients of the whole dataset (decode tolerance of p) into d_coeffs.
+int dataset_coeffs(device_ctx* ctx, dataset_handle* ds, const params& p, void* d_coeffs, size_t bytes,
+                   double* kernel_ms);
 void dataset_close(dataset_handle* ds);
+
+// Differentiable decode (adjoint.cu): elements of one field's coefficient tensor, and the
+// real-valued decode operator (adjoint = false: coefficients -> grid) or its adjoint (grid
+// gradient -> coefficient gradient) on nbatch fields of format f.
+long long synth_coeff_count(const dataset_format& f);
+int synth(device_ctx* ctx, const dataset_format& f, int nbatch, const void* d_in, void* d_out, bool adjoint,
+          double* kernel_ms);
 // Allocation-free variant of dataset_decode (device output only; see decode.cu).
 int dataset_decode_noalloc(device_ctx* ctx, dataset_handle* ds, const params& p, void* d_out,
                            size_t out_bytes, double* kernel_ms);

@@ -859,36 +859,6 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
   ENC_PHASE_FLUSH
 }
 
-// Host-side weights of one level (Core/Wavelet.cpp:111-137, Core/Wavelet.h:19).
-void level_weights(const dataset_format& f, int level, double w[8], int* mask)
-{
-  double scal[16], wave[16];
-  double n1 = 3, n2 = 23;
-  for (int i = 0; i < 16; ++i)
-  {
-    scal[i] = sqrt(n1 / (1 << (i + 1)));
-    n1 = n1 * 4 - 1;
-    wave[i] = sqrt(n2 / (1 << (i + 5)));
-    n2 = n2 * 4 - 33;
-  }
-  const bool coarsest = level + 1 == f.nlevels;
-  *mask = 0;
-  for (int s = 0; s < f.nsubbands(); ++s)
-  {
-    const subband& sb = f.subbands[(size_t)s];
-    double wx = f.brick_dims_ext.x == 1 ? 1
-                : (sb.low_high.x == 0 ? scal[level + sb.level_rev.x - 1] : wave[level + sb.level_rev.x]);
-    double wy = f.brick_dims_ext.y == 1 ? 1
-                : (sb.low_high.y == 0 ? scal[level + sb.level_rev.y - 1] : wave[level + sb.level_rev.y]);
-    double wz = f.brick_dims_ext.z == 1 ? 1
-                : (sb.low_high.z == 0 ? scal[level + sb.level_rev.z - 1] : wave[level + sb.level_rev.z]);
-    w[s] = wx * wy * wz;
-    if (s == 0 && !coarsest)
-      continue;
-    *mask |= 1 << s;
-  }
-}
-
 } // namespace
 
 // ---------------------------------------------------------------------------

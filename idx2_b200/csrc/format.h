@@ -242,6 +242,10 @@ struct traverse_item
 template <typename F>
 void traverse(u64 order, v3 from3, v3 dims3, const extent& ext, const extent& ext2, F&& body);
 
+// Subband normalisation weights of one level (Core/Wavelet.cpp:111-137): w[s] for the nsubbands
+// subbands; mask has bit s set where the weight applies (all but subband 0 below the coarsest).
+void level_weights(const dataset_format& f, int level, double w[8], int* mask);
+
 } // namespace idx2g
 
 #include "format_traverse.h"

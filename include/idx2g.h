@@ -165,6 +165,29 @@ IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2
 IDX2G_API int idx2g_encode_batch(idx2g_ctx* ctx, const idx2g_params* params, const void* const* fields,
                                  int n, int fields_on_device, int flags, idx2g_encode_info* infos);
 
+/* Differentiable decode. The reference has no counterpart: its decode is integer end to end
+   (Core/idx2Decode.cpp:141-320). Here the decode is also available as a real-valued linear
+   operator D from the dequantised zfp-domain coefficients to the grid: the reference's decode
+   with the integer inverse zfp (Core/Zfp.h:181) replaced by its real form (exact halvings in
+   place of the shifts), then de-normalisation, the inverse CDF5/3 and the parent hand-off per
+   level. D and its adjoint let gradients of a loss on the decoded grid reach the coefficients.
+
+   Coefficient tensor of one field (format given by p: dims, dtype, brick dims, levels): levels
+   0 (finest) to L-1; on each level the bricks in row-major order of their coordinates (x
+   fastest); each brick 33^3 values (33^2 for 2D) indexed (z*33 + y)*33 + x, every coefficient
+   at the position of the sample its block transforms; idx2g_coeff_count gives its length.
+   Batched calls take nbatch tensors (and grids) back to back. Values are of p's dtype. */
+IDX2G_API long long idx2g_coeff_count(const idx2g_params* p);
+/* The dataset's dequantised coefficients (at p's decode tolerance) into d_coeffs. */
+IDX2G_API int idx2g_coeffs(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p, void* d_coeffs,
+                           size_t bytes, double* kernel_ms);
+/* grid = D(coefficients) for nbatch fields (device pointers). */
+IDX2G_API int idx2g_synth(idx2g_ctx* ctx, const idx2g_params* p, int nbatch, const void* d_coeffs,
+                          void* d_grid, double* kernel_ms);
+/* coefficient gradient = D^T(grid gradient) for nbatch fields (device pointers). */
+IDX2G_API int idx2g_synth_adjoint(idx2g_ctx* ctx, const idx2g_params* p, int nbatch,
+                                  const void* d_grid_grad, void* d_coeff_grad, double* kernel_ms);
+
 /* Number of kernels this library has launched on the context so far (a diagnostic for
    benchmarks; no counterpart in the reference). */
 IDX2G_API long long idx2g_ctx_launches(const idx2g_ctx* ctx);
