@@ -476,6 +476,168 @@ def serve_leg(args):
         shutil.rmtree(tmp, ignore_errors=True)
 
 
+def _adjoint_batch(dev, nfields, side, dtype, tmp, seed):
+    """Encode nfields seeded k^-5/3 fields of side^3 (2 levels, tolerance 1e-4) and return the
+    stacked dequantised coefficients (decoded at tolerance 1e-4), the first field's bit-exact
+    decode and the compressed bytes."""
+    import torch
+    import idx2_b200
+    from idx2_b200.diff import Format, coefficients
+    from idx2_b200.synthetic import grf_field_torch
+    fmt = Format((side, side, side), "float32" if dtype == torch.float32 else "float64", 2)
+    cs, first_decode, comp = [], None, 0
+    for i in range(nfields):
+        f = grf_field_torch(side, side, side, seed=seed + i, scale="unit", device=dev).to(dtype)
+        d = os.path.join(tmp, f"a{i}")
+        info = idx2_b200.encode(f, out_dir=d, name="adj", field_name="f", num_levels=2, tolerance=1e-4)
+        comp += int(info.file_bytes)
+        del f
+        ds = idx2_b200.Dataset(os.path.join(d, "adj", "f.idx2"))
+        cs.append(coefficients(ds, fmt, 1e-4))
+        if i == 0:
+            first_decode = torch.from_numpy(ds.decode(tolerance=1e-4)).to(dev)
+        ds.close()
+        shutil.rmtree(d, ignore_errors=True)
+    return fmt, torch.stack(cs), first_decode, comp
+
+
+def _synth_bytes(fmt, nbatch, elem):
+    """Algorithmic bytes of one synth (or adjoint) pass over a batch: the coefficient tensor and
+    the grid once each, plus the kept bricks of the coarser levels written once and read once."""
+    from idx2_b200.diff import coeff_count
+    d = fmt.dims
+    grid = d[0] * d[1] * d[2]
+    coeffs = coeff_count(fmt)
+    nb0 = 33 ** 3 * (-(-d[0] // 32)) * (-(-d[1] // 32)) * (-(-d[2] // 32))
+    kept = coeffs - nb0  # coarser levels' bricks, one value per coefficient position
+    return nbatch * elem * (grid + coeffs + 2 * kept)
+
+
+def _adjoint_time(fmt, c, target, steps, warmup):
+    """Time forward (decode_diff) + MSE + backward over the batch: step ms from CUDA events on
+    torch's stream (synchronised on both sides), kernel ms from the library's events."""
+    import torch
+    from idx2_b200 import diff
+    cg = c.detach().clone().requires_grad_(True)
+
+    def step():
+        x = diff.decode_diff(cg, fmt)
+        loss = torch.mean((x - target) ** 2)
+        loss.backward()
+        return diff.last_kernel_ms["synth"], diff.last_kernel_ms["adjoint"]
+
+    for _ in range(warmup):
+        step()
+        cg.grad = None
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fw, bw = [], []
+    e0.record()
+    for _ in range(steps):
+        a, b = step()
+        fw.append(a)
+        bw.append(b)
+        cg.grad = None
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps, statistics.median(fw), statistics.median(bw)
+
+
+def adjoint_leg(args):
+    """Differentiable decode: a batch of float32 k^-5/3 fields (2 levels, decoded at downsampling
+    0 and tolerance 1e-4) through the torch.autograd.Function, loss = MSE to a second seeded
+    field set; a float64 batch at a smaller side. Checks: the float32 gradient against the
+    float64 adjoint of the same residual, the dot-product identity, FP64 central differences
+    (step 1e-3 on 200 random coefficients), D against the bit-exact decode. Prints one JSON line."""
+    import torch
+    from idx2_b200 import diff
+    from idx2_b200.synthetic import grf_field_torch
+    dev = torch.device("cuda", 0)
+    nf, side, side64 = args.adjoint_fields, args.adjoint_side, args.adjoint_f64_side
+    tmp = tempfile.mkdtemp(prefix="idx2adj_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    try:
+        t0 = time.perf_counter()
+        fmt, c, dec0, comp = _adjoint_batch(dev, nf, side, torch.float32, tmp, seed=300)
+        target = torch.stack([grf_field_torch(side, side, side, seed=900 + i, scale="unit", device=dev)
+                              for i in range(nf)])
+        setup_s = time.perf_counter() - t0
+        step_ms, fw_ms, bw_ms = _adjoint_time(fmt, c, target, args.steps, args.warmup)
+        nbytes = _synth_bytes(fmt, nf, 4)
+        grid_bytes = nf * side ** 3 * 4
+        # checks on the float32 batch
+        x = diff.synth(c, fmt)
+        d_rel = float((x[0] - dec0).abs().max() / dec0.abs().max())
+        r = 2.0 * (x - target) / x.numel()
+        g32 = diff.synth_adjoint(r, fmt)
+        fmt64 = diff.Format(fmt.dims, "float64", 2)
+        x64 = diff.synth(c.double(), fmt64)
+        g64 = diff.synth_adjoint(2.0 * (x64 - target.double()) / x64.numel(), fmt64)
+        g_rel = float((g32.double() - g64).abs().max() / g64.abs().max())
+        del x64, g64, r, x
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(5)
+        y = torch.randn(target.shape, generator=gen, device=dev, dtype=torch.float64)
+        cd = torch.randn(c.shape, generator=gen, device=dev, dtype=torch.float64)
+        lhs = float(torch.sum(diff.synth(cd, fmt64) * y))
+        rhs = float(torch.sum(cd * diff.synth_adjoint(y, fmt64)))
+        dot64 = abs(lhs - rhs) / abs(lhs)
+        lhs = float(torch.sum(diff.synth(cd.float(), fmt).double() * y))
+        rhs = float(torch.sum(cd * diff.synth_adjoint(y.float(), fmt).double()))
+        dot32 = abs(lhs - rhs) / abs(lhs)
+        del y, cd, target, c
+        torch.cuda.empty_cache()
+        # float64 batch at side64
+        fmt_d, c_d, dec0_d, comp_d = _adjoint_batch(dev, nf, side64, torch.float64, tmp, seed=500)
+        target_d = torch.stack([grf_field_torch(side64, side64, side64, seed=1900 + i, scale="unit", device=dev)
+                                for i in range(nf)]).double()
+        step_ms_d, fw_ms_d, bw_ms_d = _adjoint_time(fmt_d, c_d, target_d, args.steps, args.warmup)
+        nbytes_d = _synth_bytes(fmt_d, nf, 8)
+        x = diff.synth(c_d, fmt_d)
+        d_rel64 = float((x[0] - dec0_d).abs().max() / dec0_d.abs().max())
+        n_all = x.numel()
+        grad = diff.synth_adjoint(2.0 * (x - target_d) / n_all, fmt_d)[0]
+        # FP64 central differences on field 0 (only its samples depend on its coefficients)
+        c0 = c_d[0].clone()
+        t0f = target_d[0]
+        rng = np.random.default_rng(8)
+        nz = np.nonzero(grad.abs().cpu().numpy() > 0)[0]
+        idx = [int(i) for i in rng.permutation(nz)[:200]]
+        h = 1e-3
+        fd_err = 0.0
+        for i in idx:
+            old = float(c0[i])
+            c0[i] = old + h
+            xp = diff.synth(c0, fmt_d)
+            c0[i] = old - h
+            xm = diff.synth(c0, fmt_d)
+            c0[i] = old
+            fd = float(torch.sum((xp - t0f) ** 2 - (xm - t0f) ** 2)) / n_all / (2 * h)
+            fd_err = max(fd_err, abs(fd - float(grad[i])) / max(abs(fd), 1e-300))
+        line = {"metric": "differentiable decode step ms (forward + MSE + backward)", "impl": "ours",
+                "unit": "ms", "higher_is_better": False, "steps": args.steps, "warmup": args.warmup,
+                "data": "synthetic", "dtype": "f32 (f64 variant)",
+                "config": {"workload": f"differentiable decode: {nf} float32 k^-5/3 fields of {side}^3, 2 levels, "
+                                       f"coefficients decoded at downsampling 0 and tolerance 1e-4, loss = MSE to "
+                                       f"{nf} second seeded fields; float64 variant {nf} fields of {side64}^3",
+                           "compressed_bytes": comp, "setup_s": setup_s,
+                           "l2": "inputs larger than L2 (coefficients and grid)"},
+                "float32": {"step_ms": step_ms, "forward_kernel_ms": fw_ms, "backward_kernel_ms": bw_ms,
+                            "grid_gbs_per_step": grid_bytes / step_ms / 1e6,
+                            "forward_gbs": nbytes / fw_ms / 1e6, "backward_gbs": nbytes / bw_ms / 1e6,
+                            "algorithmic_bytes_per_pass": nbytes},
+                "float64": {"step_ms": step_ms_d, "forward_kernel_ms": fw_ms_d, "backward_kernel_ms": bw_ms_d,
+                            "forward_gbs": nbytes_d / fw_ms_d / 1e6, "backward_gbs": nbytes_d / bw_ms_d / 1e6,
+                            "algorithmic_bytes_per_pass": nbytes_d},
+                "checks": {"grad_f32_vs_f64_rel": g_rel, "grad_f32_target": 1e-5,
+                           "fd_f64_max_rel": fd_err, "fd_points": len(idx), "fd_step": h,
+                           "dot_identity_rel_f64": dot64, "dot_identity_rel_f32": dot32,
+                           "synth_vs_decode_rel_f32": d_rel, "synth_vs_decode_rel_f64": d_rel64},
+                "gpu_launches_per_step": 4}
+        print(json.dumps(line))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -487,6 +649,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline leg (profiling runs)")
     ap.add_argument("--no-batch", action="store_true", help="skip the uneven-field batched-encode leg")
     ap.add_argument("--serve", action="store_true", help="run the decode-serving benchmark instead")
+    ap.add_argument("--adjoint", action="store_true", help="run the differentiable-decode benchmark instead")
+    ap.add_argument("--adjoint-fields", type=int, default=32, help="fields per batch (differentiable decode)")
+    ap.add_argument("--adjoint-side", type=int, default=256, help="float32 field side (differentiable decode)")
+    ap.add_argument("--adjoint-f64-side", type=int, default=128, help="float64 field side (differentiable decode)")
     ap.add_argument("--serve-dims", default="2048x2048x1024", help="serving field dims (x, y, z)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrival rate (per second)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests per mode")
@@ -497,6 +663,10 @@ def main():
     if args.serve:
         if rank == 0:
             serve_leg(args)
+        return
+    if args.adjoint:
+        if rank == 0:
+            adjoint_leg(args)
         return
     if args.impl == "reference":
         reference_arm(args, rank, world)

@@ -204,6 +204,16 @@ def check_params(p: Params) -> int:
     return int(lib().idx2g_check_params(ctypes.byref(cp)))
 
 
+def torch_ready(device) -> None:
+    """Wait for torch's current stream on a CUDA device. The library runs on its own
+    non-blocking stream, so a tensor that torch has just written (or memory torch's allocator has
+    just handed back) must be complete before its pointer crosses the C ABI; the library
+    synchronises its own stream before it returns."""
+    import torch
+    if torch.cuda.is_available():
+        torch.cuda.current_stream(device).synchronize()
+
+
 def _field_ptr(field):
     """(pointer, on_device, dtype-name, dims(x,y,z), keepalive) of a numpy array or torch tensor
     shaped (nz, ny, nx) with x fastest."""
@@ -253,6 +263,8 @@ def encode(field, out_dir: str = ".", name: str = "field", field_name: str = "da
     cp = p.to_c()
     info = EncodeInfo()
     c = ctx(device)
+    if on_dev:
+        torch_ready(keep.device)
     rc = lib().idx2g_encode(c.h, ctypes.byref(cp), ctypes.c_void_p(ptr), int(on_dev), ctypes.byref(info))
     del keep
     if rc:
@@ -271,6 +283,7 @@ def encode_device(field, num_levels: int, tolerance: float, brick_dims=None, dev
                tolerance=tolerance)
     cp = p.to_c()
     info = EncodeInfo()
+    torch_ready(keep.device)
     rc = lib().idx2g_encode_device(ctx(device).h, ctypes.byref(cp), ctypes.c_void_p(ptr), ctypes.byref(info))
     del keep
     if rc:
@@ -323,6 +336,8 @@ def encode_batch(fields, out_dir: str = ".", names=None, field_names=None, num_l
     L = lib()
     L.idx2g_encode_batch.argtypes = [ctypes.c_void_p, ctypes.POINTER(_CParams), ctypes.c_void_p, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int, ctypes.POINTER(EncodeInfo)]
+    if on_dev:
+        torch_ready(keeps[0].device)
     rc = L.idx2g_encode_batch(ctx(device).h, cps, arr, n, int(bool(on_dev)), flags, infos)
     del keeps
     if rc:

@@ -8,7 +8,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import Idx2Error, Params, _CParams, ctx, lib
+from ._lib import Idx2Error, Params, _CParams, ctx, lib, torch_ready
 
 
 class Dataset:
@@ -66,6 +66,8 @@ class Dataset:
                 ptr, nbytes = out.ctypes.data, out.nbytes
         except ImportError:
             ptr, nbytes = out.ctypes.data, out.nbytes
+        if on_dev:
+            torch_ready(out.device)
         kms = ctypes.c_double(0)
         rc = lib().idx2g_decode(self._ctx.h, self.h, ctypes.byref(cp), ctypes.c_void_p(ptr),
                                 ctypes.c_size_t(nbytes), on_dev, ctypes.byref(kms))
@@ -109,6 +111,8 @@ class Dataset:
         L.idx2g_decode_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_CParams), ctypes.c_int,
                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_double)]
+        if device_out:
+            torch_ready(torch.device("cuda", self.device))
         rc = L.idx2g_decode_batch(self._ctx.h, self.h, cps, n, arr, szs, int(device_out), ctypes.byref(kms))
         if rc:
             raise Idx2Error(rc, "idx2g_decode_batch")

@@ -20,7 +20,7 @@ from typing import Sequence
 
 import numpy as np
 
-from ._lib import Idx2Error, Params, ctx, lib
+from ._lib import Idx2Error, Params, ctx, lib, torch_ready
 
 
 @dataclass(frozen=True)
@@ -73,6 +73,7 @@ def coefficients(ds, fmt: Format, tolerance: float = 0.0):
     p = Params(input_file=ds.params.input_file, in_dir=ds.params.in_dir, decode_tolerance=float(tolerance))
     cp = p.to_c()
     kms = ctypes.c_double(0)
+    torch_ready(c.device)
     rc = _setup(lib()).idx2g_coeffs(ds._ctx.h, ds.h, ctypes.byref(cp), ctypes.c_void_p(c.data_ptr()),
                                     ctypes.c_size_t(c.numel() * c.element_size()), ctypes.byref(kms))
     if rc:
@@ -80,9 +81,14 @@ def coefficients(ds, fmt: Format, tolerance: float = 0.0):
     return c
 
 
+# Kernel milliseconds of the last synth / adjoint call (CUDA events on the library's stream).
+last_kernel_ms = {"synth": 0.0, "adjoint": 0.0}
+
+
 def _run(fn, fmt: Format, src, nbatch: int, out):
     cp = fmt.params().to_c()
     kms = ctypes.c_double(0)
+    torch_ready(src.device)
     rc = fn(ctx(src.device.index or 0).h, ctypes.byref(cp), nbatch, ctypes.c_void_p(src.data_ptr()),
             ctypes.c_void_p(out.data_ptr()), ctypes.byref(kms))
     if rc:
@@ -99,7 +105,7 @@ def synth(coeffs, fmt: Format):
     if c.shape[-1] != coeff_count(fmt) or c.dtype != _torch_dtype(fmt) or not c.is_cuda:
         raise Idx2Error(101, "synth: coefficient tensor does not match the format")
     out = torch.empty((nb,) + fmt.shape, dtype=c.dtype, device=c.device)
-    _run(_setup(lib()).idx2g_synth, fmt, c, nb, out)
+    last_kernel_ms["synth"] = _run(_setup(lib()).idx2g_synth, fmt, c, nb, out)
     return out if batched else out[0]
 
 
@@ -110,7 +116,9 @@ def synth_adjoint(grad, fmt: Format):
     batched = g.dim() == 4
     nb = g.shape[0] if batched else 1
     out = torch.empty((nb, coeff_count(fmt)), dtype=g.dtype, device=g.device)
-    _run(_setup(lib()).idx2g_synth_adjoint, fmt, g, nb, out)
+    if g.shape[-3:] != fmt.shape or g.dtype != _torch_dtype(fmt) or not g.is_cuda:
+        raise Idx2Error(101, "synth_adjoint: gradient tensor does not match the format")
+    last_kernel_ms["adjoint"] = _run(_setup(lib()).idx2g_synth_adjoint, fmt, g, nb, out)
     return out if batched else out[0]
 
 
