@@ -14,6 +14,7 @@
 #include "codec_device.cuh"
 #include "decode_device.h"
 
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 
@@ -135,243 +136,233 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
   else
     for (size_t i = 0; i < n; ++i)
       d_out[i] = outs[i];
-  for (size_t i = 0; i < n; ++i)
-    if (out_bytes[i])
-      cudaMemsetAsync(d_out[i], 0, out_bytes[i], st);
   // coefficient mode: brick base of every level in the tensor (finest level first)
   std::vector<long long> coeff_base((size_t)L + 1, 0);
   if (coeff_out)
-  {
     for (int l = 0; l < L; ++l)
     {
       const size_t k = (size_t)(L - 1 - l);
       coeff_base[(size_t)l + 1] =
         coeff_base[(size_t)l] + (k < r0.levels.size() ? (long long)r0.levels[k].bricks.size() : 0);
     }
-    cudaMemsetAsync(coeff_out, 0, (size_t)coeff_base[(size_t)L] * (size_t)NB * (r0.f32 ? 4 : 8), st);
-  }
-  int* d_err = (int*)ctx->ws("dec.err", 16);  // [0] brick kernel, [1] plane kernel
+  int* d_err = (int*)ctx->ws("dec.err", 16);  // [0] brick kernel, [1] plane kernels (bit flags)
   uint64_t* d_geom = (uint64_t*)ctx->ws("dec.geom", sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
   if (!d_err || !d_geom)
     return OutOfMemory;
-  cudaMemsetAsync(d_err, 0, 16, st);
   const size_t smem = sizeof(dec_smem);
   cudaFuncSetAttribute(k_decode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaEvent_t e0 = ctx->ev0, e1 = ctx->ev1;
-  float total_ms = 0;
-  double* prev = nullptr;
-  std::vector<int> prev_base(n, -1), cur_base(n, -1);
-  std::vector<decode_brick> hb;
-  std::vector<decode_target> targets;
-  int li = 0;
-  for (int l = L - 1; l >= 0; --l)
+  // The levels run back to back without the host waiting in between: the host prepares a
+  // level's tables while the previous level runs (stream order protects the device tables
+  // that every level reuses), the plane kernels' error flags are read once at the end, and a
+  // plane table that overflowed (rare) makes the whole call run again with a larger one.
+  unsigned long long min_cap = 0;
+  for (int attempt = 0; attempt < 4; ++attempt)
   {
-    const size_t k = (size_t)(L - 1 - l);  // entry of level l in a request's level list
-    hb.clear();
-    targets.clear();
-    const decode_level* lw = nullptr;  // level-wide tables (common to all requests)
-    int nstore = 0;
     for (size_t i = 0; i < n; ++i)
+      if (out_bytes[i])
+        cudaMemsetAsync(d_out[i], 0, out_bytes[i], st);
+    if (coeff_out)
+      cudaMemsetAsync(coeff_out, 0, (size_t)coeff_base[(size_t)L] * (size_t)NB * (r0.f32 ? 4 : 8), st);
+    cudaMemsetAsync(d_err, 0, 16, st);
+    size_t nev = 0;  // levels timed (event pairs of the pool)
+    double* prev = nullptr;
+    std::vector<int> prev_base(n, -1), cur_base(n, -1);
+    std::vector<decode_brick> hb;
+    std::vector<decode_target> targets;
+    int li = 0;
+    for (int l = L - 1; l >= 0; --l)
     {
-      cur_base[i] = -1;
-      const decode_request& rq = *rqs[i];
-      if (k >= rq.levels.size())
-        continue;
-      const decode_level& lv = rq.levels[k];
-      if (lv.bricks.empty())
-        continue;
-      lw = &lv;
-      decode_target t;
-      memset(&t, 0, sizeof t);
-      t.mask = lv.mask;
-      t.is_output = lv.is_output;
-      t.etol = rq.etol;
-      memcpy(t.spacing, lv.spacing, sizeof t.spacing);
-      t.out = d_out[i];
-      t.out_dims[0] = rq.out_dims.x;
-      t.out_dims[1] = rq.out_dims.y;
-      t.out_dims[2] = rq.out_dims.z;
-      const int ti = (int)targets.size();
-      targets.push_back(t);
-      cur_base[i] = lv.is_output || coeff_out ? -1 : nstore;
-      int li_in_level = 0;
-      for (const decode_brick& b : lv.bricks)
+      const size_t k = (size_t)(L - 1 - l);  // entry of level l in a request's level list
+      hb.clear();
+      targets.clear();
+      const decode_level* lw = nullptr;  // level-wide tables (common to all requests)
+      int nstore = 0;
+      for (size_t i = 0; i < n; ++i)
       {
-        decode_brick db = b;
-        db.req = ti;
-        db.parent = b.parent >= 0 && prev_base[i] >= 0 ? prev_base[i] + b.parent : -1;
-        if (coeff_out)
-          db.store = (int)(coeff_base[(size_t)l] + li_in_level++);
-        else
-          db.store = lv.is_output ? -1 : nstore++;
-        hb.push_back(db);
+        cur_base[i] = -1;
+        const decode_request& rq = *rqs[i];
+        if (k >= rq.levels.size())
+          continue;
+        const decode_level& lv = rq.levels[k];
+        if (lv.bricks.empty())
+          continue;
+        lw = &lv;
+        decode_target t;
+        memset(&t, 0, sizeof t);
+        t.mask = lv.mask;
+        t.is_output = lv.is_output;
+        t.etol = rq.etol;
+        memcpy(t.spacing, lv.spacing, sizeof t.spacing);
+        t.out = d_out[i];
+        t.out_dims[0] = rq.out_dims.x;
+        t.out_dims[1] = rq.out_dims.y;
+        t.out_dims[2] = rq.out_dims.z;
+        const int ti = (int)targets.size();
+        targets.push_back(t);
+        cur_base[i] = lv.is_output || coeff_out ? -1 : nstore;
+        int li_in_level = 0;
+        for (const decode_brick& b : lv.bricks)
+        {
+          decode_brick db = b;
+          db.req = ti;
+          db.parent = b.parent >= 0 && prev_base[i] >= 0 ? prev_base[i] + b.parent : -1;
+          if (coeff_out)
+            db.store = (int)(coeff_base[(size_t)l] + li_in_level++);
+          else
+            db.store = lv.is_output ? -1 : nstore++;
+          hb.push_back(db);
+        }
       }
-    }
-    prev_base = cur_base;
-    const int nbr = (int)hb.size();
-    if (nbr == 0)
-    {
-      prev = nullptr;
-      continue;
-    }
-    ++li;
-    decode_brick* d_bricks = (decode_brick*)ctx->ws("dec.bricks", sizeof(decode_brick) * (size_t)nbr);
-    decode_target* d_reqs = (decode_target*)ctx->ws("dec.reqs", sizeof(decode_target) * targets.size());
-    double* d_level = nstore ? (double*)ctx->ws(li % 2 ? "dec.levA" : "dec.levB", (size_t)nstore * (size_t)NB * 8)
-                             : nullptr;
-    int grid = nbr < 2 * ctx->num_sms ? nbr : 2 * ctx->num_sms;
-    double* d_slots = (double*)ctx->ws("dec.slots", (size_t)grid * (size_t)NB * 8);
-    if (!d_bricks || !d_reqs || (nstore && !d_level) || !d_slots)
-      return OutOfMemory;
-    cudaMemcpyAsync(d_bricks, hb.data(), sizeof(decode_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_reqs, targets.data(), sizeof(decode_target) * targets.size(), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_geom, lw->geom, sizeof(uint64_t) * 8 * kMaxBlocksPerSubband, cudaMemcpyHostToDevice, st);
-    dec_args a;
-    memset(&a, 0, sizeof a);
-    a.level = l;
-    a.nlevels = L;
-    a.is2d = r0.is2d;
-    a.nsb = r0.nsb;
-    a.nbricks = nbr;
-    a.end_bp = r0.f32 ? 32 : 64;
-    a.norm_mask = lw->norm_mask;
-    a.out_f32 = r0.f32;
-    memcpy(a.nblocks, lw->nblocks, sizeof a.nblocks);
-    memcpy(a.inv_weight, lw->inv_weight, sizeof a.inv_weight);
-    a.geom = d_geom;
-    a.bricks = d_bricks;
-    a.exps = exps_;
-    a.ckmin = kmin_;
-    a.cn = n_;
-    a.cfirst = first_;
-    a.coff = off_;
-    a.blob = blob_;
-    a.blob_bytes = blob_bytes_;
-    a.parents = prev;
-    a.bricks_out = d_level;
-    a.slots = d_slots;
-    a.reqs = d_reqs;
-    a.error = d_err;
-    a.coeff_out = coeff_out;
+      prev_base = cur_base;
+      const int nbr = (int)hb.size();
+      if (nbr == 0)
+      {
+        prev = nullptr;
+        continue;
+      }
+      ++li;
+      decode_brick* d_bricks = (decode_brick*)ctx->ws("dec.bricks", sizeof(decode_brick) * (size_t)nbr);
+      decode_target* d_reqs = (decode_target*)ctx->ws("dec.reqs", sizeof(decode_target) * targets.size());
+      double* d_level = nstore ? (double*)ctx->ws(li % 2 ? "dec.levA" : "dec.levB", (size_t)nstore * (size_t)NB * 8)
+                               : nullptr;
+      int grid = nbr < 2 * ctx->num_sms ? nbr : 2 * ctx->num_sms;
+      double* d_slots = (double*)ctx->ws("dec.slots", (size_t)grid * (size_t)NB * 8);
+      if (!d_bricks || !d_reqs || (nstore && !d_level) || !d_slots)
+        return OutOfMemory;
+      // the level's tables through pinned staging of its own (copies stay asynchronous; the
+      // call's final synchronisation comes before any reuse)
+      const size_t hb_bytes = sizeof(decode_brick) * (size_t)nbr;
+      const size_t tg_bytes = sizeof(decode_target) * targets.size();
+      const size_t gm_bytes = sizeof(uint64_t) * 8 * kMaxBlocksPerSubband;
+      char pn[32];
+      snprintf(pn, sizeof pn, "dec.hstage%d", l);
+      uint8_t* hs = (uint8_t*)ctx->pinned(pn, hb_bytes + tg_bytes + gm_bytes);
+      if (!hs)
+        return OutOfMemory;
+      memcpy(hs, hb.data(), hb_bytes);
+      memcpy(hs + hb_bytes, targets.data(), tg_bytes);
+      memcpy(hs + hb_bytes + tg_bytes, lw->geom, gm_bytes);
+      cudaMemcpyAsync(d_bricks, hs, hb_bytes, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(d_reqs, hs + hb_bytes, tg_bytes, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(d_geom, hs + hb_bytes + tg_bytes, gm_bytes, cudaMemcpyHostToDevice, st);
+      dec_args a;
+      memset(&a, 0, sizeof a);
+      a.level = l;
+      a.nlevels = L;
+      a.is2d = r0.is2d;
+      a.nsb = r0.nsb;
+      a.nbricks = nbr;
+      a.end_bp = r0.f32 ? 32 : 64;
+      a.norm_mask = lw->norm_mask;
+      a.out_f32 = r0.f32;
+      memcpy(a.nblocks, lw->nblocks, sizeof a.nblocks);
+      memcpy(a.inv_weight, lw->inv_weight, sizeof a.inv_weight);
+      a.geom = d_geom;
+      a.bricks = d_bricks;
+      a.exps = exps_;
+      a.ckmin = kmin_;
+      a.cn = n_;
+      a.cfirst = first_;
+      a.coff = off_;
+      a.blob = blob_;
+      a.blob_bytes = blob_bytes_;
+      a.parents = prev;
+      a.bricks_out = d_level;
+      a.slots = d_slots;
+      a.reqs = d_reqs;
+      a.error = d_err;
+      a.coeff_out = coeff_out;
 
-    // bit planes of every (brick, subband) of the level: one warp each, tables allocated
-    // with a cursor in a grow-only workspace (relaunched larger if it overflows)
-    const size_t nunits = (size_t)nbr * (size_t)r0.nsb;
-    unsigned long long* d_uoff = (unsigned long long*)ctx->ws("dec.unitoff", nunits * 8);
-    unsigned long long* d_pcur = (unsigned long long*)ctx->ws("dec.pcursor", 16);
-    int* d_wide = (int*)ctx->ws("dec.widelist", nunits * 4);
-    if (!d_uoff || !d_pcur || !d_wide)
-      return OutOfMemory;
-    unsigned long long cap = (unsigned long long)nunits * 16384ull + (16ull << 20);
-    if (ctx->ws_size("dec.planes") > cap)
-      cap = ctx->ws_size("dec.planes");
-    dec1_args pa;
-    memset(&pa, 0, sizeof pa);
-    pa.nsb = r0.nsb;
-    pa.nbricks = nbr;
-    pa.end_bp = a.end_bp;
-    pa.reqs = d_reqs;
-    memcpy(pa.nblocks, lw->nblocks, sizeof pa.nblocks);
-    pa.geom = d_geom;
-    pa.bricks = d_bricks;
-    pa.exps = exps_;
-    pa.ckmin = kmin_;
-    pa.cn = n_;
-    pa.cfirst = first_;
-    pa.coff = off_;
-    pa.blob = blob_;
-    pa.blob_bytes = blob_bytes_;
-    pa.cursor = d_pcur;
-    pa.unit_off = d_uoff;
-    pa.error = d_err + 1;
-    pa.wide_count = (int*)(d_pcur + 1);
-    pa.wide_list = d_wide;
-    const int pgrid = (int)((nunits + kPlaneWarps - 1) / kPlaneWarps);
-    float level_ms = 0;
-    for (int attempt = 0; attempt < 3; ++attempt)
-    {
+      // bit planes of every (brick, subband) of the level: one warp each, tables allocated
+      // with a cursor in a grow-only workspace; units of more than 32 channels go to a second
+      // pass, whose count the kernel reads on the device
+      const size_t nunits = (size_t)nbr * (size_t)r0.nsb;
+      unsigned long long* d_uoff = (unsigned long long*)ctx->ws("dec.unitoff", nunits * 8);
+      unsigned long long* d_pcur = (unsigned long long*)ctx->ws("dec.pcursor", 16);
+      int* d_wide = (int*)ctx->ws("dec.widelist", nunits * 4);
+      if (!d_uoff || !d_pcur || !d_wide)
+        return OutOfMemory;
+      unsigned long long cap = (unsigned long long)nunits * 16384ull + (16ull << 20);
+      if (cap < min_cap)
+        cap = min_cap;
+      if (ctx->ws_size("dec.planes") > cap)
+        cap = ctx->ws_size("dec.planes");
       unsigned long long* d_planes = (unsigned long long*)ctx->ws("dec.planes", (size_t)cap);
       if (!d_planes)
         return OutOfMemory;
       cap = ctx->ws_size("dec.planes");
+      dec1_args pa;
+      memset(&pa, 0, sizeof pa);
+      pa.nsb = r0.nsb;
+      pa.nbricks = nbr;
+      pa.end_bp = a.end_bp;
+      pa.reqs = d_reqs;
+      memcpy(pa.nblocks, lw->nblocks, sizeof pa.nblocks);
+      pa.geom = d_geom;
+      pa.bricks = d_bricks;
+      pa.exps = exps_;
+      pa.ckmin = kmin_;
+      pa.cn = n_;
+      pa.cfirst = first_;
+      pa.coff = off_;
+      pa.blob = blob_;
+      pa.blob_bytes = blob_bytes_;
+      pa.cursor = d_pcur;
+      pa.unit_off = d_uoff;
+      pa.error = d_err + 1;
+      pa.wide_count = (int*)(d_pcur + 1);
+      pa.wide_list = d_wide;
       pa.planes = d_planes;
       pa.cap_bytes = cap;
-      cudaMemsetAsync(d_pcur, 0, 16, st);
-      cudaMemsetAsync(d_err + 1, 0, 4, st);
-      cudaEventRecord(e0, st);
-      k_decode_planes<false><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
-      ++ctx->launches;
-      cudaEventRecord(e1, st);
-      if (cudaGetLastError() != cudaSuccess)
-        return CudaError;
-      unsigned long long pc[2] = { 0, 0 };
-      cudaMemcpyAsync(pc, d_pcur, 16, cudaMemcpyDeviceToHost, st);
-      if (cudaStreamSynchronize(st) != cudaSuccess)
-        return CudaError;
-      float pms = 0;
-      cudaEventElapsedTime(&pms, e0, e1);
-      level_ms += pms;
-      const int nwide = (int)(pc[1] & 0xffffffffu);
-      if (nwide > 0)
-      {
-        // units of more than 32 channels
-        cudaEventRecord(e0, st);
-        k_decode_planes<true><<<(nwide + kPlaneWarps - 1) / kPlaneWarps, kPlaneWarps * 32, 0, st>>>(pa);
-        ++ctx->launches;
-        cudaEventRecord(e1, st);
-        if (cudaGetLastError() != cudaSuccess)
-          return CudaError;
-      }
-      int perr = 0;
-      unsigned long long used = 0;
-      cudaMemcpyAsync(&perr, d_err + 1, 4, cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(&used, d_pcur, 8, cudaMemcpyDeviceToHost, st);
-      if (cudaStreamSynchronize(st) != cudaSuccess)
-        return CudaError;
-      if (nwide > 0)
-      {
-        cudaEventElapsedTime(&pms, e0, e1);
-        level_ms += pms;
-      }
-      if (perr == 1)
-        return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
-      if (perr == 2)
-      {
-        cap = used + (1ull << 20);
-        continue;
-      }
       a.planes = d_planes;
       a.unit_off = d_uoff;
-      break;
+      cudaMemsetAsync(d_pcur, 0, 16, st);
+      const int pgrid = (int)((nunits + kPlaneWarps - 1) / kPlaneWarps);
+      cudaEvent_t t0 = ctx->ev(2 * nev), t1 = ctx->ev(2 * nev + 1);
+      if (!t0 || !t1)
+        return CudaError;
+      ++nev;
+      cudaEventRecord(t0, st);
+      k_decode_planes<false><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
+      k_decode_planes<true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(pa);
+      k_decode_level<<<grid, kThreads, smem, st>>>(a);
+      cudaEventRecord(t1, st);
+      ctx->launches += 3;
+      if (cudaGetLastError() != cudaSuccess)
+        return CudaError;
+      prev = d_level;
     }
-    if (!a.planes)
-      return DeviceStreamOverflow;
-    cudaEventRecord(e0, st);
-    k_decode_level<<<grid, kThreads, smem, st>>>(a);
-    ++ctx->launches;
-    cudaEventRecord(e1, st);
-    if (cudaGetLastError() != cudaSuccess)
-      return CudaError;
+    int herr[2] = { 0, 0 };
+    cudaMemcpyAsync(herr, d_err, 8, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess)
       return CudaError;
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    total_ms += ms + level_ms;
-    prev = d_level;
+    if (herr[1] & 2)
+    {
+      min_cap = 2ull * (unsigned long long)ctx->ws_size("dec.planes");
+      continue;
+    }
+    if ((herr[1] & 1) || herr[0])
+      return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband, or stream error
+    float total_ms = 0;
+    for (size_t e = 0; e < nev; ++e)
+    {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ctx->ev(2 * e), ctx->ev(2 * e + 1));
+      total_ms += ms;
+    }
+    if (!out_on_device)
+    {
+      for (size_t i = 0; i < n; ++i)
+        if (out_bytes[i])
+          cudaMemcpyAsync(outs[i], d_out[i], out_bytes[i], cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess)
+        return CudaError;
+    }
+    if (kernel_ms)
+      *kernel_ms = total_ms;
+    return NoError;
   }
-  int herr = 0;
-  cudaMemcpyAsync(&herr, d_err, 4, cudaMemcpyDeviceToHost, st);
-  if (!out_on_device)
-    for (size_t i = 0; i < n; ++i)
-      if (out_bytes[i])
-        cudaMemcpyAsync(outs[i], d_out[i], out_bytes[i], cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess)
-    return CudaError;
-  if (herr)
-    return DeviceStreamOverflow;
-  if (kernel_ms)
-    *kernel_ms = total_ms;
-  return NoError;
+  return DeviceStreamOverflow;
 }
 
 

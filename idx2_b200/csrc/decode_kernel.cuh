@@ -81,7 +81,7 @@ struct dec1_args
   unsigned long long cap_bytes;
   unsigned long long* cursor;
   unsigned long long* unit_off;
-  int* error;                       // 1: too many channels, 2: table capacity exceeded
+  int* error;                       // bit flags: 1 too many channels, 2 table capacity exceeded
   int* wide_count;                  // units with more than 32 channels, deferred by the first pass
   int* wide_list;
 };
@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_plane
     if (nkeys > kKeyWindow)
     {
       if (lane == 0)
-        atomicExch(a.error, 1);
+        atomicOr(a.error, 1);
       nkeys = 0;
     }
     if (nkeys == 0)
@@ -495,7 +495,7 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_plane
     {
       if (lane == 0)
       {
-        atomicExch(a.error, 2);
+        atomicOr(a.error, 2);
         a.unit_off[unit] = ~0ull;
       }
       continue;

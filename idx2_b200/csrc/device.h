@@ -22,6 +22,7 @@ struct device_ctx
   bool own_stream = false;
   int num_sms = 148;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> evpool;  // timing events of calls that time several launches
   long long launches = 0;  // kernels launched on this context so far
   std::map<std::string, int> tuned;  // batched encode: CTAs per SM chosen per batch signature
 
@@ -39,11 +40,15 @@ struct device_ctx
     buf& b = bufs[name];
     if (b.n < bytes || !b.p)
     {
+      // a buffer that has to grow again grows by half at least, so a run of growing requests
+      // (serving batches of rising size) reallocates a logarithmic number of times
+      size_t want = bytes + bytes / 8 + 256;
+      if (b.n && want < b.n + b.n / 2)
+        want = b.n + b.n / 2;
       if (b.p)
         cudaFree(b.p);
       b.p = nullptr;
       b.n = 0;
-      size_t want = bytes + bytes / 8 + 256;
       if (cudaMalloc(&b.p, want) != cudaSuccess)
         return nullptr;
       b.n = want;
@@ -93,8 +98,23 @@ struct device_ctx
     }
     return b.p;
   }
+  // Timing event i of the pool (created on first use), or null.
+  cudaEvent_t ev(size_t i)
+  {
+    while (evpool.size() <= i)
+    {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreate(&e) != cudaSuccess)
+        return nullptr;
+      evpool.push_back(e);
+    }
+    return evpool[i];
+  }
   void release()
   {
+    for (cudaEvent_t e : evpool)
+      cudaEventDestroy(e);
+    evpool.clear();
     for (auto& kv : bufs)
       if (kv.second.p)
         cudaFree(kv.second.p);

@@ -30,6 +30,18 @@ class Dataset:
         if rc:
             raise Idx2Error(rc, "idx2g_dataset_open")
         self.h = h
+        name, field = ctypes.create_string_buffer(64), ctypes.create_string_buffer(64)
+        dims, dt, nl = (ctypes.c_int * 3)(), ctypes.c_int(), ctypes.c_int()
+        tol, res = ctypes.c_double(), ctypes.c_longlong()
+        rc = lib().idx2g_dataset_info(h, name, field, dims, ctypes.byref(dt), ctypes.byref(nl), ctypes.byref(tol),
+                                      ctypes.byref(res))
+        if rc:
+            raise Idx2Error(rc, "idx2g_dataset_info")
+        self._dtype = np.float32 if dt.value == 0 else np.float64  # IDX2G_FLOAT32 = 0
+        self.dims = tuple(dims)
+        self.num_levels = nl.value
+        self.tolerance = tol.value
+        self.resident_bytes = res.value
 
     def _req(self, first, last, downsampling, tolerance) -> Params:
         p = Params(input_file=self.params.input_file, in_dir=self.params.in_dir,
@@ -84,8 +96,9 @@ class Dataset:
         if n == 0:
             return []
         cps = (_CParams * n)()
-        outs, ptrs, sizes = [], [], []
+        outs, ptrs, sizes, shapes = [], [], [], []
         dt = self.dtype
+        esz = np.dtype(dt).itemsize
         import torch
         for i, r in enumerate(requests):
             first, last = r.get("first"), r.get("last")
@@ -93,17 +106,26 @@ class Dataset:
             p = self._req(first, last, ds, r.get("tolerance", 0.0))
             cps[i] = p.to_c()
             _, dims, _ = self.output_grid(first, last, ds)
-            shape = (dims[2], dims[1], dims[0])
-            if device_out:
-                o = torch.empty(shape, dtype=torch.float32 if dt == np.float32 else torch.float64,
-                                device=torch.device("cuda", self.device))
-                ptrs.append(o.data_ptr())
-                sizes.append(o.numel() * o.element_size())
-            else:
+            shapes.append((dims[2], dims[1], dims[0]))
+            sizes.append(int(np.prod(shapes[-1])) * esz)
+        if device_out:
+            # one allocation for the whole call (each grid 256-byte aligned), the grids are views
+            # of it: a serving loop of varying batches then reuses a few cached blocks
+            offs, total = [], 0
+            for b in sizes:
+                offs.append(total)
+                total += (b + 255) & ~255
+            arena = torch.empty(max(total, 1), dtype=torch.uint8, device=torch.device("cuda", self.device))
+            tdt = torch.float32 if dt == np.float32 else torch.float64
+            for shape, off, b in zip(shapes, offs, sizes):
+                o = arena[off:off + b].view(tdt).view(shape)
+                outs.append(o)
+                ptrs.append(arena.data_ptr() + off)
+        else:
+            for shape in shapes:
                 o = np.empty(shape, dtype=dt)
+                outs.append(o)
                 ptrs.append(o.ctypes.data)
-                sizes.append(o.nbytes)
-            outs.append(o)
         arr = (ctypes.c_void_p * n)(*[ctypes.c_void_p(q) for q in ptrs])
         szs = (ctypes.c_size_t * n)(*sizes)
         kms = ctypes.c_double(0)
@@ -121,9 +143,7 @@ class Dataset:
 
     @property
     def dtype(self):
-        with open(self.params.input_file) as f:
-            txt = f.read()
-        return np.float32 if '"float32"' in txt else np.float64
+        return self._dtype
 
     def close(self):
         if getattr(self, "h", None):

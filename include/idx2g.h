@@ -146,9 +146,6 @@ IDX2G_API int idx2g_decode_batch(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_
 IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p,
                                    void* d_out, size_t out_bytes, double* kernel_ms);
 
-/* Metadata of an open dataset (the fields of the .idx2 file): name and field (64 bytes
-   each, NUL-terminated), dims, dtype, number of levels, encode tolerance, and the bytes
-   the dataset keeps resident on the device. */
 /* Batched encode: n fields (params[i], field[i]) through one device stage, then each is
    packed and written as idx2g_encode writes it (the files are identical). The reference
    encodes one field per call (Core/idx2Encode.cpp:390 Encode); here the bricks of every
@@ -176,7 +173,11 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* ctx, const idx2g_params* params, con
    0 (finest) to L-1; on each level the bricks in row-major order of their coordinates (x
    fastest); each brick 33^3 values (33^2 for 2D) indexed (z*33 + y)*33 + x, every coefficient
    at the position of the sample its block transforms; idx2g_coeff_count gives its length.
-   Batched calls take nbatch tensors (and grids) back to back. Values are of p's dtype. */
+   Batched calls take nbatch tensors (and grids) back to back. Values are of p's dtype.
+   D(idx2g_coeffs(...)) equals idx2g_decode's grid up to the floors of the integer inverse
+   zfp, except in 2D where a low-band block below the coarsest level had no bit plane above
+   the decode tolerance: the decode keeps the parent's values there, D writes the block's
+   (zero) coefficients. */
 IDX2G_API long long idx2g_coeff_count(const idx2g_params* p);
 /* The dataset's dequantised coefficients (at p's decode tolerance) into d_coeffs. */
 IDX2G_API int idx2g_coeffs(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p, void* d_coeffs,
@@ -192,6 +193,9 @@ IDX2G_API int idx2g_synth_adjoint(idx2g_ctx* ctx, const idx2g_params* p, int nba
    benchmarks; no counterpart in the reference). */
 IDX2G_API long long idx2g_ctx_launches(const idx2g_ctx* ctx);
 
+/* Metadata of an open dataset (the fields of the .idx2 file): name and field (64 bytes
+   each, NUL-terminated), dims, dtype, number of levels, encode tolerance, and the bytes
+   the dataset keeps resident on the device. */
 IDX2G_API int idx2g_dataset_info(const idx2g_dataset* ds, char* name, char* field, int dims3[3],
                                  int* dtype, int* num_levels, double* tolerance,
                                  long long* resident_bytes);
