@@ -43,6 +43,11 @@ FALLBACK_HBM = 6650.0
 LEVELS = 3
 TOL = 1e-3
 METRIC = "encode+decode GB/s (raw field bytes) at 1e-3 tol"
+# DRAM bytes (read + write) of one level-0 k_encode_level launch per brick, from an ncu capture
+# of the grf512 workload (4,096 bricks: 1.710 GB read + 2.923 GB written); the traffic of a
+# launch grows with its bricks (every brick makes the same slot sweeps), so a full launch's
+# traffic is this figure times its bricks.
+ENC_L0_TRAFFIC_PER_BRICK = (1.709702e9 + 2.922549e9) / 4096
 
 
 def hbm_peak():
@@ -344,7 +349,10 @@ def ours(args, rank, world, local_rank):
         "roofline": {"bound": "hbm", "kernel": "k_encode_level (level 0)", "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else kind,
-                     "algorithmic_bytes": l0_bytes, "traffic": None},
+                     "algorithmic_bytes": l0_bytes,
+                     "traffic": ENC_L0_TRAFFIC_PER_BRICK * (side // 32) ** 3,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the level-0 launch "
+                                       "at 512^3 (4,096 bricks), scaled by bricks"},
         "cpu_baseline": base,
         "e2e": {"value": world * 2 * raw_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "s_per_step": e2e_s,
