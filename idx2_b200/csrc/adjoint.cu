@@ -328,35 +328,6 @@ __device__ __forceinline__ void cdf_x(const T* sw, T* S, int np, int z0, int tid
   }
 }
 
-// 32-bit address of a shared-memory location of CTA `rank` of the cluster, and loads / stores
-// through it (distributed shared memory).
-__device__ __forceinline__ unsigned cluster_addr(const void* p, int rank)
-{
-  unsigned r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"((unsigned)__cvta_generic_to_shared(p)), "r"(rank));
-  return r;
-}
-
-template <typename T>
-__device__ __forceinline__ T ld_cluster(unsigned addr)
-{
-  T v;
-  if constexpr (sizeof(T) == 4)
-    asm volatile("ld.shared::cluster.f32 %0, [%1];\n" : "=f"(v) : "r"(addr) : "memory");
-  else
-    asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(addr) : "memory");
-  return v;
-}
-
-template <typename T>
-__device__ __forceinline__ void st_cluster(unsigned addr, T v)
-{
-  if constexpr (sizeof(T) == 4)
-    asm volatile("st.shared::cluster.f32 [%0], %1;\n" ::"r"(addr), "f"(v) : "memory");
-  else
-    asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(addr), "d"(v) : "memory");
-}
-
 // The cluster CTA holding plane z of the brick.
 __device__ __forceinline__ int plane_rank(int z)
 {
@@ -389,7 +360,7 @@ __global__ void __launch_bounds__(kSynThreads, syn_ctas_per_sm<T>()) k_synth(con
     rank = (int)cg::this_cluster().block_rank();
 #pragma unroll
     for (int r = 0; r < CS; ++r)
-      base[r] = cluster_addr(S, r);
+      base[r] = dev::cluster_addr(S, r);
     cluster_sync<CS>();  // every CTA of the cluster has started before any remote access
   }
   const int z0 = IS2D ? 0 : rank * kPPC;
@@ -442,7 +413,7 @@ __global__ void __launch_bounds__(kSynThreads, syn_ctas_per_sm<T>()) k_synth(con
         T v[33];
 #pragma unroll
         for (int z = 0; z < 33; ++z)
-          v[z] = ld_cluster<T>(base[plane_rank(z)] + (unsigned)(((z - plane_rank(z) * kPPC) * kPlane + c) * sizeof(T)));
+          v[z] = dev::ld_cluster<T>(base[plane_rank(z)] + (unsigned)(((z - plane_rank(z) * kPPC) * kPlane + c) * sizeof(T)));
         rilift33(v);
         if (a.finest)
         {
@@ -519,7 +490,7 @@ __global__ void __launch_bounds__(kSynThreads, syn_ctas_per_sm<T>()) k_synth_adj
     rank = (int)cg::this_cluster().block_rank();
 #pragma unroll
     for (int r = 0; r < CS; ++r)
-      base[r] = cluster_addr(S, r);
+      base[r] = dev::cluster_addr(S, r);
     cluster_sync<CS>();  // every CTA of the cluster has started before any remote access
   }
   const int z0 = IS2D ? 0 : rank * kPPC;
@@ -562,7 +533,7 @@ __global__ void __launch_bounds__(kSynThreads, syn_ctas_per_sm<T>()) k_synth_adj
         rilift33_adj(v);
 #pragma unroll
         for (int z = 0; z < 33; ++z)
-          st_cluster<T>(base[plane_rank(z)] + (unsigned)(((z - plane_rank(z) * kPPC) * kPlane + c) * sizeof(T)), v[z]);
+          dev::st_cluster<T>(base[plane_rank(z)] + (unsigned)(((z - plane_rank(z) * kPPC) * kPlane + c) * sizeof(T)), v[z]);
       }
       cluster_sync<CS>();
       cdf_x<T, false, true, false>(sw, S, np, z0, tid);

@@ -509,6 +509,16 @@ IDX2G_API long long idx2g_coeff_count(const idx2g_params* in)
   return synth_coeff_count(f);
 }
 
+IDX2G_API int idx2g_decode_brick_map(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* in, const char* path,
+                                     double* kernel_ms)
+{
+  if (!c || !ds || !in || !path)
+    return InvalidArgument;
+  params p;
+  to_params(in, &p);
+  return dataset_decode_brick_map(&c->d, (dataset_handle*)ds, p, path, kernel_ms);
+}
+
 IDX2G_API int idx2g_coeffs(idx2g_ctx* c, idx2g_dataset* ds, const idx2g_params* in, void* d_coeffs, size_t bytes,
                            double* kernel_ms)
 {

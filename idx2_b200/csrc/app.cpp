@@ -7,7 +7,7 @@
 //             [--name N --field F --dims X Y Z --type float32|float64]
 //   idx2g_app --decode D/Name/Field.idx2 [--first x y z --last x y z]
 //             [--downsampling a b c] [--tolerance t] [--in_dir D] [--out_dir D]
-//             [--out_file F] [--dry]
+//             [--out_file F] [--dry] [--brick_map]
 #include "../../include/idx2g.h"
 
 #include <chrono>
@@ -226,6 +226,22 @@ int do_decode(int argc, char** argv)
   {
     idx2g_ctx_destroy(ctx);
     return die("open", e);
+  }
+  if (find(argc, argv, "--brick_map") >= 0)
+  {
+    // Applications/idx2App.cpp:51-53: the HashMap output mode, written to "bricks" in the
+    // working directory (Core/idx2Decode.cpp:477)
+    double kms = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    e = idx2g_decode_brick_map(ctx, ds, &p, "bricks", &kms);
+    auto t1 = std::chrono::steady_clock::now();
+    idx2g_dataset_close(ds);
+    idx2g_ctx_destroy(ctx);
+    if (e)
+      return die("decode", e);
+    printf("kernel time         = %f ms\n", kms);
+    printf("total decode time   = %f\n", std::chrono::duration<double>(t1 - t0).count());
+    return 0;
   }
   int from[3], dims[3], strd[3];
   idx2g_output_grid(ds, &p, from, dims, strd);

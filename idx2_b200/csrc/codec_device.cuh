@@ -735,5 +735,37 @@ __device__ __forceinline__ void or_code(uint32_t* words, unsigned long long pos,
   }
 }
 
+// Distributed shared memory of a thread-block cluster: the 32-bit shared::cluster address of
+// a location of CTA `rank`'s shared memory (the same variable as `p` in this CTA), and loads /
+// stores through it.
+__device__ __forceinline__ unsigned cluster_addr(const void* p, int rank)
+{
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n"
+               : "=r"(r)
+               : "r"((unsigned)__cvta_generic_to_shared(p)), "r"(rank));
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T ld_cluster(unsigned addr)
+{
+  T v;
+  if constexpr (sizeof(T) == 4)
+    asm volatile("ld.shared::cluster.f32 %0, [%1];\n" : "=f"(v) : "r"(addr) : "memory");
+  else
+    asm volatile("ld.shared::cluster.f64 %0, [%1];\n" : "=d"(v) : "r"(addr) : "memory");
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ void st_cluster(unsigned addr, T v)
+{
+  if constexpr (sizeof(T) == 4)
+    asm volatile("st.shared::cluster.f32 [%0], %1;\n" ::"r"(addr), "f"(v) : "memory");
+  else
+    asm volatile("st.shared::cluster.f64 [%0], %1;\n" ::"r"(addr), "d"(v) : "memory");
+}
+
 } // namespace dev
 } // namespace idx2g

@@ -106,7 +106,7 @@ int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, 
 
 int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_request*>& rqs,
                                 void* const* outs, const size_t* out_bytes, bool out_on_device, double* kernel_ms,
-                                void* coeff_out)
+                                void* coeff_out, decode_keep* keep)
 {
   const size_t n = rqs.size();
   if (n == 0)
@@ -164,6 +164,11 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
     if (coeff_out)
       cudaMemsetAsync(coeff_out, 0, (size_t)coeff_base[(size_t)L] * (size_t)NB * (r0.f32 ? 4 : 8), st);
     cudaMemsetAsync(d_err, 0, 16, st);
+    if (keep)
+    {
+      keep->bricks.assign((size_t)L, nullptr);
+      keep->sig.assign((size_t)L, std::vector<int>());
+    }
     size_t nev = 0;  // levels timed (event pairs of the pool)
     double* prev = nullptr;
     std::vector<int> prev_base(n, -1), cur_base(n, -1);
@@ -190,7 +195,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         decode_target t;
         memset(&t, 0, sizeof t);
         t.mask = lv.mask;
-        t.is_output = lv.is_output;
+        t.is_output = keep ? 0 : lv.is_output;  // brick-map mode keeps the output level's bricks too
         t.etol = rq.etol;
         memcpy(t.spacing, lv.spacing, sizeof t.spacing);
         t.out = d_out[i];
@@ -199,7 +204,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         t.out_dims[2] = rq.out_dims.z;
         const int ti = (int)targets.size();
         targets.push_back(t);
-        cur_base[i] = lv.is_output || coeff_out ? -1 : nstore;
+        cur_base[i] = (lv.is_output && !keep) || coeff_out ? -1 : nstore;
         int li_in_level = 0;
         for (const decode_brick& b : lv.bricks)
         {
@@ -209,7 +214,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
           if (coeff_out)
             db.store = (int)(coeff_base[(size_t)l] + li_in_level++);
           else
-            db.store = lv.is_output ? -1 : nstore++;
+            db.store = lv.is_output && !keep ? -1 : nstore++;
           hb.push_back(db);
         }
       }
@@ -223,8 +228,22 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       ++li;
       decode_brick* d_bricks = (decode_brick*)ctx->ws("dec.bricks", sizeof(decode_brick) * (size_t)nbr);
       decode_target* d_reqs = (decode_target*)ctx->ws("dec.reqs", sizeof(decode_target) * targets.size());
-      double* d_level = nstore ? (double*)ctx->ws(li % 2 ? "dec.levA" : "dec.levB", (size_t)nstore * (size_t)NB * 8)
+      char kn[32];
+      snprintf(kn, sizeof kn, "dec.keep%d", l);
+      double* d_level = nstore ? (double*)ctx->ws(keep ? kn : (li % 2 ? "dec.levA" : "dec.levB"),
+                                                  (size_t)nstore * (size_t)NB * 8)
                                : nullptr;
+      int* d_sig = nullptr;
+      if (keep)
+      {
+        snprintf(kn, sizeof kn, "dec.sig%d", l);
+        d_sig = (int*)ctx->ws(kn, (size_t)nstore * 4 + 4);
+        if (!d_sig)
+          return OutOfMemory;
+        cudaMemsetAsync(d_sig, 0, (size_t)nstore * 4, st);
+        keep->bricks[(size_t)l] = d_level;
+        keep->sig[(size_t)l].assign((size_t)nstore, 0);
+      }
       int grid = nbr < 2 * ctx->num_sms ? nbr : 2 * ctx->num_sms;
       double* d_slots = (double*)ctx->ws("dec.slots", (size_t)grid * (size_t)NB * 8);
       if (!d_bricks || !d_reqs || (nstore && !d_level) || !d_slots)
@@ -271,6 +290,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       a.slots = d_slots;
       a.reqs = d_reqs;
       a.error = d_err;
+      a.sig = d_sig;
       a.coeff_out = coeff_out;
 
       // bit planes of every (brick, subband) of the level: one warp each, tables allocated
@@ -334,6 +354,15 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
     }
     int herr[2] = { 0, 0 };
     cudaMemcpyAsync(herr, d_err, 8, cudaMemcpyDeviceToHost, st);
+    if (keep)
+      for (int l = 0; l < L; ++l)
+        if (!keep->sig[(size_t)l].empty())
+        {
+          char kn[32];
+          snprintf(kn, sizeof kn, "dec.sig%d", l);
+          cudaMemcpyAsync(keep->sig[(size_t)l].data(), ctx->ws(kn, keep->sig[(size_t)l].size() * 4 + 4),
+                          keep->sig[(size_t)l].size() * 4, cudaMemcpyDeviceToHost, st);
+        }
     if (cudaStreamSynchronize(st) != cudaSuccess)
       return CudaError;
     if (herr[1] & 2)
@@ -365,6 +394,48 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
   return DeviceStreamOverflow;
 }
 
+
+namespace
+{
+
+// Pieces of kept bricks (subband-major) to a dense buffer, x fastest: a CTA per piece.
+__global__ void k_gather_pieces(const brick_piece* pieces, int n, int is2d, double* out)
+{
+  for (int pi = blockIdx.x; pi < n; pi += gridDim.x)
+  {
+    const brick_piece p = pieces[pi];
+    const int nxy = p.dims[0] * p.dims[1];
+    const int cnt = nxy * p.dims[2];
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x)
+    {
+      const int x = i % p.dims[0], y = (i / p.dims[0]) % p.dims[1], z = i / nxy;
+      out[p.out + i] = p.src[sbm(p.from[0] + x, p.from[1] + y, p.from[2] + z, is2d)];
+    }
+  }
+}
+
+} // namespace
+
+int decode_device::gather_bricks(device_ctx* ctx, const std::vector<brick_piece>& pieces, bool is2d, size_t total,
+                                 double* host_out)
+{
+  if (pieces.empty() || total == 0)
+    return NoError;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  brick_piece* d_p = (brick_piece*)ctx->ws("dec.pieces", sizeof(brick_piece) * pieces.size());
+  double* d_out = (double*)ctx->ws("dec.piecesout", total * 8);
+  if (!d_p || !d_out)
+    return OutOfMemory;
+  cudaMemcpyAsync(d_p, pieces.data(), sizeof(brick_piece) * pieces.size(), cudaMemcpyHostToDevice, st);
+  const int n = (int)pieces.size();
+  k_gather_pieces<<<n < 8 * ctx->num_sms ? n : 8 * ctx->num_sms, 256, 0, st>>>(d_p, n, is2d ? 1 : 0, d_out);
+  ++ctx->launches;
+  if (cudaGetLastError() != cudaSuccess)
+    return CudaError;
+  cudaMemcpyAsync(host_out, d_out, total * 8, cudaMemcpyDeviceToHost, st);
+  return cudaStreamSynchronize(st) == cudaSuccess ? NoError : CudaError;
+}
 
 // ---------------------------------------------------------------------------
 // Allocation-free decode (idx2g_decode_noalloc)

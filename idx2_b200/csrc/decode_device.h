@@ -46,6 +46,7 @@ struct decode_level
   double inv_weight[8] = {};
   int norm_mask = 0;
   std::vector<decode_brick> bricks;
+  std::vector<v3> b3;  // brick coordinates of `bricks` (host side)
 };
 
 struct decode_request
@@ -55,6 +56,24 @@ struct decode_request
   int etol = 0;
   v3 out_from, out_dims, out_strd;
   std::vector<decode_level> levels;  // coarsest first
+};
+
+// Brick-map mode (the reference's HashMap output, Core/idx2Decode.cpp:446-477): every decoded
+// level's bricks are kept on the device (subband-major, in plan order) with a significance flag
+// per brick (a block of a subband > 0, or of the coarsest level, was decoded).
+struct decode_keep
+{
+  std::vector<const double*> bricks;     // per level l: [plan bricks][33^3] or null (not decoded)
+  std::vector<std::vector<int>> sig;     // per level l: significance per plan brick
+};
+
+// A part of a kept brick copied out by gather_bricks: samples [from, from + dims) of the
+// brick at src, x fastest, to out (elements).
+struct brick_piece
+{
+  const double* src;
+  int from[3], dims[3];
+  long long out;
 };
 
 class decode_device
@@ -70,8 +89,13 @@ public:
   // bricks of every request that decodes the level. outs[i] receives request i's grid.
   // coeff_out (coefficient mode, one full-field request): the dequantised coefficients of every
   // brick (levels finest first, bricks row-major, 33^3 each) in place of the grid.
+  // keep (brick-map mode, one full-field request): every level's bricks kept, see decode_keep.
   int decode_batch(device_ctx* ctx, const std::vector<const decode_request*>& rqs, void* const* outs,
-                   const size_t* out_bytes, bool out_on_device, double* kernel_ms, void* coeff_out = nullptr);
+                   const size_t* out_bytes, bool out_on_device, double* kernel_ms, void* coeff_out = nullptr,
+                   decode_keep* keep = nullptr);
+  // Copy pieces of kept bricks (subband-major) into a host buffer of `total` doubles.
+  static int gather_bricks(device_ctx* ctx, const std::vector<brick_piece>& pieces, bool is2d, size_t total,
+                           double* host_out);
   // Allocation-free decode into a device buffer: every temporary lives in a fixed static
   // device array of decode.cu (limits and semantics there and in include/idx2g.h).
   int decode_noalloc(device_ctx* ctx, const decode_request& rq, void* d_out, size_t out_bytes,

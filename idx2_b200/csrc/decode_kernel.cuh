@@ -53,6 +53,7 @@ struct dec_args
   double* slots;                      // per-CTA slots (output bricks)
   const decode_target* reqs;          // request table of the launch
   int* error;
+  int* sig;                           // brick-map mode: significance per stored brick (or null)
   // coefficient mode: the dequantised zfp-domain coefficients of every brick, at their sample
   // positions in a 33^3 (33^2) brick of the dataset's dtype (brick `store` of the tensor), in
   // place of the decoded grid
@@ -111,6 +112,7 @@ struct dec_smem
   uint8_t stop[2][kKeyWindow];
   int kmax[8], nkeys[8];
   int wide;
+  int sig;           // a block of a subband > 0 (or of the coarsest level) was decoded
   decode_target rq;  // the current brick's request
 };
 
@@ -560,6 +562,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       for (int i = tid; i < (int)(sizeof(decode_target) / 4); i += kThreads)
         dst[i] = src[i];
     }
+    if (tid == 0)
+      sm.sig = 0;
     __syncthreads();
     const decode_target& rq = sm.rq;
     double* F = rq.is_output ? a.slots + (size_t)blockIdx.x * (size_t)NB
@@ -712,6 +716,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
           const bool actA = sm.np[s][bA] > 0 && !sm.bypass[s][bA];
           const bool actB = hasB && sm.np[s][bB] > 0 && !sm.bypass[s][bB];
           const int npA = sm.np[s][bA], npB = hasB ? sm.np[s][bB] : 0;
+          // Core/idx2Decode.cpp:209-211: a decoded block of a subband > 0, or of the coarsest
+          // level, makes the brick significant
+          if (lane == 0 && (actA || actB) && (s > 0 || a.level + 1 == a.nlevels))
+            sm.sig = 1;
           unsigned long long uA0, uA1, uB0, uB1;
           transpose(cA0, cA1, npA > 32, uA0, uA1);
           transpose(cB0, cB1, npB > 32, uB0, uB1);
@@ -991,6 +999,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
     }
     __syncthreads();
     DEC_PHASE(2)
+    if (a.sig && tid == 0 && br.store >= 0)
+      a.sig[br.store] = sm.sig;
 
     if (a.coeff_out)
       continue;

@@ -663,6 +663,7 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
           db.store = lv.is_output ? -1 : (int)lv.bricks.size();
           pos_of[(size_t)l][bi] = (int)lv.bricks.size();
           lv.bricks.push_back(db);
+          lv.b3.push_back(b);
         }
     for (int s = 0; s < nsb; ++s)
     {
@@ -742,6 +743,125 @@ int dataset_coeffs(device_ctx* ctx, dataset_handle* h, const params& p, void* d_
   void* none = nullptr;
   size_t zero = 0;
   return h->dev.decode_batch(ctx, rqs, &none, &zero, true, kernel_ms, d_coeffs);
+}
+
+// The reference's HashMap output (--brick_map; Core/idx2Decode.cpp:446-477 and
+// Core/idx2SparseBricks.cpp:69-230): decode the whole field keeping every significant brick,
+// give every finest brick the finest level at which its ancestor (or itself) is significant
+// (ComputeBrickResolution), and write, for the finest bricks in row-major order, that
+// brick's samples over the finest brick's part of it (GetBrickVolume, WriteBricks).
+int dataset_decode_brick_map(device_ctx* ctx, dataset_handle* h, const params& p, const char* path,
+                             double* kernel_ms)
+{
+  params q = p;
+  q.has_extent = false;
+  decode_request rq;
+  size_t need = 0;
+  int e = plan_decode(h, q, &rq, &need);
+  if (e)
+    return e;
+  decode_keep keep;
+  std::vector<const decode_request*> rqs(1, &rq);
+  void* none = nullptr;
+  size_t zero = 0;
+  e = h->dev.decode_batch(ctx, rqs, &none, &zero, true, kernel_ms, nullptr, &keep);
+  if (e)
+    return e;
+  const dataset_format& f = h->f;
+  const int L = f.nlevels;
+  const bool is2d = f.is2d();
+  const size_t NB = is2d ? 33 * 33 : 33 * 33 * 33;
+  // level, brick coordinates -> plan index
+  std::vector<std::unordered_map<long long, int>> at((size_t)L);
+  auto key = [&](int l, const v3& b) {
+    const v3 n = f.nbricks3[(size_t)l];
+    return ((long long)b.z * n.y + b.y) * n.x + b.x;
+  };
+  for (const decode_level& lv : rq.levels)
+    for (size_t i = 0; i < lv.b3.size(); ++i)
+      at[(size_t)lv.level][key(lv.level, lv.b3[i])] = (int)i;
+  auto find = [&](int l, const v3& b) -> int {
+    auto it = at[(size_t)l].find(key(l, b));
+    return it == at[(size_t)l].end() ? -1 : it->second;
+  };
+  auto group_pow = [&](int r) {
+    v3 g(1);
+    for (int k = 0; k < r; ++k)
+      g = g * f.group_brick3;
+    return g;
+  };
+  const v3 n0 = f.nbricks3[0];
+  std::vector<brick_piece> pieces;
+  std::vector<v3> dims_of;
+  pieces.reserve((size_t)prod(n0));
+  long long total = 0;
+  for (int bz = 0; bz < n0.z; ++bz)
+    for (int by = 0; by < n0.y; ++by)
+      for (int bx = 0; bx < n0.x; ++bx)
+      {
+        const v3 b3(bx, by, bz);
+        // ComputeBrickResolution: the finest significant level along the chain, else the
+        // coarsest level
+        int r = L - 1;
+        for (int l = L - 1; l >= 0; --l)
+        {
+          const int i = find(l, b3 / group_pow(l));
+          if (i >= 0 && keep.sig[(size_t)l][(size_t)i])
+            r = l;
+        }
+        const v3 a3 = b3 / group_pow(r);
+        const int i = find(r, a3);
+        if (i < 0 || !keep.bricks[(size_t)r])
+          return BrickNotFound;
+        brick_piece pc;
+        memset(&pc, 0, sizeof pc);
+        pc.src = keep.bricks[(size_t)r] + (size_t)i * NB;
+        v3 from(0), dims = f.brick_dims_ext;
+        if (r > 0)
+        {
+          const v3 bd(f.brick_dims.x >> r, f.brick_dims.y >> r, f.brick_dims.z >> r);
+          dims = v3(bd.x + (bd.x > 1), bd.y + (bd.y > 1), bd.z + (bd.z > 1));  // idx2_ExtDims
+          from = (b3 % group_pow(r)) * bd;
+        }
+        pc.from[0] = from.x;
+        pc.from[1] = from.y;
+        pc.from[2] = from.z;
+        pc.dims[0] = dims.x;
+        pc.dims[1] = dims.y;
+        pc.dims[2] = dims.z;
+        pc.out = total;
+        total += (long long)dims.x * dims.y * dims.z;
+        pieces.push_back(pc);
+        dims_of.push_back(dims);
+      }
+  std::vector<double> samples((size_t)total);
+  e = decode_device::gather_bricks(ctx, pieces, is2d, (size_t)total, samples.data());
+  if (e)
+    return e;
+  FILE* fp = fopen(path, "wb");
+  if (!fp)
+    return FileCreateFailed;
+  bool ok = true;
+  auto put3 = [&](const v3& v) {
+    const int32_t w[3] = { (int32_t)v.x, (int32_t)v.y, (int32_t)v.z };
+    ok = ok && fwrite(w, sizeof w, 1, fp) == 1;
+  };
+  put3(f.dims);
+  put3(f.brick_dims);
+  put3(n0);
+  size_t k = 0;
+  for (int bz = 0; bz < n0.z; ++bz)
+    for (int by = 0; by < n0.y; ++by)
+      for (int bx = 0; bx < n0.x; ++bx, ++k)
+      {
+        put3(v3(bx, by, bz));
+        put3(dims_of[k]);
+        const size_t cnt = (size_t)prod(dims_of[k]);
+        if (cnt)
+          ok = ok && fwrite(samples.data() + pieces[k].out, 8, cnt, fp) == cnt;
+      }
+  ok = fclose(fp) == 0 && ok;
+  return ok ? NoError : FileWriteFailed;
 }
 
 void dataset_close(dataset_handle* h) { delete h; }

@@ -23,6 +23,8 @@ int dataset_decode(device_ctx* ctx, dataset_handle* ds, const params& p, void* o
 int dataset_decode_batch(device_ctx* ctx, dataset_handle* ds, const params* ps, int n, void* const* outs,
                          const size_t* out_bytes, bool out_on_device, double* kernel_ms);
 // The dequantised coefficients of the whole dataset (decode tolerance of p) into d_coeffs.
+int dataset_decode_brick_map(device_ctx* ctx, dataset_handle* ds, const params& p, const char* path,
+                             double* kernel_ms);
 int dataset_coeffs(device_ctx* ctx, dataset_handle* ds, const params& p, void* d_coeffs, size_t bytes,
                    double* kernel_ms);
 void dataset_close(dataset_handle* ds);

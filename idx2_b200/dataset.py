@@ -141,6 +141,22 @@ class Dataset:
         self.last_kernel_ms = kms.value
         return outs
 
+    def decode_brick_map(self, path: str, downsampling=(0, 0, 0), tolerance: float = 0.0):
+        """The reference's HashMap output mode (idx2App --brick_map): every finest brick at
+        the finest resolution that is significant for it, written to `path` in the reference's
+        bricks-file layout (idx2g_decode_brick_map)."""
+        p = self._req(None, None, downsampling, tolerance)
+        cp = p.to_c()
+        kms = ctypes.c_double(0)
+        L = lib()
+        L.idx2g_decode_brick_map.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_CParams),
+                                             ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+        rc = L.idx2g_decode_brick_map(self._ctx.h, self.h, ctypes.byref(cp), os.fsencode(path), ctypes.byref(kms))
+        if rc:
+            raise Idx2Error(rc, "idx2g_decode_brick_map")
+        self.last_kernel_ms = kms.value
+        return path
+
     @property
     def dtype(self):
         return self._dtype

@@ -146,6 +146,19 @@ IDX2G_API int idx2g_decode_batch(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_
 IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p,
                                    void* d_out, size_t out_bytes, double* kernel_ms);
 
+/* Brick-map decode: replaces the reference's HashMap output mode (idx2App --brick_map,
+   params::out_mode::HashMap; Core/idx2Decode.cpp:446-477, Core/idx2SparseBricks.cpp:69-230).
+   Decodes the whole field at p's downsampling and decode tolerance (p's extent is ignored, as
+   the reference's brick map covers every brick), keeping each significant brick (a decoded
+   block of a subband > 0, or of the coarsest level); every finest brick takes the finest level
+   at which it or an ancestor is significant, and the file at `path` receives the reference's
+   WriteBricks layout: int32 dims[3], brick dims[3], finest brick counts[3], then per finest
+   brick in row-major order int32 brick[3], int32 sample dims[3] and the float64 samples (x
+   fastest) of that level's brick over the finest brick's part of it. Where no brick of a
+   chain is significant the reference fails; here the coarsest brick is written. */
+IDX2G_API int idx2g_decode_brick_map(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p,
+                                     const char* path, double* kernel_ms);
+
 /* Batched encode: n fields (params[i], field[i]) through one device stage, then each is
    packed and written as idx2g_encode writes it (the files are identical). The reference
    encodes one field per call (Core/idx2Encode.cpp:390 Encode); here the bricks of every
