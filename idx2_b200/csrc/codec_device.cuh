@@ -581,6 +581,39 @@ __device__ __forceinline__ int coded_planes(int emax, int etol, int end_bp)
   return low <= 63 ? 64 - low : 0;
 }
 
+// Number of coded planes of a block with BitPlanesPerChunk bpc (Core/idx2Encode.cpp:195-206,
+// Core/idx2Decode.cpp:144-162): planes from 63 down, stopping at the first plane past the
+// tolerance whose key value RealBp + 1024 is a multiple of bpc; the channel key of plane Bp is
+// (Bp + EMax + 1024) / bpc.
+__device__ __forceinline__ int coded_planes(int emax, int etol, int end_bp, int bpc)
+{
+  if (bpc == 1)
+    return coded_planes(emax, etol, end_bp);
+  int np = 0;
+  for (int bp = 63; bp >= 64 - end_bp; --bp)
+  {
+    const int realbp = bp + emax;
+    if (58 > realbp - etol + 1 && ((realbp + 1024) % bpc) == 0)
+      break;
+    ++np;
+  }
+  return np;
+}
+
+// Channel key of plane kk (0 = plane 63) of a block whose top plane has key value top =
+// EMax + 63 + 1024.
+__device__ __forceinline__ int plane_key(int top, int kk, int bpc) { return (top - kk) / bpc; }
+
+// Planes [kk0, kk1] of a block (np coded planes, top as above) that are in channel key; empty
+// when kk0 > kk1. Key values of coded planes are non-negative (checked by the kernels).
+__device__ __forceinline__ void key_planes(int top, int np, int key, int bpc, int& kk0, int& kk1)
+{
+  kk0 = top - key * bpc - (bpc - 1);
+  kk1 = top - key * bpc;
+  kk0 = kk0 < 0 ? 0 : kk0;
+  kk1 = kk1 > np - 1 ? np - 1 : kk1;
+}
+
 // Bit length of one plane of the group-test coder (Core/Zfp.h:771 Encode<u64>) with
 // nin significant coefficients before the plane and plane bits x.
 __device__ __forceinline__ int plane_bits(unsigned long long x, int nin, int nvals)

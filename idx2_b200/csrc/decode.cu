@@ -274,6 +274,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       a.end_bp = r0.f32 ? 32 : 64;
       a.norm_mask = lw->norm_mask;
       a.out_f32 = r0.f32;
+      a.bpc = r0.bpc;
       memcpy(a.nblocks, lw->nblocks, sizeof a.nblocks);
       memcpy(a.inv_weight, lw->inv_weight, sizeof a.inv_weight);
       a.geom = d_geom;
@@ -316,6 +317,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       pa.nsb = r0.nsb;
       pa.nbricks = nbr;
       pa.end_bp = a.end_bp;
+      pa.bpc = r0.bpc;
       pa.reqs = d_reqs;
       memcpy(pa.nblocks, lw->nblocks, sizeof pa.nblocks);
       pa.geom = d_geom;
@@ -500,6 +502,8 @@ int scratch_address(int device, unsigned char** out)
 int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, void* d_out, size_t out_bytes,
                                   double* kernel_ms)
 {
+  if (rq.bpc != 1)
+    return OptionNotSupported;  // the single-kernel wavefront decodes one plane per channel
   // limits of the fixed scratch
   bool seen_output = false;
   for (const decode_level& lv : rq.levels)
@@ -568,6 +572,7 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
     a.end_bp = rq.f32 ? 32 : 64;
     a.norm_mask = lv.norm_mask;
     a.out_f32 = rq.f32;
+    a.bpc = 1;
     memcpy(a.nblocks, lv.nblocks, sizeof a.nblocks);
     memcpy(a.inv_weight, lv.inv_weight, sizeof a.inv_weight);
     a.geom = d_geom;

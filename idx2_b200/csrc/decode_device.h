@@ -54,6 +54,7 @@ struct decode_request
   int nlevels = 1, nsb = 8;
   bool is2d = false, f32 = false;
   int etol = 0;
+  int bpc = 1;  // BitPlanesPerChunk of the dataset
   v3 out_from, out_dims, out_strd;
   std::vector<decode_level> levels;  // coarsest first
 };

@@ -37,6 +37,7 @@ constexpr int kRing = 32;  // steps a decoded plane stays in the per-warp ring (
 struct dec_args
 {
   int level, nlevels, is2d, nsb, nbricks, end_bp, norm_mask, out_f32;
+  int bpc;                            // BitPlanesPerChunk: bit planes per channel key
   int nblocks[8];
   double inv_weight[8];
   const uint64_t* geom;               // [8][kMaxBlocksPerSubband]
@@ -66,6 +67,7 @@ struct dec_args
 // Arguments of the bit-plane kernel (one warp per (brick, subband) unit).
 struct dec1_args
 {
+  int bpc;                          // BitPlanesPerChunk: bit planes per channel key
   int nsb, nbricks, end_bp;
   const decode_target* reqs;
   int nblocks[8];
@@ -103,6 +105,7 @@ struct dec_smem
   int16_t emax[8][kMaxBlocksPerSubband];
   int16_t ktop[8][kMaxBlocksPerSubband];
   uint8_t np[8][kMaxBlocksPerSubband];
+  uint8_t nuse[8][kMaxBlocksPerSubband];  // planes that enter the coefficients (0: block not rebuilt)
   uint8_t nbps[8][kMaxBlocksPerSubband];
   uint8_t nd[8][kMaxBlocksPerSubband];
   uint8_t bypass[8][kMaxBlocksPerSubband];
@@ -396,27 +399,55 @@ __device__ __forceinline__ void plane_wavefront(const dec1_args& a, size_t fs, i
       unsigned long long X = 0;
       n_out[g] = 0;
       stop_out[g] = 0;
-      if (c < nkeys && b >= 0 && b < nb)
+      if (a.bpc == 1)
       {
-        const int top = ktop[b], np = npl[b], key = kmax - c;
-        if (np > 0 && key <= top && key > top - np)
+        if (c < nkeys && b >= 0 && b < nb)
         {
-          int n = key == top ? 0 : nl[g];
-          const int stopped = key == top ? 0 : sl[g];
-          if (stopped || !has[g])
+          const int top = ktop[b], np = npl[b], key = kmax - c;
+          if (np > 0 && key <= top && key > top - np)
           {
-            stop_out[g] = 1;
-            n_out[g] = n;
+            int n = key == top ? 0 : nl[g];
+            const int stopped = key == top ? 0 : sl[g];
+            if (stopped || !has[g])
+            {
+              stop_out[g] = 1;
+              n_out[g] = n;
+            }
+            else
+            {
+              X = decode_plane(rd[g], n, 1 << nvl[b]);
+              n_out[g] = n;
+            }
           }
-          else
+        }
+        if (c < nkeys)
+          T[(size_t)t * (size_t)nkeys + (size_t)c] = X;
+      }
+      else if (c < nkeys)
+      {
+        // several planes per key: the block's planes of this key, top-down, from the same
+        // stream; slot j of the (step, channel) entry holds key value key * bpc + bpc - 1 - j
+        unsigned long long* row = T + ((size_t)t * (size_t)nkeys + (size_t)c) * (size_t)a.bpc;
+        for (int j = 0; j < a.bpc; ++j)
+          row[j] = 0ull;
+        if (b >= 0 && b < nb && npl[b] > 0)
+        {
+          const int top = ktop[b], key = kmax - c;
+          int kk0, kk1;
+          dev::key_planes(top, npl[b], key, a.bpc, kk0, kk1);
+          if (kk0 <= kk1)
           {
-            X = decode_plane(rd[g], n, 1 << nvl[b]);
+            int n = kk0 == 0 ? 0 : nl[g];
+            const int stopped = kk0 == 0 ? 0 : sl[g];
+            if (stopped || !has[g])
+              stop_out[g] = 1;
+            else
+              for (int kk = kk0; kk <= kk1; ++kk)
+                row[key * a.bpc + a.bpc - 1 - (top - kk)] = decode_plane(rd[g], n, 1 << nvl[b]);
             n_out[g] = n;
           }
         }
       }
-      if (c < nkeys)
-        T[(size_t)t * (size_t)nkeys + (size_t)c] = X;
     }
   }
 }
@@ -451,15 +482,18 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_plane
       int d3[3], bd[3];
       unpack_geom(a.geom[(size_t)s * kMaxBlocksPerSubband + b], d3, bd);
       const int emax = a.exps[fs * kMaxBlocksPerSubband + (size_t)b];
-      const int np = dev::coded_planes(emax, rq.etol, a.end_bp);
+      const int np = dev::coded_planes(emax, rq.etol, a.end_bp, a.bpc);
       const int top = emax + 63 + 1024;
       ktop[b] = (int16_t)top;
       npl[b] = (uint8_t)np;
       nvl[b] = (uint8_t)(2 * ((bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1)));
       if (np)
       {
-        kmax = top > kmax ? top : kmax;
-        kmin = top - np + 1 < kmin ? top - np + 1 : kmin;
+        if (top - np + 1 < 0)
+          atomicOr(a.error, 1);  // negative key value: a tolerance below 2^-1070 (unsupported)
+        const int kh = dev::plane_key(top, 0, a.bpc), kl = dev::plane_key(top, np - 1, a.bpc);
+        kmax = kh > kmax ? kh : kmax;
+        kmin = kl < kmin ? kl : kmin;
       }
     }
     for (int o = 16; o > 0; o >>= 1)
@@ -488,7 +522,8 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_plane
         a.wide_list[atomicAdd(a.wide_count, 1)] = unit;
       continue;
     }
-    const unsigned long long bytes = (unsigned long long)(nb + nkeys - 1) * (unsigned long long)nkeys * 8ull;
+    const unsigned long long bytes =
+      (unsigned long long)(nb + nkeys - 1) * (unsigned long long)nkeys * 8ull * (unsigned long long)a.bpc;
     unsigned long long base = 0;
     if (lane == 0)
       base = atomicAdd(a.cursor, bytes);
@@ -599,7 +634,27 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       const int emax = a.exps[fs * kMaxBlocksPerSubband + (size_t)b];
       sm.emax[s][b] = (int16_t)emax;
       sm.ktop[s][b] = (int16_t)(emax + 63 + 1024);
-      sm.np[s][b] = (uint8_t)dev::coded_planes(emax, rq.etol, a.end_bp);
+      const int np = dev::coded_planes(emax, rq.etol, a.end_bp, a.bpc);
+      sm.np[s][b] = (uint8_t)np;
+      // Core/idx2Decode.cpp:161-206: NBps counts the decoded planes within the tolerance; a
+      // block with none is not rebuilt, and when more than 8 planes are decoded
+      // (Exponent(tol) - 6 - EMax + 1 > 8) the planes go through TransposeRecursive
+      // (Core/Zfp.h:1140), which reads plane rows below NBps rounded up to even only. With one
+      // plane per key every decoded plane is within the tolerance.
+      int nuse = np;
+      if (a.bpc > 1)
+      {
+        const int np1 = dev::coded_planes(emax, rq.etol, a.end_bp);
+        const int nbps = np1 < np ? np1 : np;
+        if (nbps == 0)
+          nuse = 0;
+        else if (rq.etol - 6 - emax + 1 > 8)
+        {
+          const int r = (nbps + 1) & ~1;
+          nuse = r < np ? r : np;
+        }
+      }
+      sm.nuse[s][b] = (uint8_t)nuse;
       sm.nbps[s][b] = 0;
       sm.nd[s][b] = (uint8_t)((bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1));
       sm.bypass[s][b] = (uint8_t)((d3[0] % rq.spacing[s][0]) != 0 || (d3[1] % rq.spacing[s][1]) != 0 ||
@@ -615,8 +670,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         {
           if (!sm.np[s][b])
             continue;
-          kmax = sm.ktop[s][b] > kmax ? sm.ktop[s][b] : kmax;
-          int lo = sm.ktop[s][b] - sm.np[s][b] + 1;
+          const int hi = dev::plane_key(sm.ktop[s][b], 0, a.bpc);
+          const int lo = dev::plane_key(sm.ktop[s][b], sm.np[s][b] - 1, a.bpc);
+          kmax = hi > kmax ? hi : kmax;
           kmin = lo < kmin ? lo : kmin;
         }
       int nk = kmax >= kmin ? kmax - kmin + 1 : 0;
@@ -674,14 +730,22 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
           x1 = 0;
           if (b >= nb)
             return;
-          const int np = sm.np[s][b];
+          const int np = sm.nuse[s][b];
           if (!np || sm.bypass[s][b])
             return;
-          const int c0 = kmax - sm.ktop[s][b];
-          if (lane < np && c0 + lane < nkeys)
-            x0 = T[(size_t)(b + c0 + lane) * (size_t)nkeys + (size_t)(c0 + lane)];
-          if (lane + 32 < np && c0 + lane + 32 < nkeys)
-            x1 = T[(size_t)(b + c0 + lane + 32) * (size_t)nkeys + (size_t)(c0 + lane + 32)];
+          const int top = sm.ktop[s][b], bpc = a.bpc;
+          // plane kk: channel c = kmax - key, step b + c, slot key * bpc + bpc - 1 - (top - kk)
+          auto at = [&](int kk) -> unsigned long long {
+            const int key = dev::plane_key(top, kk, bpc), c = kmax - key;
+            if (c >= nkeys)
+              return 0ull;
+            return T[((size_t)(b + c) * (size_t)nkeys + (size_t)c) * (size_t)bpc +
+                     (size_t)(key * bpc + bpc - 1 - (top - kk))];
+          };
+          if (lane < np)
+            x0 = at(lane);
+          if (lane + 32 < np)
+            x1 = at(lane + 32);
         };
         // coefficient bit vectors from plane masks: lane l gets bit l (u0) and bit l + 32 (u1)
         // of every plane, plane k at bit 63 - k
@@ -713,9 +777,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
           }
           const int bA = 2 * pr, bB = 2 * pr + 1;
           const bool hasB = bB < nb;
-          const bool actA = sm.np[s][bA] > 0 && !sm.bypass[s][bA];
-          const bool actB = hasB && sm.np[s][bB] > 0 && !sm.bypass[s][bB];
-          const int npA = sm.np[s][bA], npB = hasB ? sm.np[s][bB] : 0;
+          const bool actA = sm.nuse[s][bA] > 0 && !sm.bypass[s][bA];
+          const bool actB = hasB && sm.nuse[s][bB] > 0 && !sm.bypass[s][bB];
+          const int npA = sm.nuse[s][bA], npB = hasB ? sm.nuse[s][bB] : 0;
           // Core/idx2Decode.cpp:209-211: a decoded block of a subband > 0, or of the coarsest
           // level, makes the brick significant
           if (lane == 0 && (actA || actB) && (s > 0 || a.level + 1 == a.nlevels))

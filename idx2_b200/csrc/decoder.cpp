@@ -584,6 +584,9 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
   rq.is2d = f.is2d();
   rq.f32 = f.type == dtype::float32;
   rq.etol = exponent_f64(tol);
+  rq.bpc = f.bit_planes_per_chunk;
+  if (rq.bpc < 1 || rq.bpc > 8)
+    return OptionNotSupported;  // keys of coded planes stay non-negative up to 8 planes per key
   rq.out_from = og.from;
   rq.out_dims = og.dims;
   rq.out_strd = og.strd;

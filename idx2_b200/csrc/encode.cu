@@ -91,6 +91,7 @@ struct enc_field
   const int* nblocks;        // [nsb]
   double weight[8];
   int norm_mask;
+  int bpc;                   // BitPlanesPerChunk: bit planes per channel key
 };
 
 constexpr int kNB3 = 33 * 33 * 33;  // brick stride of slots and parent arrays (2D bricks use 33^2)
@@ -611,8 +612,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         if (lane + 32 < nvB)
           uB1 = ((unsigned long long)qB[qpad(permj(ndB, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
         __syncwarp();
-        const int npA = dev::coded_planes(eA, fp.etol, fp.end_bp);
-        const int npB = hasB ? dev::coded_planes(eB, fp.etol, fp.end_bp) : 0;
+        const int npA = dev::coded_planes(eA, fp.etol, fp.end_bp, fp.bpc);
+        const int npB = hasB ? dev::coded_planes(eB, fp.etol, fp.end_bp, fp.bpc) : 0;
         const int npM = npA > npB ? npA : npB;
         unsigned long long* XA = Xp + bA;  // plane k at XA[k * kRowX]
         unsigned long long* XB = Xp + bB;
@@ -703,8 +704,11 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
           if (!n)
             continue;
           const int t = sm.ktop[b];
-          lo = t - n + 1 < lo ? t - n + 1 : lo;
-          hi = t > hi ? t : hi;
+          if (t - n + 1 < 0)
+            atomicExch(a.error, 1);  // negative key value: a tolerance below 2^-1070 (unsupported)
+          const int kl = dev::plane_key(t, n - 1, fp.bpc), kh = dev::plane_key(t, 0, fp.bpc);
+          lo = kl < lo ? kl : lo;
+          hi = kh > hi ? kh : hi;
         }
         for (int o = 16; o > 0; o >>= 1)
         {
@@ -731,8 +735,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       const int nkeys = sm.ok ? kmax - kmin + 1 : 0;
       ENC_PHASE(11)
 
-      // D3: per channel key (a warp each), bit offsets of the blocks in Morton order: an
-      // exclusive scan of the plane lengths, in place
+      // D3: per channel key (a warp each), bit offsets in the channel's stream: blocks in
+      // Morton order, within a block its planes of the key top-down (one plane per key when
+      // BitPlanesPerChunk is 1); an exclusive scan of the plane lengths, in place
       for (int t = warp; t < nkeys; t += kWarps)
       {
         const int key = kmin + t;
@@ -740,9 +745,12 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         for (int b0 = 0; b0 < nb; b0 += 32)
         {
           const int b = b0 + lane;
-          int kk = b < nb ? sm.ktop[b] - key : -1;
-          kk = (kk >= 0 && b < nb && kk < sm.np[b]) ? kk : -1;
-          const uint32_t v = kk >= 0 ? OFF[kk * kRowOff + b] : 0u;
+          int kk0 = 1, kk1 = 0;
+          if (b < nb && sm.np[b])
+            dev::key_planes(sm.ktop[b], sm.np[b], key, fp.bpc, kk0, kk1);
+          uint32_t v = 0;
+          for (int kk = kk0; kk <= kk1; ++kk)
+            v += OFF[kk * kRowOff + b];
           uint32_t inc = v;
           for (int o = 1; o < 32; o <<= 1)
           {
@@ -750,12 +758,21 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
             if (lane >= o)
               inc += y;
           }
-          if (kk >= 0)
-            OFF[kk * kRowOff + b] = (uint16_t)(carry + inc - v);
+          uint32_t run = carry + inc - v;
+          for (int kk = kk0; kk <= kk1; ++kk)
+          {
+            const uint32_t len = OFF[kk * kRowOff + b];
+            OFF[kk * kRowOff + b] = (uint16_t)run;
+            run += len;
+          }
           carry += __shfl_sync(0xffffffffu, inc, 31);
         }
         if (lane == 0)
+        {
           sm.key_bits[t] = carry;
+          if (carry > 65535u)
+            atomicExch(a.error, 1);  // offsets are 16-bit: a key stream of more than 65535 bits
+        }
       }
       __syncthreads();
       ENC_PHASE(12)
@@ -836,7 +853,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
           const int b = idx & (kMaxBlocksPerSubband - 1), kk = idx / kMaxBlocksPerSubband;
           if (b >= nb || kk >= sm.np[b])
             continue;
-          const int t = sm.ktop[b] - kk - kmin;
+          const int t = dev::plane_key(sm.ktop[b], kk, fp.bpc) - kmin;
           const unsigned long long pos = ((unsigned long long)hdr + sm.key_base[t]) * 8ull +
                                          (unsigned long long)OFF[kk * kRowOff + b];
           dev::bits192 c;
@@ -907,8 +924,8 @@ int batch_encoder::prepare(const batch_tuning& t)
   for (batch_field& j : J)
   {
     const dataset_format& f = *j.f;
-    if (f.bit_planes_per_chunk != 1)
-      return OptionNotSupported;
+    if (f.bit_planes_per_chunk < 1 || f.bit_planes_per_chunk > 8)
+      return OptionNotSupported;  // keys of coded planes stay non-negative up to 8 planes per key
     if (f.brick_dims.x != 32 || f.brick_dims.y != 32 || (f.brick_dims.z != 32 && f.brick_dims.z != 1))
       return OptionNotSupported;
     L = f.nlevels > L ? f.nlevels : L;
@@ -957,6 +974,7 @@ int batch_encoder::prepare(const batch_tuning& t)
       ef.fdims[1] = f.dims.y;
       ef.fdims[2] = f.dims.z;
       level_weights(f, l, ef.weight, &ef.norm_mask);
+      ef.bpc = f.bit_planes_per_chunk;
       if (ef.end_bp == 64)
         ll.planes = 64;
       ll.fields.push_back(ef);
