@@ -602,14 +602,17 @@ __device__ __forceinline__ int coded_planes(int emax, int etol, int end_bp, int 
 
 // Channel key of plane kk (0 = plane 63) of a block whose top plane has key value top =
 // EMax + 63 + 1024.
-__device__ __forceinline__ int plane_key(int top, int kk, int bpc) { return (top - kk) / bpc; }
+__device__ __forceinline__ int plane_key(int top, int kk, int bpc)
+{
+  return bpc == 1 ? top - kk : (top - kk) / bpc;  // (the common case without a division)
+}
 
 // Planes [kk0, kk1] of a block (np coded planes, top as above) that are in channel key; empty
 // when kk0 > kk1. Key values of coded planes are non-negative (checked by the kernels).
 __device__ __forceinline__ void key_planes(int top, int np, int key, int bpc, int& kk0, int& kk1)
 {
-  kk0 = top - key * bpc - (bpc - 1);
   kk1 = top - key * bpc;
+  kk0 = kk1 - (bpc - 1);
   kk0 = kk0 < 0 ? 0 : kk0;
   kk1 = kk1 > np - 1 ? np - 1 : kk1;
 }

@@ -345,8 +345,16 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         return CudaError;
       ++nev;
       cudaEventRecord(t0, st);
-      k_decode_planes<false><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
-      k_decode_planes<true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(pa);
+      if (r0.bpc == 1)
+      {
+        k_decode_planes<false><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
+        k_decode_planes<true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(pa);
+      }
+      else
+      {
+        k_decode_planes<false, true><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
+        k_decode_planes<true, true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(pa);
+      }
       k_decode_level<<<grid, kThreads, smem, st>>>(a);
       cudaEventRecord(t1, st);
       ctx->launches += 3;

@@ -345,7 +345,7 @@ struct plane_smem
   uint8_t nvl[kPlaneWarps][kMaxBlocksPerSubband];
 };
 
-template <int G>
+template <int G, bool MULTI>
 __device__ __forceinline__ void plane_wavefront(const dec1_args& a, size_t fs, int nb, int nkeys, int kmax,
                                                 const int16_t* ktop, const uint8_t* npl, const uint8_t* nvl,
                                                 unsigned long long* T, int lane)
@@ -399,7 +399,7 @@ __device__ __forceinline__ void plane_wavefront(const dec1_args& a, size_t fs, i
       unsigned long long X = 0;
       n_out[g] = 0;
       stop_out[g] = 0;
-      if (a.bpc == 1)
+      if constexpr (!MULTI)
       {
         if (c < nkeys && b >= 0 && b < nb)
         {
@@ -454,7 +454,7 @@ __device__ __forceinline__ void plane_wavefront(const dec1_args& a, size_t fs, i
 
 // WIDE = false: every unit, those of up to 32 channels decoded at once (few registers, many
 // warps per SM), the others listed; WIDE = true: the listed units (up to kKeyWindow channels).
-template <bool WIDE>
+template <bool WIDE, bool MULTI = false>
 __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_planes(const dec1_args a)
 {
   __shared__ plane_smem sm;
@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_plane
     }
     __syncwarp();
     int nkeys = kmax >= kmin ? kmax - kmin + 1 : 0;
-    if (nkeys > kKeyWindow)
+    if (nkeys > (MULTI ? 64 : kKeyWindow))
     {
       if (lane == 0)
         atomicOr(a.error, 1);
@@ -540,16 +540,24 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_plane
     if (lane == 0)
       a.unit_off[unit] = base;
     unsigned long long* T = a.planes + base / 8;
-    if (!WIDE)
-      plane_wavefront<1>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+    if constexpr (MULTI)
+    {
+      // several planes per key: units of up to 32 keys here, up to 64 in the second pass
+      if (!WIDE)
+        plane_wavefront<1, true>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+      else
+        plane_wavefront<2, true>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+    }
+    else if (!WIDE)
+      plane_wavefront<1, false>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
     else if (nkeys <= 32)
-      plane_wavefront<1>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+      plane_wavefront<1, false>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
     else if (nkeys <= 64)
-      plane_wavefront<2>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+      plane_wavefront<2, false>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
     else if (nkeys <= 96)
-      plane_wavefront<3>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+      plane_wavefront<3, false>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
     else
-      plane_wavefront<4>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
+      plane_wavefront<4, false>(a, fs, nb, nkeys, kmax, ktop, npl, nvl, T, lane);
     __syncwarp();
   }
 }
@@ -734,6 +742,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
           if (!np || sm.bypass[s][b])
             return;
           const int top = sm.ktop[s][b], bpc = a.bpc;
+          if (bpc == 1)
+          {
+            // plane kk in channel c0 + kk, table row b + c0 + kk
+            const int c0 = kmax - top;
+            if (lane < np && c0 + lane < nkeys)
+              x0 = T[(size_t)(b + c0 + lane) * (size_t)nkeys + (size_t)(c0 + lane)];
+            if (lane + 32 < np && c0 + lane + 32 < nkeys)
+              x1 = T[(size_t)(b + c0 + lane + 32) * (size_t)nkeys + (size_t)(c0 + lane + 32)];
+            return;
+          }
           // plane kk: channel c = kmax - key, step b + c, slot key * bpc + bpc - 1 - (top - kk)
           auto at = [&](int kk) -> unsigned long long {
             const int key = dev::plane_key(top, kk, bpc), c = kmax - key;
@@ -782,7 +800,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
           const int npA = sm.nuse[s][bA], npB = hasB ? sm.nuse[s][bB] : 0;
           // Core/idx2Decode.cpp:209-211: a decoded block of a subband > 0, or of the coarsest
           // level, makes the brick significant
-          if (lane == 0 && (actA || actB) && (s > 0 || a.level + 1 == a.nlevels))
+          if (a.sig && lane == 0 && (actA || actB) && (s > 0 || a.level + 1 == a.nlevels))
             sm.sig = 1;
           unsigned long long uA0, uA1, uB0, uB1;
           transpose(cA0, cA1, npA > 32, uA0, uA1);

@@ -293,42 +293,65 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
       const long long gx0 = (long long)br.b3[0] * 32, gy0 = (long long)br.b3[1] * 32,
                       gz0 = (long long)br.b3[2] * (fp.is2d ? 1 : 32);
-      // rows (y, z) of the brick, one warp per row, lanes along x; samples outside the
-      // valid region (and the x = 32 column) are zero
-      const int nrows = 33 * N[2];
-      constexpr int U = 4;
-      for (int r0 = warp * U; r0 < nrows; r0 += kWarps * U)
-      {
-        float fv[U];
-        double dv[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u)
+      // The brick's samples come through shared memory in chunks of kGz z-planes,
+      // double-buffered in the coding tables' space (idle here): asynchronous copies of chunk
+      // c + 1 are in flight while chunk c is widened into the brick; samples outside the
+      // valid region (and the x = 32, y = 32, z = 32 faces) are zero.
+      constexpr int kGz = 4;
+      const int esz = fp.field_f32 ? 4 : 8;
+      unsigned char* const stage = reinterpret_cast<unsigned char*>(Xp);
+      const unsigned stage_bytes = (unsigned)(kGz * 32 * 32 * esz);
+      const int nch = (N[2] + kGz - 1) / kGz;
+      auto issue = [&](int c) {
+        const int z0 = c * kGz;
+        const int nz = vz - z0 < kGz ? vz - z0 : kGz;
+        const unsigned s0 = (unsigned)__cvta_generic_to_shared(stage) + (unsigned)(c & 1) * stage_bytes;
+        for (int i = tid; i < nz * vy * 32; i += kThreads)
         {
-          const int r = r0 + u, y = r % 33, z = r / 33;
-          const bool in = r < nrows && y < vy && z < vz && lane < vx;
-          const long long src = ((gz0 + z) * fp.fdims[1] + gy0 + y) * fp.fdims[0] + gx0 + lane;
+          const int x = i & 31, row = i >> 5, y = row % vy, zz = row / vy;
+          if (x >= vx)
+            continue;
+          const long long src = ((gz0 + z0 + zz) * fp.fdims[1] + gy0 + y) * fp.fdims[0] + gx0 + x;
+          const unsigned d = s0 + (unsigned)(((zz * 32 + y) * 32 + x) * esz);
           if (fp.field_f32)
-            fv[u] = in ? __ldcs((const float*)fp.field + src) : 0.0f;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"((const float*)fp.field + src)
+                         : "memory");
           else
-            dv[u] = in ? __ldcs((const double*)fp.field + src) : 0.0;
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"((const double*)fp.field + src)
+                         : "memory");
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u)
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+      };
+      issue(0);
+      for (int c = 0; c < nch; ++c)
+      {
+        if (c + 1 < nch)
         {
-          const int r = r0 + u, y = r % 33, z = r / 33;
-          if (r >= nrows)
-            break;
-          const bool in = y < vy && z < vz && lane < vx;
-          const double v = fp.field_f32 ? (double)fv[u] : dv[u];
-          F[r * 33 + lane] = v;
-          if (lane == 0)
-            F[r * 33 + 32] = 0.0;
+          issue(c + 1);
+          asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        }
+        else
+          asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();
+        const unsigned char* buf = stage + (size_t)(c & 1) * stage_bytes;
+        const int z0 = c * kGz;
+        const int nz = N[2] - z0 < kGz ? N[2] - z0 : kGz;
+        for (int i = tid; i < nz * 33 * 33; i += kThreads)
+        {
+          const int x = i % 33, row = i / 33, y = row % 33, zz = row / 33, z = z0 + zz;
+          const bool in = x < vx && y < vy && z < vz;
+          double v = 0.0;
+          if (in)
+            v = fp.field_f32 ? (double)reinterpret_cast<const float*>(buf)[(zz * 32 + y) * 32 + x]
+                             : reinterpret_cast<const double*>(buf)[(zz * 32 + y) * 32 + x];
+          F[(z * 33 + y) * 33 + x] = v;
           if (in)
           {
             mn = v < mn ? v : mn;
             mx = mx < v ? v : mx;
           }
         }
+        __syncthreads();  // the buffer is refilled by the next chunk but one
       }
       for (int o = 16; o > 0; o >>= 1)
       {
@@ -738,7 +761,32 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       // D3: per channel key (a warp each), bit offsets in the channel's stream: blocks in
       // Morton order, within a block its planes of the key top-down (one plane per key when
       // BitPlanesPerChunk is 1); an exclusive scan of the plane lengths, in place
-      for (int t = warp; t < nkeys; t += kWarps)
+      for (int t = warp; t < nkeys && fp.bpc == 1; t += kWarps)
+      {
+        // one plane per key: plane ktop - key of each block
+        const int key = kmin + t;
+        uint32_t carry = 0;
+        for (int b0 = 0; b0 < nb; b0 += 32)
+        {
+          const int b = b0 + lane;
+          int kk = b < nb ? sm.ktop[b] - key : -1;
+          kk = (kk >= 0 && b < nb && kk < sm.np[b]) ? kk : -1;
+          const uint32_t v = kk >= 0 ? OFF[kk * kRowOff + b] : 0u;
+          uint32_t inc = v;
+          for (int o = 1; o < 32; o <<= 1)
+          {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o)
+              inc += y;
+          }
+          if (kk >= 0)
+            OFF[kk * kRowOff + b] = (uint16_t)(carry + inc - v);
+          carry += __shfl_sync(0xffffffffu, inc, 31);
+        }
+        if (lane == 0)
+          sm.key_bits[t] = carry;
+      }
+      for (int t = warp; t < nkeys && fp.bpc > 1; t += kWarps)
       {
         const int key = kmin + t;
         uint32_t carry = 0;
