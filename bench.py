@@ -162,6 +162,40 @@ def cpu_baseline(side, steps=1, warmup=0):
                       f"tol {TOL}) + sequential --decode, median of {len(times)}, {t:.2f} s per pass"}
 
 
+def run_reference_parallel(sample, tmp, procs, steps, warmup):
+    """The reference CLI on every host core: per step, `procs` independent pipelines (encode of
+    the sample + sequential decode, each in its own directory) run at once; the reference
+    encoder is single-threaded, so one pipeline per core is how it uses the host. Returns the
+    wall time of each timed step."""
+    app = os.path.join(ROOT, "oracle", "_ref", "idx2App")
+    nz, ny, nx = sample.shape
+    raw = os.path.join(tmp, f"grf-f-[{nx}-{ny}-{nz}]-Float32.raw")
+    sample.tofile(raw)
+    times = []
+    for i in range(warmup + steps):
+        cmds = []
+        for k in range(procs):
+            out = os.path.join(tmp, f"refds{k}")
+            shutil.rmtree(out, ignore_errors=True)
+            os.makedirs(out)
+            enc = [app, "--encode", raw, "--num_levels", str(LEVELS), "--tolerance", str(TOL), "--out_dir", out]
+            dec = [app, "--decode", os.path.join(out, "grf", "f.idx2"), "--out_dir", out, "--out_file", "dec.raw"]
+            cmds.append((enc, dec))
+        t0 = time.perf_counter()
+        running = [subprocess.Popen(enc, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE) for enc, _ in cmds]
+        for pr in running:
+            if pr.wait():
+                raise RuntimeError("reference encode failed: " + pr.stderr.read().decode()[-300:])
+        running = [subprocess.Popen(dec, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE) for _, dec in cmds]
+        for pr in running:
+            if pr.wait():
+                raise RuntimeError("reference decode failed: " + pr.stderr.read().decode()[-300:])
+        t1 = time.perf_counter()
+        if i >= warmup:
+            times.append(t1 - t0)
+    return times
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
@@ -170,21 +204,23 @@ def reference_arm(args, rank, world):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference built from "
                           "its sources) is not present on this machine"}))
         return
+    procs = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
     sample = reference_sample(args.side)
     with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as tmp:
-        times = run_reference_cli(sample, tmp, args.steps, args.warmup)
+        times = run_reference_parallel(sample, tmp, procs, args.steps, args.warmup)
     t = sum(times) / len(times)
     nz, ny, nx = sample.shape
-    v = 2 * sample.nbytes / t / 1e9
-    desc = (f"{nx}x{ny}x{nz} float32 region of the {args.side}^3 field per step; idx2App --encode + "
-            f"sequential --decode (the reference encode is single-threaded)")
+    v = procs * 2 * sample.nbytes / t / 1e9
+    desc = (f"{procs} concurrent pipelines (one per host core), each idx2App --encode + sequential --decode "
+            f"of a {nx}x{ny}x{nz} float32 region of the {args.side}^3 field per step (the reference encode is "
+            f"single-threaded); value = all pipelines' raw bytes / wall time")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"grf{args.side}: {args.side}^3 float32 k^-5/3 GRF + 20 fronts, "
                        f"{LEVELS} levels, 32^3 bricks, tol {TOL}; encode + full-res decode",
                        "parallelism": f"dp{world}"},
-            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": 1, "kind": "reference", "sample": desc},
+            "cpu_baseline": {"value": v, "unit": "GB/s", "cores": procs, "kind": "reference", "sample": desc},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
