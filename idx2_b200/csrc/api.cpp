@@ -207,7 +207,10 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
   std::vector<long long> lbytes;
   {
     gpu_coder coder(&c->d, f, d_field, f32);
-    e = encode_dataset(&f, &p, &coder, nullptr, true, &tm);
+    const encode_plan* plan = c->d.plan_for(f, &e);
+    if (!plan)
+      return e;
+    e = encode_dataset(&f, &p, &coder, nullptr, true, &tm, plan);
     stream_bytes = coder.stream_bytes();
     exp_bytes = coder.exp_bytes();
     kms = coder.kernel_ms();
@@ -259,7 +262,10 @@ IDX2G_API int idx2g_encode_device(idx2g_ctx* c, const idx2g_params* in, const vo
   coder.set_keep_device(true);
   std::vector<level_output> outs;
   auto t0 = std::chrono::steady_clock::now();
-  e = encode_levels(&f, &coder, &outs);
+  const encode_plan* plan = c->d.plan_for(f, &e);
+  if (!plan)
+    return e;
+  e = encode_levels(&f, &coder, &outs, *plan);
   auto t1 = std::chrono::steady_clock::now();
   if (e)
     return e;
@@ -295,7 +301,7 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<params> ps((size_t)n);
   std::vector<dataset_format> fs((size_t)n);
-  std::vector<encode_plan> plans((size_t)n);
+  std::vector<const encode_plan*> plans((size_t)n);
   std::vector<std::vector<level_output>> outs((size_t)n);
   size_t host_bytes = 0;
   long long total_bricks = 0;
@@ -308,12 +314,12 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
     int e = finalize(&fs[(size_t)i], &ps[(size_t)i]);
     if (e)
       return e;
-    e = make_encode_plan(fs[(size_t)i], &plans[(size_t)i]);
-    if (e)
+    plans[(size_t)i] = c->d.plan_for(fs[(size_t)i], &e);
+    if (!plans[(size_t)i])
       return e;
     host_bytes += (((size_t)prod(ps[(size_t)i].dims) * (ps[(size_t)i].type == dtype::float32 ? 4 : 8)) + 255) &
                   ~(size_t)255;
-    total_bricks += (long long)plans[(size_t)i].levels[0].size();
+    total_bricks += (long long)plans[(size_t)i]->levels[0].size();
     nf64 += ps[(size_t)i].type == dtype::float64;
   }
   // fields to the device (one staging buffer of the context's workspace)
@@ -339,7 +345,7 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
   for (int i = 0; i < n; ++i)
   {
     bf[(size_t)i].f = &fs[(size_t)i];
-    bf[(size_t)i].plan = &plans[(size_t)i];
+    bf[(size_t)i].plan = plans[(size_t)i];
     bf[(size_t)i].d_field = dptr[(size_t)i];
     bf[(size_t)i].f32 = ps[(size_t)i].type == dtype::float32;
     bf[(size_t)i].outs = &outs[(size_t)i];
@@ -405,7 +411,7 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
     auto work = [&]() {
       for (int i; (i = next.fetch_add(1)) < n;)
       {
-        const int r = pack_dataset(&fs[(size_t)i], &ps[(size_t)i], plans[(size_t)i], outs[(size_t)i], nullptr,
+        const int r = pack_dataset(&fs[(size_t)i], &ps[(size_t)i], *plans[(size_t)i], outs[(size_t)i], nullptr,
                                    true, &tm[(size_t)i]);
         if (r)
           err = r;

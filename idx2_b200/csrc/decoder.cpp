@@ -20,6 +20,7 @@
 #include <atomic>
 #include <fcntl.h>
 #include <map>
+#include <memory>
 #include <sys/stat.h>
 #include <thread>
 #include <unistd.h>
@@ -155,6 +156,15 @@ struct dataset_handle
   size_t blob_bytes = 0;
   // device copies
   decode_device dev;
+  // plans of the last few single-request decodes, by request (a request repeated on the
+  // dataset, such as every time step's full read, plans once)
+  struct cached_plan
+  {
+    std::string key;
+    decode_request rq;
+    size_t need = 0;
+  };
+  std::vector<std::unique_ptr<cached_plan>> plans;
 };
 
 namespace
@@ -552,17 +562,44 @@ int dataset_output_grid(const dataset_handle* h, const params& p, grid* g)
   return NoError;
 }
 
+// The plan of a request from the dataset's cache (planned and kept on a miss).
+static int cached_plan_decode(dataset_handle* h, const params& p, const decode_request** rq, size_t* need)
+{
+  char key[256];
+  snprintf(key, sizeof key, "%d|%d %d %d|%d %d %d|%d %d %d|%.17g", p.has_extent ? 1 : 0, p.decode_extent.from.x,
+           p.decode_extent.from.y, p.decode_extent.from.z, p.decode_extent.dims.x, p.decode_extent.dims.y,
+           p.decode_extent.dims.z, p.downsampling.x, p.downsampling.y, p.downsampling.z, p.decode_tolerance);
+  for (auto& c : h->plans)
+    if (c->key == key)
+    {
+      *rq = &c->rq;
+      *need = c->need;
+      return NoError;
+    }
+  std::unique_ptr<dataset_handle::cached_plan> c(new dataset_handle::cached_plan());
+  c->key = key;
+  int e = plan_decode(h, p, &c->rq, &c->need);
+  if (e)
+    return e;
+  if (h->plans.size() >= 4)
+    h->plans.erase(h->plans.begin());
+  h->plans.push_back(std::move(c));
+  *rq = &h->plans.back()->rq;
+  *need = h->plans.back()->need;
+  return NoError;
+}
+
 int dataset_decode(device_ctx* ctx, dataset_handle* h, const params& p, void* out, size_t out_bytes,
                    bool out_on_device, double* kernel_ms)
 {
-  decode_request rq;
+  const decode_request* rq = nullptr;
   size_t need = 0;
-  int e = plan_decode(h, p, &rq, &need);
+  int e = cached_plan_decode(h, p, &rq, &need);
   if (e)
     return e;
   if (out_bytes < need)
     return SizeTooSmall;
-  return h->dev.decode(ctx, rq, out, need, out_on_device, kernel_ms);
+  return h->dev.decode(ctx, *rq, out, need, out_on_device, kernel_ms);
 }
 
 int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out, size_t* need_out)

@@ -4,6 +4,7 @@
 #include "encoder.h"
 
 #include <cuda_runtime.h>
+#include <cstdio>
 #include <map>
 #include <memory>
 #include <string>
@@ -25,6 +26,27 @@ struct device_ctx
   std::vector<cudaEvent_t> evpool;  // timing events of calls that time several launches
   long long launches = 0;  // kernels launched on this context so far
   std::map<std::string, int> tuned;  // batched encode: CTAs per SM chosen per batch signature
+  // Encode plans by format: the brick order and the EncodeSubband events depend only on the
+  // dims, the brick dims and the number of levels, so repeated encodes of fields of one shape
+  // (the time steps of a simulation) plan once.
+  std::map<std::string, std::shared_ptr<const encode_plan>> plans;
+  const encode_plan* plan_for(const dataset_format& f, int* err)
+  {
+    char key[128];
+    snprintf(key, sizeof key, "%d %d %d/%d %d %d/%d", f.dims.x, f.dims.y, f.dims.z, f.brick_dims.x, f.brick_dims.y,
+             f.brick_dims.z, f.nlevels);
+    auto it = plans.find(key);
+    if (it != plans.end())
+      return it->second.get();
+    std::shared_ptr<encode_plan> pl = std::make_shared<encode_plan>();
+    *err = make_encode_plan(f, pl.get());
+    if (*err)
+      return nullptr;
+    if (plans.size() >= 16)
+      plans.erase(plans.begin());
+    plans[key] = pl;
+    return pl.get();
+  }
 
   struct buf
   {

@@ -167,14 +167,9 @@ static double now_s()
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_output>* outs,
-                  encode_plan* plan_out)
+int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_output>* outs, const encode_plan& plan)
 {
-  encode_plan local;
-  encode_plan& plan = plan_out ? *plan_out : local;
-  int e = make_encode_plan(*f, &plan);
-  if (e)
-    return e;
+  int e = NoError;
   outs->assign((size_t)f->nlevels, level_output());
   for (int l = 0; l < f->nlevels; ++l)
   {
@@ -188,16 +183,23 @@ int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_outpu
 
 int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
                    std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
-                   encode_timing* timing)
+                   encode_timing* timing, const encode_plan* plan)
 {
-  encode_plan plan;
   double t0 = now_s();
+  encode_plan local;
+  if (!plan)
+  {
+    int e = make_encode_plan(*f, &local);
+    if (e)
+      return e;
+    plan = &local;
+  }
   std::vector<level_output> outs;
-  int e = encode_levels(f, coder, &outs, &plan);
+  int e = encode_levels(f, coder, &outs, *plan);
   if (e)
     return e;
   double t1 = now_s();
-  e = pack_dataset(f, p, plan, outs, files, write_files, timing);
+  e = pack_dataset(f, p, *plan, outs, files, write_files, timing);
   if (timing)
     timing->device_s = t1 - t0;
   return e;

@@ -121,18 +121,18 @@ struct encode_timing
 // Full encode: plan, device stage for every level, packing, files (Core/idx2Encode.cpp:390).
 // files (may be null) receives path -> bytes; write_files controls whether they are
 // written to disk (several files at a time).
+// plan (may be null): the format's encode plan, made here when null.
 int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
                    std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
-                   encode_timing* timing);
+                   encode_timing* timing, const encode_plan* plan = nullptr);
 
 // Packing and files for the device stage's outputs (the second half of encode_dataset).
 int pack_dataset(const dataset_format* f, const params* p, const encode_plan& plan,
                  const std::vector<level_output>& outs, std::map<std::string, std::vector<uint8_t>>* files,
                  bool write_files, encode_timing* timing);
 
-// The device stage only: plan + every level through the coder.
-int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_output>* outs,
-                  encode_plan* plan_out = nullptr);
+// The device stage only: every level through the coder, with the given plan.
+int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_output>* outs, const encode_plan& plan);
 
 int write_file(const std::string& path, const std::vector<uint8_t>& data);
 int make_dirs_for(const std::string& path);
