@@ -347,7 +347,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       cudaEventRecord(t0, st);
       if (r0.bpc == 1)
       {
-        k_decode_planes<false><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
+        k_decode_planes<false><<<(pgrid + 1) / 2, kPlaneWarps * 32, 0, st>>>(pa);  // two units per warp
         k_decode_planes<true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(pa);
       }
       else

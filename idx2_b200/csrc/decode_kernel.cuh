@@ -340,9 +340,9 @@ constexpr int kPlaneWarps = 8;
 
 struct plane_smem
 {
-  int16_t ktop[kPlaneWarps][kMaxBlocksPerSubband];
-  uint8_t np[kPlaneWarps][kMaxBlocksPerSubband];
-  uint8_t nvl[kPlaneWarps][kMaxBlocksPerSubband];
+  int16_t ktop[kPlaneWarps][2][kMaxBlocksPerSubband];  // [warp][unit of the warp][block]
+  uint8_t np[kPlaneWarps][2][kMaxBlocksPerSubband];
+  uint8_t nvl[kPlaneWarps][2][kMaxBlocksPerSubband];
 };
 
 template <int G, bool MULTI>
@@ -454,92 +454,226 @@ __device__ __forceinline__ void plane_wavefront(const dec1_args& a, size_t fs, i
 
 // WIDE = false: every unit, those of up to 32 channels decoded at once (few registers, many
 // warps per SM), the others listed; WIDE = true: the listed units (up to kKeyWindow channels).
+// A (brick, subband) unit of the plane kernel after its preparation: block tables filled,
+// channel window known, table allocated. run = 0: nothing to decode here (skipped, empty,
+// deferred to the second pass, or no room).
+struct plane_unit
+{
+  int run, nb, nkeys, kmax;
+  size_t fs;
+  unsigned long long* T;
+};
+
+template <bool WIDE, bool MULTI>
+__device__ __forceinline__ plane_unit prep_unit(const dec1_args& a, int unit, int16_t* ktop, uint8_t* npl,
+                                                uint8_t* nvl, int lane)
+{
+  plane_unit u;
+  u.run = 0;
+  u.nb = u.nkeys = u.kmax = 0;
+  u.fs = 0;
+  u.T = nullptr;
+  const int bi = unit / a.nsb, s = unit - bi * a.nsb;
+  const decode_target& rq = a.reqs[a.bricks[bi].req];
+  if (!((rq.mask >> s) & 1))
+  {
+    if (lane == 0)
+      a.unit_off[unit] = ~0ull;
+    return u;
+  }
+  const int nb = a.nblocks[s];
+  const size_t fs = (size_t)a.bricks[bi].flat * (size_t)a.nsb + (size_t)s;
+  int kmin = 1 << 30, kmax = -(1 << 30);
+  for (int b = lane; b < nb; b += 32)
+  {
+    int d3[3], bd[3];
+    unpack_geom(a.geom[(size_t)s * kMaxBlocksPerSubband + b], d3, bd);
+    const int emax = a.exps[fs * kMaxBlocksPerSubband + (size_t)b];
+    const int np = dev::coded_planes(emax, rq.etol, a.end_bp, a.bpc);
+    const int top = emax + 63 + 1024;
+    ktop[b] = (int16_t)top;
+    npl[b] = (uint8_t)np;
+    nvl[b] = (uint8_t)(2 * ((bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1)));
+    if (np)
+    {
+      if (top - np + 1 < 0)
+        atomicOr(a.error, 1);  // negative key value: a tolerance below 2^-1070 (unsupported)
+      const int kh = dev::plane_key(top, 0, a.bpc), kl = dev::plane_key(top, np - 1, a.bpc);
+      kmax = kh > kmax ? kh : kmax;
+      kmin = kl < kmin ? kl : kmin;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+  {
+    const int x = __shfl_xor_sync(0xffffffffu, kmax, o), y = __shfl_xor_sync(0xffffffffu, kmin, o);
+    kmax = x > kmax ? x : kmax;
+    kmin = y < kmin ? y : kmin;
+  }
+  __syncwarp();
+  int nkeys = kmax >= kmin ? kmax - kmin + 1 : 0;
+  if (nkeys > (MULTI ? 64 : kKeyWindow))
+  {
+    if (lane == 0)
+      atomicOr(a.error, 1);
+    nkeys = 0;
+  }
+  if (nkeys == 0)
+  {
+    if (lane == 0)
+      a.unit_off[unit] = ~0ull;
+    return u;
+  }
+  if (!WIDE && nkeys > 32)
+  {
+    if (lane == 0)
+      a.wide_list[atomicAdd(a.wide_count, 1)] = unit;
+    return u;
+  }
+  const unsigned long long bytes =
+    (unsigned long long)(nb + nkeys - 1) * (unsigned long long)nkeys * 8ull * (unsigned long long)a.bpc;
+  unsigned long long base = 0;
+  if (lane == 0)
+    base = atomicAdd(a.cursor, bytes);
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (base + bytes > a.cap_bytes)
+  {
+    if (lane == 0)
+    {
+      atomicOr(a.error, 2);
+      a.unit_off[unit] = ~0ull;
+    }
+    return u;
+  }
+  if (lane == 0)
+    a.unit_off[unit] = base;
+  u.run = 1;
+  u.nb = nb;
+  u.nkeys = nkeys;
+  u.kmax = kmax;
+  u.fs = fs;
+  u.T = a.planes + base / 8;
+  return u;
+}
+
+// Two units of at most 16 channels in one warp, lanes 0-15 the first, 16-31 the second: the
+// wavefront of plane_wavefront<1, false> with each half on its own unit. A half's lane 0 owns
+// its unit's top key, where every block starts with no significant coefficient, so the
+// significance count shuffled across the halves is never used.
+__device__ __forceinline__ void plane_wavefront_pair(const dec1_args& a, const plane_unit& A, const plane_unit& B,
+                                                     const int16_t* ktopA, const uint8_t* nplA, const uint8_t* nvlA,
+                                                     const int16_t* ktopB, const uint8_t* nplB, const uint8_t* nvlB,
+                                                     int lane)
+{
+  const int h = lane >> 4, c = lane & 15;
+  const plane_unit& U = h ? B : A;
+  const int16_t* ktop = h ? ktopB : ktopA;
+  const uint8_t* npl = h ? nplB : nplA;
+  const uint8_t* nvl = h ? nvlB : nvlA;
+  const int nkeys = U.nkeys, nb = U.nb, kmax = U.kmax, key = kmax - c;
+  bit_reader rd;
+  bool has = false;
+  if (c < nkeys)
+  {
+    const int ck = a.ckmin[U.fs], cn = a.cn[U.fs];
+    if (key >= ck && key < ck + cn)
+    {
+      const unsigned long long o = a.coff[a.cfirst[U.fs] + (unsigned long long)(key - ck)];
+      if (o != ~0ull)
+      {
+        rd.init(a.blob, a.blob_bytes, o * 8ull);
+        has = true;
+      }
+    }
+  }
+  const int my_steps = nb + nkeys - 1;
+  const int sA = A.nb + A.nkeys - 1, sB = B.nb + B.nkeys - 1;
+  const int steps = sA > sB ? sA : sB;
+  int n_out = 0, stop_out = 0;
+  for (int t = 0; t < steps; ++t)
+  {
+    int nl = __shfl_up_sync(0xffffffffu, n_out, 1);
+    int sl = __shfl_up_sync(0xffffffffu, stop_out, 1);
+    if (c == 0)
+    {
+      nl = 0;
+      sl = 0;
+    }
+    const int b = t - c;
+    unsigned long long X = 0;
+    n_out = 0;
+    stop_out = 0;
+    if (c < nkeys && b >= 0 && b < nb)
+    {
+      const int top = ktop[b], np = npl[b];
+      if (np > 0 && key <= top && key > top - np)
+      {
+        int n = key == top ? 0 : nl;
+        const int stopped = key == top ? 0 : sl;
+        if (stopped || !has)
+        {
+          stop_out = 1;
+          n_out = n;
+        }
+        else
+        {
+          X = decode_plane(rd, n, 1 << nvl[b]);
+          n_out = n;
+        }
+      }
+    }
+    if (c < nkeys && t < my_steps)
+      U.T[(size_t)t * (size_t)nkeys + (size_t)c] = X;
+  }
+}
+
 template <bool WIDE, bool MULTI = false>
-__global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : 6) k_decode_planes(const dec1_args a)
+__global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : (MULTI ? 6 : 4)) k_decode_planes(const dec1_args a)
 {
   __shared__ plane_smem sm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nunits = WIDE ? *a.wide_count : a.nbricks * a.nsb;
+  if constexpr (!WIDE && !MULTI)
+  {
+    // two consecutive units per warp; a pair of units of up to 16 channels shares the warp
+    for (int i = 2 * (blockIdx.x * kPlaneWarps + warp); i < nunits; i += 2 * gridDim.x * kPlaneWarps)
+    {
+      const plane_unit A = prep_unit<false, false>(a, i, sm.ktop[warp][0], sm.np[warp][0], sm.nvl[warp][0], lane);
+      plane_unit B;
+      B.run = 0;
+      B.nb = B.nkeys = B.kmax = 0;
+      B.fs = 0;
+      B.T = nullptr;
+      if (i + 1 < nunits)
+        B = prep_unit<false, false>(a, i + 1, sm.ktop[warp][1], sm.np[warp][1], sm.nvl[warp][1], lane);
+      __syncwarp();
+      if (A.run && B.run && A.nkeys <= 16 && B.nkeys <= 16)
+        plane_wavefront_pair(a, A, B, sm.ktop[warp][0], sm.np[warp][0], sm.nvl[warp][0], sm.ktop[warp][1],
+                             sm.np[warp][1], sm.nvl[warp][1], lane);
+      else
+      {
+        if (A.run)
+          plane_wavefront<1, false>(a, A.fs, A.nb, A.nkeys, A.kmax, sm.ktop[warp][0], sm.np[warp][0],
+                                    sm.nvl[warp][0], A.T, lane);
+        if (B.run)
+          plane_wavefront<1, false>(a, B.fs, B.nb, B.nkeys, B.kmax, sm.ktop[warp][1], sm.np[warp][1],
+                                    sm.nvl[warp][1], B.T, lane);
+      }
+      __syncwarp();
+    }
+    return;
+  }
   for (int i = blockIdx.x * kPlaneWarps + warp; i < nunits; i += gridDim.x * kPlaneWarps)
   {
     const int unit = WIDE ? a.wide_list[i] : i;
-    const int bi = unit / a.nsb, s = unit - bi * a.nsb;
-    const decode_target& rq = a.reqs[a.bricks[bi].req];
-    if (!((rq.mask >> s) & 1))
-    {
-      if (lane == 0)
-        a.unit_off[unit] = ~0ull;
+    int16_t* ktop = sm.ktop[warp][0];
+    uint8_t* npl = sm.np[warp][0];
+    uint8_t* nvl = sm.nvl[warp][0];
+    const plane_unit U = prep_unit<WIDE, MULTI>(a, unit, ktop, npl, nvl, lane);
+    if (!U.run)
       continue;
-    }
-    const int nb = a.nblocks[s];
-    const size_t fs = (size_t)a.bricks[bi].flat * (size_t)a.nsb + (size_t)s;
-    int16_t* ktop = sm.ktop[warp];
-    uint8_t* npl = sm.np[warp];
-    uint8_t* nvl = sm.nvl[warp];
-    int kmin = 1 << 30, kmax = -(1 << 30);
-    for (int b = lane; b < nb; b += 32)
-    {
-      int d3[3], bd[3];
-      unpack_geom(a.geom[(size_t)s * kMaxBlocksPerSubband + b], d3, bd);
-      const int emax = a.exps[fs * kMaxBlocksPerSubband + (size_t)b];
-      const int np = dev::coded_planes(emax, rq.etol, a.end_bp, a.bpc);
-      const int top = emax + 63 + 1024;
-      ktop[b] = (int16_t)top;
-      npl[b] = (uint8_t)np;
-      nvl[b] = (uint8_t)(2 * ((bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1)));
-      if (np)
-      {
-        if (top - np + 1 < 0)
-          atomicOr(a.error, 1);  // negative key value: a tolerance below 2^-1070 (unsupported)
-        const int kh = dev::plane_key(top, 0, a.bpc), kl = dev::plane_key(top, np - 1, a.bpc);
-        kmax = kh > kmax ? kh : kmax;
-        kmin = kl < kmin ? kl : kmin;
-      }
-    }
-    for (int o = 16; o > 0; o >>= 1)
-    {
-      const int x = __shfl_xor_sync(0xffffffffu, kmax, o), y = __shfl_xor_sync(0xffffffffu, kmin, o);
-      kmax = x > kmax ? x : kmax;
-      kmin = y < kmin ? y : kmin;
-    }
-    __syncwarp();
-    int nkeys = kmax >= kmin ? kmax - kmin + 1 : 0;
-    if (nkeys > (MULTI ? 64 : kKeyWindow))
-    {
-      if (lane == 0)
-        atomicOr(a.error, 1);
-      nkeys = 0;
-    }
-    if (nkeys == 0)
-    {
-      if (lane == 0)
-        a.unit_off[unit] = ~0ull;
-      continue;
-    }
-    if (!WIDE && nkeys > 32)
-    {
-      if (lane == 0)
-        a.wide_list[atomicAdd(a.wide_count, 1)] = unit;
-      continue;
-    }
-    const unsigned long long bytes =
-      (unsigned long long)(nb + nkeys - 1) * (unsigned long long)nkeys * 8ull * (unsigned long long)a.bpc;
-    unsigned long long base = 0;
-    if (lane == 0)
-      base = atomicAdd(a.cursor, bytes);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base + bytes > a.cap_bytes)
-    {
-      if (lane == 0)
-      {
-        atomicOr(a.error, 2);
-        a.unit_off[unit] = ~0ull;
-      }
-      continue;
-    }
-    if (lane == 0)
-      a.unit_off[unit] = base;
-    unsigned long long* T = a.planes + base / 8;
+    const size_t fs = U.fs;
+    const int nb = U.nb, nkeys = U.nkeys, kmax = U.kmax;
+    unsigned long long* T = U.T;
     if constexpr (MULTI)
     {
       // several planes per key: units of up to 32 keys here, up to 64 in the second pass
