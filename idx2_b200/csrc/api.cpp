@@ -207,10 +207,10 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
   std::vector<long long> lbytes;
   {
     gpu_coder coder(&c->d, f, d_field, f32);
-    const encode_plan* plan = c->d.plan_for(f, &e);
+    const std::shared_ptr<const encode_plan> plan = c->d.plan_for(f, &e);
     if (!plan)
       return e;
-    e = encode_dataset(&f, &p, &coder, nullptr, true, &tm, plan);
+    e = encode_dataset(&f, &p, &coder, nullptr, true, &tm, plan.get());
     stream_bytes = coder.stream_bytes();
     exp_bytes = coder.exp_bytes();
     kms = coder.kernel_ms();
@@ -262,7 +262,7 @@ IDX2G_API int idx2g_encode_device(idx2g_ctx* c, const idx2g_params* in, const vo
   coder.set_keep_device(true);
   std::vector<level_output> outs;
   auto t0 = std::chrono::steady_clock::now();
-  const encode_plan* plan = c->d.plan_for(f, &e);
+  const std::shared_ptr<const encode_plan> plan = c->d.plan_for(f, &e);
   if (!plan)
     return e;
   e = encode_levels(&f, &coder, &outs, *plan);
@@ -301,7 +301,7 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<params> ps((size_t)n);
   std::vector<dataset_format> fs((size_t)n);
-  std::vector<const encode_plan*> plans((size_t)n);
+  std::vector<std::shared_ptr<const encode_plan>> plans((size_t)n);  // held for the whole call
   std::vector<std::vector<level_output>> outs((size_t)n);
   size_t host_bytes = 0;
   long long total_bricks = 0;
@@ -345,7 +345,7 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
   for (int i = 0; i < n; ++i)
   {
     bf[(size_t)i].f = &fs[(size_t)i];
-    bf[(size_t)i].plan = plans[(size_t)i];
+    bf[(size_t)i].plan = plans[(size_t)i].get();
     bf[(size_t)i].d_field = dptr[(size_t)i];
     bf[(size_t)i].f32 = ps[(size_t)i].type == dtype::float32;
     bf[(size_t)i].outs = &outs[(size_t)i];

@@ -29,15 +29,17 @@ struct device_ctx
   // Encode plans by format: the brick order and the EncodeSubband events depend only on the
   // dims, the brick dims and the number of levels, so repeated encodes of fields of one shape
   // (the time steps of a simulation) plan once.
+  // Callers hold the returned pointer for as long as they use the plan: the cache keeps 16
+  // shapes and may drop one while an earlier holder still uses it.
   std::map<std::string, std::shared_ptr<const encode_plan>> plans;
-  const encode_plan* plan_for(const dataset_format& f, int* err)
+  std::shared_ptr<const encode_plan> plan_for(const dataset_format& f, int* err)
   {
     char key[128];
     snprintf(key, sizeof key, "%d %d %d/%d %d %d/%d", f.dims.x, f.dims.y, f.dims.z, f.brick_dims.x, f.brick_dims.y,
              f.brick_dims.z, f.nlevels);
     auto it = plans.find(key);
     if (it != plans.end())
-      return it->second.get();
+      return it->second;
     std::shared_ptr<encode_plan> pl = std::make_shared<encode_plan>();
     *err = make_encode_plan(f, pl.get());
     if (*err)
@@ -45,7 +47,7 @@ struct device_ctx
     if (plans.size() >= 16)
       plans.erase(plans.begin());
     plans[key] = pl;
-    return pl.get();
+    return pl;
   }
 
   struct buf
