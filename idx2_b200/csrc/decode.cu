@@ -14,6 +14,7 @@
 #include "codec_device.cuh"
 #include "decode_device.h"
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -48,50 +49,49 @@ decode_device::~decode_device()
   cudaFree(blob_);
 }
 
-template <typename T>
-static int up(T** dst, const std::vector<T>& v, cudaStream_t st, size_t pad = 0)
+int decode_device::alloc(device_ctx* ctx, size_t nslots, size_t blob_bytes)
 {
-  size_t bytes = v.size() * sizeof(T);
-  if (cudaMalloc((void**)dst, bytes + pad + 16) != cudaSuccess)
+  cudaSetDevice(ctx->device);
+  // the blob is padded with zero bytes for the bit readers' look-ahead
+  if (cudaMalloc((void**)&exps_, nslots * kMaxBlocksPerSubband * sizeof(int16_t) + 16) != cudaSuccess ||
+      cudaMalloc((void**)&kmin_, nslots * sizeof(int32_t) + 16) != cudaSuccess ||
+      cudaMalloc((void**)&n_, nslots * sizeof(int32_t) + 16) != cudaSuccess ||
+      cudaMalloc((void**)&first_, nslots * sizeof(uint64_t) + 16) != cudaSuccess ||
+      cudaMalloc((void**)&blob_, blob_bytes + 32) != cudaSuccess)
     return OutOfMemory;
-  if (bytes)
-    cudaMemcpyAsync(*dst, v.data(), bytes, cudaMemcpyHostToDevice, st);
-  if (pad)
-    cudaMemsetAsync((char*)*dst + bytes, 0, pad + 16, st);
+  cudaMemsetAsync(blob_ + blob_bytes, 0, 32, ctx->stream);
+  nslots_ = nslots;
+  blob_bytes_ = blob_bytes;
   return NoError;
 }
 
-int decode_device::upload(device_ctx* ctx, const std::vector<int16_t>& exps, const std::vector<int32_t>& kmin,
-                          const std::vector<int32_t>& n, const std::vector<uint64_t>& first,
-                          const std::vector<uint64_t>& off, const uint8_t* blob, size_t blob_bytes)
+void decode_device::upload_blob(device_ctx* ctx, const uint8_t* src, size_t offset, size_t bytes)
+{
+  cudaSetDevice(ctx->device);
+  if (bytes && offset + bytes <= blob_bytes_)
+    cudaMemcpyAsync(blob_ + offset, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+}
+
+int decode_device::upload_tables(device_ctx* ctx, const int16_t* exps, const int32_t* kmin, const int32_t* n,
+                                 const uint64_t* first, const uint64_t* off, size_t nchan)
 {
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
-  int e = up(&exps_, exps, st);
-  if (!e)
-    e = up(&kmin_, kmin, st);
-  if (!e)
-    e = up(&n_, n, st);
-  if (!e)
-    e = up((uint64_t**)&first_, first, st);
-  if (!e)
-    e = up((uint64_t**)&off_, off, st);
-  if (!e)
+  if (cudaMalloc((void**)&off_, nchan * sizeof(uint64_t) + 16) != cudaSuccess)
+    return OutOfMemory;
+  const size_t ns = nslots_;
+  if (ns)
   {
-    // the blob (padded with 16 zero bytes for the bit readers' look-ahead)
-    if (cudaMalloc((void**)&blob_, blob_bytes + 32) != cudaSuccess)
-      e = OutOfMemory;
-    else
-    {
-      if (blob_bytes)
-        cudaMemcpyAsync(blob_, blob, blob_bytes, cudaMemcpyHostToDevice, st);
-      cudaMemsetAsync(blob_ + blob_bytes, 0, 32, st);
-    }
+    cudaMemcpyAsync(exps_, exps, ns * kMaxBlocksPerSubband * sizeof(int16_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(kmin_, kmin, ns * sizeof(int32_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(n_, n, ns * sizeof(int32_t), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(first_, first, ns * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
   }
-  if (e)
-    return e;
-  resident_ = exps.size() * 2 + kmin.size() * 4 + n.size() * 4 + first.size() * 8 + off.size() * 8 + blob_bytes;
-  blob_bytes_ = blob_bytes;
+  if (nchan)
+    cudaMemcpyAsync(off_, off, nchan * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
+  resident_ = ns * (kMaxBlocksPerSubband * sizeof(int16_t) + 2 * sizeof(int32_t) + sizeof(uint64_t)) +
+              nchan * sizeof(uint64_t) + blob_bytes_;
+  // the staging buffers are reused by the next open on this context
   if (cudaStreamSynchronize(st) != cudaSuccess)
     return CudaError;
   return NoError;
@@ -145,6 +145,20 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       coeff_base[(size_t)l + 1] =
         coeff_base[(size_t)l] + (k < r0.levels.size() ? (long long)r0.levels[k].bricks.size() : 0);
     }
+  // One request into pinned host memory: the output level runs as several launches over rows
+  // of bricks (ordered by output z), and each band of output planes that the launches so far
+  // have finished goes to the host on the copy stream while the next launches run.
+  bool split_out = false;
+  const size_t out_elem = r0.f32 ? 4 : 8;
+  if (!out_on_device && n == 1 && !keep && !coeff_out && out_bytes[0] >= ((size_t)8 << 20))
+  {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, outs[0]) == cudaSuccess && pa.type == cudaMemoryTypeHost && ctx->copies() &&
+        (size_t)r0.out_dims.x * (size_t)r0.out_dims.y * (size_t)r0.out_dims.z * out_elem <= out_bytes[0])
+      split_out = true;
+    cudaGetLastError();
+  }
+  cudaStream_t cs = split_out ? ctx->copies() : nullptr;
   int* d_err = (int*)ctx->ws("dec.err", 16);  // [0] brick kernel, [1] plane kernels (bit flags)
   uint64_t* d_geom = (uint64_t*)ctx->ws("dec.geom", sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
   if (!d_err || !d_geom)
@@ -170,6 +184,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       keep->sig.assign((size_t)L, std::vector<int>());
     }
     size_t nev = 0;  // levels timed (event pairs of the pool)
+    bool out_copied = false;  // the output went to the host band by band
     double* prev = nullptr;
     std::vector<int> prev_base(n, -1), cur_base(n, -1);
     std::vector<decode_brick> hb;
@@ -225,6 +240,11 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         prev = nullptr;
         continue;
       }
+      // output level of a split call: bricks by output z (output bricks are independent)
+      const bool split_level = split_out && targets.size() == 1 && targets[0].is_output;
+      if (split_level)
+        std::stable_sort(hb.begin(), hb.end(),
+                         [](const decode_brick& x, const decode_brick& y) { return x.dst_from[2] < y.dst_from[2]; });
       ++li;
       decode_brick* d_bricks = (decode_brick*)ctx->ws("dec.bricks", sizeof(decode_brick) * (size_t)nbr);
       decode_target* d_reqs = (decode_target*)ctx->ws("dec.reqs", sizeof(decode_target) * targets.size());
@@ -355,9 +375,55 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         k_decode_planes<false, true><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
         k_decode_planes<true, true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(pa);
       }
-      k_decode_level<<<grid, kThreads, smem, st>>>(a);
+      if (split_level)
+      {
+        // about 8 launches, each of whole rows of bricks; after launch g every output plane
+        // below the first plane of the bricks still to come is final
+        constexpr int kBands = 8;
+        std::vector<int> cuts(1, 0);
+        for (int g = 1; g < kBands; ++g)
+        {
+          int c = (int)((long long)nbr * g / kBands);
+          while (c > 0 && c < nbr && hb[(size_t)c].dst_from[2] == hb[(size_t)c - 1].dst_from[2])
+            ++c;
+          if (c > cuts.back() && c < nbr)
+            cuts.push_back(c);
+        }
+        cuts.push_back(nbr);
+        const size_t plane = (size_t)r0.out_dims.x * (size_t)r0.out_dims.y * out_elem;
+        size_t z_done = 0;
+        for (size_t g = 0; g + 1 < cuts.size(); ++g)
+        {
+          dec_args ag = a;
+          ag.bricks = d_bricks + cuts[g];
+          ag.nbricks = cuts[g + 1] - cuts[g];
+          ag.unit_off = d_uoff + (size_t)cuts[g] * (size_t)r0.nsb;
+          const int gg = ag.nbricks < grid ? ag.nbricks : grid;
+          k_decode_level<<<gg, kThreads, smem, st>>>(ag);
+          ++ctx->launches;
+          const size_t z_next =
+            g + 2 < cuts.size() ? (size_t)hb[(size_t)cuts[g + 1]].dst_from[2] : (size_t)r0.out_dims.z;
+          if (z_next > z_done)
+          {
+            cudaEvent_t ge = ctx->ev(64 + g);
+            if (!ge)
+              return CudaError;
+            cudaEventRecord(ge, st);
+            cudaStreamWaitEvent(cs, ge, 0);
+            cudaMemcpyAsync((uint8_t*)outs[0] + z_done * plane, (const uint8_t*)d_out[0] + z_done * plane,
+                            (z_next - z_done) * plane, cudaMemcpyDeviceToHost, cs);
+            z_done = z_next;
+          }
+        }
+        out_copied = true;
+        ctx->launches += 2;
+      }
+      else
+      {
+        k_decode_level<<<grid, kThreads, smem, st>>>(a);
+        ctx->launches += 3;
+      }
       cudaEventRecord(t1, st);
-      ctx->launches += 3;
       if (cudaGetLastError() != cudaSuccess)
         return CudaError;
       prev = d_level;
@@ -373,7 +439,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
           cudaMemcpyAsync(keep->sig[(size_t)l].data(), ctx->ws(kn, keep->sig[(size_t)l].size() * 4 + 4),
                           keep->sig[(size_t)l].size() * 4, cudaMemcpyDeviceToHost, st);
         }
-    if (cudaStreamSynchronize(st) != cudaSuccess)
+    if (cudaStreamSynchronize(st) != cudaSuccess || (cs && cudaStreamSynchronize(cs) != cudaSuccess))
       return CudaError;
     if (herr[1] & 2)
     {
@@ -389,7 +455,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       cudaEventElapsedTime(&ms, ctx->ev(2 * e), ctx->ev(2 * e + 1));
       total_ms += ms;
     }
-    if (!out_on_device)
+    if (!out_on_device && !out_copied)
     {
       for (size_t i = 0; i < n; ++i)
         if (out_bytes[i])

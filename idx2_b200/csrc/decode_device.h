@@ -81,9 +81,13 @@ class decode_device
 {
 public:
   ~decode_device();
-  int upload(device_ctx* ctx, const std::vector<int16_t>& exps, const std::vector<int32_t>& kmin,
-             const std::vector<int32_t>& n, const std::vector<uint64_t>& first,
-             const std::vector<uint64_t>& off, const uint8_t* blob, size_t blob_bytes);
+  // Opening a dataset: alloc() the per-(brick, subband) tables of nslots entries and the blob,
+  // upload_blob() each range of the files as it is read (any thread), upload_tables() once the
+  // host index is built (waits for every copy).
+  int alloc(device_ctx* ctx, size_t nslots, size_t blob_bytes);
+  void upload_blob(device_ctx* ctx, const uint8_t* src, size_t offset, size_t bytes);
+  int upload_tables(device_ctx* ctx, const int16_t* exps, const int32_t* kmin, const int32_t* n,
+                    const uint64_t* first, const uint64_t* off, size_t nchan);
   int decode(device_ctx* ctx, const decode_request& rq, void* out, size_t out_bytes, bool out_on_device,
              double* kernel_ms);
   // Several requests on this dataset at once: per level one launch (of each kernel) over the
@@ -111,6 +115,7 @@ private:
   unsigned long long* off_ = nullptr;
   uint8_t* blob_ = nullptr;
   size_t blob_bytes_ = 0;
+  size_t nslots_ = 0;
   size_t resident_ = 0;
 };
 

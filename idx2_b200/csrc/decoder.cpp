@@ -12,6 +12,8 @@
 #include "decoder.h"
 #include "decode_device.h"
 #include "packer.h"
+#include "parallel.h"
+#include "trace.h"
 
 #include <algorithm>
 #include <cmath>
@@ -114,27 +116,6 @@ bool read_whole(const std::string& path, std::vector<uint8_t>* out)
   return r == out->size();
 }
 
-// Run f(i) for i in [0, n) on a pool of threads.
-template <typename F>
-void parallel_for(size_t n, F&& f)
-{
-  unsigned nt = std::thread::hardware_concurrency();
-  nt = nt ? (nt > 32 ? 32 : nt) : 4;
-  if (nt > n)
-    nt = (unsigned)(n ? n : 1);
-  std::atomic<size_t> next{ 0 };
-  auto work = [&]() {
-    for (size_t i; (i = next.fetch_add(1)) < n;)
-      f(i);
-  };
-  std::vector<std::thread> th;
-  for (unsigned t = 1; t < nt; ++t)
-    th.emplace_back(work);
-  work();
-  for (auto& t : th)
-    t.join();
-}
-
 } // namespace
 
 struct dataset_handle
@@ -146,12 +127,13 @@ struct dataset_handle
   std::vector<std::vector<v3>> brick3;           // per level, per brick index
   std::vector<std::vector<int>> brick_in_chunk;  // per level, per brick index
   std::vector<std::vector<int>> blocks_per_sb;   // per level, per subband (coded blocks)
-  // host index
-  std::vector<int16_t> exps;                     // [level offset + brick][sb][kMaxBlocksPerSubband]
   std::vector<size_t> level_brick_base;          // brick index base of each level in flat tables
-  std::vector<int32_t> chan_kmin, chan_n;        // [flat brick][sb]
-  std::vector<uint64_t> chan_first;              // [flat brick][sb] index into chan_off
-  std::vector<uint64_t> chan_off;                // byte offset in blob, ~0 = absent
+  // host index, built while the dataset opens in pinned staging buffers of the context
+  size_t nslots = 0, nchan = 0;
+  int16_t* exps = nullptr;                       // [level offset + brick][sb][kMaxBlocksPerSubband]
+  int32_t* chan_kmin = nullptr, *chan_n = nullptr;  // [flat brick][sb]
+  uint64_t* chan_first = nullptr;                // [flat brick][sb] index into chan_off
+  uint64_t* chan_off = nullptr;                  // byte offset in blob, ~0 = absent
   const uint8_t* blob = nullptr;                 // every data file back to back (pinned host memory)
   size_t blob_bytes = 0;
   // device copies
@@ -200,6 +182,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   dataset_format& f = h->f;
   const int L = f.nlevels;
   const int nsb = f.nsubbands();
+  stage_timer tt;
   h->brick_index.assign((size_t)L, {});
   h->brick3.assign((size_t)L, {});
   h->brick_in_chunk.assign((size_t)L, {});
@@ -247,17 +230,40 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   const size_t nslots = nflat * (size_t)nsb;
   if (nslots >= 0xFFFFFFFFull)
     return OptionNotSupported;
-  h->exps.assign(nslots * kMaxBlocksPerSubband, 0);
-  h->chan_kmin.assign(nslots, 0);
-  h->chan_n.assign(nslots, 0);
-  h->chan_first.assign(nslots, 0);
+  h->nslots = nslots;
+  h->exps = (int16_t*)ctx->pinned("dec.exps", nslots * kMaxBlocksPerSubband * sizeof(int16_t));
+  h->chan_kmin = (int32_t*)ctx->pinned("dec.kmin", nslots * sizeof(int32_t));
+  h->chan_n = (int32_t*)ctx->pinned("dec.n", nslots * sizeof(int32_t));
+  h->chan_first = (uint64_t*)ctx->pinned("dec.first", nslots * sizeof(uint64_t));
+  if (!h->exps || !h->chan_kmin || !h->chan_n || !h->chan_first)
+    return OutOfMemory;
+  parallel_ranges(nslots, [&](size_t i0, size_t i1) {
+    memset(h->exps + i0 * kMaxBlocksPerSubband, 0, (i1 - i0) * kMaxBlocksPerSubband * sizeof(int16_t));
+  });
 
+  tt.lap("open.bricks");
   // the set of data files: one per (level, brick >> log2(bricks per file)); a missing file
-  // leaves its bricks undecoded (Core/idx2Decode.cpp:166-168)
+  // leaves its bricks undecoded (Core/idx2Decode.cpp:166-168). A file's path depends on the
+  // bits of the linear brick index above `shift` only, so it is built once per run of bricks
+  // that share them.
   std::map<std::string, int> names;
   for (int l = 0; l < L; ++l)
+  {
+    const std::vector<int>& dd = f.files_dirs_depth[(size_t)l];
+    int shift = (int)f.bricks_order_str[(size_t)l].size();
+    for (size_t d = 0; d + 1 < dd.size(); ++d)
+      shift -= dd[d];
+    shift = shift < 0 ? 0 : shift > 63 ? 63 : shift;
+    u64 prev = ~0ull;
     for (size_t i = 0; i < h->brick3[(size_t)l].size(); ++i)
-      names[file_path(f, linear_brick(f, l, h->brick3[(size_t)l][i]), l)] = l;
+    {
+      const u64 lin = linear_brick(f, l, h->brick3[(size_t)l][i]);
+      if ((lin >> shift) == prev)
+        continue;
+      prev = lin >> shift;
+      names[file_path(f, lin, l)] = l;
+    }
+  }
   std::vector<data_file> files;
   size_t total = 0;
   for (auto& kv : names)
@@ -274,10 +280,14 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     files.push_back(df);
   }
 
-  // every file into one pinned buffer, in ranges of 16 MB read by a pool of threads
+  // every file into one pinned buffer, in ranges of 16 MB read by a pool of threads; each
+  // range goes on to the device as soon as it is read, while the other threads read on and
+  // the index below is built
   uint8_t* blob = (uint8_t*)ctx->pinned("dec.files", total + 16);
   if (!blob)
     return OutOfMemory;
+  if (int ae = h->dev.alloc(ctx, nslots, total))
+    return ae;
   {
     struct range
     {
@@ -308,6 +318,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
         }
         done += (size_t)got;
       }
+      h->dev.upload_blob(ctx, blob + files[(size_t)r.file].base + r.off, files[(size_t)r.file].base + r.off, r.n);
     });
     for (int fd : fds)
       if (fd >= 0)
@@ -317,6 +328,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   }
   h->blob = blob;
   h->blob_bytes = total;
+  tt.lap("open.read");
 
   // file tails: exponent chunks and bit-plane chunks
   std::vector<chunk_ref> exp_chunks, bp_chunks;
@@ -383,6 +395,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     }
   }
 
+  tt.lap("open.tails");
   // exponent chunks: decompress and spread over their bricks (chunks own disjoint rows)
   const int esz = f.type == dtype::float32 ? 1 : 2;
   std::atomic<int> err{ 0 };
@@ -410,7 +423,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
         continue;
       size_t pos = (size_t)h->brick_in_chunk[(size_t)lv][(size_t)bi] * (size_t)bc * (size_t)esz;
       size_t flat = h->level_brick_base[(size_t)lv] + (size_t)bi;
-      int16_t* dst = h->exps.data() + (flat * (size_t)nsb + (size_t)sb) * kMaxBlocksPerSubband;
+      int16_t* dst = h->exps + (flat * (size_t)nsb + (size_t)sb) * kMaxBlocksPerSubband;
       for (int b = 0; b < bc; ++b)
       {
         size_t q = pos + (size_t)b * (size_t)esz;
@@ -424,6 +437,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   if (err)
     return err;
 
+  tt.lap("open.exponents");
   // bit-plane chunk headers (Core/idx2Decode.cpp:507 DecompressChunk), one task per chunk
   std::vector<std::vector<chan_entry>> entries(bp_chunks.size());
   parallel_for(bp_chunks.size(), [&](size_t k) {
@@ -482,16 +496,27 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   if (err)
     return err;
 
-  // channel table: key range per (brick, subband), then the offsets
+  tt.lap("open.chunk_headers");
+  // channel table: key range per (brick, subband), then the offsets. The chunks of one
+  // (level, subband) touch only that subband's slots, so each (level, subband) is one task.
   std::vector<int32_t> kmax(nslots, -1);
-  std::vector<int32_t>& kmin = h->chan_kmin;
-  std::fill(kmin.begin(), kmin.end(), 1 << 30);
-  for (const auto& v : entries)
-    for (const chan_entry& e : v)
-    {
-      kmin[e.slot] = std::min(kmin[e.slot], e.bpkey);
-      kmax[e.slot] = std::max(kmax[e.slot], e.bpkey);
-    }
+  int32_t* kmin = h->chan_kmin;
+  parallel_ranges(nslots, [&](size_t i0, size_t i1) { std::fill(kmin + i0, kmin + i1, 1 << 30); });
+  std::vector<std::vector<size_t>> by_sb((size_t)L * (size_t)nsb);
+  for (size_t k = 0; k < bp_chunks.size(); ++k)
+  {
+    const int sb = (int)((bp_chunks[k].addr >> 12) & 0x3F), lv = (int)((bp_chunks[k].addr >> 60) & 0xF);
+    if (lv == bp_chunks[k].level && lv < L && sb < nsb)
+      by_sb[(size_t)lv * (size_t)nsb + (size_t)sb].push_back(k);
+  }
+  parallel_for(by_sb.size(), [&](size_t g) {
+    for (size_t k : by_sb[g])
+      for (const chan_entry& e : entries[k])
+      {
+        kmin[e.slot] = std::min(kmin[e.slot], e.bpkey);
+        kmax[e.slot] = std::max(kmax[e.slot], e.bpkey);
+      }
+  });
   uint64_t nchan = 0;
   for (size_t i = 0; i < nslots; ++i)
   {
@@ -505,11 +530,16 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     h->chan_first[i] = nchan;
     nchan += (uint64_t)h->chan_n[i];
   }
-  h->chan_off.assign(nchan, ~0ull);
+  h->nchan = nchan;
+  h->chan_off = (uint64_t*)ctx->pinned("dec.off", (nchan ? nchan : 1) * sizeof(uint64_t));
+  if (!h->chan_off)
+    return OutOfMemory;
+  parallel_ranges(nchan, [&](size_t i0, size_t i1) { std::fill(h->chan_off + i0, h->chan_off + i1, ~0ull); });
   parallel_for(entries.size(), [&](size_t k) {
     for (const chan_entry& e : entries[k])
       h->chan_off[h->chan_first[e.slot] + (size_t)(e.bpkey - kmin[e.slot])] = e.off;
   });
+  tt.lap("open.channels");
   return NoError;
 }
 
@@ -530,10 +560,15 @@ int dataset_open(device_ctx* ctx, const params& pin, dataset_handle** out)
   }
   if (!e)
     e = load_index(ctx, h);
+  stage_timer tt;
   if (!e)
-    e = h->dev.upload(ctx, h->exps, h->chan_kmin, h->chan_n, h->chan_first, h->chan_off, h->blob,
-                      h->blob_bytes);
-  h->blob = nullptr;  // the pinned staging buffer stays with the context
+    e = h->dev.upload_tables(ctx, h->exps, h->chan_kmin, h->chan_n, h->chan_first, h->chan_off, h->nchan);
+  tt.lap("open.upload");
+  // the pinned staging buffers stay with the context
+  h->blob = nullptr;
+  h->exps = nullptr;
+  h->chan_kmin = h->chan_n = nullptr;
+  h->chan_first = h->chan_off = nullptr;
   if (e)
   {
     delete h;
@@ -594,12 +629,16 @@ int dataset_decode(device_ctx* ctx, dataset_handle* h, const params& p, void* ou
 {
   const decode_request* rq = nullptr;
   size_t need = 0;
+  stage_timer tt;
   int e = cached_plan_decode(h, p, &rq, &need);
   if (e)
     return e;
   if (out_bytes < need)
     return SizeTooSmall;
-  return h->dev.decode(ctx, *rq, out, need, out_on_device, kernel_ms);
+  tt.lap("decode.plan");
+  e = h->dev.decode(ctx, *rq, out, need, out_on_device, kernel_ms);
+  tt.lap("decode.device");
+  return e;
 }
 
 int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out, size_t* need_out)

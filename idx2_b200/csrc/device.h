@@ -24,6 +24,14 @@ struct device_ctx
   int num_sms = 148;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> evpool;  // timing events of calls that time several launches
+  // second stream for host copies that overlap the kernels of `stream` (created on first use)
+  cudaStream_t copy_stream = nullptr;
+  cudaStream_t copies()
+  {
+    if (!copy_stream && cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking) != cudaSuccess)
+      copy_stream = nullptr;
+    return copy_stream;
+  }
   long long launches = 0;  // kernels launched on this context so far
   std::map<std::string, int> tuned;  // batched encode: CTAs per SM chosen per batch signature
   // Encode plans by format: the brick order and the EncodeSubband events depend only on the
@@ -136,6 +144,12 @@ struct device_ctx
   }
   void release()
   {
+    if (copy_stream)
+    {
+      cudaStreamSynchronize(copy_stream);
+      cudaStreamDestroy(copy_stream);
+      copy_stream = nullptr;
+    }
     for (cudaEvent_t e : evpool)
       cudaEventDestroy(e);
     evpool.clear();

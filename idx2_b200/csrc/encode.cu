@@ -14,6 +14,7 @@
 #include "codec_device.cuh"
 #include "device.h"
 #include "encoder.h"
+#include "trace.h"
 
 #include <cmath>
 #include <cstdio>
@@ -1334,6 +1335,7 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
   if (level >= enc_->nlevels())
     return UnknownError;
   const double before = enc_->kernel_ms();
+  stage_timer tt;
   cudaEventRecord(ctx_->ev0, st);
   int e = enc_->enqueue_level(level);
   cudaEventRecord(ctx_->ev1, st);
@@ -1341,11 +1343,13 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     return e;
   if (cudaStreamSynchronize(st) != cudaSuccess)
     return CudaError;
+  tt.lap(level == 0 ? "encode.level0" : level == 1 ? "encode.level1" : "encode.level2+");
   float ms = 0;
   cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
   e = enc_->collect_level(level, keep_device_);
   if (e)
     return e;
+  tt.lap(level == 0 ? "encode.collect0" : level == 1 ? "encode.collect1" : "encode.collect2+");
   fields_[0].level_ms[(size_t)level] = ms + (float)(enc_->kernel_ms() - before);
   enc_->add_kernel_ms(ms);
   *out = std::move(outs_[(size_t)level]);

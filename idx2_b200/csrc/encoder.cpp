@@ -1,5 +1,7 @@
 // Encode driver (Core/idx2Encode.cpp:276-444).
 #include "encoder.h"
+#include "parallel.h"
+#include "trace.h"
 
 #include <atomic>
 #include <chrono>
@@ -210,31 +212,39 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
                  bool write_files, encode_timing* timing)
 {
   double t1 = now_s();
+  stage_timer tt;
   int e = NoError;
   packer pk(*f, f->tolerance);
-  for (const encode_event& ev : plan.events)
-  {
-    const level_output& o = outs[(size_t)ev.level];
-    size_t bs = (size_t)ev.brick * (size_t)o.nsb + (size_t)ev.subband;
-    subband_result r;
-    r.level = ev.level;
-    r.brick = plan.levels[(size_t)ev.level][(size_t)ev.brick].linear;
-    r.subband = ev.subband;
-    r.nexps = o.nexps[(size_t)ev.subband];
-    region_view v = view_region(o.bytes() + o.offset[bs], r.nexps);
-    r.exps = v.exps;
-    r.kmin = v.kmin;
-    r.kmax = v.kmax;
-    r.sizes = v.sizes;
-    r.bytes = v.bytes;
-    e = pk.add(r);
-    if (e)
-      return e;
-  }
+  // the coder's regions, parsed in parallel, recorded in the plan's event order
+  std::vector<subband_result> rs(plan.events.size());
+  parallel_ranges(rs.size(), [&](size_t i0, size_t i1) {
+    for (size_t i = i0; i < i1; ++i)
+    {
+      const encode_event& ev = plan.events[i];
+      const level_output& o = outs[(size_t)ev.level];
+      size_t bs = (size_t)ev.brick * (size_t)o.nsb + (size_t)ev.subband;
+      subband_result& r = rs[i];
+      r.level = ev.level;
+      r.brick = plan.levels[(size_t)ev.level][(size_t)ev.brick].linear;
+      r.subband = ev.subband;
+      r.nexps = o.nexps[(size_t)ev.subband];
+      region_view v = view_region(o.bytes() + o.offset[bs], r.nexps);
+      r.exps = v.exps;
+      r.kmin = v.kmin;
+      r.kmax = v.kmax;
+      r.sizes = v.sizes;
+      r.bytes = v.bytes;
+    }
+  });
+  e = pk.add_all(std::move(rs));
+  if (e)
+    return e;
+  tt.lap("pack.events");
   e = pk.finish();
   if (e)
     return e;
   double t2 = now_s();
+  tt.t = stage_timer::now();
 
   std::string meta = meta_text(*f, *p) + pk.stats_text();
   std::string meta_path = p->out_dir + "/" + p->name + "/" + p->field + ".idx2";
@@ -252,8 +262,7 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
     {
       std::vector<uint8_t>& d = (*files)[kv->first];
       d.reserve(kv->second.nbytes);
-      for (const segment& s : kv->second.parts)
-        d.insert(d.end(), s.p, s.p + s.n);
+      kv->second.for_each_segment([&](const segment& s) { d.insert(d.end(), s.p, s.p + s.n); });
     }
     (*files)[meta_path] = std::vector<uint8_t>(meta.begin(), meta.end());
   }
@@ -266,9 +275,11 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
     wl.reserve(list.size());
     for (auto* kv : list)
       wl.push_back({ kv->first, &kv->second });
+    tt.lap("write.meta");
     e = idx2g::write_files(wl);
     if (e)
       return e;
+    tt.lap("write.files");
   }
   double t3 = now_s();
   if (timing)

@@ -2,6 +2,8 @@
 #include "packer.h"
 
 #include "encoder.h"
+#include "parallel.h"
+#include "trace.h"
 
 #include <algorithm>
 #include <atomic>
@@ -160,21 +162,28 @@ void file_buffer::append_owned(std::vector<uint8_t>&& v)
   if (v.empty())
     return;
   owned.push_back(std::move(v));
-  parts.push_back({ owned.back().data(), owned.back().size() });
-  nbytes += owned.back().size();
+  append_ref(owned.back().data(), owned.back().size());
 }
 
 void file_buffer::append_ref(const uint8_t* p, size_t n)
 {
   if (!n)
     return;
-  parts.push_back({ p, n });
-  nbytes += n;
+  singles.push_back({ p, n });
+  append_run(&singles.back(), 1, n);
+}
+
+void file_buffer::append_run(const segment* s, size_t n, size_t bytes)
+{
+  if (!bytes)
+    return;
+  parts.push_back({ s, n, bytes });
+  nbytes += bytes;
 }
 
 int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& files)
 {
-  // Every file is cut into ranges of whole parts of about kRange bytes, copied by a pool of
+  // Every file is cut into ranges of whole runs of about kRange bytes, copied by a pool of
   // threads. Large files are written through a shared mapping (writes to one file through
   // write(2) are serialised by the kernel); small files, and any file that cannot be mapped,
   // with pwrite from a staging buffer.
@@ -211,11 +220,11 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
       else if (ftruncate(fds[i], 0) != 0)
         err = FileWriteFailed;
     }
-    const std::vector<segment>& parts = files[i].second->parts;
+    const std::vector<segment_run>& parts = files[i].second->parts;
     size_t off = 0, start = 0, acc = 0;
     for (size_t k = 0; k < parts.size(); ++k)
     {
-      acc += parts[k].n;
+      acc += parts[k].bytes;
       if (acc >= kRange || k + 1 == parts.size())
       {
         ranges.push_back({ (int)i, start, k + 1, off, acc });
@@ -238,29 +247,27 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
       for (size_t i; (i = next.fetch_add(1)) < ranges.size();)
       {
         const range& r = ranges[i];
-        const std::vector<segment>& parts = files[(size_t)r.file].second->parts;
+        const std::vector<segment_run>& parts = files[(size_t)r.file].second->parts;
+        auto gather = [&](uint8_t* dst) {
+          for (size_t k = r.p0; k < r.p1; ++k)
+            for (size_t j = 0; j < parts[k].nseg; ++j)
+            {
+              memcpy(dst, parts[k].seg[j].p, parts[k].seg[j].n);
+              dst += parts[k].seg[j].n;
+            }
+        };
         if (maps[(size_t)r.file])
         {
-          uint8_t* dst = maps[(size_t)r.file] + r.offset;
-          for (size_t k = r.p0; k < r.p1; ++k)
-          {
-            memcpy(dst, parts[k].p, parts[k].n);
-            dst += parts[k].n;
-          }
+          gather(maps[(size_t)r.file] + r.offset);
           continue;
         }
         const uint8_t* src;
-        if (r.p1 - r.p0 == 1)
-          src = parts[r.p0].p;
+        if (r.p1 - r.p0 == 1 && parts[r.p0].nseg == 1)
+          src = parts[r.p0].seg[0].p;
         else
         {
           stage.resize(r.bytes);
-          size_t at = 0;
-          for (size_t k = r.p0; k < r.p1; ++k)
-          {
-            memcpy(stage.data() + at, parts[k].p, parts[k].n);
-            at += parts[k].n;
-          }
+          gather(stage.data());
           src = stage.data();
         }
         size_t done = 0;
@@ -301,26 +308,6 @@ namespace
 {
 
 constexpr uint64_t kFinalFlush = ~0ull;  // stamp of the writes of the final flushes
-
-template <typename F>
-void run_parallel(size_t n, F&& fn)
-{
-  unsigned nt = std::thread::hardware_concurrency();
-  nt = nt ? (nt > 32 ? 32 : nt) : 4;
-  if (nt > n)
-    nt = (unsigned)(n ? n : 1);
-  std::atomic<size_t> next{ 0 };
-  auto work = [&]() {
-    for (size_t i; (i = next.fetch_add(1)) < n;)
-      fn(i);
-  };
-  std::vector<std::thread> th;
-  for (unsigned t = 1; t < nt; ++t)
-    th.emplace_back(work);
-  work();
-  for (auto& t : th)
-    t.join();
-}
 
 struct channel
 {
@@ -442,6 +429,18 @@ int packer::add(const subband_result& r)
   return NoError;
 }
 
+int packer::add_all(std::vector<subband_result>&& rs)
+{
+  for (const subband_result& r : rs)
+    if (r.level < 0 || r.level >= 16 || r.subband < 0 || r.subband >= 64)
+      return InvalidArgument;
+  if (events_.empty())
+    events_ = std::move(rs);
+  else
+    events_.insert(events_.end(), rs.begin(), rs.end());
+  return NoError;
+}
+
 static void put_i32(std::vector<uint8_t>* v, int32_t x)
 {
   uint8_t b[4];
@@ -452,6 +451,7 @@ static void put_i32(std::vector<uint8_t>* v, int32_t x)
 int packer::finish()
 {
   constexpr int kKeySpace = 4096;  // bit-plane keys are 12-bit (Core/idx2Lookup.h:21)
+  stage_timer tt;
   // events by (level, subband), in order
   {
     std::map<std::pair<int, int>, size_t> gi;
@@ -473,9 +473,10 @@ int packer::finish()
   const int end_bp = f_.type == dtype::float32 ? 32 : 64;
   const int bpc = f_.bit_planes_per_chunk;
   std::atomic<int> err{ 0 };
+  tt.lap("pack.groups");
 
   // the state machine of every (level, subband) (Core/idx2Encode.cpp:41-137, :157-249)
-  run_parallel(groups_.size(), [&](size_t gidx) {
+  parallel_for(groups_.size(), [&](size_t gidx) {
     group& g = *groups_[gidx];
     const int L = g.level;
     const u64 bpc_bricks = (u64)f_.bricks_per_chunk[(size_t)L];
@@ -587,6 +588,7 @@ int packer::finish()
   });
   if (err)
     return err;
+  tt.lap("pack.channels");
 
   // FlushChunks (Core/idx2Write.cpp:317): every channel in channel-key order
   {
@@ -618,6 +620,7 @@ int packer::finish()
       gs[i]->write_exps(kFinalFlush, (uint32_t)i);
   }
 
+  tt.lap("pack.flush");
   // bit-plane chunks in the sequential order: statistics and files
   struct chunk_ref
   {
@@ -637,12 +640,12 @@ int packer::finish()
     stats_.brick_sizes.add(c.sizes_bytes);
     stats_.bit_plane_chunks.add((double)c.bytes);
     file_buffer& fb = files_[file_path(f_, c.last_brick, cr.level)];
-    for (const segment& sg : c.parts)
-      fb.append_ref(sg.p, sg.n);
+    fb.append_run(c.parts.data(), c.parts.size(), c.bytes);
     fb.has_chunks = true;
     fb.chunk_sizes.put_varbyte(c.bytes);
     fb.chunk_addrs.push_back(chunk_address(f_, c.last_brick, cr.level, cr.subband, c.bpkey));
   }
+  tt.lap("pack.chunk_files");
   // exponent chunks in the sequential order, compressed in parallel
   struct exp_ref
   {
@@ -656,7 +659,7 @@ int packer::finish()
   std::sort(exps.begin(), exps.end(), [](const exp_ref& a, const exp_ref& b) { return stamp_less(a.e, b.e); });
   for (const exp_ref& er : exps)
     stats_.exp_chunks_raw.add((double)er.e->raw.size());
-  run_parallel(exps.size(), [&](size_t i) {
+  parallel_for(exps.size(), [&](size_t i) {
     if (zstd_compress(exps[i].e->raw.data(), exps[i].e->raw.size(), &exps[i].e->z))
       err = UnknownError;
   });
@@ -671,6 +674,7 @@ int packer::finish()
     fb.exp_addrs.push_back(chunk_address(f_, er.e->last_brick, er.level, er.subband, 0));
   }
 
+  tt.lap("pack.exponents");
   // file tails
   for (auto& kv : files_)
   {
@@ -725,6 +729,7 @@ int packer::finish()
     put_i32(&tail, (int32_t)total);
     fb.append_owned(std::move(tail));
   }
+  tt.lap("pack.tails");
   return NoError;
 }
 

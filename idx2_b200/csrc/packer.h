@@ -77,10 +77,20 @@ struct segment
   size_t n;
 };
 
+// Consecutive segments of a file: a whole bit-plane chunk (header, then its bricks' data),
+// or one piece of the tail.
+struct segment_run
+{
+  const segment* seg;
+  size_t nseg;
+  size_t bytes;
+};
+
 struct file_buffer
 {
-  std::vector<segment> parts;                       // file content, in order
+  std::vector<segment_run> parts;                   // file content, in order
   std::deque<std::vector<uint8_t>> owned;           // bytes the parts point into
+  std::deque<segment> singles;                      // the segments of one-segment runs
   size_t nbytes = 0;
   bit_writer chunk_sizes;                           // varbyte sizes of bit-plane chunks
   std::vector<u64> chunk_addrs;                     // chunk addresses
@@ -90,6 +100,15 @@ struct file_buffer
   bool has_exps = false;
   void append_owned(std::vector<uint8_t>&& v);
   void append_ref(const uint8_t* p, size_t n);
+  // n segments that stay in place while the file is alive
+  void append_run(const segment* s, size_t n, size_t bytes);
+  template <typename F>
+  void for_each_segment(F&& fn) const
+  {
+    for (const segment_run& r : parts)
+      for (size_t k = 0; k < r.nseg; ++k)
+        fn(r.seg[k]);
+  }
 };
 
 // The packer records the (brick, subband) results in the reference's encode order and, at
@@ -106,6 +125,8 @@ public:
   // One EncodeSubband call of the reference (Core/idx2Encode.cpp:261); r's arrays must
   // outlive the packer.
   int add(const subband_result& r);
+  // add() of every result, in order
+  int add_all(std::vector<subband_result>&& rs);
   // Channel / chunk state machine, FlushChunks + FlushChunkExponents (Core/idx2Write.cpp:317,
   // :121), file assembly.
   int finish();
