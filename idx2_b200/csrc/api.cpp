@@ -1,6 +1,7 @@
 // C ABI of the library (include/idx2g.h).
 #include "../../include/idx2g.h"
 
+#include "decode_device.h"
 #include "decoder.h"
 #include "device.h"
 #include "encoder.h"
@@ -160,6 +161,7 @@ IDX2G_API int idx2g_ctx_destroy(idx2g_ctx* c)
   c->d.release();
   if (c->d.own_stream && c->d.stream)
     cudaStreamDestroy(c->d.stream);
+  trim_dataset_pool(c->d.device);
   delete c;
   return NoError;
 }
@@ -190,13 +192,21 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
   const size_t bytes = (size_t)prod(p.dims) * (f32 ? 4 : 8);
   auto t0 = std::chrono::steady_clock::now();
   const void* d_field = field;
+  const void* host_field = nullptr;
   if (!field_on_device)
   {
-    // the field goes to a device buffer of the context's workspace (kept across calls)
+    // the field goes to a device buffer of the context's workspace (kept across calls); from
+    // pinned memory, a 3D field is copied in bands that overlap level 0's launches
     void* staged = c->d.ws("enc.field", bytes);
     if (!staged)
       return OutOfMemory;
-    cudaMemcpyAsync(staged, field, bytes, cudaMemcpyHostToDevice, c->d.stream);
+    cudaPointerAttributes pa;
+    const bool pinned = cudaPointerGetAttributes(&pa, field) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (pinned && p.dims.z > 1 && c->d.copies())
+      host_field = field;
+    else
+      cudaMemcpyAsync(staged, field, bytes, cudaMemcpyHostToDevice, c->d.stream);
     d_field = staged;
   }
   encode_timing tm;
@@ -207,6 +217,7 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
   std::vector<long long> lbytes;
   {
     gpu_coder coder(&c->d, f, d_field, f32);
+    coder.set_host_field(host_field);
     const std::shared_ptr<const encode_plan> plan = c->d.plan_for(f, &e);
     if (!plan)
       return e;

@@ -13,10 +13,12 @@
 //   5  keep the brick for the next level, or crop + cast it into the output grid.
 #include "codec_device.cuh"
 #include "decode_device.h"
+#include "trace.h"
 
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 
 namespace idx2g
@@ -39,26 +41,106 @@ extern "C" __attribute__((visibility("default"))) void idx2g_debug_dec_phase_cyc
 }
 #endif
 
+namespace
+{
+
+// Device memory of open datasets comes from one stream-ordered pool per device that keeps the
+// memory of closed datasets for the next one: on a busy node a cudaMalloc or cudaFree of a
+// dataset's gigabyte-sized blob took from milliseconds to over a second, where the pool's
+// reuse takes microseconds. idx2g_ctx_destroy trims the memory no dataset holds.
+struct dataset_pool
+{
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t stream = nullptr;  // orders the frees
+};
+
+dataset_pool* pool_for(int device)
+{
+  static std::mutex m;
+  static std::map<int, dataset_pool> pools;
+  std::lock_guard<std::mutex> lk(m);
+  auto it = pools.find(device);
+  if (it != pools.end())
+    return it->second.pool ? &it->second : nullptr;
+  dataset_pool& p = pools[device];
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof props);
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  if (cudaMemPoolCreate(&p.pool, &props) != cudaSuccess)
+  {
+    cudaGetLastError();
+    p.pool = nullptr;
+    return nullptr;
+  }
+  uint64_t keep = ~0ull;
+  cudaMemPoolSetAttribute(p.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking) != cudaSuccess)
+  {
+    cudaMemPoolDestroy(p.pool);
+    p.pool = nullptr;
+    return nullptr;
+  }
+  return &p;
+}
+
+// `bytes` of the pool on `stream` (plain cudaMalloc where no pool could be made)
+cudaError_t pool_alloc(int device, void** p, size_t bytes, cudaStream_t stream)
+{
+  dataset_pool* dp = pool_for(device);
+  if (!dp)
+    return cudaMalloc(p, bytes);
+  return cudaMallocFromPoolAsync(p, bytes, dp->pool, stream);
+}
+
+} // namespace
+
+void trim_dataset_pool(int device)
+{
+  dataset_pool* dp = pool_for(device);
+  if (dp)
+  {
+    cudaStreamSynchronize(dp->stream);
+    cudaMemPoolTrimTo(dp->pool, 0);
+  }
+}
+
 decode_device::~decode_device()
 {
-  cudaFree(exps_);
-  cudaFree(kmin_);
-  cudaFree(n_);
-  cudaFree(first_);
-  cudaFree(off_);
-  cudaFree(blob_);
+  void* ps[6] = { exps_, kmin_, n_, first_, off_, blob_ };
+  dataset_pool* dp = pool_for(device_);
+  if (!dp)
+  {
+    for (void* p : ps)
+      cudaFree(p);
+    return;
+  }
+  // kernels of any stream may still read the dataset (as with cudaFree, which waits for the
+  // device): its memory returns to the pool once the device is idle
+  cudaSetDevice(device_);
+  cudaDeviceSynchronize();
+  for (void* p : ps)
+    if (p)
+      cudaFreeAsync(p, dp->stream);
 }
 
 int decode_device::alloc(device_ctx* ctx, size_t nslots, size_t blob_bytes)
 {
   cudaSetDevice(ctx->device);
+  device_ = ctx->device;
+  cudaStream_t st = ctx->stream;
   // the blob is padded with zero bytes for the bit readers' look-ahead
-  if (cudaMalloc((void**)&exps_, nslots * kMaxBlocksPerSubband * sizeof(int16_t) + 16) != cudaSuccess ||
-      cudaMalloc((void**)&kmin_, nslots * sizeof(int32_t) + 16) != cudaSuccess ||
-      cudaMalloc((void**)&n_, nslots * sizeof(int32_t) + 16) != cudaSuccess ||
-      cudaMalloc((void**)&first_, nslots * sizeof(uint64_t) + 16) != cudaSuccess ||
-      cudaMalloc((void**)&blob_, blob_bytes + 32) != cudaSuccess)
+  if (pool_alloc(device_, (void**)&exps_, nslots * kMaxBlocksPerSubband * sizeof(int16_t) + 16, st) != cudaSuccess ||
+      pool_alloc(device_, (void**)&kmin_, nslots * sizeof(int32_t) + 16, st) != cudaSuccess ||
+      pool_alloc(device_, (void**)&n_, nslots * sizeof(int32_t) + 16, st) != cudaSuccess ||
+      pool_alloc(device_, (void**)&first_, nslots * sizeof(uint64_t) + 16, st) != cudaSuccess ||
+      pool_alloc(device_, (void**)&blob_, blob_bytes + 32, st) != cudaSuccess)
+  {
+    cudaGetLastError();
     return OutOfMemory;
+  }
   cudaMemsetAsync(blob_ + blob_bytes, 0, 32, ctx->stream);
   nslots_ = nslots;
   blob_bytes_ = blob_bytes;
@@ -77,8 +159,13 @@ int decode_device::upload_tables(device_ctx* ctx, const int16_t* exps, const int
 {
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
-  if (cudaMalloc((void**)&off_, nchan * sizeof(uint64_t) + 16) != cudaSuccess)
+  stage_timer tt;
+  if (pool_alloc(device_, (void**)&off_, nchan * sizeof(uint64_t) + 16, st) != cudaSuccess)
+  {
+    cudaGetLastError();
     return OutOfMemory;
+  }
+  tt.lap("open.upload.alloc");
   const size_t ns = nslots_;
   if (ns)
   {
@@ -94,6 +181,7 @@ int decode_device::upload_tables(device_ctx* ctx, const int16_t* exps, const int
   // the staging buffers are reused by the next open on this context
   if (cudaStreamSynchronize(st) != cudaSuccess)
     return CudaError;
+  tt.lap("open.upload.wait");
   return NoError;
 }
 

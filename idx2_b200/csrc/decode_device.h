@@ -116,7 +116,11 @@ private:
   uint8_t* blob_ = nullptr;
   size_t blob_bytes_ = 0;
   size_t nslots_ = 0;
+  int device_ = 0;
   size_t resident_ = 0;
 };
+
+// Give the device memory that no open dataset holds back to the driver.
+void trim_dataset_pool(int device);
 
 } // namespace idx2g

@@ -280,6 +280,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     files.push_back(df);
   }
 
+  tt.lap("open.files");
   // every file into one pinned buffer, in ranges of 16 MB read by a pool of threads; each
   // range goes on to the device as soon as it is read, while the other threads read on and
   // the index below is built
@@ -288,6 +289,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     return OutOfMemory;
   if (int ae = h->dev.alloc(ctx, nslots, total))
     return ae;
+  tt.lap("open.alloc");
   {
     struct range
     {
@@ -943,7 +945,12 @@ int dataset_decode_brick_map(device_ctx* ctx, dataset_handle* h, const params& p
   return ok ? NoError : FileWriteFailed;
 }
 
-void dataset_close(dataset_handle* h) { delete h; }
+void dataset_close(dataset_handle* h)
+{
+  stage_timer tt;
+  delete h;
+  tt.lap("close");
+}
 
 int dataset_decode_noalloc(device_ctx* ctx, dataset_handle* h, const params& p, void* d_out, size_t out_bytes,
                            double* kernel_ms)

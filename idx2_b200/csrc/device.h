@@ -200,6 +200,10 @@ public:
   int prepare(const batch_tuning& t);
   int nlevels() const { return (int)levels_.size(); }
   int enqueue_level(int l);
+  // Level 0 of one 3D field whose samples are in pinned host memory: bands of brick rows are
+  // copied to `staged` on the context's copy stream, each band's launch waits for its copy
+  // only. *nbands: launches made (timed by event pairs 2g, 2g + 1 of the context's pool).
+  int enqueue_level0_streamed(const void* host, void* staged, int* nbands);
   // Wait for level l, relaunch it with more room if its streams overflowed, read back the
   // region offsets and streams (unless keep_device) into the fields' level outputs.
   int collect_level(int l, bool keep_device);
@@ -231,6 +235,9 @@ public:
   void value_range(double* vmin, double* vmax) override;
   // Leave the coder output on the device (no copies for the packer).
   void set_keep_device(bool v) { keep_device_ = v; }
+  // The field's samples are in pinned host memory `host`; d_field (given at construction) is
+  // the device buffer they go to, copied while level 0 runs.
+  void set_host_field(const void* host) { host_field_ = host; }
   double kernel_ms() const { return enc_ ? enc_->kernel_ms() : 0.0; }
   long long kernel_launches() const { return enc_ ? enc_->launches() : 0; }
   long long stream_bytes() const { return fields_[0].stream_bytes; }
@@ -242,6 +249,7 @@ private:
   device_ctx* ctx_;
   const dataset_format& f_;
   bool keep_device_ = false;
+  const void* host_field_ = nullptr;
   std::vector<level_output> outs_;
   std::vector<batch_field> fields_;
   std::unique_ptr<batch_encoder> enc_;

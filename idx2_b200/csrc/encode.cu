@@ -16,6 +16,7 @@
 #include "encoder.h"
 #include "trace.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -100,6 +101,8 @@ constexpr int kNB3 = 33 * 33 * 33;  // brick stride of slots and parent arrays (
 struct enc_args
 {
   int level, nbricks;
+  int first, last;    // the launch codes entries [first, last) of the brick list, or of `order`
+  const int* order;   // null, or the brick of each entry
   int planes;  // plane capacity per block in shared memory (32 or 64)
   const enc_field* fields;
   const enc_brick* bricks;
@@ -270,8 +273,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
     sm.perm2[tid] = dev::perm(2, tid);
   ENC_PHASE_INIT
 
-  for (int bi = blockIdx.x; bi < a.nbricks; bi += gridDim.x)
+  for (int it = a.first + (int)blockIdx.x; it < a.last; it += gridDim.x)
   {
+    const int bi = a.order ? a.order[it] : it;
     const enc_brick& br = a.bricks[bi];
     {
       // the field's parameters to shared memory (read often, and across barriers)
@@ -530,8 +534,11 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
     for (int s = 0; s < fp.nsb; ++s)
     {
       // towards the end of the brick, ask L2 for the rows of this CTA's next brick
-      if (a.level == 0 && s == (fp.nsb * 5) / 8 && bi + (int)gridDim.x < a.nbricks)
-        prefetch_rows(a.fields[a.bricks[bi + gridDim.x].field], a.bricks[bi + gridDim.x]);
+      if (a.level == 0 && s == (fp.nsb * 5) / 8 && it + (int)gridDim.x < a.last)
+      {
+        const int nx = a.order ? a.order[it + gridDim.x] : it + (int)gridDim.x;
+        prefetch_rows(a.fields[a.bricks[nx].field], a.bricks[nx]);
+      }
       int from[3], dims[3], strd[3];
       subband_grid(fp.is2d, s, from, dims, strd);
       const int nb = fp.nblocks[s];
@@ -1096,6 +1103,9 @@ int batch_encoder::prepare(const batch_tuning& t)
     memset(&a, 0, sizeof a);
     a.level = l;
     a.nbricks = nbr;
+    a.first = 0;
+    a.last = nbr;
+    a.order = nullptr;
     a.planes = ll.planes;
     a.fields = ll.d_fields;
     a.bricks = ll.d_bricks;
@@ -1136,6 +1146,89 @@ int batch_encoder::enqueue_level(int l)
     ++launches_;
     ++ctx_->launches;
   }
+  return cudaGetLastError() == cudaSuccess ? NoError : CudaError;
+}
+
+int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* nbands)
+{
+  *nbands = 0;
+  level_launch& ll = *levels_[0];
+  cudaStream_t st = ctx_->stream, cs = ctx_->copies();
+  const int nbr = ll.args.nbricks;
+  if (!cs || ll.fields.size() != 1 || ll.fields[0].is2d || nbr <= 0)
+    return InvalidArgument;
+  const enc_field& ef = ll.fields[0];
+  const size_t plane = (size_t)ef.fdims[0] * (size_t)ef.fdims[1] * (ef.field_f32 ? 4 : 8);
+  const long long nz = ef.fdims[2];
+  // entries by brick row (z); bands of whole rows, about kBands of them
+  std::vector<int> order((size_t)nbr);
+  for (int i = 0; i < nbr; ++i)
+    order[(size_t)i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return ll.bricks[(size_t)x].b3[2] < ll.bricks[(size_t)y].b3[2]; });
+  constexpr int kBands = 16;
+  std::vector<int> cuts(1, 0);
+  auto row = [&](int i) { return ll.bricks[(size_t)order[(size_t)i]].b3[2]; };
+  for (int g = 1; g < kBands; ++g)
+  {
+    int c = (int)((long long)nbr * g / kBands);
+    while (c > 0 && c < nbr && row(c) == row(c - 1))
+      ++c;
+    if (c > cuts.back() && c < nbr)
+      cuts.push_back(c);
+  }
+  cuts.push_back(nbr);
+  const int nb = (int)cuts.size() - 1;
+  int* d_order = (int*)ctx_->ws("enc.order", (size_t)nbr * 4);
+  int* h_order = (int*)ctx_->pinned("enc.order", (size_t)nbr * 4);
+  if (!d_order || !h_order)
+    return OutOfMemory;
+  memcpy(h_order, order.data(), (size_t)nbr * 4);
+  cudaMemcpyAsync(d_order, h_order, (size_t)nbr * 4, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(ll.d_misc, 0, 64, st);
+  if (ll.nparents > 0)
+    cudaMemsetAsync(ll.d_parents, 0, (size_t)ll.nparents * (size_t)kNB3 * 8, st);
+  // the copy stream starts after the work already on the stream (the staging buffer may
+  // still be read by it)
+  cudaEvent_t start = ctx_->ev(127);
+  if (!start)
+    return CudaError;
+  cudaEventRecord(start, st);
+  cudaStreamWaitEvent(cs, start, 0);
+  // every band's planes on the copy stream, then each band's launch after its copy
+  for (int g = 0; g < nb; ++g)
+  {
+    const long long z0 = (long long)row(cuts[(size_t)g]) * 32;
+    long long z1 = ((long long)row(cuts[(size_t)g + 1] - 1) + 1) * 32;
+    z1 = z1 < nz ? z1 : nz;
+    if (g + 1 == nb)
+      z1 = nz;
+    cudaEvent_t ce = ctx_->ev(128 + (size_t)g);
+    if (!ce)
+      return CudaError;
+    if (z1 > z0)
+      cudaMemcpyAsync((uint8_t*)staged + (size_t)z0 * plane, (const uint8_t*)host + (size_t)z0 * plane,
+                      (size_t)(z1 - z0) * plane, cudaMemcpyHostToDevice, cs);
+    cudaEventRecord(ce, cs);
+  }
+  for (int g = 0; g < nb; ++g)
+  {
+    cudaEvent_t t0 = ctx_->ev(2 * (size_t)g), t1 = ctx_->ev(2 * (size_t)g + 1);
+    if (!t0 || !t1)
+      return CudaError;
+    cudaStreamWaitEvent(st, ctx_->ev(128 + (size_t)g), 0);
+    cudaEventRecord(t0, st);
+    enc_args a = ll.args;
+    a.first = cuts[(size_t)g];
+    a.last = cuts[(size_t)g + 1];
+    a.order = d_order;
+    const int n = a.last - a.first;
+    k_encode_level<<<n < ll.grid ? n : ll.grid, kThreads, ll.smem, st>>>(a);
+    cudaEventRecord(t1, st);
+    ++launches_;
+    ++ctx_->launches;
+  }
+  *nbands = nb;
   return cudaGetLastError() == cudaSuccess ? NoError : CudaError;
 }
 
@@ -1336,16 +1429,36 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     return UnknownError;
   const double before = enc_->kernel_ms();
   stage_timer tt;
-  cudaEventRecord(ctx_->ev0, st);
-  int e = enc_->enqueue_level(level);
-  cudaEventRecord(ctx_->ev1, st);
-  if (e)
-    return e;
-  if (cudaStreamSynchronize(st) != cudaSuccess)
-    return CudaError;
-  tt.lap(level == 0 ? "encode.level0" : level == 1 ? "encode.level1" : "encode.level2+");
   float ms = 0;
-  cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
+  if (level == 0 && host_field_)
+  {
+    // the field is still in pinned host memory: its copy overlaps the level's launches
+    int nb = 0;
+    int e = enc_->enqueue_level0_streamed(host_field_, (void*)fields_[0].d_field, &nb);
+    if (e)
+      return e;
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    for (int g = 0; g < nb; ++g)
+    {
+      float m = 0;
+      cudaEventElapsedTime(&m, ctx_->ev(2 * (size_t)g), ctx_->ev(2 * (size_t)g + 1));
+      ms += m;
+    }
+  }
+  else
+  {
+    cudaEventRecord(ctx_->ev0, st);
+    int e = enc_->enqueue_level(level);
+    cudaEventRecord(ctx_->ev1, st);
+    if (e)
+      return e;
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
+  }
+  tt.lap(level == 0 ? "encode.level0" : level == 1 ? "encode.level1" : "encode.level2+");
+  int e = NoError;
   e = enc_->collect_level(level, keep_device_);
   if (e)
     return e;

@@ -9,6 +9,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <dlfcn.h>
 #include <fcntl.h>
@@ -185,8 +186,9 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
 {
   // Every file is cut into ranges of whole runs of about kRange bytes, copied by a pool of
   // threads. Large files are written through a shared mapping (writes to one file through
-  // write(2) are serialised by the kernel); small files, and any file that cannot be mapped,
-  // with pwrite from a staging buffer.
+  // write(2) are serialised by the kernel), their pages allocated up front in one call where
+  // the file system allows it (page faults of the copies then find the pages in place);
+  // small files, and any file that cannot be mapped, with pwrite from a staging buffer.
   constexpr size_t kRange = (size_t)16 << 20;
   constexpr size_t kMapMin = (size_t)64 << 20;
   struct range
@@ -212,7 +214,7 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
       err = FileCreateFailed;
       break;
     }
-    if (total >= kMapMin && ftruncate(fds[i], (off_t)total) == 0)
+    if (total >= kMapMin && (fallocate(fds[i], 0, 0, (off_t)total) == 0 || ftruncate(fds[i], (off_t)total) == 0))
     {
       void* m = mmap(nullptr, total, PROT_WRITE, MAP_SHARED, fds[i], 0);
       if (m != MAP_FAILED)
@@ -448,9 +450,341 @@ static void put_i32(std::vector<uint8_t>* v, int32_t x)
   v->insert(v->end(), b, b + 4);
 }
 
+// ----------------------------------------------------------------------------
+// channel state machine
+// ----------------------------------------------------------------------------
+
+namespace
+{
+
+bool pack_sequential()
+{
+  static const bool on = std::getenv("IDX2G_PACK_SEQUENTIAL") != nullptr;
+  return on;
+}
+
+constexpr int kKeySpace = 4096;  // bit-plane keys are 12-bit (Core/idx2Lookup.h:21)
+
+struct machine
+{
+  const std::vector<subband_result>& events;
+  const dataset_format& f;
+  int etol, end_bp, bpc;
+
+  // keys of r's coded planes in first-touch order: blocks in Morton order, planes top-down
+  void touch_order(const subband_result& r, std::vector<int>* order, std::vector<char>* seen) const
+  {
+    order->clear();
+    if (r.kmin > r.kmax)
+      return;
+    seen->assign((size_t)(r.kmax - r.kmin + 1), 0);
+    for (int b = 0; b < r.nexps; ++b)
+    {
+      const int emax = r.exps[b];
+      for (int bp = 63; bp >= 64 - end_bp; --bp)
+      {
+        if (!plane_coded(bp, emax, etol, bpc))
+          break;
+        const int key = (bp + emax + 1024) / bpc;
+        if (key < r.kmin || key > r.kmax)
+          continue;
+        char& sn = (*seen)[(size_t)(key - r.kmin)];
+        if (!sn)
+        {
+          sn = 1;
+          order->push_back(key);
+        }
+      }
+    }
+  }
+
+  // exponents of one brick (Core/idx2Encode.cpp:41 EncodeBrickSubbandExponents)
+  void append_exps(const subband_result& r, std::vector<uint8_t>* out) const
+  {
+    const size_t at = out->size();
+    if (f.type == dtype::float64)
+    {
+      out->resize(at + 2 * (size_t)r.nexps);
+      for (int i = 0; i < r.nexps; ++i)
+      {
+        const uint16_t v = (uint16_t)(r.exps[i] + 1023);
+        (*out)[at + 2 * (size_t)i] = (uint8_t)(v & 0xFF);
+        (*out)[at + 2 * (size_t)i + 1] = (uint8_t)(v >> 8);
+      }
+    }
+    else
+    {
+      out->resize(at + (size_t)r.nexps);
+      for (int i = 0; i < r.nexps; ++i)
+        (*out)[at + (size_t)i] = (uint8_t)(r.exps[i] + 127);
+    }
+  }
+};
+
+// brick metadata and data of one channel (Core/idx2Encode.cpp:84)
+inline void append_brick(channel& c, u64 brick, const uint8_t* p, uint32_t nb)
+{
+  if (c.nbricks == 0)
+    c.deltas.put_varbyte(brick);
+  else
+    c.deltas.put_unary(brick - c.last_brick - 1);
+  c.sizes.put_varbyte(nb);
+  c.bricks.push_back({ p, nb });
+  c.brick_bytes += nb;
+  ++c.nbricks;
+  c.last_brick = brick;
+}
+
+inline bool bad_keys(const subband_result& r)
+{
+  return r.kmin <= r.kmax && (r.kmin < 0 || r.kmax >= kKeySpace);
+}
+
+// The state machine of one group, event by event.
+int run_group(packer::group& g, const machine& m)
+{
+  const int L = g.level;
+  const u64 bpc_bricks = (u64)m.f.bricks_per_chunk[(size_t)L];
+  const int shift = log2_ceil(m.f.bricks_per_chunk[(size_t)L]);
+  std::vector<int> order;
+  std::vector<char> seen;
+  for (uint32_t ei : g.events)
+  {
+    const subband_result& r = m.events[ei];
+    const u64 brick = r.brick;
+    if (bad_keys(r))
+      return InvalidArgument;
+    // pass 1: channels in first-touch order; a channel entering a new chunk flushes the
+    // previous one
+    bool any_new = false;
+    for (int k = r.kmin; k <= r.kmax && !any_new; ++k)
+    {
+      if (!r.sizes[k - r.kmin])
+        continue;
+      const int32_t ci = g.index[(size_t)k];
+      const u64 last_chunk = ci >= 0 ? g.chans[(size_t)ci].last_chunk : 0;
+      any_new = brick >= (last_chunk + 1) * bpc_bricks;
+    }
+    if (any_new)
+    {
+      m.touch_order(r, &order, &seen);
+      uint32_t rank = 0;
+      for (int k : order)
+      {
+        channel& c = g.chan(k);
+        if (brick >= (c.last_chunk + 1) * bpc_bricks)
+        {
+          if (c.brick_bytes)
+            g.write_chunk(c, ei, rank++);
+          c.nbricks = 0;
+          c.last_chunk = brick >> shift;
+        }
+      }
+    }
+    // exponents: a brick in a new chunk flushes the previous exponent chunk
+    if (brick >= (g.exp_last_chunk + 1) * bpc_bricks)
+    {
+      g.write_exps(ei, 0);
+      g.exp_last_chunk = brick >> shift;
+    }
+    m.append_exps(r, &g.brick_exps);
+    g.exp_last_brick = brick;
+    // pass 2: brick metadata and data per channel
+    size_t off = 0;
+    for (int k = r.kmin; k <= r.kmax; ++k)
+    {
+      const uint32_t nb = r.sizes[k - r.kmin];
+      if (!nb)
+        continue;
+      append_brick(g.chan(k), brick, r.bytes + off, nb);
+      off += nb;
+    }
+  }
+  return NoError;
+}
+
+// The events of one group that fall in one chunk, run on their own. With bricks in chunk order,
+// every channel's state at the range's start is the same for the sequential machine: a channel
+// not yet seen in the range enters it at its first touch (flushing what it holds, with the
+// stamp of that event and its place in the touch order), and its data in the range is a
+// chunk of its own; the exponents of the range are one exponent chunk. merge_segments applies
+// the ranges to the group in order.
+struct seg_key
+{
+  channel ch;  // the range's data (after the channel entered)
+  bool entered = false;
+  uint64_t event = 0;
+  uint32_t rank = 0;
+};
+
+struct segment_run
+{
+  packer::group* g = nullptr;
+  size_t e0 = 0, e1 = 0;  // entries of g->events
+  u64 chunk = 0;
+  std::deque<seg_key> keys;
+  std::vector<uint8_t> exps;
+  u64 exp_last_brick = 0;
+  int status = NoError;  // NoError, InvalidArgument, or -1: the range needs the sequential machine
+};
+
+void run_segment(segment_run& s, const machine& m)
+{
+  thread_local std::vector<int32_t> index;
+  if (index.empty())
+    index.assign(kKeySpace, -1);
+  auto key = [&](int k) -> seg_key& {
+    int32_t& i = index[(size_t)k];
+    if (i < 0)
+    {
+      i = (int32_t)s.keys.size();
+      s.keys.emplace_back();
+      s.keys.back().ch.bpkey = k;
+    }
+    return s.keys[(size_t)i];
+  };
+  std::vector<int> order;
+  std::vector<char> seen;
+  for (size_t i = s.e0; i < s.e1 && s.status == NoError; ++i)
+  {
+    const uint32_t ei = s.g->events[i];
+    const subband_result& r = m.events[ei];
+    const u64 brick = r.brick;
+    if (bad_keys(r))
+    {
+      s.status = InvalidArgument;
+      break;
+    }
+    if (s.chunk >= 1)
+    {
+      bool any_new = false;
+      for (int k = r.kmin; k <= r.kmax && !any_new; ++k)
+        any_new = r.sizes[k - r.kmin] && (index[(size_t)k] < 0 || !s.keys[(size_t)index[(size_t)k]].entered);
+      if (any_new)
+      {
+        m.touch_order(r, &order, &seen);
+        for (size_t pos = 0; pos < order.size(); ++pos)
+        {
+          seg_key& st = key(order[pos]);
+          if (!st.entered)
+          {
+            st.entered = true;
+            st.event = ei;
+            st.rank = (uint32_t)pos;
+          }
+        }
+      }
+    }
+    m.append_exps(r, &s.exps);
+    s.exp_last_brick = brick;
+    size_t off = 0;
+    for (int k = r.kmin; k <= r.kmax; ++k)
+    {
+      const uint32_t nb = r.sizes[k - r.kmin];
+      if (!nb)
+        continue;
+      seg_key& st = key(k);
+      if (s.chunk >= 1 && !st.entered)
+      {
+        s.status = -1;  // data of a channel that did not enter: not separable
+        break;
+      }
+      append_brick(st.ch, brick, r.bytes + off, nb);
+      off += nb;
+    }
+  }
+  for (const seg_key& st : s.keys)
+    index[(size_t)st.ch.bpkey] = -1;
+}
+
+void merge_segments(packer::group& g, std::vector<segment_run>& segs)
+{
+  for (segment_run& s : segs)
+  {
+    if (s.chunk >= 1)
+      g.write_exps(g.events[s.e0], 0);
+    for (seg_key& st : s.keys)
+    {
+      channel& c = g.chan(st.ch.bpkey);
+      if (st.entered)
+      {
+        if (c.brick_bytes)
+          g.write_chunk(c, st.event, st.rank);
+        c.nbricks = 0;
+      }
+      if (st.ch.nbricks)
+      {
+        c.deltas = std::move(st.ch.deltas);
+        c.sizes = std::move(st.ch.sizes);
+        c.bricks = std::move(st.ch.bricks);
+        c.brick_bytes = st.ch.brick_bytes;
+        c.nbricks = st.ch.nbricks;
+        c.last_brick = st.ch.last_brick;
+      }
+    }
+    g.brick_exps = std::move(s.exps);
+    g.exp_last_brick = s.exp_last_brick;
+  }
+}
+
+int run_machines(std::vector<std::unique_ptr<packer::group>>& groups, const machine& m, bool by_chunk)
+{
+  // chunk ranges of every group whose bricks come in chunk order
+  std::vector<std::vector<segment_run>> segs(groups.size());
+  std::vector<std::pair<size_t, size_t>> tasks;
+  if (by_chunk)
+    for (size_t gi = 0; gi < groups.size(); ++gi)
+    {
+      packer::group& g = *groups[gi];
+      const int shift = log2_ceil(m.f.bricks_per_chunk[(size_t)g.level]);
+      std::vector<segment_run>& v = segs[gi];
+      bool ordered = true;
+      for (size_t i = 0; i < g.events.size() && ordered; ++i)
+      {
+        const u64 c = m.events[g.events[i]].brick >> shift;
+        if (v.empty() || c != v.back().chunk)
+        {
+          ordered = v.empty() || c > v.back().chunk;
+          v.emplace_back();
+          v.back().g = &g;
+          v.back().e0 = i;
+          v.back().chunk = c;
+        }
+        v.back().e1 = i + 1;
+      }
+      if (!ordered)
+        v.clear();
+      for (size_t k = 0; k < v.size(); ++k)
+        tasks.push_back({ gi, k });
+    }
+  parallel_for(tasks.size(), [&](size_t t) { run_segment(segs[tasks[t].first][tasks[t].second], m); });
+  std::atomic<int> err{ 0 };
+  std::atomic<int> merged{ 0 };
+  parallel_for(groups.size(), [&](size_t gi) {
+    bool separable = !segs[gi].empty();
+    for (const segment_run& s : segs[gi])
+    {
+      if (s.status > 0)
+        err = s.status;
+      separable = separable && s.status == NoError;
+    }
+    if (separable)
+    {
+      merge_segments(*groups[gi], segs[gi]);
+      ++merged;
+    }
+    else if (int e = run_group(*groups[gi], m))
+      err = e;
+  });
+  if (trace_on())
+    fprintf(stderr, "idx2g pack.groups_by_chunk %d of %zu (%zu ranges)\n", merged.load(), groups.size(), tasks.size());
+  return err;
+}
+
+} // namespace
+
 int packer::finish()
 {
-  constexpr int kKeySpace = 4096;  // bit-plane keys are 12-bit (Core/idx2Lookup.h:21)
   stage_timer tt;
   // events by (level, subband), in order
   {
@@ -475,119 +809,12 @@ int packer::finish()
   std::atomic<int> err{ 0 };
   tt.lap("pack.groups");
 
-  // the state machine of every (level, subband) (Core/idx2Encode.cpp:41-137, :157-249)
-  parallel_for(groups_.size(), [&](size_t gidx) {
-    group& g = *groups_[gidx];
-    const int L = g.level;
-    const u64 bpc_bricks = (u64)f_.bricks_per_chunk[(size_t)L];
-    const int shift = log2_ceil(f_.bricks_per_chunk[(size_t)L]);
-    std::vector<int> order;
-    std::vector<char> seen;
-    for (uint32_t ei : g.events)
-    {
-      const subband_result& r = events_[ei];
-      const u64 brick = r.brick;
-      if (r.kmin <= r.kmax && (r.kmin < 0 || r.kmax >= kKeySpace))
-      {
-        err = InvalidArgument;
-        return;
-      }
-      // pass 1: channels in first-touch order (blocks in Morton order, planes top-down);
-      // a channel entering a new chunk flushes the previous one
-      bool any_new = false;
-      for (int k = r.kmin; k <= r.kmax && !any_new; ++k)
-      {
-        if (!r.sizes[k - r.kmin])
-          continue;
-        const int32_t ci = g.index[(size_t)k];
-        const u64 last_chunk = ci >= 0 ? g.chans[(size_t)ci].last_chunk : 0;
-        any_new = brick >= (last_chunk + 1) * bpc_bricks;
-      }
-      if (any_new)
-      {
-        order.clear();
-        if (r.kmin <= r.kmax)
-        {
-          seen.assign((size_t)(r.kmax - r.kmin + 1), 0);
-          for (int b = 0; b < r.nexps; ++b)
-          {
-            const int emax = r.exps[b];
-            for (int bp = 63; bp >= 64 - end_bp; --bp)
-            {
-              if (!plane_coded(bp, emax, etol_, bpc))
-                break;
-              const int key = (bp + emax + 1024) / bpc;
-              if (key < r.kmin || key > r.kmax)
-                continue;
-              char& sn = seen[(size_t)(key - r.kmin)];
-              if (!sn)
-              {
-                sn = 1;
-                order.push_back(key);
-              }
-            }
-          }
-        }
-        uint32_t rank = 0;
-        for (int k : order)
-        {
-          channel& c = g.chan(k);
-          if (brick >= (c.last_chunk + 1) * bpc_bricks)
-          {
-            if (c.brick_bytes)
-              g.write_chunk(c, ei, rank++);
-            c.nbricks = 0;
-            c.last_chunk = brick >> shift;
-          }
-        }
-      }
-      // exponents (Core/idx2Encode.cpp:41 EncodeBrickSubbandExponents)
-      if (brick >= (g.exp_last_chunk + 1) * bpc_bricks)
-      {
-        g.write_exps(ei, 0);
-        g.exp_last_chunk = brick >> shift;
-      }
-      const size_t at = g.brick_exps.size();
-      if (f_.type == dtype::float64)
-      {
-        g.brick_exps.resize(at + 2 * (size_t)r.nexps);
-        for (int i = 0; i < r.nexps; ++i)
-        {
-          const uint16_t v = (uint16_t)(r.exps[i] + 1023);
-          g.brick_exps[at + 2 * (size_t)i] = (uint8_t)(v & 0xFF);
-          g.brick_exps[at + 2 * (size_t)i + 1] = (uint8_t)(v >> 8);
-        }
-      }
-      else
-      {
-        g.brick_exps.resize(at + (size_t)r.nexps);
-        for (int i = 0; i < r.nexps; ++i)
-          g.brick_exps[at + (size_t)i] = (uint8_t)(r.exps[i] + 127);
-      }
-      g.exp_last_brick = brick;
-      // pass 2: brick metadata and data per channel (Core/idx2Encode.cpp:84)
-      size_t off = 0;
-      for (int k = r.kmin; k <= r.kmax; ++k)
-      {
-        const uint32_t nb = r.sizes[k - r.kmin];
-        if (!nb)
-          continue;
-        channel& c = g.chan(k);
-        if (c.nbricks == 0)
-          c.deltas.put_varbyte(brick);
-        else
-          c.deltas.put_unary(brick - c.last_brick - 1);
-        c.sizes.put_varbyte(nb);
-        c.bricks.push_back({ r.bytes + off, nb });
-        c.brick_bytes += nb;
-        off += nb;
-        ++c.nbricks;
-        c.last_brick = brick;
-      }
-    }
-  });
-  if (err)
-    return err;
+  // the state machine of every (level, subband) (Core/idx2Encode.cpp:41-137, :157-249): over
+  // the group's chunk ranges in parallel where the group allows it, else in event order
+  const machine m{ events_, f_, etol_, end_bp, bpc };
+  int e = run_machines(groups_, m, !pack_sequential());
+  if (e)
+    return e;
   tt.lap("pack.channels");
 
   // FlushChunks (Core/idx2Write.cpp:317): every channel in channel-key order

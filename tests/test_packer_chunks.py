@@ -45,8 +45,12 @@ def ref_encode_chunked(ref_app, tmp, f, case):
     return raw, os.path.join(tmp, "ref", "kat")
 
 
+@pytest.mark.parametrize("machine", ["by_chunk", "sequential"])
 @pytest.mark.parametrize("case", CHUNK_CASES, ids=chunk_case_id)
-def test_packer_chunk_boundaries(ref_app, tmp_path, case):
+def test_packer_chunk_boundaries(ref_app, tmp_path, case, machine):
+    """The channel state machine run over each group's chunk ranges in parallel (the default)
+    and event by event (IDX2G_PACK_SEQUENTIAL) both give the reference's files; with IDX2G_TRACE
+    the packer reports how many groups took the chunk-range path (all of them here)."""
     dims, dtype, levels, tol, bd, bpc, cpf, fpd, seed = case
     f = chunk_field(dims, dtype, seed)
     raw, ref_dir = ref_encode_chunked(ref_app, str(tmp_path), f, case)
@@ -55,7 +59,15 @@ def test_packer_chunk_boundaries(ref_app, tmp_path, case):
     exe = build_oracle_encode()
     args = [exe, raw, str(dims[0]), str(dims[1]), str(dims[2]), dtype, str(levels), repr(tol),
             str(tmp_path / "o"), "kat", "f"] + [str(b) for b in bd] + [str(bpc), str(cpf), str(fpd)]
-    r = subprocess.run(args, capture_output=True, text=True)
+    env = dict(os.environ, IDX2G_TRACE="1")
+    env.pop("IDX2G_PACK_SEQUENTIAL", None)
+    if machine == "sequential":
+        env["IDX2G_PACK_SEQUENTIAL"] = "1"
+    r = subprocess.run(args, capture_output=True, text=True, env=env)
     assert r.returncode == 0, r.stderr
+    by_chunk = [ln.split() for ln in r.stderr.splitlines() if ln.startswith("idx2g pack.groups_by_chunk")]
+    assert len(by_chunk) == 1
+    merged, total = int(by_chunk[0][2]), int(by_chunk[0][4])
+    assert merged == (total if machine == "by_chunk" else 0), by_chunk
     diffs = compare_dirs(ref_dir, str(tmp_path / "o" / "kat"))
     assert diffs == [], diffs[:3]
