@@ -24,13 +24,20 @@ struct device_ctx
   int num_sms = 148;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> evpool;  // timing events of calls that time several launches
-  // second stream for host copies that overlap the kernels of `stream` (created on first use)
-  cudaStream_t copy_stream = nullptr;
+  // streams for host copies that overlap the kernels of `stream`, one per direction (created
+  // on first use)
+  cudaStream_t copy_stream = nullptr, copy_out_stream = nullptr;
   cudaStream_t copies()
   {
     if (!copy_stream && cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking) != cudaSuccess)
       copy_stream = nullptr;
     return copy_stream;
+  }
+  cudaStream_t copies_out()
+  {
+    if (!copy_out_stream && cudaStreamCreateWithFlags(&copy_out_stream, cudaStreamNonBlocking) != cudaSuccess)
+      copy_out_stream = nullptr;
+    return copy_out_stream;
   }
   long long launches = 0;  // kernels launched on this context so far
   std::map<std::string, int> tuned;  // batched encode: CTAs per SM chosen per batch signature
@@ -114,6 +121,11 @@ struct device_ctx
   }
   // Pinned host buffer of at least `bytes` bytes (grow-only, kept across calls).
   std::map<std::string, buf> pins;
+  size_t pinned_size(const std::string& name)
+  {
+    auto it = pins.find(name);
+    return it == pins.end() ? 0 : it->second.n;
+  }
   void* pinned(const std::string& name, size_t bytes)
   {
     buf& b = pins[name];
@@ -144,12 +156,13 @@ struct device_ctx
   }
   void release()
   {
-    if (copy_stream)
-    {
-      cudaStreamSynchronize(copy_stream);
-      cudaStreamDestroy(copy_stream);
-      copy_stream = nullptr;
-    }
+    for (cudaStream_t* s : { &copy_stream, &copy_out_stream })
+      if (*s)
+      {
+        cudaStreamSynchronize(*s);
+        cudaStreamDestroy(*s);
+        *s = nullptr;
+      }
     for (cudaEvent_t e : evpool)
       cudaEventDestroy(e);
     evpool.clear();
@@ -204,6 +217,10 @@ public:
   // copied to `staged` on the context's copy stream, each band's launch waits for its copy
   // only. *nbands: launches made (timed by event pairs 2g, 2g + 1 of the context's pool).
   int enqueue_level0_streamed(const void* host, void* staged, int* nbands);
+  // While the bands of enqueue_level0_streamed run: as each band ends, its stream bytes go to
+  // the level's pinned host buffer on the copy-out stream (when the buffer is already large
+  // enough), so that collect_level finds them there.
+  void stream_out_level0(int nbands);
   // Wait for level l, relaunch it with more room if its streams overflowed, read back the
   // region offsets and streams (unless keep_device) into the fields' level outputs.
   int collect_level(int l, bool keep_device);

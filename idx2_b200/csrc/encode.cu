@@ -963,6 +963,7 @@ struct batch_encoder::level_launch
   double* d_parents = nullptr;
   std::string sname;
   enc_args args;
+  unsigned long long prefetched = 0;  // stream bytes copied to the pinned buffer while running
 };
 
 batch_encoder::batch_encoder(device_ctx* ctx, std::vector<batch_field>* fields, const std::string& tag)
@@ -1211,10 +1212,14 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
                       (size_t)(z1 - z0) * plane, cudaMemcpyHostToDevice, cs);
     cudaEventRecord(ce, cs);
   }
+  unsigned long long* h_cur = (unsigned long long*)ctx_->pinned("enc.cursor", (size_t)nb * 8);
+  if (!h_cur)
+    return OutOfMemory;
   for (int g = 0; g < nb; ++g)
   {
     cudaEvent_t t0 = ctx_->ev(2 * (size_t)g), t1 = ctx_->ev(2 * (size_t)g + 1);
-    if (!t0 || !t1)
+    cudaEvent_t tc = ctx_->ev(160 + (size_t)g);
+    if (!t0 || !t1 || !tc)
       return CudaError;
     cudaStreamWaitEvent(st, ctx_->ev(128 + (size_t)g), 0);
     cudaEventRecord(t0, st);
@@ -1225,6 +1230,9 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
     const int n = a.last - a.first;
     k_encode_level<<<n < ll.grid ? n : ll.grid, kThreads, ll.smem, st>>>(a);
     cudaEventRecord(t1, st);
+    // the region cursor after the band: its regions end there
+    cudaMemcpyAsync(h_cur + g, ll.d_misc, 8, cudaMemcpyDeviceToHost, st);
+    cudaEventRecord(tc, st);
     ++launches_;
     ++ctx_->launches;
   }
@@ -1232,10 +1240,43 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
   return cudaGetLastError() == cudaSuccess ? NoError : CudaError;
 }
 
+void batch_encoder::stream_out_level0(int nbands)
+{
+  level_launch& ll = *levels_[0];
+  ll.prefetched = 0;
+  char name[96];
+  snprintf(name, sizeof name, "enc.pin.%s.%d", tag_.c_str(), 0);
+  const size_t room = ctx_->pinned_size(name);
+  cudaStream_t os = ctx_->copies_out();
+  const unsigned long long* h_cur = (const unsigned long long*)ctx_->pinned("enc.cursor", (size_t)nbands * 8);
+  if (!room || !os || !h_cur)
+    return;
+  uint8_t* pin = (uint8_t*)ctx_->pinned(name, room);
+  unsigned long long done = 0;
+  for (int g = 0; g < nbands; ++g)
+  {
+    if (cudaEventSynchronize(ctx_->ev(160 + (size_t)g)) != cudaSuccess)
+      break;
+    const unsigned long long end = h_cur[g];
+    if (end > ll.cap || end > room)
+      break;  // the regions overflowed (the level runs again) or the buffer is short
+    if (end > done)
+      cudaMemcpyAsync(pin + done, (const uint8_t*)ll.args.stream + done, (size_t)(end - done),
+                      cudaMemcpyDeviceToHost, os);
+    done = end;
+  }
+  ll.prefetched = done;
+}
+
 int batch_encoder::collect_level(int l, bool keep_device)
 {
   level_launch& ll = *levels_[(size_t)l];
   cudaStream_t st = ctx_->stream;
+  // copies of this level's streams still in flight end before the buffer is looked at
+  const unsigned long long prefetched = ll.prefetched;
+  ll.prefetched = 0;
+  if (prefetched && cudaStreamSynchronize(ctx_->copies_out()) != cudaSuccess)
+    return CudaError;
   std::vector<batch_field>& J = *fields_;
   const int nbr = ll.args.nbricks;
   unsigned long long misc[2] = { 0, 0 };
@@ -1283,10 +1324,12 @@ int batch_encoder::collect_level(int l, bool keep_device)
     {
       char name[96];
       snprintf(name, sizeof name, "enc.pin.%s.%d", tag_.c_str(), l);
+      const bool have = prefetched == used && ctx_->pinned_size(name) >= (size_t)used;
       pin = (const uint8_t*)ctx_->pinned(name, (size_t)used);
       if (!pin)
         return OutOfMemory;
-      cudaMemcpyAsync((void*)pin, ll.args.stream, (size_t)used, cudaMemcpyDeviceToHost, st);
+      if (!have)
+        cudaMemcpyAsync((void*)pin, ll.args.stream, (size_t)used, cudaMemcpyDeviceToHost, st);
     }
   }
   std::vector<double> mn, mx;
@@ -1437,6 +1480,8 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
     int e = enc_->enqueue_level0_streamed(host_field_, (void*)fields_[0].d_field, &nb);
     if (e)
       return e;
+    if (!keep_device_)
+      enc_->stream_out_level0(nb);
     if (cudaStreamSynchronize(st) != cudaSuccess)
       return CudaError;
     for (int g = 0; g < nb; ++g)
