@@ -221,7 +221,9 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
     const std::shared_ptr<const encode_plan> plan = c->d.plan_for(f, &e);
     if (!plan)
       return e;
-    e = encode_dataset(&f, &p, &coder, nullptr, true, &tm, plan.get());
+    e = encode_dataset(&f, &p, &coder, nullptr, true, &tm, plan.get(), c->d.file_hint(f));
+    if (!e)
+      c->d.set_file_hint(f, tm.level_file_bytes);
     stream_bytes = coder.stream_bytes();
     exp_bytes = coder.exp_bytes();
     kms = coder.kernel_ms();

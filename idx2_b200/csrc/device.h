@@ -47,11 +47,16 @@ struct device_ctx
   // Callers hold the returned pointer for as long as they use the plan: the cache keeps 16
   // shapes and may drop one while an earlier holder still uses it.
   std::map<std::string, std::shared_ptr<const encode_plan>> plans;
-  std::shared_ptr<const encode_plan> plan_for(const dataset_format& f, int* err)
+  static std::string plan_key(const dataset_format& f)
   {
     char key[128];
     snprintf(key, sizeof key, "%d %d %d/%d %d %d/%d", f.dims.x, f.dims.y, f.dims.z, f.brick_dims.x, f.brick_dims.y,
              f.brick_dims.z, f.nlevels);
+    return key;
+  }
+  std::shared_ptr<const encode_plan> plan_for(const dataset_format& f, int* err)
+  {
+    const std::string key = plan_key(f);
     auto it = plans.find(key);
     if (it != plans.end())
       return it->second;
@@ -63,6 +68,27 @@ struct device_ctx
       plans.erase(plans.begin());
     plans[key] = pl;
     return pl;
+  }
+  // Bytes of each level's data file in the last encode of a shape (by plan_key): the next
+  // encode of that shape has the file system allocate about as many pages while its device
+  // stage runs (a guess only: the writer sets every file's size and writes every byte).
+  std::map<std::string, std::vector<unsigned long long>> file_hints;
+  const std::vector<unsigned long long>* file_hint(const dataset_format& f)
+  {
+    auto it = file_hints.find(plan_key(f));
+    return it == file_hints.end() ? nullptr : &it->second;
+  }
+  void set_file_hint(const dataset_format& f, const std::vector<unsigned long long>& sizes)
+  {
+    const std::string key = plan_key(f);
+    if (sizes.empty())
+    {
+      file_hints.erase(key);
+      return;
+    }
+    if (file_hints.size() >= 16 && !file_hints.count(key))
+      file_hints.erase(file_hints.begin());
+    file_hints[key] = sizes;
   }
 
   struct buf

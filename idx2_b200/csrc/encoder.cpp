@@ -8,8 +8,10 @@
 #include <cstdio>
 #include <cstring>
 #include <errno.h>
+#include <fcntl.h>
 #include <functional>
 #include <sys/stat.h>
+#include <unistd.h>
 #include <thread>
 #include <unordered_map>
 
@@ -183,9 +185,37 @@ int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_outpu
   return NoError;
 }
 
+std::thread preallocate_files(const dataset_format& f, const encode_plan& plan,
+                              const std::vector<unsigned long long>& sizes)
+{
+  constexpr unsigned long long kMin = 64ull << 20;
+  std::vector<std::pair<std::string, unsigned long long>> todo;
+  for (int l = 0; l < f.nlevels && l < (int)sizes.size() && l < (int)plan.levels.size(); ++l)
+    if (sizes[(size_t)l] >= kMin && !plan.levels[(size_t)l].empty())
+      todo.push_back({ file_path(f, plan.levels[(size_t)l][0].linear, l), sizes[(size_t)l] });
+  if (todo.empty())
+    return std::thread();
+  return std::thread([todo]() {
+    // the writer sets each file's size and writes every byte, so pages of an older file of
+    // the same name are as good as new ones
+    for (const auto& t : todo)
+    {
+      if (make_dirs_for(t.first) != NoError)
+        continue;
+      const int fd = open(t.first.c_str(), O_RDWR | O_CREAT, 0644);
+      if (fd < 0)
+        continue;
+      if (fallocate(fd, FALLOC_FL_KEEP_SIZE, 0, (off_t)t.second) != 0)
+        errno = 0;
+      close(fd);
+    }
+  });
+}
+
 int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
                    std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
-                   encode_timing* timing, const encode_plan* plan)
+                   encode_timing* timing, const encode_plan* plan,
+                   const std::vector<unsigned long long>* prealloc)
 {
   double t0 = now_s();
   encode_plan local;
@@ -196,12 +226,24 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
       return e;
     plan = &local;
   }
+  std::thread pre;
+  if (write_files && prealloc)
+    pre = preallocate_files(*f, *plan, *prealloc);
+  struct joiner
+  {
+    std::thread& t;
+    ~joiner()
+    {
+      if (t.joinable())
+        t.join();
+    }
+  } join_pre{ pre };
   std::vector<level_output> outs;
   int e = encode_levels(f, coder, &outs, *plan);
   if (e)
     return e;
   double t1 = now_s();
-  e = pack_dataset(f, p, *plan, outs, files, write_files, timing);
+  e = pack_dataset(f, p, *plan, outs, files, write_files, timing, &pre);
   if (timing)
     timing->device_s = t1 - t0;
   return e;
@@ -209,7 +251,7 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
 
 int pack_dataset(const dataset_format* f, const params* p, const encode_plan& plan,
                  const std::vector<level_output>& outs, std::map<std::string, std::vector<uint8_t>>* files,
-                 bool write_files, encode_timing* timing)
+                 bool write_files, encode_timing* timing, std::thread* before_write)
 {
   double t1 = now_s();
   stage_timer tt;
@@ -243,6 +285,27 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
   e = pk.finish();
   if (e)
     return e;
+  if (timing)
+  {
+    timing->level_file_bytes.clear();
+    if ((int)pk.files().size() == f->nlevels && (int)plan.levels.size() >= f->nlevels)
+    {
+      std::vector<unsigned long long> v((size_t)f->nlevels, 0);
+      bool one_each = true;
+      for (int l = 0; l < f->nlevels && one_each; ++l)
+      {
+        one_each = !plan.levels[(size_t)l].empty();
+        if (!one_each)
+          break;
+        auto it = pk.files().find(file_path(*f, plan.levels[(size_t)l][0].linear, l));
+        one_each = it != pk.files().end();
+        if (one_each)
+          v[(size_t)l] = it->second.nbytes;
+      }
+      if (one_each)
+        timing->level_file_bytes = v;
+    }
+  }
   double t2 = now_s();
   tt.t = stage_timer::now();
 
@@ -268,6 +331,8 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
   }
   if (write_files)
   {
+    if (before_write && before_write->joinable())
+      before_write->join();
     e = write_file(meta_path, std::vector<uint8_t>(meta.begin(), meta.end()));
     if (e)
       return e;

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace idx2g
@@ -116,20 +117,32 @@ struct encode_timing
   double device_s = 0, pack_s = 0, write_s = 0;
   unsigned long long file_bytes = 0;  // data files + metadata file
   int nfiles = 0;
+  // bytes of every level's data file when each level has exactly one (else empty)
+  std::vector<unsigned long long> level_file_bytes;
 };
 
 // Full encode: plan, device stage for every level, packing, files (Core/idx2Encode.cpp:390).
 // files (may be null) receives path -> bytes; write_files controls whether they are
 // written to disk (several files at a time).
 // plan (may be null): the format's encode plan, made here when null.
+// prealloc (may be null): expected bytes of each level's data file (one file per level, such as
+// the sizes of the previous encode of this shape); the file system allocates their pages on a
+// thread of its own while the device stage runs.
 int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
                    std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
-                   encode_timing* timing, const encode_plan* plan = nullptr);
+                   encode_timing* timing, const encode_plan* plan = nullptr,
+                   const std::vector<unsigned long long>* prealloc = nullptr);
 
 // Packing and files for the device stage's outputs (the second half of encode_dataset).
+// before_write (may be null) is joined before the first file is opened.
 int pack_dataset(const dataset_format* f, const params* p, const encode_plan& plan,
                  const std::vector<level_output>& outs, std::map<std::string, std::vector<uint8_t>>* files,
-                 bool write_files, encode_timing* timing);
+                 bool write_files, encode_timing* timing, std::thread* before_write = nullptr);
+
+// Allocate the pages of each level's data file (sizes[l] bytes, file size unchanged) on a new
+// thread; levels with fewer than 64 MB are left alone.
+std::thread preallocate_files(const dataset_format& f, const encode_plan& plan,
+                              const std::vector<unsigned long long>& sizes);
 
 // The device stage only: every level through the coder, with the given plan.
 int encode_levels(dataset_format* f, brick_coder* coder, std::vector<level_output>* outs, const encode_plan& plan);

@@ -9,11 +9,13 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cerrno>
 #include <cstdlib>
 #include <cstring>
 #include <dlfcn.h>
 #include <fcntl.h>
 #include <sys/mman.h>
+#include <sys/stat.h>
 #include <thread>
 #include <unistd.h>
 
@@ -208,13 +210,25 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
       break;
     }
     const size_t total = files[i].second->nbytes;
-    fds[i] = open(files[i].first.c_str(), O_RDWR | O_CREAT | O_TRUNC, 0644);
+    // a large file keeps the pages it has (every byte is written, the size set first)
+    fds[i] = open(files[i].first.c_str(), O_RDWR | O_CREAT | (total >= kMapMin ? 0 : O_TRUNC), 0644);
     if (fds[i] < 0)
     {
       err = FileCreateFailed;
       break;
     }
-    if (total >= kMapMin && (fallocate(fds[i], 0, 0, (off_t)total) == 0 || ftruncate(fds[i], (off_t)total) == 0))
+    if (total >= kMapMin && ftruncate(fds[i], (off_t)total) != 0)
+    {
+      err = FileWriteFailed;
+      break;
+    }
+    // pages for the whole file in one call, unless it has them already (allocated ahead, or
+    // an older file's): a second allocation over allocated pages costs more than it saves
+    struct stat sb;
+    if (total >= kMapMin && (fstat(fds[i], &sb) != 0 || (size_t)sb.st_blocks * 512 < total) &&
+        fallocate(fds[i], 0, 0, (off_t)total) != 0)
+      errno = 0;  // pages come with the copies' page faults instead
+    if (total >= kMapMin)
     {
       void* m = mmap(nullptr, total, PROT_WRITE, MAP_SHARED, fds[i], 0);
       if (m != MAP_FAILED)
