@@ -6,6 +6,7 @@
 #include "device.h"
 #include "encoder.h"
 #include "format.h"
+#include "trace.h"
 
 #include <chrono>
 #include <cstdio>
@@ -312,6 +313,7 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
   cudaSetDevice(c->d.device);
   cudaStream_t st = c->d.stream;
   const auto t0 = std::chrono::steady_clock::now();
+  stage_timer tt;
   std::vector<params> ps((size_t)n);
   std::vector<dataset_format> fs((size_t)n);
   std::vector<std::shared_ptr<const encode_plan>> plans((size_t)n);  // held for the whole call
@@ -335,6 +337,7 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
     total_bricks += (long long)plans[(size_t)i]->levels[0].size();
     nf64 += ps[(size_t)i].type == dtype::float64;
   }
+  tt.lap("batch.plans");
   // fields to the device (one staging buffer of the context's workspace)
   std::vector<const void*> dptr((size_t)n);
   if (!fields_on_device)
@@ -400,12 +403,15 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
     }
     tune.ctas_per_sm = it->second;
   }
+  tt.lap("batch.tune");
   batch_encoder enc(&c->d, &bf, "b");
   int e = enc.prepare(tune);
+  tt.lap("batch.prepare");
   if (!e)
     e = enc.run_all(graph, device_only);
   if (e)
     return e;
+  tt.lap("batch.run");
   const auto t1 = std::chrono::steady_clock::now();
   for (int i = 0; i < n; ++i)
   {

@@ -676,8 +676,8 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
       break;
     lmin = l;
   }
-  std::vector<std::vector<int>> sel((size_t)L);  // selected brick indices per level
-  std::vector<std::unordered_map<int, int>> pos_of((size_t)L);
+  // per level and brick index: the brick's entry in the level's list (-1: not decoded)
+  std::vector<std::vector<int>> pos_of((size_t)L);
   for (int l = L - 1; l >= lmin; --l)
   {
     v3 b3 = f.brick_dims;
@@ -685,6 +685,7 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
       b3 = b3 * f.group_brick3;
     v3 bf = ext.from / b3, bl = ext.last() / b3;
     bl = vmin(bl, f.nbricks3[(size_t)l] - v3(1));
+    pos_of[(size_t)l].assign(h->brick3[(size_t)l].size(), -1);
     decode_level lv;
     lv.level = l;
     lv.mask = f.decode_masks[(size_t)l];
@@ -712,8 +713,7 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
             v3 pb = b / f.group_brick3;
             u64 plin = linear_brick(f, l + 1, pb);
             int pbi = plin < h->brick_index[(size_t)l + 1].size() ? h->brick_index[(size_t)l + 1][plin] : -1;
-            auto it = pbi >= 0 ? pos_of[(size_t)l + 1].find(pbi) : pos_of[(size_t)l + 1].end();
-            db.parent = it == pos_of[(size_t)l + 1].end() ? -1 : it->second;
+            db.parent = pbi >= 0 && (size_t)pbi < pos_of[(size_t)l + 1].size() ? pos_of[(size_t)l + 1][(size_t)pbi] : -1;
             v3 lp = b % f.group_brick3;
             db.pos[0] = lp.x;
             db.pos[1] = lp.y;

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdio>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <string>
@@ -44,9 +45,20 @@ struct device_ctx
   // Encode plans by format: the brick order and the EncodeSubband events depend only on the
   // dims, the brick dims and the number of levels, so repeated encodes of fields of one shape
   // (the time steps of a simulation) plan once.
-  // Callers hold the returned pointer for as long as they use the plan: the cache keeps 16
-  // shapes and may drop one while an earlier holder still uses it.
+  // Callers hold the returned pointer for as long as they use the plan: the cache keeps the
+  // plans of the last shapes up to 256 MB of plan tables (IDX2G_PLAN_CACHE_MB overrides it; a
+  // batch of many small shapes, or a few 1024^3 ones) and may drop one while an earlier
+  // holder still uses it.
   std::map<std::string, std::shared_ptr<const encode_plan>> plans;
+  std::vector<std::string> plan_order;  // keys, oldest first
+  size_t plan_bytes = 0;
+  static size_t plan_size(const encode_plan& p)
+  {
+    size_t b = p.events.size() * sizeof(encode_event) + 256;
+    for (const auto& l : p.levels)
+      b += l.size() * sizeof(brick_entry);
+    return b;
+  }
   static std::string plan_key(const dataset_format& f)
   {
     char key[128];
@@ -64,9 +76,24 @@ struct device_ctx
     *err = make_encode_plan(f, pl.get());
     if (*err)
       return nullptr;
-    if (plans.size() >= 16)
-      plans.erase(plans.begin());
+    const size_t sz = plan_size(*pl);
+    const char* mb = std::getenv("IDX2G_PLAN_CACHE_MB");
+    const size_t kBudget = (mb ? (size_t)std::strtoull(mb, nullptr, 10) : (size_t)256) << 20;
+    size_t drop = 0;
+    while (drop < plan_order.size() && plan_bytes + sz > kBudget)
+    {
+      auto old = plans.find(plan_order[drop]);
+      if (old != plans.end())
+      {
+        plan_bytes -= plan_size(*old->second);
+        plans.erase(old);
+      }
+      ++drop;
+    }
+    plan_order.erase(plan_order.begin(), plan_order.begin() + (long)drop);
     plans[key] = pl;
+    plan_order.push_back(key);
+    plan_bytes += sz;
     return pl;
   }
   // Bytes of each level's data file in the last encode of a shape (by plan_key): the next

@@ -20,6 +20,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <string>
 #include <vector>
 
 namespace idx2g
@@ -943,8 +945,9 @@ struct batch_encoder::level_launch
   int level = 0;
   std::vector<enc_brick> bricks;
   std::vector<enc_field> fields;  // geom / nblocks device pointers filled by prepare
-  std::vector<uint64_t> geom;     // [field][8][kMaxBlocksPerSubband]
-  std::vector<int> nblocks;       // [field][8]
+  std::vector<uint64_t> geom;     // [layout][8][kMaxBlocksPerSubband]
+  std::vector<int> nblocks;       // [layout][8]
+  std::vector<int> layout;        // field table entry -> its block layout
   std::vector<int> field_job;     // field table entry -> index in the batch
   std::vector<int> job_first;     // batch index -> first brick (-1: no such level)
   int nparents = 0;
@@ -1011,6 +1014,10 @@ int batch_encoder::prepare(const batch_tuning& t)
     ll.job_first = first[(size_t)l];
     ll.nparents = count[(size_t)l + 1];
     unsigned long long cap = 16ull << 20;
+    // block geometry tables: one per distinct subband layout (2D or 3D, brick and block dims,
+    // coarsest level or not), shared by the fields that have it
+    std::map<std::string, int> layouts;
+    std::vector<int>& field_layout = ll.layout;
     for (size_t j = 0; j < J.size(); ++j)
     {
       const dataset_format& f = *J[j].f;
@@ -1036,18 +1043,28 @@ int batch_encoder::prepare(const batch_tuning& t)
         ll.planes = 64;
       ll.fields.push_back(ef);
       ll.field_job.push_back((int)j);
-      ll.geom.resize(ll.fields.size() * 8 * kMaxBlocksPerSubband, 0);
-      ll.nblocks.resize(ll.fields.size() * 8, 0);
-      for (int sb = 0; sb < ef.nsb; ++sb)
+      char lk[96];
+      snprintf(lk, sizeof lk, "%d %d %d %d/%d %d %d/%d", (int)ef.is2d, f.brick_dims_ext.x, f.brick_dims_ext.y,
+               f.brick_dims_ext.z, f.block_dims.x, f.block_dims.y, f.block_dims.z, (int)(l + 1 < f.nlevels));
+      auto li = layouts.find(lk);
+      if (li == layouts.end())
       {
-        std::vector<block_geom> g;
-        subband_blocks(f, l, sb, &g);
-        ll.nblocks[(size_t)fi * 8 + (size_t)sb] = (int)g.size();
-        for (size_t b = 0; b < g.size(); ++b)
-          ll.geom[((size_t)fi * 8 + (size_t)sb) * kMaxBlocksPerSubband + b] =
-            (uint64_t)g[b].dx | ((uint64_t)g[b].dy << 8) | ((uint64_t)g[b].dz << 16) |
-            ((uint64_t)g[b].bx << 24) | ((uint64_t)g[b].by << 32) | ((uint64_t)g[b].bz << 40);
+        const int slot = (int)layouts.size();
+        li = layouts.emplace(lk, slot).first;
+        ll.geom.resize((size_t)(slot + 1) * 8 * kMaxBlocksPerSubband, 0);
+        ll.nblocks.resize((size_t)(slot + 1) * 8, 0);
+        for (int sb = 0; sb < ef.nsb; ++sb)
+        {
+          std::vector<block_geom> g;
+          subband_blocks(f, l, sb, &g);
+          ll.nblocks[(size_t)slot * 8 + (size_t)sb] = (int)g.size();
+          for (size_t b = 0; b < g.size(); ++b)
+            ll.geom[((size_t)slot * 8 + (size_t)sb) * kMaxBlocksPerSubband + b] =
+              (uint64_t)g[b].dx | ((uint64_t)g[b].dy << 8) | ((uint64_t)g[b].dz << 16) |
+              ((uint64_t)g[b].bx << 24) | ((uint64_t)g[b].by << 32) | ((uint64_t)g[b].bz << 40);
+        }
       }
+      field_layout.push_back(li->second);
       const std::vector<brick_entry>& bricks = J[j].plan->levels[(size_t)l];
       const bool has_parent = l + 1 < f.nlevels;
       for (const brick_entry& e : bricks)
@@ -1092,8 +1109,8 @@ int batch_encoder::prepare(const batch_tuning& t)
     ll.cap = ctx_->ws_size(ll.sname);
     for (size_t fi = 0; fi < ll.fields.size(); ++fi)
     {
-      ll.fields[fi].geom = ll.d_geom + fi * 8 * kMaxBlocksPerSubband;
-      ll.fields[fi].nblocks = ll.d_nblocks + fi * 8;
+      ll.fields[fi].geom = ll.d_geom + (size_t)field_layout[fi] * 8 * kMaxBlocksPerSubband;
+      ll.fields[fi].nblocks = ll.d_nblocks + (size_t)field_layout[fi] * 8;
     }
     if (nbr > 0)
       cudaMemcpyAsync(ll.d_bricks, ll.bricks.data(), sizeof(enc_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
@@ -1356,7 +1373,7 @@ int batch_encoder::collect_level(int l, bool keep_device)
     long long eb = 0;
     for (int sb = 0; sb < nsb; ++sb)
     {
-      o.nexps[(size_t)sb] = ll.nblocks[fi * 8 + (size_t)sb];
+      o.nexps[(size_t)sb] = ll.nblocks[(size_t)ll.layout[fi] * 8 + (size_t)sb];
       eb += (long long)jn * o.nexps[(size_t)sb] * (f.type == dtype::float32 ? 1 : 2);
     }
     bf.exp_bytes += eb;
@@ -1404,10 +1421,12 @@ int batch_encoder::run_all(bool use_graph, bool keep_device)
         cudaGraphDestroy(g);
       return e ? e : CudaError;
     }
+    stage_timer tt;
     cudaEventRecord(ctx_->ev0, st);
     cudaGraphLaunch(ge, st);
     cudaEventRecord(ctx_->ev1, st);
     const cudaError_t se = cudaStreamSynchronize(st);
+    tt.lap("batch.graph_run");
     cudaGraphExecDestroy(ge);
     cudaGraphDestroy(g);
     if (se != cudaSuccess)
@@ -1421,6 +1440,7 @@ int batch_encoder::run_all(bool use_graph, bool keep_device)
       if (e)
         return e;
     }
+    tt.lap("batch.collect");
     return NoError;
   }
   for (int l = 0; l < L; ++l)

@@ -85,18 +85,21 @@ def test_batch_device_only(idx2g, tmp_path):
 
 
 @pytest.mark.gpu
-def test_batch_of_more_shapes_than_the_plan_cache(idx2g, tmp_path):
-    """A batch of more distinct field shapes than the context keeps plans for (16): every
-    field's plan stays valid for the whole call, the files match single-field encodes."""
+def test_batch_of_more_shapes_than_the_plan_cache(idx2g, tmp_path, monkeypatch):
+    """A batch of more distinct field shapes than the context keeps plans for (a zero budget
+    here, IDX2G_PLAN_CACHE_MB=0: each new plan drops the older ones): every field's plan stays
+    valid for the whole call, the files match single-field encodes."""
     fields = _batch_fields(24, seed=33, max_side=48)
     assert len({f.shape + (lv,) for f, lv in fields}) > 16
     names = [f"m{i}" for i in range(len(fields))]
     for (f, lv), nm in zip(fields, names):
         idx2g.encode(f, out_dir=str(tmp_path / "single"), name=nm, field_name="f", num_levels=lv,
                      tolerance=1e-3)
+    monkeypatch.setenv("IDX2G_PLAN_CACHE_MB", "0")
     idx2g.encode_batch([f for f, _ in fields], out_dir=str(tmp_path / "batch"), names=names,
                        field_names=["f"] * len(fields), num_levels=[lv for _, lv in fields],
                        tolerances=[1e-3] * len(fields), graph=True, autotune=False)
+    monkeypatch.delenv("IDX2G_PLAN_CACHE_MB")
     for nm in names:
         diffs = compare_dirs(str(tmp_path / "single" / nm), str(tmp_path / "batch" / nm))
         assert diffs == [], (nm, diffs[:3])
