@@ -16,6 +16,8 @@
 #include "encoder.h"
 #include "trace.h"
 
+#include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime's entry point)
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -73,6 +75,7 @@ constexpr int kRowX = kMaxBlocksPerSubband + 1;    // unsigned long long
 constexpr int kRowOff = kMaxBlocksPerSubband + 2;  // uint16_t
 constexpr int kRowNin = kMaxBlocksPerSubband + 4;  // uint8_t
 constexpr unsigned kStageBytes = 8192;
+constexpr int kGz = 4;  // z-planes per chunk of the level-0 gather
 
 struct enc_brick
 {
@@ -96,6 +99,8 @@ struct enc_field
   double weight[8];
   int norm_mask;
   int bpc;                   // BitPlanesPerChunk: bit planes per channel key
+  int pad_;
+  const CUtensorMap* tmap;   // level 0: the field as a 3D tensor (boxes of 32 x 32 x kGz), or null
 };
 
 constexpr int kNB3 = 33 * 33 * 33;  // brick stride of slots and parent arrays (2D bricks use 33^2)
@@ -144,6 +149,7 @@ struct enc_smem
   int kmin, kmax;
   unsigned long long region;
   int ok;
+  unsigned long long tma_bar[2];  // completion of the gather's two chunk buffers (TMA path)
 };
 
 inline size_t enc_smem_bytes(int planes)
@@ -151,7 +157,7 @@ inline size_t enc_smem_bytes(int planes)
   // the coding tables, which also hold the 17^3 even lattice during the transform
   const size_t tables = (size_t)planes * ((size_t)kRowX * 8 + (size_t)kRowOff * 2 + (size_t)kRowNin);
   const size_t lattice = (size_t)17 * 17 * 17 * 8;
-  return ((sizeof(enc_smem) + 15) & ~(size_t)15) + (tables > lattice ? tables : lattice);
+  return ((sizeof(enc_smem) + 127) & ~(size_t)127) + (tables > lattice ? tables : lattice);
 }
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
@@ -260,11 +266,12 @@ __device__ __forceinline__ block_info block_at(const uint64_t* geom, int b, cons
 
 __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc_args a)
 {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   enc_smem& sm = *reinterpret_cast<enc_smem*>(smem_raw);
   const int P = a.planes;
+  // the tables start 128-byte aligned: the gather's chunk buffers there are TMA destinations
   unsigned long long* const Xp =
-    reinterpret_cast<unsigned long long*>(smem_raw + ((sizeof(enc_smem) + 15) & ~(size_t)15));
+    reinterpret_cast<unsigned long long*>(smem_raw + ((sizeof(enc_smem) + 127) & ~(size_t)127));
   uint16_t* const OFF = reinterpret_cast<uint16_t*>(Xp + (size_t)kRowX * P);
   uint8_t* const NIN = reinterpret_cast<uint8_t*>(OFF + (size_t)kRowOff * P);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -273,6 +280,14 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
     sm.perm3[tid] = dev::perm(3, tid);
   if (tid < 16)
     sm.perm2[tid] = dev::perm(2, tid);
+  if (tid == 0 && a.level == 0)
+  {
+    const unsigned b0 = (unsigned)__cvta_generic_to_shared(&sm.tma_bar[0]);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b0 + 8u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  unsigned tma_parity = 0;  // bit b: phase parity of chunk buffer b's next completion
   ENC_PHASE_INIT
 
   for (int it = a.first + (int)blockIdx.x; it < a.last; it += gridDim.x)
@@ -304,15 +319,35 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       // double-buffered in the coding tables' space (idle here): asynchronous copies of chunk
       // c + 1 are in flight while chunk c is widened into the brick; samples outside the
       // valid region (and the x = 32, y = 32, z = 32 faces) are zero.
-      constexpr int kGz = 4;
+      // With a tensor map (the usual case), one thread loads each chunk as one bulk tensor copy
+      // (TMA) of a 32 x 32 x kGz box completing on an mbarrier; samples past the volume's
+      // edge arrive as zeros, planes of the next brick are loaded and not used.
       const int esz = fp.field_f32 ? 4 : 8;
       unsigned char* const stage = reinterpret_cast<unsigned char*>(Xp);
       const unsigned stage_bytes = (unsigned)(kGz * 32 * 32 * esz);
+      const unsigned box_bytes = (unsigned)((fp.is2d ? 1 : kGz) * 32 * 32 * esz);
       const int nch = (N[2] + kGz - 1) / kGz;
+      const bool tma = fp.tmap != nullptr;
       auto issue = [&](int c) {
         const int z0 = c * kGz;
         const int nz = vz - z0 < kGz ? vz - z0 : kGz;
         const unsigned s0 = (unsigned)__cvta_generic_to_shared(stage) + (unsigned)(c & 1) * stage_bytes;
+        if (tma)
+        {
+          if (tid == 0 && nz > 0)
+          {
+            const unsigned bar = (unsigned)__cvta_generic_to_shared(&sm.tma_bar[c & 1]);
+            // the buffer was last written and read by ordinary accesses
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(box_bytes)
+                         : "memory");
+            asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                         " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(s0),
+                         "l"(fp.tmap), "r"((int)gx0), "r"((int)gy0), "r"((int)(gz0 + z0)), "r"(bar)
+                         : "memory");
+          }
+          return;
+        }
         for (int i = tid; i < nz * vy * 32; i += kThreads)
         {
           const int x = i & 31, row = i >> 5, y = row % vy, zz = row / vy;
@@ -329,17 +364,63 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
       };
+      // chunk c in shared memory; false (in every thread) if its bulk copy did not complete
+      // within the wait's bound (the copy then counts as lost)
+      auto wait_chunk = [&](int c) -> bool {
+        if (!tma)
+        {
+          if (c + 1 < nch)
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+          else
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+          __syncthreads();
+          return true;
+        }
+        int ok = 1;
+        if (c * kGz < vz)
+        {
+          const unsigned bar = (unsigned)__cvta_generic_to_shared(&sm.tma_bar[c & 1]);
+          const unsigned par = (tma_parity >> (c & 1)) & 1u;
+          ok = 0;
+          for (int it = 0; it < (1 << 22) && !ok; ++it)
+            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                         " selp.u32 %0, 1, 0, p;\n}\n"
+                         : "=r"(ok)
+                         : "r"(bar), "r"(par)
+                         : "memory");
+          tma_parity ^= 1u << (c & 1);
+        }
+        return __syncthreads_and(ok) != 0;
+      };
       issue(0);
       for (int c = 0; c < nch; ++c)
       {
         if (c + 1 < nch)
-        {
           issue(c + 1);
-          asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        if (!wait_chunk(c))
+        {
+          // a lost copy: report it and end this CTA (uniformly) after a bounded wait for the
+          // copies still in flight
+          if (tid == 0)
+          {
+            atomicExch(a.error, 4);
+            for (int k = c; k <= c + 1 && k < nch; ++k)
+            {
+              if (k * kGz >= vz)
+                continue;
+              const unsigned bar = (unsigned)__cvta_generic_to_shared(&sm.tma_bar[k & 1]);
+              const unsigned par = k == c ? ((tma_parity >> (k & 1)) & 1u) ^ 1u : (tma_parity >> (k & 1)) & 1u;
+              int ok = 0;
+              for (int it = 0; it < (1 << 22) && !ok; ++it)
+                asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                             " selp.u32 %0, 1, 0, p;\n}\n"
+                             : "=r"(ok)
+                             : "r"(bar), "r"(par)
+                             : "memory");
+            }
+          }
+          return;
         }
-        else
-          asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();
         const unsigned char* buf = stage + (size_t)(c & 1) * stage_bytes;
         const int z0 = c * kGz;
         const int nz = N[2] - z0 < kGz ? N[2] - z0 : kGz;
@@ -976,6 +1057,54 @@ batch_encoder::batch_encoder(device_ctx* ctx, std::vector<batch_field>* fields, 
 
 batch_encoder::~batch_encoder() = default;
 
+namespace
+{
+
+using encode_tiled_fn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                     const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                     CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+encode_tiled_fn tensor_map_encoder()
+{
+  static encode_tiled_fn fn = []() -> encode_tiled_fn {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+    {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return (encode_tiled_fn)p;
+  }();
+  return fn;
+}
+
+// The field of f as a 3D tensor (x fastest) read in boxes of 32 x 32 x kGz samples (one plane
+// for 2D fields). TMA wants the base address and the row and plane pitches in multiples of 16
+// bytes; fields that do not have them are gathered with ordinary copies. Box origins are
+// brick origins, multiples of 32 samples along x: 16-byte aligned for either sample type.
+bool field_tensor_map(const enc_field& f, CUtensorMap* map)
+{
+  encode_tiled_fn enc = tensor_map_encoder();
+  const size_t esz = f.field_f32 ? 4 : 8;
+  if (!enc || !f.field || ((uintptr_t)f.field & 15) || ((size_t)f.fdims[0] * esz) % 16 ||
+      f.fdims[0] < 1 || f.fdims[1] < 1 || f.fdims[2] < 1 || f.fdims[0] > (1ll << 31) || f.fdims[1] > (1ll << 31) ||
+      f.fdims[2] > (1ll << 31))
+    return false;
+  const cuuint64_t dims[3] = { (cuuint64_t)f.fdims[0], (cuuint64_t)f.fdims[1], (cuuint64_t)f.fdims[2] };
+  const cuuint64_t pitch[2] = { (cuuint64_t)f.fdims[0] * esz, (cuuint64_t)f.fdims[0] * (cuuint64_t)f.fdims[1] * esz };
+  const cuuint32_t box[3] = { 32, 32, (cuuint32_t)(f.is2d ? 1 : kGz) };
+  const cuuint32_t estr[3] = { 1, 1, 1 };
+  memset(map, 0, sizeof *map);
+  return enc(map, f.field_f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+             const_cast<void*>(f.field), dims, pitch, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+} // namespace
+
 int batch_encoder::prepare(const batch_tuning& t)
 {
   tune_ = t;
@@ -1111,6 +1240,30 @@ int batch_encoder::prepare(const batch_tuning& t)
     {
       ll.fields[fi].geom = ll.d_geom + (size_t)field_layout[fi] * 8 * kMaxBlocksPerSubband;
       ll.fields[fi].nblocks = ll.d_nblocks + (size_t)field_layout[fi] * 8;
+    }
+    if (l == 0)
+    {
+      // level 0 reads each field through a tensor map where the field's layout allows TMA
+      std::vector<CUtensorMap> maps(ll.fields.size());
+      std::vector<char> has(ll.fields.size(), 0);
+      size_t nmaps = 0;
+      for (size_t fi = 0; fi < ll.fields.size(); ++fi)
+        if (field_tensor_map(ll.fields[fi], &maps[fi]))
+        {
+          has[fi] = 1;
+          ++nmaps;
+        }
+      if (nmaps)
+      {
+        CUtensorMap* d_maps = (CUtensorMap*)wsn("tmaps", sizeof(CUtensorMap) * ll.fields.size());
+        CUtensorMap* h_maps = (CUtensorMap*)ctx_->pinned("enc." + tag_ + ".tmaps", sizeof(CUtensorMap) * ll.fields.size());
+        if (!d_maps || !h_maps)
+          return OutOfMemory;
+        memcpy(h_maps, maps.data(), sizeof(CUtensorMap) * ll.fields.size());
+        cudaMemcpyAsync(d_maps, h_maps, sizeof(CUtensorMap) * ll.fields.size(), cudaMemcpyHostToDevice, st);
+        for (size_t fi = 0; fi < ll.fields.size(); ++fi)
+          ll.fields[fi].tmap = has[fi] ? d_maps + fi : nullptr;
+      }
     }
     if (nbr > 0)
       cudaMemcpyAsync(ll.d_bricks, ll.bricks.data(), sizeof(enc_brick) * (size_t)nbr, cudaMemcpyHostToDevice, st);
