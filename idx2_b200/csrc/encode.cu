@@ -1456,6 +1456,8 @@ int batch_encoder::collect_level(int l, bool keep_device)
     if (cudaStreamSynchronize(st) != cudaSuccess)
       return CudaError;
     const int err = (int)(misc[1] & 0xffffffffu);
+    if (err == 4)
+      return CudaError;  // a bulk copy of the gather did not complete
     if (err == 1)
       return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
     if (err != 2)
