@@ -424,6 +424,8 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       memset(&pa, 0, sizeof pa);
       pa.nsb = r0.nsb;
       pa.nbricks = nbr;
+      pa.unit_first = 0;
+      pa.unit_last = (int)nunits;
       pa.end_bp = a.end_bp;
       pa.bpc = r0.bpc;
       pa.reqs = d_reqs;
@@ -453,16 +455,24 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         return CudaError;
       ++nev;
       cudaEventRecord(t0, st);
-      if (r0.bpc == 1)
-      {
-        k_decode_planes<false><<<(pgrid + 1) / 2, kPlaneWarps * 32, 0, st>>>(pa);  // two units per warp
-        k_decode_planes<true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(pa);
-      }
-      else
-      {
-        k_decode_planes<false, true><<<pgrid, kPlaneWarps * 32, 0, st>>>(pa);
-        k_decode_planes<true, true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(pa);
-      }
+      // the plane kernels over units [p.unit_first, p.unit_last): the first pass, then the
+      // units it deferred (more than 32 channels)
+      auto launch_planes = [&](const dec1_args& p) {
+        const int g1 = (p.unit_last - p.unit_first + kPlaneWarps - 1) / kPlaneWarps;
+        if (r0.bpc == 1)
+        {
+          k_decode_planes<false><<<(g1 + 1) / 2, kPlaneWarps * 32, 0, st>>>(p);  // two units per warp
+          k_decode_planes<true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(p);
+        }
+        else
+        {
+          k_decode_planes<false, true><<<g1, kPlaneWarps * 32, 0, st>>>(p);
+          k_decode_planes<true, true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(p);
+        }
+      };
+      (void)pgrid;
+      if (!split_level)
+        launch_planes(pa);
       if (split_level)
       {
         // about 8 launches, each of whole rows of bricks; after launch g every output plane
@@ -482,6 +492,14 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         size_t z_done = 0;
         for (size_t g = 0; g + 1 < cuts.size(); ++g)
         {
+          // the band's plane tables (the deferred-unit list starts empty for each band)
+          dec1_args pg = pa;
+          pg.unit_first = cuts[g] * r0.nsb;
+          pg.unit_last = cuts[g + 1] * r0.nsb;
+          if (g > 0)
+            cudaMemsetAsync((int*)(d_pcur + 1), 0, sizeof(int), st);
+          launch_planes(pg);
+          ctx->launches += 2;
           dec_args ag = a;
           ag.bricks = d_bricks + cuts[g];
           ag.nbricks = cuts[g + 1] - cuts[g];
@@ -504,7 +522,6 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
           }
         }
         out_copied = true;
-        ctx->launches += 2;
       }
       else
       {

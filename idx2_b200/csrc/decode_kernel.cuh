@@ -69,6 +69,7 @@ struct dec1_args
 {
   int bpc;                          // BitPlanesPerChunk: bit planes per channel key
   int nsb, nbricks, end_bp;
+  int unit_first, unit_last;        // the first pass decodes units [unit_first, unit_last)
   const decode_target* reqs;
   int nblocks[8];
   const uint64_t* geom;  // [8][kMaxBlocksPerSubband]
@@ -631,11 +632,12 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : (MULTI ? 6 : 4)) 
 {
   __shared__ plane_smem sm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nunits = WIDE ? *a.wide_count : a.nbricks * a.nsb;
+  const int ufirst = WIDE ? 0 : a.unit_first;
+  const int nunits = WIDE ? *a.wide_count : a.unit_last;
   if constexpr (!WIDE && !MULTI)
   {
     // two consecutive units per warp; a pair of units of up to 16 channels shares the warp
-    for (int i = 2 * (blockIdx.x * kPlaneWarps + warp); i < nunits; i += 2 * gridDim.x * kPlaneWarps)
+    for (int i = ufirst + 2 * (blockIdx.x * kPlaneWarps + warp); i < nunits; i += 2 * gridDim.x * kPlaneWarps)
     {
       const plane_unit A = prep_unit<false, false>(a, i, sm.ktop[warp][0], sm.np[warp][0], sm.nvl[warp][0], lane);
       plane_unit B;
@@ -662,7 +664,7 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : (MULTI ? 6 : 4)) 
     }
     return;
   }
-  for (int i = blockIdx.x * kPlaneWarps + warp; i < nunits; i += gridDim.x * kPlaneWarps)
+  for (int i = ufirst + blockIdx.x * kPlaneWarps + warp; i < nunits; i += gridDim.x * kPlaneWarps)
   {
     const int unit = WIDE ? a.wide_list[i] : i;
     int16_t* ktop = sm.ktop[warp][0];

@@ -33,3 +33,23 @@ def test_pinned_host_encode_matches(idx2g, tmp_path, ci):
     for other in ("device", "pinned0", "pinned1"):
         diffs = compare_dirs(str(tmp_path / "pageable" / "e"), str(tmp_path / other / "e"))
         assert diffs == [], (other, diffs[:3])
+
+
+@pytest.mark.gpu
+def test_device_field_off_16_byte_alignment(idx2g, tmp_path):
+    """A device field that starts 4 bytes past a 16-byte boundary (a view into a larger
+    tensor) cannot be read through a tensor map: the gather falls back to ordinary copies and
+    the files are the same."""
+    import torch
+    from idx2_b200.synthetic import bumps_field
+    dims = (128, 96, 80)
+    f = bumps_field(dims[0], dims[1], dims[2], seed=90).astype(np.float32)
+    kw = dict(field_name="f", num_levels=2, tolerance=1e-4)
+    idx2g.encode(f, out_dir=str(tmp_path / "aligned"), name="e", **kw)
+    big = torch.empty(f.size + 1, dtype=torch.float32, device="cuda")
+    view = big[1:].view(dims[2], dims[1], dims[0])
+    view.copy_(torch.from_numpy(f))
+    assert view.data_ptr() % 16 == 4
+    idx2g.encode(view, out_dir=str(tmp_path / "offset"), name="e", **kw)
+    diffs = compare_dirs(str(tmp_path / "aligned" / "e"), str(tmp_path / "offset" / "e"))
+    assert diffs == [], diffs[:3]
