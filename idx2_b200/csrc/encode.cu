@@ -528,14 +528,76 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       }
       __syncthreads();
       ENC_PHASE(4)
-      for (int i = ci - 1; i >= 1; --i)
+      // With the first level's sweeps in Z, Y, X order on the whole 33^3 brick (the usual
+      // transform order), the sweeps that stay inside z-planes -- the inverse Y, the inverse
+      // then forward X, and the forward Y -- run on bands of kPlanes z-planes in shared
+      // memory (the coding tables' space, idle here): one read and one write of the brick
+      // instead of three of each. The same line functions run on the same values.
+      auto full33 = [&](const dev::dgrid& g) {
+        return g.from[0] == 0 && g.from[1] == 0 && g.from[2] == 0 && g.dims[0] == 33 && g.dims[1] == 33 &&
+               g.dims[2] == 33 && g.strd[0] == 1 && g.strd[1] == 1 && g.strd[2] == 1;
+      };
+      const bool planar = !fp.is2d && ci == 3 && sm.stack.axis[2] == 2 && sm.stack.axis[1] == 1 &&
+                          sm.stack.axis[0] == 0 && full33(sm.stack.g[2]) && full33(sm.stack.g[1]);
+      for (int i = ci - 1; i >= (planar ? 2 : 1); --i)
       {
         dev::lift_sweep_regs<false>(F, N, sm.stack.g[i], sm.stack.axis[i]);
         __syncthreads();
       }
       ENC_PHASE(5)
+      if (planar)
+      {
+        constexpr int kPlanes = 4;  // 4 x 33 x 33 doubles: 34.8 KB, within the tables' space
+        double* T = reinterpret_cast<double*>(Xp);
+        for (int z0 = 0; z0 < 33; z0 += kPlanes)
+        {
+          const int nzc = 33 - z0 < kPlanes ? 33 - z0 : kPlanes;
+          const int n = nzc * 33 * 33;
+          const double* src = F + (size_t)z0 * 33 * 33;
+          for (int i = tid; i < n; i += kThreads)
+            T[i] = src[i];
+          __syncthreads();
+          // inverse Y (columns of each plane)
+          for (int li = tid; li < 33 * nzc; li += kThreads)
+            dev::lift_line_strided<33, false, 33>(T + (li / 33) * 33 * 33 + li % 33);
+          __syncthreads();
+          // inverse X (D = 33) then forward X of the one-level transform (Core/Wavelet.cpp:81)
+          for (int li = tid; li < 33 * nzc; li += kThreads)
+          {
+            double* row = T + li * 33;
+            double v[33];
+#pragma unroll
+            for (int k = 0; k < 33; ++k)
+              v[k] = row[k];
+            dev::lift_regs<false>(v, 33);
+            dev::lift_regs<true>(v, 33);
+#pragma unroll
+            for (int k = 0; k < 33; ++k)
+              row[k] = v[k];
+          }
+          __syncthreads();
+          // forward Y
+          for (int li = tid; li < 33 * nzc; li += kThreads)
+          {
+            double* col = T + (li / 33) * 33 * 33 + li % 33;
+            double v[33];
+#pragma unroll
+            for (int k = 0; k < 33; ++k)
+              v[k] = col[k * 33];
+            dev::lift_regs<true>(v, 33);
+#pragma unroll
+            for (int k = 0; k < 33; ++k)
+              col[k * 33] = v[k];
+          }
+          __syncthreads();
+          double* dst = F + (size_t)z0 * 33 * 33;
+          for (int i = tid; i < n; i += kThreads)
+            dst[i] = T[i];
+          __syncthreads();
+        }
+      }
       // inverse X (D = 33) then forward X of the one-level transform (Core/Wavelet.cpp:81)
-      for (int li = tid; li < 33 * N[2]; li += kThreads)
+      for (int li = tid; !planar && li < 33 * N[2]; li += kThreads)
       {
         double* row = F + li * 33;
         double v[33];
@@ -550,9 +612,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       }
       __syncthreads();
       ENC_PHASE(6)
-      // forward Y, and forward Z; subband normalisation applied as the last sweep stores
-      // (Core/Wavelet.cpp:111-137)
-      for (int li = tid; li < 33 * N[2]; li += kThreads)
+      // forward Y (done above for planar bricks), and forward Z; subband normalisation applied
+      // as the last sweep stores (Core/Wavelet.cpp:111-137)
+      for (int li = tid; !planar && li < 33 * N[2]; li += kThreads)
       {
         const int x = li % 33, z = li / 33;
         double* col = F + z * 33 * 33 + x;
