@@ -157,7 +157,11 @@ inline size_t enc_smem_bytes(int planes)
   // the coding tables, which also hold the 17^3 even lattice during the transform
   const size_t tables = (size_t)planes * ((size_t)kRowX * 8 + (size_t)kRowOff * 2 + (size_t)kRowNin);
   const size_t lattice = (size_t)17 * 17 * 17 * 8;
-  return ((sizeof(enc_smem) + 127) & ~(size_t)127) + (tables > lattice ? tables : lattice);
+  // the level-0 gather with its first sweeps: one chunk buffer and a 4-plane FP64 band
+  const size_t band = (size_t)kGz * 32 * 32 * (planes == 32 ? 4 : 8) + (size_t)kGz * 33 * 33 * 8;
+  size_t space = tables > lattice ? tables : lattice;
+  space = space > band ? space : band;
+  return ((sizeof(enc_smem) + 127) & ~(size_t)127) + space;
 }
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
@@ -307,9 +311,147 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
     const int N[3] = { 33, 33, fp.is2d ? 1 : 33 };
     const int NB = N[0] * N[1] * N[2];
     const int SZ = fp.is2d ? 0 : 2 * 33 * 33;  // sample stride along z inside a subband
+    // the extrapolation's sweeps on the valid dims (Core/Wavelet.cpp:68)
+    if (tid == 0)
+      dev::build_stack(br.valid, 5, fp.order, &sm.stack);
+    __syncthreads();
+    auto level_one = [&](const dev::dgrid& g) {
+      return g.from[0] == 0 && g.from[1] == 0 && g.from[2] == 0 && g.strd[0] == 1 && g.strd[1] == 1 && g.strd[2] == 1;
+    };
+    // A level-0 brick read through TMA whose first two sweeps are X and Y (in either order)
+    // takes them during the gather, on each chunk of planes in shared memory
+    const bool gather_xy = a.level == 0 && fp.tmap != nullptr && !fp.is2d && sm.stack.coarse >= 2 &&
+                           sm.stack.axis[0] + sm.stack.axis[1] == 1 && level_one(sm.stack.g[0]) &&
+                           level_one(sm.stack.g[1]);
     ENC_PHASE_START
     // ---------------- A: gather ----------------
-    if (a.level == 0)
+    if (a.level == 0 && gather_xy)
+    {
+      // one chunk buffer: the copy of chunk c + 1 runs while chunk c's sweeps do
+      const int vx = br.valid[0], vy = br.valid[1], vz = br.valid[2];
+      double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
+      const long long gx0 = (long long)br.b3[0] * 32, gy0 = (long long)br.b3[1] * 32, gz0 = (long long)br.b3[2] * 32;
+      const int esz = fp.field_f32 ? 4 : 8;
+      unsigned char* const stage = reinterpret_cast<unsigned char*>(Xp);
+      const unsigned box_bytes = (unsigned)(kGz * 32 * 32 * esz);
+      double* const T = reinterpret_cast<double*>(stage + box_bytes);  // kGz x 33 x 33
+      const unsigned s0 = (unsigned)__cvta_generic_to_shared(stage);
+      const unsigned bar = (unsigned)__cvta_generic_to_shared(&sm.tma_bar[0]);
+      const int nch = (33 + kGz - 1) / kGz;
+      auto issue = [&](int c) {
+        if (tid == 0 && c < nch && c * kGz < vz)
+        {
+          asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(box_bytes) : "memory");
+          asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+                       " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(s0),
+                       "l"(fp.tmap), "r"((int)gx0), "r"((int)gy0), "r"((int)(gz0 + c * kGz)), "r"(bar)
+                       : "memory");
+        }
+      };
+      // a first-level forward sweep (lift_sweep_regs<true>) restricted to planes [z0, z0 + nz)
+      auto band_sweep = [&](const dev::dgrid& G, int ax, int z0, int nz) {
+        const int D = G.dims[ax];
+        const int nu = G.dims[1 - ax];
+        const int zhi = z0 + nz < G.dims[2] ? z0 + nz : G.dims[2];
+        if (D == 1 || zhi <= z0)
+          return;
+        const int su = ax == 0 ? 33 : 1;
+        for (int li = tid; li < nu * (zhi - z0); li += kThreads)
+        {
+          double* L = T + (li / nu) * 33 * 33 + (li % nu) * su;
+          if (D == 32)
+            ax == 0 ? dev::lift_line_strided<32, true, 1>(L) : dev::lift_line_strided<32, true, 33>(L);
+          else if (D == 33)
+            ax == 0 ? dev::lift_line_strided<33, true, 1>(L) : dev::lift_line_strided<33, true, 33>(L);
+          else
+            dev::lift_line<true>(L, ax == 0 ? 1 : 33, D);
+        }
+      };
+      issue(0);
+      for (int c = 0; c < nch; ++c)
+      {
+        const int z0 = c * kGz;
+        const int nz = 33 - z0 < kGz ? 33 - z0 : kGz;
+        int ok = 1;
+        if (z0 < vz)
+        {
+          const unsigned par = tma_parity & 1u;
+          ok = 0;
+          for (int it = 0; it < (1 << 22) && !ok; ++it)
+            asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                         " selp.u32 %0, 1, 0, p;\n}\n"
+                         : "=r"(ok)
+                         : "r"(bar), "r"(par)
+                         : "memory");
+          tma_parity ^= 1u;
+        }
+        if (!__syncthreads_and(ok))
+        {
+          if (tid == 0)
+          {
+            // a lost copy: report it, wait (bounded) for it once more, end this CTA
+            atomicExch(a.error, 4);
+            int done = 0;
+            for (int it = 0; it < (1 << 22) && !done; ++it)
+              asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                           " selp.u32 %0, 1, 0, p;\n}\n"
+                           : "=r"(done)
+                           : "r"(bar), "r"((tma_parity & 1u) ^ 1u)
+                           : "memory");
+          }
+          return;
+        }
+        for (int i = tid; i < nz * 33 * 33; i += kThreads)
+        {
+          const int x = i % 33, row = i / 33, y = row % 33, zz = row / 33, z = z0 + zz;
+          const bool in = x < vx && y < vy && z < vz;
+          double v = 0.0;
+          if (in)
+            v = fp.field_f32 ? (double)reinterpret_cast<const float*>(stage)[(zz * 32 + y) * 32 + x]
+                             : reinterpret_cast<const double*>(stage)[(zz * 32 + y) * 32 + x];
+          T[i] = v;
+          if (in)
+          {
+            mn = v < mn ? v : mn;
+            mx = mx < v ? v : mx;
+          }
+        }
+        __syncthreads();
+        issue(c + 1);
+        band_sweep(sm.stack.g[0], sm.stack.axis[0], z0, nz);
+        __syncthreads();
+        band_sweep(sm.stack.g[1], sm.stack.axis[1], z0, nz);
+        __syncthreads();
+        double* dst = F + (size_t)z0 * 33 * 33;
+        for (int i = tid; i < nz * 33 * 33; i += kThreads)
+          dst[i] = T[i];
+        __syncthreads();
+      }
+      for (int o = 16; o > 0; o >>= 1)
+      {
+        double w1 = __shfl_xor_sync(0xffffffffu, mn, o), w2 = __shfl_xor_sync(0xffffffffu, mx, o);
+        mn = w1 < mn ? w1 : mn;
+        mx = mx < w2 ? w2 : mx;
+      }
+      if (lane == 0)
+      {
+        sm.red[0][warp] = mn;
+        sm.red[1][warp] = mx;
+      }
+      __syncthreads();
+      if (tid == 0)
+      {
+        for (int w = 1; w < kWarps; ++w)
+        {
+          mn = sm.red[0][w] < mn ? sm.red[0][w] : mn;
+          mx = mx < sm.red[1][w] ? sm.red[1][w] : mx;
+        }
+        a.bmin[bi] = mn;
+        a.bmax[bi] = mx;
+      }
+    }
+    else if (a.level == 0)
     {
       const int vx = br.valid[0], vy = br.valid[1], vz = br.valid[2];
       double mn = 1.7976931348623157e308, mx = -1.7976931348623157e308;
@@ -486,11 +628,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       double* S = reinterpret_cast<double*>(Xp);
       const int NS[3] = { 17, 17, fp.is2d ? 1 : 17 };
       const int nsub = NS[0] * NS[1] * NS[2];
-      if (tid == 0)
-        dev::build_stack(br.valid, 5, fp.order, &sm.stack);
-      __syncthreads();
       const int nf = sm.stack.n, cf = sm.stack.coarse;
-      for (int i = 0; i < cf; ++i)
+      for (int i = gather_xy ? 2 : 0; i < cf; ++i)
       {
         dev::lift_sweep_regs<true>(F, N, sm.stack.g[i], sm.stack.axis[i]);
         __syncthreads();
