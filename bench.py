@@ -44,10 +44,10 @@ LEVELS = 3
 TOL = 1e-3
 METRIC = "encode+decode GB/s (raw field bytes) at 1e-3 tol"
 # DRAM bytes (read + write) of one level-0 k_encode_level launch per brick, from an ncu capture
-# of the grf512 workload (4,096 bricks: 2.186 GB read + 2.972 GB written); the traffic of a
+# of the grf512 workload (4,096 bricks: 2.182 GB read + 2.882 GB written); the traffic of a
 # launch grows with its bricks (every brick makes the same slot sweeps), so a full launch's
 # traffic is this figure times its bricks.
-ENC_L0_TRAFFIC_PER_BRICK = (2.186139e9 + 2.972184e9) / 4096
+ENC_L0_TRAFFIC_PER_BRICK = (2.182016e9 + 2.882242e9) / 4096
 
 
 def hbm_peak():
