@@ -23,6 +23,7 @@
 #include <fcntl.h>
 #include <map>
 #include <memory>
+#include <tuple>
 #include <sys/stat.h>
 #include <thread>
 #include <unistd.h>
@@ -441,6 +442,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
 
   tt.lap("open.exponents");
   // bit-plane chunk headers (Core/idx2Decode.cpp:507 DecompressChunk), one task per chunk
+  std::atomic<int> mixed_ranges{ 0 };
   std::vector<std::vector<chan_entry>> entries(bp_chunks.size());
   parallel_for(bp_chunks.size(), [&](size_t k) {
     const chunk_ref& c = bp_chunks[k];
@@ -449,6 +451,10 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     int bpkey = (int)(c.addr & 0xFFF);
     if (lv != c.level || sb >= nsb)
       return;
+    // whether every brick of the chunk lies in the chunk's brick range (then chunks of
+    // different ranges touch different slots of the channel table below)
+    const int cshift = log2_ceil(f.bricks_per_chunk[(size_t)lv]);
+    const u64 crange = (c.addr >> 18) & 0x3FFFFFFFFFFull;
     bit_reader cr{ blob + c.off, c.size };
     const uint64_t nbr64 = cr.varbyte();
     if (nbr64 > c.size * 8 + 1)
@@ -485,6 +491,8 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     for (int i = 0; i < nbr; ++i)
     {
       u64 lin = bricks[(size_t)i];
+      if ((lin >> cshift) != crange)
+        mixed_ranges = 1;
       if (lin >= index.size())
         continue;
       int bi = index[lin];
@@ -500,16 +508,24 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
 
   tt.lap("open.chunk_headers");
   // channel table: key range per (brick, subband), then the offsets. The chunks of one
-  // (level, subband) touch only that subband's slots, so each (level, subband) is one task.
+  // (level, subband, brick range) -- one per key -- are the only ones to touch that range's
+  // slots of that subband, so each such group is one task (each (level, subband) if some
+  // chunk holds bricks outside its range).
   std::vector<int32_t> kmax(nslots, -1);
   int32_t* kmin = h->chan_kmin;
   parallel_ranges(nslots, [&](size_t i0, size_t i1) { std::fill(kmin + i0, kmin + i1, 1 << 30); });
-  std::vector<std::vector<size_t>> by_sb((size_t)L * (size_t)nsb);
+  std::map<std::tuple<int, int, u64>, size_t> group_of;
+  std::vector<std::vector<size_t>> by_sb;
   for (size_t k = 0; k < bp_chunks.size(); ++k)
   {
     const int sb = (int)((bp_chunks[k].addr >> 12) & 0x3F), lv = (int)((bp_chunks[k].addr >> 60) & 0xF);
-    if (lv == bp_chunks[k].level && lv < L && sb < nsb)
-      by_sb[(size_t)lv * (size_t)nsb + (size_t)sb].push_back(k);
+    const u64 chunk = mixed_ranges ? 0 : (bp_chunks[k].addr >> 18) & 0x3FFFFFFFFFFull;
+    if (lv != bp_chunks[k].level || lv >= L || sb >= nsb)
+      continue;
+    auto it = group_of.emplace(std::make_tuple(lv, sb, chunk), by_sb.size()).first;
+    if (it->second == by_sb.size())
+      by_sb.emplace_back();
+    by_sb[it->second].push_back(k);
   }
   parallel_for(by_sb.size(), [&](size_t g) {
     for (size_t k : by_sb[g])
@@ -539,7 +555,11 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   parallel_ranges(nchan, [&](size_t i0, size_t i1) { std::fill(h->chan_off + i0, h->chan_off + i1, ~0ull); });
   parallel_for(entries.size(), [&](size_t k) {
     for (const chan_entry& e : entries[k])
-      h->chan_off[h->chan_first[e.slot] + (size_t)(e.bpkey - kmin[e.slot])] = e.off;
+    {
+      const int d = e.bpkey - kmin[e.slot];
+      if (d >= 0 && d < h->chan_n[e.slot])
+        h->chan_off[h->chan_first[e.slot] + (size_t)d] = e.off;
+    }
   });
   tt.lap("open.channels");
   return NoError;

@@ -636,7 +636,7 @@ struct segment_run
   packer::group* g = nullptr;
   size_t e0 = 0, e1 = 0;  // entries of g->events
   u64 chunk = 0;
-  std::deque<seg_key> keys;
+  std::vector<seg_key> keys;  // references into it live within one event
   std::vector<uint8_t> exps;
   u64 exp_last_brick = 0;
   int status = NoError;  // NoError, InvalidArgument, or -1: the range needs the sequential machine
@@ -647,6 +647,8 @@ void run_segment(segment_run& s, const machine& m)
   thread_local std::vector<int32_t> index;
   if (index.empty())
     index.assign(kKeySpace, -1);
+  s.keys.reserve(64);
+  s.exps.reserve((size_t)(s.e1 - s.e0) * 128);
   auto key = [&](int k) -> seg_key& {
     int32_t& i = index[(size_t)k];
     if (i < 0)
