@@ -247,6 +247,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
     cudaGetLastError();
   }
   cudaStream_t cs = split_out ? ctx->copies() : nullptr;
+  stream_fence out_copies{ cs };  // band copies into the caller's buffer end before any return
   int* d_err = (int*)ctx->ws("dec.err", 16);  // [0] brick kernel, [1] plane kernels (bit flags)
   uint64_t* d_geom = (uint64_t*)ctx->ws("dec.geom", sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
   if (!d_err || !d_geom)

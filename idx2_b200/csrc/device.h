@@ -235,6 +235,18 @@ struct device_ctx
   }
 };
 
+// Waits for a stream when it goes out of scope: a call that has copies of a caller's host
+// buffer in flight on a side stream returns only after them, on its error paths too.
+struct stream_fence
+{
+  cudaStream_t s = nullptr;
+  ~stream_fence()
+  {
+    if (s)
+      cudaStreamSynchronize(s);
+  }
+};
+
 // One field of a device encode (a launch may cover the bricks of many fields).
 struct batch_field
 {

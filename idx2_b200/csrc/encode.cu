@@ -1849,6 +1849,7 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
   const double before = enc_->kernel_ms();
   stage_timer tt;
   float ms = 0;
+  stream_fence host_copies{ level == 0 && host_field_ ? ctx_->copies() : nullptr };
   if (level == 0 && host_field_)
   {
     // the field is still in pinned host memory: its copy overlaps the level's launches
