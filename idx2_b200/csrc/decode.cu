@@ -450,7 +450,6 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       a.planes = d_planes;
       a.unit_off = d_uoff;
       cudaMemsetAsync(d_pcur, 0, 16, st);
-      const int pgrid = (int)((nunits + kPlaneWarps - 1) / kPlaneWarps);
       cudaEvent_t t0 = ctx->ev(2 * nev), t1 = ctx->ev(2 * nev + 1);
       if (!t0 || !t1)
         return CudaError;
@@ -471,7 +470,6 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
           k_decode_planes<true, true><<<2 * ctx->num_sms, kPlaneWarps * 32, 0, st>>>(p);
         }
       };
-      (void)pgrid;
       if (!split_level)
         launch_planes(pa);
       if (split_level)
