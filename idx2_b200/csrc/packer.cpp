@@ -46,6 +46,23 @@ void bit_writer::put(uint64_t v, int n)
 
 void bit_writer::put_varbyte(uint64_t v)
 {
+  if ((nbits & 7) == 0)
+  {
+    // byte-aligned (every size stream): the bytes go in whole
+    const size_t byte = (size_t)(nbits >> 3);
+    if (bytes.size() < byte + 16)
+      bytes.resize(std::max(byte + 16, bytes.size() * 2), 0);
+    uint8_t* d = bytes.data() + byte;
+    size_t n = 0;
+    do
+    {
+      const uint64_t more = (v >> 7) != 0;
+      d[n++] = (uint8_t)((v & 0x7F) | (more << 7));
+      v >>= 7;
+    } while (v && n < 10);
+    nbits += 8 * (uint64_t)n;
+    return;
+  }
   for (;;)
   {
     uint64_t more = (v >> 7) != 0;
