@@ -12,8 +12,10 @@ than L2 (126 MB), so no L2 flush is needed between steps.
           the compressed dataset resident in HBM (idx2g_encode_device + idx2g_decode into a
           device buffer), timed with CUDA events on the library's stream, max over ranks.
   e2e   : the same metric through the C ABI with host buffers: idx2g_encode of a pinned host
-          field (H2D, kernels, D2H, packing, zstd, files in a tmpfs) + idx2g_dataset_open of
-          the files + idx2g_decode into a pinned host buffer.
+          field (H2D in bands under level 0's launches, kernels, D2H of the streams, packing,
+          zstd, files in a tmpfs) + idx2g_dataset_open of the files (read, upload, index) +
+          idx2g_decode into a pinned host buffer (D2H in bands under the output level's
+          launches). Every copy of the step's data crosses PCIe inside the timed region.
 
 N > 1 (torchrun): every rank encodes/decodes its own independent field (weak scaling, no
 collective on the data path; timing uses a barrier and a max-reduction over ranks).
