@@ -124,6 +124,22 @@ def reference_sample(side):
     return f[:nz, :ny, :nx].contiguous().cpu().numpy()
 
 
+def reference_tiles(side):
+    """The whole workload field cut into 512 x 512 x 256 tiles (16 distinct tiles at 1024^3), x
+    fastest, each a contiguous array: the reference encodes one field per process, single
+    threaded, so the host cores share the field tile by tile."""
+    import torch
+    f = make_field(side, 7, "cuda" if torch.cuda.is_available() else "cpu")
+    tx, ty, tz = min(512, side), min(512, side), min(256, side)
+    tiles = []
+    for z in range(0, side, tz):
+        for y in range(0, side, ty):
+            for x in range(0, side, tx):
+                tiles.append(f[z:z + tz, y:y + ty, x:x + tx].contiguous().cpu().numpy())
+    del f
+    return tiles
+
+
 def run_reference_cli(sample, tmp, steps, warmup):
     """Encode + sequential decode of the sample with the reference's own CLI (oracle/_ref)."""
     app = os.path.join(ROOT, "oracle", "_ref", "idx2App")
@@ -149,7 +165,9 @@ def run_reference_cli(sample, tmp, steps, warmup):
     return times
 
 
-def cpu_baseline(side, steps=1, warmup=0):
+def cpu_baseline(side, steps=5, warmup=1):
+    """The reference CLI on one host core: encode + sequential decode of one 512 x 512 x 256
+    tile of the workload field, median of `steps` passes after `warmup` (about 25 s)."""
     app = os.path.join(ROOT, "oracle", "_ref", "idx2App")
     if not os.path.exists(app):
         return {"value": None, "unit": "GB/s", "cores": 1, "kind": "reference",
@@ -160,41 +178,47 @@ def cpu_baseline(side, steps=1, warmup=0):
     t = statistics.median(times)
     nz, ny, nx = sample.shape
     return {"value": 2 * sample.nbytes / t / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
-            "sample": f"{nx}x{ny}x{nz} float32 region of the same field; idx2App --encode (L={LEVELS}, "
-                      f"tol {TOL}) + sequential --decode, median of {len(times)}, {t:.2f} s per pass"}
+            "sample": f"{nx}x{ny}x{nz} float32 tile of the same field; idx2App --encode (L={LEVELS}, "
+                      f"tol {TOL}) + sequential --decode, median of {len(times)} after {warmup} warm-up, "
+                      f"{t:.2f} s per pass"}
 
 
-def run_reference_parallel(sample, tmp, procs, steps, warmup):
-    """The reference CLI on every host core: per step, `procs` independent pipelines (encode of
-    the sample + sequential decode, each in its own directory) run at once; the reference
-    encoder is single-threaded, so one pipeline per core is how it uses the host. Returns the
-    wall time of each timed step."""
+def run_reference_parallel(tiles, tmp, procs, steps, warmup):
+    """The reference CLI on every host core: per step, every tile of the field is encoded and
+    decoded (sequential decode) by its own idx2App pipeline, at most `procs` pipelines at once
+    (the reference encoder is single-threaded, so one pipeline per core is how it uses the
+    host). Returns the wall time of each timed step."""
     app = os.path.join(ROOT, "oracle", "_ref", "idx2App")
-    nz, ny, nx = sample.shape
-    raw = os.path.join(tmp, f"grf-f-[{nx}-{ny}-{nz}]-Float32.raw")
-    sample.tofile(raw)
+    raws = []
+    for k, t in enumerate(tiles):
+        nz, ny, nx = t.shape
+        d = os.path.join(tmp, f"t{k}")
+        os.makedirs(d, exist_ok=True)
+        raw = os.path.join(d, f"grf-f-[{nx}-{ny}-{nz}]-Float32.raw")
+        t.tofile(raw)
+        raws.append((d, raw))
+
+    def pipeline(d, raw):
+        out = os.path.join(d, "ds")
+        shutil.rmtree(out, ignore_errors=True)
+        os.makedirs(out)
+        enc = [app, "--encode", raw, "--num_levels", str(LEVELS), "--tolerance", str(TOL), "--out_dir", out]
+        dec = [app, "--decode", os.path.join(out, "grf", "f.idx2"), "--out_dir", out, "--out_file", "dec.raw"]
+        for cmd in (enc, dec):
+            r = subprocess.run(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+            if r.returncode:
+                raise RuntimeError("reference pipeline failed: " + r.stderr.decode()[-300:])
+
+    from concurrent.futures import ThreadPoolExecutor
     times = []
-    for i in range(warmup + steps):
-        cmds = []
-        for k in range(procs):
-            out = os.path.join(tmp, f"refds{k}")
-            shutil.rmtree(out, ignore_errors=True)
-            os.makedirs(out)
-            enc = [app, "--encode", raw, "--num_levels", str(LEVELS), "--tolerance", str(TOL), "--out_dir", out]
-            dec = [app, "--decode", os.path.join(out, "grf", "f.idx2"), "--out_dir", out, "--out_file", "dec.raw"]
-            cmds.append((enc, dec))
-        t0 = time.perf_counter()
-        running = [subprocess.Popen(enc, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE) for enc, _ in cmds]
-        for pr in running:
-            if pr.wait():
-                raise RuntimeError("reference encode failed: " + pr.stderr.read().decode()[-300:])
-        running = [subprocess.Popen(dec, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE) for _, dec in cmds]
-        for pr in running:
-            if pr.wait():
-                raise RuntimeError("reference decode failed: " + pr.stderr.read().decode()[-300:])
-        t1 = time.perf_counter()
-        if i >= warmup:
-            times.append(t1 - t0)
+    with ThreadPoolExecutor(max_workers=procs) as pool:
+        for i in range(warmup + steps):
+            t0 = time.perf_counter()
+            for fut in [pool.submit(pipeline, d, raw) for d, raw in raws]:
+                fut.result()
+            t1 = time.perf_counter()
+            if i >= warmup:
+                times.append(t1 - t0)
     return times
 
 
@@ -207,21 +231,24 @@ def reference_arm(args, rank, world):
                           "its sources) is not present on this machine"}))
         return
     procs = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
-    sample = reference_sample(args.side)
+    tiles = reference_tiles(args.side)
+    raw = sum(t.nbytes for t in tiles)
+    nz, ny, nx = tiles[0].shape
     with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as tmp:
-        times = run_reference_parallel(sample, tmp, procs, args.steps, args.warmup)
+        times = run_reference_parallel(tiles, tmp, procs, args.steps, args.warmup)
     t = sum(times) / len(times)
-    nz, ny, nx = sample.shape
-    v = procs * 2 * sample.nbytes / t / 1e9
-    desc = (f"{procs} concurrent pipelines (one per host core), each idx2App --encode + sequential --decode "
-            f"of a {nx}x{ny}x{nz} float32 region of the {args.side}^3 field per step (the reference encode is "
-            f"single-threaded); value = all pipelines' raw bytes / wall time")
+    v = 2 * raw / t / 1e9
+    desc = (f"the whole {args.side}^3 field per step as {len(tiles)} distinct {nx}x{ny}x{nz} float32 tiles, "
+            f"each encoded (idx2App --encode, L={LEVELS}, tol {TOL}) and decoded (sequential --decode) by "
+            f"its own reference pipeline, {procs} pipelines at once on the {procs} host cores (the "
+            f"reference encode is single-threaded); value = 2 x field bytes / wall time")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"grf{args.side}: {args.side}^3 float32 k^-5/3 GRF + 20 fronts, "
                        f"{LEVELS} levels, 32^3 bricks, tol {TOL}; encode + full-res decode",
-                       "parallelism": f"dp{world}"},
+                       "parallelism": f"dp{world}",
+                       "tiling": f"{len(tiles)} tiles of {nx}x{ny}x{nz}, each its own dataset"},
             "cpu_baseline": {"value": v, "unit": "GB/s", "cores": procs, "kind": "reference", "sample": desc},
             "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -400,10 +427,22 @@ def ours(args, rank, world, local_rank):
         "gpu_launches": int(timed_launches),
         "batched_encode": batch,
     }
+    # the whole decode (plane and level kernels of every level) against the same roof: the
+    # compressed streams and exponents it reads plus the grid it writes
+    dec_bytes = int(sum(lvl_bytes)) + raw_bytes
+    line["roofline_decode"] = {"bound": "hbm", "kernel": "k_decode_planes + k_decode_level (all levels)",
+                               "achieved": dec_bytes / (dec_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                               "frac": dec_bytes / (dec_ms * 1e-3) / 1e9 / peak, "algorithmic_bytes": dec_bytes}
+    _lib.lib().idx2g_ctx_destroy(h)
+    del field, out_dev, out_host, host
+    torch.cuda.empty_cache()
+    if world == 1 and not args.no_serve:
+        line["serving"] = serve_leg(args, requests=args.bench_serve_requests)
+    if world == 1 and not args.no_adjoint:
+        line["adjoint"] = adjoint_leg(args)
     print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
-    _lib.lib().idx2g_ctx_destroy(h)
 
 
 def batched_leg(dev, h, nfields=512, seed=7, reps=3):
@@ -475,11 +514,12 @@ def batched_leg(dev, h, nfields=512, seed=7, reps=3):
             "timing": "wall clock of the device stage (fields resident on the device), median of 3"}
 
 
-def serve_leg(args):
+def serve_leg(args, requests=None):
     """Decode serving: a device-resident compressed k^-5/3 field (3 levels, encoded at 1e-6)
     answering a Poisson stream of ROI requests (sides 32-512, per-axis downsampling 0-3,
     tolerance log-uniform 1e-6..1e-1), batched on arrival under the free-HBM budget, against
-    one-request-at-a-time decode of the same schedule. Prints one JSON line."""
+    one-request-at-a-time decode of the same schedule. Returns the result as a dict."""
+    requests = requests or args.serve_requests
     import torch
     import idx2_b200
     from idx2_b200.synthetic import grf_field_torch
@@ -506,7 +546,7 @@ def serve_leg(args):
         dec(srv.admit(poisson_schedule(srv.max_batch, args.serve_rate, dims, seed=3)))
         res = {}
         for mode in ("batched", "one-at-a-time"):
-            sched = poisson_schedule(args.serve_requests, args.serve_rate, dims, seed=2)
+            sched = poisson_schedule(requests, args.serve_rate, dims, seed=2)
             st = Server(dec, budget).run(sched, batched=(mode == "batched"))
             d = st.as_dict()
             d["decoded_gbs"] = st.decoded_bytes / st.elapsed_s / 1e9
@@ -514,16 +554,17 @@ def serve_leg(args):
         line = {"metric": "decode serving p50/p99 ms (ROI requests)", "impl": "ours",
                 "config": {"workload": f"serving: {dims[0]}x{dims[1]}x{dims[2]} float32 k^-5/3 field, 3 levels, "
                                        f"encoded at 1e-6; Poisson {args.serve_rate:g} req/s, "
-                                       f"{args.serve_requests} requests, ROI sides 32-512, downsampling 0-3, "
+                                       f"{requests} requests per mode, ROI sides 32-512, downsampling 0-3, "
                                        f"tolerance log-uniform 1e-6..1e-1",
                            "raw_bytes": int(raw), "compressed_bytes": int(info.file_bytes),
                            "hbm_budget_bytes": int(budget), "setup_s": setup_s},
                 "batched": res["batched"], "one_at_a_time": res["one-at-a-time"],
                 "p99_speedup": res["one-at-a-time"]["p99_ms"] / max(res["batched"]["p99_ms"], 1e-9)}
-        print(json.dumps(line))
         ds.close()
+        return line
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+        torch.cuda.empty_cache()
 
 
 def _adjoint_batch(dev, nfields, side, dtype, tmp, seed):
@@ -598,7 +639,8 @@ def adjoint_leg(args):
     0 and tolerance 1e-4) through the torch.autograd.Function, loss = MSE to a second seeded
     field set; a float64 batch at a smaller side. Checks: the float32 gradient against the
     float64 adjoint of the same residual, the dot-product identity, FP64 central differences
-    (step 1e-3 on 200 random coefficients), D against the bit-exact decode. Prints one JSON line."""
+    (step 1e-3 on 200 random coefficients), D against the bit-exact decode. Returns the result
+    as a dict."""
     import torch
     from idx2_b200 import diff
     from idx2_b200.synthetic import grf_field_torch
@@ -683,9 +725,10 @@ def adjoint_leg(args):
                            "dot_identity_rel_f64": dot64, "dot_identity_rel_f32": dot32,
                            "synth_vs_decode_rel_f32": d_rel, "synth_vs_decode_rel_f64": d_rel64},
                 "gpu_launches_per_step": 4}
-        print(json.dumps(line))
+        return line
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+        torch.cuda.empty_cache()
 
 
 def main():
@@ -706,17 +749,32 @@ def main():
     ap.add_argument("--serve-dims", default="2048x2048x1024", help="serving field dims (x, y, z)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrival rate (per second)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests per mode")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg of the default run")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-decode leg of the default run")
+    ap.add_argument("--bench-serve-requests", type=int, default=400,
+                    help="requests per mode of the serving leg inside the default run")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: launch the ranks here (the same command under torchrun)
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+        sys.exit(subprocess.call(cmd))
+    if world != args.gpus and rank == 0:
+        print(f"bench: --gpus {args.gpus} but WORLD_SIZE={world}; using {world} ranks", file=sys.stderr)
     if args.serve:
         if rank == 0:
-            serve_leg(args)
+            print(json.dumps(serve_leg(args)))
         return
     if args.adjoint:
         if rank == 0:
-            adjoint_leg(args)
+            print(json.dumps(adjoint_leg(args)))
         return
     if args.impl == "reference":
         reference_arm(args, rank, world)

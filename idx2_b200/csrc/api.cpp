@@ -146,6 +146,12 @@ IDX2G_API int idx2g_ctx_create(int device, void* stream, idx2g_ctx** out)
   }
   cudaEventCreate(&c->d.ev0);
   cudaEventCreate(&c->d.ev1);
+  // the allocation-free decode's fixed array is taken here, not at its first call
+  if (noalloc_prepare(device) != NoError)
+  {
+    idx2g_ctx_destroy(c);
+    return CudaError;
+  }
   *out = c;
   return NoError;
 }

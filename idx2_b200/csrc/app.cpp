@@ -7,7 +7,11 @@
 //             [--name N --field F --dims X Y Z --type float32|float64]
 //   idx2g_app --decode D/Name/Field.idx2 [--first x y z --last x y z]
 //             [--downsampling a b c] [--tolerance t] [--in_dir D] [--out_dir D]
-//             [--out_file F] [--dry] [--brick_map]
+//             [--out_file F] [--dry] [--brick_map] [--parallel]
+//
+// --parallel selects the reference's thread-pool decode (Applications/idx2App.cpp:56,
+// Core/idx2ParallelDecode.cpp:484), whose output equals its sequential decode's; every decode
+// here runs in parallel on the GPU, so the option is accepted and changes nothing.
 #include "../../include/idx2g.h"
 
 #include <chrono>

@@ -627,8 +627,9 @@ int decode_device::gather_bricks(device_ctx* ctx, const std::vector<brick_piece>
 // allocates the resident dataset) and then decodes into its own device buffer; every
 // temporary of the decode lives in the fixed array below.
 //
-// The array is a file-scope __device__ variable: every GPU that loads this library holds its
-// kNoAllocScratchBytes (about 7.3 MB) until the process exits. Limits: at most
+// The array is a file-scope __device__ variable: a device holds its kNoAllocScratchBytes
+// (about 7.3 MB) from the creation of the first context on it (noalloc_prepare loads this
+// file's module there) until the process exits. Limits: at most
 // kNoAllocMaxBricks bricks on the output level and at most kNoAllocLevelBricks bricks on each
 // coarser level a request decodes; larger requests are rejected with ScratchTooSmall.
 // All calls share the array and it keeps the last call's contents: the error word is cleared
@@ -654,28 +655,69 @@ constexpr size_t kNoAllocScratchBytes = kOffReq + ((sizeof(decode_target) + 255)
 
 static __device__ __align__(256) unsigned char g_decode_scratch[kNoAllocScratchBytes];
 
-// Device address of g_decode_scratch per device, resolved once per device by the first call
-// on that device (with that device current). In host code the symbol is only a stand-in.
+// Device address of g_decode_scratch, resolved with the device current and cached per
+// (device, CUDA context): a process that resets a device or makes a non-primary context current
+// gets the address of the array in that context. In host code the symbol is only a stand-in.
 std::mutex g_scratch_mu;
-void* g_scratch_addr[64] = {};
+struct scratch_entry
+{
+  void* cu_ctx;
+  void* addr;
+};
+scratch_entry g_scratch_addr[64] = {};
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link against libcuda)
+void* current_cu_context()
+{
+  using get_fn = int (*)(void**);
+  static get_fn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (get_fn) nullptr;
+    return (get_fn)p;
+  }();
+  void* c = nullptr;
+  if (!fn || fn(&c) != 0)
+    return nullptr;
+  return c;
+}
 
 int scratch_address(int device, unsigned char** out)
 {
   if (device < 0 || device >= 64)
     return InvalidArgument;
+  void* cu = current_cu_context();
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[device])
+  scratch_entry& e = g_scratch_addr[device];
+  if (!e.addr || e.cu_ctx != cu)
   {
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_decode_scratch) != cudaSuccess || !p)
       return CudaError;
-    g_scratch_addr[device] = p;
+    e.addr = p;
+    e.cu_ctx = cu;
   }
-  *out = (unsigned char*)g_scratch_addr[device];
+  *out = (unsigned char*)e.addr;
   return NoError;
 }
 
 } // namespace
+
+// Loads this file's kernels into the current context and resolves the scratch array's
+// address. With lazy module loading (the CUDA default since 12.2) the module, and with it the
+// array's device memory, would otherwise come into being at the first launch from this file;
+// the context set-up calls this so that the memory is taken there, before any
+// allocation-free decode.
+int noalloc_prepare(int device)
+{
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, k_decode_level) != cudaSuccess)
+    return CudaError;
+  unsigned char* base = nullptr;
+  return scratch_address(device, &base);
+}
 
 int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, void* d_out, size_t out_bytes,
                                   double* kernel_ms)
@@ -700,6 +742,10 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
   }
   if (cudaSetDevice(ctx->device) != cudaSuccess)
     return CudaError;
+  // the call waits for its stream after every level, which a stream under capture does not allow
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(ctx->stream, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+    return InvalidArgument;
   unsigned char* base = nullptr;
   int e = scratch_address(ctx->device, &base);
   if (e)

@@ -123,4 +123,8 @@ private:
 // Give the device memory that no open dataset holds back to the driver.
 void trim_dataset_pool(int device);
 
+// Loads the decode kernels into the current context and resolves the allocation-free
+// decode's scratch array there (called when a context is created on the device).
+int noalloc_prepare(int device);
+
 } // namespace idx2g

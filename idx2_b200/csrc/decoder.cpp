@@ -23,11 +23,13 @@
 #include <fcntl.h>
 #include <map>
 #include <memory>
+#include <set>
 #include <tuple>
 #include <sys/stat.h>
 #include <thread>
 #include <unistd.h>
 #include <unordered_map>
+#include <unordered_set>
 
 namespace idx2g
 {
@@ -148,6 +150,12 @@ struct dataset_handle
     size_t need = 0;
   };
   std::vector<std::unique_ptr<cached_plan>> plans;
+  // what the files lack, for the reference's decode-time errors: the data files that were not
+  // found (per level, the bits of the linear brick index that select the file) and the
+  // exponent chunks present (their chunk addresses)
+  std::vector<std::map<u64, int>> bad_files;  // per level: file bits -> FileNotFound / SizeMismatched
+  std::vector<int> file_shift;
+  std::unordered_set<u64> exp_chunk_addrs;
 };
 
 namespace
@@ -157,6 +165,7 @@ struct data_file
 {
   std::string path;
   int level;
+  u64 bits = 0;  // the bits of the linear brick index that select this file
   size_t base = 0, size = 0;
 };
 
@@ -247,7 +256,9 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   // leaves its bricks undecoded (Core/idx2Decode.cpp:166-168). A file's path depends on the
   // bits of the linear brick index above `shift` only, so it is built once per run of bricks
   // that share them.
-  std::map<std::string, int> names;
+  std::map<std::string, std::pair<int, u64>> names;  // path -> (level, file bits of the brick index)
+  h->bad_files.assign((size_t)L, {});
+  h->file_shift.assign((size_t)L, 0);
   for (int l = 0; l < L; ++l)
   {
     const std::vector<int>& dd = f.files_dirs_depth[(size_t)l];
@@ -255,6 +266,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     for (size_t d = 0; d + 1 < dd.size(); ++d)
       shift -= dd[d];
     shift = shift < 0 ? 0 : shift > 63 ? 63 : shift;
+    h->file_shift[(size_t)l] = shift;
     u64 prev = ~0ull;
     for (size_t i = 0; i < h->brick3[(size_t)l].size(); ++i)
     {
@@ -262,7 +274,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
       if ((lin >> shift) == prev)
         continue;
       prev = lin >> shift;
-      names[file_path(f, lin, l)] = l;
+      names[file_path(f, lin, l)] = { l, lin >> shift };
     }
   }
   std::vector<data_file> files;
@@ -271,10 +283,15 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   {
     struct stat st;
     if (stat(kv.first.c_str(), &st) != 0 || !S_ISREG(st.st_mode))
+    {
+      // decoding a brick of this file fails with FileNotFound (Core/idx2Read.cpp:270,380)
+      h->bad_files[(size_t)kv.second.first][kv.second.second] = FileNotFound;
       continue;
+    }
     data_file df;
     df.path = kv.first;
-    df.level = kv.second;
+    df.level = kv.second.first;
+    df.bits = kv.second.second;
     df.base = total;
     df.size = (size_t)st.st_size;
     total += (df.size + 15) & ~(size_t)15;
@@ -355,6 +372,23 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     if (ssz < 0 || (size_t)ssz + (size_t)asz + 16 > (size_t)total_e)
       return CorruptStream;
     bit_reader sr{ d + E - 16 - (size_t)asz - (size_t)ssz, (size_t)ssz };
+    {
+      // the reference counts the size varbytes (to the end of their section) against the
+      // chunk count, and wants whole sets of subbands; otherwise decoding any brick of the
+      // file fails with SizeMismatched (Core/idx2Read.cpp:304-323)
+      bit_reader cnt{ sr.p, sr.n };
+      long long n2 = 0;
+      while ((cnt.pos >> 3) < (uint64_t)ssz)
+      {
+        cnt.varbyte();
+        ++n2;
+      }
+      if (n2 != nexp || nexp % nsb != 0)
+      {
+        h->bad_files[(size_t)level][df.bits] = SizeMismatched;
+        continue;
+      }
+    }
     const size_t exp_beg = E - (size_t)total_e;
     size_t off = exp_beg;
     for (int c = 0; c < nexp; ++c)
@@ -398,6 +432,8 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     }
   }
 
+  for (const chunk_ref& c : exp_chunks)
+    h->exp_chunk_addrs.insert(c.addr);
   tt.lap("open.tails");
   // exponent chunks: decompress and spread over their bricks (chunks own disjoint rows)
   const int esz = f.type == dtype::float32 ? 1 : 2;
@@ -724,6 +760,18 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
           int bi = h->brick_index[(size_t)l][lin];
           if (bi < 0)
             continue;
+          // the reference reads the brick's exponents for every decoded subband first and
+          // fails with FileNotFound / ChunkNotFound when its file or exponent chunk is absent
+          // (Core/idx2Decode.cpp:104-106, Core/idx2Read.cpp:378-388)
+          if (!h->bad_files[(size_t)l].empty())
+          {
+            auto bf = h->bad_files[(size_t)l].find(lin >> h->file_shift[(size_t)l]);
+            if (bf != h->bad_files[(size_t)l].end())
+              return bf->second;
+          }
+          for (int s = 0; s < nsb; ++s)
+            if (((lv.mask >> s) & 1) && !h->exp_chunk_addrs.count(chunk_address(f, lin, l, s, 0)))
+              return ChunkNotFound;
           decode_brick db;
           db.flat = (long long)(h->level_brick_base[(size_t)l] + (size_t)bi);
           db.parent = -1;

@@ -135,14 +135,15 @@ IDX2G_API int idx2g_decode_batch(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_
    latency-bound serving loops, where cudaMalloc fails or synchronises the device. Open the
    dataset first (idx2g_dataset_open allocates the resident dataset), then call this with a
    device output buffer; it calls no cudaMalloc / cudaFree and no allocating library routine.
-   Its temporaries live in a fixed device array of about 7.3 MB that every GPU loading the
-   library holds until the process exits. Limits: at most 4096 bricks on the output level and
+   Its temporaries live in a fixed device array of about 7.3 MB, taken on a device when the
+   first context is created there (idx2g_ctx_create loads the library's decode kernels and
+   resolves the array's device address with cudaGetSymbolAddress, that device current) and
+   held until the process exits. Limits: at most 4096 bricks on the output level and
    8 bricks on each coarser level the request decodes; larger requests return
-   ScratchTooSmall (104). The first call on a device resolves the array's device address
-   (cudaGetSymbolAddress) with that device current; make that first call before any stream
-   capture. All calls share the array and it keeps the last call's contents (the error word
-   is cleared by every call); calls that overlap on the GPU race on it. The result equals
-   idx2g_decode's. */
+   ScratchTooSmall (104). The call waits for the context's stream between levels, so on a
+   stream that is being captured it returns InvalidArgument. All calls share the array and it
+   keeps the last call's contents (the error word is cleared by every call); calls that
+   overlap on the GPU race on it. The result equals idx2g_decode's. */
 IDX2G_API int idx2g_decode_noalloc(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_params* p,
                                    void* d_out, size_t out_bytes, double* kernel_ms);
 

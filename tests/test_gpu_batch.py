@@ -103,3 +103,54 @@ def test_batch_of_more_shapes_than_the_plan_cache(idx2g, tmp_path, monkeypatch):
     for nm in names:
         diffs = compare_dirs(str(tmp_path / "single" / nm), str(tmp_path / "batch" / nm))
         assert diffs == [], (nm, diffs[:3])
+
+
+@pytest.mark.gpu
+def test_uneven_batch_of_64_fields_matches_reference(idx2g, ref_app, tmp_path):
+    """The uneven-field workload at scale: 64 accepted fields drawn like the batched-encode
+    benchmark (k^-5/3 Gaussian random fields scaled to [-1, 1], each axis 17-300, 1 in 8 2D,
+    float32 and float64 alternating, levels 1-3, tolerance 1e-3) in one batched call; every
+    field's files equal the reference CLI's encode of that field."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from idx2_b200.synthetic import grf_field_torch
+    rng = np.random.default_rng(77)
+    fields, params = [], []
+    i = 0
+    while len(fields) < 64:
+        dims = [int(rng.integers(17, 301)) for _ in range(3)]
+        if rng.integers(0, 8) == 0:
+            dims[2] = 1
+        dt = "float32" if i % 2 == 0 else "float64"
+        lv = int(rng.integers(1, 4))
+        bd = (32, 32, 1) if dims[2] == 1 else (32, 32, 32)
+        i += 1
+        if idx2g.check_params(idx2g.Params(dims=dims, dtype=dt, brick_dims=bd, num_levels=lv, tolerance=1e-3)):
+            continue
+        f = grf_field_torch(dims[0], dims[1], dims[2], seed=9000 + i, scale="range", device=torch.device("cuda", 0))
+        fields.append(f.to(torch.float32 if dt == "float32" else torch.float64).contiguous())
+        params.append((dims, dt, lv))
+    assert {p[1] for p in params} == {"float32", "float64"} and any(p[0][2] == 1 for p in params)
+    names = [f"u{k}" for k in range(len(fields))]
+    idx2g.encode_batch(fields, out_dir=str(tmp_path / "batch"), names=names, field_names=["f"] * len(fields),
+                       num_levels=[p[2] for p in params], tolerances=[1e-3] * len(fields), graph=True,
+                       autotune=True)
+
+    def ref_one(k):
+        (nx, ny, nz), dt, lv = params[k]
+        raw = str(tmp_path / f"{names[k]}-f-[{nx}-{ny}-{nz}]-{dt.capitalize()}.raw")
+        fields[k].cpu().numpy().tofile(raw)
+        args = [ref_app, "--encode", raw, "--num_levels", str(lv), "--tolerance", "0.001",
+                "--out_dir", str(tmp_path / "ref")]
+        if nz == 1:
+            args += ["--brick_size", "32", "32", "1"]
+        r = subprocess.run(args, capture_output=True, text=True)
+        os.remove(raw)
+        return r.returncode, r.stdout[-300:] + r.stderr[-300:]
+
+    with ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1))) as pool:
+        results = list(pool.map(ref_one, range(len(fields))))
+    for k, (rc, msg) in enumerate(results):
+        assert rc == 0, (names[k], msg)
+        diffs = compare_dirs(str(tmp_path / "ref" / names[k]), str(tmp_path / "batch" / names[k]))
+        assert diffs == [], (names[k], params[k], diffs[:3])
