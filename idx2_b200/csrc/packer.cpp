@@ -1,5 +1,6 @@
 // Chunk/file packer (Core/idx2Write.cpp, Core/idx2Encode.cpp:41-137,233-249).
 #include "packer.h"
+#include "zstd_frame.h"
 
 #include "encoder.h"
 #include "parallel.h"
@@ -87,7 +88,7 @@ double pack_stats::acc::sd() const
 }
 
 // ----------------------------------------------------------------------------
-// zstd through the system library
+// zstd: frames written by zstd_frame.cpp, read through the system library
 // ----------------------------------------------------------------------------
 
 namespace
@@ -131,17 +132,12 @@ const char* zstd_version()
 
 int zstd_compress(const uint8_t* src, size_t n, std::vector<uint8_t>* out)
 {
-  // Core/idx2Encode.cpp:23 CompressBufZstd: empty input gives an empty output
+  // Core/idx2Encode.cpp:23 CompressBufZstd: empty input gives an empty output; otherwise one
+  // level-1 frame, byte-identical to the reference's vendored zstd 1.4.5 (zstd_frame.cpp)
   out->clear();
   if (n == 0)
     return NoError;
-  if (!zapi().ok)
-    return UnknownError;
-  out->resize(zapi().bound(n));
-  size_t r = zapi().compress(out->data(), out->size(), src, n, 1);
-  if (zapi().is_error(r))
-    return UnknownError;
-  out->resize(r);
+  zstd145::compress(src, n, out);
   return NoError;
 }
 

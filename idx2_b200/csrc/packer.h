@@ -147,7 +147,8 @@ private:
   pack_stats stats_;
 };
 
-// zstd level 1 through the system libzstd (loaded at run time).
+// zstd level 1: frames byte-identical to the reference's zstd 1.4.5 (zstd_frame.cpp); the
+// decompression goes through the system libzstd (loaded at run time; any version reads them).
 int zstd_compress(const uint8_t* src, size_t n, std::vector<uint8_t>* out);
 int zstd_decompress(const uint8_t* src, size_t n, std::vector<uint8_t>* out);
 const char* zstd_version();

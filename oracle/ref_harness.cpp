@@ -15,6 +15,10 @@
 
 #include <string.h>
 
+// the reference's vendored zstd 1.4.5 (compiled into the reference library)
+extern "C" size_t ZSTD_compress(void* dst, size_t cap, const void* src, size_t n, int level);
+extern "C" size_t ZSTD_compressBound(size_t n);
+
 using namespace idx2;
 
 namespace
@@ -330,6 +334,25 @@ ref_output_grid(int nx, int ny, int nz, int bx, int by, int bz, int nlevels, int
   }
   Dealloc(&F);
   return 0;
+}
+
+/* The reference's exponent-chunk / address-table compression (Core/idx2Encode.cpp:23
+   CompressBufZstd): ZSTD_compress at level 1 of the vendored zstd 1.4.5. Returns the frame size
+   (0 for an empty input, as CompressBufZstd writes nothing then). */
+size_t
+ref_zstd_compress(const void* src, size_t n, void* dst, size_t cap)
+{
+  if (n == 0)
+    return 0;
+  if (cap < ZSTD_compressBound(n))
+    return 0;
+  return ZSTD_compress(dst, cap, src, n, 1);
+}
+
+size_t
+ref_zstd_bound(size_t n)
+{
+  return ZSTD_compressBound(n);
 }
 
 } // extern "C"

@@ -10,6 +10,7 @@ SRCS = [
     os.path.join(ROOT, "tests", "cpp", "oracle_encode.cpp"),
     os.path.join(ROOT, "idx2_b200", "csrc", "format.cpp"),
     os.path.join(ROOT, "idx2_b200", "csrc", "packer.cpp"),
+    os.path.join(ROOT, "idx2_b200", "csrc", "zstd_frame.cpp"),
     os.path.join(ROOT, "idx2_b200", "csrc", "encoder.cpp"),
 ]
 ORACLE_C = os.path.join(ROOT, "oracle", "idx2_oracle.c")

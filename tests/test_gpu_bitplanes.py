@@ -1,7 +1,7 @@
 """BitPlanesPerChunk > 1 (several bit planes per channel key, Core/idx2Encode.cpp:195-206 and
 Core/idx2Decode.cpp:144-162) on the device: dataset files against the reference encoder's
-(every byte outside zstd frames identical, every frame identical after decompression), and
-decoded grids against the reference decoder's, byte for byte."""
+(every byte identical, zstd frames included), and decoded grids against the reference
+decoder's, byte for byte."""
 import ctypes
 import os
 import subprocess

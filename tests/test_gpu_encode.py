@@ -1,8 +1,8 @@
 """GPU encode parity: the CUDA library's dataset files against the reference's.
 
-Every data-file byte outside the zstd frames must be identical, and every zstd
-frame must decompress to identical bytes (the reference vendors zstd 1.4.5, this
-library uses the system libzstd, so compressed frame bytes may differ)."""
+Every file must be byte-identical to the reference's, the zstd frames of the exponent
+chunks and address tables included (the library writes the frames of the reference's
+vendored zstd 1.4.5)."""
 import os
 import shutil
 import subprocess
