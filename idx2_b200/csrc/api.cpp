@@ -6,6 +6,7 @@
 #include "device.h"
 #include "encoder.h"
 #include "format.h"
+#include "shard.h"
 #include "trace.h"
 
 #include <chrono>
@@ -307,6 +308,149 @@ IDX2G_API int idx2g_encode_device(idx2g_ctx* c, const idx2g_params* in, const vo
     }
   }
   return NoError;
+}
+
+namespace
+{
+
+// A sharded encode between idx2g_encode_shard and idx2g_encode_shard_finish.
+struct shard_job
+{
+  params p;
+  dataset_format f;
+  std::shared_ptr<const encode_plan> plan;
+  shard_plan sp;
+  std::unique_ptr<gpu_coder> coder;
+  std::vector<level_output> outs;
+  std::vector<uint8_t> headers;
+  double device_s = 0;
+};
+
+int shard_setup(const idx2g_params* in, int shard, int nshards, params* p, dataset_format* f,
+                encode_plan* own_plan, shard_plan* sp)
+{
+  to_params(in, p);
+  int e = finalize(f, p);
+  if (e)
+    return e;
+  e = make_encode_plan(*f, own_plan);
+  if (e)
+    return e;
+  return make_shard_plan(*f, *own_plan, nshards, shard, sp);
+}
+
+} // namespace
+
+IDX2G_API int idx2g_shard_region(const idx2g_params* in, int shard, int nshards, int from3[3], int dims3[3])
+{
+  if (!in || !from3 || !dims3)
+    return InvalidArgument;
+  params p;
+  dataset_format f;
+  encode_plan plan;
+  shard_plan sp;
+  int e = shard_setup(in, shard, nshards, &p, &f, &plan, &sp);
+  if (e)
+    return e;
+  for (int k = 0; k < 3; ++k)
+  {
+    from3[k] = k == 0 ? sp.region.from.x : k == 1 ? sp.region.from.y : sp.region.from.z;
+    dims3[k] = k == 0 ? sp.region.dims.x : k == 1 ? sp.region.dims.y : sp.region.dims.z;
+  }
+  return NoError;
+}
+
+IDX2G_API int idx2g_encode_shard(idx2g_ctx* c, const idx2g_params* in, const void* d_field, const int origin3[3],
+                                 const int dims3[3], int shard, int nshards, const void** headers,
+                                 size_t* header_bytes, double* vmin, double* vmax, idx2g_encode_info* info)
+{
+  if (!c || !in || !d_field || !origin3 || !dims3 || !headers || !header_bytes)
+    return InvalidArgument;
+  cudaSetDevice(c->d.device);
+  c->d.shard.reset();
+  auto job = std::make_shared<shard_job>();
+  to_params(in, &job->p);
+  int e = finalize(&job->f, &job->p);
+  if (e)
+    return e;
+  job->plan = c->d.plan_for(job->f, &e);
+  if (!job->plan)
+    return e;
+  e = make_shard_plan(job->f, *job->plan, nshards, shard, &job->sp);
+  if (e)
+    return e;
+  // the buffer must hold the shard's region, from a brick-aligned origin
+  const v3 o(origin3[0], origin3[1], origin3[2]), d(dims3[0], dims3[1], dims3[2]);
+  const extent& r = job->sp.region;
+  const v3 bd = job->f.brick_dims;
+  if (o.x % bd.x || o.y % bd.y || o.z % bd.z || o.x > r.from.x || o.y > r.from.y || o.z > r.from.z ||
+      o.x + d.x < r.from.x + r.dims.x || o.y + d.y < r.from.y + r.dims.y || o.z + d.z < r.from.z + r.dims.z)
+    return InvalidArgument;
+  job->coder.reset(new gpu_coder(&c->d, job->f, d_field, job->p.type == dtype::float32));
+  job->coder->set_field_region(o, d);
+  const auto t0 = std::chrono::steady_clock::now();
+  e = encode_levels(&job->f, job->coder.get(), &job->outs, job->sp.local);
+  if (e)
+    return e;
+  job->device_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  e = shard_headers(job->f, *job->plan, job->sp, job->outs, &job->headers);
+  if (e)
+    return e;
+  *headers = job->headers.data();
+  *header_bytes = job->headers.size();
+  if (vmin)
+    *vmin = job->f.value_min;
+  if (vmax)
+    *vmax = job->f.value_max;
+  if (info)
+  {
+    memset(info, 0, sizeof *info);
+    info->kernel_ms = job->coder->kernel_ms();
+    info->device_s = job->device_s;
+    info->stream_bytes = job->coder->stream_bytes();
+    info->exp_bytes = job->coder->exp_bytes();
+    info->kernel_launches = job->coder->kernel_launches();
+    info->value_min = job->f.value_min;
+    info->value_max = job->f.value_max;
+    info->num_levels = (int)job->coder->level_ms().size();
+    for (size_t i = 0; i < job->coder->level_ms().size() && i < 16; ++i)
+    {
+      info->level_kernel_ms[i] = job->coder->level_ms()[i];
+      info->level_out_bytes[i] = job->coder->level_bytes()[i];
+    }
+  }
+  c->d.shard = job;
+  return NoError;
+}
+
+IDX2G_API int idx2g_encode_shard_finish(idx2g_ctx* c, const idx2g_params* in, int shard, int nshards,
+                                        const void* const* headers, const size_t* header_bytes, double vmin,
+                                        double vmax, idx2g_encode_info* info)
+{
+  if (!c || !in || !headers || !header_bytes)
+    return InvalidArgument;
+  std::shared_ptr<shard_job> job = std::static_pointer_cast<shard_job>(c->d.shard);
+  if (!job || job->sp.shard != shard || job->sp.nshards != nshards)
+    return InvalidArgument;  // no idx2g_encode_shard of this shard before
+  c->d.shard.reset();
+  job->f.value_min = vmin;
+  job->f.value_max = vmax;
+  std::vector<const uint8_t*> blobs((size_t)nshards);
+  std::vector<size_t> sizes((size_t)nshards);
+  for (int s = 0; s < nshards; ++s)
+  {
+    blobs[(size_t)s] = (const uint8_t*)headers[s];
+    sizes[(size_t)s] = header_bytes[s];
+  }
+  encode_timing tm;
+  const int e = pack_shard(&job->f, &job->p, *job->plan, job->sp, job->outs, blobs, sizes, &tm);
+  if (info)
+  {
+    info->pack_s = tm.pack_s;
+    info->write_s = tm.write_s;
+    info->file_bytes = (long long)tm.file_bytes;
+  }
+  return e;
 }
 
 IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const void* const* fields, int n,

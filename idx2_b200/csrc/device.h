@@ -42,6 +42,7 @@ struct device_ctx
   }
   long long launches = 0;  // kernels launched on this context so far
   std::map<std::string, int> tuned;  // batched encode: CTAs per SM chosen per batch signature
+  std::shared_ptr<void> shard;       // a sharded encode between its two calls (api.cpp)
   // Encode plans by format: the brick order and the EncodeSubband events depend only on the
   // dims, the brick dims and the number of levels, so repeated encodes of fields of one shape
   // (the time steps of a simulation) plan once.
@@ -254,6 +255,9 @@ struct batch_field
   const encode_plan* plan = nullptr;
   const void* d_field = nullptr;  // device pointer
   bool f32 = true;
+  // the samples d_field holds: [field_origin, field_origin + field_dims) of the dataset
+  // (field_dims 0: the whole dataset); the origin is a multiple of the brick size
+  v3 field_origin, field_dims;
   std::vector<level_output>* outs = nullptr;  // receives one entry per level
   double vmin = 1.7976931348623157e308, vmax = -1.7976931348623157e308;
   long long stream_bytes = 0, exp_bytes = 0;
@@ -320,6 +324,13 @@ public:
   // The field's samples are in pinned host memory `host`; d_field (given at construction) is
   // the device buffer they go to, copied while level 0 runs.
   void set_host_field(const void* host) { host_field_ = host; }
+  // d_field holds only the samples [origin, origin + dims) of the dataset (a shard's region;
+  // origin a multiple of the brick size)
+  void set_field_region(v3 origin, v3 dims)
+  {
+    fields_[0].field_origin = origin;
+    fields_[0].field_dims = dims;
+  }
   double kernel_ms() const { return enc_ ? enc_->kernel_ms() : 0.0; }
   long long kernel_launches() const { return enc_ ? enc_->launches() : 0; }
   long long stream_bytes() const { return fields_[0].stream_bytes; }

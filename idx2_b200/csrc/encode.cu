@@ -1364,9 +1364,10 @@ int batch_encoder::prepare(const batch_tuning& t)
       ef.order = f.transform_order;
       ef.field = J[j].d_field;
       ef.field_f32 = J[j].f32;
-      ef.fdims[0] = f.dims.x;
-      ef.fdims[1] = f.dims.y;
-      ef.fdims[2] = f.dims.z;
+      const v3 fd = J[j].field_dims.x > 0 ? J[j].field_dims : f.dims;
+      ef.fdims[0] = fd.x;
+      ef.fdims[1] = fd.y;
+      ef.fdims[2] = fd.z;
       level_weights(f, l, ef.weight, &ef.norm_mask);
       ef.bpc = f.bit_planes_per_chunk;
       if (ef.end_bp == 64)
@@ -1397,8 +1398,10 @@ int batch_encoder::prepare(const batch_tuning& t)
       field_layout.push_back(li->second);
       const std::vector<brick_entry>& bricks = J[j].plan->levels[(size_t)l];
       const bool has_parent = l + 1 < f.nlevels;
+      // level 0 reads the field: brick coordinates relative to the samples the buffer holds
+      const v3 ob = l == 0 ? J[j].field_origin / f.brick_dims : v3(0);
       for (const brick_entry& e : bricks)
-        ll.bricks.push_back(enc_brick{ { e.brick3.x, e.brick3.y, e.brick3.z },
+        ll.bricks.push_back(enc_brick{ { e.brick3.x - ob.x, e.brick3.y - ob.y, e.brick3.z - ob.z },
                                        { e.valid.x, e.valid.y, e.valid.z },
                                        has_parent ? first[(size_t)l + 1][j] + e.parent : -1,
                                        { e.pos_in_parent.x, e.pos_in_parent.y, e.pos_in_parent.z },

@@ -623,7 +623,7 @@ int run_group(packer::group& g, const machine& m)
       const uint32_t nb = r.sizes[k - r.kmin];
       if (!nb)
         continue;
-      append_brick(g.chan(k), brick, r.bytes + off, nb);
+      append_brick(g.chan(k), brick, r.bytes ? r.bytes + off : nullptr, nb);
       off += nb;
     }
   }
@@ -718,7 +718,7 @@ void run_segment(segment_run& s, const machine& m)
         s.status = -1;  // data of a channel that did not enter: not separable
         break;
       }
-      append_brick(st.ch, brick, r.bytes + off, nb);
+      append_brick(st.ch, brick, r.bytes ? r.bytes + off : nullptr, nb);
       off += nb;
     }
   }

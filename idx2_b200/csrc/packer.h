@@ -49,7 +49,8 @@ struct subband_result
   int nexps = 0;
   int kmin = 1, kmax = 0;            // bit-plane channel keys present (kmin > kmax: none)
   const uint32_t* sizes = nullptr;   // bytes per key, index key - kmin (0: absent)
-  const uint8_t* bytes = nullptr;    // channel streams back to back, ascending key order
+  const uint8_t* bytes = nullptr;    // channel streams back to back, ascending key order; null
+                                     // for another shard's brick (its segments stay null)
 };
 
 struct pack_stats

@@ -176,6 +176,31 @@ IDX2G_API int idx2g_decode_brick_map(idx2g_ctx* ctx, idx2g_dataset* ds, const id
 IDX2G_API int idx2g_encode_batch(idx2g_ctx* ctx, const idx2g_params* params, const void* const* fields,
                                  int n, int fields_on_device, int flags, idx2g_encode_info* infos);
 
+/* Sharded encode: one field encoded by several processes (one GPU each) into one dataset,
+   the files identical to a single encode's. No counterpart in the reference, whose encode
+   runs on one thread (Core/idx2Encode.cpp:390); the split follows its depth-first order
+   (Core/idx2Encode.cpp:276-340): the coarsest level's bricks, in encode order, are cut into
+   nshards runs and every shard codes the subtrees under its run. The coded data never moves
+   between shards; they exchange only the headers of their (brick, subband) regions.
+
+   idx2g_shard_region gives the samples shard `shard` reads ([from3, from3 + dims3)).
+   idx2g_encode_shard codes that shard's bricks from d_field (a device buffer holding the
+   dataset's samples [origin3, origin3 + dims3), which must cover the shard's region; origin3
+   a multiple of the brick size) and returns its header payload (valid until the shard's
+   finish call on the same context) and the value range of its samples. The caller exchanges
+   the payloads (all-gather) and reduces the value range, then every shard calls
+   idx2g_encode_shard_finish with all payloads in shard order: each writes its bricks' bytes
+   into the shared data files at offsets every shard computes alike, shard 0 also the chunk
+   headers, tables, exponent chunks and the metadata file. The files are complete once every
+   shard's finish call has returned. */
+IDX2G_API int idx2g_shard_region(const idx2g_params* p, int shard, int nshards, int from3[3], int dims3[3]);
+IDX2G_API int idx2g_encode_shard(idx2g_ctx* ctx, const idx2g_params* p, const void* d_field, const int origin3[3],
+                                 const int dims3[3], int shard, int nshards, const void** headers,
+                                 size_t* header_bytes, double* vmin, double* vmax, idx2g_encode_info* info);
+IDX2G_API int idx2g_encode_shard_finish(idx2g_ctx* ctx, const idx2g_params* p, int shard, int nshards,
+                                        const void* const* headers, const size_t* header_bytes, double vmin,
+                                        double vmax, idx2g_encode_info* info);
+
 /* Differentiable decode. The reference has no counterpart: its decode is integer end to end
    (Core/idx2Decode.cpp:141-320). Here the decode is also available as a real-valued linear
    operator D from the dequantised zfp-domain coefficients to the grid: the reference's decode
