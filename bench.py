@@ -17,8 +17,13 @@ than L2 (126 MB), so no L2 flush is needed between steps.
           idx2g_decode into a pinned host buffer (D2H in bands under the output level's
           launches). Every copy of the step's data crosses PCIe inside the timed region.
 
-N > 1 (torchrun): every rank encodes/decodes its own independent field (weak scaling, no
-collective on the data path; timing uses a barrier and a max-reduction over ranks).
+N > 1 (torchrun, or --gpus N, which launches the ranks itself): one dataset of N side^3
+blocks (2048x1024x1024 for 2 GPUs, 2048^3 for 8), encoded as N shards: each GPU codes the
+subtrees of its run of coarsest bricks from its own block of samples and decodes that block
+(weak scaling). The device-resident leg has no collective on its data path; the end-to-end leg
+all-gathers the shards' region headers and all-reduces the value range over NCCL before every
+rank writes its bytes into the shared files. Timing: barriers, CUDA events on the library's
+stream, max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--side 1024]
 """
@@ -254,12 +259,171 @@ def reference_arm(args, rank, world):
     print(json.dumps(line))
 
 
+def global_dims(side, world):
+    """One dataset for `world` GPUs: a side^3 block per GPU, the blocks doubling the dataset
+    along x, then y, then z (powers of two; other counts line the blocks up along x)."""
+    d = [side, side, side]
+    n, k = world, 0
+    if n & (n - 1):
+        return (side * world, side, side)
+    while n > 1:
+        d[k % 3] *= 2
+        n //= 2
+        k += 1
+    return tuple(d)
+
+
+def ours_sharded(args, rank, world, local_rank):
+    """N > 1: one dataset of N side^3 blocks (weak scaling), encoded as N shards (each GPU the
+    subtrees of its run of coarsest bricks, read from its own block of samples) and decoded
+    block by block. value: the device stage of every shard (idx2g_encode_shard, device only)
+    + the decode of its block from the resident dataset, max over ranks; e2e: per step the
+    block crosses to the device, each shard codes, the ranks all-gather their region headers
+    and all-reduce the value range over NCCL, every rank writes its bytes into the shared
+    files, opens the dataset and decodes its block into pinned host memory."""
+    import ctypes
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from idx2_b200 import _lib
+    from idx2_b200.sharded import ShardEncode, exchange, shard_region
+    from idx2_b200.synthetic import grf_field_torch
+
+    # --dist-backend gloo runs the ranks' logic on fewer GPUs than ranks (a functional check of
+    # the multi-process path: the ranks' kernels never wait on one another); measurements use NCCL
+    local_rank = local_rank % max(1, torch.cuda.device_count())
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=300))
+    stream = torch.cuda.Stream(device=dev)
+    _lib.ctx_on_stream(local_rank, stream)  # the library's work on a stream the events can bracket
+    side = args.side
+    gd = global_dims(side, world)
+    lo, sz = shard_region(gd, "float32", LEVELS, TOL, rank, world)
+    field = grf_field_torch(sz[0], sz[1], sz[2], seed=7 + rank, scale="unit", n_fronts=20, device=dev)
+    raw_bytes = field.numel() * field.element_size()
+    tmp = os.path.join("/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir(),
+                       f"idx2bench_{os.environ.get('MASTER_PORT', '0')}")
+    last = [lo[k] + sz[k] - 1 for k in range(3)]
+    L = _lib.lib()
+    L.idx2g_ctx_launches.restype = ctypes.c_longlong
+    L.idx2g_ctx_launches.argtypes = [ctypes.c_void_p]
+
+    def encode_to(out_dir, src):
+        job = ShardEncode(src, lo, gd, out_dir, "grf", "f", LEVELS, TOL, rank, world, local_rank)
+        payloads, vmin, vmax = exchange(job.headers, job.vmin, job.vmax)
+        info = job.finish(payloads, vmin, vmax)
+        dist.barrier()
+        return job, info
+
+    def decode_block(ds, out):
+        torch.cuda.current_stream(dev).synchronize()
+        ds.decode(first=lo, last=last, out=out)
+
+    try:
+        if rank == 0:
+            shutil.rmtree(tmp, ignore_errors=True)
+        dist.barrier()
+        import idx2_b200 as idx2
+        encode_to(os.path.join(tmp, "setup"), field)
+        ds = idx2.Dataset(os.path.join(tmp, "setup", "grf", "f.idx2"))
+        out_dev = torch.empty_like(field)
+        recs = []
+
+        def device_step():
+            job = ShardEncode(field, lo, gd, tmp, "grf", "f", LEVELS, TOL, rank, world, local_rank, device_only=True)
+            decode_block(ds, out_dev)
+            recs.append(([job.info.level_kernel_ms[i] for i in range(job.info.num_levels)],
+                         [job.info.level_out_bytes[i] for i in range(job.info.num_levels)], ds.last_kernel_ms))
+
+        for _ in range(args.warmup):
+            device_step()
+        recs.clear()
+        torch.cuda.synchronize()
+        dist.barrier()
+        launches0 = L.idx2g_ctx_launches(_lib.ctx(local_rank).h)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local_rank) as clocks:
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(args.steps):
+                device_step()
+            e1.record(stream)
+            torch.cuda.synchronize()
+        timed_launches = L.idx2g_ctx_launches(_lib.ctx(local_rank).h) - launches0
+        dev_ms = e0.elapsed_time(e1) / args.steps
+        max_err = float((out_dev.double() - field.double()).abs().max())
+        t = torch.tensor([dev_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t)
+        ds.close()
+        # e2e: host block in, files out, the dataset read back and this block decoded to the host
+        host = field.cpu().pin_memory()
+        out_host = torch.empty(field.shape, dtype=field.dtype).pin_memory()
+        staged = torch.empty_like(field)
+        e2e = []
+        for i in range(args.warmup + args.steps):
+            d = os.path.join(tmp, f"e2e{i % 2}")
+            if rank == 0:
+                shutil.rmtree(d, ignore_errors=True)
+            dist.barrier()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            staged.copy_(host, non_blocking=True)
+            torch.cuda.synchronize()
+            encode_to(d, staged)
+            ds2 = idx2.Dataset(os.path.join(d, "grf", "f.idx2"))
+            ds2.decode(first=lo, last=last, out=out_host)
+            ds2.close()
+            dist.barrier()
+            if i >= args.warmup:
+                e2e.append(time.perf_counter() - t0)
+        tt = torch.tensor([sum(e2e) / len(e2e)], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt)
+    finally:
+        dist.barrier()
+        if rank == 0:
+            shutil.rmtree(tmp, ignore_errors=True)
+    if rank == 0:
+        lvl_ms, lvl_bytes, dec_ms = recs[-1]
+        l0_ms = sum(r[0][0] for r in recs) / len(recs)
+        l0_bytes = raw_bytes + lvl_bytes[0]
+        peak, kind = hbm_peak()
+        achieved = l0_bytes / (l0_ms * 1e-3) / 1e9
+        line = {
+            "metric": METRIC, "value": world * 2 * raw_bytes / (dev_ms * 1e-3) / 1e9, "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded k^-5/3 GRF, 20 tanh fronts, one block per GPU)",
+            "config": {"workload": f"grf{side} x {world}: one {gd[0]}x{gd[1]}x{gd[2]} float32 dataset of {world} "
+                                   f"{side}^3 blocks, {LEVELS} levels, 32^3 bricks, tol {TOL}; step = sharded encode "
+                                   f"(all levels) + decode of each GPU's block",
+                       "parallelism": f"{world} shards of one dataset (coarsest-brick runs), no data exchange; "
+                                      f"the e2e leg all-gathers region headers over NCCL",
+                       "l2": "inputs (4.3 GB per GPU) >> L2; no flush needed"},
+            "encode_level_ms": lvl_ms, "decode_ms": dec_ms, "decode_max_abs_err": max_err,
+            "roofline": {"bound": "hbm", "kernel": "k_encode_level (level 0, rank 0)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{kind} (MEASURED_PEAKS.json hbm_gbs)" if kind == "measured" else kind,
+                         "algorithmic_bytes": l0_bytes, "traffic": None},
+            "cpu_baseline": None,
+            "e2e": {"value": world * 2 * raw_bytes / e2e_s / 1e9, "unit": "GB/s", "h2d_bytes_per_step": int(raw_bytes),
+                    "d2h_bytes_per_step": int(raw_bytes), "s_per_step": e2e_s},
+            "clocks": clocks.summary(), "gpu_launches": int(timed_launches),
+        }
+        print(json.dumps(line))
+    dist.destroy_process_group()
+
+
 def ours(args, rank, world, local_rank):
     import ctypes
     import torch
     import idx2_b200 as idx2
     from idx2_b200 import _lib
 
+    if world > 1:
+        return ours_sharded(args, rank, world, local_rank)
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     dist = None
@@ -749,6 +913,8 @@ def main():
     ap.add_argument("--serve-dims", default="2048x2048x1024", help="serving field dims (x, y, z)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="request arrival rate (per second)")
     ap.add_argument("--serve-requests", type=int, default=2000, help="requests per mode")
+    ap.add_argument("--dist-backend", default="nccl", choices=["nccl", "gloo"],
+                    help="process group backend for N > 1 (gloo: functional runs with fewer GPUs than ranks)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg of the default run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the differentiable-decode leg of the default run")
     ap.add_argument("--bench-serve-requests", type=int, default=400,

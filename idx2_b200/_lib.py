@@ -170,9 +170,10 @@ class Params:
 
 
 class _Ctx:
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, stream=None):
         h = ctypes.c_void_p()
-        rc = lib().idx2g_ctx_create(device, None, ctypes.byref(h))
+        rc = lib().idx2g_ctx_create(device, ctypes.c_void_p(stream.cuda_stream) if stream is not None else None,
+                                    ctypes.byref(h))
         if rc:
             raise Idx2Error(rc, "idx2g_ctx_create (is a CUDA device visible?)")
         self.h = h
@@ -195,6 +196,17 @@ def ctx(device: int = 0) -> _Ctx:
             _ctxs[device] = None
     if _ctxs[device] is None:
         _ctxs[device] = _Ctx(device)
+    return _ctxs[device]
+
+
+def ctx_on_stream(device: int, stream) -> _Ctx:
+    """Make the per-device context run on a given torch CUDA stream (events recorded on that
+    stream then bracket the library's work). Must come before the device's first use."""
+    with _lock:
+        if _ctxs.get(device) is not None:
+            raise Idx2Error(101, "the device's context exists already")
+        _ctxs[device] = _Ctx(device, stream)
+        _ctxs[device]._stream = stream
     return _ctxs[device]
 
 

@@ -361,10 +361,11 @@ IDX2G_API int idx2g_shard_region(const idx2g_params* in, int shard, int nshards,
 }
 
 IDX2G_API int idx2g_encode_shard(idx2g_ctx* c, const idx2g_params* in, const void* d_field, const int origin3[3],
-                                 const int dims3[3], int shard, int nshards, const void** headers,
+                                 const int dims3[3], int shard, int nshards, int flags, const void** headers,
                                  size_t* header_bytes, double* vmin, double* vmax, idx2g_encode_info* info)
 {
-  if (!c || !in || !d_field || !origin3 || !dims3 || !headers || !header_bytes)
+  const bool device_only = (flags & IDX2G_SHARD_DEVICE_ONLY) != 0;
+  if (!c || !in || !d_field || !origin3 || !dims3 || (!device_only && (!headers || !header_bytes)))
     return InvalidArgument;
   cudaSetDevice(c->d.device);
   c->d.shard.reset();
@@ -388,16 +389,20 @@ IDX2G_API int idx2g_encode_shard(idx2g_ctx* c, const idx2g_params* in, const voi
     return InvalidArgument;
   job->coder.reset(new gpu_coder(&c->d, job->f, d_field, job->p.type == dtype::float32));
   job->coder->set_field_region(o, d);
+  job->coder->set_keep_device(device_only);
   const auto t0 = std::chrono::steady_clock::now();
   e = encode_levels(&job->f, job->coder.get(), &job->outs, job->sp.local);
   if (e)
     return e;
   job->device_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  e = shard_headers(job->f, *job->plan, job->sp, job->outs, &job->headers);
-  if (e)
-    return e;
-  *headers = job->headers.data();
-  *header_bytes = job->headers.size();
+  if (!device_only)
+  {
+    e = shard_headers(job->f, *job->plan, job->sp, job->outs, &job->headers);
+    if (e)
+      return e;
+    *headers = job->headers.data();
+    *header_bytes = job->headers.size();
+  }
   if (vmin)
     *vmin = job->f.value_min;
   if (vmax)
@@ -419,7 +424,8 @@ IDX2G_API int idx2g_encode_shard(idx2g_ctx* c, const idx2g_params* in, const voi
       info->level_out_bytes[i] = job->coder->level_bytes()[i];
     }
   }
-  c->d.shard = job;
+  if (!device_only)
+    c->d.shard = job;
   return NoError;
 }
 

@@ -192,10 +192,13 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* ctx, const idx2g_params* params, con
    idx2g_encode_shard_finish with all payloads in shard order: each writes its bricks' bytes
    into the shared data files at offsets every shard computes alike, shard 0 also the chunk
    headers, tables, exponent chunks and the metadata file. The files are complete once every
-   shard's finish call has returned. */
+   shard's finish call has returned. flags IDX2G_SHARD_DEVICE_ONLY: the device stage alone
+   (the streams stay in the context's device workspace, as idx2g_encode_device leaves them; no
+   payload, no finish call). */
+#define IDX2G_SHARD_DEVICE_ONLY 1
 IDX2G_API int idx2g_shard_region(const idx2g_params* p, int shard, int nshards, int from3[3], int dims3[3]);
 IDX2G_API int idx2g_encode_shard(idx2g_ctx* ctx, const idx2g_params* p, const void* d_field, const int origin3[3],
-                                 const int dims3[3], int shard, int nshards, const void** headers,
+                                 const int dims3[3], int shard, int nshards, int flags, const void** headers,
                                  size_t* header_bytes, double* vmin, double* vmax, idx2g_encode_info* info);
 IDX2G_API int idx2g_encode_shard_finish(idx2g_ctx* ctx, const idx2g_params* p, int shard, int nshards,
                                         const void* const* headers, const size_t* header_bytes, double vmin,
