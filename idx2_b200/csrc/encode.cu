@@ -16,6 +16,7 @@
 #include "encoder.h"
 #include "trace.h"
 
+#include <cooperative_groups.h>
 #include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime's entry point)
 
 #include <algorithm>
@@ -36,25 +37,31 @@ namespace
 // (-DIDX2G_PHASE_TIMING); compiled out otherwise.
 #ifdef IDX2G_PHASE_TIMING
 __device__ unsigned long long g_phase_cycles[16];
-#define ENC_PHASE_INIT \
-  long long ph_[16] = {};  \
-  long long ph_t = 0;
+struct phase_acc
+{
+  long long ph[16];
+  long long t;
+};
+#define ENC_PHASE_INIT phase_acc pacc_ = {};
 #define ENC_PHASE_START \
   if (threadIdx.x == 0) \
-    ph_t = clock64();
+    pacc_.t = clock64();
 #define ENC_PHASE(k)                 \
   if (threadIdx.x == 0)              \
   {                                  \
     const long long t_ = clock64();  \
-    ph_[k] += t_ - ph_t;             \
-    ph_t = t_;                       \
+    pacc_.ph[k] += t_ - pacc_.t;     \
+    pacc_.t = t_;                    \
   }
 #define ENC_PHASE_FLUSH            \
   if (threadIdx.x == 0)            \
     for (int k = 0; k < 16; ++k)   \
-      atomicAdd(&g_phase_cycles[k], (unsigned long long)ph_[k]);
+      atomicAdd(&g_phase_cycles[k], (unsigned long long)pacc_.ph[k]);
 #else
-#define ENC_PHASE_INIT
+struct phase_acc
+{
+};
+#define ENC_PHASE_INIT phase_acc pacc_;
 #define ENC_PHASE_START
 #define ENC_PHASE(k)
 #define ENC_PHASE_FLUSH
@@ -130,9 +137,11 @@ struct enc_args
 //   unsigned long long X[P][kRowX]   plane bit masks
 //   uint16_t off[P][kRowOff]         plane bit lengths, then bit offsets in the channel
 //   uint8_t nin[P][kRowNin]          significant coefficients before the plane
-struct enc_smem
+template <int NT>
+struct enc_smem_t
 {
-  long long q[kWarps][2][kQStride];  // per-warp scratch of two blocks
+  static constexpr int W = NT / 32;
+  long long q[W][2][kQStride];  // per-warp scratch of two blocks
   int16_t emax[kMaxBlocksPerSubband];
   int16_t ktop[kMaxBlocksPerSubband];
   uint8_t np[kMaxBlocksPerSubband];
@@ -145,12 +154,13 @@ struct enc_smem
   unsigned alloc, hdr;
   enc_field fp;  // parameters of the current brick's field
   dev::lift_stack stack;
-  double red[2][kWarps];
+  double red[2][W];
   int kmin, kmax;
   unsigned long long region;
   int ok;
   unsigned long long tma_bar[2];  // completion of the gather's two chunk buffers (TMA path)
 };
+using enc_smem = enc_smem_t<kThreads>;
 
 inline size_t enc_smem_bytes(int planes)
 {
@@ -256,16 +266,423 @@ struct block_info
   int base, lx, ly, nd;
 };
 
-__device__ __forceinline__ block_info block_at(const uint64_t* geom, int b, const int from[3], int is2d)
+__device__ __forceinline__ block_info block_at(const uint64_t* geom, int b, const int from[3], int is2d,
+                                              bool zsplit = false)
 {
   int d3[3], bd[3];
   unpack_geom(geom[b], d3, bd);
   block_info bi;
-  bi.base = (from[2] + (is2d ? 0 : 2 * d3[2])) * 33 * 33 + (from[1] + 2 * d3[1]) * 33 + from[0] + 2 * d3[0];
+  // zsplit: the subband's planes (z = from[2] + 2k) are packed, plane k at k * 33 * 33
+  const int zp = is2d ? 0 : (zsplit ? d3[2] : from[2] + 2 * d3[2]);
+  bi.base = zp * 33 * 33 + (from[1] + 2 * d3[1]) * 33 + from[0] + 2 * d3[0];
   bi.lx = bd[0] > 1 ? 3 : 0;
   bi.ly = bd[1] > 1 ? 3 : 0;
   bi.nd = (bd[0] > 1) + (bd[1] > 1) + (bd[2] > 1);
   return bi;
+}
+
+// Block coding of subband s of brick bi, its samples at F in the 33^3 layout (SZ: the stride
+// between the subband's z-planes), or, with zsplit, with the subband's planes (one z parity)
+// packed one after the other (SZ = 33 * 33):
+// exponents, quantisation, zfp, shuffle, bit planes, channel scans, the region's
+// allocation and the bit scatter (Core/idx2Encode.cpp:141-256 EncodeSubbandBlocks).
+template <int NT>
+__device__ __forceinline__ void code_subband(const enc_args& a, enc_smem_t<NT>& sm, unsigned long long* const Xp,
+                                             uint16_t* const OFF, uint8_t* const NIN, const int P,
+                                             const double* const F, const int SZ, const bool zsplit, const int bi,
+                                             const int s, phase_acc& pacc_)
+{
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const enc_field& fp = sm.fp;
+  int from[3], dims[3], strd[3];
+  subband_grid(fp.is2d, s, from, dims, strd);
+  const int nb = fp.nblocks[s];
+  const uint64_t* geom = fp.geom + (size_t)s * kMaxBlocksPerSubband;
+  const size_t bs = (size_t)bi * 8 + (size_t)s;
+
+  // D1: a warp codes two blocks (lanes own samples j and j + 32 of each): exponent,
+  // quantisation, zfp transform, shuffle, bit-plane masks by ballot; then the
+  // significance chain and the plane lengths, lane-parallel over the planes.
+  // The samples of the warp's next pair are loaded while the current pair is coded.
+  const int npairs = (nb + 1) >> 1;
+  double cv[4];
+  block_info cA, cB;
+  auto load_pair = [&](int pr, double v[4], block_info& A, block_info& B) {
+    const int b0 = 2 * pr, b1 = 2 * pr + 1;
+    A = block_at(geom, b0, from, fp.is2d, zsplit);
+    const bool hb = b1 < nb;
+    B = hb ? block_at(geom, b1, from, fp.is2d, zsplit) : A;
+    const int nvA = 1 << (2 * A.nd), nvB = hb ? 1 << (2 * B.nd) : 0;
+    v[0] = lane < nvA ? F[block_sample(A.base, A.lx, A.ly, lane, 66, SZ)] : 0.0;
+    v[1] = lane + 32 < nvA ? F[block_sample(A.base, A.lx, A.ly, lane + 32, 66, SZ)] : 0.0;
+    v[2] = lane < nvB ? F[block_sample(B.base, B.lx, B.ly, lane, 66, SZ)] : 0.0;
+    v[3] = lane + 32 < nvB ? F[block_sample(B.base, B.lx, B.ly, lane + 32, 66, SZ)] : 0.0;
+  };
+  if (warp < npairs)
+    load_pair(warp, cv, cA, cB);
+  for (int pr = warp; pr < npairs; pr += NW)
+  {
+    double nv_[4] = { 0, 0, 0, 0 };
+    block_info nA = cA, nB = cB;
+    if (pr + NW < npairs)
+      load_pair(pr + NW, nv_, nA, nB);
+    const int bA = 2 * pr, bB = 2 * pr + 1;
+    const bool hasB = bB < nb;
+    const int ndA = cA.nd, ndB = hasB ? cB.nd : 0;
+    const int nvA = 1 << (2 * ndA), nvB = hasB ? 1 << (2 * ndB) : 0;
+    // block maxima
+    double mA = fabs(cv[0]), mB = fabs(cv[2]);
+    {
+      const double m1 = fabs(cv[1]), m3 = fabs(cv[3]);
+      mA = mA < m1 ? m1 : mA;
+      mB = mB < m3 ? m3 : mB;
+    }
+    mA = warp_max(mA);
+    mB = warp_max(mB);
+    const int eA = fp.f32_exp ? dev::exponent_f32(__double2float_rn(mA)) : dev::exponent_f64(mA);
+    const int eB = fp.f32_exp ? dev::exponent_f32(__double2float_rn(mB)) : dev::exponent_f64(mB);
+    const double sA = dev::pow2(63 - ndA - 1 - eA), sB = dev::pow2(63 - ndB - 1 - eB);
+    long long* qA = sm.q[warp][0];
+    long long* qB = sm.q[warp][1];
+    if (lane < nvA)
+      qA[qpad(lane)] = dev::trunc_i64(__dmul_rn(sA, cv[0]));
+    if (lane + 32 < nvA)
+      qA[qpad(lane + 32)] = dev::trunc_i64(__dmul_rn(sA, cv[1]));
+    if (lane < nvB)
+      qB[qpad(lane)] = dev::trunc_i64(__dmul_rn(sB, cv[2]));
+    if (lane + 32 < nvB)
+      qB[qpad(lane + 32)] = dev::trunc_i64(__dmul_rn(sB, cv[3]));
+    __syncwarp();
+    // zfp transform (Core/Zfp.h:262): the 16 lines of a pass of block A on lanes 0-15,
+    // of block B on lanes 16-31
+    {
+      // (the halves share no data: each synchronises on its own 16 lanes)
+      const int h = lane >> 4, l = lane & 15;
+      const unsigned hm = h ? 0xffff0000u : 0x0000ffffu;
+      long long* q = h ? qB : qA;
+      const int nd = h ? ndB : ndA;
+      if (nd == 3)
+      {
+        lift4_padded(q, 4 * (l & 3) + 16 * (l >> 2), 1);
+        __syncwarp(hm);
+        lift4_padded(q, 16 * (l & 3) + (l >> 2), 4);
+        __syncwarp(hm);
+        lift4_padded(q, (l & 3) + 4 * (l >> 2), 16);
+      }
+      else if (nd == 2)
+      {
+        if (l < 4)
+          lift4_padded(q, 4 * l, 1);
+        __syncwarp(hm);
+        if (l < 4)
+          lift4_padded(q, l, 4);
+      }
+      else if (nd == 1)
+      {
+        if (l == 0)
+          lift4_padded(q, 0, 1);
+      }
+      __syncwarp();
+    }
+    // shuffle to sequency order, negabinary (Core/Zfp.h:419-520)
+    auto permj = [&](int nd, int j) -> int {
+      return nd == 3 ? (int)sm.perm3[j] : (nd == 2 ? (int)sm.perm2[j & 15] : j);
+    };
+    unsigned long long uA0 = 0, uA1 = 0, uB0 = 0, uB1 = 0;
+    if (lane < nvA)
+      uA0 = ((unsigned long long)qA[qpad(permj(ndA, lane))] + dev::kNegaMask) ^ dev::kNegaMask;
+    if (lane + 32 < nvA)
+      uA1 = ((unsigned long long)qA[qpad(permj(ndA, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
+    if (lane < nvB)
+      uB0 = ((unsigned long long)qB[qpad(permj(ndB, lane))] + dev::kNegaMask) ^ dev::kNegaMask;
+    if (lane + 32 < nvB)
+      uB1 = ((unsigned long long)qB[qpad(permj(ndB, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
+    __syncwarp();
+    const int npA = dev::coded_planes(eA, fp.etol, fp.end_bp, fp.bpc);
+    const int npB = hasB ? dev::coded_planes(eB, fp.etol, fp.end_bp, fp.bpc) : 0;
+    const int npM = npA > npB ? npA : npB;
+    unsigned long long* XA = Xp + bA;  // plane k at XA[k * kRowX]
+    unsigned long long* XB = Xp + bB;
+    if (lane == 0)
+    {
+      sm.emax[bA] = (int16_t)eA;
+      sm.ktop[bA] = (int16_t)(eA + 63 + 1024);
+      sm.np[bA] = (uint8_t)npA;
+      sm.nvals_log[bA] = (uint8_t)(2 * ndA);
+    }
+    if (lane == 1 && hasB)
+    {
+      sm.emax[bB] = (int16_t)eB;
+      sm.ktop[bB] = (int16_t)(eB + 63 + 1024);
+      sm.np[bB] = (uint8_t)npB;
+      sm.nvals_log[bB] = (uint8_t)(2 * ndB);
+    }
+    // Bit planes by warp transposes: transposing the high words of (uA0 | uA1) gives lane c
+    // the mask of plane k = 31 - c (bit 63 - k of every coefficient), the low words planes
+    // 32..63 (k = 63 - c). Then the significance chain (Core/Zfp.h:771): nin(k) = max over
+    // planes k' < k of the highest one-bit + 1, a suffix maximum over the lanes; and the
+    // plane lengths.
+    {
+      int carryA = 0, carryB = 0;
+      const int ngroups = npM > 32 ? 2 : 1;
+      for (int g = 0; g < ngroups; ++g)
+      {
+        const int sh = g ? 0 : 32;
+        const int k = 31 - lane + 32 * g;
+        unsigned long long xa =
+          (unsigned long long)dev::warp_transpose32((uint32_t)(uA0 >> sh), lane) |
+          ((unsigned long long)dev::warp_transpose32((uint32_t)(uA1 >> sh), lane) << 32);
+        unsigned long long xb =
+          (unsigned long long)dev::warp_transpose32((uint32_t)(uB0 >> sh), lane) |
+          ((unsigned long long)dev::warp_transpose32((uint32_t)(uB1 >> sh), lane) << 32);
+        xa = k < npA ? xa : 0ull;
+        xb = k < npB ? xb : 0ull;
+        if (k < npA)
+          XA[k * kRowX] = xa;
+        if (k < npB)
+          XB[k * kRowX] = xb;
+        // inclusive maximum over planes <= k, i.e. over lanes >= lane
+        int ia = xa ? 64 - __clzll(xa) : 0, ib = xb ? 64 - __clzll(xb) : 0;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+          const int ta = __shfl_down_sync(0xffffffffu, ia, o), tb = __shfl_down_sync(0xffffffffu, ib, o);
+          if (lane + o < 32)
+          {
+            ia = ia > ta ? ia : ta;
+            ib = ib > tb ? ib : tb;
+          }
+        }
+        int ea = __shfl_down_sync(0xffffffffu, ia, 1), eb = __shfl_down_sync(0xffffffffu, ib, 1);
+        ea = lane < 31 ? ea : 0;
+        eb = lane < 31 ? eb : 0;
+        const int nA_ = ea > carryA ? ea : carryA, nB_ = eb > carryB ? eb : carryB;
+        if (k < npA)
+        {
+          NIN[k * kRowNin + bA] = (uint8_t)nA_;
+          OFF[k * kRowOff + bA] = (uint16_t)dev::plane_bits(xa, nA_, nvA);
+        }
+        if (k < npB)
+        {
+          NIN[k * kRowNin + bB] = (uint8_t)nB_;
+          OFF[k * kRowOff + bB] = (uint16_t)dev::plane_bits(xb, nB_, nvB);
+        }
+        const int ta = __shfl_sync(0xffffffffu, ia, 0), tb = __shfl_sync(0xffffffffu, ib, 0);
+        carryA = carryA > ta ? carryA : ta;
+        carryB = carryB > tb ? carryB : tb;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      cv[i] = nv_[i];
+    cA = nA;
+    cB = nB;
+  }
+  __syncthreads();
+  ENC_PHASE(10)
+
+  // key range of the subband
+  if (warp == 0)
+  {
+    int lo = 1 << 30, hi = -(1 << 30);
+    for (int b = lane; b < nb; b += 32)
+    {
+      const int n = sm.np[b];
+      if (!n)
+        continue;
+      const int t = sm.ktop[b];
+      if (t - n + 1 < 0)
+        atomicExch(a.error, 1);  // negative key value: a tolerance below 2^-1070 (unsupported)
+      const int kl = dev::plane_key(t, n - 1, fp.bpc), kh = dev::plane_key(t, 0, fp.bpc);
+      lo = kl < lo ? kl : lo;
+      hi = kh > hi ? kh : hi;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+      const int l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+      lo = l2 < lo ? l2 : lo;
+      hi = h2 > hi ? h2 : hi;
+    }
+    if (lane == 0)
+    {
+      if (hi < lo)
+      {
+        lo = 1;
+        hi = 0;
+      }
+      sm.kmin = lo;
+      sm.kmax = hi;
+      sm.ok = (hi - lo + 1) <= kKeyWindow;
+      if (!sm.ok)
+        atomicExch(a.error, 1);
+    }
+  }
+  __syncthreads();
+  const int kmin = sm.kmin, kmax = sm.kmax;
+  const int nkeys = sm.ok ? kmax - kmin + 1 : 0;
+  ENC_PHASE(11)
+
+  // D3: per channel key (a warp each), bit offsets in the channel's stream: blocks in
+  // Morton order, within a block its planes of the key top-down (one plane per key when
+  // BitPlanesPerChunk is 1); an exclusive scan of the plane lengths, in place
+  for (int t = warp; t < nkeys && fp.bpc == 1; t += NW)
+  {
+    // one plane per key: plane ktop - key of each block
+    const int key = kmin + t;
+    uint32_t carry = 0;
+    for (int b0 = 0; b0 < nb; b0 += 32)
+    {
+      const int b = b0 + lane;
+      int kk = b < nb ? sm.ktop[b] - key : -1;
+      kk = (kk >= 0 && b < nb && kk < sm.np[b]) ? kk : -1;
+      const uint32_t v = kk >= 0 ? OFF[kk * kRowOff + b] : 0u;
+      uint32_t inc = v;
+      for (int o = 1; o < 32; o <<= 1)
+      {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o)
+          inc += y;
+      }
+      if (kk >= 0)
+        OFF[kk * kRowOff + b] = (uint16_t)(carry + inc - v);
+      carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0)
+      sm.key_bits[t] = carry;
+  }
+  for (int t = warp; t < nkeys && fp.bpc > 1; t += NW)
+  {
+    const int key = kmin + t;
+    uint32_t carry = 0;
+    for (int b0 = 0; b0 < nb; b0 += 32)
+    {
+      const int b = b0 + lane;
+      int kk0 = 1, kk1 = 0;
+      if (b < nb && sm.np[b])
+        dev::key_planes(sm.ktop[b], sm.np[b], key, fp.bpc, kk0, kk1);
+      uint32_t v = 0;
+      for (int kk = kk0; kk <= kk1; ++kk)
+        v += OFF[kk * kRowOff + b];
+      uint32_t inc = v;
+      for (int o = 1; o < 32; o <<= 1)
+      {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o)
+          inc += y;
+      }
+      uint32_t run = carry + inc - v;
+      for (int kk = kk0; kk <= kk1; ++kk)
+      {
+        const uint32_t len = OFF[kk * kRowOff + b];
+        OFF[kk * kRowOff + b] = (uint16_t)run;
+        run += len;
+      }
+      carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (lane == 0)
+    {
+      sm.key_bits[t] = carry;
+      if (carry > 65535u)
+        atomicExch(a.error, 1);  // offsets are 16-bit: a key stream of more than 65535 bits
+    }
+  }
+  __syncthreads();
+  ENC_PHASE(12)
+
+  // D4: channel byte bases and the region of this (brick, subband)
+  // (regions are whole 32-bit words so every CTA owns the words it writes)
+  if (warp == 0)
+  {
+    uint32_t v[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+      const int t = lane * 4 + i;
+      v[i] = t < nkeys ? (sm.key_bits[t] + 7u) / 8u : 0u;
+    }
+    const uint32_t tot = v[0] + v[1] + v[2] + v[3];
+    uint32_t inc = tot;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o)
+        inc += y;
+    }
+    uint32_t acc = inc - tot;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+    {
+      const int t = lane * 4 + i;
+      if (t < nkeys)
+        sm.key_base[t] = acc;
+      acc += v[i];
+    }
+    const uint32_t base = __shfl_sync(0xffffffffu, inc, 31);
+    if (lane == 0)
+    {
+      // region: header (kmin, nkeys), exponents, channel sizes, channel streams
+      const unsigned hdr = 8u + ((2u * (unsigned)nb + 3u) & ~3u) + 4u * (unsigned)nkeys;
+      const unsigned alloc = hdr + ((base + 3u) & ~3u);
+      unsigned long long region = atomicAdd(a.cursor, (unsigned long long)alloc);
+      if (region + alloc > a.cap_bytes)
+        atomicExch(a.error, 2);
+      sm.region = region;
+      sm.alloc = alloc;
+      sm.hdr = hdr;
+      a.offset[bs] = region;
+    }
+  }
+  __syncthreads();
+  const unsigned long long region = sm.region;
+  const unsigned alloc = sm.alloc;
+  const unsigned hdr = sm.hdr;
+  const bool fits = region + alloc <= a.cap_bytes;
+  ENC_PHASE(13)
+
+  // D5: the plane codes, built in registers and ORed into shared memory when the region
+  // is small enough, else straight into the (zeroed) global region; then the region is
+  // stored with plain writes
+  if (fits && alloc)
+  {
+    const bool staged = alloc <= kStageBytes;
+    uint32_t* words = staged ? sm.stage : a.stream + region / 4;
+    for (unsigned i = tid; i < alloc / 4; i += NT)
+      words[i] = 0u;
+    __syncthreads();
+    if (tid == 0)
+    {
+      words[0] = (uint32_t)(nkeys ? kmin : 1);
+      words[1] = (uint32_t)nkeys;
+    }
+    uint16_t* ew = reinterpret_cast<uint16_t*>(words + 2);
+    for (int b = tid; b < nb; b += NT)
+      ew[b] = (uint16_t)sm.emax[b];
+    uint32_t* sw = words + 2 + ((2u * (unsigned)nb + 3u) >> 2);
+    for (int t = tid; t < nkeys; t += NT)
+      sw[t] = (sm.key_bits[t] + 7) / 8;
+    for (int idx = tid; idx < P * kMaxBlocksPerSubband; idx += NT)
+    {
+      const int b = idx & (kMaxBlocksPerSubband - 1), kk = idx / kMaxBlocksPerSubband;
+      if (b >= nb || kk >= sm.np[b])
+        continue;
+      const int t = dev::plane_key(sm.ktop[b], kk, fp.bpc) - kmin;
+      const unsigned long long pos = ((unsigned long long)hdr + sm.key_base[t]) * 8ull +
+                                     (unsigned long long)OFF[kk * kRowOff + b];
+      dev::bits192 c;
+      const int len =
+        dev::plane_code(Xp[kk * kRowX + b], NIN[kk * kRowNin + b], 1 << sm.nvals_log[b], &c);
+      dev::or_code(words, pos, c, len);
+    }
+    __syncthreads();
+    if (staged)
+    {
+      uint32_t* dst = a.stream + region / 4;
+      for (unsigned i = tid; i < alloc / 4; i += NT)
+        __stcs(dst + i, sm.stage[i]);
+    }
+  }
+  __syncthreads();
+  ENC_PHASE(14)
 }
 
 __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc_args a)
@@ -823,398 +1240,14 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
         const int nx = a.order ? a.order[it + gridDim.x] : it + (int)gridDim.x;
         prefetch_rows(a.fields[a.bricks[nx].field], a.bricks[nx]);
       }
-      int from[3], dims[3], strd[3];
-      subband_grid(fp.is2d, s, from, dims, strd);
-      const int nb = fp.nblocks[s];
-      const uint64_t* geom = fp.geom + (size_t)s * kMaxBlocksPerSubband;
-      const size_t bs = (size_t)bi * 8 + (size_t)s;
-
-      // D1: a warp codes two blocks (lanes own samples j and j + 32 of each): exponent,
-      // quantisation, zfp transform, shuffle, bit-plane masks by ballot; then the
-      // significance chain and the plane lengths, lane-parallel over the planes.
-      // The samples of the warp's next pair are loaded while the current pair is coded.
-      const int npairs = (nb + 1) >> 1;
-      double cv[4];
-      block_info cA, cB;
-      auto load_pair = [&](int pr, double v[4], block_info& A, block_info& B) {
-        const int b0 = 2 * pr, b1 = 2 * pr + 1;
-        A = block_at(geom, b0, from, fp.is2d);
-        const bool hb = b1 < nb;
-        B = hb ? block_at(geom, b1, from, fp.is2d) : A;
-        const int nvA = 1 << (2 * A.nd), nvB = hb ? 1 << (2 * B.nd) : 0;
-        v[0] = lane < nvA ? F[block_sample(A.base, A.lx, A.ly, lane, 66, SZ)] : 0.0;
-        v[1] = lane + 32 < nvA ? F[block_sample(A.base, A.lx, A.ly, lane + 32, 66, SZ)] : 0.0;
-        v[2] = lane < nvB ? F[block_sample(B.base, B.lx, B.ly, lane, 66, SZ)] : 0.0;
-        v[3] = lane + 32 < nvB ? F[block_sample(B.base, B.lx, B.ly, lane + 32, 66, SZ)] : 0.0;
-      };
-      if (warp < npairs)
-        load_pair(warp, cv, cA, cB);
-      for (int pr = warp; pr < npairs; pr += kWarps)
-      {
-        double nv_[4] = { 0, 0, 0, 0 };
-        block_info nA = cA, nB = cB;
-        if (pr + kWarps < npairs)
-          load_pair(pr + kWarps, nv_, nA, nB);
-        const int bA = 2 * pr, bB = 2 * pr + 1;
-        const bool hasB = bB < nb;
-        const int ndA = cA.nd, ndB = hasB ? cB.nd : 0;
-        const int nvA = 1 << (2 * ndA), nvB = hasB ? 1 << (2 * ndB) : 0;
-        // block maxima
-        double mA = fabs(cv[0]), mB = fabs(cv[2]);
-        {
-          const double m1 = fabs(cv[1]), m3 = fabs(cv[3]);
-          mA = mA < m1 ? m1 : mA;
-          mB = mB < m3 ? m3 : mB;
-        }
-        mA = warp_max(mA);
-        mB = warp_max(mB);
-        const int eA = fp.f32_exp ? dev::exponent_f32(__double2float_rn(mA)) : dev::exponent_f64(mA);
-        const int eB = fp.f32_exp ? dev::exponent_f32(__double2float_rn(mB)) : dev::exponent_f64(mB);
-        const double sA = dev::pow2(63 - ndA - 1 - eA), sB = dev::pow2(63 - ndB - 1 - eB);
-        long long* qA = sm.q[warp][0];
-        long long* qB = sm.q[warp][1];
-        if (lane < nvA)
-          qA[qpad(lane)] = dev::trunc_i64(__dmul_rn(sA, cv[0]));
-        if (lane + 32 < nvA)
-          qA[qpad(lane + 32)] = dev::trunc_i64(__dmul_rn(sA, cv[1]));
-        if (lane < nvB)
-          qB[qpad(lane)] = dev::trunc_i64(__dmul_rn(sB, cv[2]));
-        if (lane + 32 < nvB)
-          qB[qpad(lane + 32)] = dev::trunc_i64(__dmul_rn(sB, cv[3]));
-        __syncwarp();
-        // zfp transform (Core/Zfp.h:262): the 16 lines of a pass of block A on lanes 0-15,
-        // of block B on lanes 16-31
-        {
-          // (the halves share no data: each synchronises on its own 16 lanes)
-          const int h = lane >> 4, l = lane & 15;
-          const unsigned hm = h ? 0xffff0000u : 0x0000ffffu;
-          long long* q = h ? qB : qA;
-          const int nd = h ? ndB : ndA;
-          if (nd == 3)
-          {
-            lift4_padded(q, 4 * (l & 3) + 16 * (l >> 2), 1);
-            __syncwarp(hm);
-            lift4_padded(q, 16 * (l & 3) + (l >> 2), 4);
-            __syncwarp(hm);
-            lift4_padded(q, (l & 3) + 4 * (l >> 2), 16);
-          }
-          else if (nd == 2)
-          {
-            if (l < 4)
-              lift4_padded(q, 4 * l, 1);
-            __syncwarp(hm);
-            if (l < 4)
-              lift4_padded(q, l, 4);
-          }
-          else if (nd == 1)
-          {
-            if (l == 0)
-              lift4_padded(q, 0, 1);
-          }
-          __syncwarp();
-        }
-        // shuffle to sequency order, negabinary (Core/Zfp.h:419-520)
-        auto permj = [&](int nd, int j) -> int {
-          return nd == 3 ? (int)sm.perm3[j] : (nd == 2 ? (int)sm.perm2[j & 15] : j);
-        };
-        unsigned long long uA0 = 0, uA1 = 0, uB0 = 0, uB1 = 0;
-        if (lane < nvA)
-          uA0 = ((unsigned long long)qA[qpad(permj(ndA, lane))] + dev::kNegaMask) ^ dev::kNegaMask;
-        if (lane + 32 < nvA)
-          uA1 = ((unsigned long long)qA[qpad(permj(ndA, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
-        if (lane < nvB)
-          uB0 = ((unsigned long long)qB[qpad(permj(ndB, lane))] + dev::kNegaMask) ^ dev::kNegaMask;
-        if (lane + 32 < nvB)
-          uB1 = ((unsigned long long)qB[qpad(permj(ndB, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
-        __syncwarp();
-        const int npA = dev::coded_planes(eA, fp.etol, fp.end_bp, fp.bpc);
-        const int npB = hasB ? dev::coded_planes(eB, fp.etol, fp.end_bp, fp.bpc) : 0;
-        const int npM = npA > npB ? npA : npB;
-        unsigned long long* XA = Xp + bA;  // plane k at XA[k * kRowX]
-        unsigned long long* XB = Xp + bB;
-        if (lane == 0)
-        {
-          sm.emax[bA] = (int16_t)eA;
-          sm.ktop[bA] = (int16_t)(eA + 63 + 1024);
-          sm.np[bA] = (uint8_t)npA;
-          sm.nvals_log[bA] = (uint8_t)(2 * ndA);
-        }
-        if (lane == 1 && hasB)
-        {
-          sm.emax[bB] = (int16_t)eB;
-          sm.ktop[bB] = (int16_t)(eB + 63 + 1024);
-          sm.np[bB] = (uint8_t)npB;
-          sm.nvals_log[bB] = (uint8_t)(2 * ndB);
-        }
-        // Bit planes by warp transposes: transposing the high words of (uA0 | uA1) gives lane c
-        // the mask of plane k = 31 - c (bit 63 - k of every coefficient), the low words planes
-        // 32..63 (k = 63 - c). Then the significance chain (Core/Zfp.h:771): nin(k) = max over
-        // planes k' < k of the highest one-bit + 1, a suffix maximum over the lanes; and the
-        // plane lengths.
-        {
-          int carryA = 0, carryB = 0;
-          const int ngroups = npM > 32 ? 2 : 1;
-          for (int g = 0; g < ngroups; ++g)
-          {
-            const int sh = g ? 0 : 32;
-            const int k = 31 - lane + 32 * g;
-            unsigned long long xa =
-              (unsigned long long)dev::warp_transpose32((uint32_t)(uA0 >> sh), lane) |
-              ((unsigned long long)dev::warp_transpose32((uint32_t)(uA1 >> sh), lane) << 32);
-            unsigned long long xb =
-              (unsigned long long)dev::warp_transpose32((uint32_t)(uB0 >> sh), lane) |
-              ((unsigned long long)dev::warp_transpose32((uint32_t)(uB1 >> sh), lane) << 32);
-            xa = k < npA ? xa : 0ull;
-            xb = k < npB ? xb : 0ull;
-            if (k < npA)
-              XA[k * kRowX] = xa;
-            if (k < npB)
-              XB[k * kRowX] = xb;
-            // inclusive maximum over planes <= k, i.e. over lanes >= lane
-            int ia = xa ? 64 - __clzll(xa) : 0, ib = xb ? 64 - __clzll(xb) : 0;
-            for (int o = 1; o < 32; o <<= 1)
-            {
-              const int ta = __shfl_down_sync(0xffffffffu, ia, o), tb = __shfl_down_sync(0xffffffffu, ib, o);
-              if (lane + o < 32)
-              {
-                ia = ia > ta ? ia : ta;
-                ib = ib > tb ? ib : tb;
-              }
-            }
-            int ea = __shfl_down_sync(0xffffffffu, ia, 1), eb = __shfl_down_sync(0xffffffffu, ib, 1);
-            ea = lane < 31 ? ea : 0;
-            eb = lane < 31 ? eb : 0;
-            const int nA_ = ea > carryA ? ea : carryA, nB_ = eb > carryB ? eb : carryB;
-            if (k < npA)
-            {
-              NIN[k * kRowNin + bA] = (uint8_t)nA_;
-              OFF[k * kRowOff + bA] = (uint16_t)dev::plane_bits(xa, nA_, nvA);
-            }
-            if (k < npB)
-            {
-              NIN[k * kRowNin + bB] = (uint8_t)nB_;
-              OFF[k * kRowOff + bB] = (uint16_t)dev::plane_bits(xb, nB_, nvB);
-            }
-            const int ta = __shfl_sync(0xffffffffu, ia, 0), tb = __shfl_sync(0xffffffffu, ib, 0);
-            carryA = carryA > ta ? carryA : ta;
-            carryB = carryB > tb ? carryB : tb;
-          }
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          cv[i] = nv_[i];
-        cA = nA;
-        cB = nB;
-      }
-      __syncthreads();
-      ENC_PHASE(10)
-
-      // key range of the subband
-      if (warp == 0)
-      {
-        int lo = 1 << 30, hi = -(1 << 30);
-        for (int b = lane; b < nb; b += 32)
-        {
-          const int n = sm.np[b];
-          if (!n)
-            continue;
-          const int t = sm.ktop[b];
-          if (t - n + 1 < 0)
-            atomicExch(a.error, 1);  // negative key value: a tolerance below 2^-1070 (unsupported)
-          const int kl = dev::plane_key(t, n - 1, fp.bpc), kh = dev::plane_key(t, 0, fp.bpc);
-          lo = kl < lo ? kl : lo;
-          hi = kh > hi ? kh : hi;
-        }
-        for (int o = 16; o > 0; o >>= 1)
-        {
-          const int l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
-          lo = l2 < lo ? l2 : lo;
-          hi = h2 > hi ? h2 : hi;
-        }
-        if (lane == 0)
-        {
-          if (hi < lo)
-          {
-            lo = 1;
-            hi = 0;
-          }
-          sm.kmin = lo;
-          sm.kmax = hi;
-          sm.ok = (hi - lo + 1) <= kKeyWindow;
-          if (!sm.ok)
-            atomicExch(a.error, 1);
-        }
-      }
-      __syncthreads();
-      const int kmin = sm.kmin, kmax = sm.kmax;
-      const int nkeys = sm.ok ? kmax - kmin + 1 : 0;
-      ENC_PHASE(11)
-
-      // D3: per channel key (a warp each), bit offsets in the channel's stream: blocks in
-      // Morton order, within a block its planes of the key top-down (one plane per key when
-      // BitPlanesPerChunk is 1); an exclusive scan of the plane lengths, in place
-      for (int t = warp; t < nkeys && fp.bpc == 1; t += kWarps)
-      {
-        // one plane per key: plane ktop - key of each block
-        const int key = kmin + t;
-        uint32_t carry = 0;
-        for (int b0 = 0; b0 < nb; b0 += 32)
-        {
-          const int b = b0 + lane;
-          int kk = b < nb ? sm.ktop[b] - key : -1;
-          kk = (kk >= 0 && b < nb && kk < sm.np[b]) ? kk : -1;
-          const uint32_t v = kk >= 0 ? OFF[kk * kRowOff + b] : 0u;
-          uint32_t inc = v;
-          for (int o = 1; o < 32; o <<= 1)
-          {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o)
-              inc += y;
-          }
-          if (kk >= 0)
-            OFF[kk * kRowOff + b] = (uint16_t)(carry + inc - v);
-          carry += __shfl_sync(0xffffffffu, inc, 31);
-        }
-        if (lane == 0)
-          sm.key_bits[t] = carry;
-      }
-      for (int t = warp; t < nkeys && fp.bpc > 1; t += kWarps)
-      {
-        const int key = kmin + t;
-        uint32_t carry = 0;
-        for (int b0 = 0; b0 < nb; b0 += 32)
-        {
-          const int b = b0 + lane;
-          int kk0 = 1, kk1 = 0;
-          if (b < nb && sm.np[b])
-            dev::key_planes(sm.ktop[b], sm.np[b], key, fp.bpc, kk0, kk1);
-          uint32_t v = 0;
-          for (int kk = kk0; kk <= kk1; ++kk)
-            v += OFF[kk * kRowOff + b];
-          uint32_t inc = v;
-          for (int o = 1; o < 32; o <<= 1)
-          {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-            if (lane >= o)
-              inc += y;
-          }
-          uint32_t run = carry + inc - v;
-          for (int kk = kk0; kk <= kk1; ++kk)
-          {
-            const uint32_t len = OFF[kk * kRowOff + b];
-            OFF[kk * kRowOff + b] = (uint16_t)run;
-            run += len;
-          }
-          carry += __shfl_sync(0xffffffffu, inc, 31);
-        }
-        if (lane == 0)
-        {
-          sm.key_bits[t] = carry;
-          if (carry > 65535u)
-            atomicExch(a.error, 1);  // offsets are 16-bit: a key stream of more than 65535 bits
-        }
-      }
-      __syncthreads();
-      ENC_PHASE(12)
-
-      // D4: channel byte bases and the region of this (brick, subband)
-      // (regions are whole 32-bit words so every CTA owns the words it writes)
-      if (warp == 0)
-      {
-        uint32_t v[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-        {
-          const int t = lane * 4 + i;
-          v[i] = t < nkeys ? (sm.key_bits[t] + 7u) / 8u : 0u;
-        }
-        const uint32_t tot = v[0] + v[1] + v[2] + v[3];
-        uint32_t inc = tot;
-        for (int o = 1; o < 32; o <<= 1)
-        {
-          const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-          if (lane >= o)
-            inc += y;
-        }
-        uint32_t acc = inc - tot;
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-        {
-          const int t = lane * 4 + i;
-          if (t < nkeys)
-            sm.key_base[t] = acc;
-          acc += v[i];
-        }
-        const uint32_t base = __shfl_sync(0xffffffffu, inc, 31);
-        if (lane == 0)
-        {
-          // region: header (kmin, nkeys), exponents, channel sizes, channel streams
-          const unsigned hdr = 8u + ((2u * (unsigned)nb + 3u) & ~3u) + 4u * (unsigned)nkeys;
-          const unsigned alloc = hdr + ((base + 3u) & ~3u);
-          unsigned long long region = atomicAdd(a.cursor, (unsigned long long)alloc);
-          if (region + alloc > a.cap_bytes)
-            atomicExch(a.error, 2);
-          sm.region = region;
-          sm.alloc = alloc;
-          sm.hdr = hdr;
-          a.offset[bs] = region;
-        }
-      }
-      __syncthreads();
-      const unsigned long long region = sm.region;
-      const unsigned alloc = sm.alloc;
-      const unsigned hdr = sm.hdr;
-      const bool fits = region + alloc <= a.cap_bytes;
-      ENC_PHASE(13)
-
-      // D5: the plane codes, built in registers and ORed into shared memory when the region
-      // is small enough, else straight into the (zeroed) global region; then the region is
-      // stored with plain writes
-      if (fits && alloc)
-      {
-        const bool staged = alloc <= kStageBytes;
-        uint32_t* words = staged ? sm.stage : a.stream + region / 4;
-        for (unsigned i = tid; i < alloc / 4; i += kThreads)
-          words[i] = 0u;
-        __syncthreads();
-        if (tid == 0)
-        {
-          words[0] = (uint32_t)(nkeys ? kmin : 1);
-          words[1] = (uint32_t)nkeys;
-        }
-        uint16_t* ew = reinterpret_cast<uint16_t*>(words + 2);
-        for (int b = tid; b < nb; b += kThreads)
-          ew[b] = (uint16_t)sm.emax[b];
-        uint32_t* sw = words + 2 + ((2u * (unsigned)nb + 3u) >> 2);
-        for (int t = tid; t < nkeys; t += kThreads)
-          sw[t] = (sm.key_bits[t] + 7) / 8;
-        for (int idx = tid; idx < P * kMaxBlocksPerSubband; idx += kThreads)
-        {
-          const int b = idx & (kMaxBlocksPerSubband - 1), kk = idx / kMaxBlocksPerSubband;
-          if (b >= nb || kk >= sm.np[b])
-            continue;
-          const int t = dev::plane_key(sm.ktop[b], kk, fp.bpc) - kmin;
-          const unsigned long long pos = ((unsigned long long)hdr + sm.key_base[t]) * 8ull +
-                                         (unsigned long long)OFF[kk * kRowOff + b];
-          dev::bits192 c;
-          const int len =
-            dev::plane_code(Xp[kk * kRowX + b], NIN[kk * kRowNin + b], 1 << sm.nvals_log[b], &c);
-          dev::or_code(words, pos, c, len);
-        }
-        __syncthreads();
-        if (staged)
-        {
-          uint32_t* dst = a.stream + region / 4;
-          for (unsigned i = tid; i < alloc / 4; i += kThreads)
-            __stcs(dst + i, sm.stage[i]);
-        }
-      }
-      __syncthreads();
-      ENC_PHASE(14)
+      code_subband<kThreads>(a, sm, Xp, OFF, NIN, P, F, SZ, false, bi, s, pacc_);
     }
   }
   ENC_PHASE_FLUSH
 }
+
+namespace cg = cooperative_groups;
+#include "encode_split.cuh"
 
 } // namespace
 
@@ -1235,6 +1268,7 @@ struct batch_encoder::level_launch
   int nparents = 0;
   int planes = 32;
   int grid = 1;
+  bool split = false;  // k_encode_split (3D float32 datasets; bricks in shared memory)
   size_t smem = 0;
   unsigned long long cap = 0;
   enc_brick* d_bricks = nullptr;
@@ -1302,6 +1336,47 @@ bool field_tensor_map(const enc_field& f, CUtensorMap* map)
              const_cast<void*>(f.field), dims, pitch, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+} // namespace
+
+namespace
+{
+
+// Clusters of k_encode_split that fit on the device at once (0: the kernel cannot run; its
+// shared memory is set once per process).
+int split_clusters()
+{
+  static int n = [] {
+    const size_t smem = split_smem_bytes();
+    if (cudaFuncSetAttribute(k_encode_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    {
+      cudaGetLastError();
+      return 0;
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(sms > 1 ? sms & ~1 : 2));
+    cfg.blockDim = dim3(kSplitThreads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = 2;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, k_encode_split, &cfg) != cudaSuccess)
+    {
+      cudaGetLastError();
+      return 0;
+    }
+    return clusters;
+  }();
+  return n;
 }
 
 } // namespace
@@ -1412,6 +1487,19 @@ int batch_encoder::prepare(const batch_tuning& t)
     const int nbr = (int)ll.bricks.size();
     const int lim = tune_.ctas_per_sm * ctx_->num_sms;
     ll.grid = nbr < lim ? (nbr > 0 ? nbr : 1) : lim;
+    {
+      // the split kernel takes levels whose datasets are all 3D float32 (32 coded planes)
+      const char* env = std::getenv("IDX2G_ENC_SPLIT");
+      bool ok = nbr > 0 && ll.planes == 32 && env && env[0] == '1' && split_clusters() > 0;
+      for (const enc_field& ef : ll.fields)
+        ok = ok && !ef.is2d && ef.f32_exp && ef.end_bp == 32;
+      ll.split = ok;
+      if (ok)
+      {
+        const int nc = split_clusters();
+        ll.grid = 2 * (nbr < nc ? nbr : nc);
+      }
+    }
     max_grid = (size_t)ll.grid > max_grid ? (size_t)ll.grid : max_grid;
     char name[96];
     snprintf(name, sizeof name, "enc.%s.L%d.stream", tag_.c_str(), l);
@@ -1517,7 +1605,10 @@ int batch_encoder::enqueue_level(int l)
     cudaMemsetAsync(ll.d_parents, 0, (size_t)ll.nparents * (size_t)kNB3 * 8, st);
   if (ll.args.nbricks > 0)
   {
-    k_encode_level<<<ll.grid, kThreads, ll.smem, st>>>(ll.args);
+    if (ll.split)
+      k_encode_split<<<ll.grid, kSplitThreads, split_smem_bytes(), st>>>(ll.args);
+    else
+      k_encode_level<<<ll.grid, kThreads, ll.smem, st>>>(ll.args);
     ++launches_;
     ++ctx_->launches;
   }
@@ -1602,7 +1693,10 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
     a.last = cuts[(size_t)g + 1];
     a.order = d_order;
     const int n = a.last - a.first;
-    k_encode_level<<<n < ll.grid ? n : ll.grid, kThreads, ll.smem, st>>>(a);
+    if (ll.split)
+      k_encode_split<<<2 * (n < ll.grid / 2 ? n : ll.grid / 2), kSplitThreads, split_smem_bytes(), st>>>(a);
+    else
+      k_encode_level<<<n < ll.grid ? n : ll.grid, kThreads, ll.smem, st>>>(a);
     cudaEventRecord(t1, st);
     // the region cursor after the band: its regions end there
     cudaMemcpyAsync(h_cur + g, ll.d_misc, 8, cudaMemcpyDeviceToHost, st);
