@@ -399,8 +399,17 @@ __device__ __forceinline__ void code_subband(const enc_args& a, enc_smem_t<NT>& 
     if (lane + 32 < nvB)
       uB1 = ((unsigned long long)qB[qpad(permj(ndB, lane + 32))] + dev::kNegaMask) ^ dev::kNegaMask;
     __syncwarp();
-    const int npA = dev::coded_planes(eA, fp.etol, fp.end_bp, fp.bpc);
-    const int npB = hasB ? dev::coded_planes(eB, fp.etol, fp.end_bp, fp.bpc) : 0;
+    int npA = dev::coded_planes(eA, fp.etol, fp.end_bp, fp.bpc);
+    int npB = hasB ? dev::coded_planes(eB, fp.etol, fp.end_bp, fp.bpc) : 0;
+    if (npA > P || npB > P)
+    {
+      // more planes than the tables hold (a float64 block in a 32-plane launch): the level is
+      // coded again by a launch with room for them; this one's output is void
+      if (lane == 0)
+        atomicExch(a.error, 8);
+      npA = npA < P ? npA : P;
+      npB = npB < P ? npB : P;
+    }
     const int npM = npA > npB ? npA : npB;
     unsigned long long* XA = Xp + bA;  // plane k at XA[k * kRowX]
     unsigned long long* XB = Xp + bB;
@@ -1268,7 +1277,8 @@ struct batch_encoder::level_launch
   int nparents = 0;
   int planes = 32;
   int grid = 1;
-  bool split = false;  // k_encode_split (3D float32 datasets; bricks in shared memory)
+  bool split = false;  // k_encode_split (3D datasets; bricks in shared memory)
+  int split_grid = 2;
   size_t smem = 0;
   unsigned long long cap = 0;
   enc_brick* d_bricks = nullptr;
@@ -1490,15 +1500,12 @@ int batch_encoder::prepare(const batch_tuning& t)
     {
       // the split kernel takes levels whose datasets are all 3D float32 (32 coded planes)
       const char* env = std::getenv("IDX2G_ENC_SPLIT");
-      bool ok = nbr > 0 && ll.planes == 32 && env && env[0] == '1' && split_clusters() > 0;
+      bool ok = nbr > 0 && env && env[0] == '1' && split_clusters() > 0;
       for (const enc_field& ef : ll.fields)
-        ok = ok && !ef.is2d && ef.f32_exp && ef.end_bp == 32;
+        ok = ok && !ef.is2d;
       ll.split = ok;
-      if (ok)
-      {
-        const int nc = split_clusters();
-        ll.grid = 2 * (nbr < nc ? nbr : nc);
-      }
+      const int nc = split_clusters();
+      ll.split_grid = 2 * (nbr < nc ? nbr : nc);
     }
     max_grid = (size_t)ll.grid > max_grid ? (size_t)ll.grid : max_grid;
     char name[96];
@@ -1606,7 +1613,7 @@ int batch_encoder::enqueue_level(int l)
   if (ll.args.nbricks > 0)
   {
     if (ll.split)
-      k_encode_split<<<ll.grid, kSplitThreads, split_smem_bytes(), st>>>(ll.args);
+      k_encode_split<<<ll.split_grid, kSplitThreads, split_smem_bytes(), st>>>(ll.args);
     else
       k_encode_level<<<ll.grid, kThreads, ll.smem, st>>>(ll.args);
     ++launches_;
@@ -1694,7 +1701,7 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
     a.order = d_order;
     const int n = a.last - a.first;
     if (ll.split)
-      k_encode_split<<<2 * (n < ll.grid / 2 ? n : ll.grid / 2), kSplitThreads, split_smem_bytes(), st>>>(a);
+      k_encode_split<<<2 * (n < ll.split_grid / 2 ? n : ll.split_grid / 2), kSplitThreads, split_smem_bytes(), st>>>(a);
     else
       k_encode_level<<<n < ll.grid ? n : ll.grid, kThreads, ll.smem, st>>>(a);
     cudaEventRecord(t1, st);
@@ -1758,10 +1765,27 @@ int batch_encoder::collect_level(int l, bool keep_device)
       return CudaError;  // a bulk copy of the gather did not complete
     if (err == 1)
       return DeviceStreamOverflow;  // more than kKeyWindow channels in one subband
-    if (err != 2)
+    if (err != 2 && err != 8)
       break;
     if (attempt >= 3)
       return DeviceStreamOverflow;
+    if (err == 8)
+    {
+      // a block of the split kernel needed more than its 32-plane tables: the level again with
+      // the global-slot kernel (tables of ll.planes planes)
+      ll.split = false;
+      cudaEventRecord(ctx_->ev0, st);
+      int e = enqueue_level(l);
+      cudaEventRecord(ctx_->ev1, st);
+      if (e)
+        return e;
+      if (cudaStreamSynchronize(st) != cudaSuccess)
+        return CudaError;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ctx_->ev0, ctx_->ev1);
+      kernel_ms_ += ms;
+      continue;
+    }
     // the regions did not fit: the level again with room for all of them (its outputs for
     // the next level are recomputed identically)
     uint32_t* d_stream = (uint32_t*)ctx_->ws(ll.sname, (size_t)(misc[0] + (1ull << 20)));

@@ -1,4 +1,4 @@
-// k_encode_split: the encode of 3D float32 bricks with each brick held in shared memory,
+// k_encode_split: the encode of 3D bricks with each brick held in shared memory,
 // split over the two CTAs of a cluster by z parity (included by encode.cu inside its
 // anonymous namespace, after k_encode_level, whose helpers it uses).
 //
@@ -12,7 +12,9 @@
 // from its own slab, with the same coder as k_encode_level (code_subband). The even lattice
 // of the coarser extrapolation levels lies on even planes: CTA 0 lifts it in its table space.
 // The lifting functions and their operation order are those of k_encode_level, so the
-// coefficients, and with them the bit streams, are the same bit for bit.
+// coefficients, and with them the bit streams, are the same bit for bit. The coding tables
+// hold 32 bit planes (all a float32 dataset codes); a float64 block that needs more raises
+// the level's error word 8 and the host codes the level again with k_encode_level.
 
 constexpr int kSplitThreads = 512;
 using split_smem = enc_smem_t<kSplitThreads>;
@@ -188,7 +190,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSplitThreads, 1) k_
           __syncthreads();
         }
       };
-      if (fp.tmap != nullptr)
+      if (fp.tmap != nullptr && fp.field_f32)
       {
         // chunks of kGz planes by TMA (the field's tensor map, boxes 32 x 32 x kGz), double
         // buffered in the table space; this CTA keeps the planes of its parity
@@ -252,7 +254,8 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kSplitThreads, 1) k_
       }
       else
       {
-        // fields TMA cannot take (pitches that are not multiples of 16 bytes): plain loads
+        // float64 fields, and fields TMA cannot take (pitches that are not multiples of 16
+        // bytes): plain loads
         for (int i = tid; i < my_planes * kPlaneStride; i += kSplitThreads)
         {
           const int pl = i / kPlaneStride, j = i % kPlaneStride, z = 2 * pl + r;
