@@ -533,18 +533,21 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
     auto it = c->d.tuned.find(key);
     if (it == c->d.tuned.end())
     {
+      // candidates: the global-slot kernel at 1 and 2 CTAs per SM, and the 3D bricks in shared
+      // memory over CTA pairs (the 2D bricks then on the slot kernel at 2 CTAs per SM)
+      const batch_tuning cands[3] = { { 1, 0 }, { 2, 0 }, { 2, 1 } };
       double best = 1e300;
-      int best_ctas = 2;
-      for (int ctas = 1; ctas <= 2; ++ctas)
+      int best_code = 2;
+      for (const batch_tuning& cand : cands)
       {
+        if (cand.split == 1 && !split_kernel_available())
+          continue;
         std::vector<batch_field> trial = bf;
         std::vector<std::vector<level_output>> touts((size_t)n);
         for (int i = 0; i < n; ++i)
           trial[(size_t)i].outs = &touts[(size_t)i];
         batch_encoder te(&c->d, &trial, "b");
-        batch_tuning tt;
-        tt.ctas_per_sm = ctas;
-        int e = te.prepare(tt);
+        int e = te.prepare(cand);
         if (!e)
           e = te.run_all(graph, true);
         if (e)
@@ -552,12 +555,13 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
         if (te.kernel_ms() < best)
         {
           best = te.kernel_ms();
-          best_ctas = ctas;
+          best_code = cand.ctas_per_sm + 10 * cand.split;
         }
       }
-      it = c->d.tuned.emplace(key, best_ctas).first;
+      it = c->d.tuned.emplace(key, best_code).first;
     }
-    tune.ctas_per_sm = it->second;
+    tune.ctas_per_sm = it->second % 10;
+    tune.split = it->second / 10;
   }
   tt.lap("batch.tune");
   batch_encoder enc(&c->d, &bf, "b");

@@ -41,8 +41,17 @@ struct device_ctx
     return copy_out_stream;
   }
   long long launches = 0;  // kernels launched on this context so far
-  std::map<std::string, int> tuned;  // batched encode: CTAs per SM chosen per batch signature
+  // batched encode: the launch shape chosen per batch signature (CTAs per SM + 10 * split kernel)
+  std::map<std::string, int> tuned;
   std::shared_ptr<void> shard;       // a sharded encode between its two calls (api.cpp)
+  // instantiated CUDA graphs of batched encodes, by batch tag: the launches they were captured
+  // from (a byte image of every launch's arguments) and the executable graph
+  struct cached_graph
+  {
+    std::string launches;
+    cudaGraphExec_t exec = nullptr;
+  };
+  std::map<std::string, cached_graph> graphs;
   // Encode plans by format: the brick order and the EncodeSubband events depend only on the
   // dims, the brick dims and the number of levels, so repeated encodes of fields of one shape
   // (the time steps of a simulation) plan once.
@@ -210,6 +219,10 @@ struct device_ctx
   }
   void release()
   {
+    for (auto& kv : graphs)
+      if (kv.second.exec)
+        cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
     for (cudaStream_t* s : { &copy_stream, &copy_out_stream })
       if (*s)
       {
@@ -268,8 +281,15 @@ struct batch_field
 // Launch shape of the device encode.
 struct batch_tuning
 {
-  int ctas_per_sm = 2;  // 1 or 2 CTAs per SM
+  int ctas_per_sm = 2;  // global-slot kernel: 1 or 2 CTAs per SM
+  // 3D bricks in shared memory over 2-CTA clusters (k_encode_split): 1 on, 0 off, -1 the
+  // library's default; the environment variable IDX2G_ENC_SPLIT (0 or 1) overrides either
+  int split = -1;
 };
+
+// Whether the split encode kernel (3D bricks in shared memory over CTA pairs) can be offered to
+// the batch tuner on this device (encode.cu).
+bool split_kernel_available();
 
 // The device stage for a set of fields: per level, one launch of the encode kernel over the
 // bricks of every field that has the level. Levels can be enqueued one by one (with the
@@ -309,6 +329,7 @@ private:
   std::vector<std::unique_ptr<level_launch>> levels_;
   double kernel_ms_ = 0;
   long long launches_ = 0;
+  long long graph_launches_ = 0;  // kernels in the cached graph of this batch's launches
 };
 
 // Device brick coder for one field (brick_coder interface): a batch of one.

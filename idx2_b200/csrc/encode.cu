@@ -1277,8 +1277,13 @@ struct batch_encoder::level_launch
   int nparents = 0;
   int planes = 32;
   int grid = 1;
-  bool split = false;  // k_encode_split (3D datasets; bricks in shared memory)
+  bool split = false;  // k_encode_split for the 3D bricks (bricks in shared memory)
   int split_grid = 2;
+  // a level with 2D and 3D bricks: the 3D bricks (split_order) go to k_encode_split, the 2D
+  // ones (slot_order) to k_encode_level
+  std::vector<int> split_order, slot_order;
+  int* d_split_order = nullptr;
+  int* d_slot_order = nullptr;
   size_t smem = 0;
   unsigned long long cap = 0;
   enc_brick* d_bricks = nullptr;
@@ -1389,7 +1394,21 @@ int split_clusters()
   return n;
 }
 
+// Whether the 3D bricks of a launch go to k_encode_split: IDX2G_ENC_SPLIT=0 / 1 decides, else
+// the tuning's choice, else the library's default.
+bool split_wanted(const batch_tuning& t)
+{
+  const char* env = std::getenv("IDX2G_ENC_SPLIT");
+  if (env && (env[0] == '0' || env[0] == '1'))
+    return env[0] == '1';
+  if (t.split >= 0)
+    return t.split == 1;
+  return kSplitByDefault;
+}
+
 } // namespace
+
+bool split_kernel_available() { return kSplitOffered && split_clusters() > 0; }
 
 int batch_encoder::prepare(const batch_tuning& t)
 {
@@ -1498,14 +1517,27 @@ int batch_encoder::prepare(const batch_tuning& t)
     const int lim = tune_.ctas_per_sm * ctx_->num_sms;
     ll.grid = nbr < lim ? (nbr > 0 ? nbr : 1) : lim;
     {
-      // the split kernel takes levels whose datasets are all 3D float32 (32 coded planes)
-      const char* env = std::getenv("IDX2G_ENC_SPLIT");
-      bool ok = nbr > 0 && env && env[0] == '1' && split_clusters() > 0;
-      for (const enc_field& ef : ll.fields)
-        ok = ok && !ef.is2d;
-      ll.split = ok;
-      const int nc = split_clusters();
-      ll.split_grid = 2 * (nbr < nc ? nbr : nc);
+      // the 3D bricks go to the split kernel when it is wanted and the device runs it
+      ll.split_order.clear();
+      ll.slot_order.clear();
+      for (int i = 0; i < nbr; ++i)
+        (ll.fields[(size_t)ll.bricks[(size_t)i].field].is2d ? ll.slot_order : ll.split_order).push_back(i);
+      ll.split = !ll.split_order.empty() && split_wanted(tune_) && split_clusters() > 0;
+      const int n3 = (int)ll.split_order.size(), nc = split_clusters();
+      ll.split_grid = 2 * (n3 < nc ? n3 : nc);
+      if (ll.split && !ll.slot_order.empty())
+      {
+        char on[96];
+        snprintf(on, sizeof on, "enc.%s.L%d.order3", tag_.c_str(), l);
+        ll.d_split_order = (int*)ctx_->ws(on, ll.split_order.size() * 4);
+        snprintf(on, sizeof on, "enc.%s.L%d.order2", tag_.c_str(), l);
+        ll.d_slot_order = (int*)ctx_->ws(on, ll.slot_order.size() * 4);
+        if (!ll.d_split_order || !ll.d_slot_order)
+          return OutOfMemory;
+        cudaMemcpyAsync(ll.d_split_order, ll.split_order.data(), ll.split_order.size() * 4, cudaMemcpyHostToDevice,
+                        st);
+        cudaMemcpyAsync(ll.d_slot_order, ll.slot_order.data(), ll.slot_order.size() * 4, cudaMemcpyHostToDevice, st);
+      }
     }
     max_grid = (size_t)ll.grid > max_grid ? (size_t)ll.grid : max_grid;
     char name[96];
@@ -1612,12 +1644,29 @@ int batch_encoder::enqueue_level(int l)
     cudaMemsetAsync(ll.d_parents, 0, (size_t)ll.nparents * (size_t)kNB3 * 8, st);
   if (ll.args.nbricks > 0)
   {
-    if (ll.split)
-      k_encode_split<<<ll.split_grid, kSplitThreads, split_smem_bytes(), st>>>(ll.args);
+    if (ll.split && !ll.slot_order.empty())
+    {
+      // 3D bricks by the split kernel, 2D bricks by the slot kernel, one after the other
+      enc_args a3 = ll.args;
+      a3.order = ll.d_split_order;
+      a3.last = (int)ll.split_order.size();
+      k_encode_split<<<ll.split_grid, kSplitThreads, split_smem_bytes(), st>>>(a3);
+      enc_args a2 = ll.args;
+      a2.order = ll.d_slot_order;
+      a2.last = (int)ll.slot_order.size();
+      k_encode_level<<<a2.last < ll.grid ? a2.last : ll.grid, kThreads, ll.smem, st>>>(a2);
+      launches_ += 2;
+      ctx_->launches += 2;
+    }
     else
-      k_encode_level<<<ll.grid, kThreads, ll.smem, st>>>(ll.args);
-    ++launches_;
-    ++ctx_->launches;
+    {
+      if (ll.split)
+        k_encode_split<<<ll.split_grid, kSplitThreads, split_smem_bytes(), st>>>(ll.args);
+      else
+        k_encode_level<<<ll.grid, kThreads, ll.smem, st>>>(ll.args);
+      ++launches_;
+      ++ctx_->launches;
+    }
   }
   return cudaGetLastError() == cudaSuccess ? NoError : CudaError;
 }
@@ -1884,28 +1933,58 @@ int batch_encoder::run_all(bool use_graph, bool keep_device)
   const int L = nlevels();
   if (use_graph)
   {
-    cudaGraph_t g = nullptr;
-    cudaGraphExec_t ge = nullptr;
-    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-      return CudaError;
-    int e = NoError;
-    for (int l = 0; l < L && !e; ++l)
-      e = enqueue_level(l);
-    const cudaError_t ce = cudaStreamEndCapture(st, &g);
-    if (e || ce != cudaSuccess || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+    // the level launches as one graph, kept on the context for the next batch of the same
+    // launches: a byte image of every launch's parameters says whether the cached graph
+    // (captured with the same workspace buffers, grids and arguments) still applies
+    std::string sig;
+    for (int l = 0; l < L; ++l)
     {
-      if (g)
-        cudaGraphDestroy(g);
-      return e ? e : CudaError;
+      const level_launch& ll = *levels_[(size_t)l];
+      const int nsplit = (int)ll.split_order.size(), nslot = (int)ll.slot_order.size();
+      const void* ptrs[5] = { ll.d_misc, ll.d_parents, ll.d_split_order, ll.d_slot_order, nullptr };
+      const long long v[8] = { ll.grid, ll.split_grid, (long long)ll.split, (long long)ll.smem, ll.nparents,
+                               nsplit, nslot, 0 };
+      sig.append(reinterpret_cast<const char*>(&ll.args), sizeof ll.args);
+      sig.append(reinterpret_cast<const char*>(ptrs), sizeof ptrs);
+      sig.append(reinterpret_cast<const char*>(v), sizeof v);
+    }
+    device_ctx::cached_graph& cg_ = ctx_->graphs[tag_];
+    if (!cg_.exec || cg_.launches != sig)
+    {
+      if (cg_.exec)
+        cudaGraphExecDestroy(cg_.exec);
+      cg_.exec = nullptr;
+      cg_.launches.clear();
+      cudaGraph_t g = nullptr;
+      if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return CudaError;
+      int e = NoError;
+      const long long before = launches_;
+      for (int l = 0; l < L && !e; ++l)
+        e = enqueue_level(l);
+      const cudaError_t ce = cudaStreamEndCapture(st, &g);
+      cudaGraphExec_t ge = nullptr;
+      if (e || ce != cudaSuccess || cudaGraphInstantiate(&ge, g, 0) != cudaSuccess)
+      {
+        if (g)
+          cudaGraphDestroy(g);
+        return e ? e : CudaError;
+      }
+      cudaGraphDestroy(g);
+      cg_.exec = ge;
+      cg_.launches = sig;
+      graph_launches_ = launches_ - before;
+      launches_ = before;
+      ctx_->launches -= graph_launches_;
     }
     stage_timer tt;
     cudaEventRecord(ctx_->ev0, st);
-    cudaGraphLaunch(ge, st);
+    cudaGraphLaunch(cg_.exec, st);
     cudaEventRecord(ctx_->ev1, st);
+    launches_ += graph_launches_;
+    ctx_->launches += graph_launches_;
     const cudaError_t se = cudaStreamSynchronize(st);
     tt.lap("batch.graph_run");
-    cudaGraphExecDestroy(ge);
-    cudaGraphDestroy(g);
     if (se != cudaSuccess)
       return CudaError;
     float ms = 0;
@@ -1913,7 +1992,7 @@ int batch_encoder::run_all(bool use_graph, bool keep_device)
     kernel_ms_ += ms;
     for (int l = 0; l < L; ++l)
     {
-      e = collect_level(l, keep_device);
+      const int e = collect_level(l, keep_device);
       if (e)
         return e;
     }

@@ -17,6 +17,9 @@
 // the level's error word 8 and the host codes the level again with k_encode_level.
 
 constexpr int kSplitThreads = 512;
+// encodes without a tuned choice take this kernel for their 3D bricks; the batch tuner offers it
+constexpr bool kSplitByDefault = false;
+constexpr bool kSplitOffered = false;
 using split_smem = enc_smem_t<kSplitThreads>;
 constexpr int kPlaneStride = 33 * 33;
 constexpr size_t kSlabBytes = (size_t)17 * kPlaneStride * sizeof(double);
