@@ -57,6 +57,29 @@ METRIC = "encode+decode GB/s (raw field bytes) at 1e-3 tol"
 ENC_L0_TRAFFIC_PER_BRICK = (2.182016e9 + 2.882242e9) / 4096
 
 
+def fp64_peak(dev):
+    """FP64 throughput of this GPU in TFLOP/s: a library DGEMM (torch.matmul in float64,
+    4096^3, 2 N^3 flops), best of 5 after two warm-ups, timed with CUDA events. The encode's
+    lifting runs separate FP64 adds and multiplies (no fused multiply-add, for bit parity), one
+    flop each, against this peak of fused multiply-adds counted as two."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    c = torch.empty_like(a)
+    best = float("inf")
+    for i in range(7):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        torch.cuda.synchronize()
+        if i >= 2:
+            best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
 def hbm_peak():
     try:
         with open(PEAKS) as f:

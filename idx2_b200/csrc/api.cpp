@@ -533,11 +533,11 @@ IDX2G_API int idx2g_encode_batch(idx2g_ctx* c, const idx2g_params* in, const voi
     auto it = c->d.tuned.find(key);
     if (it == c->d.tuned.end())
     {
-      // candidates: the global-slot kernel at 1 and 2 CTAs per SM, and the 3D bricks in shared
-      // memory over CTA pairs (the 2D bricks then on the slot kernel at 2 CTAs per SM)
-      const batch_tuning cands[3] = { { 1, 0 }, { 2, 0 }, { 2, 1 } };
+      // candidates: the global-slot kernel at 1 CTA per SM and at as many as can reside, and
+      // the 3D bricks in shared memory over CTA pairs (the 2D bricks then on the slot kernel)
+      const batch_tuning cands[3] = { { 1, 0 }, { 0, 0 }, { 0, 1 } };
       double best = 1e300;
-      int best_code = 2;
+      int best_code = 0;
       for (const batch_tuning& cand : cands)
       {
         if (cand.split == 1 && !split_kernel_available())

@@ -641,7 +641,7 @@ namespace
 {
 
 constexpr int kNoAllocSlots = 8;          // output-level brick slots (= CTAs of that launch)
-constexpr int kNoAllocLevelBricks = 8;    // bricks of each coarser (non-output) level
+constexpr int kNoAllocLevelBricks = 8;    // 3D bricks of each coarser (non-output) level
 constexpr int kNoAllocMaxBricks = 4096;   // bricks of the output level
 constexpr size_t kBrickBytes = (size_t)33 * 33 * 33 * sizeof(double);
 constexpr size_t kOffSlots = 0;
@@ -724,7 +724,9 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
 {
   if (rq.bpc != 1)
     return OptionNotSupported;  // the single-kernel wavefront decodes one plane per channel
-  // limits of the fixed scratch
+  // limits of the fixed scratch: bricks of the output level; bytes of each kept coarser level
+  // (a 2D brick takes 33 x 33 of the 33^3 samples of a 3D one)
+  const size_t brick_bytes = (size_t)33 * 33 * (rq.is2d ? 1 : 33) * sizeof(double);
   bool seen_output = false;
   for (const decode_level& lv : rq.levels)
   {
@@ -737,7 +739,7 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
       if (nbr > (size_t)kNoAllocMaxBricks)
         return ScratchTooSmall;
     }
-    else if (nbr > (size_t)kNoAllocLevelBricks)
+    else if (nbr > (size_t)kNoAllocMaxBricks || nbr * brick_bytes > (size_t)kNoAllocLevelBricks * kBrickBytes)
       return ScratchTooSmall;
   }
   if (cudaSetDevice(ctx->device) != cudaSuccess)

@@ -281,7 +281,7 @@ struct batch_field
 // Launch shape of the device encode.
 struct batch_tuning
 {
-  int ctas_per_sm = 2;  // global-slot kernel: 1 or 2 CTAs per SM
+  int ctas_per_sm = 0;  // global-slot kernel: CTAs per SM, 0 as many as can reside
   // 3D bricks in shared memory over 2-CTA clusters (k_encode_split): 1 on, 0 off, -1 the
   // library's default; the environment variable IDX2G_ENC_SPLIT (0 or 1) overrides either
   int split = -1;

@@ -73,7 +73,10 @@ struct phase_acc
 #endif
 constexpr int kThreads = IDX2G_ENC_THREADS;
 constexpr int kWarps = kThreads / 32;
-constexpr int kCtasPerSm = kThreads >= 512 ? 1 : 2;
+#ifndef IDX2G_ENC_CTAS
+#define IDX2G_ENC_CTAS (IDX2G_ENC_THREADS >= 512 ? 1 : 2)
+#endif
+constexpr int kCtasPerSm = IDX2G_ENC_CTAS;
 // per-block zfp scratch, one padding word after every 4 (conflict-free 4-point passes)
 constexpr int kQStride = 80;
 __device__ __forceinline__ int qpad(int i) { return i + (i >> 2); }
@@ -148,6 +151,7 @@ struct enc_smem_t
   uint8_t nvals_log[kMaxBlocksPerSubband];
   uint8_t perm3[64];
   uint8_t perm2[16];
+  uint16_t npre[kMaxBlocksPerSubband + 1];  // coded planes of the blocks before each block
   uint32_t key_bits[kKeyWindow];
   uint32_t key_base[kKeyWindow];
   uint32_t stage[kStageBytes / 4];  // one (brick, subband) region being assembled
@@ -172,6 +176,23 @@ inline size_t enc_smem_bytes(int planes)
   size_t space = tables > lattice ? tables : lattice;
   space = space > band ? space : band;
   return ((sizeof(enc_smem) + 127) & ~(size_t)127) + space;
+}
+
+__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc_args a);
+
+// Resident CTAs of k_encode_level per SM with `smem` bytes of dynamic shared memory on the
+// current device (at least 1, at most the kernel's launch bound).
+inline int enc_occupancy(size_t smem)
+{
+  int n = 0;
+  if (cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode_level, kThreads, smem) != cudaSuccess)
+  {
+    cudaGetLastError();
+    n = 1;
+  }
+  n = n < 1 ? 1 : n;
+  return n < kCtasPerSm ? n : kCtasPerSm;
 }
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
@@ -512,6 +533,31 @@ __device__ __forceinline__ void code_subband(const enc_args& a, enc_smem_t<NT>& 
       lo = l2 < lo ? l2 : lo;
       hi = h2 > hi ? h2 : hi;
     }
+    {
+      // exclusive prefix of the coded planes over the blocks (lane: blocks 4 lane .. 4 lane + 3)
+      static_assert(kMaxBlocksPerSubband == 128, "four blocks per lane");
+      int c[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        c[i] = 4 * lane + i < nb ? (int)sm.np[4 * lane + i] : 0;
+      const int tot = c[0] + c[1] + c[2] + c[3];
+      int inc = tot;
+      for (int o = 1; o < 32; o <<= 1)
+      {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o)
+          inc += y;
+      }
+      int run = inc - tot;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+      {
+        sm.npre[4 * lane + i] = (uint16_t)run;
+        run += c[i];
+      }
+      if (lane == 31)
+        sm.npre[kMaxBlocksPerSubband] = (uint16_t)inc;
+    }
     if (lane == 0)
     {
       if (hi < lo)
@@ -669,11 +715,15 @@ __device__ __forceinline__ void code_subband(const enc_args& a, enc_smem_t<NT>& 
     uint32_t* sw = words + 2 + ((2u * (unsigned)nb + 3u) >> 2);
     for (int t = tid; t < nkeys; t += NT)
       sw[t] = (sm.key_bits[t] + 7) / 8;
-    for (int idx = tid; idx < P * kMaxBlocksPerSubband; idx += NT)
+    // the coded (block, plane) pairs, enumerated through the prefix of the blocks' plane counts
+    const int npairs = sm.npre[kMaxBlocksPerSubband];
+    for (int idx = tid; idx < npairs; idx += NT)
     {
-      const int b = idx & (kMaxBlocksPerSubband - 1), kk = idx / kMaxBlocksPerSubband;
-      if (b >= nb || kk >= sm.np[b])
-        continue;
+      int b = 0;
+#pragma unroll
+      for (int step = kMaxBlocksPerSubband / 2; step > 0; step >>= 1)
+        b = sm.npre[b + step] <= idx ? b + step : b;
+      const int kk = idx - sm.npre[b];
       const int t = dev::plane_key(sm.ktop[b], kk, fp.bpc) - kmin;
       const unsigned long long pos = ((unsigned long long)hdr + sm.key_base[t]) * 8ull +
                                      (unsigned long long)OFF[kk * kRowOff + b];
@@ -1514,7 +1564,11 @@ int batch_encoder::prepare(const batch_tuning& t)
       cap += (unsigned long long)bricks.size() * NB * 2ull;
     }
     const int nbr = (int)ll.bricks.size();
-    const int lim = tune_.ctas_per_sm * ctx_->num_sms;
+    // CTAs per SM: as many as the level's shared memory and the kernel's registers let reside
+    // (or fewer, when the tuning asks), so that no CTA of the grid waits for a place
+    const int occ = enc_occupancy(enc_smem_bytes(ll.planes));
+    const int cps = tune_.ctas_per_sm > 0 && tune_.ctas_per_sm < occ ? tune_.ctas_per_sm : occ;
+    const int lim = cps * ctx_->num_sms;
     ll.grid = nbr < lim ? (nbr > 0 ? nbr : 1) : lim;
     {
       // the 3D bricks go to the split kernel when it is wanted and the device runs it

@@ -18,7 +18,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
-from ._lib import EncodeInfo, Idx2Error, Params, _CParams, _field_ptr, ctx, lib, torch_ready
+from ._lib import EncodeInfo, Idx2Error, Params, _CParams, _Ctx, _field_ptr, ctx, lib, torch_ready
 
 
 def _params(dims, dtype, num_levels, tolerance, out_dir=".", name="field", field_name="data"):
@@ -57,16 +57,18 @@ def shard_region(dims: Sequence[int], dtype: str, num_levels: int, tolerance: fl
 
 class ShardEncode:
     """The two halves of one shard's encode on one context: code (begin), then, with every
-    shard's header payload, write (finish). For callers that exchange the payloads themselves."""
+    shard's header payload, write (finish). For callers that exchange the payloads themselves.
+    A context holds one shard's coded state between the halves: shards whose halves interleave
+    in one process need a context each (`own_context`)."""
 
     def __init__(self, field, origin, dims, out_dir, name, field_name, num_levels, tolerance, shard, nshards,
-                 device: int = 0, device_only: bool = False):
+                 device: int = 0, device_only: bool = False, own_context: bool = False):
         ptr, on_dev, dt, ldims, self._keep = _field_ptr(field)
         if not on_dev:
             raise Idx2Error(101, "a shard's field must be a CUDA tensor")
         self.shard, self.nshards = shard, nshards
         self._cp = _params(dims, dt, num_levels, tolerance, out_dir, name, field_name).to_c()
-        self._ctx = ctx(device)
+        self._ctx = _Ctx(device) if own_context else ctx(device)
         self.info = EncodeInfo()
         hp, hn = ctypes.c_void_p(), ctypes.c_size_t()
         lo, hi = ctypes.c_double(), ctypes.c_double()

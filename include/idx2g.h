@@ -138,9 +138,9 @@ IDX2G_API int idx2g_decode_batch(idx2g_ctx* ctx, idx2g_dataset* ds, const idx2g_
    Its temporaries live in a fixed device array of about 7.3 MB, taken on a device when the
    first context is created there (idx2g_ctx_create loads the library's decode kernels and
    resolves the array's device address with cudaGetSymbolAddress, that device current) and
-   held until the process exits. Limits: at most 4096 bricks on the output level and
-   8 bricks on each coarser level the request decodes; larger requests return
-   ScratchTooSmall (104). The call waits for the context's stream between levels, so on a
+   held until the process exits. Limits: at most 4096 bricks on the output level and, on
+   each coarser level the request decodes, 8 bricks of a 3D dataset (264 of a 2D one, whose
+   bricks are 33 times smaller); larger requests return ScratchTooSmall (104). The call waits for the context's stream between levels, so on a
    stream that is being captured it returns InvalidArgument. All calls share the array and it
    keeps the last call's contents (the error word is cleared by every call); calls that
    overlap on the GPU race on it. The result equals idx2g_decode's. */

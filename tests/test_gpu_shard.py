@@ -33,7 +33,8 @@ def test_shards_on_one_gpu_match_single_encode(idx2g, ref_app, tmp_path, case):
         lo, sz = shard_region(dims, dt, levels, tol, s, n)
         # the shard's region only (a copy), as a process of a multi-GPU job would hold it
         region = full[lo[2]:lo[2] + sz[2], lo[1]:lo[1] + sz[1], lo[0]:lo[0] + sz[0]].contiguous()
-        jobs.append(ShardEncode(region, lo, dims, str(tmp_path / "sharded"), "shd", "f", levels, tol, s, n))
+        jobs.append(ShardEncode(region, lo, dims, str(tmp_path / "sharded"), "shd", "f", levels, tol, s, n,
+                                own_context=True))
     payloads = [j.headers for j in jobs]
     vmin, vmax = min(j.vmin for j in jobs), max(j.vmax for j in jobs)
     for j in jobs:

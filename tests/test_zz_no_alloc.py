@@ -73,10 +73,12 @@ def test_noalloc_decode_matches_decode_twice(idx2g, name):
 @pytest.mark.gpu
 def test_noalloc_2d_downsampled_matches_decode(idx2g):
     import torch
-    # 2D bricks (32 x 32 x 1): at downsampling 1 1 0 the output level is level 1 (12 bricks)
+    # 2D bricks (32 x 32 x 1), 200 x 150, 2 levels: level 0 has 35 bricks, level 1 12; these
+    # requests decode level 0 (its low band alone at downsampling 1 1 0) over level 1 kept on
+    # the device (12 2D bricks fit the bytes of 8 3D bricks)
     ds = idx2g.Dataset(os.path.join(GOLDEN, "datasets", "f32c", "f.idx2"))
-    _check_twice(idx2g, ds, {"ds": (1, 1, 0), "tol": 0.0}, torch.float32)
-    _check_twice(idx2g, ds, {"ds": (1, 1, 0), "tol": 0.1}, torch.float32)
+    for req in ({"ds": (1, 1, 0), "tol": 0.0}, {"ds": (1, 1, 0), "tol": 0.1}, {"ds": (0, 0, 0), "tol": 0.0}):
+        _check_twice(idx2g, ds, req, torch.float32)
     ds.close()
 
 
@@ -98,13 +100,20 @@ def test_noalloc_at_the_limits(idx2g, shape, levels):
 @pytest.mark.gpu
 def test_noalloc_rejects_requests_beyond_scratch(idx2g):
     import torch
-    # the 2D golden dataset has 12 bricks on level 1, more than the scratch's 8
-    ds = idx2g.Dataset(os.path.join(GOLDEN, "datasets", "f32c", "f.idx2"))
-    req = {"ds": (0, 0, 0), "tol": 0.0}
-    _, dims, _ = ds.output_grid(None, None, req["ds"])
-    out = torch.zeros((dims[2], dims[1], dims[0]), dtype=torch.float32, device="cuda")
-    assert _noalloc(idx2g, ds, req, out) == SCRATCH_TOO_SMALL
-    ds.close()
+    from idx2_b200.synthetic import grf_field_torch
+    # 192 x 128 x 128 with 2 levels: level 1 (96 x 64 x 64) has 3 x 2 x 2 = 12 bricks, more than
+    # the scratch's 8 3D bricks per kept level; at downsampling 2 2 2 no subband of level 0 is
+    # decoded, level 1 is the output level and the request fits
+    f = grf_field_torch(192, 128, 128, seed=6, scale="unit", n_fronts=2, device=torch.device("cuda", 0))
+    with tempfile.TemporaryDirectory(dir="/dev/shm" if os.path.isdir("/dev/shm") else None) as tmp:
+        idx2g.encode(f, out_dir=tmp, name="big", field_name="f", num_levels=2, tolerance=1e-3)
+        ds = idx2g.Dataset(os.path.join(tmp, "big", "f.idx2"))
+        req = {"ds": (0, 0, 0), "tol": 0.0}
+        _, dims, _ = ds.output_grid(None, None, req["ds"])
+        out = torch.zeros((dims[2], dims[1], dims[0]), dtype=torch.float32, device="cuda")
+        assert _noalloc(idx2g, ds, req, out) == SCRATCH_TOO_SMALL
+        _check_twice(idx2g, ds, {"ds": (2, 2, 2), "tol": 0.0}, torch.float32)
+        ds.close()
 
 
 _LAZY_CHILD = r"""
