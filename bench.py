@@ -51,10 +51,15 @@ LEVELS = 3
 TOL = 1e-3
 METRIC = "encode+decode GB/s (raw field bytes) at 1e-3 tol"
 # DRAM bytes (read + write) of one level-0 k_encode_level launch per brick, from an ncu capture
-# of the grf512 workload (4,096 bricks: 2.182 GB read + 2.882 GB written); the traffic of a
+# of the grf512 workload (4,096 bricks: 2.268 GB read + 2.807 GB written); the traffic of a
 # launch grows with its bricks (every brick makes the same slot sweeps), so a full launch's
 # traffic is this figure times its bricks.
-ENC_L0_TRAFFIC_PER_BRICK = (2.182016e9 + 2.882242e9) / 4096
+ENC_L0_TRAFFIC_PER_BRICK = (2.267987e9 + 2.807463e9) / 4096
+# FP64 operations of one level-0 k_encode_level launch per brick, from the same kind of ncu
+# capture (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum: 2,872,791,040 adds,
+# 1,577,402,368 multiplies, no fused multiply-adds over 4,096 bricks); every brick runs the same
+# lifting sweeps, so a launch's count is this figure times its bricks.
+ENC_L0_FP64_OPS_PER_BRICK = (2872791040 + 1577402368) / 4096
 
 
 def fp64_peak(dev):
@@ -617,6 +622,15 @@ def ours(args, rank, world, local_rank):
     # the whole decode (plane and level kernels of every level) against the same roof: the
     # compressed streams and exponents it reads plus the grid it writes
     dec_bytes = int(sum(lvl_bytes)) + raw_bytes
+    # the same launch against the FP64 roof (its lifting is FP64 adds and multiplies)
+    fp64_tf = fp64_peak(dev)
+    fp64_ach = ENC_L0_FP64_OPS_PER_BRICK * (side // 32) ** 3 / (l0_ms * 1e-3) / 1e12
+    line["roofline_fp64"] = {"bound": "fp64", "kernel": "k_encode_level (level 0)", "achieved": fp64_ach,
+                             "peak": fp64_tf, "unit": "TFLOP/s", "frac": fp64_ach / fp64_tf,
+                             "peak_source": "measured here: DGEMM 4096^3 (torch.matmul float64), best of 5",
+                             "ops_per_brick": ENC_L0_FP64_OPS_PER_BRICK,
+                             "ops_source": "ncu smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum of "
+                                           "the level-0 launch at 512^3 (4,096 bricks), scaled by bricks"}
     line["roofline_decode"] = {"bound": "hbm", "kernel": "k_decode_planes + k_decode_level (all levels)",
                                "achieved": dec_bytes / (dec_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                                "frac": dec_bytes / (dec_ms * 1e-3) / 1e9 / peak, "algorithmic_bytes": dec_bytes}

@@ -4,6 +4,7 @@
 #include "decode_device.h"
 #include "decoder.h"
 #include "device.h"
+#include "dpack_device.h"
 #include "encoder.h"
 #include "format.h"
 #include "shard.h"
@@ -11,6 +12,7 @@
 
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <atomic>
@@ -229,7 +231,16 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
     const std::shared_ptr<const encode_plan> plan = c->d.plan_for(f, &e);
     if (!plan)
       return e;
-    e = encode_dataset(&f, &p, &coder, nullptr, true, &tm, plan.get(), c->d.file_hint(f));
+    // packed on the device where the plan allows it (every plan of the reference's brick
+    // orders does); IDX2G_HOST_PACK=1 packs on the host
+    static const bool host_pack = [] {
+      const char* v = std::getenv("IDX2G_HOST_PACK");
+      return v && v[0] == '1';
+    }();
+    if (!host_pack && device_pack_applies(f, *plan))
+      e = encode_dataset_dpack(&c->d, &f, &p, &coder, &tm, *plan, c->d.file_hint(f));
+    else
+      e = encode_dataset(&f, &p, &coder, nullptr, true, &tm, plan.get(), c->d.file_hint(f));
     if (!e)
       c->d.set_file_hint(f, tm.level_file_bytes);
     stream_bytes = coder.stream_bytes();

@@ -318,6 +318,12 @@ public:
   double kernel_ms() const { return kernel_ms_; }
   void add_kernel_ms(double ms) { kernel_ms_ += ms; }
   long long launches() const { return launches_; }
+  // A collected level's regions on the device (one field's batch): stream and region offsets
+  // (index brick * 8 + subband), valid while the encoder and its context's workspaces live.
+  void device_level(int l, const uint8_t** stream, const unsigned long long** offset) const;
+  // A level collected with keep_device: its offsets and streams read back into o (one
+  // field's batch), as collect_level does without keep_device.
+  int copy_level_out(int l, level_output* o);
 
   struct level_launch;
 
@@ -354,6 +360,13 @@ public:
   }
   double kernel_ms() const { return enc_ ? enc_->kernel_ms() : 0.0; }
   long long kernel_launches() const { return enc_ ? enc_->launches() : 0; }
+  // After a keep_device encode: the levels' regions on the device, or read back into outs
+  // (whose nexps are set).
+  void device_level(int l, const uint8_t** stream, const unsigned long long** offset) const
+  {
+    enc_->device_level(l, stream, offset);
+  }
+  int copy_level_out(int l, level_output* o) { return enc_->copy_level_out(l, o); }
   long long stream_bytes() const { return fields_[0].stream_bytes; }
   long long exp_bytes() const { return fields_[0].exp_bytes; }
   const std::vector<float>& level_ms() const { return fields_[0].level_ms; }

@@ -1,0 +1,53 @@
+// Device packer, device side: the kernel launches and the encode path around them (dpack.h).
+#pragma once
+
+#include "device.h"
+#include "dpack.h"
+
+namespace idx2g
+{
+
+// One level's coder output on the device: the stream of regions and the region offset of
+// every (brick, subband) (index brick * 8 + subband).
+struct device_level_stream
+{
+  const uint8_t* stream = nullptr;
+  const unsigned long long* offset = nullptr;
+  int nsb = 0;
+  std::vector<int> nexps;  // per subband
+};
+
+struct dpack_args
+{
+  const dpack_segment* segs;
+  int nseg;
+  const dpack_event* evs;
+  const uint8_t* streams[16];
+  const unsigned long long* offsets[16];
+  int etol, end_bp, bpc, exp_bytes;  // exp_bytes: 1 (float32) or 2 (float64)
+  int* seg_kmin;                     // [nseg]: key of slot 0 (or a large value: no keys)
+  dpack_key* keys;                   // [nseg][kSegKeys]
+  const unsigned long long* chunk_off;  // [nseg][kSegKeys]: first byte of the chunk in image
+  uint32_t* image;                   // zeroed
+  uint8_t* exps;                     // raw exponents of every segment
+  int* error;                        // 1: a segment spans more than kSegKeys keys
+};
+
+void dpack_launch_keys(const dpack_args& a, int grid, cudaStream_t st);
+void dpack_launch_write(const dpack_args& a, int grid, cudaStream_t st);
+
+// Packs the levels' regions on ctx's device. Returns NoError, or NotApplicable when a segment
+// holds more keys than the kernels' window (the caller then packs on the host).
+constexpr int kDpackNotApplicable = -2;
+int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& plan,
+                const std::vector<device_level_stream>& levels, packed_dataset* out);
+
+// encode_dataset with the device packer: every level coded with its regions kept on the
+// device, packed there, and the files written. When the packer does not take a segment (more
+// keys than its window), the regions are read back and packed on the host instead.
+// timing: device_s the coding, pack_s the packing (with the copy of the chunk sections to the
+// host), write_s the files.
+int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_coder* coder, encode_timing* timing,
+                         const encode_plan& plan, const std::vector<unsigned long long>* prealloc);
+
+} // namespace idx2g

@@ -1,0 +1,162 @@
+// Device packer, device side (dpack_device.h): the launches of k_pack_keys and k_pack_write
+// between the host stages of dpack_plan.cpp, and the encode path that uses them.
+#include "dpack_device.h"
+
+#include "trace.h"
+
+#include <chrono>
+#include <cstring>
+#include <thread>
+
+namespace idx2g
+{
+
+int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& plan,
+                const std::vector<device_level_stream>& levels, packed_dataset* out)
+{
+  stage_timer tt;
+  cudaStream_t st = ctx->stream;
+  if (levels.size() > 16)
+    return InvalidArgument;
+  std::vector<std::vector<int>> nexps(levels.size());
+  for (size_t l = 0; l < levels.size(); ++l)
+    nexps[l] = levels[l].nexps;
+  dpack_plan P;
+  int e = dpack_make_plan(f, plan, nexps, &P);
+  if (e)
+    return e;
+  const int nseg = (int)P.segs.size();
+  dpack_segment* d_segs = (dpack_segment*)ctx->ws("dpack.segs", sizeof(dpack_segment) * (size_t)nseg);
+  dpack_event* d_evs = (dpack_event*)ctx->ws("dpack.evs", sizeof(dpack_event) * P.evs.size());
+  int* d_kmin = (int*)ctx->ws("dpack.kmin", 4 * (size_t)nseg);
+  dpack_key* d_keys = (dpack_key*)ctx->ws("dpack.keys", sizeof(dpack_key) * (size_t)nseg * kSegKeys);
+  unsigned long long* d_coff = (unsigned long long*)ctx->ws("dpack.coff", 8 * (size_t)nseg * kSegKeys);
+  uint8_t* d_exps = (uint8_t*)ctx->ws("dpack.exps", (size_t)P.exp_total + 16);
+  int* d_err = (int*)ctx->ws("dpack.err", 16);
+  if (!d_segs || !d_evs || !d_kmin || !d_keys || !d_coff || !d_exps || !d_err)
+    return OutOfMemory;
+  cudaMemcpyAsync(d_segs, P.segs.data(), sizeof(dpack_segment) * (size_t)nseg, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_evs, P.evs.data(), sizeof(dpack_event) * P.evs.size(), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(d_err, 0, 16, st);
+  dpack_args a;
+  memset(&a, 0, sizeof a);
+  a.segs = d_segs;
+  a.nseg = nseg;
+  a.evs = d_evs;
+  for (size_t l = 0; l < levels.size(); ++l)
+  {
+    a.streams[l] = levels[l].stream;
+    a.offsets[l] = levels[l].offset;
+  }
+  a.etol = exponent_f64(f.tolerance);
+  a.end_bp = f.type == dtype::float32 ? 32 : 64;
+  a.bpc = f.bit_planes_per_chunk;
+  a.exp_bytes = P.exp_bytes;
+  a.seg_kmin = d_kmin;
+  a.keys = d_keys;
+  a.chunk_off = d_coff;
+  a.exps = d_exps;
+  a.error = d_err;
+  // k_pack_keys: a CTA per segment; k_pack_write: kSegKeys / 8 CTAs per segment
+  const int grid = nseg < 4 * ctx->num_sms ? nseg : 4 * ctx->num_sms;
+  const int wgrid = nseg < 2048 ? nseg : 2048;
+  dpack_launch_keys(a, grid, st);
+  ctx->launches += 1;
+  std::vector<dpack_key> keys((size_t)nseg * kSegKeys);
+  std::vector<int> kmin((size_t)nseg);
+  int err = 0;
+  cudaMemcpyAsync(keys.data(), d_keys, sizeof(dpack_key) * keys.size(), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(kmin.data(), d_kmin, 4 * (size_t)nseg, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return CudaError;
+  if (err)
+    return kDpackNotApplicable;
+  tt.lap("dpack.keys");
+  out->files.clear();
+  out->stats = pack_stats();
+  dpack_layout L;
+  e = dpack_make_layout(f, P, keys, kmin, &L, out);
+  if (e)
+    return e;
+  tt.lap("dpack.layout");
+  const size_t img_words = (size_t)((L.total + 3) / 4) + 1;
+  uint32_t* d_img = (uint32_t*)ctx->ws("dpack.image", img_words * 4);
+  uint8_t* h_img = (uint8_t*)ctx->pinned("dpack.himage", (size_t)L.total + 16);
+  uint8_t* h_exps = (uint8_t*)ctx->pinned("dpack.hexps", (size_t)P.exp_total + 16);
+  if (!d_img || !h_img || !h_exps)
+    return OutOfMemory;
+  cudaMemcpyAsync(d_coff, L.chunk_off.data(), 8 * L.chunk_off.size(), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(d_img, 0, img_words * 4, st);
+  a.image = d_img;
+  dpack_launch_write(a, wgrid, st);
+  ctx->launches += 1;
+  if (L.total)
+    cudaMemcpyAsync(h_img, d_img, (size_t)L.total, cudaMemcpyDeviceToHost, st);
+  if (P.exp_total)
+    cudaMemcpyAsync(h_exps, d_exps, (size_t)P.exp_total, cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return CudaError;
+  tt.lap("dpack.write");
+  e = dpack_finish(f, P, L, h_img, h_exps, out);
+  tt.lap("dpack.finish");
+  return e;
+}
+
+int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_coder* coder, encode_timing* timing,
+                         const encode_plan& plan, const std::vector<unsigned long long>* prealloc)
+{
+  auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+  const double t0 = now();
+  std::thread pre;
+  if (prealloc)
+    pre = preallocate_files(*f, plan, *prealloc);
+  struct joiner
+  {
+    std::thread& t;
+    ~joiner()
+    {
+      if (t.joinable())
+        t.join();
+    }
+  } join_pre{ pre };
+  coder->set_keep_device(true);
+  std::vector<level_output> outs;
+  int e = encode_levels(f, coder, &outs, plan);
+  if (e)
+    return e;
+  const double t1 = now();
+  std::vector<device_level_stream> lv(outs.size());
+  for (size_t l = 0; l < outs.size(); ++l)
+  {
+    coder->device_level((int)l, &lv[l].stream, &lv[l].offset);
+    lv[l].nsb = outs[l].nsb;
+    lv[l].nexps = outs[l].nexps;
+  }
+  packed_dataset pd;
+  e = device_pack(ctx, *f, plan, lv, &pd);
+  if (e == kDpackNotApplicable)
+  {
+    // a segment with more keys than the kernels' window: the regions to the host packer
+    e = NoError;
+    for (size_t l = 0; l < outs.size() && !e; ++l)
+      e = coder->copy_level_out((int)l, &outs[l]);
+    if (e)
+      return e;
+    e = pack_dataset(f, p, plan, outs, nullptr, true, timing, &pre);
+    if (timing)
+      timing->device_s = t1 - t0;
+    return e;
+  }
+  if (e)
+    return e;
+  if (timing)
+    note_level_files(*f, plan, pd.files, timing);
+  const double t2 = now();
+  e = write_dataset(f, p, pd.files, pack_stats_text(pd.stats), nullptr, true, timing, &pre, t2 - t1);
+  if (timing)
+    timing->device_s = t1 - t0;
+  return e;
+}
+
+} // namespace idx2g

@@ -1981,6 +1981,46 @@ int batch_encoder::collect_level(int l, bool keep_device)
   return NoError;
 }
 
+void batch_encoder::device_level(int l, const uint8_t** stream, const unsigned long long** offset) const
+{
+  const level_launch& ll = *levels_[(size_t)l];
+  *stream = reinterpret_cast<const uint8_t*>(ll.args.stream);
+  *offset = ll.d_off;
+}
+
+int batch_encoder::copy_level_out(int l, level_output* o)
+{
+  level_launch& ll = *levels_[(size_t)l];
+  cudaStream_t st = ctx_->stream;
+  const int nbr = (int)ll.bricks.size();
+  unsigned long long used = 0;
+  cudaMemcpyAsync(&used, ll.d_misc, 8, cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return CudaError;
+  std::vector<unsigned long long> off((size_t)nbr * 8);
+  const uint8_t* pin = nullptr;
+  if (nbr > 0)
+    cudaMemcpyAsync(off.data(), ll.d_off, off.size() * 8, cudaMemcpyDeviceToHost, st);
+  if (used)
+  {
+    char name[96];
+    snprintf(name, sizeof name, "enc.pin.%s.%d", tag_.c_str(), l);
+    pin = (const uint8_t*)ctx_->pinned(name, (size_t)used);
+    if (!pin)
+      return OutOfMemory;
+    cudaMemcpyAsync((void*)pin, ll.args.stream, (size_t)used, cudaMemcpyDeviceToHost, st);
+  }
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return CudaError;
+  const int nsb = o->nsb;
+  o->offset.resize((size_t)nbr * (size_t)nsb);
+  for (int b = 0; b < nbr; ++b)
+    for (int sb = 0; sb < nsb; ++sb)
+      o->offset[(size_t)b * (size_t)nsb + (size_t)sb] = off[(size_t)b * 8 + (size_t)sb];
+  o->ext_stream = pin;
+  return NoError;
+}
+
 int batch_encoder::run_all(bool use_graph, bool keep_device)
 {
   cudaStream_t st = ctx_->stream;

@@ -249,6 +249,26 @@ int encode_dataset(dataset_format* f, params* p, brick_coder* coder,
   return e;
 }
 
+// Bytes of every level's data file when each level has exactly one.
+void note_level_files(const dataset_format& f, const encode_plan& plan, const std::map<std::string, file_buffer>& data,
+                      encode_timing* timing)
+{
+  timing->level_file_bytes.clear();
+  if ((int)data.size() != f.nlevels || (int)plan.levels.size() < f.nlevels)
+    return;
+  std::vector<unsigned long long> v((size_t)f.nlevels, 0);
+  for (int l = 0; l < f.nlevels; ++l)
+  {
+    if (plan.levels[(size_t)l].empty())
+      return;
+    auto it = data.find(file_path(f, plan.levels[(size_t)l][0].linear, l));
+    if (it == data.end())
+      return;
+    v[(size_t)l] = it->second.nbytes;
+  }
+  timing->level_file_bytes = v;
+}
+
 int pack_dataset(const dataset_format* f, const params* p, const encode_plan& plan,
                  const std::vector<level_output>& outs, std::map<std::string, std::vector<uint8_t>>* files,
                  bool write_files, encode_timing* timing, std::thread* before_write)
@@ -286,34 +306,23 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
   if (e)
     return e;
   if (timing)
-  {
-    timing->level_file_bytes.clear();
-    if ((int)pk.files().size() == f->nlevels && (int)plan.levels.size() >= f->nlevels)
-    {
-      std::vector<unsigned long long> v((size_t)f->nlevels, 0);
-      bool one_each = true;
-      for (int l = 0; l < f->nlevels && one_each; ++l)
-      {
-        one_each = !plan.levels[(size_t)l].empty();
-        if (!one_each)
-          break;
-        auto it = pk.files().find(file_path(*f, plan.levels[(size_t)l][0].linear, l));
-        one_each = it != pk.files().end();
-        if (one_each)
-          v[(size_t)l] = it->second.nbytes;
-      }
-      if (one_each)
-        timing->level_file_bytes = v;
-    }
-  }
+    note_level_files(*f, plan, pk.files(), timing);
   double t2 = now_s();
-  tt.t = stage_timer::now();
+  return write_dataset(f, p, pk.files(), pk.stats_text(), files, write_files, timing, before_write, t2 - t1);
+}
 
-  std::string meta = meta_text(*f, *p) + pk.stats_text();
+int write_dataset(const dataset_format* f, const params* p, std::map<std::string, file_buffer>& data,
+                  const std::string& stats, std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
+                  encode_timing* timing, std::thread* before_write, double pack_s)
+{
+  stage_timer tt;
+  const double t2 = now_s();
+  int e = NoError;
+  std::string meta = meta_text(*f, *p) + stats;
   std::string meta_path = p->out_dir + "/" + p->name + "/" + p->field + ".idx2";
   std::vector<const std::pair<const std::string, file_buffer>*> list;
   unsigned long long total = meta.size();
-  for (auto& kv : pk.files())
+  for (auto& kv : data)
   {
     list.push_back(&kv);
     total += kv.second.nbytes;
@@ -349,7 +358,7 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
   double t3 = now_s();
   if (timing)
   {
-    timing->pack_s = t2 - t1;
+    timing->pack_s = pack_s;
     timing->write_s = t3 - t2;
     timing->file_bytes = total;
     timing->nfiles = (int)list.size() + 1;

@@ -139,6 +139,18 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
                  const std::vector<level_output>& outs, std::map<std::string, std::vector<uint8_t>>* files,
                  bool write_files, encode_timing* timing, std::thread* before_write = nullptr);
 
+// The second half of pack_dataset: the metadata file (format text + stats) and the data
+// files from their parts; files / write_files / timing / before_write as pack_dataset.
+struct file_buffer;
+int write_dataset(const dataset_format* f, const params* p, std::map<std::string, file_buffer>& data,
+                  const std::string& stats, std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
+                  encode_timing* timing, std::thread* before_write, double pack_s);
+
+// Bytes of every level's data file into timing->level_file_bytes, when each level has
+// exactly one (else empty).
+void note_level_files(const dataset_format& f, const encode_plan& plan, const std::map<std::string, file_buffer>& data,
+                      encode_timing* timing);
+
 // Allocate the pages of each level's data file (sizes[l] bytes, file size unchanged) on a new
 // thread; levels with fewer than 64 MB are left alone.
 std::thread preallocate_files(const dataset_format& f, const encode_plan& plan,

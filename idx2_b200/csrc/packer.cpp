@@ -989,40 +989,44 @@ int packer::finish()
   return NoError;
 }
 
-std::string packer::stats_text() const
+std::string pack_stats_text(const pack_stats& st)
 {
   // Core/idx2Write.cpp:389 PrintStats
   char buf[1024];
   std::string o;
   o += "\n\n---------------- Statistics ----------------\n\n";
-  snprintf(buf, sizeof buf, "num chunks = %lld (bit plane) and %lld (exponent) \n",
-           stats_.bit_plane_chunks.n, stats_.exp_chunks_z.n);
+  snprintf(buf, sizeof buf, "num chunks = %lld (bit plane) and %lld (exponent) \n", st.bit_plane_chunks.n,
+           st.exp_chunks_z.n);
   o += buf;
-  snprintf(buf, sizeof buf, "bit plane chunk: total = %d avg = %d stddev = %d bytes\n",
-           (int)stats_.bit_plane_chunks.s, (int)stats_.bit_plane_chunks.avg(),
-           (int)stats_.bit_plane_chunks.sd());
+  snprintf(buf, sizeof buf, "bit plane chunk: total = %d avg = %d stddev = %d bytes\n", (int)st.bit_plane_chunks.s,
+           (int)st.bit_plane_chunks.avg(), (int)st.bit_plane_chunks.sd());
   o += buf;
-  snprintf(buf, sizeof buf, "  (metadata) brick deltas = %d bytes\n", (int)stats_.brick_deltas.s);
+  snprintf(buf, sizeof buf, "  (metadata) brick deltas = %d bytes\n", (int)st.brick_deltas.s);
   o += buf;
-  snprintf(buf, sizeof buf, "  (metadata) brick sizes = %d bytes\n", (int)stats_.brick_sizes.s);
+  snprintf(buf, sizeof buf, "  (metadata) brick sizes = %d bytes\n", (int)st.brick_sizes.s);
   o += buf;
-  snprintf(buf, sizeof buf, "  (metadata) chunk sizes = %d bytes\n", (int)stats_.chunk_sizes.s);
+  snprintf(buf, sizeof buf, "  (metadata) chunk sizes = %d bytes\n", (int)st.chunk_sizes.s);
   o += buf;
   snprintf(buf, sizeof buf, "  (metadata) chunk addresses: uncompressed = %d, compressed = %d bytes\n",
-           (int)stats_.chunk_addrs_raw.s, (int)stats_.chunk_addrs_z.s);
+           (int)st.chunk_addrs_raw.s, (int)st.chunk_addrs_z.s);
   o += buf;
   o += "exponent chunk:\n";
-  snprintf(buf, sizeof buf, "  uncompressed: total = %d bytes\n", (int)stats_.exp_chunks_raw.s);
+  snprintf(buf, sizeof buf, "  uncompressed: total = %d bytes\n", (int)st.exp_chunks_raw.s);
   o += buf;
-  snprintf(buf, sizeof buf, "  compressed: total = %d avg = %d stddev = %d bytes\n",
-           (int)stats_.exp_chunks_z.s, (int)stats_.exp_chunks_z.avg(), (int)stats_.exp_chunks_z.sd());
+  snprintf(buf, sizeof buf, "  compressed: total = %d avg = %d stddev = %d bytes\n", (int)st.exp_chunks_z.s,
+           (int)st.exp_chunks_z.avg(), (int)st.exp_chunks_z.sd());
   o += buf;
-  snprintf(buf, sizeof buf, "  (metadata) chunk sizes = %d bytes\n", (int)stats_.exp_chunk_sizes.s);
+  snprintf(buf, sizeof buf, "  (metadata) chunk sizes = %d bytes\n", (int)st.exp_chunk_sizes.s);
   o += buf;
   snprintf(buf, sizeof buf, "  (metadata) chunk addresses: uncompressed = %d, compressed = %d bytes\n",
-           (int)stats_.exp_addrs_raw.s, (int)stats_.exp_addrs_z.s);
+           (int)st.exp_addrs_raw.s, (int)st.exp_addrs_z.s);
   o += buf;
   return o;
+}
+
+std::string packer::stats_text() const
+{
+  return pack_stats_text(stats_);
 }
 
 } // namespace idx2g

@@ -148,6 +148,9 @@ private:
   pack_stats stats_;
 };
 
+// The statistics block the reference appends to the metadata file (Core/idx2Write.cpp:389).
+std::string pack_stats_text(const pack_stats& s);
+
 // zstd level 1: frames byte-identical to the reference's zstd 1.4.5 (zstd_frame.cpp); the
 // decompression goes through the system libzstd (loaded at run time; any version reads them).
 int zstd_compress(const uint8_t* src, size_t n, std::vector<uint8_t>* out);
