@@ -1225,41 +1225,43 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         const int s0 = (hx << 2) | (hy << 1), s1 = s0 | 1;
         const bool n0 = (a.norm_mask >> s0) & 1, n1 = (a.norm_mask >> s1) & 1;
         const double w0 = a.inv_weight[s0], w1 = a.inv_weight[s1];
-        auto even = [&](int e) -> double {
-          const double f = c0[(e >> 1) * sz];
-          return n0 ? __dmul_rn(f, w0) : f;
-        };
-        auto odd = [&](int o) -> double {
-          const double f = c1[(o >> 1) * sz];
-          return n1 ? __dmul_rn(f, w1) : f;
-        };
-        int e = z0 & ~1;
-        double Om = e > 0 ? odd(e - 1) : 0.0;   // c(e - 1)
-        double Op = odd(e + 1);                 // c(e + 1), e <= 30 here
-        double Ee = even(e);
-        if (e > 0)
-          Ee = __dsub_rn(Ee, __dmul_rn(Om, 0.25));
-        Ee = __dsub_rn(Ee, __dmul_rn(Op, 0.25));
-        double* col_out = S + col;
-        for (;;)
+        // the column's coefficients at z = z0 - 2 .. z0 + kZGroup + 1 (those in 0..32), loaded
+        // together; then the even planes' updates in place, then the odd planes
+        constexpr int W = kZGroup + 4;
+        double c[W];
+#pragma unroll
+        for (int t = 0; t < W; ++t)
         {
-          if (e >= z0 && e < z0 + gz)
-            col_out[(e - z0) * 33 * 33] = Ee;
-          if (e == 32 || e + 1 >= z0 + gz)
-            break;
-          // even plane e + 2 from c(e + 1) and c(e + 3), then odd plane e + 1
-          double E2 = even(e + 2);
-          E2 = __dsub_rn(E2, __dmul_rn(Op, 0.25));
-          double O3 = 0.0;
-          if (e + 3 <= 31)
+          const int z = z0 - 2 + t;
+          double v = 0.0;
+          if (z >= 0 && z <= 32 && z < z0 + gz + 2)
           {
-            O3 = odd(e + 3);
-            E2 = __dsub_rn(E2, __dmul_rn(O3, 0.25));
+            const double f = (z & 1) ? c1[(z >> 1) * sz] : c0[(z >> 1) * sz];
+            v = (z & 1) ? (n1 ? __dmul_rn(f, w1) : f) : (n0 ? __dmul_rn(f, w0) : f);
           }
-          col_out[(e + 1 - z0) * 33 * 33] = __dadd_rn(Op, __dmul_rn(__dadd_rn(Ee, E2), 0.5));
-          e += 2;
-          Ee = E2;
-          Op = O3;
+          c[t] = v;
+        }
+#pragma unroll
+        for (int t = 1; t < W - 1; ++t)
+        {
+          const int z = z0 - 2 + t;
+          if ((z & 1) || z < 0 || z > 32 || z > z0 + gz)
+            continue;
+          double v = c[t];
+          if (z > 0)
+            v = __dsub_rn(v, __dmul_rn(c[t - 1], 0.25));
+          if (z < 32)
+            v = __dsub_rn(v, __dmul_rn(c[t + 1], 0.25));
+          c[t] = v;
+        }
+        double* col_out = S + col;
+#pragma unroll
+        for (int t = 2; t < W - 2; ++t)
+        {
+          const int z = z0 - 2 + t;
+          if (z >= z0 + gz)
+            break;
+          col_out[(t - 2) * 33 * 33] = (z & 1) ? __dadd_rn(c[t], __dmul_rn(__dadd_rn(c[t - 1], c[t + 1]), 0.5)) : c[t];
         }
       }
       __syncthreads();

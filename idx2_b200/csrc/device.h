@@ -48,8 +48,9 @@ struct device_ctx
   // from (a byte image of every launch's arguments) and the executable graph
   struct cached_graph
   {
-    std::string launches;
+    std::string launches;            // signature of the captured launches
     cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;           // kernels the graph launches
   };
   std::map<std::string, cached_graph> graphs;
   // Encode plans by format: the brick order and the EncodeSubband events depend only on the

@@ -2067,10 +2067,11 @@ int batch_encoder::run_all(bool use_graph, bool keep_device)
       cudaGraphDestroy(g);
       cg_.exec = ge;
       cg_.launches = sig;
-      graph_launches_ = launches_ - before;
+      cg_.kernels = launches_ - before;
       launches_ = before;
-      ctx_->launches -= graph_launches_;
+      ctx_->launches -= cg_.kernels;
     }
+    graph_launches_ = cg_.kernels;
     stage_timer tt;
     cudaEventRecord(ctx_->ev0, st);
     cudaGraphLaunch(cg_.exec, st);
