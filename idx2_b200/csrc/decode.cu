@@ -578,8 +578,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
 namespace
 {
 
-// Pieces of kept bricks (33^3 or 33^2 samples, x fastest) to a dense buffer, x fastest: a CTA
-// per piece.
+// Pieces of kept bricks (subband-major) to a dense buffer, x fastest: a CTA per piece.
 __global__ void k_gather_pieces(const brick_piece* pieces, int n, int is2d, double* out)
 {
   for (int pi = blockIdx.x; pi < n; pi += gridDim.x)
@@ -590,7 +589,7 @@ __global__ void k_gather_pieces(const brick_piece* pieces, int n, int is2d, doub
     for (int i = threadIdx.x; i < cnt; i += blockDim.x)
     {
       const int x = i % p.dims[0], y = (i / p.dims[0]) % p.dims[1], z = i / nxy;
-      out[p.out + i] = p.src[((p.from[2] + z) * 33 + p.from[1] + y) * 33 + p.from[0] + x];
+      out[p.out + i] = p.src[sbm(p.from[0] + x, p.from[1] + y, p.from[2] + z, is2d)];
     }
   }
 }

@@ -60,7 +60,7 @@ struct decode_request
 };
 
 // Brick-map mode (the reference's HashMap output, Core/idx2Decode.cpp:446-477): every decoded
-// level's bricks are kept on the device (33^3 or 33^2 samples x fastest, in plan order) with a significance flag
+// level's bricks are kept on the device (subband-major, in plan order) with a significance flag
 // per brick (a block of a subband > 0, or of the coarsest level, was decoded).
 struct decode_keep
 {
@@ -98,7 +98,7 @@ public:
   int decode_batch(device_ctx* ctx, const std::vector<const decode_request*>& rqs, void* const* outs,
                    const size_t* out_bytes, bool out_on_device, double* kernel_ms, void* coeff_out = nullptr,
                    decode_keep* keep = nullptr);
-  // Copy pieces of kept bricks into a host buffer of `total` doubles.
+  // Copy pieces of kept bricks (subband-major) into a host buffer of `total` doubles.
   static int gather_bricks(device_ctx* ctx, const std::vector<brick_piece>& pieces, bool is2d, size_t total,
                            double* host_out);
   // Allocation-free decode into a device buffer: every temporary lives in a fixed static

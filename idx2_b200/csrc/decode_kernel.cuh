@@ -33,7 +33,6 @@ __device__ unsigned long long g_dec_phase_cycles[16];
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRing = 32;  // steps a decoded plane stays in the per-warp ring (>= channels)
-constexpr int kZGroup = 7;  // z-planes per group of the streamed inverse transform (33 = 4 x 7 + 5)
 
 struct dec_args
 {
@@ -97,7 +96,11 @@ struct dec_smem
   {
     unsigned long long coef[kMaxBlocksPerSubband][64];  // CTA-wide path: one subband
     unsigned long long ring[kWarps][kRing][32];         // warp path: decoded planes in flight
-    double planes[kZGroup][33][33];  // inverse transform: the group of z-planes being made
+    struct
+    {
+      double v[kWarps][32][33];     // output rows of the X sweep, one per lane
+      long long base[kWarps][32];   // their offsets in the output (-1: no output)
+    } out;
   } u;
   long long q[kWarps][2][80];  // per-warp block scratch (two blocks, padded in the table path)
   int16_t emax[8][kMaxBlocksPerSubband];
@@ -158,14 +161,22 @@ __device__ __forceinline__ void subband_grid(int is2d, int s, int from[3], int d
   }
 }
 
-// The coefficients of a brick are held subband-major in its slot: the 33^3 samples are the 8
-// subbands (index 4hx + 2hy + hz, of 17 - h samples per axis) one after the other, each dense
-// and x-fastest. Blocks then land in contiguous rows, and a column of the inverse Z lifting
-// reads two dense streams (its even and odd samples).
+// Decoded bricks are stored subband-major: the 33^3 samples are the 8 subbands (index
+// 4hx + 2hy + hz, of 17 - h samples per axis) one after the other, each dense and x-fastest.
+// Blocks then land in contiguous rows, and a line of the inverse transform reads two dense
+// streams (its even and odd samples).
 __device__ __forceinline__ int sbm_base(int hx, int hy, int hz, int is2d)
 {
   const int dx = 17 - hx, dy = 17 - hy;
   return is2d ? hx * 17 * 33 + hy * dx * 17 : hx * 17 * 33 * 33 + hy * dx * 17 * 33 + hz * dx * dy * 17;
+}
+
+// Position (x, y, z) of the brick in the subband-major layout.
+__device__ __forceinline__ int sbm(int x, int y, int z, int is2d)
+{
+  const int hx = x & 1, hy = y & 1, hz = z & 1;
+  const int dx = 17 - hx, dy = 17 - hy;
+  return sbm_base(hx, hy, hz, is2d) + (((z >> 1) * dy + (y >> 1)) * dx + (x >> 1));
 }
 
 // LSB-first bit reader over the blob with a 128-bit register window (Core/BitStream.h
@@ -323,9 +334,8 @@ __device__ __forceinline__ void ilift33(double (&v)[33])
 // Bit planes of one (brick, subband): the wavefront of the group-test decoder alone
 // (Core/idx2Decode.cpp:141-202). Channel c = kmax - key is owned by lane c % 32 (G groups of
 // 32 channels); at step t it decodes its plane of block t - c, taking the block's significance
-// count from channel c - 1 at step t - 1. The unit's table is block-major (row length nkeys):
-// block b's plane in channel c is row b, column c, so that the blocks' rebuild reads a block's
-// planes as one dense row (the wavefront's stores scatter instead).
+// count from channel c - 1 at step t - 1. The plane masks of step t are stored as row t of the
+// unit's table (row length nkeys): block b's plane in channel c is row b + c, column c.
 // ---------------------------------------------------------------------------
 constexpr int kPlaneWarps = 8;
 
@@ -411,17 +421,17 @@ __device__ __forceinline__ void plane_wavefront(const dec1_args& a, size_t fs, i
             }
           }
         }
-        if (c < nkeys && b >= 0 && b < nb)
-          T[(size_t)b * (size_t)nkeys + (size_t)c] = X;
+        if (c < nkeys)
+          T[(size_t)t * (size_t)nkeys + (size_t)c] = X;
       }
-      else if (c < nkeys && b >= 0 && b < nb)
+      else if (c < nkeys)
       {
         // several planes per key: the block's planes of this key, top-down, from the same
-        // stream; slot j of the (block, channel) entry holds key value key * bpc + bpc - 1 - j
-        unsigned long long* row = T + ((size_t)b * (size_t)nkeys + (size_t)c) * (size_t)a.bpc;
+        // stream; slot j of the (step, channel) entry holds key value key * bpc + bpc - 1 - j
+        unsigned long long* row = T + ((size_t)t * (size_t)nkeys + (size_t)c) * (size_t)a.bpc;
         for (int j = 0; j < a.bpc; ++j)
           row[j] = 0ull;
-        if (npl[b] > 0)
+        if (b >= 0 && b < nb && npl[b] > 0)
         {
           const int top = ktop[b], key = kmax - c;
           int kk0, kk1;
@@ -521,7 +531,7 @@ __device__ __forceinline__ plane_unit prep_unit(const dec1_args& a, int unit, in
     return u;
   }
   const unsigned long long bytes =
-    (unsigned long long)nb * (unsigned long long)nkeys * 8ull * (unsigned long long)a.bpc;
+    (unsigned long long)(nb + nkeys - 1) * (unsigned long long)nkeys * 8ull * (unsigned long long)a.bpc;
   unsigned long long base = 0;
   if (lane == 0)
     base = atomicAdd(a.cursor, bytes);
@@ -576,6 +586,7 @@ __device__ __forceinline__ void plane_wavefront_pair(const dec1_args& a, const p
       }
     }
   }
+  const int my_steps = nb + nkeys - 1;
   const int sA = A.nb + A.nkeys - 1, sB = B.nb + B.nkeys - 1;
   const int steps = sA > sB ? sA : sB;
   int n_out = 0, stop_out = 0;
@@ -611,8 +622,8 @@ __device__ __forceinline__ void plane_wavefront_pair(const dec1_args& a, const p
         }
       }
     }
-    if (c < nkeys && b >= 0 && b < nb)
-      U.T[(size_t)b * (size_t)nkeys + (size_t)c] = X;
+    if (c < nkeys && t < my_steps)
+      U.T[(size_t)t * (size_t)nkeys + (size_t)c] = X;
   }
 }
 
@@ -687,6 +698,24 @@ __global__ void __launch_bounds__(kPlaneWarps * 32, WIDE ? 2 : (MULTI ? 6 : 4)) 
   }
 }
 
+// One inverse line over two dense streams (even samples at c0, odd at c1, compile-time stride
+// ST), with the de-normalisation weights of the two streams applied as they are loaded.
+template <int ST>
+__device__ __forceinline__ void ilift_streams(double* c0, double* c1, bool n0, double w0, bool n1, double w1)
+{
+  double v[33];
+#pragma unroll
+  for (int k = 0; k < 33; ++k)
+  {
+    const double f = (k & 1) ? c1[(k >> 1) * ST] : c0[(k >> 1) * ST];
+    v[k] = (k & 1) ? (n1 ? __dmul_rn(f, w1) : f) : (n0 ? __dmul_rn(f, w0) : f);
+  }
+  ilift33(v);
+#pragma unroll
+  for (int k = 0; k < 33; ++k)
+    ((k & 1) ? c1 : c0)[(k >> 1) * ST] = v[k];
+}
+
 __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -716,9 +745,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       sm.sig = 0;
     __syncthreads();
     const decode_target& rq = sm.rq;
-    // the brick's coefficients, then its inverse transform's input, in this CTA's slot
-    // (subband-major); decoded samples go to the output or to the kept brick (x fastest)
-    double* F = a.slots + (size_t)blockIdx.x * (size_t)NB;
+    double* F = rq.is_output ? a.slots + (size_t)blockIdx.x * (size_t)NB
+                             : a.bricks_out + (size_t)br.store * (size_t)NB;
     // 1: zero + parent low band (Core/idx2Decode.cpp:285-293)
     if (!a.coeff_out)
       for (int i = tid; i < NB; i += kThreads)
@@ -732,7 +760,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
       {
         int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
         // even positions of the child: its subband 0, dense
-        F[(z * 17 + y) * 17 + x] = P[((br.pos[2] * nz + z) * 33 + br.pos[1] * 16 + y) * 33 + br.pos[0] * 16 + x];
+        F[(z * 17 + y) * 17 + x] =
+          P[sbm(br.pos[0] * 16 + x, br.pos[1] * 16 + y, br.pos[2] * nz + z, a.is2d)];
       }
     }
 
@@ -838,7 +867,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         }
         const int dx = 17 - hx, dy = 17 - hy;
         double* const sbase = F + sbm_base(hx, hy, hz, a.is2d);
-        // plane k of block b (bit plane 63 - k) is in channel c0 + k: row b, column c0 + k;
+        // plane k of block b (bit plane 63 - k) is in channel c0 + k, table row b + c0 + k;
         // blocks with nothing to decode (no planes, or not part of the request) stay zero
         auto load_planes = [&](int b, unsigned long long& x0, unsigned long long& x1) {
           x0 = 0;
@@ -851,20 +880,20 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
           const int top = sm.ktop[s][b], bpc = a.bpc;
           if (bpc == 1)
           {
-            // plane kk in channel c0 + kk: a dense run of the block's row
+            // plane kk in channel c0 + kk, table row b + c0 + kk
             const int c0 = kmax - top;
             if (lane < np && c0 + lane < nkeys)
-              x0 = T[(size_t)b * (size_t)nkeys + (size_t)(c0 + lane)];
+              x0 = T[(size_t)(b + c0 + lane) * (size_t)nkeys + (size_t)(c0 + lane)];
             if (lane + 32 < np && c0 + lane + 32 < nkeys)
-              x1 = T[(size_t)b * (size_t)nkeys + (size_t)(c0 + lane + 32)];
+              x1 = T[(size_t)(b + c0 + lane + 32) * (size_t)nkeys + (size_t)(c0 + lane + 32)];
             return;
           }
-          // plane kk: channel c = kmax - key, slot key * bpc + bpc - 1 - (top - kk) of (b, c)
+          // plane kk: channel c = kmax - key, step b + c, slot key * bpc + bpc - 1 - (top - kk)
           auto at = [&](int kk) -> unsigned long long {
             const int key = dev::plane_key(top, kk, bpc), c = kmax - key;
             if (c >= nkeys)
               return 0ull;
-            return T[((size_t)b * (size_t)nkeys + (size_t)c) * (size_t)bpc +
+            return T[((size_t)(b + c) * (size_t)nkeys + (size_t)c) * (size_t)bpc +
                      (size_t)(key * bpc + bpc - 1 - (top - kk))];
           };
           if (lane < np)
@@ -1193,140 +1222,114 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
 
     if (a.coeff_out)
       continue;
-    // 4: de-normalise + inverse CDF5/3 Z, Y, X (Core/Wavelet.cpp:144-203), streamed over
-    // groups of z-planes: the inverse Z lifting makes a group's planes from the coefficients in
-    // the slot (de-normalised as they are loaded), then they are lifted along Y and X in shared
-    // memory and cropped, cast and written to the output (or copied whole to the kept brick).
-    // Per line the operations and their order are those of a sweep over the whole brick.
-    double* const S = sm.u.planes[0][0];
-    const int nplanes = a.is2d ? 1 : 33;
-    double* const K = rq.is_output ? nullptr : a.bricks_out + (size_t)br.store * (size_t)NB;
-    for (int z0 = 0; z0 < nplanes; z0 += kZGroup)
+    // 4: de-normalise + inverse CDF5/3 Z, Y, X (Core/Wavelet.cpp:144-203); the
+    // de-normalisation is applied as the Z lines are loaded, the output crop and cast as the
+    // X lines are stored.
+    if (!a.is2d)
     {
-      const int gz = nplanes - z0 < kZGroup ? nplanes - z0 : kZGroup;
-      // Z (Core/Wavelet.h:250 ILiftCdf53 along z): per column, even plane e is
-      // E(e) = (c(e) - c(e-1) / 4) - c(e+1) / 4 and odd plane o is c(o) + (E(o-1) + E(o+1)) / 2,
-      // c the de-normalised coefficients; in 2D the one plane is c itself
-      for (int col = tid; col < 33 * 33; col += kThreads)
+      for (int li = tid; li < 33 * 33; li += kThreads)
       {
-        const int x = col % 33, y = col / 33;
+        const int x = li % 33, y = li / 33;
+        // even and odd z samples of the column: two dense streams of stride dx * dy
         const int hx = x & 1, hy = y & 1, dx = 17 - hx, dy = 17 - hy;
-        const int off = (y >> 1) * dx + (x >> 1);
-        if (a.is2d)
-        {
-          const int sb = (hx << 1) | hy;
-          const double f = F[sbm_base(hx, hy, 0, 1) + off];
-          S[col] = (a.norm_mask >> sb) & 1 ? __dmul_rn(f, a.inv_weight[sb]) : f;
-          continue;
-        }
-        const double* c0 = F + sbm_base(hx, hy, 0, 0) + off;
-        const double* c1 = F + sbm_base(hx, hy, 1, 0) + off;
-        const int sz = dx * dy;
+        const int off = (y >> 1) * dx + (x >> 1), sz = dx * dy;
+        double* c0 = F + sbm_base(hx, hy, 0, 0) + off;
+        double* c1 = F + sbm_base(hx, hy, 1, 0) + off;
         const int s0 = (hx << 2) | (hy << 1), s1 = s0 | 1;
         const bool n0 = (a.norm_mask >> s0) & 1, n1 = (a.norm_mask >> s1) & 1;
         const double w0 = a.inv_weight[s0], w1 = a.inv_weight[s1];
-        // the column's coefficients at z = z0 - 2 .. z0 + kZGroup + 1 (those in 0..32), loaded
-        // together; then the even planes' updates in place, then the odd planes
-        constexpr int W = kZGroup + 4;
-        double c[W];
-#pragma unroll
-        for (int t = 0; t < W; ++t)
-        {
-          const int z = z0 - 2 + t;
-          double v = 0.0;
-          if (z >= 0 && z <= 32 && z < z0 + gz + 2)
-          {
-            const double f = (z & 1) ? c1[(z >> 1) * sz] : c0[(z >> 1) * sz];
-            v = (z & 1) ? (n1 ? __dmul_rn(f, w1) : f) : (n0 ? __dmul_rn(f, w0) : f);
-          }
-          c[t] = v;
-        }
-#pragma unroll
-        for (int t = 1; t < W - 1; ++t)
-        {
-          const int z = z0 - 2 + t;
-          if ((z & 1) || z < 0 || z > 32 || z > z0 + gz)
-            continue;
-          double v = c[t];
-          if (z > 0)
-            v = __dsub_rn(v, __dmul_rn(c[t - 1], 0.25));
-          if (z < 32)
-            v = __dsub_rn(v, __dmul_rn(c[t + 1], 0.25));
-          c[t] = v;
-        }
-        double* col_out = S + col;
-#pragma unroll
-        for (int t = 2; t < W - 2; ++t)
-        {
-          const int z = z0 - 2 + t;
-          if (z >= z0 + gz)
-            break;
-          col_out[(t - 2) * 33 * 33] = (z & 1) ? __dadd_rn(c[t], __dmul_rn(__dadd_rn(c[t - 1], c[t + 1]), 0.5)) : c[t];
-        }
+        if (sz == 17 * 17)
+          ilift_streams<17 * 17>(c0, c1, n0, w0, n1, w1);
+        else if (sz == 16 * 17)
+          ilift_streams<16 * 17>(c0, c1, n0, w0, n1, w1);
+        else
+          ilift_streams<16 * 16>(c0, c1, n0, w0, n1, w1);
       }
       __syncthreads();
       DEC_PHASE(3)
-      // Y: a line per (plane, x), lanes along x
-      for (int li = tid; li < gz * 33; li += kThreads)
+    }
+    for (int li = tid; li < 33 * N[2]; li += kThreads)
+    {
+      const int x = li % 33, z = li / 33;
+      // even and odd y samples of the line: two dense streams of stride dx
+      const int hx = x & 1, hz = z & 1, dx = 17 - hx;
+      double* c0 = F + sbm_base(hx, 0, hz, a.is2d) + (z >> 1) * dx * 17 + (x >> 1);
+      double* c1 = F + sbm_base(hx, 1, hz, a.is2d) + (z >> 1) * dx * 16 + (x >> 1);
+      const int s0 = a.is2d ? (hx << 1) : ((hx << 2) | hz), s1 = a.is2d ? (s0 | 1) : (s0 | 2);
+      const bool n0 = a.is2d && ((a.norm_mask >> s0) & 1), n1 = a.is2d && ((a.norm_mask >> s1) & 1);
+      const double w0 = a.inv_weight[s0], w1 = a.inv_weight[s1];
+      if (dx == 17)
+        ilift_streams<17>(c0, c1, n0, w0, n1, w1);
+      else
+        ilift_streams<16>(c0, c1, n0, w0, n1, w1);
+    }
+    __syncthreads();
+    DEC_PHASE(4)
+    // X, warp-uniform iterations (the output rows are staged per warp and written back
+    // row by row, lanes along x)
+    for (int li0 = warp * 32; li0 < 33 * N[2]; li0 += kThreads)
+    {
+      const int li = li0 + lane;
+      const bool active = li < 33 * N[2];
+      const int y = li % 33, z = li / 33;
+      // 5: output (Core/idx2Decode.cpp:431-442 CopyGridGrid): where this row goes, decided
+      // before the row is loaded (fewer live registers around the lift)
+      long long obase = -1;
+      if (rq.is_output && active)
       {
-        double* L = S + (li / 33) * 33 * 33 + (li % 33);
-        double v[33];
-#pragma unroll
-        for (int k = 0; k < 33; ++k)
-          v[k] = L[k * 33];
-        ilift33(v);
-#pragma unroll
-        for (int k = 0; k < 33; ++k)
-          L[k * 33] = v[k];
-      }
-      __syncthreads();
-      DEC_PHASE(4)
-      // X: a line per (plane, y)
-      for (int li = tid; li < gz * 33; li += kThreads)
-      {
-        double* L = S + li * 33;
-        double v[33];
-#pragma unroll
-        for (int k = 0; k < 33; ++k)
-          v[k] = L[k];
-        ilift33(v);
-#pragma unroll
-        for (int k = 0; k < 33; ++k)
-          L[k] = v[k];
-      }
-      __syncthreads();
-      // 5: output (Core/idx2Decode.cpp:431-442 CopyGridGrid), a warp per row, lanes along x;
-      // a kept brick takes the group's planes whole
-      if (rq.is_output)
-      {
-        const int n0 = br.dims[0];
-        for (int r = warp; r < gz * 33; r += kWarps)
+        const int ry = y - br.src_from[1], rz = z - br.src_from[2];
+        if (ry >= 0 && rz >= 0 && ry % br.src_strd[1] == 0 && rz % br.src_strd[2] == 0 &&
+            ry / br.src_strd[1] < br.dims[1] && rz / br.src_strd[2] < br.dims[2])
         {
-          const int y = r % 33, z = z0 + r / 33;
-          const int ry = y - br.src_from[1], rz = z - br.src_from[2];
-          if (ry < 0 || rz < 0 || ry % br.src_strd[1] != 0 || rz % br.src_strd[2] != 0 ||
-              ry / br.src_strd[1] >= br.dims[1] || rz / br.src_strd[2] >= br.dims[2] || lane >= n0)
-            continue;
           const long long oy = br.dst_from[1] + (long long)(ry / br.src_strd[1]) * br.dst_strd[1];
           const long long oz = br.dst_from[2] + (long long)(rz / br.src_strd[2]) * br.dst_strd[2];
-          const long long di = (oz * rq.out_dims[1] + oy) * rq.out_dims[0] + br.dst_from[0] +
-                               (long long)lane * br.dst_strd[0];
-          const double val = S[r * 33 + br.src_from[0] + lane * br.src_strd[0]];
+          obase = (oz * rq.out_dims[1] + oy) * rq.out_dims[0] + br.dst_from[0];
+        }
+      }
+      if (active && (!rq.is_output || obase >= 0))
+      {
+        // even and odd x samples of the row: two dense runs
+        const int hy = y & 1, hz = z & 1, dy = 17 - hy;
+        double* r0 = F + sbm_base(0, hy, hz, a.is2d) + ((z >> 1) * dy + (y >> 1)) * 17;
+        double* r1 = F + sbm_base(1, hy, hz, a.is2d) + ((z >> 1) * dy + (y >> 1)) * 16;
+        double v[33];
+#pragma unroll
+        for (int x = 0; x < 33; ++x)
+          v[x] = (x & 1) ? r1[x >> 1] : r0[x >> 1];
+        ilift33(v);
+        double* dst = rq.is_output ? sm.u.out.v[warp][lane] : nullptr;
+#pragma unroll
+        for (int x = 0; x < 33; ++x)
+        {
+          if (rq.is_output)
+            dst[x] = v[x];
+          else
+            ((x & 1) ? r1 : r0)[x >> 1] = v[x];
+        }
+      }
+      if (rq.is_output)
+      {
+        // the warp's rows, lanes along x
+        sm.u.out.base[warp][lane] = obase;
+        __syncwarp();
+        const int n0 = br.dims[0];
+        for (int r = 0; r < 32; ++r)
+        {
+          const long long ob = sm.u.out.base[warp][r];
+          if (ob < 0 || lane >= n0)
+            continue;
+          const long long di = ob + (long long)lane * br.dst_strd[0];
+          const double val = sm.u.out.v[warp][r][br.src_from[0] + lane * br.src_strd[0]];
           if (a.out_f32)
             ((float*)rq.out)[di] = __double2float_rn(val);
           else
             ((double*)rq.out)[di] = val;
         }
+        __syncwarp();
       }
-      else
-      {
-        double* dst = K + (size_t)z0 * 33 * 33;
-        for (int i = tid; i < gz * 33 * 33; i += kThreads)
-          dst[i] = S[i];
-      }
-      __syncthreads();
-      DEC_PHASE(5)
     }
+    __syncthreads();
+    DEC_PHASE(5)
   }
   DEC_PHASE_FLUSH
 }

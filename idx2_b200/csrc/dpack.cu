@@ -66,93 +66,155 @@ __device__ __forceinline__ void put_varbyte(uint32_t* img, unsigned long long p,
 }
 
 // ---------------------------------------------------------------------------
-// per segment: key totals, first / last brick, and the event and rank of each key's entry
+// key totals, over every event at once (a warp per event), then per segment the entry ranks
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPackThreads) k_pack_keys(const dpack_args a)
+__global__ void __launch_bounds__(kPackThreads) k_pack_init(const dpack_args a)
 {
-  __shared__ int s_kmin, s_kmax, s_ev;
-  __shared__ unsigned s_n[kSegKeys], s_szb[kSegKeys], s_rank[kSegKeys];
-  __shared__ int s_first[kSegKeys], s_last[kSegKeys];
-  __shared__ unsigned long long s_db[kSegKeys];
-  __shared__ int s_fb[kKeyWindow];  // first block covering each key of the entry event
+  const size_t n = (size_t)a.nseg * kSegKeys;
+  for (size_t i = (size_t)blockIdx.x * kPackThreads + threadIdx.x; i < n; i += (size_t)gridDim.x * kPackThreads)
+  {
+    dpack_acc z;
+    z.n = 0;
+    z.szb = 0;
+    z.first = kNoEvent;
+    z.last = -1;
+    z.db = 0;
+    a.acc[i] = z;
+    if (i < (size_t)a.nseg)
+    {
+      a.seg_kmin[i] = 0x7fffffff;
+      a.seg_kmax[i] = -0x7fffffff;
+    }
+  }
+}
+
+// Per event: its region's key window, the byte offsets of its key streams (an exclusive scan
+// of the per-key sizes into kb), and its segment's key range.
+__global__ void __launch_bounds__(kPackThreads) k_pack_events(const dpack_args a)
+{
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * kPackThreads + (int)threadIdx.x) >> 5; i < a.nev; i += (gridDim.x * kPackThreads) >> 5)
+  {
+    const dpack_event& e = a.evs[i];
+    const dpack_segment& S = a.segs[e.seg];
+    const region_dev r = region_of(a, S, e);
+    unsigned long long base = 0;
+    if (lane == 0)
+    {
+      a.ev_region[i] = (unsigned long long)(size_t)(r.exps) - 8ull;
+      a.ev_kmin[i] = r.kmin;
+      a.ev_nkeys[i] = r.nkeys;
+      if (r.nkeys > 0)
+      {
+        atomicMin(&a.seg_kmin[e.seg], r.kmin);
+        atomicMax(&a.seg_kmax[e.seg], r.kmin + r.nkeys - 1);
+        base = atomicAdd(a.cursor, (unsigned long long)r.nkeys);
+        if (base + (unsigned long long)r.nkeys > a.kb_cap)
+        {
+          atomicOr(a.error, 2);
+          base = ~0ull;
+        }
+      }
+      a.ev_kb[i] = base;
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (r.nkeys == 0 || base == ~0ull)
+      continue;
+    unsigned long long carry = 0;
+    for (int j0 = 0; j0 < r.nkeys; j0 += 32)
+    {
+      const int j = j0 + lane;
+      const uint32_t sz = j < r.nkeys ? r.sizes[j] : 0u;
+      unsigned long long inc = sz;
+      for (int o = 1; o < 32; o <<= 1)
+      {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o)
+          inc += y;
+      }
+      if (j < r.nkeys)
+        a.kb[base + (unsigned long long)j] = (uint32_t)(carry + inc - sz);
+      carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+  }
+}
+
+// Per event and key with bytes: the key's totals in its segment (order-free atomics).
+__global__ void __launch_bounds__(kPackThreads) k_pack_totals(const dpack_args a)
+{
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * kPackThreads + (int)threadIdx.x) >> 5; i < a.nev; i += (gridDim.x * kPackThreads) >> 5)
+  {
+    const int nkeys = a.ev_nkeys[i];
+    if (nkeys <= 0)
+      continue;
+    const dpack_event& e = a.evs[i];
+    const dpack_segment& S = a.segs[e.seg];
+    const int K0 = a.seg_kmin[e.seg];
+    if (a.seg_kmax[e.seg] - K0 + 1 > kSegKeys)
+    {
+      if (lane == 0)
+        atomicOr(a.error, 1);
+      continue;
+    }
+    const int kmin = a.ev_kmin[i];
+    const uint32_t* sizes = reinterpret_cast<const uint32_t*>(
+      (size_t)a.ev_region[i] + 8 + (((size_t)S.nexps * 2 + 3) & ~(size_t)3));
+    dpack_acc* acc = a.acc + (size_t)e.seg * kSegKeys;
+    const int li = i - S.ev0;
+    for (int j = lane; j < nkeys; j += 32)
+    {
+      const uint32_t sz = sizes[j];
+      if (!sz)
+        continue;
+      dpack_acc* t = acc + (kmin + j - K0);
+      atomicAdd(&t->n, 1u);
+      atomicAdd(&t->szb, (unsigned)vb_len(sz));
+      atomicAdd(&t->db, (unsigned long long)sz);
+      atomicMin(&t->first, li);
+      atomicMax(&t->last, li);
+    }
+  }
+}
+
+// Per segment: the entry rank of each key (its place in the first-touch order of keys of its
+// entry event: blocks in Morton order, each block's coded planes top-down, i.e. keys by first
+// covering block, then descending), and the key records.
+__global__ void __launch_bounds__(kPackThreads) k_pack_ranks(const dpack_args a)
+{
+  __shared__ int s_ev;
+  __shared__ unsigned s_rank[kSegKeys];
+  __shared__ int s_first[kSegKeys];
   __shared__ uint8_t s_done[kSegKeys];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ int s_fb[kKeyWindow];  // first block covering each key of the entry event
+  const int tid = threadIdx.x;
   for (int si = blockIdx.x; si < a.nseg; si += gridDim.x)
   {
     const dpack_segment& S = a.segs[si];
-    if (tid == 0)
+    const int K0 = a.seg_kmin[si];
+    const bool any = a.seg_kmax[si] >= K0;
+    if (any && a.seg_kmax[si] - K0 + 1 > kSegKeys)
     {
-      s_kmin = 0x7fffffff;
-      s_kmax = -0x7fffffff;
+      if (tid == 0)
+        a.seg_kmin[si] = 0x7fffffff;  // (the error flag is set: the host packs)
+      continue;
     }
+    const int nk = any ? a.seg_kmax[si] - K0 + 1 : 0;
+    const dpack_acc* acc = a.acc + (size_t)si * kSegKeys;
     for (int k = tid; k < kSegKeys; k += kPackThreads)
     {
-      s_n[k] = 0;
-      s_szb[k] = 0;
       s_rank[k] = 0;
-      s_first[k] = kNoEvent;
-      s_last[k] = -1;
-      s_db[k] = 0;
+      s_first[k] = k < nk && acc[k].n ? acc[k].first : kNoEvent;
       s_done[k] = 0;
     }
     __syncthreads();
-    // the segment's key range
-    for (int i = S.ev0 + tid; i < S.ev1; i += kPackThreads)
-    {
-      const region_dev r = region_of(a, S, a.evs[i]);
-      if (r.nkeys > 0)
-      {
-        atomicMin(&s_kmin, r.kmin);
-        atomicMax(&s_kmax, r.kmin + r.nkeys - 1);
-      }
-    }
-    __syncthreads();
-    const int K0 = s_kmin;
-    const bool any = s_kmax >= s_kmin;
-    if (tid == 0)
-      a.seg_kmin[si] = any ? K0 : 0x7fffffff;
-    if (any && s_kmax - s_kmin + 1 > kSegKeys)
-    {
-      if (tid == 0)
-      {
-        atomicOr(a.error, 1);
-        a.seg_kmin[si] = 0x7fffffff;
-      }
-      for (int k = tid; k < kSegKeys; k += kPackThreads)
-        a.keys[(size_t)si * kSegKeys + k].n = 0;
-      __syncthreads();
-      continue;
-    }
-    // per key: bricks, bytes, varbyte sizes, first and last event (order-free)
-    for (int i = S.ev0 + warp; i < S.ev1; i += kPackWarps)
-    {
-      const region_dev r = region_of(a, S, a.evs[i]);
-      for (int j = lane; j < r.nkeys; j += 32)
-      {
-        const uint32_t sz = r.sizes[j];
-        if (!sz)
-          continue;
-        const int k = r.kmin + j - K0;
-        atomicAdd(&s_n[k], 1u);
-        atomicAdd(&s_szb[k], (unsigned)vb_len(sz));
-        atomicAdd(&s_db[k], (unsigned long long)sz);
-        atomicMin(&s_first[k], i - S.ev0);
-        atomicMax(&s_last[k], i - S.ev0);
-      }
-    }
-    __syncthreads();
-    // entry ranks: a key enters at its first event with bytes, at its place in that event's
-    // first-touch order of keys (blocks in Morton order, each block's coded planes top-down:
-    // keys by first covering block, then descending); the entry events are taken one at a
-    // time, earliest first
-    const int nk = any ? s_kmax - K0 + 1 : 0;
     for (;;)
     {
       if (tid == 0)
         s_ev = kNoEvent;
       __syncthreads();
       for (int k = tid; k < nk; k += kPackThreads)
-        if (s_n[k] && !s_done[k])
+        if (s_first[k] != kNoEvent && !s_done[k])
           atomicMin(&s_ev, s_first[k]);
       __syncthreads();
       const int ev = s_ev;
@@ -180,7 +242,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_keys(const dpack_args a)
       __syncthreads();
       for (int k = tid; k < nk; k += kPackThreads)
       {
-        if (!s_n[k] || s_done[k] || s_first[k] != ev)
+        if (s_first[k] != ev || s_done[k])
           continue;
         const int jk = K0 + k - r.kmin;  // the key's index in the event's window
         const int fk = jk >= 0 && jk < kKeyWindow ? s_fb[jk] : 0x7fffffff;
@@ -199,16 +261,17 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_keys(const dpack_args a)
     for (int k = tid; k < kSegKeys; k += kPackThreads)
     {
       dpack_key out;
-      out.n = k < nk ? s_n[k] : 0;
-      out.sizes_bytes = s_szb[k];
-      out.data_bytes = s_db[k];
+      const dpack_acc t = acc[k];
+      out.n = k < nk ? t.n : 0;
+      out.sizes_bytes = t.szb;
+      out.data_bytes = t.db;
       out.enter_rank = s_rank[k];
       if (out.n)
       {
-        const dpack_event& e0 = a.evs[S.ev0 + s_first[k]];
+        const dpack_event& e0 = a.evs[S.ev0 + t.first];
         out.enter_event = e0.gevent;
         out.first_brick = e0.linear;
-        out.last_brick = a.evs[S.ev0 + s_last[k]].linear;
+        out.last_brick = a.evs[S.ev0 + t.last].linear;
       }
       else
       {
@@ -282,19 +345,18 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_write(const dpack_args a)
         unsigned long long linear = 0;
         if (i < S.ev1)
         {
-          const dpack_event& e = a.evs[i];
-          const region_dev r = region_of(a, S, e);
-          const int j = key - r.kmin;
-          if (j >= 0 && j < r.nkeys)
+          const int kmin = a.ev_kmin[i], nkeys = a.ev_nkeys[i];
+          const int j = key - kmin;
+          if (j >= 0 && j < nkeys)
           {
-            sz = r.sizes[j];
+            const uint8_t* reg = reinterpret_cast<const uint8_t*>((size_t)a.ev_region[i]);
+            const size_t eb = ((size_t)S.nexps * 2 + 3) & ~(size_t)3;
+            sz = reinterpret_cast<const uint32_t*>(reg + 8 + eb)[j];
             if (sz)
             {
-              unsigned long long kb = 0;  // the key's stream after the lower keys' streams
-              for (int t = 0; t < j; ++t)
-                kb += r.sizes[t];
-              src = r.bytes + kb;
-              linear = e.linear;
+              // the key's stream after the lower keys' streams
+              src = reg + 8 + eb + (size_t)nkeys * 4 + a.kb[a.ev_kb[i] + (unsigned long long)j];
+              linear = a.evs[i].linear;
             }
           }
         }
@@ -358,7 +420,14 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_write(const dpack_args a)
 
 void dpack_launch_keys(const dpack_args& a, int grid, cudaStream_t st)
 {
-  k_pack_keys<<<grid, kPackThreads, 0, st>>>(a);
+  // a warp per event for the per-event passes
+  const int eg = (int)((a.nev + kPackWarps - 1) / kPackWarps);
+  const int egrid = eg < 65535 ? (eg > 0 ? eg : 1) : 65535;
+  const int igrid = (int)(((size_t)a.nseg * kSegKeys + kPackThreads - 1) / kPackThreads);
+  k_pack_init<<<igrid < 4096 ? igrid : 4096, kPackThreads, 0, st>>>(a);
+  k_pack_events<<<egrid, kPackThreads, 0, st>>>(a);
+  k_pack_totals<<<egrid, kPackThreads, 0, st>>>(a);
+  k_pack_ranks<<<grid, kPackThreads, 0, st>>>(a);
 }
 
 void dpack_launch_write(const dpack_args& a, int grid, cudaStream_t st)

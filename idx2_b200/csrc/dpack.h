@@ -69,6 +69,8 @@ struct dpack_event
   unsigned long long linear;  // linear brick index on the level
   unsigned gevent;            // index in the encode's event order
   int brick;                  // brick index in the level's list (region offset lookup)
+  int seg;                    // its segment
+  int pad_;
 };
 
 // per (segment, key slot); n = 0: the key has no bytes in the segment

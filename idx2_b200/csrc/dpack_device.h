@@ -17,11 +17,30 @@ struct device_level_stream
   std::vector<int> nexps;  // per subband
 };
 
+// per (segment, key slot): running totals of the key's pairs (order-free atomics)
+struct dpack_acc
+{
+  unsigned n, szb;
+  int first, last;  // first / last event of the segment with bytes for the key
+  unsigned long long db;
+};
+
 struct dpack_args
 {
   const dpack_segment* segs;
   int nseg;
   const dpack_event* evs;
+  int nev;
+  // per event: its region, key window and the start of its key offsets in kb
+  unsigned long long* ev_region;  // byte address of the region
+  int* ev_kmin;
+  int* ev_nkeys;
+  unsigned long long* ev_kb;
+  uint32_t* kb;                   // per event and key: the key stream's byte offset in the region's streams
+  unsigned long long kb_cap;      // entries of kb
+  unsigned long long* cursor;     // kb entries taken
+  int* seg_kmax;                  // [nseg]
+  dpack_acc* acc;                 // [nseg][kSegKeys]
   const uint8_t* streams[16];
   const unsigned long long* offsets[16];
   int etol, end_bp, bpc, exp_bytes;  // exp_bytes: 1 (float32) or 2 (float64)
@@ -30,7 +49,7 @@ struct dpack_args
   const unsigned long long* chunk_off;  // [nseg][kSegKeys]: first byte of the chunk in image
   uint32_t* image;                   // zeroed
   uint8_t* exps;                     // raw exponents of every segment
-  int* error;                        // 1: a segment spans more than kSegKeys keys
+  int* error;                        // 1: a segment spans more than kSegKeys keys, 2: kb too small
 };
 
 void dpack_launch_keys(const dpack_args& a, int grid, cudaStream_t st);

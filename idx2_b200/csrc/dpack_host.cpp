@@ -38,11 +38,34 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   cudaMemcpyAsync(d_segs, P.segs.data(), sizeof(dpack_segment) * (size_t)nseg, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(d_evs, P.evs.data(), sizeof(dpack_event) * P.evs.size(), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(d_err, 0, 16, st);
+  const size_t nev = P.evs.size();
+  const unsigned long long kb_cap = (unsigned long long)nev * kKeyWindow;
+  unsigned long long* d_evreg = (unsigned long long*)ctx->ws("dpack.evreg", 8 * nev);
+  int* d_evkmin = (int*)ctx->ws("dpack.evkmin", 4 * nev);
+  int* d_evnkeys = (int*)ctx->ws("dpack.evnkeys", 4 * nev);
+  unsigned long long* d_evkb = (unsigned long long*)ctx->ws("dpack.evkb", 8 * nev);
+  uint32_t* d_kb = (uint32_t*)ctx->ws("dpack.kb", 4 * (size_t)kb_cap);
+  unsigned long long* d_cursor = (unsigned long long*)ctx->ws("dpack.cursor", 16);
+  int* d_kmax = (int*)ctx->ws("dpack.kmax", 4 * (size_t)nseg);
+  dpack_acc* d_acc = (dpack_acc*)ctx->ws("dpack.acc", sizeof(dpack_acc) * (size_t)nseg * kSegKeys);
+  if (!d_evreg || !d_evkmin || !d_evnkeys || !d_evkb || !d_kb || !d_cursor || !d_kmax || !d_acc)
+    return OutOfMemory;
+  cudaMemsetAsync(d_cursor, 0, 16, st);
   dpack_args a;
   memset(&a, 0, sizeof a);
   a.segs = d_segs;
   a.nseg = nseg;
   a.evs = d_evs;
+  a.nev = (int)nev;
+  a.ev_region = d_evreg;
+  a.ev_kmin = d_evkmin;
+  a.ev_nkeys = d_evnkeys;
+  a.ev_kb = d_evkb;
+  a.kb = d_kb;
+  a.kb_cap = kb_cap;
+  a.cursor = d_cursor;
+  a.seg_kmax = d_kmax;
+  a.acc = d_acc;
   for (size_t l = 0; l < levels.size(); ++l)
   {
     a.streams[l] = levels[l].stream;
@@ -57,11 +80,12 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   a.chunk_off = d_coff;
   a.exps = d_exps;
   a.error = d_err;
-  // k_pack_keys: a CTA per segment; k_pack_write: kSegKeys / 8 CTAs per segment
+  // the key pass (a warp per event, then a CTA per segment for the ranks); k_pack_write:
+  // kSegKeys / 8 CTAs per segment
   const int grid = nseg < 4 * ctx->num_sms ? nseg : 4 * ctx->num_sms;
   const int wgrid = nseg < 2048 ? nseg : 2048;
   dpack_launch_keys(a, grid, st);
-  ctx->launches += 1;
+  ctx->launches += 4;
   std::vector<dpack_key> keys((size_t)nseg * kSegKeys);
   std::vector<int> kmin((size_t)nseg);
   int err = 0;
@@ -91,15 +115,23 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   a.image = d_img;
   dpack_launch_write(a, wgrid, st);
   ctx->launches += 1;
-  if (L.total)
-    cudaMemcpyAsync(h_img, d_img, (size_t)L.total, cudaMemcpyDeviceToHost, st);
+  // the raw exponents first: their compression (and the file tails) run on the host while
+  // the image comes back
   if (P.exp_total)
     cudaMemcpyAsync(h_exps, d_exps, (size_t)P.exp_total, cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess)
+  cudaEvent_t ex = ctx->ev(0);
+  if (!ex || cudaEventRecord(ex, st) != cudaSuccess)
+    return CudaError;
+  if (L.total)
+    cudaMemcpyAsync(h_img, d_img, (size_t)L.total, cudaMemcpyDeviceToHost, st);
+  if (cudaEventSynchronize(ex) != cudaSuccess)
     return CudaError;
   tt.lap("dpack.write");
   e = dpack_finish(f, P, L, h_img, h_exps, out);
   tt.lap("dpack.finish");
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return CudaError;
+  tt.lap("dpack.image");
   return e;
 }
 

@@ -152,7 +152,7 @@ int dpack_make_plan(const dataset_format& f, const encode_plan& plan, const std:
         segs.push_back(s);
         seg_chunk.push_back(c);
       }
-      evs.push_back(dpack_event{ lin, e, ev.brick });
+      evs.push_back(dpack_event{ lin, e, ev.brick, (int)segs.size() - 1, 0 });
       segs.back().ev1 = (int)evs.size();
     }
     if (segs.size() > P->group_segs[gi].first)
@@ -350,8 +350,15 @@ int dpack_finish(const dataset_format& f, const dpack_plan& P, const dpack_layou
   for (auto& kv : files)
   {
     auto sp = L.file_span.find(kv.first);
-    if (sp != L.file_span.end() && sp->second.second)
-      kv.second.append_ref(h_img + sp->second.first, (size_t)sp->second.second);
+    if (sp == L.file_span.end())
+      continue;
+    // in pieces of at most 16 MB, so that the writer's threads share a large file
+    constexpr unsigned long long kPiece = 16ull << 20;
+    for (unsigned long long o = 0; o < sp->second.second; o += kPiece)
+    {
+      const unsigned long long n = sp->second.second - o < kPiece ? sp->second.second - o : kPiece;
+      kv.second.append_ref(h_img + sp->second.first + o, (size_t)n);
+    }
   }
   for (auto& kv : files)
   {
