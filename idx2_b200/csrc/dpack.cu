@@ -139,41 +139,76 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_events(const dpack_args a
   }
 }
 
-// Per event and key with bytes: the key's totals in its segment (order-free atomics).
+// Per sub-range of a segment (a CTA each): the keys' totals over its events in shared memory
+// (order-free), written per sub-range and added to the segment's totals.
 __global__ void __launch_bounds__(kPackThreads) k_pack_totals(const dpack_args a)
 {
-  const int lane = threadIdx.x & 31;
-  for (int i = (blockIdx.x * kPackThreads + (int)threadIdx.x) >> 5; i < a.nev; i += (gridDim.x * kPackThreads) >> 5)
+  __shared__ unsigned s_n[kSegKeys], s_szb[kSegKeys];
+  __shared__ int s_first[kSegKeys], s_last[kSegKeys];
+  __shared__ unsigned long long s_db[kSegKeys];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int ci = blockIdx.x; ci < a.nsub; ci += gridDim.x)
   {
-    const int nkeys = a.ev_nkeys[i];
-    if (nkeys <= 0)
-      continue;
-    const dpack_event& e = a.evs[i];
-    const dpack_segment& S = a.segs[e.seg];
-    const int K0 = a.seg_kmin[e.seg];
-    if (a.seg_kmax[e.seg] - K0 + 1 > kSegKeys)
+    const int4 sr = a.subs[ci];
+    const int seg = sr.x;
+    const dpack_segment& S = a.segs[seg];
+    const int K0 = a.seg_kmin[seg];
+    if (a.seg_kmax[seg] < K0)
+      continue;  // no keys in the segment
+    if (a.seg_kmax[seg] - K0 + 1 > kSegKeys)
     {
-      if (lane == 0)
+      if (tid == 0)
         atomicOr(a.error, 1);
       continue;
     }
-    const int kmin = a.ev_kmin[i];
-    const uint32_t* sizes = reinterpret_cast<const uint32_t*>(
-      (size_t)a.ev_region[i] + 8 + (((size_t)S.nexps * 2 + 3) & ~(size_t)3));
-    dpack_acc* acc = a.acc + (size_t)e.seg * kSegKeys;
-    const int li = i - S.ev0;
-    for (int j = lane; j < nkeys; j += 32)
+    for (int k = tid; k < kSegKeys; k += kPackThreads)
     {
-      const uint32_t sz = sizes[j];
-      if (!sz)
-        continue;
-      dpack_acc* t = acc + (kmin + j - K0);
-      atomicAdd(&t->n, 1u);
-      atomicAdd(&t->szb, (unsigned)vb_len(sz));
-      atomicAdd(&t->db, (unsigned long long)sz);
-      atomicMin(&t->first, li);
-      atomicMax(&t->last, li);
+      s_n[k] = 0;
+      s_szb[k] = 0;
+      s_db[k] = 0;
+      s_first[k] = kNoEvent;
+      s_last[k] = -1;
     }
+    __syncthreads();
+    const size_t eb = ((size_t)S.nexps * 2 + 3) & ~(size_t)3;
+    for (int i = sr.y + warp; i < sr.z; i += kPackWarps)
+    {
+      const int nkeys = a.ev_nkeys[i];
+      if (nkeys <= 0)
+        continue;
+      const int kmin = a.ev_kmin[i];
+      const uint32_t* sizes = reinterpret_cast<const uint32_t*>((size_t)a.ev_region[i] + 8 + eb);
+      const int li = i - S.ev0;
+      for (int j = lane; j < nkeys; j += 32)
+      {
+        const uint32_t sz = sizes[j];
+        if (!sz)
+          continue;
+        const int k = kmin + j - K0;
+        atomicAdd(&s_n[k], 1u);
+        atomicAdd(&s_szb[k], (unsigned)vb_len(sz));
+        atomicAdd(&s_db[k], (unsigned long long)sz);
+        atomicMin(&s_first[k], li);
+        atomicMax(&s_last[k], li);
+      }
+    }
+    __syncthreads();
+    const int nk = a.seg_kmax[seg] - K0 + 1;
+    dpack_acc* acc = a.acc + (size_t)seg * kSegKeys;
+    dpack_sub* sub = a.sub_acc + ((size_t)a.seg_sub0[seg] + (size_t)sr.w) * kSegKeys;
+    for (int k = tid; k < nk; k += kPackThreads)
+    {
+      sub[k].vb = s_szb[k];
+      sub[k].data = s_db[k];
+      if (!s_n[k])
+        continue;
+      atomicAdd(&acc[k].n, s_n[k]);
+      atomicAdd(&acc[k].szb, s_szb[k]);
+      atomicAdd(&acc[k].db, s_db[k]);
+      atomicMin(&acc[k].first, s_first[k]);
+      atomicMax(&acc[k].last, s_last[k]);
+    }
+    __syncthreads();
   }
 }
 
@@ -279,6 +314,21 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_ranks(const dpack_args a)
         out.first_brick = out.last_brick = 0;
       }
       a.keys[(size_t)si * kSegKeys + k] = out;
+      // the key's offsets at the start of each sub-range: exclusive prefixes over them
+      if (out.n)
+      {
+        const int ns = (S.ev1 - S.ev0 + kPackSub - 1) / kPackSub;
+        dpack_sub* sub = a.sub_acc + (size_t)a.seg_sub0[si] * kSegKeys + k;
+        unsigned long long vb = 0, data = 0;
+        for (int q = 0; q < ns; ++q)
+        {
+          const dpack_sub t = sub[(size_t)q * kSegKeys];
+          sub[(size_t)q * kSegKeys].vb = vb;
+          sub[(size_t)q * kSegKeys].data = data;
+          vb += t.vb;
+          data += t.data;
+        }
+      }
     }
     __syncthreads();
   }
@@ -290,14 +340,15 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_ranks(const dpack_args a)
 __global__ void __launch_bounds__(kPackThreads) k_pack_write(const dpack_args a)
 {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  // CTA (x, y): segment x, keys y * kPackWarps .. (y + 1) * kPackWarps - 1 (a warp each)
-  for (int si = blockIdx.x; si < a.nseg; si += gridDim.x)
+  // a CTA per sub-range of a segment, a warp per key
+  for (int ci = blockIdx.x; ci < a.nsub; ci += gridDim.x)
   {
+    const int4 sr = a.subs[ci];
+    const int si = sr.x;
     const dpack_segment& S = a.segs[si];
     // raw exponents (Core/idx2Encode.cpp:41 EncodeBrickSubbandExponents): EMax + 127 as a
-    // byte (float32) or EMax + 1023 as a little-endian 16-bit word (float64), events in order,
-    // spread over the segment's CTAs
-    for (int i = S.ev0 + (int)blockIdx.y * kPackWarps + warp; i < S.ev1; i += (int)gridDim.y * kPackWarps)
+    // byte (float32) or EMax + 1023 as a little-endian 16-bit word (float64), events in order
+    for (int i = sr.y + warp; i < sr.z; i += kPackWarps)
     {
       const region_dev r = region_of(a, S, a.evs[i]);
       uint8_t* dst = a.exps + S.exp_off + (size_t)(i - S.ev0) * (size_t)S.nexps * (size_t)a.exp_bytes;
@@ -317,7 +368,7 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_write(const dpack_args a)
     const int K0 = a.seg_kmin[si];
     if (K0 == 0x7fffffff)
       continue;
-    for (int k = (int)blockIdx.y * kPackWarps + warp; k < kSegKeys; k += (int)gridDim.y * kPackWarps)
+    for (int k = warp; k < kSegKeys; k += kPackWarps)
     {
       const dpack_key rec = a.keys[(size_t)si * kSegKeys + k];
       if (!rec.n)
@@ -331,19 +382,21 @@ __global__ void __launch_bounds__(kPackThreads) k_pack_write(const dpack_args a)
       const unsigned long long dbits = 8ull * (unsigned long long)vbf + (rec.last_brick - rec.first_brick);
       const unsigned long long s0 = d0 + (dbits + 7) / 8;
       const unsigned long long x0 = s0 + rec.sizes_bytes;
-      if (lane == 0)
+      if (lane == 0 && sr.w == 0)
       {
         put_varbyte(a.image, base, rec.n);
         put_varbyte(a.image, d0, rec.first_brick);
       }
-      unsigned long long vb_carry = 0, data_carry = 0;
-      for (int i0 = S.ev0; i0 < S.ev1; i0 += 32)
+      // the key's varbyte-size and data offsets at the start of the sub-range
+      const dpack_sub c0 = a.sub_acc[((size_t)a.seg_sub0[si] + (size_t)sr.w) * kSegKeys + k];
+      unsigned long long vb_carry = c0.vb, data_carry = c0.data;
+      for (int i0 = sr.y; i0 < sr.z; i0 += 32)
       {
         const int i = i0 + lane;
         uint32_t sz = 0;
         const uint8_t* src = nullptr;
         unsigned long long linear = 0;
-        if (i < S.ev1)
+        if (i < sr.z)
         {
           const int kmin = a.ev_kmin[i], nkeys = a.ev_nkeys[i];
           const int j = key - kmin;
@@ -426,13 +479,16 @@ void dpack_launch_keys(const dpack_args& a, int grid, cudaStream_t st)
   const int igrid = (int)(((size_t)a.nseg * kSegKeys + kPackThreads - 1) / kPackThreads);
   k_pack_init<<<igrid < 4096 ? igrid : 4096, kPackThreads, 0, st>>>(a);
   k_pack_events<<<egrid, kPackThreads, 0, st>>>(a);
-  k_pack_totals<<<egrid, kPackThreads, 0, st>>>(a);
+  const int sgrid = a.nsub < 65535 ? a.nsub : 65535;
+  k_pack_totals<<<sgrid > 0 ? sgrid : 1, kPackThreads, 0, st>>>(a);
   k_pack_ranks<<<grid, kPackThreads, 0, st>>>(a);
 }
 
 void dpack_launch_write(const dpack_args& a, int grid, cudaStream_t st)
 {
-  k_pack_write<<<dim3((unsigned)grid, kSegKeys / kPackWarps), kPackThreads, 0, st>>>(a);
+  (void)grid;
+  const int sgrid = a.nsub < 65535 ? a.nsub : 65535;
+  k_pack_write<<<sgrid > 0 ? sgrid : 1, kPackThreads, 0, st>>>(a);
 }
 
 } // namespace idx2g

@@ -11,9 +11,11 @@
 // channel enters a chunk at the first brick of the range with bytes for it (at its place in
 // that brick's first-touch order of keys), which writes the data it held, and what it holds
 // at the end is written by FlushChunks in channel-key order. So:
-//   k_pack_keys (a CTA per (level, subband, chunk) segment): per key of the segment, its
-//     brick count, first / last brick, byte and varbyte-size totals (shared-memory atomics,
-//     order-free), and the event and touch rank at which it enters the chunk;
+//   the key pass (dpack.cu), over every event at once with a warp each: its region's key
+//     window and key-stream offsets, its segment's key range, then per key of the
+//     (level, subband, chunk) segment its brick count, first / last brick, byte and
+//     varbyte-size totals (atomics, order-free); then a CTA per segment finds the event and
+//     touch rank at which each key enters the chunk;
 //   the host orders the chunks by their flush stamps, assigns file offsets, builds the file
 //     tails and the statistics (no brick data touched);
 //   k_pack_write (a CTA per segment, a warp per chunk): exclusive scans over the segment's
@@ -104,7 +106,7 @@ struct dpack_layout
   unsigned long long total = 0;
   std::map<std::string, std::pair<unsigned long long, unsigned long long>> file_span;
 };
-// From k_pack_keys' output: chunk flush stamps, file order and offsets; out receives the
+// From the key pass's output: chunk flush stamps, file order and offsets; out receives the
 // files' chunk tables (sizes, addresses) and the bit-plane statistics.
 int dpack_make_layout(const dataset_format& f, const dpack_plan& P, const std::vector<dpack_key>& keys,
                       const std::vector<int>& kmin, dpack_layout* L, packed_dataset* out);

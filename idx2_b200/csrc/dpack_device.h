@@ -25,6 +25,15 @@ struct dpack_acc
   unsigned long long db;
 };
 
+constexpr int kPackSub = 256;  // events of a sub-range
+
+// per (segment, key, sub-range): the key's varbyte-size and data bytes in the sub-range, then
+// (after the ranks pass) those of the segment's earlier sub-ranges
+struct dpack_sub
+{
+  unsigned long long vb, data;
+};
+
 struct dpack_args
 {
   const dpack_segment* segs;
@@ -41,6 +50,11 @@ struct dpack_args
   unsigned long long* cursor;     // kb entries taken
   int* seg_kmax;                  // [nseg]
   dpack_acc* acc;                 // [nseg][kSegKeys]
+  // sub-ranges of kPackSub events of a segment (a CTA each in the totals and write passes)
+  const int4* subs;               // (segment, first event, end event, index of the sub-range in its segment)
+  int nsub;
+  const int* seg_sub0;            // [nseg]: the segment's first entry of sub_acc (x kSegKeys)
+  dpack_sub* sub_acc;             // per (segment, key, sub-range): totals, then exclusive prefixes
   const uint8_t* streams[16];
   const unsigned long long* offsets[16];
   int etol, end_bp, bpc, exp_bytes;  // exp_bytes: 1 (float32) or 2 (float64)

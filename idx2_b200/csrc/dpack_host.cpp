@@ -1,9 +1,10 @@
-// Device packer, device side (dpack_device.h): the launches of k_pack_keys and k_pack_write
+// Device packer, device side (dpack_device.h): the launches of the key pass and k_pack_write
 // between the host stages of dpack_plan.cpp, and the encode path that uses them.
 #include "dpack_device.h"
 
 #include "trace.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <thread>
@@ -48,8 +49,24 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   unsigned long long* d_cursor = (unsigned long long*)ctx->ws("dpack.cursor", 16);
   int* d_kmax = (int*)ctx->ws("dpack.kmax", 4 * (size_t)nseg);
   dpack_acc* d_acc = (dpack_acc*)ctx->ws("dpack.acc", sizeof(dpack_acc) * (size_t)nseg * kSegKeys);
-  if (!d_evreg || !d_evkmin || !d_evnkeys || !d_evkb || !d_kb || !d_cursor || !d_kmax || !d_acc)
+  // sub-ranges of kPackSub events per segment
+  std::vector<int4> subs;
+  std::vector<int> seg_sub0((size_t)nseg);
+  for (int si = 0; si < nseg; ++si)
+  {
+    seg_sub0[(size_t)si] = (int)subs.size();
+    int q = 0;
+    for (int i = P.segs[(size_t)si].ev0; i < P.segs[(size_t)si].ev1; i += kPackSub, ++q)
+      subs.push_back(make_int4(si, i, std::min(i + kPackSub, P.segs[(size_t)si].ev1), q));
+  }
+  int4* d_subs = (int4*)ctx->ws("dpack.subs", sizeof(int4) * subs.size());
+  int* d_sub0 = (int*)ctx->ws("dpack.sub0", 4 * (size_t)nseg);
+  dpack_sub* d_subacc = (dpack_sub*)ctx->ws("dpack.subacc", sizeof(dpack_sub) * subs.size() * kSegKeys);
+  if (!d_evreg || !d_evkmin || !d_evnkeys || !d_evkb || !d_kb || !d_cursor || !d_kmax || !d_acc || !d_subs ||
+      !d_sub0 || !d_subacc)
     return OutOfMemory;
+  cudaMemcpyAsync(d_subs, subs.data(), sizeof(int4) * subs.size(), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_sub0, seg_sub0.data(), 4 * (size_t)nseg, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(d_cursor, 0, 16, st);
   dpack_args a;
   memset(&a, 0, sizeof a);
@@ -66,6 +83,10 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   a.cursor = d_cursor;
   a.seg_kmax = d_kmax;
   a.acc = d_acc;
+  a.subs = d_subs;
+  a.nsub = (int)subs.size();
+  a.seg_sub0 = d_sub0;
+  a.sub_acc = d_subacc;
   for (size_t l = 0; l < levels.size(); ++l)
   {
     a.streams[l] = levels[l].stream;
@@ -80,8 +101,8 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   a.chunk_off = d_coff;
   a.exps = d_exps;
   a.error = d_err;
-  // the key pass (a warp per event, then a CTA per segment for the ranks); k_pack_write:
-  // kSegKeys / 8 CTAs per segment
+  // the key pass (a warp per event, a CTA per sub-range for the totals, a CTA per segment for
+  // the ranks); k_pack_write: a CTA per sub-range
   const int grid = nseg < 4 * ctx->num_sms ? nseg : 4 * ctx->num_sms;
   const int wgrid = nseg < 2048 ? nseg : 2048;
   dpack_launch_keys(a, grid, st);
