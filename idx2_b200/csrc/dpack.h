@@ -30,6 +30,7 @@
 #include "packer.h"
 
 #include <cstdint>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -46,6 +47,9 @@ struct packed_dataset
   pack_stats stats;
   const uint8_t* image = nullptr;  // pinned host copy of the chunk sections
   std::vector<std::vector<uint8_t>> exps_z;
+  // waits until the bytes [p, p + n) of the image have arrived (set by the device packer,
+  // whose copy of the image runs on while the files are being written)
+  std::function<void(const uint8_t*, size_t)> ready;
 };
 
 // Whether the device packer takes this plan (every (level, subband)'s bricks in chunk order,

@@ -143,16 +143,35 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   cudaEvent_t ex = ctx->ev(0);
   if (!ex || cudaEventRecord(ex, st) != cudaSuccess)
     return CudaError;
-  if (L.total)
-    cudaMemcpyAsync(h_img, d_img, (size_t)L.total, cudaMemcpyDeviceToHost, st);
+  // the image in pieces, each with an event: the file writer starts on the first pieces
+  // while the later ones are still on their way
+  constexpr unsigned long long kCopyPiece = 32ull << 20;
+  const size_t npiece = (size_t)((L.total + kCopyPiece - 1) / kCopyPiece);
+  std::vector<cudaEvent_t> pev(npiece);
+  for (size_t i = 0; i < npiece; ++i)
+  {
+    const unsigned long long o = (unsigned long long)i * kCopyPiece;
+    const unsigned long long n = L.total - o < kCopyPiece ? L.total - o : kCopyPiece;
+    cudaMemcpyAsync(h_img + o, (const uint8_t*)d_img + o, (size_t)n, cudaMemcpyDeviceToHost, st);
+    pev[i] = ctx->ev(1 + i);
+    if (!pev[i] || cudaEventRecord(pev[i], st) != cudaSuccess)
+      return CudaError;
+  }
   if (cudaEventSynchronize(ex) != cudaSuccess)
     return CudaError;
   tt.lap("dpack.write");
   e = dpack_finish(f, P, L, h_img, h_exps, out);
   tt.lap("dpack.finish");
-  if (cudaStreamSynchronize(st) != cudaSuccess)
-    return CudaError;
-  tt.lap("dpack.image");
+  const uint8_t* img = h_img;
+  const unsigned long long total = L.total;
+  out->ready = [pev, img, total](const uint8_t* p, size_t n) {
+    if (p < img || p >= img + total || n == 0)
+      return;
+    const size_t i0 = (size_t)((unsigned long long)(p - img) / kCopyPiece);
+    const size_t i1 = (size_t)(((unsigned long long)(p - img) + n - 1) / kCopyPiece);
+    for (size_t i = i0; i <= i1 && i < pev.size(); ++i)
+      cudaEventSynchronize(pev[i]);
+  };
   return e;
 }
 
@@ -188,6 +207,8 @@ int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_code
   }
   packed_dataset pd;
   e = device_pack(ctx, *f, plan, lv, &pd);
+  if (e && e != kDpackNotApplicable)
+    cudaStreamSynchronize(ctx->stream);  // (no copy left running into the pinned image)
   if (e == kDpackNotApplicable)
   {
     // a segment with more keys than the kernels' window: the regions to the host packer
@@ -206,7 +227,10 @@ int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_code
   if (timing)
     note_level_files(*f, plan, pd.files, timing);
   const double t2 = now();
-  e = write_dataset(f, p, pd.files, pack_stats_text(pd.stats), nullptr, true, timing, &pre, t2 - t1);
+  e = write_dataset(f, p, pd.files, pack_stats_text(pd.stats), nullptr, true, timing, &pre, t2 - t1, &pd.ready);
+  // (every piece of the image has been waited for by now, unless the write failed first)
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && !e)
+    e = CudaError;
   if (timing)
     timing->device_s = t1 - t0;
   return e;

@@ -313,7 +313,8 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
 
 int write_dataset(const dataset_format* f, const params* p, std::map<std::string, file_buffer>& data,
                   const std::string& stats, std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
-                  encode_timing* timing, std::thread* before_write, double pack_s)
+                  encode_timing* timing, std::thread* before_write, double pack_s,
+                  const std::function<void(const uint8_t*, size_t)>* ready)
 {
   stage_timer tt;
   const double t2 = now_s();
@@ -334,7 +335,11 @@ int write_dataset(const dataset_format* f, const params* p, std::map<std::string
     {
       std::vector<uint8_t>& d = (*files)[kv->first];
       d.reserve(kv->second.nbytes);
-      kv->second.for_each_segment([&](const segment& s) { d.insert(d.end(), s.p, s.p + s.n); });
+      kv->second.for_each_segment([&](const segment& s) {
+        if (ready && *ready)
+          (*ready)(s.p, s.n);
+        d.insert(d.end(), s.p, s.p + s.n);
+      });
     }
     (*files)[meta_path] = std::vector<uint8_t>(meta.begin(), meta.end());
   }
@@ -350,7 +355,7 @@ int write_dataset(const dataset_format* f, const params* p, std::map<std::string
     for (auto* kv : list)
       wl.push_back({ kv->first, &kv->second });
     tt.lap("write.meta");
-    e = idx2g::write_files(wl);
+    e = idx2g::write_files(wl, ready);
     if (e)
       return e;
     tt.lap("write.files");

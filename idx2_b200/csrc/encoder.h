@@ -13,6 +13,7 @@
 #include "packer.h"
 
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <thread>
@@ -142,9 +143,11 @@ int pack_dataset(const dataset_format* f, const params* p, const encode_plan& pl
 // The second half of pack_dataset: the metadata file (format text + stats) and the data
 // files from their parts; files / write_files / timing / before_write as pack_dataset.
 struct file_buffer;
+// ready (may be null): waited on before a part's bytes are read (write_files).
 int write_dataset(const dataset_format* f, const params* p, std::map<std::string, file_buffer>& data,
                   const std::string& stats, std::map<std::string, std::vector<uint8_t>>* files, bool write_files,
-                  encode_timing* timing, std::thread* before_write, double pack_s);
+                  encode_timing* timing, std::thread* before_write, double pack_s,
+                  const std::function<void(const uint8_t*, size_t)>* ready = nullptr);
 
 // Bytes of every level's data file into timing->level_file_bytes, when each level has
 // exactly one (else empty).

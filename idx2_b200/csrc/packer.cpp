@@ -197,7 +197,7 @@ void file_buffer::append_run(const segment* s, size_t n, size_t bytes)
   nbytes += bytes;
 }
 
-int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& files)
+int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& files, const ready_fn* ready)
 {
   // Every file is cut into ranges of whole runs of about kRange bytes, copied by a pool of
   // threads. Large files are written through a shared mapping (writes to one file through
@@ -281,6 +281,8 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
           for (size_t k = r.p0; k < r.p1; ++k)
             for (size_t j = 0; j < parts[k].nseg; ++j)
             {
+              if (ready && *ready)
+                (*ready)(parts[k].seg[j].p, parts[k].seg[j].n);
               memcpy(dst, parts[k].seg[j].p, parts[k].seg[j].n);
               dst += parts[k].seg[j].n;
             }
@@ -292,7 +294,11 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
         }
         const uint8_t* src;
         if (r.p1 - r.p0 == 1 && parts[r.p0].nseg == 1)
+        {
           src = parts[r.p0].seg[0].p;
+          if (ready && *ready)
+            (*ready)(src, parts[r.p0].seg[0].n);
+        }
         else
         {
           stage.resize(r.bytes);

@@ -15,6 +15,7 @@
 
 #include <cstdint>
 #include <deque>
+#include <functional>
 #include <map>
 #include <memory>
 #include <string>
@@ -166,7 +167,11 @@ inline bool plane_coded(int bp, int emax, int etol, int bpc)
 }
 int exponent_f64(double v);
 
+// Called before the bytes [p, p + n) of a part are read: waits until they are in place
+// (parts whose bytes are still arriving, e.g. from the device).
+using ready_fn = std::function<void(const uint8_t* p, size_t n)>;
+
 // Write files from their parts (creating directories), with several threads.
-int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& files);
+int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& files, const ready_fn* ready = nullptr);
 
 } // namespace idx2g
