@@ -238,7 +238,7 @@ IDX2G_API int idx2g_encode(idx2g_ctx* c, const idx2g_params* in, const void* fie
       return v && v[0] == '1';
     }();
     if (!host_pack && device_pack_applies(f, *plan))
-      e = encode_dataset_dpack(&c->d, &f, &p, &coder, &tm, *plan, c->d.file_hint(f));
+      e = encode_dataset_dpack(&c->d, &f, &p, &coder, &tm, plan, c->d.file_hint(f));
     else
       e = encode_dataset(&f, &p, &coder, nullptr, true, &tm, plan.get(), c->d.file_hint(f));
     if (!e)

@@ -44,6 +44,7 @@ struct device_ctx
   // batched encode: the launch shape chosen per batch signature (CTAs per SM + 10 * split kernel)
   std::map<std::string, int> tuned;
   std::shared_ptr<void> shard;       // a sharded encode between its two calls (api.cpp)
+  std::shared_ptr<void> dpack;       // the device packer's tables of the last plan (dpack_host.cpp)
   // instantiated CUDA graphs of batched encodes, by batch tag: the launches they were captured
   // from (a byte image of every launch's arguments) and the executable graph
   struct cached_graph

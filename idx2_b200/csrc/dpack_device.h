@@ -72,7 +72,9 @@ void dpack_launch_write(const dpack_args& a, int grid, cudaStream_t st);
 // Packs the levels' regions on ctx's device. Returns NoError, or NotApplicable when a segment
 // holds more keys than the kernels' window (the caller then packs on the host).
 constexpr int kDpackNotApplicable = -2;
-int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& plan,
+// The plan's segment tables are made and uploaded once and kept on the context for the next
+// encode of the same plan.
+int device_pack(device_ctx* ctx, const dataset_format& f, const std::shared_ptr<const encode_plan>& plan,
                 const std::vector<device_level_stream>& levels, packed_dataset* out);
 
 // encode_dataset with the device packer: every level coded with its regions kept on the
@@ -81,6 +83,7 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
 // timing: device_s the coding, pack_s the packing (with the copy of the chunk sections to the
 // host), write_s the files.
 int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_coder* coder, encode_timing* timing,
-                         const encode_plan& plan, const std::vector<unsigned long long>* prealloc);
+                         const std::shared_ptr<const encode_plan>& plan,
+                         const std::vector<unsigned long long>* prealloc);
 
 } // namespace idx2g

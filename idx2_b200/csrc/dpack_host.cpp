@@ -12,32 +12,81 @@
 namespace idx2g
 {
 
-int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& plan,
+namespace
+{
+
+// The segment tables of one plan, on the host and uploaded (kept on the context).
+struct dpack_tables
+{
+  std::shared_ptr<const encode_plan> plan;  // (kept alive: the key is its identity)
+  std::vector<std::vector<int>> nexps;
+  std::vector<unsigned> bricks_per_chunk;
+  dpack_plan P;
+  std::vector<int4> subs;
+  std::vector<int> seg_sub0;
+  dpack_segment* d_segs = nullptr;
+  dpack_event* d_evs = nullptr;
+  int4* d_subs = nullptr;
+  int* d_sub0 = nullptr;
+};
+
+} // namespace
+
+int device_pack(device_ctx* ctx, const dataset_format& f, const std::shared_ptr<const encode_plan>& plan,
                 const std::vector<device_level_stream>& levels, packed_dataset* out)
 {
   stage_timer tt;
   cudaStream_t st = ctx->stream;
-  if (levels.size() > 16)
+  if (levels.size() > 16 || !plan)
     return InvalidArgument;
   std::vector<std::vector<int>> nexps(levels.size());
   for (size_t l = 0; l < levels.size(); ++l)
     nexps[l] = levels[l].nexps;
-  dpack_plan P;
-  int e = dpack_make_plan(f, plan, nexps, &P);
-  if (e)
-    return e;
+  std::vector<unsigned> bpc(f.bricks_per_chunk.begin(), f.bricks_per_chunk.end());
+  std::shared_ptr<dpack_tables> T = std::static_pointer_cast<dpack_tables>(ctx->dpack);
+  if (!T || T->plan != plan || T->nexps != nexps || T->bricks_per_chunk != bpc)
+  {
+    ctx->dpack.reset();
+    T = std::make_shared<dpack_tables>();
+    T->plan = plan;
+    T->nexps = nexps;
+    T->bricks_per_chunk = bpc;
+    int e = dpack_make_plan(f, *plan, nexps, &T->P);
+    if (e)
+      return e;
+    // sub-ranges of kPackSub events per segment
+    const int ns = (int)T->P.segs.size();
+    T->seg_sub0.resize((size_t)ns);
+    for (int si = 0; si < ns; ++si)
+    {
+      T->seg_sub0[(size_t)si] = (int)T->subs.size();
+      int q = 0;
+      for (int i = T->P.segs[(size_t)si].ev0; i < T->P.segs[(size_t)si].ev1; i += kPackSub, ++q)
+        T->subs.push_back(make_int4(si, i, std::min(i + kPackSub, T->P.segs[(size_t)si].ev1), q));
+    }
+    T->d_segs = (dpack_segment*)ctx->ws("dpack.segs", sizeof(dpack_segment) * (size_t)ns);
+    T->d_evs = (dpack_event*)ctx->ws("dpack.evs", sizeof(dpack_event) * T->P.evs.size());
+    T->d_subs = (int4*)ctx->ws("dpack.subs", sizeof(int4) * T->subs.size());
+    T->d_sub0 = (int*)ctx->ws("dpack.sub0", 4 * (size_t)ns);
+    if (!T->d_segs || !T->d_evs || !T->d_subs || !T->d_sub0)
+      return OutOfMemory;
+    cudaMemcpyAsync(T->d_segs, T->P.segs.data(), sizeof(dpack_segment) * (size_t)ns, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(T->d_evs, T->P.evs.data(), sizeof(dpack_event) * T->P.evs.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(T->d_subs, T->subs.data(), sizeof(int4) * T->subs.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(T->d_sub0, T->seg_sub0.data(), 4 * (size_t)ns, cudaMemcpyHostToDevice, st);
+    ctx->dpack = T;
+  }
+  const dpack_plan& P = T->P;
   const int nseg = (int)P.segs.size();
-  dpack_segment* d_segs = (dpack_segment*)ctx->ws("dpack.segs", sizeof(dpack_segment) * (size_t)nseg);
-  dpack_event* d_evs = (dpack_event*)ctx->ws("dpack.evs", sizeof(dpack_event) * P.evs.size());
+  dpack_segment* d_segs = T->d_segs;
+  dpack_event* d_evs = T->d_evs;
   int* d_kmin = (int*)ctx->ws("dpack.kmin", 4 * (size_t)nseg);
   dpack_key* d_keys = (dpack_key*)ctx->ws("dpack.keys", sizeof(dpack_key) * (size_t)nseg * kSegKeys);
   unsigned long long* d_coff = (unsigned long long*)ctx->ws("dpack.coff", 8 * (size_t)nseg * kSegKeys);
   uint8_t* d_exps = (uint8_t*)ctx->ws("dpack.exps", (size_t)P.exp_total + 16);
   int* d_err = (int*)ctx->ws("dpack.err", 16);
-  if (!d_segs || !d_evs || !d_kmin || !d_keys || !d_coff || !d_exps || !d_err)
+  if (!d_kmin || !d_keys || !d_coff || !d_exps || !d_err)
     return OutOfMemory;
-  cudaMemcpyAsync(d_segs, P.segs.data(), sizeof(dpack_segment) * (size_t)nseg, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d_evs, P.evs.data(), sizeof(dpack_event) * P.evs.size(), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(d_err, 0, 16, st);
   const size_t nev = P.evs.size();
   const unsigned long long kb_cap = (unsigned long long)nev * kKeyWindow;
@@ -49,25 +98,11 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   unsigned long long* d_cursor = (unsigned long long*)ctx->ws("dpack.cursor", 16);
   int* d_kmax = (int*)ctx->ws("dpack.kmax", 4 * (size_t)nseg);
   dpack_acc* d_acc = (dpack_acc*)ctx->ws("dpack.acc", sizeof(dpack_acc) * (size_t)nseg * kSegKeys);
-  // sub-ranges of kPackSub events per segment
-  std::vector<int4> subs;
-  std::vector<int> seg_sub0((size_t)nseg);
-  for (int si = 0; si < nseg; ++si)
-  {
-    seg_sub0[(size_t)si] = (int)subs.size();
-    int q = 0;
-    for (int i = P.segs[(size_t)si].ev0; i < P.segs[(size_t)si].ev1; i += kPackSub, ++q)
-      subs.push_back(make_int4(si, i, std::min(i + kPackSub, P.segs[(size_t)si].ev1), q));
-  }
-  int4* d_subs = (int4*)ctx->ws("dpack.subs", sizeof(int4) * subs.size());
-  int* d_sub0 = (int*)ctx->ws("dpack.sub0", 4 * (size_t)nseg);
-  dpack_sub* d_subacc = (dpack_sub*)ctx->ws("dpack.subacc", sizeof(dpack_sub) * subs.size() * kSegKeys);
-  if (!d_evreg || !d_evkmin || !d_evnkeys || !d_evkb || !d_kb || !d_cursor || !d_kmax || !d_acc || !d_subs ||
-      !d_sub0 || !d_subacc)
+  dpack_sub* d_subacc = (dpack_sub*)ctx->ws("dpack.subacc", sizeof(dpack_sub) * T->subs.size() * kSegKeys);
+  if (!d_evreg || !d_evkmin || !d_evnkeys || !d_evkb || !d_kb || !d_cursor || !d_kmax || !d_acc || !d_subacc)
     return OutOfMemory;
-  cudaMemcpyAsync(d_subs, subs.data(), sizeof(int4) * subs.size(), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d_sub0, seg_sub0.data(), 4 * (size_t)nseg, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(d_cursor, 0, 16, st);
+  int e = NoError;
   dpack_args a;
   memset(&a, 0, sizeof a);
   a.segs = d_segs;
@@ -83,9 +118,9 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
   a.cursor = d_cursor;
   a.seg_kmax = d_kmax;
   a.acc = d_acc;
-  a.subs = d_subs;
-  a.nsub = (int)subs.size();
-  a.seg_sub0 = d_sub0;
+  a.subs = T->d_subs;
+  a.nsub = (int)T->subs.size();
+  a.seg_sub0 = T->d_sub0;
   a.sub_acc = d_subacc;
   for (size_t l = 0; l < levels.size(); ++l)
   {
@@ -176,8 +211,10 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const encode_plan& pla
 }
 
 int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_coder* coder, encode_timing* timing,
-                         const encode_plan& plan, const std::vector<unsigned long long>* prealloc)
+                         const std::shared_ptr<const encode_plan>& plan_sp,
+                         const std::vector<unsigned long long>* prealloc)
 {
+  const encode_plan& plan = *plan_sp;
   auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
   const double t0 = now();
   std::thread pre;
@@ -206,7 +243,7 @@ int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_code
     lv[l].nexps = outs[l].nexps;
   }
   packed_dataset pd;
-  e = device_pack(ctx, *f, plan, lv, &pd);
+  e = device_pack(ctx, *f, plan_sp, lv, &pd);
   if (e && e != kDpackNotApplicable)
     cudaStreamSynchronize(ctx->stream);  // (no copy left running into the pinned image)
   if (e == kDpackNotApplicable)

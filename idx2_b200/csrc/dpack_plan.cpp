@@ -43,17 +43,17 @@ struct group_events
 std::vector<group_events> plan_groups(const encode_plan& plan)
 {
   std::vector<group_events> gs;
-  std::map<std::pair<int, int>, size_t> gi;
+  std::vector<int> gi(16 * 64, -1);  // (level, subband) -> group
   for (size_t e = 0; e < plan.events.size(); ++e)
   {
     const encode_event& ev = plan.events[e];
-    auto it = gi.find({ ev.level, ev.subband });
-    if (it == gi.end())
+    const size_t k = (size_t)(ev.level & 15) * 64 + (size_t)(ev.subband & 63);
+    if (gi[k] < 0)
     {
-      it = gi.emplace(std::make_pair(ev.level, ev.subband), gs.size()).first;
+      gi[k] = (int)gs.size();
       gs.push_back(group_events{ ev.level, ev.subband, {} });
     }
-    gs[it->second].events.push_back((uint32_t)e);
+    gs[(size_t)gi[k]].events.push_back((uint32_t)e);
   }
   return gs;
 }

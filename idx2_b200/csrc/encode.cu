@@ -1099,8 +1099,9 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       // with the first sweep of the real transform below
       // The sweeps from the second level on touch only the even positions: the forward
       // sweeps of levels 2.. and the inverse ones back to level 2 run on the 17^3 even
-      // lattice copied into shared memory (the coding tables' space, idle here), lifted in
-      // place sample by sample.
+      // lattice copied into shared memory (the coding tables' space, idle here), a line at a
+      // time in registers (every lattice position is below 17, so the reference's clamps to
+      // the grid's dims never apply).
       double* S = reinterpret_cast<double*>(Xp);
       const int NS[3] = { 17, 17, fp.is2d ? 1 : 17 };
       const int nsub = NS[0] * NS[1] * NS[2];
@@ -1123,7 +1124,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       __syncthreads();
       for (int i = cf; i < nf; ++i)
       {
-        dev::lift_sweep(S, NS, dev::half_grid(sm.stack.g[i]), NS, sm.stack.axis[i], true);
+        dev::lift_sweep_regs<true>(S, NS, dev::half_grid(sm.stack.g[i]), sm.stack.axis[i]);
         __syncthreads();
       }
       ENC_PHASE(3)
@@ -1133,7 +1134,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       const int ni = sm.stack.n, ci = sm.stack.coarse;
       for (int i = ni - 1; i >= ci; --i)
       {
-        dev::lift_sweep(S, NS, dev::half_grid(sm.stack.g[i]), NS, sm.stack.axis[i], false);
+        dev::lift_sweep_regs<false>(S, NS, dev::half_grid(sm.stack.g[i]), sm.stack.axis[i]);
         __syncthreads();
       }
       for (int i = tid; i < nsub; i += kThreads)
