@@ -151,7 +151,6 @@ struct enc_smem_t
   uint8_t nvals_log[kMaxBlocksPerSubband];
   uint8_t perm3[64];
   uint8_t perm2[16];
-  uint16_t npre[kMaxBlocksPerSubband + 1];  // coded planes of the blocks before each block
   uint32_t key_bits[kKeyWindow];
   uint32_t key_base[kKeyWindow];
   uint32_t stage[kStageBytes / 4];  // one (brick, subband) region being assembled
@@ -178,21 +177,36 @@ inline size_t enc_smem_bytes(int planes)
   return ((sizeof(enc_smem) + 127) & ~(size_t)127) + space;
 }
 
-__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc_args a);
+template <int CPS>
+__global__ void __launch_bounds__(kThreads, CPS) k_encode_level(const enc_args a);
 
-// Resident CTAs of k_encode_level per SM with `smem` bytes of dynamic shared memory on the
+// The encode kernel compiled for kCtasPerSm CTAs per SM, or (three) for three CTAs of 256
+// threads per SM (80 registers): the same code; the second suits the level-0 launch of a
+// large field, whose many bricks keep the third CTA busy.
+constexpr bool kThreeCtas = kThreads == 256;
+using enc_kernel_fn = void (*)(const enc_args);
+inline enc_kernel_fn enc_kernel(bool three)
+{
+  if constexpr (kThreeCtas)
+    return three ? k_encode_level<3> : k_encode_level<kCtasPerSm>;
+  return k_encode_level<kCtasPerSm>;
+}
+
+// Resident CTAs of the encode kernel per SM with `smem` bytes of dynamic shared memory on the
 // current device (at least 1, at most the kernel's launch bound).
-inline int enc_occupancy(size_t smem)
+inline int enc_occupancy(size_t smem, bool three = false)
 {
   int n = 0;
-  if (cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_encode_level, kThreads, smem) != cudaSuccess)
+  const enc_kernel_fn k = enc_kernel(three);
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, kThreads, smem) != cudaSuccess)
   {
     cudaGetLastError();
     n = 1;
   }
   n = n < 1 ? 1 : n;
-  return n < kCtasPerSm ? n : kCtasPerSm;
+  const int cap = three && kThreeCtas ? 3 : kCtasPerSm;
+  return n < cap ? n : cap;
 }
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
@@ -533,31 +547,6 @@ __device__ __forceinline__ void code_subband(const enc_args& a, enc_smem_t<NT>& 
       lo = l2 < lo ? l2 : lo;
       hi = h2 > hi ? h2 : hi;
     }
-    {
-      // exclusive prefix of the coded planes over the blocks (lane: blocks 4 lane .. 4 lane + 3)
-      static_assert(kMaxBlocksPerSubband == 128, "four blocks per lane");
-      int c[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        c[i] = 4 * lane + i < nb ? (int)sm.np[4 * lane + i] : 0;
-      const int tot = c[0] + c[1] + c[2] + c[3];
-      int inc = tot;
-      for (int o = 1; o < 32; o <<= 1)
-      {
-        const int y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o)
-          inc += y;
-      }
-      int run = inc - tot;
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-      {
-        sm.npre[4 * lane + i] = (uint16_t)run;
-        run += c[i];
-      }
-      if (lane == 31)
-        sm.npre[kMaxBlocksPerSubband] = (uint16_t)inc;
-    }
     if (lane == 0)
     {
       if (hi < lo)
@@ -715,15 +704,11 @@ __device__ __forceinline__ void code_subband(const enc_args& a, enc_smem_t<NT>& 
     uint32_t* sw = words + 2 + ((2u * (unsigned)nb + 3u) >> 2);
     for (int t = tid; t < nkeys; t += NT)
       sw[t] = (sm.key_bits[t] + 7) / 8;
-    // the coded (block, plane) pairs, enumerated through the prefix of the blocks' plane counts
-    const int npairs = sm.npre[kMaxBlocksPerSubband];
-    for (int idx = tid; idx < npairs; idx += NT)
+    for (int idx = tid; idx < P * kMaxBlocksPerSubband; idx += NT)
     {
-      int b = 0;
-#pragma unroll
-      for (int step = kMaxBlocksPerSubband / 2; step > 0; step >>= 1)
-        b = sm.npre[b + step] <= idx ? b + step : b;
-      const int kk = idx - sm.npre[b];
+      const int b = idx & (kMaxBlocksPerSubband - 1), kk = idx / kMaxBlocksPerSubband;
+      if (b >= nb || kk >= sm.np[b])
+        continue;
       const int t = dev::plane_key(sm.ktop[b], kk, fp.bpc) - kmin;
       const unsigned long long pos = ((unsigned long long)hdr + sm.key_base[t]) * 8ull +
                                      (unsigned long long)OFF[kk * kRowOff + b];
@@ -744,7 +729,8 @@ __device__ __forceinline__ void code_subband(const enc_args& a, enc_smem_t<NT>& 
   ENC_PHASE(14)
 }
 
-__global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc_args a)
+template <int CPS>
+__global__ void __launch_bounds__(kThreads, CPS) k_encode_level(const enc_args a)
 {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   enc_smem& sm = *reinterpret_cast<enc_smem*>(smem_raw);
@@ -1099,9 +1085,8 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       // with the first sweep of the real transform below
       // The sweeps from the second level on touch only the even positions: the forward
       // sweeps of levels 2.. and the inverse ones back to level 2 run on the 17^3 even
-      // lattice copied into shared memory (the coding tables' space, idle here), a line at a
-      // time in registers (every lattice position is below 17, so the reference's clamps to
-      // the grid's dims never apply).
+      // lattice copied into shared memory (the coding tables' space, idle here), lifted in
+      // place sample by sample.
       double* S = reinterpret_cast<double*>(Xp);
       const int NS[3] = { 17, 17, fp.is2d ? 1 : 17 };
       const int nsub = NS[0] * NS[1] * NS[2];
@@ -1124,7 +1109,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       __syncthreads();
       for (int i = cf; i < nf; ++i)
       {
-        dev::lift_sweep_regs<true>(S, NS, dev::half_grid(sm.stack.g[i]), sm.stack.axis[i]);
+        dev::lift_sweep(S, NS, dev::half_grid(sm.stack.g[i]), NS, sm.stack.axis[i], true);
         __syncthreads();
       }
       ENC_PHASE(3)
@@ -1134,7 +1119,7 @@ __global__ void __launch_bounds__(kThreads, kCtasPerSm) k_encode_level(const enc
       const int ni = sm.stack.n, ci = sm.stack.coarse;
       for (int i = ni - 1; i >= ci; --i)
       {
-        dev::lift_sweep_regs<false>(S, NS, dev::half_grid(sm.stack.g[i]), sm.stack.axis[i]);
+        dev::lift_sweep(S, NS, dev::half_grid(sm.stack.g[i]), NS, sm.stack.axis[i], false);
         __syncthreads();
       }
       for (int i = tid; i < nsub; i += kThreads)
@@ -1329,6 +1314,7 @@ struct batch_encoder::level_launch
   int planes = 32;
   int grid = 1;
   bool split = false;  // k_encode_split for the 3D bricks (bricks in shared memory)
+  bool three = false;  // the three-CTA build of k_encode_level
   int split_grid = 2;
   // a level with 2D and 3D bricks: the 3D bricks (split_order) go to k_encode_split, the 2D
   // ones (slot_order) to k_encode_level
@@ -1567,7 +1553,10 @@ int batch_encoder::prepare(const batch_tuning& t)
     const int nbr = (int)ll.bricks.size();
     // CTAs per SM: as many as the level's shared memory and the kernel's registers let reside
     // (or fewer, when the tuning asks), so that no CTA of the grid waits for a place
-    const int occ = enc_occupancy(enc_smem_bytes(ll.planes));
+    // the level-0 launch of many bricks takes the three-CTA build when three CTAs fit
+    ll.three = kThreeCtas && l == 0 && tune_.ctas_per_sm == 0 && nbr >= 6 * ctx_->num_sms &&
+               enc_occupancy(enc_smem_bytes(ll.planes), true) >= 3;
+    const int occ = enc_occupancy(enc_smem_bytes(ll.planes), ll.three);
     const int cps = tune_.ctas_per_sm > 0 && tune_.ctas_per_sm < occ ? tune_.ctas_per_sm : occ;
     const int lim = cps * ctx_->num_sms;
     ll.grid = nbr < lim ? (nbr > 0 ? nbr : 1) : lim;
@@ -1686,7 +1675,8 @@ int batch_encoder::prepare(const batch_tuning& t)
     ll->args.slots = d_slots;
     max_smem = ll->smem > max_smem ? ll->smem : max_smem;
   }
-  cudaFuncSetAttribute(k_encode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+  cudaFuncSetAttribute(enc_kernel(false), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
+  cudaFuncSetAttribute(enc_kernel(true), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)max_smem);
   return cudaGetLastError() == cudaSuccess ? NoError : CudaError;
 }
 
@@ -1709,7 +1699,7 @@ int batch_encoder::enqueue_level(int l)
       enc_args a2 = ll.args;
       a2.order = ll.d_slot_order;
       a2.last = (int)ll.slot_order.size();
-      k_encode_level<<<a2.last < ll.grid ? a2.last : ll.grid, kThreads, ll.smem, st>>>(a2);
+      enc_kernel(ll.three)<<<a2.last < ll.grid ? a2.last : ll.grid, kThreads, ll.smem, st>>>(a2);
       launches_ += 2;
       ctx_->launches += 2;
     }
@@ -1718,7 +1708,7 @@ int batch_encoder::enqueue_level(int l)
       if (ll.split)
         k_encode_split<<<ll.split_grid, kSplitThreads, split_smem_bytes(), st>>>(ll.args);
       else
-        k_encode_level<<<ll.grid, kThreads, ll.smem, st>>>(ll.args);
+        enc_kernel(ll.three)<<<ll.grid, kThreads, ll.smem, st>>>(ll.args);
       ++launches_;
       ++ctx_->launches;
     }
@@ -1807,7 +1797,7 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
     if (ll.split)
       k_encode_split<<<2 * (n < ll.split_grid / 2 ? n : ll.split_grid / 2), kSplitThreads, split_smem_bytes(), st>>>(a);
     else
-      k_encode_level<<<n < ll.grid ? n : ll.grid, kThreads, ll.smem, st>>>(a);
+      enc_kernel(ll.three)<<<n < ll.grid ? n : ll.grid, kThreads, ll.smem, st>>>(a);
     cudaEventRecord(t1, st);
     // the region cursor after the band: its regions end there
     cudaMemcpyAsync(h_cur + g, ll.d_misc, 8, cudaMemcpyDeviceToHost, st);
