@@ -154,36 +154,344 @@ void decode_device::upload_blob(device_ctx* ctx, const uint8_t* src, size_t offs
     cudaMemcpyAsync(blob_ + offset, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
 }
 
-int decode_device::upload_tables(device_ctx* ctx, const int16_t* exps, const int32_t* kmin, const int32_t* n,
-                                 const uint64_t* first, const uint64_t* off, size_t nchan)
+namespace
+{
+
+// ---------------------------------------------------------------------------
+// device index: channel tables from the chunk headers in the blob
+// ---------------------------------------------------------------------------
+struct index_args
+{
+  const index_chunk* chunks;
+  int nchunks, nsb;
+  const uint8_t* blob;
+  const int* bmap;  // per level: flat brick of each linear brick, or -1
+  long long bmap_base[16];
+  int bmap_size[16];
+  int* kmin;
+  int* kmax;
+  int* n;
+  unsigned long long* first;
+  unsigned long long* off;
+  unsigned long long* block_sums;
+  unsigned long long* nchan;
+  size_t nslots;
+  int* error;
+};
+
+// LSB-first bit reader over one chunk's bytes [p, p + n) (bytes past the end read as zero),
+// with the host index reader's varbyte and unary rules (Core/VarInt.h:30 ReadVarByte, :90
+// ReadUnary).
+struct chunk_reader
+{
+  const uint8_t* p;
+  unsigned long long n, pos;
+  __device__ __forceinline__ unsigned long long peek() const
+  {
+    const unsigned long long b = pos >> 3;
+    unsigned long long w = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      if (b + (unsigned long long)i < n)
+        w |= (unsigned long long)__ldg(p + b + i) << (8 * i);
+    return w >> (pos & 7);
+  }
+  __device__ __forceinline__ unsigned long long varbyte()
+  {
+    unsigned long long v = 0;
+    int sh = 0;
+    for (;;)
+    {
+      const unsigned long long b = peek() & 0xFFull;
+      pos += 8;
+      v = ((b & 0x7Full) << ((7 * sh++) & 63)) + v;
+      if (!(b >> 7) || sh > 10)
+        break;
+    }
+    return v;
+  }
+  __device__ __forceinline__ unsigned long long unary()
+  {
+    unsigned long long v = 0;
+    for (;;)
+    {
+      const unsigned long long w = peek() & ((1ull << 57) - 1);
+      if (w)
+      {
+        const int z = __ffsll((long long)w) - 1;
+        pos += (unsigned long long)z + 1;
+        return v + (unsigned long long)z;
+      }
+      v += 57;
+      pos += 57;
+      if ((pos >> 3) > n)
+        return v;
+    }
+  }
+  __device__ __forceinline__ void next_byte() { pos = (pos + 7) & ~7ull; }
+};
+
+// Every brick of every chunk, a chunk per thread: PASS 0 the key range of its slot, PASS 1
+// the brick's data offset into the slot's row of the offset table.
+template <int PASS>
+__global__ void __launch_bounds__(128) k_index_chunks(const index_args a)
+{
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.nchunks; c += gridDim.x * blockDim.x)
+  {
+    const index_chunk C = a.chunks[c];
+    chunk_reader cr{ a.blob + C.off, C.size, 0 };
+    const unsigned long long nbr64 = cr.varbyte();
+    if (nbr64 > C.size * 8 + 1)
+    {
+      atomicOr(a.error, 1);
+      continue;
+    }
+    const long long nbr = (long long)nbr64;
+    // the sizes follow the gaps (byte-aligned); the data follows the sizes
+    chunk_reader s = cr;
+    if (nbr > 0)
+    {
+      s.varbyte();
+      for (long long i = 1; i < nbr; ++i)
+        s.unary();
+    }
+    s.next_byte();
+    chunk_reader e = s;
+    for (long long i = 0; i < nbr; ++i)
+      e.varbyte();
+    const unsigned long long data = C.off + (e.pos >> 3);
+    const long long base = a.bmap_base[C.level & 15];
+    const int msize = a.bmap_size[C.level & 15];
+    unsigned long long b = 0, acc = 0;
+    for (long long i = 0; i < nbr; ++i)
+    {
+      b = i == 0 ? cr.varbyte() : b + cr.unary() + 1;
+      const unsigned long long o = acc;
+      acc += s.varbyte();
+      if (b >= (unsigned long long)msize)
+        continue;
+      const int flat = a.bmap[base + (long long)b];
+      if (flat < 0)
+        continue;
+      const size_t slot = (size_t)flat * (size_t)a.nsb + (size_t)C.subband;
+      if (PASS == 0)
+      {
+        atomicMin(&a.kmin[slot], C.bpkey);
+        atomicMax(&a.kmax[slot], C.bpkey);
+      }
+      else
+      {
+        const int d = C.bpkey - a.kmin[slot];
+        if (d >= 0 && d < a.n[slot])
+          a.off[a.first[slot] + (unsigned long long)d] = data + o;
+      }
+    }
+  }
+}
+
+constexpr int kScanBlock = 1024;  // slots per CTA of the key-count scan (256 threads x 4)
+
+__global__ void __launch_bounds__(256) k_index_init(const index_args a)
+{
+  for (size_t i = (size_t)blockIdx.x * 256 + threadIdx.x; i < a.nslots; i += (size_t)gridDim.x * 256)
+  {
+    a.kmin[i] = 1 << 30;
+    a.kmax[i] = -1;
+  }
+}
+
+// key counts per slot and their exclusive prefix within each block of kScanBlock slots
+__global__ void __launch_bounds__(256) k_index_scan_blocks(const index_args a)
+{
+  __shared__ unsigned long long s_part[8];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const size_t b0 = (size_t)blockIdx.x * kScanBlock;
+  unsigned long long v[4], t = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+  {
+    const size_t i = b0 + (size_t)tid * 4 + (size_t)k;
+    unsigned long long c = 0;
+    if (i < a.nslots)
+    {
+      if (a.kmax[i] < 0)
+      {
+        a.kmin[i] = 1;
+        a.n[i] = 0;
+      }
+      else
+      {
+        a.n[i] = a.kmax[i] - a.kmin[i] + 1;
+        c = (unsigned long long)a.n[i];
+      }
+    }
+    v[k] = c;
+    t += c;
+  }
+  unsigned long long inc = t;
+  for (int o = 1; o < 32; o <<= 1)
+  {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o)
+      inc += y;
+  }
+  if (lane == 31)
+    s_part[warp] = inc;
+  __syncthreads();
+  unsigned long long wbase = 0;
+  for (int w = 0; w < warp; ++w)
+    wbase += s_part[w];
+  unsigned long long run = wbase + inc - t;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+  {
+    const size_t i = b0 + (size_t)tid * 4 + (size_t)k;
+    if (i < a.nslots)
+      a.first[i] = run;
+    run += v[k];
+  }
+  if (tid == 255)
+    a.block_sums[blockIdx.x] = wbase + inc;
+}
+
+// the blocks' totals to exclusive prefixes (one CTA), and the table's size
+__global__ void __launch_bounds__(1024) k_index_scan_sums(const index_args a, int nblocks)
+{
+  __shared__ unsigned long long s_part[32];
+  __shared__ unsigned long long s_carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0)
+    s_carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < nblocks; b0 += 1024)
+  {
+    const int i = b0 + tid;
+    const unsigned long long c = i < nblocks ? a.block_sums[i] : 0ull;
+    unsigned long long inc = c;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o)
+        inc += y;
+    }
+    if (lane == 31)
+      s_part[warp] = inc;
+    __syncthreads();
+    unsigned long long wbase = 0;
+    for (int w = 0; w < warp; ++w)
+      wbase += s_part[w];
+    const unsigned long long carry = s_carry;
+    if (i < nblocks)
+      a.block_sums[i] = carry + wbase + inc - c;
+    __syncthreads();
+    if (tid == 1023)
+      s_carry = carry + wbase + inc;
+    __syncthreads();
+  }
+  if (tid == 0)
+    *a.nchan = s_carry;
+}
+
+__global__ void __launch_bounds__(256) k_index_scan_add(const index_args a)
+{
+  const size_t b0 = (size_t)blockIdx.x * kScanBlock;
+  const unsigned long long add = a.block_sums[blockIdx.x];
+  for (int k = threadIdx.x; k < kScanBlock; k += 256)
+    if (b0 + (size_t)k < a.nslots)
+      a.first[b0 + (size_t)k] += add;
+}
+
+} // namespace
+
+int decode_device::build_index(device_ctx* ctx, const std::vector<index_chunk>& chunks, const std::vector<int>& brick_map,
+                               const std::vector<long long>& level_base, const std::vector<int>& level_size, int nsb,
+                               const int16_t* exps, size_t* nchan_out)
 {
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
   stage_timer tt;
+  if (level_base.size() > 16 || level_size.size() != level_base.size())
+    return InvalidArgument;
+  const size_t ns = nslots_;
+  const int nblocks = (int)((ns + kScanBlock - 1) / kScanBlock);
+  index_chunk* d_chunks = (index_chunk*)ctx->ws("dec.ix.chunks", sizeof(index_chunk) * (chunks.size() + 1));
+  int* d_bmap = (int*)ctx->ws("dec.ix.bmap", sizeof(int) * (brick_map.size() + 1));
+  int* d_kmax = (int*)ctx->ws("dec.ix.kmax", sizeof(int) * (ns + 1));
+  unsigned long long* d_sums = (unsigned long long*)ctx->ws("dec.ix.sums", 8 * ((size_t)nblocks + 2));
+  int* d_err = (int*)ctx->ws("dec.ix.err", 16);
+  if (!d_chunks || !d_bmap || !d_kmax || !d_sums || !d_err)
+    return OutOfMemory;
+  if (!chunks.empty())
+    cudaMemcpyAsync(d_chunks, chunks.data(), sizeof(index_chunk) * chunks.size(), cudaMemcpyHostToDevice, st);
+  if (!brick_map.empty())
+    cudaMemcpyAsync(d_bmap, brick_map.data(), sizeof(int) * brick_map.size(), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(d_err, 0, 16, st);
+  index_args a;
+  memset(&a, 0, sizeof a);
+  a.chunks = d_chunks;
+  a.nchunks = (int)chunks.size();
+  a.nsb = nsb;
+  a.blob = blob_;
+  a.bmap = d_bmap;
+  for (size_t l = 0; l < level_base.size(); ++l)
+  {
+    a.bmap_base[l] = level_base[l];
+    a.bmap_size[l] = level_size[l];
+  }
+  a.kmin = kmin_;
+  a.kmax = d_kmax;
+  a.n = n_;
+  a.first = first_;
+  a.block_sums = d_sums;
+  a.nchan = d_sums + nblocks + 1;
+  a.nslots = ns;
+  a.error = d_err;
+  const int cgrid = (int)((chunks.size() + 127) / 128);
+  if (ns)
+  {
+    k_index_init<<<ns / 256 + 1 < 4096 ? (unsigned)(ns / 256 + 1) : 4096u, 256, 0, st>>>(a);
+    if (cgrid)
+      k_index_chunks<0><<<cgrid, 128, 0, st>>>(a);
+    k_index_scan_blocks<<<nblocks, 256, 0, st>>>(a);
+    k_index_scan_sums<<<1, 1024, 0, st>>>(a, nblocks);
+    k_index_scan_add<<<nblocks, 256, 0, st>>>(a);
+    ctx->launches += 5;
+  }
+  else
+    cudaMemsetAsync(a.nchan, 0, 8, st);
+  unsigned long long nchan = 0;
+  int err = 0;
+  cudaMemcpyAsync(&nchan, a.nchan, 8, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, st);
+  if (ns)
+    cudaMemcpyAsync(exps_, exps, ns * kMaxBlocksPerSubband * sizeof(int16_t), cudaMemcpyHostToDevice, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return CudaError;
+  if (err)
+    return CorruptStream;
+  tt.lap("open.index.keys");
   if (pool_alloc(device_, (void**)&off_, nchan * sizeof(uint64_t) + 16, st) != cudaSuccess)
   {
     cudaGetLastError();
     return OutOfMemory;
   }
-  tt.lap("open.upload.alloc");
-  const size_t ns = nslots_;
-  if (ns)
-  {
-    cudaMemcpyAsync(exps_, exps, ns * kMaxBlocksPerSubband * sizeof(int16_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(kmin_, kmin, ns * sizeof(int32_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(n_, n, ns * sizeof(int32_t), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(first_, first, ns * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
-  }
   if (nchan)
-    cudaMemcpyAsync(off_, off, nchan * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(off_, 0xFF, nchan * sizeof(uint64_t), st);
+  a.off = off_;
+  if (ns && cgrid)
+  {
+    k_index_chunks<1><<<cgrid, 128, 0, st>>>(a);
+    ctx->launches += 1;
+  }
   resident_ = ns * (kMaxBlocksPerSubband * sizeof(int16_t) + 2 * sizeof(int32_t) + sizeof(uint64_t)) +
               nchan * sizeof(uint64_t) + blob_bytes_;
-  // the staging buffers are reused by the next open on this context
   if (cudaStreamSynchronize(st) != cudaSuccess)
     return CudaError;
-  tt.lap("open.upload.wait");
+  tt.lap("open.index.offsets");
+  *nchan_out = (size_t)nchan;
   return NoError;
 }
+
 
 int decode_device::decode(device_ctx* ctx, const decode_request& rq, void* out, size_t out_bytes,
                           bool out_on_device, double* kernel_ms)

@@ -77,17 +77,31 @@ struct brick_piece
   long long out;
 };
 
+// A bit-plane chunk of an opened dataset, as the file tails locate it (host).
+struct index_chunk
+{
+  unsigned long long off, size;  // bytes of the chunk in the blob
+  int level, subband, bpkey, pad_;
+};
+
 class decode_device
 {
 public:
   ~decode_device();
   // Opening a dataset: alloc() the per-(brick, subband) tables of nslots entries and the blob,
-  // upload_blob() each range of the files as it is read (any thread), upload_tables() once the
-  // host index is built (waits for every copy).
+  // upload_blob() each range of the files as it is read (any thread), build_index() once the
+  // exponents are on the host (waits for every copy).
   int alloc(device_ctx* ctx, size_t nslots, size_t blob_bytes);
   void upload_blob(device_ctx* ctx, const uint8_t* src, size_t offset, size_t bytes);
-  int upload_tables(device_ctx* ctx, const int16_t* exps, const int32_t* kmin, const int32_t* n,
-                    const uint64_t* first, const uint64_t* off, size_t nchan);
+  // The channel tables, built on the device (after every upload_blob): the chunk
+  // headers in the blob (Core/idx2Decode.cpp:507 DecompressChunk: varbyte NBricks, the first
+  // brick as a varbyte then unary gaps, varbyte sizes) are read a chunk per thread, twice:
+  // the key range of every (brick, subband) slot, an exclusive scan of the slots' key counts,
+  // then each brick's data offset. brick_map: per level (from level_base[l], level_size[l]
+  // entries) the flat brick of each linear brick index, or -1. Then the exponents go up.
+  int build_index(device_ctx* ctx, const std::vector<index_chunk>& chunks, const std::vector<int>& brick_map,
+                  const std::vector<long long>& level_base, const std::vector<int>& level_size, int nsb,
+                  const int16_t* exps, size_t* nchan);
   int decode(device_ctx* ctx, const decode_request& rq, void* out, size_t out_bytes, bool out_on_device,
              double* kernel_ms);
   // Several requests on this dataset at once: per level one launch (of each kernel) over the

@@ -134,9 +134,13 @@ struct dataset_handle
   // host index, built while the dataset opens in pinned staging buffers of the context
   size_t nslots = 0, nchan = 0;
   int16_t* exps = nullptr;                       // [level offset + brick][sb][kMaxBlocksPerSubband]
-  int32_t* chan_kmin = nullptr, *chan_n = nullptr;  // [flat brick][sb]
-  uint64_t* chan_first = nullptr;                // [flat brick][sb] index into chan_off
-  uint64_t* chan_off = nullptr;                  // byte offset in blob, ~0 = absent
+  // the bit-plane chunks and the linear -> flat brick maps, from which the device builds the
+  // channel tables (per (brick, subband): key range, first entry; per entry: byte offset in
+  // the blob, ~0 = absent)
+  std::vector<index_chunk> ix_chunks;
+  std::vector<int> ix_bmap;
+  std::vector<long long> ix_base;
+  std::vector<int> ix_size;
   const uint8_t* blob = nullptr;                 // every data file back to back (pinned host memory)
   size_t blob_bytes = 0;
   // device copies
@@ -178,12 +182,6 @@ struct chunk_ref
 };
 
 // one brick's data inside a bit-plane chunk
-struct chan_entry
-{
-  uint32_t slot;  // flat brick * nsb + subband
-  int32_t bpkey;
-  uint64_t off;   // byte offset in the blob
-};
 
 } // namespace
 
@@ -242,10 +240,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     return OptionNotSupported;
   h->nslots = nslots;
   h->exps = (int16_t*)ctx->pinned("dec.exps", nslots * kMaxBlocksPerSubband * sizeof(int16_t));
-  h->chan_kmin = (int32_t*)ctx->pinned("dec.kmin", nslots * sizeof(int32_t));
-  h->chan_n = (int32_t*)ctx->pinned("dec.n", nslots * sizeof(int32_t));
-  h->chan_first = (uint64_t*)ctx->pinned("dec.first", nslots * sizeof(uint64_t));
-  if (!h->exps || !h->chan_kmin || !h->chan_n || !h->chan_first)
+  if (!h->exps)
     return OutOfMemory;
   parallel_ranges(nslots, [&](size_t i0, size_t i1) {
     memset(h->exps + i0 * kMaxBlocksPerSubband, 0, (i1 - i0) * kMaxBlocksPerSubband * sizeof(int16_t));
@@ -477,127 +472,36 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     return err;
 
   tt.lap("open.exponents");
-  // bit-plane chunk headers (Core/idx2Decode.cpp:507 DecompressChunk), one task per chunk
-  std::atomic<int> mixed_ranges{ 0 };
-  std::vector<std::vector<chan_entry>> entries(bp_chunks.size());
-  parallel_for(bp_chunks.size(), [&](size_t k) {
-    const chunk_ref& c = bp_chunks[k];
-    int sb = (int)((c.addr >> 12) & 0x3F);
-    int lv = (int)((c.addr >> 60) & 0xF);
-    int bpkey = (int)(c.addr & 0xFFF);
-    if (lv != c.level || sb >= nsb)
-      return;
-    // whether every brick of the chunk lies in the chunk's brick range (then chunks of
-    // different ranges touch different slots of the channel table below)
-    const int cshift = log2_ceil(f.bricks_per_chunk[(size_t)lv]);
-    const u64 crange = (c.addr >> 18) & 0x3FFFFFFFFFFull;
-    bit_reader cr{ blob + c.off, c.size };
-    const uint64_t nbr64 = cr.varbyte();
-    if (nbr64 > c.size * 8 + 1)
-    {
-      err = CorruptStream;
-      return;
-    }
-    const int nbr = (int)nbr64;
-    std::vector<u64> bricks((size_t)nbr);
-    if (nbr > 0)
-    {
-      u64 b = cr.varbyte();
-      bricks[0] = b;
-      for (int i = 1; i < nbr; ++i)
-      {
-        b += cr.unary() + 1;
-        bricks[(size_t)i] = b;
-      }
-    }
-    cr.next_byte();
-    std::vector<uint64_t> offs((size_t)nbr, 0);
-    uint64_t acc = 0;
-    for (int i = 1; i < nbr; ++i)
-    {
-      acc += cr.varbyte();
-      offs[(size_t)i] = acc;
-    }
-    if (nbr > 0)
-      cr.varbyte();
-    const uint64_t data_start = cr.pos >> 3;
-    std::vector<chan_entry>& out = entries[k];
-    out.reserve((size_t)nbr);
-    const std::vector<int>& index = h->brick_index[(size_t)lv];
-    for (int i = 0; i < nbr; ++i)
-    {
-      u64 lin = bricks[(size_t)i];
-      if ((lin >> cshift) != crange)
-        mixed_ranges = 1;
-      if (lin >= index.size())
-        continue;
-      int bi = index[lin];
-      if (bi < 0)
-        continue;
-      size_t flat = h->level_brick_base[(size_t)lv] + (size_t)bi;
-      out.push_back({ (uint32_t)(flat * (size_t)nsb + (size_t)sb), bpkey,
-                      (uint64_t)(c.off + data_start + offs[(size_t)i]) });
-    }
-  });
-  if (err)
-    return err;
-
-  tt.lap("open.chunk_headers");
-  // channel table: key range per (brick, subband), then the offsets. The chunks of one
-  // (level, subband, brick range) -- one per key -- are the only ones to touch that range's
-  // slots of that subband, so each such group is one task (each (level, subband) if some
-  // chunk holds bricks outside its range).
-  std::vector<int32_t> kmax(nslots, -1);
-  int32_t* kmin = h->chan_kmin;
-  parallel_ranges(nslots, [&](size_t i0, size_t i1) { std::fill(kmin + i0, kmin + i1, 1 << 30); });
-  std::map<std::tuple<int, int, u64>, size_t> group_of;
-  std::vector<std::vector<size_t>> by_sb;
-  for (size_t k = 0; k < bp_chunks.size(); ++k)
+  // bit-plane chunks for the device index (decode_device::build_index parses their headers,
+  // Core/idx2Decode.cpp:507 DecompressChunk)
+  h->ix_chunks.clear();
+  h->ix_chunks.reserve(bp_chunks.size());
+  for (const chunk_ref& c : bp_chunks)
   {
-    const int sb = (int)((bp_chunks[k].addr >> 12) & 0x3F), lv = (int)((bp_chunks[k].addr >> 60) & 0xF);
-    const u64 chunk = mixed_ranges ? 0 : (bp_chunks[k].addr >> 18) & 0x3FFFFFFFFFFull;
-    if (lv != bp_chunks[k].level || lv >= L || sb >= nsb)
+    const int sb = (int)((c.addr >> 12) & 0x3F), lv = (int)((c.addr >> 60) & 0xF);
+    if (lv != c.level || lv >= L || sb >= nsb)
       continue;
-    auto it = group_of.emplace(std::make_tuple(lv, sb, chunk), by_sb.size()).first;
-    if (it->second == by_sb.size())
-      by_sb.emplace_back();
-    by_sb[it->second].push_back(k);
+    h->ix_chunks.push_back(index_chunk{ (unsigned long long)c.off, (unsigned long long)c.size, lv, sb,
+                                        (int)(c.addr & 0xFFF), 0 });
   }
-  parallel_for(by_sb.size(), [&](size_t g) {
-    for (size_t k : by_sb[g])
-      for (const chan_entry& e : entries[k])
-      {
-        kmin[e.slot] = std::min(kmin[e.slot], e.bpkey);
-        kmax[e.slot] = std::max(kmax[e.slot], e.bpkey);
-      }
-  });
-  uint64_t nchan = 0;
-  for (size_t i = 0; i < nslots; ++i)
+  h->ix_base.assign((size_t)L, 0);
+  h->ix_size.assign((size_t)L, 0);
+  size_t nmap = 0;
+  for (int l = 0; l < L; ++l)
   {
-    if (kmax[i] < 0)
-    {
-      kmin[i] = 1;
-      h->chan_n[i] = 0;
-    }
-    else
-      h->chan_n[i] = kmax[i] - kmin[i] + 1;
-    h->chan_first[i] = nchan;
-    nchan += (uint64_t)h->chan_n[i];
+    h->ix_base[(size_t)l] = (long long)nmap;
+    h->ix_size[(size_t)l] = (int)h->brick_index[(size_t)l].size();
+    nmap += h->brick_index[(size_t)l].size();
   }
-  h->nchan = nchan;
-  h->chan_off = (uint64_t*)ctx->pinned("dec.off", (nchan ? nchan : 1) * sizeof(uint64_t));
-  if (!h->chan_off)
-    return OutOfMemory;
-  parallel_ranges(nchan, [&](size_t i0, size_t i1) { std::fill(h->chan_off + i0, h->chan_off + i1, ~0ull); });
-  parallel_for(entries.size(), [&](size_t k) {
-    for (const chan_entry& e : entries[k])
-    {
-      const int d = e.bpkey - kmin[e.slot];
-      if (d >= 0 && d < h->chan_n[e.slot])
-        h->chan_off[h->chan_first[e.slot] + (size_t)d] = e.off;
-    }
-  });
-  tt.lap("open.channels");
+  h->ix_bmap.resize(nmap);
+  for (int l = 0; l < L; ++l)
+  {
+    const std::vector<int>& index = h->brick_index[(size_t)l];
+    int* dst = h->ix_bmap.data() + h->ix_base[(size_t)l];
+    for (size_t lin = 0; lin < index.size(); ++lin)
+      dst[lin] = index[lin] < 0 ? -1 : (int)(h->level_brick_base[(size_t)l] + (size_t)index[lin]);
+  }
+  tt.lap("open.chunks");
   return NoError;
 }
 
@@ -620,13 +524,16 @@ int dataset_open(device_ctx* ctx, const params& pin, dataset_handle** out)
     e = load_index(ctx, h);
   stage_timer tt;
   if (!e)
-    e = h->dev.upload_tables(ctx, h->exps, h->chan_kmin, h->chan_n, h->chan_first, h->chan_off, h->nchan);
-  tt.lap("open.upload");
+    e = h->dev.build_index(ctx, h->ix_chunks, h->ix_bmap, h->ix_base, h->ix_size, h->f.nsubbands(), h->exps,
+                           &h->nchan);
+  tt.lap("open.index");
   // the pinned staging buffers stay with the context
   h->blob = nullptr;
   h->exps = nullptr;
-  h->chan_kmin = h->chan_n = nullptr;
-  h->chan_first = h->chan_off = nullptr;
+  h->ix_chunks.clear();
+  h->ix_chunks.shrink_to_fit();
+  h->ix_bmap.clear();
+  h->ix_bmap.shrink_to_fit();
   if (e)
   {
     delete h;
