@@ -322,7 +322,13 @@ def ours_sharded(args, rank, world, local_rank):
     local_rank = local_rank % max(1, torch.cuda.device_count())
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=300))
+    def note(what):
+        if os.environ.get("IDX2G_BENCH_TRACE"):
+            print(f"bench rank {rank}: {what}", file=sys.stderr, flush=True)
+
+    note("init")
+    dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=120))
+    note("process group up")
     stream = torch.cuda.Stream(device=dev)
     _lib.ctx_on_stream(local_rank, stream)  # the library's work on a stream the events can bracket
     side = args.side
@@ -353,7 +359,9 @@ def ours_sharded(args, rank, world, local_rank):
             shutil.rmtree(tmp, ignore_errors=True)
         dist.barrier()
         import idx2_b200 as idx2
+        note("setup encode")
         encode_to(os.path.join(tmp, "setup"), field)
+        note("setup encoded")
         ds = idx2.Dataset(os.path.join(tmp, "setup", "grf", "f.idx2"))
         out_dev = torch.empty_like(field)
         recs = []
@@ -366,6 +374,7 @@ def ours_sharded(args, rank, world, local_rank):
 
         for _ in range(args.warmup):
             device_step()
+        note("warmed up")
         recs.clear()
         torch.cuda.synchronize()
         dist.barrier()
@@ -385,6 +394,7 @@ def ours_sharded(args, rank, world, local_rank):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_ms = float(t)
         ds.close()
+        note("timed")
         # e2e: host block in, files out, the dataset read back and this block decoded to the host
         host = field.cpu().pin_memory()
         out_host = torch.empty(field.shape, dtype=field.dtype).pin_memory()
@@ -968,7 +978,10 @@ def main():
             port = sk.getsockname()[1]
         cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
                "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
-        sys.exit(subprocess.call(cmd))
+        env = dict(os.environ)
+        if args.dist_backend == "gloo":
+            env.setdefault("GLOO_SOCKET_IFNAME", "lo")  # the ranks talk over loopback
+        sys.exit(subprocess.call(cmd, env=env))
     if world != args.gpus and rank == 0:
         print(f"bench: --gpus {args.gpus} but WORLD_SIZE={world}; using {world} ranks", file=sys.stderr)
     if args.serve:
