@@ -331,10 +331,14 @@ def ours_sharded(args, rank, world, local_rank):
     note("process group up")
     stream = torch.cuda.Stream(device=dev)
     _lib.ctx_on_stream(local_rank, stream)  # the library's work on a stream the events can bracket
+    note("context")
     side = args.side
     gd = global_dims(side, world)
     lo, sz = shard_region(gd, "float32", LEVELS, TOL, rank, world)
+    note(f"region {lo} {sz} of {gd}")
     field = grf_field_torch(sz[0], sz[1], sz[2], seed=7 + rank, scale="unit", n_fronts=20, device=dev)
+    torch.cuda.synchronize()
+    note("field")
     raw_bytes = field.numel() * field.element_size()
     tmp = os.path.join("/dev/shm" if os.path.isdir("/dev/shm") else tempfile.gettempdir(),
                        f"idx2bench_{os.environ.get('MASTER_PORT', '0')}")
@@ -358,6 +362,7 @@ def ours_sharded(args, rank, world, local_rank):
         if rank == 0:
             shutil.rmtree(tmp, ignore_errors=True)
         dist.barrier()
+        note("barrier")
         import idx2_b200 as idx2
         note("setup encode")
         encode_to(os.path.join(tmp, "setup"), field)

@@ -179,30 +179,36 @@ struct index_args
   int* error;
 };
 
-// LSB-first bit reader over one chunk's bytes [p, p + n) (bytes past the end read as zero),
-// with the host index reader's varbyte and unary rules (Core/VarInt.h:30 ReadVarByte, :90
-// ReadUnary).
-struct chunk_reader
+// Bits of one chunk of the blob, LSB-first, read through the blob's aligned 32-bit words (the
+// blob's 32 bytes of zero padding cover the look-ahead); bits at or past the chunk's end read
+// as zero, as the host index reader's bytes past a chunk do. Positions are absolute bit
+// positions in the blob. varbyte and unary follow Core/VarInt.h:30 ReadVarByte, :90 ReadUnary.
+struct chunk_bits
 {
-  const uint8_t* p;
-  unsigned long long n, pos;
-  __device__ __forceinline__ unsigned long long peek() const
+  const uint32_t* w;
+  unsigned long long hi;  // the chunk's end
+  __device__ __forceinline__ unsigned long long peek(unsigned long long pos) const
   {
-    const unsigned long long b = pos >> 3;
-    unsigned long long w = 0;
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-      if (b + (unsigned long long)i < n)
-        w |= (unsigned long long)__ldg(p + b + i) << (8 * i);
-    return w >> (pos & 7);
+    if (pos >= hi)
+      return 0ull;
+    const unsigned long long k = pos >> 5;
+    const int sh = (int)(pos & 31);
+    const unsigned long long x = (unsigned long long)__ldg(w + k) | ((unsigned long long)__ldg(w + k + 1) << 32);
+    unsigned long long v = x >> sh;
+    if (sh)
+      v |= (unsigned long long)__ldg(w + k + 2) << (64 - sh);
+    const unsigned long long left = hi - pos;
+    if (left < 64)
+      v &= (1ull << left) - 1ull;
+    return v;
   }
-  __device__ __forceinline__ unsigned long long varbyte()
+  __device__ __forceinline__ unsigned long long varbyte(unsigned long long& pos) const
   {
     unsigned long long v = 0;
     int sh = 0;
     for (;;)
     {
-      const unsigned long long b = peek() & 0xFFull;
+      const unsigned long long b = peek(pos) & 0xFFull;
       pos += 8;
       v = ((b & 0x7Full) << ((7 * sh++) & 63)) + v;
       if (!(b >> 7) || sh > 10)
@@ -210,64 +216,112 @@ struct chunk_reader
     }
     return v;
   }
-  __device__ __forceinline__ unsigned long long unary()
+  __device__ __forceinline__ unsigned long long unary(unsigned long long& pos) const
   {
     unsigned long long v = 0;
     for (;;)
     {
-      const unsigned long long w = peek() & ((1ull << 57) - 1);
-      if (w)
+      const unsigned long long x = peek(pos) & ((1ull << 57) - 1);
+      if (x)
       {
-        const int z = __ffsll((long long)w) - 1;
+        const int z = __ffsll((long long)x) - 1;
         pos += (unsigned long long)z + 1;
         return v + (unsigned long long)z;
       }
       v += 57;
       pos += 57;
-      if ((pos >> 3) > n)
+      if (pos >= hi + 8)
         return v;
     }
   }
-  __device__ __forceinline__ void next_byte() { pos = (pos + 7) & ~7ull; }
 };
 
-// Every brick of every chunk, a chunk per thread: PASS 0 the key range of its slot, PASS 1
-// the brick's data offset into the slot's row of the offset table.
+// The position just after the need-th set bit (need >= 1) of the bit string from pos (test
+// with flags() on each lane's 32 bits at pos + 32 lane), by the whole warp; or an end past
+// `limit` when the string ends first.
+template <typename Flags>
+__device__ __forceinline__ unsigned long long warp_find_nth(const chunk_bits& bb, unsigned long long pos,
+                                                            long long need, unsigned long long limit, int lane,
+                                                            Flags flags, int unit)
+{
+  while (need > 0)
+  {
+    const uint32_t f = flags((uint32_t)bb.peek(pos + 32ull * (unsigned long long)lane));
+    const int cnt = __popc(f);
+    int incl = cnt;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o)
+        incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total < need)
+    {
+      need -= total;
+      pos += 1024;
+      if (pos >= limit)
+        return pos;
+      continue;
+    }
+    const int L = __ffs(__ballot_sync(0xffffffffu, incl >= need)) - 1;
+    int j = 0;
+    if (lane == L)
+    {
+      uint32_t x = f;
+      for (long long r = need - (incl - cnt); r > 1; --r)
+        x &= x - 1;
+      j = __ffs(x) - 1;
+    }
+    j = __shfl_sync(0xffffffffu, j, L);
+    return pos + 32ull * (unsigned long long)L + (unsigned long long)(j + unit);
+  }
+  return pos;
+}
+
+// Every brick of every chunk, a warp per chunk: the ends of the gaps and of the sizes found
+// by the warp (counting one bits, then varbyte final bytes), the bricks walked by lane 0.
+// PASS 0 records the key range of each brick's slot, PASS 1 its data offset into the slot's
+// row of the offset table.
 template <int PASS>
 __global__ void __launch_bounds__(128) k_index_chunks(const index_args a)
 {
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.nchunks; c += gridDim.x * blockDim.x)
+  const int lane = threadIdx.x & 31;
+  for (int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); c < a.nchunks;
+       c += (int)((gridDim.x * blockDim.x) >> 5))
   {
     const index_chunk C = a.chunks[c];
-    chunk_reader cr{ a.blob + C.off, C.size, 0 };
-    const unsigned long long nbr64 = cr.varbyte();
+    const chunk_bits bb{ reinterpret_cast<const uint32_t*>(a.blob), (C.off + C.size) * 8ull };
+    unsigned long long pos = C.off * 8ull;
+    const unsigned long long nbr64 = bb.varbyte(pos);
     if (nbr64 > C.size * 8 + 1)
     {
-      atomicOr(a.error, 1);
+      if (lane == 0)
+        atomicOr(a.error, 1);
       continue;
     }
     const long long nbr = (long long)nbr64;
-    // the sizes follow the gaps (byte-aligned); the data follows the sizes
-    chunk_reader s = cr;
+    const unsigned long long dpos = pos;  // the first brick (varbyte), then the unary gaps
+    unsigned long long p = dpos;
     if (nbr > 0)
-    {
-      s.varbyte();
-      for (long long i = 1; i < nbr; ++i)
-        s.unary();
-    }
-    s.next_byte();
-    chunk_reader e = s;
-    for (long long i = 0; i < nbr; ++i)
-      e.varbyte();
-    const unsigned long long data = C.off + (e.pos >> 3);
+      bb.varbyte(p);
+    // past the nbr - 1 gaps (one bit each at its end), then to the next byte: the sizes
+    p = warp_find_nth(bb, p, nbr - 1, bb.hi + 8, lane, [](uint32_t x) { return x; }, 1);
+    const unsigned long long spos = (p + 7) & ~7ull;
+    // past the nbr sizes (a varbyte ends with a byte whose top bit is clear): the data
+    const unsigned long long q =
+      warp_find_nth(bb, spos, nbr, bb.hi + 8, lane, [](uint32_t x) { return ~x & 0x80808080u; }, 1);
+    const unsigned long long data = q >> 3;
+    if (lane != 0)
+      continue;
     const long long base = a.bmap_base[C.level & 15];
     const int msize = a.bmap_size[C.level & 15];
-    unsigned long long b = 0, acc = 0;
+    unsigned long long b = 0, acc = 0, dp = dpos, sp = spos;
     for (long long i = 0; i < nbr; ++i)
     {
-      b = i == 0 ? cr.varbyte() : b + cr.unary() + 1;
+      b = i == 0 ? bb.varbyte(dp) : b + bb.unary(dp) + 1;
       const unsigned long long o = acc;
-      acc += s.varbyte();
+      acc += bb.varbyte(sp);
       if (b >= (unsigned long long)msize)
         continue;
       const int flat = a.bmap[base + (long long)b];
@@ -446,7 +500,7 @@ int decode_device::build_index(device_ctx* ctx, const std::vector<index_chunk>& 
   a.nchan = d_sums + nblocks + 1;
   a.nslots = ns;
   a.error = d_err;
-  const int cgrid = (int)((chunks.size() + 127) / 128);
+  const int cgrid = (int)((chunks.size() + 3) / 4);  // a warp per chunk
   if (ns)
   {
     k_index_init<<<ns / 256 + 1 < 4096 ? (unsigned)(ns / 256 + 1) : 4096u, 256, 0, st>>>(a);
