@@ -74,8 +74,12 @@ void dpack_launch_write(const dpack_args& a, int grid, cudaStream_t st);
 constexpr int kDpackNotApplicable = -2;
 // The plan's segment tables are made and uploaded once and kept on the context for the next
 // encode of the same plan.
+// on_image (may be empty): called once the image's copy to the host is under way, with the
+// layout, the host image and the function that waits for a part of it to arrive.
+using image_hook = std::function<void(const dpack_layout&, const uint8_t*, const ready_fn&)>;
 int device_pack(device_ctx* ctx, const dataset_format& f, const std::shared_ptr<const encode_plan>& plan,
-                const std::vector<device_level_stream>& levels, packed_dataset* out);
+                const std::vector<device_level_stream>& levels, packed_dataset* out,
+                const image_hook& on_image = image_hook());
 
 // encode_dataset with the device packer: every level coded with its regions kept on the
 // device, packed there, and the files written. When the packer does not take a segment (more

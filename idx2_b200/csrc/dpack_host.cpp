@@ -7,7 +7,9 @@
 #include <algorithm>
 #include <chrono>
 #include <cstring>
+#include <fcntl.h>
 #include <thread>
+#include <unistd.h>
 
 namespace idx2g
 {
@@ -33,7 +35,7 @@ struct dpack_tables
 } // namespace
 
 int device_pack(device_ctx* ctx, const dataset_format& f, const std::shared_ptr<const encode_plan>& plan,
-                const std::vector<device_level_stream>& levels, packed_dataset* out)
+                const std::vector<device_level_stream>& levels, packed_dataset* out, const image_hook& on_image)
 {
   stage_timer tt;
   cudaStream_t st = ctx->stream;
@@ -192,11 +194,6 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const std::shared_ptr<
     if (!pev[i] || cudaEventRecord(pev[i], st) != cudaSuccess)
       return CudaError;
   }
-  if (cudaEventSynchronize(ex) != cudaSuccess)
-    return CudaError;
-  tt.lap("dpack.write");
-  e = dpack_finish(f, P, L, h_img, h_exps, out);
-  tt.lap("dpack.finish");
   const uint8_t* img = h_img;
   const unsigned long long total = L.total;
   out->ready = [pev, img, total](const uint8_t* p, size_t n) {
@@ -207,6 +204,14 @@ int device_pack(device_ctx* ctx, const dataset_format& f, const std::shared_ptr<
     for (size_t i = i0; i <= i1 && i < pev.size(); ++i)
       cudaEventSynchronize(pev[i]);
   };
+  out->image = h_img;
+  if (on_image)
+    on_image(L, h_img, out->ready);  // e.g. the chunk sections written while the rest is made
+  if (cudaEventSynchronize(ex) != cudaSuccess)
+    return CudaError;
+  tt.lap("dpack.write");
+  e = dpack_finish(f, P, L, h_img, h_exps, out);
+  tt.lap("dpack.finish");
   return e;
 }
 
@@ -242,8 +247,42 @@ int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_code
     lv[l].nsb = outs[l].nsb;
     lv[l].nexps = outs[l].nexps;
   }
+  // the chunk sections (most of every file) are written, on a thread, as their pieces arrive
+  // from the device, while the host compresses the exponent chunks and builds the tails
+  std::map<std::string, unsigned long long> sec_bytes;
+  std::map<std::string, file_buffer> sec_files;
+  int sec_err = NoError;
+  std::thread sections;
+  struct section_joiner  // (declared after what the thread uses: joined before those go)
+  {
+    std::thread& t;
+    ~section_joiner()
+    {
+      if (t.joinable())
+        t.join();
+    }
+  } join_sections{ sections };
+  const image_hook on_image = [&](const dpack_layout& L, const uint8_t* img, const ready_fn& ready) {
+    for (const auto& kv : L.file_span)
+    {
+      sec_bytes[kv.first] = kv.second.second;
+      file_buffer& fb = sec_files[kv.first];
+      constexpr unsigned long long kPiece = 16ull << 20;
+      for (unsigned long long o = 0; o < kv.second.second; o += kPiece)
+        fb.append_ref(img + kv.second.first + o,
+                      (size_t)(kv.second.second - o < kPiece ? kv.second.second - o : kPiece));
+    }
+    sections = std::thread([&, ready]() {
+      if (pre.joinable())
+        pre.join();
+      std::vector<std::pair<std::string, const file_buffer*>> wl;
+      for (auto& kv : sec_files)
+        wl.push_back({ kv.first, &kv.second });
+      sec_err = write_files(wl, &ready);
+    });
+  };
   packed_dataset pd;
-  e = device_pack(ctx, *f, plan_sp, lv, &pd);
+  e = device_pack(ctx, *f, plan_sp, lv, &pd, on_image);
   if (e && e != kDpackNotApplicable)
     cudaStreamSynchronize(ctx->stream);  // (no copy left running into the pinned image)
   if (e == kDpackNotApplicable)
@@ -264,12 +303,69 @@ int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_code
   if (timing)
     note_level_files(*f, plan, pd.files, timing);
   const double t2 = now();
-  e = write_dataset(f, p, pd.files, pack_stats_text(pd.stats), nullptr, true, timing, &pre, t2 - t1, &pd.ready);
-  // (every piece of the image has been waited for by now, unless the write failed first)
-  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess && !e)
-    e = CudaError;
+  if (sections.joinable())
+    sections.join();
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+    return CudaError;
+  if (sec_err)
+    return sec_err;
+  // the rest of every file after its chunk section, and the metadata file
+  const std::string meta = meta_text(*f, *p) + pack_stats_text(pd.stats);
+  e = write_file(p->out_dir + "/" + p->name + "/" + p->field + ".idx2", std::vector<uint8_t>(meta.begin(), meta.end()));
+  unsigned long long total = meta.size();
+  for (auto& kv : pd.files)
+  {
+    if (e)
+      break;
+    const file_buffer& fb = kv.second;
+    total += fb.nbytes;
+    const unsigned long long skip = sec_bytes.count(kv.first) ? sec_bytes[kv.first] : 0;
+    if (!skip && make_dirs_for(kv.first) != NoError)
+    {
+      e = CannotCreateDirectory;
+      break;
+    }
+    const int fd = open(kv.first.c_str(), O_RDWR | O_CREAT | (skip ? 0 : O_TRUNC), 0644);
+    if (fd < 0)
+    {
+      e = FileCreateFailed;
+      break;
+    }
+    unsigned long long at = 0;
+    fb.for_each_segment([&](const segment& sg) {
+      if (e)
+        return;
+      const unsigned long long a0 = at, a1 = at + sg.n;
+      at = a1;
+      if (a1 <= skip)
+        return;  // in the chunk section, written already
+      const unsigned long long from = a0 < skip ? skip - a0 : 0;
+      size_t done = (size_t)from;
+      while (done < sg.n)
+      {
+        const ssize_t w = pwrite(fd, sg.p + done, sg.n - done, (off_t)(a0 + done));
+        if (w <= 0)
+        {
+          e = FileWriteFailed;
+          return;
+        }
+        done += (size_t)w;
+      }
+    });
+    if (!e && ftruncate(fd, (off_t)fb.nbytes) != 0)
+      e = FileWriteFailed;
+    if (close(fd) != 0 && !e)
+      e = FileWriteFailed;
+  }
+  const double t3 = now();
   if (timing)
+  {
     timing->device_s = t1 - t0;
+    timing->pack_s = t2 - t1;
+    timing->write_s = t3 - t2;
+    timing->file_bytes = total;
+    timing->nfiles = (int)pd.files.size() + 1;
+  }
   return e;
 }
 
