@@ -330,6 +330,9 @@ def ours_sharded(args, rank, world, local_rank):
     dist.init_process_group(args.dist_backend, timeout=datetime.timedelta(seconds=120))
     note("process group up")
     stream = torch.cuda.Stream(device=dev)
+    note("stream")
+    _lib.lib()
+    note("library loaded")
     _lib.ctx_on_stream(local_rank, stream)  # the library's work on a stream the events can bracket
     note("context")
     side = args.side
