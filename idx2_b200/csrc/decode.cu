@@ -614,8 +614,17 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
   uint64_t* d_geom = (uint64_t*)ctx->ws("dec.geom", sizeof(uint64_t) * 8 * kMaxBlocksPerSubband);
   if (!d_err || !d_geom)
     return OutOfMemory;
-  const size_t smem = sizeof(dec_smem);
-  cudaFuncSetAttribute(k_decode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the plane-table path's shared memory (float staging rows for a float32 output), and the
+  // three-CTA build for an output level of many bricks with a float32 output
+  const size_t smem = dec_smem_bytes(true, r0.f32);
+  cudaFuncSetAttribute(k_decode_level<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(dec_smem));
+  cudaFuncSetAttribute(k_decode_level<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(dec_smem));
+  int occ3 = 0;
+  if (r0.f32 && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_decode_level<3>, kThreads, smem) != cudaSuccess)
+  {
+    cudaGetLastError();
+    occ3 = 0;
+  }
   // The levels run back to back without the host waiting in between: the host prepares a
   // level's tables while the previous level runs (stream order protects the device tables
   // that every level reuses), the plane kernels' error flags are read once at the end, and a
@@ -715,7 +724,12 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         keep->bricks[(size_t)l] = d_level;
         keep->sig[(size_t)l].assign((size_t)nstore, 0);
       }
-      int grid = nbr < 2 * ctx->num_sms ? nbr : 2 * ctx->num_sms;
+      bool three = false;
+      for (const decode_target& t : targets)
+        three = three || t.is_output;
+      three = three && occ3 >= 3 && nbr >= 6 * ctx->num_sms;
+      const int cps = three ? 3 : 2;
+      int grid = nbr < cps * ctx->num_sms ? nbr : cps * ctx->num_sms;
       double* d_slots = (double*)ctx->ws("dec.slots", (size_t)grid * (size_t)NB * 8);
       if (!d_bricks || !d_reqs || (nstore && !d_level) || !d_slots)
         return OutOfMemory;
@@ -866,7 +880,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
           ag.nbricks = cuts[g + 1] - cuts[g];
           ag.unit_off = d_uoff + (size_t)cuts[g] * (size_t)r0.nsb;
           const int gg = ag.nbricks < grid ? ag.nbricks : grid;
-          k_decode_level<<<gg, kThreads, smem, st>>>(ag);
+          (three ? k_decode_level<3> : k_decode_level<2>)<<<gg, kThreads, smem, st>>>(ag);
           ++ctx->launches;
           const size_t z_next =
             g + 2 < cuts.size() ? (size_t)hb[(size_t)cuts[g + 1]].dst_from[2] : (size_t)r0.out_dims.z;
@@ -886,7 +900,7 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
       }
       else
       {
-        k_decode_level<<<grid, kThreads, smem, st>>>(a);
+        (three ? k_decode_level<3> : k_decode_level<2>)<<<grid, kThreads, smem, st>>>(a);
         ctx->launches += 3;
       }
       cudaEventRecord(t1, st);
@@ -1075,7 +1089,7 @@ int scratch_address(int device, unsigned char** out)
 int noalloc_prepare(int device)
 {
   cudaFuncAttributes fa;
-  if (cudaFuncGetAttributes(&fa, k_decode_level) != cudaSuccess)
+  if (cudaFuncGetAttributes(&fa, k_decode_level<2>) != cudaSuccess)
     return CudaError;
   unsigned char* base = nullptr;
   return scratch_address(device, &base);
@@ -1125,7 +1139,7 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
   cudaMemsetAsync(d_out, 0, out_bytes, st);
   cudaMemsetAsync(d_err, 0, 16, st);
   const size_t smem = sizeof(dec_smem);
-  cudaFuncSetAttribute(k_decode_level, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_decode_level<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   float total_ms = 0;
   double* prev = nullptr;
   int li = 0;
@@ -1179,7 +1193,7 @@ int decode_device::decode_noalloc(device_ctx* ctx, const decode_request& rq, voi
     a.error = d_err;
     (void)NB;
     cudaEventRecord(ctx->ev0, st);
-    k_decode_level<<<grid, kThreads, smem, st>>>(a);
+    k_decode_level<2><<<grid, kThreads, smem, st>>>(a);
     ++ctx->launches;
     cudaEventRecord(ctx->ev1, st);
     if (cudaGetLastError() != cudaSuccess)

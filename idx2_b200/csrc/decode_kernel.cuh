@@ -90,18 +90,12 @@ struct dec1_args
   int* wide_list;
 };
 
+// The union comes last: a launch of the plane-table path with a float32 output needs only its
+// float staging rows, and passes a dynamic shared-memory size that ends there
+// (dec_smem_bytes).
 struct dec_smem
 {
-  union
-  {
-    unsigned long long coef[kMaxBlocksPerSubband][64];  // CTA-wide path: one subband
-    unsigned long long ring[kWarps][kRing][32];         // warp path: decoded planes in flight
-    struct
-    {
-      double v[kWarps][32][33];     // output rows of the X sweep, one per lane
-      long long base[kWarps][32];   // their offsets in the output (-1: no output)
-    } out;
-  } u;
+  long long out_base[kWarps][32];  // offsets in the output of the staged rows (-1: no output)
   long long q[kWarps][2][80];  // per-warp block scratch (two blocks, padded in the table path)
   int16_t emax[8][kMaxBlocksPerSubband];
   int16_t ktop[8][kMaxBlocksPerSubband];
@@ -118,7 +112,23 @@ struct dec_smem
   int wide;
   int sig;           // a block of a subband > 0 (or of the coarsest level) was decoded
   decode_target rq;  // the current brick's request
+  union
+  {
+    double v[kWarps][32][33];   // output rows of the X sweep, one per lane (float64 output)
+    float v32[kWarps][32][33];  // the same cast to float (float32 output)
+    unsigned long long coef[kMaxBlocksPerSubband][64];  // CTA-wide path: one subband
+    unsigned long long ring[kWarps][kRing][32];         // warp path: decoded planes in flight
+  } u;
 };
+
+// Dynamic shared memory of a launch: all of dec_smem, or, for the plane-table path with a
+// float32 output, up to the end of the float staging rows.
+inline size_t dec_smem_bytes(bool planes, bool out_f32)
+{
+  if (planes && out_f32)
+    return offsetof(dec_smem, u) + sizeof(float) * kWarps * 32 * 33;
+  return sizeof(dec_smem);
+}
 
 __device__ __forceinline__ void unpack_geom(uint64_t g, int d3[3], int bd[3])
 {
@@ -716,7 +726,8 @@ __device__ __forceinline__ void ilift_streams(double* c0, double* c1, bool n0, d
     ((k & 1) ? c1 : c0)[(k >> 1) * ST] = v[k];
 }
 
-__global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
+template <int CPS>
+__global__ void __launch_bounds__(kThreads, CPS) k_decode_level(const dec_args a)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   dec_smem& sm = *reinterpret_cast<dec_smem*>(smem_raw);
@@ -1297,33 +1308,34 @@ __global__ void __launch_bounds__(kThreads, 2) k_decode_level(const dec_args a)
         for (int x = 0; x < 33; ++x)
           v[x] = (x & 1) ? r1[x >> 1] : r0[x >> 1];
         ilift33(v);
-        double* dst = rq.is_output ? sm.u.out.v[warp][lane] : nullptr;
 #pragma unroll
         for (int x = 0; x < 33; ++x)
         {
-          if (rq.is_output)
-            dst[x] = v[x];
-          else
+          if (!rq.is_output)
             ((x & 1) ? r1 : r0)[x >> 1] = v[x];
+          else if (a.out_f32)
+            sm.u.v32[warp][lane][x] = __double2float_rn(v[x]);
+          else
+            sm.u.v[warp][lane][x] = v[x];
         }
       }
       if (rq.is_output)
       {
         // the warp's rows, lanes along x
-        sm.u.out.base[warp][lane] = obase;
+        sm.out_base[warp][lane] = obase;
         __syncwarp();
         const int n0 = br.dims[0];
         for (int r = 0; r < 32; ++r)
         {
-          const long long ob = sm.u.out.base[warp][r];
+          const long long ob = sm.out_base[warp][r];
           if (ob < 0 || lane >= n0)
             continue;
           const long long di = ob + (long long)lane * br.dst_strd[0];
-          const double val = sm.u.out.v[warp][r][br.src_from[0] + lane * br.src_strd[0]];
+          const int sx = br.src_from[0] + lane * br.src_strd[0];
           if (a.out_f32)
-            ((float*)rq.out)[di] = __double2float_rn(val);
+            ((float*)rq.out)[di] = sm.u.v32[warp][r][sx];
           else
-            ((double*)rq.out)[di] = val;
+            ((double*)rq.out)[di] = sm.u.v[warp][r][sx];
         }
         __syncwarp();
       }
