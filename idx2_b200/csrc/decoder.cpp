@@ -656,6 +656,8 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
     for (int s = 0; s < nsb; ++s)
       for (int d = 0; d < 3; ++d)
         lv.spacing[s][d] = f.decode_spacings[(size_t)l][(size_t)s][d];
+    // the exponent chunk of each subband that was found last (bricks of a chunk come in runs)
+    std::vector<u64> chunk_seen((size_t)nsb, ~0ull);
     for (int bz = bf.z; bz <= bl.z; ++bz)
       for (int by = bf.y; by <= bl.y; ++by)
         for (int bx = bf.x; bx <= bl.x; ++bx)
@@ -677,8 +679,16 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
               return bf->second;
           }
           for (int s = 0; s < nsb; ++s)
-            if (((lv.mask >> s) & 1) && !h->exp_chunk_addrs.count(chunk_address(f, lin, l, s, 0)))
+          {
+            if (!((lv.mask >> s) & 1))
+              continue;
+            const u64 ca = chunk_address(f, lin, l, s, 0);
+            if (ca == chunk_seen[(size_t)s])
+              continue;
+            if (!h->exp_chunk_addrs.count(ca))
               return ChunkNotFound;
+            chunk_seen[(size_t)s] = ca;
+          }
           decode_brick db;
           db.flat = (long long)(h->level_brick_base[(size_t)l] + (size_t)bi);
           db.parent = -1;

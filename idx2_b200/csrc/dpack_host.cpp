@@ -273,12 +273,14 @@ int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_code
                       (size_t)(kv.second.second - o < kPiece ? kv.second.second - o : kPiece));
     }
     sections = std::thread([&, ready]() {
+      stage_timer ts;
       if (pre.joinable())
         pre.join();
       std::vector<std::pair<std::string, const file_buffer*>> wl;
       for (auto& kv : sec_files)
         wl.push_back({ kv.first, &kv.second });
       sec_err = write_files(wl, &ready);
+      ts.lap("write.sections (thread)");
     });
   };
   packed_dataset pd;
@@ -303,12 +305,14 @@ int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_code
   if (timing)
     note_level_files(*f, plan, pd.files, timing);
   const double t2 = now();
+  stage_timer tw;
   if (sections.joinable())
     sections.join();
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess)
     return CudaError;
   if (sec_err)
     return sec_err;
+  tw.lap("write.sections_wait");
   // the rest of every file after its chunk section, and the metadata file
   const std::string meta = meta_text(*f, *p) + pack_stats_text(pd.stats);
   e = write_file(p->out_dir + "/" + p->name + "/" + p->field + ".idx2", std::vector<uint8_t>(meta.begin(), meta.end()));
@@ -358,6 +362,7 @@ int encode_dataset_dpack(device_ctx* ctx, dataset_format* f, params* p, gpu_code
       e = FileWriteFailed;
   }
   const double t3 = now();
+  tw.lap("write.tails");
   if (timing)
   {
     timing->device_s = t1 - t0;

@@ -3,6 +3,7 @@
 #include "dpack.h"
 
 #include "parallel.h"
+#include "trace.h"
 
 #include <algorithm>
 #include <atomic>
@@ -263,6 +264,7 @@ int dpack_make_layout(const dataset_format& f, const dpack_plan& P, const std::v
 int dpack_finish(const dataset_format& f, const dpack_plan& P, const dpack_layout& L, const uint8_t* image,
                  const uint8_t* exps, packed_dataset* out)
 {
+  stage_timer tt;
   std::map<std::string, file_buffer>& files = out->files;
   pack_stats& stats = out->stats;
   const uint8_t* h_img = image;
@@ -330,6 +332,7 @@ int dpack_finish(const dataset_format& f, const dpack_plan& P, const dpack_layou
   });
   if (zerr)
     return zerr;
+  tt.lap("dpack.finish.exps");
   for (size_t i = 0; i < erecs.size(); ++i)
   {
     const uint8_t* p;
@@ -413,6 +416,7 @@ int dpack_finish(const dataset_format& f, const dpack_plan& P, const dpack_layou
     put_i32(&tail, (int32_t)tot);
     fb.append_owned(std::move(tail));
   }
+  tt.lap("dpack.finish.tails");
   return NoError;
 }
 

@@ -196,6 +196,7 @@ std::thread preallocate_files(const dataset_format& f, const encode_plan& plan,
   if (todo.empty())
     return std::thread();
   return std::thread([todo]() {
+    stage_timer tt;
     // the writer sets each file's size and writes every byte, so pages of an older file of
     // the same name are as good as new ones
     for (const auto& t : todo)
@@ -209,6 +210,7 @@ std::thread preallocate_files(const dataset_format& f, const encode_plan& plan,
         errno = 0;
       close(fd);
     }
+    tt.lap("write.prealloc (thread)");
   });
 }
 

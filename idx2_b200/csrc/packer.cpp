@@ -17,6 +17,7 @@
 #include <fcntl.h>
 #include <sys/mman.h>
 #include <sys/stat.h>
+#include <mutex>
 #include <thread>
 #include <unistd.h>
 
@@ -197,6 +198,37 @@ void file_buffer::append_run(const segment* s, size_t n, size_t bytes)
   nbytes += bytes;
 }
 
+namespace
+{
+
+// Unmaps a written file's mapping on a thread of its own (tearing down the page tables of a
+// 1 GB mapping takes some 15 ms); one at a time, the last one joined at exit.
+struct unmapper
+{
+  std::mutex m;
+  std::thread t;
+  void later(uint8_t* p, size_t n)
+  {
+    std::lock_guard<std::mutex> g(m);
+    if (t.joinable())
+      t.join();
+    t = std::thread([p, n]() { munmap(p, n); });
+  }
+  ~unmapper()
+  {
+    if (t.joinable())
+      t.join();
+  }
+};
+
+unmapper& unmap_queue()
+{
+  static unmapper u;
+  return u;
+}
+
+} // namespace
+
 int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& files, const ready_fn* ready)
 {
   // Every file is cut into ranges of whole runs of about kRange bytes, copied by a pool of
@@ -213,42 +245,40 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
   };
   std::vector<int> fds(files.size(), -1);
   std::vector<uint8_t*> maps(files.size(), nullptr);
+  std::vector<size_t> map_len(files.size(), 0);
   std::vector<range> ranges;
   int err = NoError;
-  for (size_t i = 0; i < files.size() && !err; ++i)
-  {
+  // opens file i (its size set and pages allocated when it is mapped); 0 or an error code
+  auto open_file = [&](size_t i, size_t total) -> int {
     if (make_dirs_for(files[i].first) != NoError)
-    {
-      err = CannotCreateDirectory;
-      break;
-    }
-    const size_t total = files[i].second->nbytes;
+      return CannotCreateDirectory;
     // a large file keeps the pages it has (every byte is written, the size set first)
     fds[i] = open(files[i].first.c_str(), O_RDWR | O_CREAT | (total >= kMapMin ? 0 : O_TRUNC), 0644);
     if (fds[i] < 0)
-    {
-      err = FileCreateFailed;
-      break;
-    }
-    if (total >= kMapMin && ftruncate(fds[i], (off_t)total) != 0)
-    {
-      err = FileWriteFailed;
-      break;
-    }
+      return FileCreateFailed;
+    if (total < kMapMin)
+      return NoError;
+    if (ftruncate(fds[i], (off_t)total) != 0)
+      return FileWriteFailed;
     // pages for the whole file in one call, unless it has them already (allocated ahead, or
     // an older file's): a second allocation over allocated pages costs more than it saves
     struct stat sb;
-    if (total >= kMapMin && (fstat(fds[i], &sb) != 0 || (size_t)sb.st_blocks * 512 < total) &&
-        fallocate(fds[i], 0, 0, (off_t)total) != 0)
+    if ((fstat(fds[i], &sb) != 0 || (size_t)sb.st_blocks * 512 < total) && fallocate(fds[i], 0, 0, (off_t)total) != 0)
       errno = 0;  // pages come with the copies' page faults instead
-    if (total >= kMapMin)
+    void* m = mmap(nullptr, total, PROT_WRITE, MAP_SHARED, fds[i], 0);
+    if (m != MAP_FAILED)
     {
-      void* m = mmap(nullptr, total, PROT_WRITE, MAP_SHARED, fds[i], 0);
-      if (m != MAP_FAILED)
-        maps[i] = (uint8_t*)m;
-      else if (ftruncate(fds[i], 0) != 0)
-        err = FileWriteFailed;
+      maps[i] = (uint8_t*)m;
+      map_len[i] = total;
     }
+    else if (ftruncate(fds[i], 0) != 0)
+      return FileWriteFailed;
+    return NoError;
+  };
+  for (size_t i = 0; i < files.size() && !err; ++i)
+  {
+    if ((err = open_file(i, files[i].second->nbytes)) != NoError)
+      break;
     const std::vector<segment_run>& parts = files[i].second->parts;
     size_t off = 0, start = 0, acc = 0;
     for (size_t k = 0; k < parts.size(); ++k)
@@ -327,8 +357,8 @@ int write_files(const std::vector<std::pair<std::string, const file_buffer*>>& f
     err = werr;
   }
   for (size_t i = 0; i < files.size(); ++i)
-    if (maps[i] && munmap(maps[i], files[i].second->nbytes) != 0 && !err)
-      err = FileWriteFailed;
+    if (maps[i])
+      unmap_queue().later(maps[i], map_len[i]);
   for (int fd : fds)
     if (fd >= 0 && close(fd) != 0 && !err)
       err = FileWriteFailed;

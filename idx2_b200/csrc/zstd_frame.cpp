@@ -88,33 +88,53 @@ u32 ml_code(u32 mlb)
 
 struct bit_writer
 {
+  // The stream goes to out[start, pos); out is grown ahead in steps (its tail past pos is
+  // scratch until close() cuts it), so that the accumulator's whole bytes are stored with one
+  // 8-byte store.
   std::vector<u8>* out;
-  size_t start;
+  size_t start, pos;
   u64 acc = 0;
-  unsigned n = 0;
-  explicit bit_writer(std::vector<u8>* o) : out(o), start(o->size()) {}
-  void add(u64 v, unsigned nb)
+  unsigned n = 0;  // bits held in acc
+  explicit bit_writer(std::vector<u8>* o) : out(o), start(o->size()), pos(o->size()) { grow(); }
+  void grow()
   {
-    if (!nb)
-      return;
+    constexpr size_t kStep = 4096;
+    out->resize(pos + kStep);
+  }
+  // nb bits of v, not stored yet (n + nb <= 64)
+  void put(u64 v, unsigned nb)
+  {
     acc |= (v & ((1ull << nb) - 1)) << n;
     n += nb;
-    while (n >= 8)
-    {
-      out->push_back((u8)acc);
-      acc >>= 8;
-      n -= 8;
-    }
+  }
+  // stores the whole bytes held; fewer than 8 bits stay
+  void flush()
+  {
+    if (pos + 8 > out->size())
+      grow();
+    memcpy(out->data() + pos, &acc, 8);
+    const unsigned nbytes = n >> 3;
+    pos += nbytes;
+    acc = nbytes == 8 ? 0 : acc >> (8 * nbytes);
+    n &= 7;
+  }
+  void add(u64 v, unsigned nb)  // nb <= 32
+  {
+    put(v, nb);
+    if (n >= 32)
+      flush();
   }
   // the end mark (one 1 bit) and the last partial byte; returns the stream's size
   size_t close()
   {
-    add(1, 1);
+    put(1, 1);
+    flush();
     if (n)
-      out->push_back((u8)acc);
+      (*out)[pos++] = (u8)acc;
     acc = 0;
     n = 0;
-    return out->size() - start;
+    out->resize(pos);
+    return pos - start;
   }
 };
 
@@ -457,26 +477,37 @@ void fse_build_rle(fse_table* t, u32 sym)
 struct fse_state
 {
   long long value;
-  const fse_table* t;
+  const u16* next;
+  const int* find;
+  const u32* nbdelta;
+  u32 log;
 };
 
 fse_state fse_start(const fse_table& t, u32 sym)
 {
-  fse_state st{ (long long)1 << t.log, &t };
+  fse_state st{ (long long)1 << t.log, t.next.data(), t.find.data(), t.nbdelta.data(), t.log };
   const u32 nb = (t.nbdelta[sym] + (1u << 15)) >> 16;
   const u32 v = (nb << 16) - t.nbdelta[sym];
   st.value = t.next[(size_t)((long long)(v >> nb) + t.find[sym])];
   return st;
 }
 
-void fse_encode(bit_writer& bw, fse_state& st, u32 sym)
+inline void fse_encode(bit_writer& bw, fse_state& st, u32 sym)
 {
-  const u32 nb = (u32)((st.value + (long long)st.t->nbdelta[sym]) >> 16);
+  const u32 nb = (u32)((st.value + (long long)st.nbdelta[sym]) >> 16);
   bw.add((u64)st.value, nb);
-  st.value = st.t->next[(size_t)((st.value >> nb) + st.t->find[sym])];
+  st.value = st.next[(size_t)((st.value >> nb) + st.find[sym])];
 }
 
-void fse_finish(bit_writer& bw, const fse_state& st) { bw.add((u64)st.value, st.t->log); }
+// as fse_encode, the bits left in the accumulator (room for them is the caller's)
+inline void fse_put(bit_writer& bw, fse_state& st, u32 sym)
+{
+  const u32 nb = (u32)((st.value + (long long)st.nbdelta[sym]) >> 16);
+  bw.put((u64)st.value, nb);
+  st.value = st.next[(size_t)((st.value >> nb) + st.find[sym])];
+}
+
+void fse_finish(bit_writer& bw, const fse_state& st) { bw.add((u64)st.value, st.log); }
 
 // FSE compression of a small byte array with two interleaved states (Huffman weights).
 // Returns the stream size, or 0 when the input is too short.
@@ -1112,17 +1143,25 @@ size_t block_body(std::vector<u8>* out, const std::vector<sequence>& seqs, const
       fse_state sml = fse_start(tml, mlc[l]);
       fse_state sof = fse_start(tof, ofc[l]);
       fse_state sll = fse_start(tll, llc[l]);
-      bw.add(seqs[l].ll, kLLBits[llc[l]]);
-      bw.add(seqs[l].mlb, kMLBits[mlc[l]]);
-      bw.add(seqs[l].off, ofc[l]);
+      // (bit budget between flushes, at most 7 bits held after one: the three states take
+      // at most 8 + 9 + 9 bits, the literal and match length bits at most 16 each, the
+      // offset bits at most 31)
+      bw.put(seqs[l].ll, kLLBits[llc[l]]);
+      bw.put(seqs[l].mlb, kMLBits[mlc[l]]);
+      bw.flush();
+      bw.put(seqs[l].off, ofc[l]);
+      bw.flush();
       for (size_t n = nseq - 1; n-- > 0;)
       {
-        fse_encode(bw, sof, ofc[n]);
-        fse_encode(bw, sml, mlc[n]);
-        fse_encode(bw, sll, llc[n]);
-        bw.add(seqs[n].ll, kLLBits[llc[n]]);
-        bw.add(seqs[n].mlb, kMLBits[mlc[n]]);
-        bw.add(seqs[n].off, ofc[n]);
+        fse_put(bw, sof, ofc[n]);
+        fse_put(bw, sml, mlc[n]);
+        fse_put(bw, sll, llc[n]);
+        bw.flush();
+        bw.put(seqs[n].ll, kLLBits[llc[n]]);
+        bw.put(seqs[n].mlb, kMLBits[mlc[n]]);
+        bw.flush();
+        bw.put(seqs[n].off, ofc[n]);
+        bw.flush();
       }
       fse_finish(bw, sml);
       fse_finish(bw, sof);
@@ -1154,10 +1193,11 @@ struct matcher
   std::vector<u32> hash;
   u32 hlog, mls, wlog;
   const u8* data;  // the frame's input; byte p has index p + 1
+  template <u32 MLS>
   size_t hpos(size_t p) const
   {
     const u8* q = data + p;
-    switch (mls)
+    switch (MLS)
     {
       case 5:
         return (size_t)(((rd64(q) << (64 - 40)) * 889523592379ull) >> (64 - hlog));
@@ -1171,9 +1211,17 @@ struct matcher
         return (size_t)((rd32(q) * 2654435761u) >> (32 - hlog));
     }
   }
+  // length of the common run of positions a and b (b < a), up to limit; 8 bytes at a time
   size_t count(size_t a, size_t b, size_t limit) const
   {
     size_t n = 0;
+    while (a + n + 8 <= limit)
+    {
+      const u64 x = rd64(data + a + n) ^ rd64(data + b + n);
+      if (x)
+        return n + ((size_t)__builtin_ctzll(x) >> 3);
+      n += 8;
+    }
     while (a + n < limit && data[a + n] == data[b + n])
       n++;
     return n;
@@ -1182,6 +1230,34 @@ struct matcher
   // Sequences of block [bs, be); the trailing literals are lits' tail. rep: the two repeat
   // offsets in and out.
   void block(size_t bs, size_t be, u32 rep[2], std::vector<sequence>* seqs, std::vector<u8>* lits)
+  {
+    // room for the worst case (a sequence per 4 bytes, every byte a literal), cut after
+    seqs->resize((be - bs) / 3 + 2);
+    lits->resize(be - bs + 8);
+    size_t ns = 0, nl = 0;
+    switch (mls)
+    {
+      case 5:
+        run<5>(bs, be, rep, seqs->data(), &ns, lits->data(), &nl);
+        break;
+      case 6:
+        run<6>(bs, be, rep, seqs->data(), &ns, lits->data(), &nl);
+        break;
+      case 7:
+        run<7>(bs, be, rep, seqs->data(), &ns, lits->data(), &nl);
+        break;
+      case 8:
+        run<8>(bs, be, rep, seqs->data(), &ns, lits->data(), &nl);
+        break;
+      default:
+        run<4>(bs, be, rep, seqs->data(), &ns, lits->data(), &nl);
+    }
+    seqs->resize(ns);
+    lits->resize(nl);
+  }
+
+  template <u32 MLS>
+  void run(size_t bs, size_t be, u32 rep[2], sequence* seq_out, size_t* nseq, u8* lit_out, size_t* nlit)
   {
     const long long end_index = (long long)be + 1;
     const long long max_dist = 1ll << wlog;
@@ -1207,14 +1283,16 @@ struct matcher
         off1 = 0;
       }
     }
+    size_t ns = 0, nl = 0;
     auto store = [&](long long ll, long long from, u32 off_value, long long mlb) {
-      lits->insert(lits->end(), data + from, data + from + ll);
-      seqs->push_back({ (u32)ll, (u32)mlb, off_value });
+      memcpy(lit_out + nl, data + from, (size_t)ll);
+      nl += (size_t)ll;
+      seq_out[ns++] = sequence{ (u32)ll, (u32)mlb, off_value };
     };
     while (ip1 < ilimit)
     {
       const long long ip2 = ip0 + 2;
-      const size_t h0 = hpos((size_t)ip0), h1 = hpos((size_t)ip1);
+      const size_t h0 = hpos<MLS>((size_t)ip0), h1 = hpos<MLS>((size_t)ip1);
       const u32 val0 = rd32(data + ip0), val1 = rd32(data + ip1);
       const u32 cur0 = (u32)(ip0 + 1), cur1 = (u32)(ip1 + 1);
       const u32 mi0 = hash[h0], mi1 = hash[h1];
@@ -1270,13 +1348,13 @@ struct matcher
       ip1 = ip0 + 1;
       if (ip0 <= ilimit)
       {
-        hash[hpos((size_t)cur0 + 1)] = cur0 + 2;
-        hash[hpos((size_t)(ip0 - 2))] = (u32)(ip0 - 1);
+        hash[hpos<MLS>((size_t)cur0 + 1)] = cur0 + 2;
+        hash[hpos<MLS>((size_t)(ip0 - 2))] = (u32)(ip0 - 1);
         while (ip0 <= ilimit && off2 > 0 && rd32(data + ip0) == rd32(data + ip0 - off2))
         {
           const long long rlen = (long long)count((size_t)(ip0 + 4), (size_t)(ip0 + 4 - off2), (size_t)iend) + 4;
           std::swap(off1, off2);
-          hash[hpos((size_t)ip0)] = (u32)(ip0 + 1);
+          hash[hpos<MLS>((size_t)ip0)] = (u32)(ip0 + 1);
           ip0 += rlen;
           ip1 = ip0 + 1;
           store(0, anchor, 1, rlen - 3);
@@ -1286,7 +1364,10 @@ struct matcher
     }
     rep[0] = off1 ? off1 : saved;
     rep[1] = off2 ? off2 : saved;
-    lits->insert(lits->end(), data + anchor, data + iend);
+    memcpy(lit_out + nl, data + anchor, (size_t)(iend - anchor));
+    nl += (size_t)(iend - anchor);
+    *nseq = ns;
+    *nlit = nl;
   }
 };
 
