@@ -279,13 +279,76 @@ __device__ __forceinline__ unsigned long long warp_find_nth(const chunk_bits& bb
   return pos;
 }
 
-// Every brick of every chunk, a warp per chunk: the ends of the gaps and of the sizes found
-// by the warp (counting one bits, then varbyte final bytes), the bricks walked by lane 0.
+// Position of the r-th set bit (1 <= r <= popc(x)) of x, by halving.
+__device__ __forceinline__ int nth_set_bit(uint32_t x, int r)
+{
+  int pos = 0;
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1)
+  {
+    const int c = __popc(x & ((1u << s) - 1u));
+    if (c < r)
+    {
+      r -= c;
+      x >>= s;
+      pos += s;
+    }
+  }
+  return pos;
+}
+
+// For each lane, the position just after the rr-th set bit (rr >= 1; rr = 0 gives cur) of the
+// bit string from cur (flags() on each lane's 32 bits of a 1024-bit window); ~0 where the
+// string reaches `limit` first. Every lane of the warp takes part.
+template <typename Flags>
+__device__ __forceinline__ unsigned long long warp_nth_each(const chunk_bits& bb, unsigned long long cur, int rr,
+                                                            unsigned long long limit, int lane, Flags flags)
+{
+  constexpr unsigned long long kNone = ~0ull;
+  unsigned long long res = rr == 0 ? cur : kNone;
+  int need = rr;
+  for (unsigned long long base = cur; __any_sync(0xffffffffu, res == kNone) && base < limit; base += 1024)
+  {
+    const uint32_t f = flags((uint32_t)bb.peek(base + 32ull * (unsigned long long)lane));
+    const int cnt = __popc(f);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o)
+        incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const bool here = res == kNone && need <= total;
+    const int r = here ? need : 1;
+    // the first lane whose inclusive count reaches r
+    int lo = 0;
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1)
+      if (__shfl_sync(0xffffffffu, incl, lo + st - 1) < r)
+        lo += st;
+    lo = lo < 31 ? lo : 31;
+    const uint32_t fw = __shfl_sync(0xffffffffu, f, lo);
+    const int before = __shfl_sync(0xffffffffu, incl - cnt, lo);
+    if (here)
+      res = base + 32ull * (unsigned long long)lo + (unsigned long long)nth_set_bit(fw, r - before) + 1ull;
+    else if (res == kNone)
+      need -= total;
+  }
+  return res;
+}
+
+// Every brick of every chunk, a warp per chunk and a lane per brick, 32 bricks at a time: the
+// bricks from the unary gaps (brick i > 0 is the first brick plus the bits up to the end of
+// the i-th gap), the sizes from the varbyte final bytes (each lane decodes its own) and their
+// exclusive sums for the data offsets (Core/idx2Decode.cpp:507-540 DecompressChunk).
 // PASS 0 records the key range of each brick's slot, PASS 1 its data offset into the slot's
 // row of the offset table.
 template <int PASS>
 __global__ void __launch_bounds__(128) k_index_chunks(const index_args a)
 {
+  constexpr unsigned long long kNone = ~0ull;
   const int lane = threadIdx.x & 31;
   for (int c = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); c < a.nchunks;
        c += (int)((gridDim.x * blockDim.x) >> 5))
@@ -301,27 +364,66 @@ __global__ void __launch_bounds__(128) k_index_chunks(const index_args a)
       continue;
     }
     const long long nbr = (long long)nbr64;
-    const unsigned long long dpos = pos;  // the first brick (varbyte), then the unary gaps
-    unsigned long long p = dpos;
-    if (nbr > 0)
-      bb.varbyte(p);
-    // past the nbr - 1 gaps (one bit each at its end), then to the next byte: the sizes
-    p = warp_find_nth(bb, p, nbr - 1, bb.hi + 8, lane, [](uint32_t x) { return x; }, 1);
-    const unsigned long long spos = (p + 7) & ~7ull;
-    // past the nbr sizes (a varbyte ends with a byte whose top bit is clear): the data
-    const unsigned long long q =
-      warp_find_nth(bb, spos, nbr, bb.hi + 8, lane, [](uint32_t x) { return ~x & 0x80808080u; }, 1);
-    const unsigned long long data = q >> 3;
-    if (lane != 0)
+    if (nbr == 0)
       continue;
+    unsigned long long gpos = pos;
+    const unsigned long long first = bb.varbyte(gpos);  // then the unary gaps from gpos
+    const unsigned long long gstart = gpos;
+    const unsigned long long limit = bb.hi + 8;
+    unsigned long long spos = 0, data = 0;
+    if (PASS == 1)
+    {
+      // past the nbr - 1 gaps, then to the next byte: the sizes; past those: the data
+      const unsigned long long p = warp_find_nth(bb, gstart, nbr - 1, limit, lane, [](uint32_t x) { return x; }, 1);
+      spos = (p + 7) & ~7ull;
+      data = warp_find_nth(bb, spos, nbr, limit, lane, [](uint32_t x) { return ~x & 0x80808080u; }, 1) >> 3;
+    }
     const long long base = a.bmap_base[C.level & 15];
     const int msize = a.bmap_size[C.level & 15];
-    unsigned long long b = 0, acc = 0, dp = dpos, sp = spos;
-    for (long long i = 0; i < nbr; ++i)
+    unsigned long long gcur = gstart, scur = spos, acc = 0;
+    bool bad = false;
+    for (long long g0 = 0; g0 < nbr && !bad; g0 += 32)
     {
-      b = i == 0 ? bb.varbyte(dp) : b + bb.unary(dp) + 1;
-      const unsigned long long o = acc;
-      acc += bb.varbyte(sp);
+      const long long i = g0 + lane;
+      const bool live = i < nbr;
+      // gap ends: brick i > 0 needs the i-th one bit from gstart (the group's from gcur)
+      const int rr = !live || i == 0 ? 0 : (g0 == 0 ? lane : lane + 1);
+      const unsigned long long ge = warp_nth_each(bb, gcur, rr, limit, lane, [](uint32_t x) { return x; });
+      unsigned long long send = 0, size = 0;
+      if (PASS == 1)
+      {
+        // size ends: the (i + 1)-th varbyte final byte from spos (the group's from scur)
+        send = warp_nth_each(bb, scur, live ? lane + 1 : 0, limit, lane,
+                             [](uint32_t x) { return ~x & 0x80808080u; });
+        unsigned long long sbeg = __shfl_up_sync(0xffffffffu, send, 1);
+        sbeg = lane == 0 ? scur : sbeg;
+        if (live && send != kNone && sbeg != kNone)
+          size = bb.varbyte(sbeg);
+      }
+      if (__any_sync(0xffffffffu, live && (ge == kNone || (PASS == 1 && send == kNone))))
+      {
+        bad = true;
+        if (lane == 0)
+          atomicOr(a.error, 1);
+        break;
+      }
+      // exclusive sums of the sizes
+      unsigned long long incl = size;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1)
+      {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o)
+          incl += y;
+      }
+      const unsigned long long o = acc + incl - size;
+      acc += __shfl_sync(0xffffffffu, incl, 31);
+      gcur = __shfl_sync(0xffffffffu, ge, 31);
+      if (PASS == 1)
+        scur = __shfl_sync(0xffffffffu, send, 31);
+      if (!live)
+        continue;
+      const unsigned long long b = i == 0 ? first : first + (ge - gstart);
       if (b >= (unsigned long long)msize)
         continue;
       const int flat = a.bmap[base + (long long)b];
@@ -850,13 +952,17 @@ int decode_device::decode_batch(device_ctx* ctx, const std::vector<const decode_
         launch_planes(pa);
       if (split_level)
       {
-        // about 8 launches, each of whole rows of bricks; after launch g every output plane
-        // below the first plane of the bricks still to come is final
+        // about 9 launches, each of whole rows of bricks; after launch g every output plane
+        // below the first plane of the bricks still to come is final. The first band is a
+        // quarter of the others, so that the copies (which take longer than the kernels)
+        // start early.
         constexpr int kBands = 8;
         std::vector<int> cuts(1, 0);
-        for (int g = 1; g < kBands; ++g)
+        for (int g = 0; g < kBands; ++g)
         {
-          int c = (int)((long long)nbr * g / kBands);
+          if (g == 0 && nbr < 32)
+            continue;
+          int c = (int)(g == 0 ? (long long)nbr / 32 : (long long)nbr * g / kBands);
           while (c > 0 && c < nbr && hb[(size_t)c].dst_from[2] == hb[(size_t)c - 1].dst_from[2])
             ++c;
           if (c > cuts.back() && c < nbr)

@@ -123,3 +123,69 @@ def test_synth_of_dataset_coefficients_matches_decode(idx2g, tmp_path, dims, dty
     tol = 1e-12 if dtype == "float64" else 1e-5
     assert float(np.abs(xd - dec).max()) <= tol * scale
     ds.close()
+
+
+@pytest.mark.gpu
+def test_differentiable_decode_at_workload_sizes(idx2g, tmp_path):
+    """The differentiable-decode workload's sizes: float32 fields of 256^3 (two of the batch of
+    32; the fields of a batch are independent) and a float64 field of 128^3, 2 levels, seeded
+    k^-5/3 fields encoded at tolerance 1e-4. D of the dataset's coefficients against the
+    bit-exact decode; the float32 gradient of the MSE against the float64 adjoint of the same
+    residual; the dot-product identity in both precisions; FP64 central differences at 20
+    coefficients of the 128^3 field."""
+    import torch
+    from idx2_b200 import diff
+    from idx2_b200.synthetic import grf_field_torch
+    dev = torch.device("cuda", 0)
+
+    def batch(n, side, dtype, seed):
+        fmt = diff.Format((side, side, side), "float32" if dtype == torch.float32 else "float64", 2)
+        cs, decs = [], []
+        for i in range(n):
+            f = grf_field_torch(side, side, side, seed=seed + i, scale="unit", device=dev).to(dtype)
+            d = str(tmp_path / f"b{seed}_{i}")
+            idx2g.encode(f, out_dir=d, name="adj", field_name="f", num_levels=2, tolerance=1e-4)
+            ds = idx2g.Dataset(os.path.join(d, "adj", "f.idx2"))
+            cs.append(diff.coefficients(ds, fmt, 1e-4))
+            decs.append(torch.from_numpy(ds.decode(tolerance=1e-4)).to(dev))
+            ds.close()
+        return fmt, torch.stack(cs), torch.stack(decs)
+
+    fmt, c, dec = batch(2, 256, torch.float32, 300)
+    x = diff.synth(c, fmt)
+    assert float((x - dec).abs().max() / dec.abs().max()) <= 1e-5
+    target = torch.stack([grf_field_torch(256, 256, 256, seed=900 + i, scale="unit", device=dev) for i in range(2)])
+    g32 = diff.synth_adjoint(2.0 * (x - target) / x.numel(), fmt)
+    fmt64 = diff.Format(fmt.dims, "float64", 2)
+    x64 = diff.synth(c.double(), fmt64)
+    g64 = diff.synth_adjoint(2.0 * (x64 - target.double()) / x64.numel(), fmt64)
+    assert float((g32.double() - g64).abs().max() / g64.abs().max()) <= 1e-5
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(5)
+    y = torch.randn(target.shape, generator=gen, device=dev, dtype=torch.float64)
+    cd = torch.randn(c.shape, generator=gen, device=dev, dtype=torch.float64)
+    lhs, rhs = float(torch.sum(diff.synth(cd, fmt64) * y)), float(torch.sum(cd * diff.synth_adjoint(y, fmt64)))
+    assert abs(lhs - rhs) <= 1e-11 * abs(lhs)
+    lhs = float(torch.sum(diff.synth(cd.float(), fmt).double() * y))
+    rhs = float(torch.sum(cd * diff.synth_adjoint(y.float(), fmt).double()))
+    assert abs(lhs - rhs) <= 1e-4 * abs(lhs)
+    del x, x64, g32, g64, y, cd, target, c, dec
+
+    fmt_d, c_d, dec_d = batch(1, 128, torch.float64, 500)
+    x = diff.synth(c_d, fmt_d)
+    assert float((x - dec_d).abs().max() / dec_d.abs().max()) <= 1e-12
+    target = grf_field_torch(128, 128, 128, seed=1900, scale="unit", device=dev).double()[None]
+    grad = diff.synth_adjoint(2.0 * (x - target) / x.numel(), fmt_d)[0]
+    c0 = c_d[0].clone()
+    rng = np.random.default_rng(8)
+    idx = [int(i) for i in rng.permutation(np.nonzero(grad.abs().cpu().numpy() > 0)[0])[:20]]
+    h = 1e-3
+    for i in idx:
+        old = float(c0[i])
+        c0[i] = old + h
+        xp = diff.synth(c0, fmt_d)
+        c0[i] = old - h
+        xm = diff.synth(c0, fmt_d)
+        c0[i] = old
+        fd = float(torch.sum((xp - target[0]) ** 2 - (xm - target[0]) ** 2)) / x.numel() / (2 * h)
+        assert abs(fd - float(grad[i])) <= 1e-6 * abs(fd) + 1e-14, (i, fd, float(grad[i]))
