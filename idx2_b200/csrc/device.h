@@ -307,7 +307,12 @@ public:
   // Level 0 of one 3D field whose samples are in pinned host memory: bands of brick rows are
   // copied to `staged` on the context's copy stream, each band's launch waits for its copy
   // only. *nbands: launches made (timed by event pairs 2g, 2g + 1 of the context's pool).
+  // The coarser levels go in bands as well, between level 0's: a brick as soon as the band
+  // holding the last of its children has run (levels that are launched so: followed()).
   int enqueue_level0_streamed(const void* host, void* staged, int* nbands);
+  // Whether level l was launched with level 0's bands, and its launches' time once they ran.
+  bool followed(int l) const { return l > 0 && (size_t)l < follow_events_.size() && !follow_events_[(size_t)l].empty(); }
+  float followed_ms(int l) const;
   // While the bands of enqueue_level0_streamed run: as each band ends, its stream bytes go to
   // the level's pinned host buffer on the copy-out stream (when the buffer is already large
   // enough), so that collect_level finds them there.
@@ -335,6 +340,7 @@ private:
   std::string tag_;
   batch_tuning tune_;
   std::vector<std::unique_ptr<level_launch>> levels_;
+  std::vector<std::vector<int>> follow_events_;  // per level: event pairs of its band launches
   double kernel_ms_ = 0;
   long long launches_ = 0;
   long long graph_launches_ = 0;  // kernels in the cached graph of this batch's launches

@@ -1755,6 +1755,57 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
   cudaMemsetAsync(ll.d_misc, 0, 64, st);
   if (ll.nparents > 0)
     cudaMemsetAsync(ll.d_parents, 0, (size_t)ll.nparents * (size_t)kNB3 * 8, st);
+  // the coarser levels by bands of level 0: a brick's band is the latest band among its
+  // children (the bricks that hand it their low bands), its bricks ordered by band
+  follow_events_.assign(levels_.size(), {});
+  std::vector<std::vector<int>> up_cuts(levels_.size());
+  std::vector<int*> up_order(levels_.size(), nullptr);
+  {
+    std::vector<int> prev_band((size_t)nbr, 0);
+    for (int g = 0; g < nb; ++g)
+      for (int i = cuts[(size_t)g]; i < cuts[(size_t)g + 1]; ++i)
+        prev_band[(size_t)order[(size_t)i]] = g;
+    for (size_t l = 1; l < levels_.size(); ++l)
+    {
+      const level_launch& pl = *levels_[l - 1];
+      level_launch& ul = *levels_[l];
+      const int n = ul.args.nbricks;
+      if (ul.split || ul.fields.size() != 1 || ul.fields[0].is2d || n <= 0)
+        break;
+      std::vector<int> band((size_t)n, 0);
+      for (size_t j = 0; j < pl.bricks.size(); ++j)
+      {
+        const int par = pl.bricks[j].parent;
+        if (par >= 0 && par < n && prev_band[j] > band[(size_t)par])
+          band[(size_t)par] = prev_band[j];
+      }
+      std::vector<int> uo((size_t)n);
+      for (int i = 0; i < n; ++i)
+        uo[(size_t)i] = i;
+      std::stable_sort(uo.begin(), uo.end(), [&](int x, int y) { return band[(size_t)x] < band[(size_t)y]; });
+      std::vector<int>& uc = up_cuts[l];
+      uc.assign((size_t)nb + 1, n);
+      for (int g = 0, i = 0; g <= nb; ++g)
+      {
+        while (i < n && band[(size_t)uo[(size_t)i]] < g)
+          ++i;
+        uc[(size_t)g] = i;
+      }
+      char nm[32];
+      snprintf(nm, sizeof nm, "enc.order%zu", l);
+      int* d_uo = (int*)ctx_->ws(nm, (size_t)n * 4);
+      int* h_uo = (int*)ctx_->pinned(nm, (size_t)n * 4);
+      if (!d_uo || !h_uo)
+        return OutOfMemory;
+      memcpy(h_uo, uo.data(), (size_t)n * 4);
+      cudaMemcpyAsync(d_uo, h_uo, (size_t)n * 4, cudaMemcpyHostToDevice, st);
+      up_order[l] = d_uo;
+      cudaMemsetAsync(ul.d_misc, 0, 64, st);
+      if (ul.nparents > 0)
+        cudaMemsetAsync(ul.d_parents, 0, (size_t)ul.nparents * (size_t)kNB3 * 8, st);
+      prev_band.swap(band);
+    }
+  }
   // the copy stream starts after the work already on the stream (the staging buffer may
   // still be read by it)
   cudaEvent_t start = ctx_->ev(127);
@@ -1804,9 +1855,45 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
     cudaEventRecord(tc, st);
     ++launches_;
     ++ctx_->launches;
+    // the coarser levels' bricks whose children have all run
+    for (size_t l = 1; l < levels_.size() && up_order[l]; ++l)
+    {
+      const int u0 = up_cuts[l][(size_t)g], u1 = up_cuts[l][(size_t)g + 1];
+      if (u1 <= u0)
+        continue;
+      level_launch& ul = *levels_[l];
+      const int ev = 256 + 2 * (int)(l - 1) * 32 + 2 * g;
+      cudaEvent_t u_t0 = ctx_->ev((size_t)ev), u_t1 = ctx_->ev((size_t)ev + 1);
+      if (!u_t0 || !u_t1)
+        return CudaError;
+      cudaEventRecord(u_t0, st);
+      enc_args ua = ul.args;
+      ua.first = u0;
+      ua.last = u1;
+      ua.order = up_order[l];
+      enc_kernel(ul.three)<<<u1 - u0 < ul.grid ? u1 - u0 : ul.grid, kThreads, ul.smem, st>>>(ua);
+      cudaEventRecord(u_t1, st);
+      follow_events_[l].push_back(ev);
+      ++launches_;
+      ++ctx_->launches;
+    }
   }
   *nbands = nb;
   return cudaGetLastError() == cudaSuccess ? NoError : CudaError;
+}
+
+float batch_encoder::followed_ms(int l) const
+{
+  float total = 0;
+  if (l <= 0 || (size_t)l >= follow_events_.size())
+    return 0;
+  for (int ev : follow_events_[(size_t)l])
+  {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx_->ev((size_t)ev), ctx_->ev((size_t)ev + 1));
+    total += ms;
+  }
+  return total;
 }
 
 void batch_encoder::stream_out_level0(int nbands)
@@ -2153,6 +2240,13 @@ int gpu_coder::run_level(int level, const encode_plan& plan, level_output* out)
       cudaEventElapsedTime(&m, ctx_->ev(2 * (size_t)g), ctx_->ev(2 * (size_t)g + 1));
       ms += m;
     }
+  }
+  else if (enc_->followed(level))
+  {
+    // launched with level 0's bands
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return CudaError;
+    ms = enc_->followed_ms(level);
   }
   else
   {
