@@ -212,12 +212,13 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     extent eb{ vol.from / b3, vol.last() / b3 - vol.from / b3 + v3(1) };
     extent ec{ vol.from / c3, vol.last() / c3 - vol.from / c3 + v3(1) };
     extent ef{ vol.from / fl3, vol.last() / fl3 - vol.from / fl3 + v3(1) };
+    const brick_linearizer lin_of(f, l, f.nbricks3[(size_t)l]);
     traverse(f.files_order[(size_t)l], v3(0), f.nfiles3[(size_t)l], ef, ef, [&](const traverse_item& fi) {
       traverse(f.chunks_order_in_file[(size_t)l], fi.from3 * f.chunks_per_file3[(size_t)l],
                f.chunks_per_file3[(size_t)l], ec, ec, [&](const traverse_item& ci) {
                  traverse(f.bricks_order_in_chunk[(size_t)l], ci.from3 * f.bricks_per_chunk3[(size_t)l],
                           f.bricks_per_chunk3[(size_t)l], eb, eb, [&](const traverse_item& bi) {
-                            u64 lin = linear_brick(f, l, bi.from3);
+                            u64 lin = lin_of(bi.from3);
                             if (lin >= nlin || h->brick_index[(size_t)l][lin] >= 0)
                               return;
                             h->brick_index[(size_t)l][lin] = (int)h->brick3[(size_t)l].size();
@@ -263,9 +264,10 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
     shift = shift < 0 ? 0 : shift > 63 ? 63 : shift;
     h->file_shift[(size_t)l] = shift;
     u64 prev = ~0ull;
+    const brick_linearizer lin_of(f, l, f.nbricks3[(size_t)l]);
     for (size_t i = 0; i < h->brick3[(size_t)l].size(); ++i)
     {
-      const u64 lin = linear_brick(f, l, h->brick3[(size_t)l][i]);
+      const u64 lin = lin_of(h->brick3[(size_t)l][i]);
       if ((lin >> shift) == prev)
         continue;
       prev = lin >> shift;
@@ -294,9 +296,10 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
   }
 
   tt.lap("open.files");
-  // every file into one pinned buffer, in ranges of 16 MB read by a pool of threads; each
+  // every file into one pinned buffer, in ranges of 4 MB read by a pool of threads; each
   // range goes on to the device as soon as it is read, while the other threads read on and
-  // the index below is built
+  // the index below is built (small ranges, so that the first copy starts after a few MB
+  // rather than after a whole round of the threads' reads)
   uint8_t* blob = (uint8_t*)ctx->pinned("dec.files", total + 16);
   if (!blob)
     return OutOfMemory;
@@ -310,7 +313,7 @@ static int load_index(device_ctx* ctx, dataset_handle* h)
       size_t off, n;
     };
     std::vector<range> rs;
-    const size_t R = (size_t)16 << 20;
+    const size_t R = (size_t)4 << 20;
     for (size_t i = 0; i < files.size(); ++i)
       for (size_t o = 0; o < files[i].size; o += R)
         rs.push_back({ (int)i, o, std::min(R, files[i].size - o) });
@@ -658,12 +661,14 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
         lv.spacing[s][d] = f.decode_spacings[(size_t)l][(size_t)s][d];
     // the exponent chunk of each subband that was found last (bricks of a chunk come in runs)
     std::vector<u64> chunk_seen((size_t)nsb, ~0ull);
+    const brick_linearizer lin_of(f, l, f.nbricks3[(size_t)l]);
+    const brick_linearizer plin_of(f, l + 1 < L ? l + 1 : l, l + 1 < L ? f.nbricks3[(size_t)l + 1] : v3(0));
     for (int bz = bf.z; bz <= bl.z; ++bz)
       for (int by = bf.y; by <= bl.y; ++by)
         for (int bx = bf.x; bx <= bl.x; ++bx)
         {
           v3 b(bx, by, bz);
-          u64 lin = linear_brick(f, l, b);
+          u64 lin = lin_of(b);
           if (lin >= h->brick_index[(size_t)l].size())
             continue;
           int bi = h->brick_index[(size_t)l][lin];
@@ -696,7 +701,7 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
           if (l + 1 < L)
           {
             v3 pb = b / f.group_brick3;
-            u64 plin = linear_brick(f, l + 1, pb);
+            u64 plin = plin_of(pb);
             int pbi = plin < h->brick_index[(size_t)l + 1].size() ? h->brick_index[(size_t)l + 1][plin] : -1;
             db.parent = pbi >= 0 && (size_t)pbi < pos_of[(size_t)l + 1].size() ? pos_of[(size_t)l + 1][(size_t)pbi] : -1;
             v3 lp = b % f.group_brick3;

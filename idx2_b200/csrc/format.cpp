@@ -507,6 +507,21 @@ u64 linear_brick(const dataset_format& f, int level, v3 b3)
   return r;
 }
 
+brick_linearizer::brick_linearizer(const dataset_format& fmt, int l, v3 n) : f(&fmt), level(l)
+{
+  for (int d = 0; d < 3; ++d)
+  {
+    const int m = n[d] > 0 ? n[d] : 0;
+    t[d].resize((size_t)m);
+    for (int c = 0; c < m; ++c)
+    {
+      v3 b(0);
+      b[d] = c;
+      t[d][(size_t)c] = linear_brick(fmt, l, b);
+    }
+  }
+}
+
 v3 spatial_brick(const dataset_format& f, int level, u64 lin)
 {
   const std::string& s = f.bricks_order_str[level];

@@ -206,6 +206,21 @@ int finalize_read(dataset_format* f, params* p);
 
 // Linear brick index on a level (Core/idx2Lookup.cpp:13 GetLinearBrick).
 u64 linear_brick(const dataset_format& f, int level, v3 brick3);
+// linear_brick of a level by table: the index interleaves the axes' bits, so it is the OR of
+// one entry per axis (tables for coordinates below n[d]; larger ones fall back to the loop).
+struct brick_linearizer
+{
+  const dataset_format* f = nullptr;
+  int level = 0;
+  std::vector<u64> t[3];
+  brick_linearizer(const dataset_format& fmt, int l, v3 n);
+  u64 operator()(v3 b) const
+  {
+    if ((unsigned)b.x < t[0].size() && (unsigned)b.y < t[1].size() && (unsigned)b.z < t[2].size())
+      return t[0][(size_t)b.x] | t[1][(size_t)b.y] | t[2][(size_t)b.z];
+    return linear_brick(*f, level, b);
+  }
+};
 v3 spatial_brick(const dataset_format& f, int level, u64 linear);
 
 // Addresses (Core/idx2Lookup.h:16-59).

@@ -60,3 +60,21 @@ def test_error_names(idx2g):
     assert idx2g.error_string(22) == "BrickSizeTooBig"
     assert idx2g.error_string(23) == "TooManyLevels"
     assert idx2g.error_string(37) == "FileNotFound"
+
+
+def test_brick_linearizer_equals_linear_brick():
+    """The table form of the linear brick index (used by the decode plan) gives linear_brick's
+    index for every brick of every level, and past the tables, over 3D and 2D shapes with
+    unequal sides and partial bricks."""
+    build = os.path.join(HERE, "_build")
+    os.makedirs(build, exist_ok=True)
+    exe = os.path.join(build, "linearizer_check")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-I" + os.path.join(ROOT, "idx2_b200", "csrc"),
+                    os.path.join(HERE, "cpp", "linearizer_check.cpp"),
+                    os.path.join(ROOT, "idx2_b200", "csrc", "format.cpp"), "-o", exe], check=True)
+    cases = ["256 256 256 32 32 32 3", "1024 512 300 32 32 32 3", "100 90 75 32 32 32 2", "300 200 1 32 32 1 2",
+             "65 66 97 32 32 32 2", "513 257 129 16 16 16 4"]
+    out = subprocess.run([exe], input="\n".join(cases) + "\n", capture_output=True, text=True)
+    rows = out.stdout.split("\n")[:len(cases)]
+    assert out.returncode == 0, out.stdout
+    assert all(r.startswith("ok ") and int(r.split()[1]) > 0 for r in rows), rows
