@@ -1862,8 +1862,8 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
       if (u1 <= u0)
         continue;
       level_launch& ul = *levels_[l];
-      const int ev = 256 + 2 * (int)(l - 1) * 32 + 2 * g;
-      cudaEvent_t u_t0 = ctx_->ev((size_t)ev), u_t1 = ctx_->ev((size_t)ev + 1);
+      const int evi = 256 + 2 * (int)(l - 1) * 32 + 2 * g;  // (an event pair per level and band)
+      cudaEvent_t u_t0 = ctx_->ev((size_t)evi), u_t1 = ctx_->ev((size_t)evi + 1);
       if (!u_t0 || !u_t1)
         return CudaError;
       cudaEventRecord(u_t0, st);
@@ -1873,7 +1873,7 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
       ua.order = up_order[l];
       enc_kernel(ul.three)<<<u1 - u0 < ul.grid ? u1 - u0 : ul.grid, kThreads, ul.smem, st>>>(ua);
       cudaEventRecord(u_t1, st);
-      follow_events_[l].push_back(ev);
+      follow_events_[l].push_back(evi);
       ++launches_;
       ++ctx_->launches;
     }
