@@ -51,10 +51,11 @@ LEVELS = 3
 TOL = 1e-3
 METRIC = "encode+decode GB/s (raw field bytes) at 1e-3 tol"
 # DRAM bytes (read + write) of one level-0 k_encode_level launch per brick, from an ncu capture
-# of the grf512 workload (4,096 bricks: 2.268 GB read + 2.807 GB written); the traffic of a
-# launch grows with its bricks (every brick makes the same slot sweeps), so a full launch's
-# traffic is this figure times its bricks.
-ENC_L0_TRAFFIC_PER_BRICK = (2.267987e9 + 2.807463e9) / 4096
+# of the grf512 workload (the three-CTA build, 444 CTAs, 4,096 bricks: 5.277 GB read + 4.294 GB
+# written; the CTAs' FP64 brick slots, 122 MB, no longer fit in L2 beside the streams); the
+# traffic of a launch grows with its bricks (every brick makes the same slot sweeps on the same
+# grid), so a full launch's traffic is this figure times its bricks.
+ENC_L0_TRAFFIC_PER_BRICK = (5.277031e9 + 4.294031e9) / 4096
 # FP64 operations of one level-0 k_encode_level launch per brick, from the same kind of ncu
 # capture (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum: 2,872,791,040 adds,
 # 1,577,402,368 multiplies, no fused multiply-adds over 4,096 bricks); every brick runs the same
