@@ -95,7 +95,8 @@ public:
   void upload_blob(device_ctx* ctx, const uint8_t* src, size_t offset, size_t bytes);
   // The channel tables, built on the device (after every upload_blob): the chunk
   // headers in the blob (Core/idx2Decode.cpp:507 DecompressChunk: varbyte NBricks, the first
-  // brick as a varbyte then unary gaps, varbyte sizes) are read a chunk per thread, twice:
+  // brick as a varbyte then unary gaps, varbyte sizes) are read a warp per chunk and a lane per
+  // brick, twice:
   // the key range of every (brick, subband) slot, an exclusive scan of the slots' key counts,
   // then each brick's data offset. brick_map: per level (from level_base[l], level_size[l]
   // entries) the flat brick of each linear brick index, or -1. Then the exponents go up.
