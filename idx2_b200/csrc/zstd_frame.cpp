@@ -1153,14 +1153,19 @@ size_t block_body(std::vector<u8>* out, const std::vector<sequence>& seqs, const
       bw.flush();
       for (size_t n = nseq - 1; n-- > 0;)
       {
+        // (at most 7 + 26 bits held after the states; the length and offset bits flushed
+        // ahead only when they would not fit, as they mostly do)
         fse_put(bw, sof, ofc[n]);
         fse_put(bw, sml, mlc[n]);
         fse_put(bw, sll, llc[n]);
-        bw.flush();
-        bw.put(seqs[n].ll, kLLBits[llc[n]]);
-        bw.put(seqs[n].mlb, kMLBits[mlc[n]]);
-        bw.flush();
-        bw.put(seqs[n].off, ofc[n]);
+        const unsigned llb = kLLBits[llc[n]], mlb = kMLBits[mlc[n]], ofb = ofc[n];
+        if (bw.n + llb + mlb >= 64)
+          bw.flush();
+        bw.put(seqs[n].ll, llb);
+        bw.put(seqs[n].mlb, mlb);
+        if (bw.n + ofb >= 64)
+          bw.flush();
+        bw.put(seqs[n].off, ofb);
         bw.flush();
       }
       fse_finish(bw, sml);
@@ -1193,6 +1198,7 @@ struct matcher
   std::vector<u32> hash;
   u32 hlog, mls, wlog;
   const u8* data;  // the frame's input; byte p has index p + 1
+  size_t size = 0;  // its bytes
   template <u32 MLS>
   size_t hpos(size_t p) const
   {
@@ -1233,7 +1239,7 @@ struct matcher
   {
     // room for the worst case (a sequence per 4 bytes, every byte a literal), cut after
     seqs->resize((be - bs) / 3 + 2);
-    lits->resize(be - bs + 8);
+    lits->resize(be - bs + 16);  // (+16: literal runs are copied 16 bytes at a time)
     size_t ns = 0, nl = 0;
     switch (mls)
     {
@@ -1285,7 +1291,12 @@ struct matcher
     }
     size_t ns = 0, nl = 0;
     auto store = [&](long long ll, long long from, u32 off_value, long long mlb) {
-      memcpy(lit_out + nl, data + from, (size_t)ll);
+      // short runs as one 16-byte copy where the input has those bytes (the bytes past the run
+      // land in the literal buffer's slack and are overwritten or cut)
+      if (ll <= 16 && (size_t)from + 16 <= size)
+        memcpy(lit_out + nl, data + from, 16);
+      else
+        memcpy(lit_out + nl, data + from, (size_t)ll);
       nl += (size_t)ll;
       seq_out[ns++] = sequence{ (u32)ll, (u32)mlb, off_value };
     };
@@ -1448,6 +1459,7 @@ void compress(const uint8_t* src, size_t n, std::vector<uint8_t>* out)
   m.mls = p.mls;
   m.wlog = p.wlog;
   m.data = src;
+  m.size = n;
   m.hash.assign((size_t)1 << p.hlog, 0);
   const size_t block_size = std::min(kBlockMax, (size_t)1 << p.wlog);
   entropy_state prev;
