@@ -663,6 +663,12 @@ int plan_decode(const dataset_handle* h, const params& p, decode_request* rq_out
     std::vector<u64> chunk_seen((size_t)nsb, ~0ull);
     const brick_linearizer lin_of(f, l, f.nbricks3[(size_t)l]);
     const brick_linearizer plin_of(f, l + 1 < L ? l + 1 : l, l + 1 < L ? f.nbricks3[(size_t)l + 1] : v3(0));
+    if (bl.x >= bf.x && bl.y >= bf.y && bl.z >= bf.z)
+    {
+      const size_t nbox = (size_t)(bl.x - bf.x + 1) * (size_t)(bl.y - bf.y + 1) * (size_t)(bl.z - bf.z + 1);
+      lv.bricks.reserve(nbox);
+      lv.b3.reserve(nbox);
+    }
     for (int bz = bf.z; bz <= bl.z; ++bz)
       for (int by = bf.y; by <= bl.y; ++by)
         for (int bx = bf.x; bx <= bl.x; ++bx)
