@@ -13,6 +13,7 @@
 // bump; the host packer reads them back by offset.
 #include "codec_device.cuh"
 #include "device.h"
+#include "band_plan.h"
 #include "encoder.h"
 #include "trace.h"
 
@@ -1772,25 +1773,12 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
       const int n = ul.args.nbricks;
       if (ul.split || ul.fields.size() != 1 || ul.fields[0].is2d || n <= 0)
         break;
-      std::vector<int> band((size_t)n, 0);
+      std::vector<int> parent_of(pl.bricks.size());
       for (size_t j = 0; j < pl.bricks.size(); ++j)
-      {
-        const int par = pl.bricks[j].parent;
-        if (par >= 0 && par < n && prev_band[j] > band[(size_t)par])
-          band[(size_t)par] = prev_band[j];
-      }
-      std::vector<int> uo((size_t)n);
-      for (int i = 0; i < n; ++i)
-        uo[(size_t)i] = i;
-      std::stable_sort(uo.begin(), uo.end(), [&](int x, int y) { return band[(size_t)x] < band[(size_t)y]; });
-      std::vector<int>& uc = up_cuts[l];
-      uc.assign((size_t)nb + 1, n);
-      for (int g = 0, i = 0; g <= nb; ++g)
-      {
-        while (i < n && band[(size_t)uo[(size_t)i]] < g)
-          ++i;
-        uc[(size_t)g] = i;
-      }
+        parent_of[j] = pl.bricks[j].parent;
+      level_bands lb = follow_bands(prev_band, parent_of, n, nb);
+      const std::vector<int>& uo = lb.order;
+      up_cuts[l] = lb.cuts;
       char nm[32];
       snprintf(nm, sizeof nm, "enc.order%zu", l);
       int* d_uo = (int*)ctx_->ws(nm, (size_t)n * 4);
@@ -1803,7 +1791,7 @@ int batch_encoder::enqueue_level0_streamed(const void* host, void* staged, int* 
       cudaMemsetAsync(ul.d_misc, 0, 64, st);
       if (ul.nparents > 0)
         cudaMemsetAsync(ul.d_parents, 0, (size_t)ul.nparents * (size_t)kNB3 * 8, st);
-      prev_band.swap(band);
+      prev_band.swap(lb.band);
     }
   }
   // the copy stream starts after the work already on the stream (the staging buffer may
